@@ -1,0 +1,383 @@
+#!/usr/bin/env python
+"""Benchmark of the coupled fluid-membrane step on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload dense|single] [--storage f32|f16]
+
+Workload (default): the 256 x 128 x 128 duct with 200 subdivision-4 red cells
+(4,064,256 fluid nodes, 512,400 vertices).  A step is one full coupled step
+(membrane forces, spreading, collide-stream, RK4 advection, volume correction).
+
+value   device-timed MLUPS (fluid-node updates per second) of K steps with the
+        state resident in HBM, CUDA events on the library's stream, barrier and
+        synchronize on both sides, max over ranks.  The lattice (0.65 GB) is
+        larger than L2, so no flush is needed between steps.
+e2e     the same metric through the public C ABI with host buffers: import of
+        the reference-layout FP64 state from pinned memory, K steps each
+        followed by a device->host read of the per-cell volume/area/centroid,
+        and a final export of the vertex positions, all inside the timed region.
+roofline  the collide-stream kernel's algorithmic bytes (180 B/LU in FP32,
+        104 B/LU in FP16) over its average launch time, from CUDA events around
+        each kernel in profiled steps on the same stream, against the measured
+        HBM copy bandwidth.
+With N > 1 each rank runs an independent replica (weak scaling): the step has no
+cross-rank exchange, so no collective is on the data path.
+--impl reference times the FP64 CPU oracle (the reference has no CPU
+implementation of the step) on the host cores, rank 0 only.
+"""
+import argparse
+import json
+import math
+import os
+import re
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "MLUPS + membrane vertices/s at stated FP64 error; FP16/batched vs plain FP32, 1 B200"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="dense", choices=["dense", "single"])
+    ap.add_argument("--storage", default="f32", choices=["f32", "f16"])
+    ap.add_argument("--profile-steps", type=int, default=20)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU-baseline sample budget")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def make_case(workload, seed_offset=0, storage="f32"):
+    from preprocess_src_b200 import configs
+    st = 1 if storage == "f16" else 0
+    if workload == "single":
+        return configs.single_cell_duct(seed=1 + seed_offset, storage=st)
+    return configs.dense_suspension(seed=2 + seed_offset, storage=st)
+
+
+def measured_hbm():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+def ncu_traffic(workload, storage):
+    """Per-launch DRAM bytes of the collide-stream kernel from the committed
+    ncu summary (line 'traffic_bytes_per_launch[<workload>/<storage>]: N')."""
+    for f in sorted((ROOT / "profiles").glob("*.md")):
+        m = re.search(rf"traffic_bytes_per_launch\[{workload}/{storage}\]:\s*([0-9.eE+]+)", f.read_text())
+        if m:
+            return float(m.group(1))
+    return None
+
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.gpu)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": smax, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        backend = "nccl" if args.impl == "ours" else "gloo"
+        if backend == "nccl":
+            import torch
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+    return world, rank, local
+
+
+def allreduce_max(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def cpu_sample(case, budget_s, warm=1):
+    """FP64 CPU oracle on the same workload: whole steps until the budget."""
+    from oracle.oracle import Oracle, num_threads
+    o = Oracle(case)
+    o.step(warm)
+    t0 = time.perf_counter()
+    n = 0
+    while True:
+        o.step(1)
+        n += 1
+        el = time.perf_counter() - t0
+        if el >= budget_s:
+            break
+    fl = case.fluid_nodes()
+    return {"value": fl * n / el / 1e6, "unit": "MLUPS", "cores": num_threads(), "kind": "port",
+            "sample": f"{n} full FP64 oracle steps of {case.name} after {warm} warm-up step(s), {el:.1f} s"}
+
+
+def run_ours(args, world, rank, local):
+    import numpy as np
+    import torch
+
+    from preprocess_src_b200.step import Simulation
+
+    case = make_case(args.workload, seed_offset=rank, storage=args.storage)
+    dev = local
+    sim = Simulation(case, device=dev)
+    fluid, nv = case.fluid_nodes(), case.ncell * case.vertex
+    stream = torch.cuda.ExternalStream(sim.stream, device=torch.device("cuda", dev))
+    torch.cuda.set_device(dev)
+
+    sim.step(args.warmup)
+    sim.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    l0 = sim.launches
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(dev) as clk:
+        time.sleep(0.3)
+        ev0.record(stream)
+        sim.step(args.steps)
+        ev1.record(stream)
+        ev1.synchronize()
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    launches = sim.launches - l0
+    ms_max = allreduce_max(ms, world)
+    flags, vcmax = sim.status()
+
+    # per-kernel device times (profiled steps, events around each kernel)
+    kern = sim.profile_steps(args.profile_steps)
+    lbm_ms = kern["lbm_collide_stream"] / args.profile_steps
+    bytes_lu = 104 if args.storage == "f16" else 180
+    achieved = bytes_lu * fluid / (lbm_ms * 1e-3) / 1e9
+    peak, peak_kind = measured_hbm()
+    traffic = ncu_traffic(args.workload, args.storage)
+
+    e2e = None
+    if not args.no_e2e:
+        e2e = run_e2e(args, case, dev, world)
+
+    result = None
+    if rank == 0:
+        value = world * fluid * args.steps / (ms_max * 1e-3) / 1e6
+        step_total = sum(kern.values()) / args.profile_steps
+        result = {
+            "metric": METRIC, "value": round(value, 2), "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 5), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": args.storage, "data": "synthetic",
+            "config": {"workload": case.name, "lattice_duct": f"{case.meta['flow']}x{case.meta['Ly']}x{case.meta['Lz']}",
+                       "fluid_nodes": fluid, "cells": case.ncell, "vertices_per_cell": case.vertex,
+                       "population_storage": args.storage, "positions": "f64", "volume_correction": "f64",
+                       "l2": "inputs larger than L2 (populations 2 x %.2f GB), no flush" % (19 * (4 if args.storage == 'f32' else 2) * case.nx * case.ny * (case.nz - 4) / 1e9),
+                       "parallelism": f"replicas x{world}" if world > 1 else "single"},
+            "vertices_per_s": round(world * nv * args.steps / (ms_max * 1e-3), 1),
+            "gpu_launches": launches,
+            "kernel_ms_per_step": {k: round(v / args.profile_steps, 5) for k, v in kern.items()},
+            "kernel_sum_ms_per_step": round(step_total, 5),
+            "roofline": {"bound": "hbm", "kernel": "lbm_collide_stream", "achieved": round(achieved, 1),
+                         "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                         "bytes_per_lu": bytes_lu, "lus_per_launch": fluid,
+                         "traffic": traffic},
+            "status_flags": flags, "vc_iters_max": vcmax,
+            "clocks": clk.summary(),
+        }
+        if e2e:
+            result["e2e"] = e2e
+        if world == 1 and not args.no_cpu:
+            result["cpu_baseline"] = cpu_sample(case, args.cpu_seconds)
+    sim.close()
+    return result
+
+
+def run_e2e(args, case, dev, world):
+    """Public-API run with host buffers (pinned), copies inside the timed region."""
+    import numpy as np
+    import torch
+
+    from preprocess_src_b200.step import Simulation
+
+    n, nv, ne, nc = case.n, case.ncell * case.vertex, case.ncell * case.element, case.ncell
+
+    def pinned(count):
+        return torch.empty(count, dtype=torch.float64, pin_memory=True).numpy()
+
+    # reference-layout initial state: rest equilibrium and the initial cells
+    w = np.array([1 / 3] + [1 / 18] * 6 + [1 / 36] * 12)
+    fn = pinned(n * 19)
+    fn.reshape(n, 19)[:] = w
+    xr = np.asarray(case.xr).reshape(-1, 3)
+    x, y, z, xd = pinned(nv), pinned(nv), pinned(nv), pinned(3 * nv)
+    x[:], y[:], z[:] = xr[:, 0], xr[:, 1], xr[:, 2]
+    xd[:] = case.xr
+    nd = pinned(4 * ne)
+    sim = Simulation(case, device=dev)
+    # reference metric as fem_init computes it (the import replaces the handle's own)
+    a, b, c = xr[case.ele_global()[0::3]], xr[case.ele_global()[1::3]], xr[case.ele_global()[2::3]]
+    v1, v2 = b - a, c - a
+    l1, l2, i12 = (v1 * v1).sum(1), (v2 * v2).sum(1), (v1 * v2).sum(1)
+    dv = l1 * l2 - i12 * i12
+    nd.reshape(-1, 4)[:] = np.stack([l2 / dv, -i12 / dv, -i12 / dv, l1 / dv], axis=1)
+    met = sim.cell_metrics()
+    vol0, gx = pinned(nc), pinned(3 * nc)
+    vol0[:], gx[:] = met["volume"], met["centroid"]
+    out_v, out_a, out_c = pinned(nc), pinned(nc), pinned(3 * nc)
+    ox, oy, oz = pinned(nv), pinned(nv), pinned(nv)
+    stream = torch.cuda.ExternalStream(sim.stream, device=torch.device("cuda", dev))
+    import ctypes as C
+
+    from preprocess_src_b200 import _native as N
+    L, h = N.lib(), sim._h
+    dp = lambda arr: arr.ctypes.data_as(N._DP)  # noqa: E731
+    sim.step(2)     # build the step graphs outside the timed region
+    sim.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0 = time.perf_counter()
+    ev0.record(stream)
+    N.check(L.rbc_import_ref_lattice(h, dp(fn)), h)
+    N.check(L.rbc_import_ref_cells(h, dp(x), dp(y), dp(z), dp(xd), dp(nd), dp(vol0), dp(gx)), h)
+    N.check(L.rbc_set_iter(h, 0), h)
+    for _ in range(args.steps):
+        N.check(L.rbc_step(h, 1), h)
+        N.check(L.rbc_cell_metrics(h, dp(out_v), dp(out_a), dp(out_c)), h)
+    N.check(L.rbc_export_ref_cells(h, dp(ox), dp(oy), dp(oz), None, None, None, None, None, None, None, None), h)
+    ev1.record(stream)
+    ev1.synchronize()
+    wall = time.perf_counter() - t0
+    ms = allreduce_max(ev0.elapsed_time(ev1), world)
+    fluid = case.fluid_nodes()
+    h2d = (fn.nbytes + x.nbytes * 3 + xd.nbytes + nd.nbytes + vol0.nbytes + gx.nbytes) / args.steps
+    d2h = (out_v.nbytes + out_a.nbytes + out_c.nbytes) + (ox.nbytes * 3) / args.steps
+    sim.close()
+    return {"value": round(world * fluid * args.steps / (ms * 1e-3) / 1e6, 2), "unit": "MLUPS",
+            "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "wall_s": round(wall, 4),
+            "path": "rbc_import_ref_lattice + rbc_import_ref_cells + K x (rbc_step(1) + rbc_cell_metrics) + "
+                    "rbc_export_ref_cells, pinned host buffers"}
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return None
+    case = make_case(args.workload)
+    from oracle.oracle import Oracle, num_threads
+    o = Oracle(case)
+    budget = 150.0
+    t_start = time.perf_counter()
+    o.step(max(1, min(args.warmup, 2)))
+    warm_s = time.perf_counter() - t_start
+    per = warm_s / max(1, min(args.warmup, 2))
+    steps = max(1, min(args.steps, int(budget / max(per, 1e-9))))
+    t0 = time.perf_counter()
+    o.step(steps)
+    el = time.perf_counter() - t0
+    fluid = case.fluid_nodes()
+    value = fluid * steps / el / 1e6
+    sample = (f"{steps} full FP64 oracle steps of {case.name} ({el:.1f} s, capped by a {budget:.0f} s budget); "
+              "the reference implements the step only as CUDA kernels, so its CPU arm is the oracle port")
+    return {"metric": METRIC, "impl": "reference", "value": round(value, 4), "unit": "MLUPS", "n_gpus": world,
+            "steps": steps, "warmup": min(args.warmup, 2), "ms_per_step": round(el / steps * 1e3, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": case.name, "fluid_nodes": fluid, "cells": case.ncell,
+                       "vertices_per_cell": case.vertex},
+            "vertices_per_s": round(case.ncell * case.vertex * steps / el, 1),
+            "cpu_baseline": {"value": round(value, 4), "unit": "MLUPS", "cores": num_threads(), "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": round(value, 4), "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        world, rank = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0"))
+        res = run_reference(args, world, rank)
+        if res is not None:
+            print(json.dumps(res), flush=True)
+        return
+    world, rank, local = dist_setup(args)
+    res = run_ours(args, world, rank, local)
+    if res is not None:
+        print(json.dumps(res), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,197 @@
+/*
+ * rbc_step.h -- C ABI of the B200-native coupled fluid-membrane time step.
+ *
+ * One handle owns the device state of one simulation: a D3Q19 lattice stored
+ * as pull-scheme SoA populations (f_i - w_i, FP32 or FP16), the Eulerian IB
+ * force and velocity fields, and the red-cell meshes (FP64 positions, shared
+ * triangle connectivity, per-element reference metric).
+ *
+ * The step entry points replace the reference's step modules one for one and
+ * keep their order and side effects (enomoto-catallaxy/preProcess_src):
+ *
+ *   rbc_stress             <- void stress(process*, domain*, cell*, fem*, lattice*)  stress.cu:580
+ *   rbc_ibm_st1            <- void ibm_st1(domain*, lattice*, cell*)                 ibm.cu:299
+ *   rbc_lbm_d3q19          <- void lbm_d3q19(process*, domain*, lattice*)            lbm.cu:1463
+ *   rbc_ibm_st2            <- void ibm_st2(domain*, lattice*, cell*, fem*)           ibm.cu:642
+ *   rbc_volume_correction  <- int  volume_correction(domain*, cell*, fem*)           volume_correction.cu:453
+ *   rbc_step               <- the time loop of main.cu:73-110 (M = 1)
+ *
+ * The reference's setup that defines the step inputs (cdo_init bc map,
+ * flu_init equilibrium, fem_init link tables and reference metric,
+ * volume_init) happens in rbc_create; the rbc_import_ref_* / rbc_export_ref_*
+ * calls move state in and out in the reference's own layouts (AoS FP64
+ * populations fn[i*19+q] with BUFF planes, SoA cel->x/y/z, AoS fem->xd,
+ * fem->nd[4*e+k]).
+ *
+ * Frame and units follow the reference's CapsuleCHANNELFLOW mode: the lattice
+ * is nx * ny * nz nodes with x fastest, z is the periodic flow axis with two
+ * BUFF planes at each end, node (ix,iy,iz) sits at physical position
+ * (ix*dx - (nx-1)dx/2, iy*dx - (ny-1)dx/2, iz*dx - (nz-1)dx/2).  The wall and
+ * fluid pattern must be the same in every z plane, as the reference's channel
+ * builds it (init1.cu:219-234).
+ *
+ * Every call returns an int status (RBC_OK = 0).  Nothing calls exit().
+ * All device work of a handle runs on one CUDA stream; calls are asynchronous
+ * unless stated.  Calls on one handle must not be made from two host threads
+ * at the same time.
+ */
+#ifndef RBC_STEP_H
+#define RBC_STEP_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define RBC_OK                 0
+#define RBC_ERR_ARG            1   /* bad argument or size */
+#define RBC_ERR_CUDA           2   /* CUDA runtime error (see rbc_last_error) */
+#define RBC_ERR_UNSUPPORTED    3   /* option outside the implemented scope */
+#define RBC_ERR_TOPOLOGY       4   /* mesh link check failed (reference error(3), init2.cu:370) */
+#define RBC_ERR_NOT_CONVERGED  5   /* volume correction hit 1000 iterations (reference exit(1)) */
+#define RBC_ERR_NONFINITE      6   /* non-finite vertex position detected */
+#define RBC_ERR_STATE          7   /* call out of order (e.g. no cells) */
+#define RBC_ERR_NO_DEVICE      8   /* no CUDA device */
+
+/* node types of the reference bc[] map (the reference's def.h values are not
+ * published; these are the values this library and its tools use) */
+#define RBC_COMP 0
+#define RBC_BUFF 1
+#define RBC_WALL 2
+
+/* population storage in HBM */
+#define RBC_STORE_F32 0            /* f_i - w_i in FP32: 180 B per lattice update */
+#define RBC_STORE_F16 1            /* (f_i - w_i) * scale in FP16: 104 B per lattice update */
+
+/* membrane constitutive law (stress.cu:94-99) */
+#define RBC_LAW_SKALAK     0
+#define RBC_LAW_NEOHOOKEAN 1
+
+/* device status flags (rbc_get_status) */
+#define RBC_FLAG_VC_NOT_CONVERGED  0x1
+#define RBC_FLAG_NONFINITE         0x2
+#define RBC_FLAG_SPREAD_OVERFLOW   0x4   /* informational: a cell used the direct-atomic spread path */
+#define RBC_FLAG_SOLVE_RESIDUAL    0x8   /* membrane load solve residual above 1e-3 */
+
+typedef struct rbc_params {
+    /* lattice (reference frame, nz includes the 4 BUFF planes) */
+    int    nx, ny, nz;
+    double dx, dt;
+    double tau;          /* BGK relaxation time (tau = 3 Df + 1/2) */
+    double Cr;           /* Courant number macro Cr */
+    double P;            /* body-force macro P (force density 2 rho P along z) */
+    double B;            /* IB-force macro B (force density 2 rho B F) */
+    int    flowstart;    /* FLOWSTART: drive off for iter <= flowstart */
+    double freq;         /* FREQ: drive factor 1 + 0.5 sin(pi dt iter / FREQ); +inf = constant */
+    /* periodic lengths and extents (reference macros LX, LZ and cdo->xmin ...) */
+    double LX, LZ;
+    double xmin, xmax, zmin, zmax;
+    /* membrane */
+    double C;            /* Skalak area-dilation ratio */
+    double rgs;          /* tension normalisation cel->rg (1.0 for red cells) */
+    int    law;          /* RBC_LAW_* */
+    double br;           /* bending modulus BR; only 0 is implemented */
+    int    M;            /* sub-cycling factor; only 1 is implemented */
+    int    rk_order;     /* RUNGE_KUTTA; only 4 is implemented */
+    /* implementation choices */
+    int    storage;      /* RBC_STORE_* */
+    int    membrane_fp64;/* 1: element mechanics in FP64, 0: FP32 */
+    int    solver_iters; /* Chebyshev iterations of the load solve; 0 = default (20) */
+    int    device;       /* CUDA device ordinal; -1 = device 0 of this library's runtime */
+} rbc_params;
+
+typedef struct rbc_mesh {
+    int ncell;           /* cel->n */
+    int vertex;          /* cel->vertex */
+    int element;         /* cel->element */
+    /* local triangle connectivity shared by every cell, [element*3], 0-based,
+     * outward winding: (x_b - x_a) x (x_c - x_a) points out of the cell */
+    const int *tri;
+    /* positions defining the reference (stress-free) shape and the initial
+     * state, AoS [3*ncell*vertex] like fem->xr / fem->x (init2.cu:311-325) */
+    const double *xr;
+} rbc_mesh;
+
+typedef struct rbc_handle rbc_handle;
+
+/* ---- lifetime -------------------------------------------------------- */
+
+/* Replaces cdo_init/flu_init/fem_init/mem_init/volume_init for the step:
+ * validates p and bc[nx*ny*nz], builds the link tables and the reference
+ * metric from mesh->xr, sets the lattice to rest equilibrium (rho = 1, u = 0),
+ * stores V0 and the centroids.  mesh may be NULL or have ncell = 0 (pure fluid).
+ * Synchronous. */
+int rbc_create(const rbc_params *p, const rbc_mesh *mesh, const int *bc, rbc_handle **out);
+int rbc_destroy(rbc_handle *h);
+/* human-readable text of the last error on h (or of the last create failure
+ * when h is NULL) */
+const char *rbc_last_error(const rbc_handle *h);
+
+/* ---- state in and out, reference layouts (synchronous) ---------------- */
+
+/* fn[nx*ny*nz*19]: pre-collision populations as lbm_d3q19 leaves them in
+ * ltc->fnD (lbm.cu:1575).  Only COMP nodes are read. */
+int rbc_import_ref_lattice(rbc_handle *h, const double *fn);
+/* Any pointer may be NULL.  fn: COMP nodes written, others untouched.
+ * dn/un/vn/wn [nx*ny*nz]: density and velocity of the last lbm step with the
+ * reference's half-force shift (lbm.cu:1116-1118); COMP and BUFF nodes are
+ * written (BUFF by periodic image, lbm.cu:1378-1432), WALL nodes untouched. */
+int rbc_export_ref_lattice(rbc_handle *h, double *fn, double *dn, double *un, double *vn, double *wn);
+/* Eulerian spread force ltc->fx/fy/fz [nx*ny*nz] after rbc_ibm_st1 and before
+ * rbc_lbm_d3q19 (COMP nodes, folded as ibm.cu:214-296 leaves them). */
+int rbc_export_ref_force(rbc_handle *h, double *fx, double *fy, double *fz);
+/* Any pointer may be NULL.  x,y,z [nv]: cel->x/y/z; xd [3*nv]: fem->xd;
+ * nd [4*ne]: fem->nd; volume0 [ncell]; gx [3*ncell]: cel->gx. */
+int rbc_import_ref_cells(rbc_handle *h, const double *x, const double *y, const double *z,
+                         const double *xd, const double *nd, const double *volume0, const double *gx);
+/* Vertex forces cel->fx/fy/fz [nv] as stress() leaves them, for running
+ * rbc_ibm_st1 on forces computed elsewhere. */
+int rbc_import_ref_vertex_force(rbc_handle *h, const double *fx, const double *fy, const double *fz);
+/* Any pointer may be NULL.  u,v,w: cel->u/v/w; fx,fy,fz: cel->fx/fy/fz. */
+int rbc_export_ref_cells(rbc_handle *h, double *x, double *y, double *z, double *xd,
+                         double *u, double *v, double *w, double *fx, double *fy, double *fz,
+                         double *gx);
+/* prc->iter as the stage entry points see it (rbc_step increments it first,
+ * as main.cu:75 does) */
+int rbc_set_iter(rbc_handle *h, int iter);
+int rbc_get_iter(const rbc_handle *h, int *iter);
+
+/* ---- the step ---------------------------------------------------------- */
+
+int rbc_stress(rbc_handle *h);
+int rbc_ibm_st1(rbc_handle *h);
+int rbc_lbm_d3q19(rbc_handle *h);
+int rbc_ibm_st2(rbc_handle *h);
+/* *iters (may be NULL) receives the reference's return value, iterations - 1.
+ * Synchronous when iters != NULL. */
+int rbc_volume_correction(rbc_handle *h, int *iters);
+/* nsteps full steps, each a replay of a CUDA graph of one step.  Asynchronous
+ * (rbc_synchronize or any export waits for it). */
+int rbc_step(rbc_handle *h, int nsteps);
+
+/* ---- diagnostics ------------------------------------------------------ */
+
+/* Synchronous.  flags: RBC_FLAG_* accumulated since the last call (cleared
+ * by the call); vc_iters_max: largest volume-correction return value seen. */
+int rbc_get_status(rbc_handle *h, int *flags, int *vc_iters_max);
+/* Synchronous.  FP64 per-cell volume, area and vertex centroid ([ncell],
+ * [ncell], [3*ncell]); any pointer may be NULL. */
+int rbc_cell_metrics(rbc_handle *h, double *volume, double *area, double *centroid);
+int rbc_synchronize(rbc_handle *h);
+/* Number of kernel launches issued by this library since creation. */
+int rbc_launch_count(const rbc_handle *h, long long *count);
+/* The CUDA stream (cudaStream_t) all work of h runs on. */
+int rbc_get_stream(const rbc_handle *h, void **stream);
+/* Runs nsteps full steps with direct launches (no graph) and a CUDA event
+ * around every kernel; kernel_ms[RBC_NUM_KERNELS] receives the summed device
+ * time per kernel in the order of RBC_KERNEL_NAMES.  Synchronous. */
+#define RBC_NUM_KERNELS 6
+#define RBC_KERNEL_NAMES {"step_begin", "membrane", "spread", "lbm_collide_stream", "advect", "volume"}
+int rbc_profile_steps(rbc_handle *h, int nsteps, double *kernel_ms);
+/* Sizes of the internal lattice and of the cells. */
+int rbc_dims(const rbc_handle *h, int *nx, int *ny, int *nz_periodic, int *ncell, int *vertex, int *element);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

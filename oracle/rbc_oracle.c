@@ -1,0 +1,688 @@
+/*
+ * rbc_oracle.c -- FP64 CPU oracle for the coupled fluid-membrane step.
+ *
+ * TEST INFRASTRUCTURE ONLY (the checker; see rbc_oracle.h).  Each function
+ * restates the reference's algorithm on the reference's own layout and cites
+ * the reference file:line it follows.  OpenMP parallelises loops whose
+ * iterations are independent; loops with scattered accumulation (the IB
+ * spread) run sequentially so results are deterministic.
+ */
+#define _DEFAULT_SOURCE   /* M_PI */
+#include "rbc_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+/* D3Q19 velocity set in the reference's slot order (lbm.cu:1038-1047):
+ * ___ p__ m__ _p_ _m_ __p __m pp_ mm_ mp_ pm_ _pp _mm _mp _pm p_p m_m p_m m_p */
+static const int EX[ORC_Q] = {0, 1,-1, 0, 0, 0, 0, 1,-1,-1, 1, 0, 0, 0, 0, 1,-1, 1,-1};
+static const int EY[ORC_Q] = {0, 0, 0, 1,-1, 0, 0, 1,-1, 1,-1, 1,-1,-1, 1, 0, 0, 0, 0};
+static const int EZ[ORC_Q] = {0, 0, 0, 0, 0, 1,-1, 0, 0, 0, 0, 1,-1, 1,-1, 1,-1,-1, 1};
+static const int OPP[ORC_Q] = {0, 2, 1, 4, 3, 6, 5, 8, 7,10, 9,12,11,14,13,16,15,18,17};
+static const double WQ[ORC_Q] = {1.0/3.0,
+    1.0/18.0, 1.0/18.0, 1.0/18.0, 1.0/18.0, 1.0/18.0, 1.0/18.0,
+    1.0/36.0, 1.0/36.0, 1.0/36.0, 1.0/36.0, 1.0/36.0, 1.0/36.0,
+    1.0/36.0, 1.0/36.0, 1.0/36.0, 1.0/36.0, 1.0/36.0, 1.0/36.0};
+
+#define COEFF_VOL_CHANGE 0.1   /* volume_correction.cu:14 */
+#define VC_EPS           1.0e-03 /* volume_correction.cu:15 (percent) */
+#define VC_ITRMAX        1000  /* volume_correction.cu:487 */
+
+int orc_num_threads(void)
+{
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+static inline double min_image(double d, double L)
+{
+    /* stress.cu:63-72: one shift by L when |d| > L/2 */
+    if (d > L * 0.5) d -= L; else if (d < -L * 0.5) d += L;
+    return d;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Setup                                                                     */
+/* ------------------------------------------------------------------------ */
+
+/* init2.cu:12-42 */
+static void add_nlink(int na, int nb, int *nln, int *ln)
+{
+    int flag = 0;
+    for (int i = 0; i < nln[na]; i++) if (nb == ln[7 * na + i]) flag = 1;
+    if (flag == 0) { ln[7 * na + nln[na]] = nb; nln[na]++; }
+}
+
+/* init2.cu:45-63 */
+static void add_elink(int ni, int ei, int *nle, int *le)
+{
+    le[6 * ni + nle[ni]] = ei;
+    nle[ni]++;
+}
+
+/* init2.cu:66-89 */
+static int checklink(int na, int nb, const int *nln, const int *ln)
+{
+    int flag = 0;
+    for (int i = 0; i < nln[na]; i++) if (nb == ln[7 * na + i]) flag = 1;
+    return flag;
+}
+
+/* init2.cu:92-166: order each one-ring counter-clockwise about the outward
+ * direction (vertex minus cell centroid). */
+static int sort_link_spring(const double *x, const int *nln, int *ln, int vertex, int ic)
+{
+    double gx = 0.0, gy = 0.0, gz = 0.0;
+    for (int j = 0; j < vertex; j++) {
+        int jid = ic * vertex + j;
+        gx += x[3 * jid + 0]; gy += x[3 * jid + 1]; gz += x[3 * jid + 2];
+    }
+    gx /= vertex; gy /= vertex; gz /= vertex;
+
+    for (int j = 0; j < vertex; j++) {
+        int jid = ic * vertex + j, n = 0, lns[7];
+        lns[0] = ln[7 * jid + 0];
+        for (int k = 1; k < nln[jid]; k++) {
+            int na = lns[k - 1];
+            double va[3] = {x[3*na+0] - x[3*jid+0], x[3*na+1] - x[3*jid+1], x[3*na+2] - x[3*jid+2]};
+            for (int l = 0; l < nln[jid]; l++) {
+                int nb = ln[7 * jid + l];
+                if (na == nb) continue;
+                if (checklink(na, nb, nln, ln) == 1) {
+                    double vb[3] = {x[3*nb+0] - x[3*jid+0], x[3*nb+1] - x[3*jid+1], x[3*nb+2] - x[3*jid+2]};
+                    double c[3] = {va[1]*vb[2] - va[2]*vb[1], va[2]*vb[0] - va[0]*vb[2], va[0]*vb[1] - va[1]*vb[0]};
+                    double inpro = c[0] * (x[3*jid+0] - gx) + c[1] * (x[3*jid+1] - gy) + c[2] * (x[3*jid+2] - gz);
+                    if (inpro > 0) { lns[k] = nb; n++; }
+                }
+            }
+        }
+        if (n + 1 != nln[jid]) return 3;
+        for (int k = 0; k < nln[jid]; k++) ln[7 * jid + k] = lns[k];
+    }
+    return 0;
+}
+
+/* init2.cu:169-203: append the vertex itself and sort ascending. */
+static void sort_link_order(const int *nln, int *lo, int vertex, int ic)
+{
+    for (int j = 0; j < vertex; j++) {
+        int jid = ic * vertex + j;
+        lo[7 * jid + nln[jid]] = jid;
+        for (int k = 0; k < nln[jid] + 1; k++)
+            for (int l = nln[jid]; l > k; l--)
+                if (lo[7*jid + l - 1] > lo[7*jid + l]) {
+                    int tmp = lo[7*jid + l]; lo[7*jid + l] = lo[7*jid + l - 1]; lo[7*jid + l - 1] = tmp;
+                }
+    }
+}
+
+/* init2.cu:206-255 */
+static void set_contravariant(const double *xr, double *n, const int *ele, int cln, int element)
+{
+    for (int ic = 0; ic < cln; ic++)
+        for (int e = 0; e < element; e++) {
+            int eid = ic * element + e;
+            int ea = ele[3*eid+0], eb = ele[3*eid+1], ec = ele[3*eid+2];
+            double v1[3], v2[3];
+            for (int j = 0; j < 3; j++) { v1[j] = xr[3*eb+j] - xr[3*ea+j]; v2[j] = xr[3*ec+j] - xr[3*ea+j]; }
+            double lv1 = v1[0]*v1[0] + v1[1]*v1[1] + v1[2]*v1[2];
+            double lv2 = v2[0]*v2[0] + v2[1]*v2[1] + v2[2]*v2[2];
+            double inv12 = v1[0]*v2[0] + v1[1]*v2[1] + v1[2]*v2[2];
+            double dv12 = lv1 * lv2 - inv12 * inv12;
+            n[4*eid+0] = lv2 / dv12;  n[4*eid+1] = -inv12 / dv12;
+            n[4*eid+2] = -inv12 / dv12; n[4*eid+3] = lv1 / dv12;
+        }
+}
+
+/* init2.cu:258-400 (fem_init, RBC branch) */
+int orc_fem_init(const orc_params *p, orc_state *s)
+{
+    int V = p->vertex, E = p->element, N = p->ncell;
+    int n_edge = V + E - 2;
+    memset(s->nln, 0, sizeof(int) * (size_t)N * V);
+    memset(s->ln, 0, sizeof(int) * (size_t)N * V * 7);
+    memset(s->lo, 0, sizeof(int) * (size_t)N * V * 7);
+    memset(s->nle, 0, sizeof(int) * (size_t)N * V);
+    memset(s->le, 0, sizeof(int) * (size_t)N * V * 6);
+    for (int i = 0; i < N; i++) {
+        for (int e = 0; e < E; e++) {
+            int eid = i * E + e;
+            int ea = s->ele[3*eid+0], eb = s->ele[3*eid+1], ec = s->ele[3*eid+2];
+            add_nlink(ea, eb, s->nln, s->ln); add_nlink(ea, ec, s->nln, s->ln);
+            add_nlink(eb, ec, s->nln, s->ln); add_nlink(eb, ea, s->nln, s->ln);
+            add_nlink(ec, ea, s->nln, s->ln); add_nlink(ec, eb, s->nln, s->ln);
+            add_elink(ea, eid, s->nle, s->le); add_elink(eb, eid, s->nle, s->le);
+            add_elink(ec, eid, s->nle, s->le);
+        }
+        int checker = 0;
+        for (int j = 0; j < V; j++) checker += s->nln[i * V + j];
+        if (checker != 2 * n_edge) return 3;
+        for (int j = 0; j < V; j++) {
+            int jid = i * V + j;
+            for (int k = 0; k < s->nln[jid]; k++) s->lo[7*jid + k] = s->ln[7*jid + k];
+        }
+        if (sort_link_spring(s->xd, s->nln, s->ln, V, i) != 0) return 3;
+        sort_link_order(s->nln, s->lo, V, i);
+    }
+    set_contravariant(s->xd, s->nd, s->ele, N, E);
+    return 0;
+}
+
+/* init1.cu:413-434 with td = 1, u = 0 (CapsuleCHANNELFLOW branch 399-407) */
+void orc_flu_init(const orc_params *p, orc_state *s)
+{
+    long n = (long)p->nx * p->ny * p->nz;
+    for (long i = 0; i < n; i++) {
+        for (int q = 0; q < ORC_Q; q++) { s->fn[i*ORC_Q + q] = WQ[q]; s->fm[i*ORC_Q + q] = 0.0; }
+        s->dn[i] = 1.0; s->un[i] = 0.0; s->vn[i] = 0.0; s->wn[i] = 0.0;
+        s->dm[i] = 1.0; s->um[i] = 0.0; s->vm[i] = 0.0; s->wm[i] = 0.0;
+        s->fx[i] = 0.0; s->fy[i] = 0.0; s->fz[i] = 0.0;
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Membrane: stress.cu                                                       */
+/* ------------------------------------------------------------------------ */
+
+/* stress.cu:29-121 (principal-tension diagnostics tp omitted) */
+void orc_calc_tension(const orc_params *p, orc_state *s)
+{
+    long ne = (long)p->ncell * p->element;
+    const double *x = s->xd, *n = s->nd;
+#pragma omp parallel for schedule(static)
+    for (long j = 0; j < ne; j++) {
+        int ea = s->ele[3*j+0], eb = s->ele[3*j+1], ec = s->ele[3*j+2];
+        double v1d[3], v2d[3];
+        for (int i = 0; i < 3; i++) {
+            v1d[i] = x[3*eb + i] - x[3*ea + i];
+            v2d[i] = x[3*ec + i] - x[3*ea + i];
+            if (i == 0) { v1d[i] = min_image(v1d[i], p->LX); v2d[i] = min_image(v2d[i], p->LX); }
+            else if (i == 2) { v1d[i] = min_image(v1d[i], p->LZ); v2d[i] = min_image(v2d[i], p->LZ); }
+        }
+        double lv1d = sqrt(v1d[0]*v1d[0] + v1d[1]*v1d[1] + v1d[2]*v1d[2]);
+        double lv2d = sqrt(v2d[0]*v2d[0] + v2d[1]*v2d[1] + v2d[2]*v2d[2]);
+        double inv12d = v1d[0]*v2d[0] + v1d[1]*v2d[1] + v1d[2]*v2d[2];
+        double dv12d = (lv1d*lv1d) * (lv2d*lv2d) - inv12d * inv12d;
+        double dn12 = n[4*j+0] * n[4*j+3] - n[4*j+1] * n[4*j+2];
+        s->rg[j] = sqrt(dv12d);
+        double vd[4] = {lv1d*lv1d, inv12d, inv12d, lv2d*lv2d};
+        double ndf[4] = {vd[3]/dv12d, -vd[1]/dv12d, -vd[2]/dv12d, vd[0]/dv12d};
+        double i1 = n[4*j+0]*vd[0] + n[4*j+1]*vd[1] + n[4*j+2]*vd[2] + n[4*j+3]*vd[3] - 2.0;
+        double i2 = dv12d * dn12 - 1.0;
+        double js = sqrt(i2 + 1.0);
+        for (int i = 0; i < 4; i++) {
+            if (p->law == 0)
+                s->t[4*j + i] = p->rgs * (i1 + 1.0) / js * n[4*j + i] + (p->C * i2 - 1.0) * js * ndf[i];
+            else
+                s->t[4*j + i] = p->rgs * (n[4*j + i] / js - ndf[i] * js / (i2 + 1.0) / (i2 + 1.0));
+        }
+    }
+}
+
+/* matrix_solver.cu:266-277 (spmv_ell) */
+static void spmv_ell(const int *ptr, const int *index, const double *value,
+                     const double *in, double *out, int n)
+{
+    for (int tid = 0; tid < n; tid++) {
+        double sum = 0.0;
+        for (int i = 0; i < ptr[tid]; i++) { int jj = i * n + tid; sum += value[jj] * in[index[jj]]; }
+        out[tid] = sum;
+    }
+}
+
+static double dot(const double *a, const double *b, int n)
+{
+    double s = 0.0;
+    for (int i = 0; i < n; i++) s += a[i] * b[i];
+    return s;
+}
+
+/* matrix_solver.cu:279-377 (bicgstab); dot_product.cu sums are plain sums here */
+static int bicgstab(const int *ptr, const int *index, const double *value, double *x, const double *b,
+                    double *ra, double *r, double *pp, double *m, double *nn, int n,
+                    double residual, int itrmax, int *iters)
+{
+    double err, alfa = 1.0, beta = 0.0, omeg = 1.0;
+    double r_dot_ra = 0.0, r_dot_ra_old;
+    int iter;
+    memset(ra, 0, sizeof(double) * n); memset(r, 0, sizeof(double) * n);
+    memset(pp, 0, sizeof(double) * n); memset(m, 0, sizeof(double) * n);
+    memset(nn, 0, sizeof(double) * n);
+    spmv_ell(ptr, index, value, x, r, n);
+    for (int i = 0; i < n; i++) { double t = b[i] - r[i]; r[i] = t; ra[i] = t; pp[i] = t; }
+    double b_dot_b = dot(b, b, n);
+    for (iter = 0; iter < itrmax; iter++) {
+        r_dot_ra_old = r_dot_ra;
+        r_dot_ra = dot(r, ra, n);
+        if (r_dot_ra == 0) { *iters = iter; return 1; }
+        if (iter > 0) {
+            beta = (r_dot_ra / r_dot_ra_old) * (alfa / omeg);
+            for (int i = 0; i < n; i++) pp[i] = r[i] + beta * (pp[i] - omeg * m[i]);
+        }
+        spmv_ell(ptr, index, value, pp, m, n);
+        alfa = r_dot_ra / dot(m, ra, n);
+        for (int i = 0; i < n; i++) r[i] = r[i] - alfa * m[i];
+        spmv_ell(ptr, index, value, r, nn, n);
+        omeg = dot(r, nn, n) / dot(nn, nn, n);
+        for (int i = 0; i < n; i++) { x[i] = x[i] + alfa * pp[i] + omeg * r[i]; r[i] = r[i] - omeg * nn[i]; }
+        err = sqrt(dot(r, r, n) / b_dot_b);
+        if (err < residual) break;
+    }
+    *iters = iter;
+    if (iter >= itrmax) return 2;
+    return 0;
+}
+
+/* stress.cu:306-373 (calc_load) with initialize (124-143), set_matrix_component
+ * (146-179), set_matrix_coefficient (182-272) and substitute_load (275-303). */
+int orc_calc_load(const orc_params *p, orc_state *s)
+{
+    int V = p->vertex, mn = p->mn, N = p->ncell, flag_all = 0, maxit = 0;
+    static const double f[3][2] = {{-1.0, -1.0}, {1.0, 0.0}, {0.0, 1.0}};
+#pragma omp parallel for schedule(dynamic, 1) reduction(|:flag_all) reduction(max:maxit)
+    for (int cid = 0; cid < N; cid++) {
+        int *ptr = (int *)calloc(mn, sizeof(int));
+        int *index = (int *)calloc((size_t)mn * 7, sizeof(int));
+        double *value = (double *)calloc((size_t)mn * 7, sizeof(double));
+        double *qc = (double *)calloc(mn, sizeof(double));
+        double *bc = (double *)calloc(mn, sizeof(double));
+        double *w = (double *)calloc((size_t)mn * 5, sizeof(double));
+        for (int j = 0; j < mn; j++) {
+            int node = j / 3, d = j % 3, jj = node + cid * V;
+            if (node < V) {
+                ptr[j] = s->nln[jj] + 1;
+                for (int i = 0; i < s->nln[jj] + 1; i++)
+                    index[i * mn + j] = 3 * (s->lo[7*jj + i] - cid * V) + d;
+            } else {
+                ptr[j] = 1;
+                index[0 * mn + j] = j;
+            }
+        }
+        for (int j = 0; j < mn; j++) {
+            int node = j / 3, d = j % 3, jj = node + cid * V;
+            if (node >= V) continue;
+            int n = s->nln[jj], oa = 0, ob = 0, oc = 0, order = 0, en = 0;
+            double tb = 0.0, tvalue[7] = {0.0};
+            for (int i = 0; i < n; i++) {
+                int element = s->le[6*jj + i];
+                double gab = s->rg[element];
+                int ea = s->ele[3*element+0], eb = s->ele[3*element+1], ec = s->ele[3*element+2];
+                for (int k = 0; k < n + 1; k++) {
+                    if (ea == s->lo[7*jj + k]) oa = k;
+                    if (eb == s->lo[7*jj + k]) ob = k;
+                    if (ec == s->lo[7*jj + k]) oc = k;
+                    if (jj == s->lo[7*jj + k]) order = k;
+                }
+                if (ea == jj) { tvalue[oa] += gab / 12.0; en = 0; } else tvalue[oa] += gab / 24.0;
+                if (eb == jj) { tvalue[ob] += gab / 12.0; en = 1; } else tvalue[ob] += gab / 24.0;
+                if (ec == jj) { tvalue[oc] += gab / 12.0; en = 2; } else tvalue[oc] += gab / 24.0;
+                double vd[2] = {s->xd[3*eb + d] - s->xd[3*ea + d], s->xd[3*ec + d] - s->xd[3*ea + d]};
+                if (d == 0) { vd[0] = min_image(vd[0], p->LX); vd[1] = min_image(vd[1], p->LX); }
+                else if (d == 2) { vd[0] = min_image(vd[0], p->LZ); vd[1] = min_image(vd[1], p->LZ); }
+                for (int k = 0; k < 4; k++) {
+                    int alpha = k / 2, beta = k % 2;
+                    tb += gab * s->t[4*element + k] * (vd[alpha] * f[en][beta] + vd[beta] * f[en][alpha]) / 4.0;
+                }
+            }
+            double jacobi = tvalue[order];
+            for (int k = 0; k < 7; k++) value[k * mn + j] = tvalue[k] / jacobi;
+            bc[j] = tb / jacobi;
+        }
+        int iters = 0;
+        int flag = bicgstab(ptr, index, value, qc, bc, w, w + mn, w + 2*mn, w + 3*mn, w + 4*mn, mn,
+                            p->residual, p->itrmax, &iters);
+        if (flag != 0) flag_all |= flag;
+        if (iters > maxit) maxit = iters;
+        /* substitute_load: qd[j + 3 cid V] = qc[j]; entries j >= 3V spill into the
+         * next cell's slice and are overwritten by it (stress.cu:292-300). */
+        for (int j = 0; j < 3 * V; j++) s->qd[j + 3 * cid * V] = qc[j];
+        free(ptr); free(index); free(value); free(qc); free(bc); free(w);
+    }
+    s->bicg_iters = maxit;
+    return flag_all;
+}
+
+/* stress.cu:376-445 (q2f) */
+void orc_q2f(const orc_params *p, orc_state *s)
+{
+    long nv = (long)p->ncell * p->vertex;
+    const double *x = s->xd;
+#pragma omp parallel for schedule(static)
+    for (long jid = 0; jid < nv; jid++) {
+        long j1 = jid;
+        double x1 = x[j1*3+0], y1 = x[j1*3+1], z1 = x[j1*3+2], ds = 0.0;
+        for (int k = 0; k < s->nln[j1]; k++) {
+            int j2 = s->ln[j1*7 + k], j3 = s->ln[j1*7 + (k+1) % s->nln[j1]];
+            double xx1 = min_image(x[j2*3+0] - x1, p->LX), yy1 = x[j2*3+1] - y1, zz1 = min_image(x[j2*3+2] - z1, p->LZ);
+            double xx2 = min_image(x[j3*3+0] - x1, p->LX), yy2 = x[j3*3+1] - y1, zz2 = min_image(x[j3*3+2] - z1, p->LZ);
+            double nvx = -(yy1*zz2 - zz1*yy2), nvy = -(zz1*xx2 - xx1*zz2), nvz = -(xx1*yy2 - yy1*xx2);
+            ds += sqrt(nvx*nvx + nvy*nvy + nvz*nvz) / 2.0 / 3.0;
+        }
+        s->cfx[jid] = -1.0 * s->qd[jid*3+0] * ds;
+        s->cfy[jid] = -1.0 * s->qd[jid*3+1] * ds;
+        s->cfz[jid] = -1.0 * s->qd[jid*3+2] * ds;
+    }
+}
+
+/* stress.cu:580-659 (bending with BR = 0 contributes nothing and is omitted) */
+int orc_stress(const orc_params *p, orc_state *s)
+{
+    orc_calc_tension(p, s);
+    int flag = orc_calc_load(p, s);
+    orc_q2f(p, s);
+    return flag;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Immersed boundary: ibm.cu                                                 */
+/* ------------------------------------------------------------------------ */
+
+/* ibm.cu:299-369: ibm_st1a (27-52), ibm_st1b (55-131), ibm_st1c (214-296,
+ * CapsuleCHANNELFLOW: fold the z BUFF planes) */
+void orc_ibm_st1(const orc_params *p, orc_state *s)
+{
+    int nx = p->nx, ny = p->ny, nz = p->nz;
+    long n = (long)nx * ny * nz, nv = (long)p->ncell * p->vertex;
+    double dx = p->dx;
+    memset(s->fx, 0, sizeof(double) * n);
+    memset(s->fy, 0, sizeof(double) * n);
+    memset(s->fz, 0, sizeof(double) * n);
+    for (long jid = 0; jid < nv; jid++) {
+        double xtr = s->x[jid] + (double)(nx - 1) * dx / 2.0;
+        double ytr = s->y[jid] + (double)(ny - 1) * dx / 2.0;
+        double ztr = s->z[jid] + (double)(nz - 1) * dx / 2.0;
+        int x1 = (int)floor(xtr / dx) - 1, x2 = (int)ceil(xtr / dx) + 1;
+        int y1 = (int)floor(ytr / dx) - 1, y2 = (int)ceil(ytr / dx) + 1;
+        int z1 = (int)floor(ztr / dx) - 1, z2 = (int)ceil(ztr / dx) + 1;
+        for (int iz = z1; iz <= z2; iz++)
+            for (int iy = y1; iy <= y2; iy++)
+                for (int ix = x1; ix <= x2; ix++) {
+                    if (ix < 0 || ix >= nx || iy < 0 || iy >= ny || iz < 0 || iz >= nz) continue;
+                    long i = ix + (long)nx * iy + (long)nx * ny * iz;
+                    double xx = fabs((double)ix * dx - xtr), yy = fabs((double)iy * dx - ytr), zz = fabs((double)iz * dx - ztr);
+                    double xcos = 1.0 + cos(M_PI * xx / (2.0 * dx));
+                    double ycos = 1.0 + cos(M_PI * yy / (2.0 * dx));
+                    double zcos = 1.0 + cos(M_PI * zz / (2.0 * dx));
+                    double dlt = xcos * ycos * zcos / (64.0 * dx * dx * dx);
+                    s->fx[i] += dlt * s->cfx[jid];
+                    s->fy[i] += dlt * s->cfy[jid];
+                    s->fz[i] += dlt * s->cfz[jid];
+                }
+    }
+    long plane = (long)nx * ny, shift = plane * (nz - 4);
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < n; i++) {
+        if (s->bc[i] != ORC_COMP) continue;
+        long iz = i / plane;
+        if (iz <= 3) { s->fx[i] += s->fx[i + shift]; s->fy[i] += s->fy[i + shift]; s->fz[i] += s->fz[i + shift]; }
+        if (iz >= nz - 4) { s->fx[i] += s->fx[i - shift]; s->fy[i] += s->fy[i - shift]; s->fz[i] += s->fz[i - shift]; }
+    }
+}
+
+/* ibm.cu:372-639 (ibm_st2a, RUNGE_KUTTA == 4) */
+void orc_ibm_st2(const orc_params *p, orc_state *s)
+{
+    int nx = p->nx, ny = p->ny, nz = p->nz;
+    long nv = (long)p->ncell * p->vertex;
+    double dx = p->dx, dt = p->dt;
+    const double Md = 1.0; /* M = 1 */
+#pragma omp parallel for schedule(static)
+    for (long jid = 0; jid < nv; jid++) {
+        double xn = s->x[jid], yn = s->y[jid], zn = s->z[jid];
+        double xr = xn, yr = yn, zr = zn;
+        double uk[4][3];
+        for (int rk = 0; rk < 4; rk++) {
+            double ur = 0.0, vr = 0.0, wr = 0.0;
+            double xtr = xr + (double)(nx - 1) * dx / 2.0;
+            double ytr = yr + (double)(ny - 1) * dx / 2.0;
+            double ztr = zr + (double)(nz - 1) * dx / 2.0;
+            int x1 = (int)floor(xtr / dx) - 1, x2 = (int)ceil(xtr / dx) + 1;
+            int y1 = (int)floor(ytr / dx) - 1, y2 = (int)ceil(ytr / dx) + 1;
+            int z1 = (int)floor(ztr / dx) - 1, z2 = (int)ceil(ztr / dx) + 1;
+            for (int iz = z1; iz <= z2; iz++)
+                for (int iy = y1; iy <= y2; iy++)
+                    for (int ix = x1; ix <= x2; ix++) {
+                        if (ix < 0 || ix >= nx || iy < 0 || iy >= ny || iz < 0 || iz >= nz) continue;
+                        long i = ix + (long)nx * iy + (long)nx * ny * iz;
+                        double xx = fabs((double)ix * dx - xtr), yy = fabs((double)iy * dx - ytr), zz = fabs((double)iz * dx - ztr);
+                        double dlt = (1.0 + cos(M_PI * xx / (2.0 * dx))) * (1.0 + cos(M_PI * yy / (2.0 * dx)))
+                                   * (1.0 + cos(M_PI * zz / (2.0 * dx))) / 64.0;
+                        ur += dlt * s->um[i]; vr += dlt * s->vm[i]; wr += dlt * s->wm[i];
+                    }
+            uk[rk][0] = ur; uk[rk][1] = vr; uk[rk][2] = wr;
+            double h = (rk < 2) ? Md * dt / 2.0 : Md * dt;
+            xr = xn + ur * h; yr = yn + vr * h; zr = zn + wr * h;
+        }
+        double um = (uk[0][0] + 2.0 * uk[1][0] + 2.0 * uk[2][0] + uk[3][0]) / 6.0;
+        double vm = (uk[0][1] + 2.0 * uk[1][1] + 2.0 * uk[2][1] + uk[3][1]) / 6.0;
+        double wm = (uk[0][2] + 2.0 * uk[1][2] + 2.0 * uk[2][2] + uk[3][2]) / 6.0;
+        xr = xn + um * Md * dt; yr = yn + vm * Md * dt; zr = zn + wm * Md * dt;
+        if (xr < p->xmin) xr += p->LX;
+        if (xr > p->xmax) xr -= p->LX;
+        if (zr < p->zmin) zr += p->LZ;
+        if (zr > p->zmax) zr -= p->LZ;
+        s->u[jid] = um; s->x[jid] = xr; s->xd[jid*3 + 0] = xr;
+        s->v[jid] = vm; s->y[jid] = yr; s->xd[jid*3 + 1] = yr;
+        s->w[jid] = wm; s->z[jid] = zr; s->xd[jid*3 + 2] = zr;
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Lattice Boltzmann: lbm.cu                                                 */
+/* ------------------------------------------------------------------------ */
+
+/* lbm.cu:983-1313 (lbm_CapsuleCHANNELFLOW) + 1378-1432 (BUFF copy) +
+ * 1435-1460 (average, M = 1) + pointer swap (1575).  LAMBDA1 = 1, so the
+ * viscosity-ratio term of omega (1131) vanishes. */
+void orc_lbm_d3q19(const orc_params *p, orc_state *s)
+{
+    int nx = p->nx, ny = p->ny, nz = p->nz, iter = s->iter;
+    long n = (long)nx * ny * nz, plane = (long)nx * ny, shift = plane * (nz - 4);
+    double Cr = p->Cr, Cr2 = Cr * Cr, P = p->P, B = p->B;
+    double t = p->dt * (double)iter;
+    double wi = (iter > p->flowstart) ? 1.0 + 0.5 * sin(M_PI * t / p->freq) : 0.0;
+    double om = 1.0 / p->tau;
+    const double *fn = s->fn; double *fm = s->fm;
+    const int *bc = s->bc;
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < n; i++) {
+        if (bc[i] != ORC_COMP) continue;
+        double f[ORC_Q];
+        for (int q = 0; q < ORC_Q; q++) f[q] = fn[i * ORC_Q + q];
+        double tfx = s->fx[i], tfy = s->fy[i], tfz = s->fz[i];
+        double td = 0.0, jx = 0.0, jy = 0.0, jz = 0.0;
+        for (int q = 0; q < ORC_Q; q++) { td += f[q]; jx += EX[q] * f[q]; jy += EY[q] * f[q]; jz += EZ[q] * f[q]; }
+        double tu = (jx + td * P * 0.0 + td * B * tfx) / (td * Cr);
+        double tv = (jy + td * P * 0.0 + td * B * tfy) / (td * Cr);
+        double tw = (jz + td * P * wi + td * B * tfz) / (td * Cr);
+        s->dn[i] = td; s->un[i] = tu; s->vn[i] = tv; s->wn[i] = tw;
+        /* (iter-1)%M == 0 with M = 1: the averages restart every step */
+        s->dm[i] = td; s->um[i] = tu; s->vm[i] = tv; s->wm[i] = tw;
+        double om1 = 1.0 - om, om2 = (1.0 - om / 2.0) * 2.0 * td * P, om3 = (1.0 - om / 2.0) * 2.0 * td * B;
+        double uvw = -1.5 * (tu*tu + tv*tv + tw*tw) * Cr2;
+        double gP[3] = {0.0, 0.0, wi}, gB[3] = {tfx, tfy, tfz}, uu[3] = {tu, tv, tw};
+        for (int q = 0; q < ORC_Q; q++) {
+            double e[3] = {EX[q], EY[q], EZ[q]};
+            double eu = e[0]*tu + e[1]*tv + e[2]*tw;
+            double feq = WQ[q] * td * (1.0 + 3.0 * eu * Cr + 4.5 * eu * eu * Cr2 + uvw);
+            double sP = 0.0, sB = 0.0;
+            for (int d = 0; d < 3; d++) {
+                double c = 3.0 * (e[d] - uu[d] * Cr) + 9.0 * Cr * eu * e[d];
+                sP += c * gP[d]; sB += c * gB[d];
+            }
+            f[q] = om1 * f[q] + om * feq + om2 * WQ[q] * sP + om3 * WQ[q] * sB;
+        }
+        /* push streaming with half-way bounce-back (lbm.cu:1050-1094, 1272-1310) */
+        for (int q = 0; q < ORC_Q; q++) {
+            long d = i + EX[q] + (long)nx * EY[q] + plane * EZ[q];
+            long j;
+            if (q == 0) j = i * ORC_Q;
+            else if (q == 5 || q == 6) {
+                if (bc[d] == ORC_BUFF) d -= EZ[q] * shift;
+                j = d * ORC_Q + q;
+            } else if (EZ[q] == 0) {
+                j = (bc[d] == ORC_WALL) ? i * ORC_Q + OPP[q] : d * ORC_Q + q;
+            } else {
+                if (bc[d] == ORC_WALL) j = i * ORC_Q + OPP[q];
+                else { if (bc[d] == ORC_BUFF) d -= EZ[q] * shift; j = d * ORC_Q + q; }
+            }
+            fm[j] = f[q];
+        }
+    }
+    /* lbm.cu:1378-1432: BUFF planes take their periodic images */
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < n; i++) {
+        if (bc[i] != ORC_BUFF) continue;
+        long iz = i / plane, i2 = i;
+        if (iz <= 1) i2 += shift;
+        if (iz >= nz - 2) i2 -= shift;
+        s->dn[i] = s->dn[i2]; s->un[i] = s->un[i2]; s->vn[i] = s->vn[i2]; s->wn[i] = s->wn[i2];
+        s->dm[i] = s->dm[i2]; s->um[i] = s->um[i2]; s->vm[i] = s->vm[i2]; s->wm[i] = s->wm[i2];
+    }
+    /* lbm.cu:1435-1460 divides by M = 1; lbm.cu:1575 swaps the buffers */
+    double *tmp = s->fn; s->fn = s->fm; s->fm = tmp;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Volume correction: volume_correction.cu                                   */
+/* ------------------------------------------------------------------------ */
+
+/* volume_correction.cu:138-200 (CalcEleNormal_GPU) + 246-281 (CalcVolume) */
+static void calc_ele_normal(const orc_params *p, const orc_state *s, double *normal, double *dS, double *vtmp)
+{
+    long ne = (long)p->ncell * p->element;
+#pragma omp parallel for schedule(static)
+    for (long e = 0; e < ne; e++) {
+        int na = s->ele[3*e+0], nb = s->ele[3*e+1], nc = s->ele[3*e+2];
+        double v1[3] = {s->x[nb] - s->x[na], s->y[nb] - s->y[na], s->z[nb] - s->z[na]};
+        double v2[3] = {s->x[nc] - s->x[na], s->y[nc] - s->y[na], s->z[nc] - s->z[na]};
+        double c[3] = {v1[1]*v2[2] - v1[2]*v2[1], v1[2]*v2[0] - v1[0]*v2[2], v1[0]*v2[1] - v1[1]*v2[0]};
+        double nc_ = sqrt(c[0]*c[0] + c[1]*c[1] + c[2]*c[2]);
+        normal[3*e+0] = c[0] / nc_; normal[3*e+1] = c[1] / nc_; normal[3*e+2] = c[2] / nc_;
+        dS[e] = nc_ / 2.0;
+        double r[3] = {(s->x[na] + s->x[nb] + s->x[nc]) / 3.0, (s->y[na] + s->y[nb] + s->y[nc]) / 3.0,
+                       (s->z[na] + s->z[nb] + s->z[nc]) / 3.0};
+        vtmp[e] = 1.0 / 3.0 * (r[0]*normal[3*e+0] + r[1]*normal[3*e+1] + r[2]*normal[3*e+2]) * dS[e];
+    }
+}
+
+void orc_calc_volume(const orc_params *p, const orc_state *s, double *volume, double *area)
+{
+    long ne = (long)p->ncell * p->element;
+    double *normal = (double *)malloc(sizeof(double) * 3 * ne);
+    double *dS = (double *)malloc(sizeof(double) * ne), *vtmp = (double *)malloc(sizeof(double) * ne);
+    calc_ele_normal(p, s, normal, dS, vtmp);
+    for (int c = 0; c < p->ncell; c++) {
+        double V = 0.0, A = 0.0;
+        for (int e = 0; e < p->element; e++) { V += vtmp[c * p->element + e]; A += dS[c * p->element + e]; }
+        volume[c] = V; area[c] = A;
+    }
+    free(normal); free(dS); free(vtmp);
+}
+
+/* volume_correction.cu:310-352 (CalcCenter, channel branch) */
+static void calc_center(const orc_params *p, orc_state *s)
+{
+    int V = p->vertex;
+    for (int c = 0; c < p->ncell; c++) {
+        double sx = 0.0, sy = 0.0, sz = 0.0;
+        for (int j = 0; j < V; j++) { sx += s->x[c*V + j]; sy += s->y[c*V + j]; sz += s->z[c*V + j]; }
+        s->gx[3*c+0] = sx / (double)V; s->gx[3*c+1] = sy / (double)V; s->gx[3*c+2] = sz / (double)V;
+        if (s->gx[3*c+2] < p->zmin) s->gx[3*c+2] += p->LZ;
+        else if (s->gx[3*c+2] > p->zmax) s->gx[3*c+2] -= p->LZ;
+    }
+}
+
+/* volume_correction.cu:427-450 */
+void orc_volume_init(const orc_params *p, orc_state *s)
+{
+    double *area = (double *)malloc(sizeof(double) * p->ncell);
+    orc_calc_volume(p, s, s->volume0, area);
+    free(area);
+    calc_center(p, s);
+}
+
+/* volume_correction.cu:453-524 (RBC branch) with CapsulePeriodicBefore/After
+ * (28-94), CalcLambda1 (378-399) and VolumeCorrection_GPU (97-135). */
+int orc_volume_correction(const orc_params *p, orc_state *s)
+{
+    int N = p->ncell, V = p->vertex;
+    long nv = (long)N * V, ne = (long)N * p->element;
+    double *normal = (double *)malloc(sizeof(double) * 3 * ne);
+    double *dS = (double *)malloc(sizeof(double) * ne), *vtmp = (double *)malloc(sizeof(double) * ne);
+    double *volume = (double *)malloc(sizeof(double) * N), *area = (double *)malloc(sizeof(double) * N);
+    double *lambda = (double *)malloc(sizeof(double) * N);
+    int *conv = (int *)calloc(N, sizeof(int));
+    /* CapsulePeriodicBefore: z unwrap about the stored centroid */
+    for (int c = 0; c < N; c++)
+        for (int j = 0; j < V; j++) {
+            long id = (long)c * V + j;
+            double dz = s->z[id] - s->gx[3*c+2];
+            if (dz > p->LZ * 0.5) s->z[id] -= p->LZ; else if (dz < -p->LZ * 0.5) s->z[id] += p->LZ;
+        }
+    int iter = 0, all_converged;
+    do {
+        calc_ele_normal(p, s, normal, dS, vtmp);
+        for (int c = 0; c < N; c++) {
+            double Vs = 0.0, As = 0.0;
+            for (int e = 0; e < p->element; e++) { Vs += vtmp[(long)c * p->element + e]; As += dS[(long)c * p->element + e]; }
+            volume[c] = Vs; area[c] = As;
+        }
+        all_converged = 1;
+        for (int c = 0; c < N; c++) {
+            double dV = fabs(volume[c] - s->volume0[c]) / s->volume0[c] * 100.0;
+            if (dV < VC_EPS) { lambda[c] = 0.0; conv[c] = 1; }
+            else lambda[c] = 18.0 * (volume[c] - s->volume0[c]) / area[c];
+            all_converged &= conv[c];
+        }
+#pragma omp parallel for schedule(static)
+        for (long id = 0; id < nv; id++) {
+            int c = (int)(id / V), nne = s->nle[id];
+            double nn[3] = {0.0, 0.0, 0.0};
+            for (int k = 0; k < nne; k++) {
+                int e = s->le[6*id + k];
+                nn[0] += normal[3*e+0] / nne; nn[1] += normal[3*e+1] / nne; nn[2] += normal[3*e+2] / nne;
+            }
+            s->x[id] += -lambda[c] / 6.0 * nn[0] * COEFF_VOL_CHANGE;
+            s->y[id] += -lambda[c] / 6.0 * nn[1] * COEFF_VOL_CHANGE;
+            s->z[id] += -lambda[c] / 6.0 * nn[2] * COEFF_VOL_CHANGE;
+        }
+        iter++;
+    } while (!all_converged && iter < VC_ITRMAX);
+    calc_center(p, s);
+    /* CapsulePeriodicAfter */
+    for (long id = 0; id < nv; id++) {
+        if (s->z[id] < p->zmin) s->z[id] += p->LZ;
+        else if (s->z[id] > p->zmax) s->z[id] -= p->LZ;
+    }
+    free(normal); free(dS); free(vtmp); free(volume); free(area); free(lambda); free(conv);
+    if (iter >= VC_ITRMAX) return -1;
+    return iter - 1;
+}
+
+/* main.cu:73-110 with M = 1 (adhesion, THINC/WLIC and front tracking are off
+ * for LAMBDA1 = 1 and CYTOADHESION = false) */
+int orc_step(const orc_params *p, orc_state *s, int nsteps)
+{
+    for (int k = 0; k < nsteps; k++) {
+        s->iter++;
+        if (p->ncell > 0) {
+            int flag = orc_stress(p, s);
+            if (flag != 0) return 4;          /* error(4) in stress.cu:366 */
+            orc_ibm_st1(p, s);
+        }
+        orc_lbm_d3q19(p, s);
+        if (p->ncell > 0) {
+            orc_ibm_st2(p, s);
+            if (orc_volume_correction(p, s) < 0) return 5;
+        }
+    }
+    return 0;
+}

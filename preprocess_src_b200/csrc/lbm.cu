@@ -1,0 +1,261 @@
+// lbm.cu -- fused D3Q19 BGK collide-stream with Guo forcing, pull scheme.
+//
+// Replaces lbm_CapsuleCHANNELFLOW + lbm_CHANNELFLOW_Boundary + lbm_AVERAGE
+// (lbm.cu:983-1313, 1378-1460 of the reference).  The reference pushes
+// post-collision populations to the neighbours (scattered stores into AoS
+// fn[i*19+q]); here each node pulls the post-collision populations of the
+// previous step from its upstream neighbours (coalesced SoA loads), collides and
+// stores its own post-collision populations.  Both orders produce the same
+// pre-collision field; the half-way bounce-back of the push form
+// (fm[i][opp q] = f*_q(i) when i + e_q is a wall) becomes, in pull form,
+// f_q(i) = f*_{opp q}(i) when i - e_q is a wall.  The BUFF planes of the
+// reference are replaced by a periodic z index.
+//
+// Populations are stored as g = f - w (FP32) or (f - w) * scale (FP16), which
+// keeps their rounding error relative to the deviation from rest rather than to
+// w itself.  Arithmetic is FP32.
+#include "rbc_internal.cuh"
+
+namespace rbc {
+
+template <int STORE> struct Store;
+template <> struct Store<RBC_STORE_F32> {
+    using T = float;
+    static __device__ __forceinline__ float ld(const T *p, float) { return __ldg(p); }
+    static __device__ __forceinline__ void st(T *p, float v, float) { __stcs(p, v); }
+};
+template <> struct Store<RBC_STORE_F16> {
+    using T = __half;
+    static __device__ __forceinline__ float ld(const T *p, float inv_scale) { return __half2float(__ldg(p)) * inv_scale; }
+    static __device__ __forceinline__ void st(T *p, float v, float scale) { __stcs(reinterpret_cast<unsigned short *>(p), __half_as_ushort(__float2half_rn(v * scale))); }
+};
+
+constexpr int LBM_THREADS = 256;
+
+// One thread per internal node (x fastest).  Per fluid node: 19 pulled loads,
+// 12 B of IB force, 19 stores, 16 B of rho/u.
+template <int STORE>
+__global__ void __launch_bounds__(LBM_THREADS)
+lbm_collide_stream(const typename Store<STORE>::T *__restrict__ gin, typename Store<STORE>::T *__restrict__ gout,
+                   float *__restrict__ rho, float *__restrict__ ux, float *__restrict__ uy, float *__restrict__ uz,
+                   float *__restrict__ Fx, float *__restrict__ Fy, float *__restrict__ Fz,
+                   const uint32_t *__restrict__ mask2d, const float *__restrict__ drive,
+                   int nx, int ny, int nzc, long long nint,
+                   float omega, float Cr, float Bc, float scale, float inv_scale)
+{
+    using S = Store<STORE>;
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= nint) return;
+    const int plane = nx * ny;
+    const int z = (int)(idx / plane);
+    const int xy = (int)(idx - (long long)z * plane);
+    const uint32_t m = __ldg(&mask2d[xy]);
+    if (!(m & MASK_FLUID)) return;
+
+    const long long zb0 = (long long)z * plane;
+    const long long zbm = (z == 0) ? (long long)(nzc - 1) * plane : zb0 - plane;       // plane z-1
+    const long long zbp = (z == nzc - 1) ? 0 : zb0 + plane;                             // plane z+1
+
+    float g[Q];
+#pragma unroll
+    for (int q = 0; q < Q; q++) {
+        const long long src = ((ez(q) == 1) ? zbm : (ez(q) == -1) ? zbp : zb0) + xy - ex(q) - nx * ey(q);
+        const bool bb = (m >> q) & 1u;
+        const typename S::T *p = bb ? (gin + (long long)opp(q) * nint + idx) : (gin + (long long)q * nint + src);
+        g[q] = S::ld(p, inv_scale);
+    }
+
+    const float fx = Fx[idx], fy = Fy[idx], fz = Fz[idx];
+    const float pd = __ldg(drive);
+
+    float drho = 0.f, jx = 0.f, jy = 0.f, jz = 0.f;
+#pragma unroll
+    for (int q = 0; q < Q; q++) {
+        drho += g[q];
+        if (ex(q)) jx += ex(q) * g[q];
+        if (ey(q)) jy += ey(q) * g[q];
+        if (ez(q)) jz += ez(q) * g[q];
+    }
+    const float r = 1.0f + drho;
+    // half of the total force density: rho P drive z^ + rho B F (lbm.cu:1116-1118)
+    const float Gx = r * Bc * fx, Gy = r * Bc * fy, Gz = r * (pd + Bc * fz);
+    const float inv = 1.0f / (r * Cr);
+    const float u = (jx + Gx) * inv, v = (jy + Gy) * inv, w = (jz + Gz) * inv;
+
+    rho[idx] = r; ux[idx] = u; uy[idx] = v; uz[idx] = w;
+    if (fx != 0.f || fy != 0.f || fz != 0.f) { Fx[idx] = 0.f; Fy[idx] = 0.f; Fz[idx] = 0.f; }
+
+    // BGK + Guo forcing (lbm.cu:1129-1213): with G the half force above,
+    // F_q = (1 - om/2) * 2 * w_q * [3 e.G - 3 Cr u.G + 9 Cr (e.u)(e.G)]
+    const float Cr2 = Cr * Cr;
+    const float om1 = 1.0f - omega;
+    const float fo = (1.0f - 0.5f * omega) * 2.0f;
+    const float usq = -1.5f * (u * u + v * v + w * w) * Cr2;
+    const float uG = 3.0f * Cr * (u * Gx + v * Gy + w * Gz);
+#pragma unroll
+    for (int q = 0; q < Q; q++) {
+        const float eu = ex(q) * u + ey(q) * v + ez(q) * w;
+        const float eG = ex(q) * Gx + ey(q) * Gy + ez(q) * Gz;
+        const float geq = wq(q) * (drho + r * (3.0f * Cr * eu + 4.5f * Cr2 * eu * eu + usq));
+        const float fq = fo * wq(q) * (3.0f * eG - uG + 9.0f * Cr * eu * eG);
+        S::st(gout + (long long)q * nint + idx, om1 * g[q] + omega * geq + fq, scale);
+    }
+}
+
+void launch_lbm(const Geom &g, int storage, const LbmArgs &a, cudaStream_t s)
+{
+    const unsigned blocks = (unsigned)((g.nint + LBM_THREADS - 1) / LBM_THREADS);
+    if (storage == RBC_STORE_F16)
+        lbm_collide_stream<RBC_STORE_F16><<<blocks, LBM_THREADS, 0, s>>>(
+            (const __half *)a.gin, (__half *)a.gout, a.rho, a.ux, a.uy, a.uz, a.Fx, a.Fy, a.Fz, a.mask2d,
+            a.drive, g.nx, g.ny, g.nzc, g.nint, a.omega, a.Cr, a.Bc, a.scale, a.inv_scale);
+    else
+        lbm_collide_stream<RBC_STORE_F32><<<blocks, LBM_THREADS, 0, s>>>(
+            (const float *)a.gin, (float *)a.gout, a.rho, a.ux, a.uy, a.uz, a.Fx, a.Fy, a.Fz, a.mask2d,
+            a.drive, g.nx, g.ny, g.nzc, g.nint, a.omega, a.Cr, a.Bc, a.scale, a.inv_scale);
+}
+
+// ---- reference layout <-> internal layout ---------------------------------
+
+__device__ __forceinline__ long long ref_index(const Geom &g, int x, int y, int z) {
+    return (long long)x + (long long)g.nx * (y + (long long)g.ny * (z + 2));
+}
+
+// Reference fn (pre-collision, AoS FP64) -> internal post-collision g*:
+// f*_q(i) = fn[i + e_q][q] when i + e_q is fluid, else fn[i][opp q]
+// (inverse of the push of lbm.cu:1272-1310).
+template <int STORE>
+__global__ void import_lattice_kernel(const Geom g, const double *__restrict__ fn, typename Store<STORE>::T *__restrict__ gout,
+                                      const uint32_t *__restrict__ mask2d, float scale)
+{
+    using S = Store<STORE>;
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= g.nint) return;
+    const int z = (int)(idx / g.plane);
+    const int xy = (int)(idx - (long long)z * g.plane);
+    const int y = xy / g.nx, x = xy - y * g.nx;
+    const uint32_t m = mask2d[xy];
+#pragma unroll
+    for (int q = 0; q < Q; q++) {
+        float val = 0.f;
+        if (m & MASK_FLUID) {
+            double f;
+            if ((m >> opp(q)) & 1u) f = fn[ref_index(g, x, y, z) * Q + opp(q)];
+            else f = fn[ref_index(g, x + ex(q), y + ey(q), wrap_z(z + ez(q), g.nzc)) * Q + q];
+            val = (float)(f - wqd(q));
+        }
+        S::st(gout + (long long)q * g.nint + idx, val, scale);
+    }
+}
+
+// Internal g* -> reference pre-collision fn (the pull of the LBM kernel without
+// the collision), plus rho/u with BUFF planes as periodic images
+// (lbm.cu:1378-1432).  Non-COMP fn entries are set to 0, WALL macroscopic
+// entries to the reference's untouched initial values (rho 1, u 0).
+template <int STORE>
+__global__ void export_lattice_kernel(const Geom g, const typename Store<STORE>::T *__restrict__ gin,
+                                      const uint32_t *__restrict__ mask2d,
+                                      const float *__restrict__ rho, const float *__restrict__ ux,
+                                      const float *__restrict__ uy, const float *__restrict__ uz,
+                                      float inv_scale, double *__restrict__ fn, double *__restrict__ dn,
+                                      double *__restrict__ un, double *__restrict__ vn, double *__restrict__ wn)
+{
+    using S = Store<STORE>;
+    const long long nref = g.plane * g.nzr;
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nref) return;
+    const int zr = (int)(i / g.plane);
+    const int xy = (int)(i - (long long)zr * g.plane);
+    const int y = xy / g.nx, x = xy - y * g.nx;
+    const uint32_t m = mask2d[xy];
+    const bool comp = (m & MASK_FLUID) && zr >= 2 && zr < g.nzr - 2;
+    if (fn) {
+#pragma unroll
+        for (int q = 0; q < Q; q++) {
+            double f = 0.0;
+            if (comp) {
+                const int z = zr - 2;
+                const long long idx = (long long)z * g.plane + xy;
+                float gv;
+                if ((m >> q) & 1u) gv = S::ld(gin + (long long)opp(q) * g.nint + idx, inv_scale);
+                else {
+                    const long long src = (long long)wrap_z(z - ez(q), g.nzc) * g.plane + (x - ex(q)) + (long long)g.nx * (y - ey(q));
+                    gv = S::ld(gin + (long long)q * g.nint + src, inv_scale);
+                }
+                f = (double)gv + wqd(q);
+            }
+            fn[i * Q + q] = f;
+        }
+    }
+    if (dn) {
+        double r = 1.0, a = 0.0, b = 0.0, c = 0.0;
+        if (m & MASK_FLUID) {
+            const long long idx = (long long)wrap_z(zr - 2, g.nzc) * g.plane + xy;
+            r = rho[idx]; a = ux[idx]; b = uy[idx]; c = uz[idx];
+        }
+        dn[i] = r; un[i] = a; vn[i] = b; wn[i] = c;
+    }
+}
+
+__global__ void export_force_kernel(const Geom g, const float *__restrict__ Fx, const float *__restrict__ Fy,
+                                    const float *__restrict__ Fz, const uint32_t *__restrict__ mask2d,
+                                    double *__restrict__ out)
+{
+    const long long nref = g.plane * g.nzr;
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nref) return;
+    const int zr = (int)(i / g.plane);
+    const int xy = (int)(i - (long long)zr * g.plane);
+    double a = 0.0, b = 0.0, c = 0.0;
+    if ((mask2d[xy] & MASK_FLUID) && zr >= 2 && zr < g.nzr - 2) {
+        const long long idx = (long long)(zr - 2) * g.plane + xy;
+        a = Fx[idx]; b = Fy[idx]; c = Fz[idx];
+    }
+    out[i] = a; out[nref + i] = b; out[2 * nref + i] = c;
+}
+
+__global__ void fill_f32_kernel(float *p, long long n, float v)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = v;
+}
+
+void launch_import_lattice(const Geom &g, int storage, const double *fn_ref, void *gout,
+                           const uint32_t *mask2d, float scale, cudaStream_t s)
+{
+    const unsigned blocks = (unsigned)((g.nint + 255) / 256);
+    if (storage == RBC_STORE_F16)
+        import_lattice_kernel<RBC_STORE_F16><<<blocks, 256, 0, s>>>(g, fn_ref, (__half *)gout, mask2d, scale);
+    else
+        import_lattice_kernel<RBC_STORE_F32><<<blocks, 256, 0, s>>>(g, fn_ref, (float *)gout, mask2d, scale);
+}
+
+void launch_export_lattice(const Geom &g, int storage, const void *gin, const uint32_t *mask2d,
+                           const float *rho, const float *ux, const float *uy, const float *uz,
+                           float inv_scale, double *fn_ref, double *dn, double *un, double *vn,
+                           double *wn, cudaStream_t s)
+{
+    const long long nref = g.plane * g.nzr;
+    const unsigned blocks = (unsigned)((nref + 255) / 256);
+    if (storage == RBC_STORE_F16)
+        export_lattice_kernel<RBC_STORE_F16><<<blocks, 256, 0, s>>>(g, (const __half *)gin, mask2d, rho, ux, uy, uz,
+                                                                     inv_scale, fn_ref, dn, un, vn, wn);
+    else
+        export_lattice_kernel<RBC_STORE_F32><<<blocks, 256, 0, s>>>(g, (const float *)gin, mask2d, rho, ux, uy, uz,
+                                                                     inv_scale, fn_ref, dn, un, vn, wn);
+}
+
+void launch_export_force(const Geom &g, const float *Fx, const float *Fy, const float *Fz,
+                         const uint32_t *mask2d, double *out3, cudaStream_t s)
+{
+    const long long nref = g.plane * g.nzr;
+    export_force_kernel<<<(unsigned)((nref + 255) / 256), 256, 0, s>>>(g, Fx, Fy, Fz, mask2d, out3);
+}
+
+void launch_fill_f32(float *p, long long n, float v, cudaStream_t s)
+{
+    if (n <= 0) return;
+    fill_f32_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(p, n, v);
+}
+
+}  // namespace rbc

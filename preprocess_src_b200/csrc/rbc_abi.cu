@@ -1,0 +1,899 @@
+// rbc_abi.cu -- host side of the C ABI declared in include/rbc_step.h.
+//
+// Owns the device state of one simulation and sequences the step kernels on
+// one CUDA stream.  rbc_step replays CUDA graphs of one step (two graphs, one
+// per population-buffer parity, since the buffers ping-pong); the reference
+// instead launches each module with a blocking
+// cudaThreadSynchronize() and host round trips inside the membrane solve and
+// the volume correction (main.cu:73-110).
+#include "rbc_internal.cuh"
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+using namespace rbc;
+
+namespace {
+
+thread_local std::string g_create_error;
+
+constexpr float F16_SCALE = 32768.0f;     // (f - w) * 2^15 keeps |g| < 2 inside FP16 range
+constexpr int DEFAULT_SOLVER_ITERS = 20;  // Chebyshev error factor <= 2 * 3^-20 ~ 6e-10
+constexpr int KERNELS_PER_STEP = 6;       // step_begin, membrane, spread, lbm, advect, volume
+
+}  // namespace
+
+struct rbc_handle {
+    rbc_params p{};
+    Geom geo{};
+    int ncell = 0, V = 0, E = 0;
+    long long nv = 0, ne = 0, nref_nodes = 0;
+    cudaStream_t stream = nullptr;
+    // lattice
+    void *g[2] = {nullptr, nullptr};
+    int cur = 0;
+    size_t gbytes = 0;
+    float *rho = nullptr, *ux = nullptr, *uy = nullptr, *uz = nullptr;
+    float *Fx = nullptr, *Fy = nullptr, *Fz = nullptr;
+    uint32_t *mask2d = nullptr;
+    // cells
+    double *X = nullptr, *Xd = nullptr, *nref = nullptr;
+    float *U = nullptr, *Fv = nullptr;
+    int *tri = nullptr, *v2e_off = nullptr, *v2e = nullptr;
+    int16_t *nbr = nullptr;
+    double *vol0 = nullptr, *gx = nullptr, *vol_out = nullptr, *area_out = nullptr, *cen_out = nullptr;
+    // device scalars: iter, flags, vc_max, vc_last
+    int *d_int = nullptr;
+    float *d_drive = nullptr;
+    // host<->reference staging
+    void *staging = nullptr;
+    size_t staging_bytes = 0;
+    int iter = 0;
+    bool force_pending = false;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};   // one step starting from buffer 0 / buffer 1
+    long long launches = 0;
+    float scale = 1.0f, inv_scale = 1.0f;
+    std::string err;
+    int device = 0;
+
+    int *d_iter() { return d_int; }
+    int *d_flags() { return d_int + 1; }
+    int *d_vcmax() { return d_int + 2; }
+    int *d_vclast() { return d_int + 3; }
+};
+
+#define CK(call)                                                                       \
+    do {                                                                               \
+        cudaError_t e_ = (call);                                                       \
+        if (e_ != cudaSuccess) {                                                       \
+            h->err = std::string(#call) + ": " + cudaGetErrorString(e_);               \
+            return RBC_ERR_CUDA;                                                       \
+        }                                                                              \
+    } while (0)
+
+#define RBC_DEVICE_GUARD(h)                                                            \
+    do {                                                                               \
+        if (cudaSetDevice((h)->device) != cudaSuccess) return RBC_ERR_CUDA;            \
+    } while (0)
+
+#define CK_LAUNCH()                                                                    \
+    do {                                                                               \
+        cudaError_t e_ = cudaGetLastError();                                           \
+        if (e_ != cudaSuccess) {                                                       \
+            h->err = std::string("kernel launch: ") + cudaGetErrorString(e_);          \
+            return RBC_ERR_CUDA;                                                       \
+        }                                                                              \
+    } while (0)
+
+namespace {
+
+int fail(rbc_handle *h, int code, const std::string &msg)
+{
+    if (h) h->err = msg; else g_create_error = msg;
+    return code;
+}
+
+template <typename T>
+int dalloc(rbc_handle *h, T **p, size_t count)
+{
+    CK(cudaMalloc((void **)p, sizeof(T) * (count ? count : 1)));
+    return RBC_OK;
+}
+
+int ensure_staging(rbc_handle *h, size_t bytes)
+{
+    if (h->staging_bytes >= bytes) return RBC_OK;
+    if (h->staging) { CK(cudaFree(h->staging)); h->staging = nullptr; h->staging_bytes = 0; }
+    CK(cudaMalloc(&h->staging, bytes));
+    h->staging_bytes = bytes;
+    return RBC_OK;
+}
+
+double drive_factor(const rbc_params &p, int iter)
+{
+    // lbm.cu:1030-1035
+    return (iter > p.flowstart) ? 1.0 + 0.5 * std::sin(M_PI * p.dt * (double)iter / p.freq) : 0.0;
+}
+
+// Link tables of the shared local connectivity (init2.cu:258-400): neighbour
+// lists in the order add_nlink builds them, vertex -> element lists in element
+// order (add_elink), the reference's link-count check, and the packed
+// incidence entries used by the membrane and volume kernels.
+int build_topology(rbc_handle *h, const int *tri, std::vector<int> &off, std::vector<int> &packed,
+                   std::vector<int16_t> &nbr6)
+{
+    const int V = h->V, E = h->E;
+    std::vector<std::vector<int>> nl(V), el(V);
+    auto add = [&](int a, int b) {
+        for (int x : nl[a]) if (x == b) return;
+        nl[a].push_back(b);
+    };
+    for (int e = 0; e < E; e++) {
+        const int a = tri[3 * e], b = tri[3 * e + 1], c = tri[3 * e + 2];
+        if (a < 0 || a >= V || b < 0 || b >= V || c < 0 || c >= V || a == b || b == c || a == c)
+            return fail(h, RBC_ERR_TOPOLOGY, "triangle " + std::to_string(e) + " has invalid vertex ids");
+        add(a, b); add(a, c); add(b, c); add(b, a); add(c, a); add(c, b);
+        el[a].push_back(e); el[b].push_back(e); el[c].push_back(e);
+    }
+    long long links = 0;
+    for (int i = 0; i < V; i++) {
+        links += (long long)nl[i].size();
+        if (nl[i].size() > 6 || el[i].size() > 6)
+            return fail(h, RBC_ERR_TOPOLOGY, "vertex " + std::to_string(i) + " has valence above 6 (the reference's link tables hold 6)");
+        if (nl[i].size() != el[i].size() || nl[i].size() < 3)
+            return fail(h, RBC_ERR_TOPOLOGY, "mesh is not a closed manifold at vertex " + std::to_string(i));
+    }
+    if (links != 2LL * (V + E - 2))   // init2.cu:369-370
+        return fail(h, RBC_ERR_TOPOLOGY, "link count check failed (closed genus-0 mesh expected)");
+    off.assign(V + 1, 0);
+    packed.clear();
+    nbr6.assign((size_t)6 * V, (int16_t)-1);
+    for (int i = 0; i < V; i++) {
+        off[i] = (int)packed.size();
+        for (size_t s = 0; s < nl[i].size(); s++) nbr6[s * V + i] = (int16_t)nl[i][s];
+        for (int e : el[i]) {
+            int en = (tri[3 * e] == i) ? 0 : (tri[3 * e + 1] == i ? 1 : 2);
+            const int o1 = tri[3 * e + (en + 1) % 3], o2 = tri[3 * e + (en + 2) % 3];
+            int sa = -1, sb = -1;
+            for (size_t s = 0; s < nl[i].size(); s++) {
+                if (nl[i][s] == o1) sa = (int)s;
+                if (nl[i][s] == o2) sb = (int)s;
+            }
+            if (sa < 0 || sb < 0) return fail(h, RBC_ERR_TOPOLOGY, "inconsistent incidence");
+            packed.push_back((int)((unsigned)e | ((unsigned)en << 24) | ((unsigned)sa << 26) | ((unsigned)sb << 29)));
+        }
+    }
+    off[V] = (int)packed.size();
+    return RBC_OK;
+}
+
+// set_contravariant (init2.cu:206-255) on the AoS reference shape; output [3][ne]
+void reference_metric(const rbc_handle *h, const int *tri, const double *xr, std::vector<double> &nref)
+{
+    const long long ne = h->ne;
+    nref.assign(3 * ne, 0.0);
+    for (int c = 0; c < h->ncell; c++)
+        for (int e = 0; e < h->E; e++) {
+            const long long a = (long long)c * h->V + tri[3 * e], b = (long long)c * h->V + tri[3 * e + 1],
+                            cc = (long long)c * h->V + tri[3 * e + 2];
+            double v1[3], v2[3];
+            for (int j = 0; j < 3; j++) { v1[j] = xr[3 * b + j] - xr[3 * a + j]; v2[j] = xr[3 * cc + j] - xr[3 * a + j]; }
+            const double lv1 = v1[0] * v1[0] + v1[1] * v1[1] + v1[2] * v1[2];
+            const double lv2 = v2[0] * v2[0] + v2[1] * v2[1] + v2[2] * v2[2];
+            const double inv12 = v1[0] * v2[0] + v1[1] * v2[1] + v1[2] * v2[2];
+            const double dv12 = lv1 * lv2 - inv12 * inv12;
+            const long long id = (long long)c * h->E + e;
+            nref[id] = lv2 / dv12;
+            nref[ne + id] = -inv12 / dv12;
+            nref[2 * ne + id] = lv1 / dv12;
+        }
+}
+
+// volume_init (volume_correction.cu:427-450): V0 and the wrapped centroid
+void initial_volume(const rbc_handle *h, const int *tri, const double *xr, std::vector<double> &vol0,
+                    std::vector<double> &gx)
+{
+    const int N = h->ncell, V = h->V;
+    vol0.assign(N, 0.0);
+    gx.assign(3 * N, 0.0);
+    for (int c = 0; c < N; c++) {
+        double vs = 0.0;
+        for (int e = 0; e < h->E; e++) {
+            const double *pa = xr + 3 * ((long long)c * V + tri[3 * e]);
+            const double *pb = xr + 3 * ((long long)c * V + tri[3 * e + 1]);
+            const double *pc = xr + 3 * ((long long)c * V + tri[3 * e + 2]);
+            const double v1[3] = {pb[0] - pa[0], pb[1] - pa[1], pb[2] - pa[2]};
+            const double v2[3] = {pc[0] - pa[0], pc[1] - pa[1], pc[2] - pa[2]};
+            const double cr[3] = {v1[1] * v2[2] - v1[2] * v2[1], v1[2] * v2[0] - v1[0] * v2[2], v1[0] * v2[1] - v1[1] * v2[0]};
+            const double nn = std::sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]);
+            const double dS = nn / 2.0;
+            const double r[3] = {(pa[0] + pb[0] + pc[0]) / 3.0, (pa[1] + pb[1] + pc[1]) / 3.0, (pa[2] + pb[2] + pc[2]) / 3.0};
+            vs += 1.0 / 3.0 * (r[0] * cr[0] / nn + r[1] * cr[1] / nn + r[2] * cr[2] / nn) * dS;
+        }
+        vol0[c] = vs;
+        double s[3] = {0, 0, 0};
+        for (int j = 0; j < V; j++)
+            for (int k = 0; k < 3; k++) s[k] += xr[3 * ((long long)c * V + j) + k];
+        for (int k = 0; k < 3; k++) s[k] /= (double)V;
+        if (s[2] < h->p.zmin) s[2] += h->p.LZ; else if (s[2] > h->p.zmax) s[2] -= h->p.LZ;
+        gx[c] = s[0]; gx[N + c] = s[1]; gx[2 * N + c] = s[2];
+    }
+}
+
+int check_params(const rbc_params *p)
+{
+    if (!p) return fail(nullptr, RBC_ERR_ARG, "params is NULL");
+    if (p->nx < 3 || p->ny < 3 || p->nz < 9)
+        return fail(nullptr, RBC_ERR_ARG, "lattice too small (nx, ny >= 3, nz >= 9 including the 4 BUFF planes)");
+    if ((long long)p->nx * p->ny > (1LL << 30) || (long long)p->nx * p->ny * p->nz > (1LL << 40))
+        return fail(nullptr, RBC_ERR_ARG, "lattice too large");
+    if (!(p->dx > 0) || !(p->dt > 0) || !(p->tau > 0.5) || !(p->Cr > 0))
+        return fail(nullptr, RBC_ERR_ARG, "dx, dt, Cr must be > 0 and tau > 1/2");
+    if (!(p->LX > 0) || !(p->LZ > 0)) return fail(nullptr, RBC_ERR_ARG, "LX and LZ must be > 0");
+    if (p->M != 1) return fail(nullptr, RBC_ERR_UNSUPPORTED, "only M = 1 (no sub-cycling) is implemented");
+    if (p->rk_order != 4) return fail(nullptr, RBC_ERR_UNSUPPORTED, "only RUNGE_KUTTA = 4 is implemented");
+    if (p->br != 0.0) return fail(nullptr, RBC_ERR_UNSUPPORTED, "bending (BR != 0) is not implemented");
+    if (p->storage != RBC_STORE_F32 && p->storage != RBC_STORE_F16) return fail(nullptr, RBC_ERR_ARG, "unknown storage");
+    if (p->law != RBC_LAW_SKALAK && p->law != RBC_LAW_NEOHOOKEAN) return fail(nullptr, RBC_ERR_ARG, "unknown law");
+    if (p->solver_iters < 0 || p->solver_iters > 200) return fail(nullptr, RBC_ERR_ARG, "solver_iters out of range");
+    return RBC_OK;
+}
+
+// Wall mask of one z plane from the reference bc map; checks z invariance.
+int build_mask(const rbc_params *p, const int *bc, std::vector<uint32_t> &mask)
+{
+    const int nx = p->nx, ny = p->ny, nz = p->nz;
+    const long long plane = (long long)nx * ny;
+    mask.assign(plane, 0u);
+    std::vector<char> fluid(plane, 0);
+    for (long long xy = 0; xy < plane; xy++) {
+        const int t = bc[2 * plane + xy];
+        if (t != RBC_COMP && t != RBC_WALL)
+            return fail(nullptr, RBC_ERR_ARG, "bc: first COMP plane (z = 2) holds a value other than COMP/WALL");
+        fluid[xy] = (t == RBC_COMP);
+        for (int z = 2; z < nz - 2; z++)
+            if (bc[z * plane + xy] != t)
+                return fail(nullptr, RBC_ERR_UNSUPPORTED, "bc: wall pattern must be the same in every COMP plane");
+        const int want = fluid[xy] ? RBC_BUFF : RBC_WALL;
+        for (int z : {0, 1, nz - 2, nz - 1})
+            if (bc[z * plane + xy] != want)
+                return fail(nullptr, RBC_ERR_ARG, "bc: BUFF planes must be BUFF over fluid columns and WALL elsewhere");
+        const int x = (int)(xy % nx), y = (int)(xy / nx);
+        if (fluid[xy] && (x == 0 || y == 0 || x == nx - 1 || y == ny - 1))
+            return fail(nullptr, RBC_ERR_ARG, "bc: fluid node on the lattice edge (walls must enclose the channel)");
+    }
+    for (long long xy = 0; xy < plane; xy++) {
+        if (!fluid[xy]) continue;
+        const int x = (int)(xy % nx), y = (int)(xy / nx);
+        uint32_t m = MASK_FLUID;
+        for (int q = 1; q < Q; q++) {
+            const int sx = x - ex(q), sy = y - ey(q);
+            if (!fluid[sx + (long long)nx * sy]) m |= (1u << q);
+        }
+        mask[xy] = m;
+    }
+    return RBC_OK;
+}
+
+void free_all(rbc_handle *h)
+{
+    if (!h) return;
+    for (cudaGraphExec_t g : h->graph) if (g) cudaGraphExecDestroy(g);
+    void *ptrs[] = {h->g[0], h->g[1], h->rho, h->ux, h->uy, h->uz, h->Fx, h->Fy, h->Fz, h->mask2d,
+                    h->X, h->Xd, h->nref, h->U, h->Fv, h->tri, h->v2e_off, h->v2e, h->nbr, h->vol0, h->gx,
+                    h->vol_out, h->area_out, h->cen_out, h->d_int, h->d_drive, h->staging};
+    for (void *q : ptrs) if (q) cudaFree(q);
+    if (h->stream) cudaStreamDestroy(h->stream);
+}
+
+// ---- stage launches -------------------------------------------------------
+
+int launch_stress(rbc_handle *h)
+{
+    if (h->ncell == 0) return RBC_OK;
+    MembraneArgs a{};
+    a.Xd = h->Xd; a.nv = h->nv; a.ne = h->ne; a.nref = h->nref;
+    a.tri = h->tri; a.v2e_off = h->v2e_off; a.v2e = h->v2e; a.nbr = h->nbr; a.Fv = h->Fv;
+    a.V = h->V; a.E = h->E; a.ncell = h->ncell;
+    a.C = h->p.C; a.rgs = h->p.rgs; a.law = h->p.law; a.LX = h->p.LX; a.LZ = h->p.LZ;
+    a.niter = h->p.solver_iters > 0 ? h->p.solver_iters : DEFAULT_SOLVER_ITERS;
+    a.flags = h->d_flags();
+    launch_membrane(a, h->p.membrane_fp64 != 0, h->stream);
+    h->launches++;
+    CK_LAUNCH();
+    return RBC_OK;
+}
+
+int launch_spread_stage(rbc_handle *h)
+{
+    if (h->ncell == 0) return RBC_OK;
+    SpreadArgs a{};
+    a.X = h->X; a.nv = h->nv; a.V = h->V; a.ncell = h->ncell; a.Fv = h->Fv;
+    a.Fx = h->Fx; a.Fy = h->Fy; a.Fz = h->Fz; a.mask2d = h->mask2d; a.flags = h->d_flags();
+    launch_spread(h->geo, a, h->stream);
+    h->launches++;
+    CK_LAUNCH();
+    return RBC_OK;
+}
+
+int launch_lbm_stage(rbc_handle *h)
+{
+    LbmArgs a{};
+    a.gin = h->g[h->cur]; a.gout = h->g[1 - h->cur];
+    a.rho = h->rho; a.ux = h->ux; a.uy = h->uy; a.uz = h->uz;
+    a.Fx = h->Fx; a.Fy = h->Fy; a.Fz = h->Fz; a.mask2d = h->mask2d; a.drive = h->d_drive;
+    a.omega = (float)(1.0 / h->p.tau); a.Cr = (float)h->p.Cr; a.Bc = (float)h->p.B;
+    a.scale = h->scale; a.inv_scale = h->inv_scale;
+    launch_lbm(h->geo, h->p.storage, a, h->stream);
+    h->launches++;
+    CK_LAUNCH();
+    h->cur ^= 1;
+    return RBC_OK;
+}
+
+int launch_advect_stage(rbc_handle *h)
+{
+    if (h->ncell == 0) return RBC_OK;
+    AdvectArgs a{};
+    a.X = h->X; a.Xd = h->Xd; a.U = h->U; a.ux = h->ux; a.uy = h->uy; a.uz = h->uz; a.nv = h->nv;
+    a.dtM = h->p.dt * h->p.M; a.flags = h->d_flags();
+    launch_advect(h->geo, a, h->stream);
+    h->launches++;
+    CK_LAUNCH();
+    return RBC_OK;
+}
+
+VolumeArgs volume_args(rbc_handle *h, int correct)
+{
+    VolumeArgs a{};
+    a.X = h->X; a.nv = h->nv; a.tri = h->tri; a.v2e_off = h->v2e_off; a.v2e = h->v2e;
+    a.vol0 = h->vol0; a.gx = h->gx; a.vol_out = h->vol_out; a.area_out = h->area_out; a.cen_out = h->cen_out;
+    a.V = h->V; a.E = h->E; a.ncell = h->ncell;
+    a.flags = h->d_flags(); a.vc_max = h->d_vcmax(); a.vc_last = h->d_vclast();
+    a.correct = correct;
+    return a;
+}
+
+int launch_volume_stage(rbc_handle *h)
+{
+    if (h->ncell == 0) return RBC_OK;
+    CK(cudaMemsetAsync(h->d_vclast(), 0, sizeof(int), h->stream));
+    launch_volume(h->geo, volume_args(h, 1), h->stream);
+    h->launches++;
+    CK_LAUNCH();
+    return RBC_OK;
+}
+
+// one full step (main.cu:73-110 with M = 1); the device increments iter
+int enqueue_step(rbc_handle *h)
+{
+    int rc;
+    launch_step_begin(h->d_iter(), h->d_drive, h->p.P, h->p.flowstart, h->p.freq, h->p.dt, h->stream);
+    h->launches++;
+    CK_LAUNCH();
+    if ((rc = launch_stress(h))) return rc;
+    if ((rc = launch_spread_stage(h))) return rc;
+    if ((rc = launch_lbm_stage(h))) return rc;
+    if ((rc = launch_advect_stage(h))) return rc;
+    if ((rc = launch_volume_stage(h))) return rc;
+    return RBC_OK;
+}
+
+// CUDA graph of one step starting from population buffer c (the step flips
+// the buffers, so two graphs alternate)
+int build_graph(rbc_handle *h, int c)
+{
+    cudaGraph_t graph = nullptr;
+    const long long launches0 = h->launches;
+    const int cur0 = h->cur;
+    h->cur = c;
+    CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = enqueue_step(h);
+    cudaError_t e = cudaStreamEndCapture(h->stream, &graph);
+    h->launches = launches0;
+    h->cur = cur0;
+    if (rc != RBC_OK) { if (graph) cudaGraphDestroy(graph); return rc; }
+    if (e != cudaSuccess) { h->err = std::string("graph capture: ") + cudaGetErrorString(e); return RBC_ERR_CUDA; }
+    e = cudaGraphInstantiate(&h->graph[c], graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) { h->graph[c] = nullptr; h->err = std::string("graph instantiate: ") + cudaGetErrorString(e); return RBC_ERR_CUDA; }
+    return RBC_OK;
+}
+
+int prepare_steps(rbc_handle *h)
+{
+    if (h->force_pending) {
+        CK(cudaMemsetAsync(h->Fx, 0, 4 * h->geo.nint, h->stream));
+        CK(cudaMemsetAsync(h->Fy, 0, 4 * h->geo.nint, h->stream));
+        CK(cudaMemsetAsync(h->Fz, 0, 4 * h->geo.nint, h->stream));
+        h->force_pending = false;
+    }
+    // the device counter follows the host's prc->iter mirror
+    CK(cudaMemcpyAsync(h->d_iter(), &h->iter, sizeof(int), cudaMemcpyHostToDevice, h->stream));
+    return RBC_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+
+extern "C" {
+
+const char *rbc_last_error(const rbc_handle *h)
+{
+    return h ? h->err.c_str() : g_create_error.c_str();
+}
+
+int rbc_create(const rbc_params *p, const rbc_mesh *mesh, const int *bc, rbc_handle **out)
+{
+    g_create_error.clear();
+    if (!out) return fail(nullptr, RBC_ERR_ARG, "out is NULL");
+    *out = nullptr;
+    int rc = check_params(p);
+    if (rc) return rc;
+    if (!bc) return fail(nullptr, RBC_ERR_ARG, "bc is NULL");
+    std::vector<uint32_t> mask;
+    if ((rc = build_mask(p, bc, mask))) return rc;
+    const bool cells = mesh && mesh->ncell > 0;
+    if (cells) {
+        if (mesh->vertex < 4 || mesh->element < 4 || !mesh->tri || !mesh->xr)
+            return fail(nullptr, RBC_ERR_ARG, "mesh needs vertex, element >= 4, tri and xr");
+        if (membrane_smem_bytes(mesh->vertex) > 227 * 1024 || mesh->vertex > 4096)
+            return fail(nullptr, RBC_ERR_UNSUPPORTED, "more vertices per cell than one CTA holds (max 3874)");
+        if (mesh->element >= (1 << 24)) return fail(nullptr, RBC_ERR_UNSUPPORTED, "too many elements per cell");
+    }
+    rbc_handle *h = new (std::nothrow) rbc_handle();
+    if (!h) return fail(nullptr, RBC_ERR_ARG, "out of host memory");
+    h->p = *p;
+    if (h->p.solver_iters == 0) h->p.solver_iters = DEFAULT_SOLVER_ITERS;
+    Geom &g = h->geo;
+    g.nx = p->nx; g.ny = p->ny; g.nzr = p->nz; g.nzc = p->nz - 4;
+    g.plane = (long long)p->nx * p->ny; g.nint = g.plane * g.nzc;
+    g.dx = p->dx;
+    g.xoff = (double)(p->nx - 1) * p->dx / 2.0;
+    g.yoff = (double)(p->ny - 1) * p->dx / 2.0;
+    g.zoff = (double)(p->nz - 1) * p->dx / 2.0;
+    g.LX = p->LX; g.LZ = p->LZ; g.xmin = p->xmin; g.xmax = p->xmax; g.zmin = p->zmin; g.zmax = p->zmax;
+    h->nref_nodes = g.plane * g.nzr;
+    if (p->storage == RBC_STORE_F16) { h->scale = F16_SCALE; h->inv_scale = 1.0f / F16_SCALE; }
+
+    auto bail = [&](int code) {
+        g_create_error = h->err;
+        free_all(h);
+        delete h;
+        return code;
+    };
+#define TRY(x) do { int r_ = (x); if (r_) return bail(r_); } while (0)
+    // host-side setup first, so argument and mesh errors are reported without a GPU
+    std::vector<int> off, packed;
+    std::vector<int16_t> nbr6;
+    std::vector<double> nref, vol0, gx, xs;
+    if (cells) {
+        h->ncell = mesh->ncell; h->V = mesh->vertex; h->E = mesh->element;
+        h->nv = (long long)h->ncell * h->V; h->ne = (long long)h->ncell * h->E;
+        TRY(build_topology(h, mesh->tri, off, packed, nbr6));
+        reference_metric(h, mesh->tri, mesh->xr, nref);
+        initial_volume(h, mesh->tri, mesh->xr, vol0, gx);
+        xs.resize(3 * h->nv);
+        for (long long j = 0; j < h->nv; j++)
+            for (int k = 0; k < 3; k++) xs[k * h->nv + j] = mesh->xr[3 * j + k];
+    }
+    {
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+            cudaGetLastError();
+            h->err = "no CUDA device";
+            return bail(RBC_ERR_NO_DEVICE);
+        }
+        h->device = p->device >= 0 ? p->device : 0;
+        if (h->device >= ndev) { h->err = "device ordinal out of range"; return bail(RBC_ERR_ARG); }
+        if (cudaSetDevice(h->device) != cudaSuccess) { h->err = "cudaSetDevice failed"; return bail(RBC_ERR_CUDA); }
+    }
+    {
+        int e = setup_kernel_attributes();
+        if (e) { h->err = std::string("kernel attributes: ") + cudaGetErrorString((cudaError_t)e); return bail(RBC_ERR_CUDA); }
+    }
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        h->err = "stream creation failed";
+        return bail(RBC_ERR_CUDA);
+    }
+    const size_t esz = p->storage == RBC_STORE_F16 ? 2 : 4;
+    h->gbytes = esz * (size_t)Q * (size_t)g.nint;
+    if (cudaMalloc(&h->g[0], h->gbytes) != cudaSuccess || cudaMalloc(&h->g[1], h->gbytes) != cudaSuccess) {
+        h->err = "out of device memory for the populations";
+        return bail(RBC_ERR_CUDA);
+    }
+    TRY(dalloc(h, &h->rho, g.nint)); TRY(dalloc(h, &h->ux, g.nint)); TRY(dalloc(h, &h->uy, g.nint));
+    TRY(dalloc(h, &h->uz, g.nint)); TRY(dalloc(h, &h->Fx, g.nint)); TRY(dalloc(h, &h->Fy, g.nint));
+    TRY(dalloc(h, &h->Fz, g.nint)); TRY(dalloc(h, &h->mask2d, g.plane));
+    TRY(dalloc(h, &h->d_int, 4)); TRY(dalloc(h, &h->d_drive, 1));
+    if (cudaMemset(h->g[0], 0, h->gbytes) != cudaSuccess || cudaMemset(h->g[1], 0, h->gbytes) != cudaSuccess ||
+        cudaMemset(h->ux, 0, 4 * g.nint) != cudaSuccess || cudaMemset(h->uy, 0, 4 * g.nint) != cudaSuccess ||
+        cudaMemset(h->uz, 0, 4 * g.nint) != cudaSuccess || cudaMemset(h->Fx, 0, 4 * g.nint) != cudaSuccess ||
+        cudaMemset(h->Fy, 0, 4 * g.nint) != cudaSuccess || cudaMemset(h->Fz, 0, 4 * g.nint) != cudaSuccess ||
+        cudaMemset(h->d_int, 0, 4 * sizeof(int)) != cudaSuccess || cudaMemset(h->d_drive, 0, sizeof(float)) != cudaSuccess ||
+        cudaMemcpy(h->mask2d, mask.data(), 4 * g.plane, cudaMemcpyHostToDevice) != cudaSuccess) {
+        h->err = "device initialisation failed";
+        return bail(RBC_ERR_CUDA);
+    }
+    launch_fill_f32(h->rho, g.nint, 1.0f, h->stream);
+
+    if (cells) {
+        TRY(dalloc(h, &h->X, 3 * h->nv)); TRY(dalloc(h, &h->Xd, 3 * h->nv)); TRY(dalloc(h, &h->nref, 3 * h->ne));
+        TRY(dalloc(h, &h->U, 3 * h->nv)); TRY(dalloc(h, &h->Fv, 3 * h->nv));
+        TRY(dalloc(h, &h->tri, 3 * h->E)); TRY(dalloc(h, &h->v2e_off, h->V + 1)); TRY(dalloc(h, &h->v2e, packed.size()));
+        TRY(dalloc(h, &h->nbr, 6 * h->V));
+        TRY(dalloc(h, &h->vol0, h->ncell)); TRY(dalloc(h, &h->gx, 3 * h->ncell));
+        TRY(dalloc(h, &h->vol_out, h->ncell)); TRY(dalloc(h, &h->area_out, h->ncell)); TRY(dalloc(h, &h->cen_out, 3 * h->ncell));
+        if (cudaMemcpy(h->X, xs.data(), 8 * 3 * h->nv, cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(h->Xd, xs.data(), 8 * 3 * h->nv, cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(h->nref, nref.data(), 8 * 3 * h->ne, cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemset(h->U, 0, 4 * 3 * h->nv) != cudaSuccess || cudaMemset(h->Fv, 0, 4 * 3 * h->nv) != cudaSuccess ||
+            cudaMemcpy(h->tri, mesh->tri, 4 * 3 * h->E, cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(h->v2e_off, off.data(), 4 * (h->V + 1), cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(h->v2e, packed.data(), 4 * packed.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(h->nbr, nbr6.data(), 2 * 6 * h->V, cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(h->vol0, vol0.data(), 8 * h->ncell, cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(h->gx, gx.data(), 8 * 3 * h->ncell, cudaMemcpyHostToDevice) != cudaSuccess) {
+            h->err = "cell upload failed";
+            return bail(RBC_ERR_CUDA);
+        }
+    }
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
+        h->err = "initialisation kernels failed";
+        return bail(RBC_ERR_CUDA);
+    }
+#undef TRY
+    *out = h;
+    return RBC_OK;
+}
+
+int rbc_destroy(rbc_handle *h)
+{
+    if (!h) return RBC_OK;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    free_all(h);
+    delete h;
+    return RBC_OK;
+}
+
+int rbc_import_ref_lattice(rbc_handle *h, const double *fn)
+{
+    if (!h || !fn) return RBC_ERR_ARG;
+    RBC_DEVICE_GUARD(h);
+    const size_t bytes = sizeof(double) * Q * (size_t)h->nref_nodes;
+    int rc = ensure_staging(h, bytes);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(h->staging, fn, bytes, cudaMemcpyHostToDevice, h->stream));
+    launch_import_lattice(h->geo, h->p.storage, (const double *)h->staging, h->g[h->cur], h->mask2d, h->scale, h->stream);
+    h->launches++;
+    CK_LAUNCH();
+    CK(cudaStreamSynchronize(h->stream));
+    return RBC_OK;
+}
+
+int rbc_export_ref_lattice(rbc_handle *h, double *fn, double *dn, double *un, double *vn, double *wn)
+{
+    if (!h) return RBC_ERR_ARG;
+    RBC_DEVICE_GUARD(h);
+    const bool macro = dn || un || vn || wn;
+    if (!fn && !macro) return RBC_OK;
+    const size_t n = (size_t)h->nref_nodes;
+    int rc = ensure_staging(h, sizeof(double) * n * (fn ? (Q + 4) : 4));
+    if (rc) return rc;
+    double *sfn = (double *)h->staging;
+    double *smac = fn ? sfn + Q * n : sfn;
+    launch_export_lattice(h->geo, h->p.storage, h->g[h->cur], h->mask2d, h->rho, h->ux, h->uy, h->uz, h->inv_scale,
+                          fn ? sfn : nullptr, macro ? smac : nullptr, smac + n, smac + 2 * n, smac + 3 * n, h->stream);
+    h->launches++;
+    CK_LAUNCH();
+    if (fn) CK(cudaMemcpyAsync(fn, sfn, sizeof(double) * Q * n, cudaMemcpyDeviceToHost, h->stream));
+    if (dn) CK(cudaMemcpyAsync(dn, smac, sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream));
+    if (un) CK(cudaMemcpyAsync(un, smac + n, sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream));
+    if (vn) CK(cudaMemcpyAsync(vn, smac + 2 * n, sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream));
+    if (wn) CK(cudaMemcpyAsync(wn, smac + 3 * n, sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return RBC_OK;
+}
+
+int rbc_export_ref_force(rbc_handle *h, double *fx, double *fy, double *fz)
+{
+    if (!h) return RBC_ERR_ARG;
+    RBC_DEVICE_GUARD(h);
+    const size_t n = (size_t)h->nref_nodes;
+    int rc = ensure_staging(h, sizeof(double) * 3 * n);
+    if (rc) return rc;
+    double *s = (double *)h->staging;
+    launch_export_force(h->geo, h->Fx, h->Fy, h->Fz, h->mask2d, s, h->stream);
+    h->launches++;
+    CK_LAUNCH();
+    if (fx) CK(cudaMemcpyAsync(fx, s, sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream));
+    if (fy) CK(cudaMemcpyAsync(fy, s + n, sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream));
+    if (fz) CK(cudaMemcpyAsync(fz, s + 2 * n, sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return RBC_OK;
+}
+
+int rbc_import_ref_cells(rbc_handle *h, const double *x, const double *y, const double *z,
+                         const double *xd, const double *nd, const double *volume0, const double *gx)
+{
+    if (!h) return RBC_ERR_ARG;
+    RBC_DEVICE_GUARD(h);
+    if (h->ncell == 0) return fail(h, RBC_ERR_STATE, "handle has no cells");
+    const long long nv = h->nv, ne = h->ne;
+    const int N = h->ncell;
+    CK(cudaStreamSynchronize(h->stream));
+    if (x) CK(cudaMemcpy(h->X, x, 8 * nv, cudaMemcpyHostToDevice));
+    if (y) CK(cudaMemcpy(h->X + nv, y, 8 * nv, cudaMemcpyHostToDevice));
+    if (z) CK(cudaMemcpy(h->X + 2 * nv, z, 8 * nv, cudaMemcpyHostToDevice));
+    if (xd) {
+        std::vector<double> t(3 * nv);
+        for (long long j = 0; j < nv; j++) for (int k = 0; k < 3; k++) t[k * nv + j] = xd[3 * j + k];
+        CK(cudaMemcpy(h->Xd, t.data(), 8 * 3 * nv, cudaMemcpyHostToDevice));
+    }
+    if (nd) {
+        std::vector<double> t(3 * ne);
+        for (long long e = 0; e < ne; e++) { t[e] = nd[4 * e]; t[ne + e] = nd[4 * e + 1]; t[2 * ne + e] = nd[4 * e + 3]; }
+        CK(cudaMemcpy(h->nref, t.data(), 8 * 3 * ne, cudaMemcpyHostToDevice));
+    }
+    if (volume0) CK(cudaMemcpy(h->vol0, volume0, 8 * N, cudaMemcpyHostToDevice));
+    if (gx) {
+        std::vector<double> t(3 * N);
+        for (int c = 0; c < N; c++) for (int k = 0; k < 3; k++) t[k * N + c] = gx[3 * c + k];
+        CK(cudaMemcpy(h->gx, t.data(), 8 * 3 * N, cudaMemcpyHostToDevice));
+    }
+    return RBC_OK;
+}
+
+int rbc_import_ref_vertex_force(rbc_handle *h, const double *fx, const double *fy, const double *fz)
+{
+    if (!h || !fx || !fy || !fz) return RBC_ERR_ARG;
+    RBC_DEVICE_GUARD(h);
+    if (h->ncell == 0) return fail(h, RBC_ERR_STATE, "handle has no cells");
+    const long long nv = h->nv;
+    std::vector<float> t(3 * nv);
+    for (long long j = 0; j < nv; j++) { t[j] = (float)fx[j]; t[nv + j] = (float)fy[j]; t[2 * nv + j] = (float)fz[j]; }
+    CK(cudaStreamSynchronize(h->stream));
+    CK(cudaMemcpy(h->Fv, t.data(), 4 * 3 * nv, cudaMemcpyHostToDevice));
+    return RBC_OK;
+}
+
+int rbc_export_ref_cells(rbc_handle *h, double *x, double *y, double *z, double *xd,
+                         double *u, double *v, double *w, double *fx, double *fy, double *fz, double *gxo)
+{
+    if (!h) return RBC_ERR_ARG;
+    RBC_DEVICE_GUARD(h);
+    if (h->ncell == 0) return fail(h, RBC_ERR_STATE, "handle has no cells");
+    const long long nv = h->nv;
+    const int N = h->ncell;
+    CK(cudaStreamSynchronize(h->stream));
+    if (x) CK(cudaMemcpy(x, h->X, 8 * nv, cudaMemcpyDeviceToHost));
+    if (y) CK(cudaMemcpy(y, h->X + nv, 8 * nv, cudaMemcpyDeviceToHost));
+    if (z) CK(cudaMemcpy(z, h->X + 2 * nv, 8 * nv, cudaMemcpyDeviceToHost));
+    if (xd) {
+        std::vector<double> t(3 * nv);
+        CK(cudaMemcpy(t.data(), h->Xd, 8 * 3 * nv, cudaMemcpyDeviceToHost));
+        for (long long j = 0; j < nv; j++) for (int k = 0; k < 3; k++) xd[3 * j + k] = t[k * nv + j];
+    }
+    if (u || v || w || fx || fy || fz) {
+        std::vector<float> t(6 * nv);
+        CK(cudaMemcpy(t.data(), h->U, 4 * 3 * nv, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(t.data() + 3 * nv, h->Fv, 4 * 3 * nv, cudaMemcpyDeviceToHost));
+        double *outs[6] = {u, v, w, fx, fy, fz};
+        for (int k = 0; k < 6; k++)
+            if (outs[k]) for (long long j = 0; j < nv; j++) outs[k][j] = t[k * nv + j];
+    }
+    if (gxo) {
+        std::vector<double> t(3 * N);
+        CK(cudaMemcpy(t.data(), h->gx, 8 * 3 * N, cudaMemcpyDeviceToHost));
+        for (int c = 0; c < N; c++) for (int k = 0; k < 3; k++) gxo[3 * c + k] = t[k * N + c];
+    }
+    return RBC_OK;
+}
+
+int rbc_set_iter(rbc_handle *h, int iter)
+{
+    if (!h) return RBC_ERR_ARG;
+    RBC_DEVICE_GUARD(h);
+    CK(cudaStreamSynchronize(h->stream));
+    h->iter = iter;
+    const float drive = (float)(h->p.P * drive_factor(h->p, iter));
+    CK(cudaMemcpy(h->d_iter(), &iter, sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(h->d_drive, &drive, sizeof(float), cudaMemcpyHostToDevice));
+    return RBC_OK;
+}
+
+int rbc_get_iter(const rbc_handle *h, int *iter)
+{
+    if (!h || !iter) return RBC_ERR_ARG;
+    *iter = h->iter;
+    return RBC_OK;
+}
+
+int rbc_stress(rbc_handle *h)
+{
+    if (!h) return RBC_ERR_ARG;
+    RBC_DEVICE_GUARD(h);
+    return launch_stress(h);
+}
+
+int rbc_ibm_st1(rbc_handle *h)
+{
+    if (!h) return RBC_ERR_ARG;
+    RBC_DEVICE_GUARD(h);
+    if (h->force_pending) {   // ibm_st1a: start from zero (ibm.cu:315-320)
+        CK(cudaMemsetAsync(h->Fx, 0, 4 * h->geo.nint, h->stream));
+        CK(cudaMemsetAsync(h->Fy, 0, 4 * h->geo.nint, h->stream));
+        CK(cudaMemsetAsync(h->Fz, 0, 4 * h->geo.nint, h->stream));
+    }
+    int rc = launch_spread_stage(h);
+    if (rc) return rc;
+    h->force_pending = true;
+    return RBC_OK;
+}
+
+int rbc_lbm_d3q19(rbc_handle *h)
+{
+    if (!h) return RBC_ERR_ARG;
+    RBC_DEVICE_GUARD(h);
+    int rc = launch_lbm_stage(h);
+    if (rc) return rc;
+    h->force_pending = false;   // the LBM kernel consumed and cleared the force
+    return RBC_OK;
+}
+
+int rbc_ibm_st2(rbc_handle *h)
+{
+    if (!h) return RBC_ERR_ARG;
+    RBC_DEVICE_GUARD(h);
+    return launch_advect_stage(h);
+}
+
+int rbc_volume_correction(rbc_handle *h, int *iters)
+{
+    if (!h) return RBC_ERR_ARG;
+    RBC_DEVICE_GUARD(h);
+    int rc = launch_volume_stage(h);
+    if (rc) return rc;
+    if (iters) {
+        int v = 0;
+        if (h->ncell > 0) {
+            CK(cudaMemcpyAsync(&v, h->d_vclast(), sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+            CK(cudaStreamSynchronize(h->stream));
+        }
+        *iters = v;
+    }
+    return RBC_OK;
+}
+
+int rbc_step(rbc_handle *h, int nsteps)
+{
+    if (!h || nsteps < 0) return RBC_ERR_ARG;
+    RBC_DEVICE_GUARD(h);
+    if (nsteps == 0) return RBC_OK;
+    int rc;
+    if ((rc = prepare_steps(h))) return rc;
+    for (int c = 0; c < 2; c++)
+        if (!h->graph[c] && (rc = build_graph(h, c))) return rc;
+    for (int k = 0; k < nsteps; k++) {
+        CK(cudaGraphLaunch(h->graph[h->cur], h->stream));
+        h->cur ^= 1;
+        h->launches += KERNELS_PER_STEP;
+    }
+    h->iter += nsteps;
+    return RBC_OK;
+}
+
+int rbc_profile_steps(rbc_handle *h, int nsteps, double *kernel_ms)
+{
+    if (!h || nsteps < 0 || !kernel_ms) return RBC_ERR_ARG;
+    RBC_DEVICE_GUARD(h);
+    for (int k = 0; k < RBC_NUM_KERNELS; k++) kernel_ms[k] = 0.0;
+    int rc;
+    if ((rc = prepare_steps(h))) return rc;
+    cudaEvent_t ev[RBC_NUM_KERNELS + 1];
+    for (auto &e : ev) CK(cudaEventCreate(&e));
+    for (int s = 0; s < nsteps && rc == RBC_OK; s++) {
+        cudaEventRecord(ev[0], h->stream);
+        launch_step_begin(h->d_iter(), h->d_drive, h->p.P, h->p.flowstart, h->p.freq, h->p.dt, h->stream);
+        h->launches++;
+        cudaEventRecord(ev[1], h->stream);
+        if (!rc) rc = launch_stress(h);
+        cudaEventRecord(ev[2], h->stream);
+        if (!rc) rc = launch_spread_stage(h);
+        cudaEventRecord(ev[3], h->stream);
+        if (!rc) rc = launch_lbm_stage(h);
+        cudaEventRecord(ev[4], h->stream);
+        if (!rc) rc = launch_advect_stage(h);
+        cudaEventRecord(ev[5], h->stream);
+        if (!rc) rc = launch_volume_stage(h);
+        cudaEventRecord(ev[6], h->stream);
+        if (cudaEventSynchronize(ev[6]) != cudaSuccess) { rc = RBC_ERR_CUDA; h->err = "profiled step failed"; break; }
+        for (int k = 0; k < RBC_NUM_KERNELS; k++) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, ev[k], ev[k + 1]);
+            kernel_ms[k] += ms;
+        }
+    }
+    for (auto &e : ev) cudaEventDestroy(e);
+    if (rc == RBC_OK) h->iter += nsteps;
+    return rc;
+}
+
+int rbc_get_stream(const rbc_handle *h, void **stream)
+{
+    if (!h || !stream) return RBC_ERR_ARG;
+    *stream = (void *)h->stream;
+    return RBC_OK;
+}
+
+int rbc_get_status(rbc_handle *h, int *flags, int *vc_iters_max)
+{
+    if (!h) return RBC_ERR_ARG;
+    RBC_DEVICE_GUARD(h);
+    int v[4];
+    CK(cudaStreamSynchronize(h->stream));
+    CK(cudaMemcpy(v, h->d_int, sizeof(v), cudaMemcpyDeviceToHost));
+    if (flags) *flags = v[1];
+    if (vc_iters_max) *vc_iters_max = v[2];
+    CK(cudaMemset(h->d_flags(), 0, sizeof(int)));
+    return RBC_OK;
+}
+
+int rbc_cell_metrics(rbc_handle *h, double *volume, double *area, double *centroid)
+{
+    if (!h) return RBC_ERR_ARG;
+    RBC_DEVICE_GUARD(h);
+    if (h->ncell == 0) return fail(h, RBC_ERR_STATE, "handle has no cells");
+    launch_volume(h->geo, volume_args(h, 0), h->stream);
+    h->launches++;
+    CK_LAUNCH();
+    const int N = h->ncell;
+    std::vector<double> t(5 * N);
+    CK(cudaMemcpyAsync(t.data(), h->vol_out, 8 * N, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(t.data() + N, h->area_out, 8 * N, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(t.data() + 2 * N, h->cen_out, 8 * 3 * N, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    for (int c = 0; c < N; c++) {
+        if (volume) volume[c] = t[c];
+        if (area) area[c] = t[N + c];
+        if (centroid) for (int k = 0; k < 3; k++) centroid[3 * c + k] = t[(2 + k) * N + c];
+    }
+    return RBC_OK;
+}
+
+int rbc_synchronize(rbc_handle *h)
+{
+    if (!h) return RBC_ERR_ARG;
+    RBC_DEVICE_GUARD(h);
+    CK(cudaStreamSynchronize(h->stream));
+    return RBC_OK;
+}
+
+int rbc_launch_count(const rbc_handle *h, long long *count)
+{
+    if (!h || !count) return RBC_ERR_ARG;
+    *count = h->launches;
+    return RBC_OK;
+}
+
+int rbc_dims(const rbc_handle *h, int *nx, int *ny, int *nz_periodic, int *ncell, int *vertex, int *element)
+{
+    if (!h) return RBC_ERR_ARG;
+    if (nx) *nx = h->geo.nx;
+    if (ny) *ny = h->geo.ny;
+    if (nz_periodic) *nz_periodic = h->geo.nzc;
+    if (ncell) *ncell = h->ncell;
+    if (vertex) *vertex = h->V;
+    if (element) *element = h->E;
+    return RBC_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,164 @@
+// rbc_internal.cuh -- shared definitions of the sm_100a step kernels.
+//
+// Internal layout in HBM (one handle):
+//   populations  g[q][z][y][x], q = 0..18 in the reference's slot order,
+//                x fastest, z = periodic axis without BUFF planes (nzc = nz - 4
+//                planes).  Each value is f_q - w_q of the post-collision state
+//                of the previous step (pull scheme), FP32 or scaled FP16.
+//   macroscopic  rho, ux, uy, uz [z][y][x] FP32 (ux..uz = the reference's
+//                um/vm/wm with M = 1, including the half-force shift).
+//   IB force     Fx, Fy, Fz [z][y][x] FP32; the LBM kernel zeroes what it read.
+//   wall mask    mask2d[y][x] uint32: bit 31 = fluid column, bit q = the pull
+//                source of direction q is a wall (half-way bounce-back).  The
+//                reference channel is z-invariant, so one plane serves all z.
+//   cells        X, Xd [3][nv] FP64 (cel->x/y/z and fem->xd), U, Fv [3][nv]
+//                FP32; nref [3][ne] FP64 reference metric (n00, n01, n11).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cuda_fp16.h>
+#include <stdint.h>
+
+#include "rbc_step.h"
+
+namespace rbc {
+
+constexpr int Q = 19;
+constexpr uint32_t MASK_FLUID = 0x80000000u;
+
+// D3Q19 in the reference's slot order (lbm.cu:1038-1047):
+// ___ p__ m__ _p_ _m_ __p __m pp_ mm_ mp_ pm_ _pp _mm _mp _pm p_p m_m p_m m_p
+__host__ __device__ constexpr int ex(int q) {
+    return (q == 1 || q == 7 || q == 10 || q == 15 || q == 17) ? 1
+         : (q == 2 || q == 8 || q == 9 || q == 16 || q == 18) ? -1 : 0;
+}
+__host__ __device__ constexpr int ey(int q) {
+    return (q == 3 || q == 7 || q == 9 || q == 11 || q == 14) ? 1
+         : (q == 4 || q == 8 || q == 10 || q == 12 || q == 13) ? -1 : 0;
+}
+__host__ __device__ constexpr int ez(int q) {
+    return (q == 5 || q == 11 || q == 13 || q == 15 || q == 18) ? 1
+         : (q == 6 || q == 12 || q == 14 || q == 16 || q == 17) ? -1 : 0;
+}
+__host__ __device__ constexpr int opp(int q) { return q == 0 ? 0 : ((q & 1) ? q + 1 : q - 1); }
+__host__ __device__ constexpr float wq(int q) { return q == 0 ? (1.0f / 3.0f) : (q <= 6 ? (1.0f / 18.0f) : (1.0f / 36.0f)); }
+__host__ __device__ constexpr double wqd(int q) { return q == 0 ? (1.0 / 3.0) : (q <= 6 ? (1.0 / 18.0) : (1.0 / 36.0)); }
+
+// Geometry of one handle, passed by value to kernels.
+struct Geom {
+    int nx, ny, nzc, nzr;      // internal dims; nzr = reference nz (nzc + 4)
+    long long plane, nint;     // nx*ny, nx*ny*nzc
+    double dx;
+    double xoff, yoff, zoff;   // lattice coordinate = (pos + off)/dx (ibm.cu:100-102)
+    double LX, LZ, xmin, xmax, zmin, zmax;
+};
+
+// Lattice coordinates of a position in the internal frame (z without BUFF).
+__device__ __forceinline__ double lat_x(const Geom &g, double x) { return (x + g.xoff) / g.dx; }
+__device__ __forceinline__ double lat_y(const Geom &g, double y) { return (y + g.yoff) / g.dx; }
+__device__ __forceinline__ double lat_z(const Geom &g, double z) { return (z + g.zoff) / g.dx - 2.0; }
+
+__device__ __forceinline__ int wrap_z(int iz, int nzc) {
+    iz %= nzc;
+    return iz < 0 ? iz + nzc : iz;
+}
+
+// 4-point cosine delta, phi(r) = (1 + cos(pi r / 2)) / 4 (ibm.cu:103-128), at the
+// four nodes floor(l)-1 .. floor(l)+2 for fraction f = l - floor(l):
+// r = 1+f, f, 1-f, 2-f  ->  (1 - s, 1 + c, 1 + s, 1 - c) / 4 with s = sin(pi f/2),
+// c = cos(pi f/2).  For f = 0 this is the reference's 3-node stencil plus a zero.
+__device__ __forceinline__ void delta4(float f, float w[4]) {
+    float s, c;
+    sincospif(0.5f * f, &s, &c);
+    w[0] = 0.25f * (1.0f - s);
+    w[1] = 0.25f * (1.0f + c);
+    w[2] = 0.25f * (1.0f + s);
+    w[3] = 0.25f * (1.0f - c);
+}
+
+// ---- launchers (defined in the .cu files, called by rbc_abi.cu) ----------
+
+struct LbmArgs {
+    const void *gin; void *gout;
+    float *rho, *ux, *uy, *uz;
+    float *Fx, *Fy, *Fz;
+    const uint32_t *mask2d;
+    const float *drive;        // device scalar: P * drive factor of this step
+    float omega, Cr, Bc;
+    float scale, inv_scale;    // FP16 storage scale
+};
+void launch_lbm(const Geom &g, int storage, const LbmArgs &a, cudaStream_t s);
+void launch_import_lattice(const Geom &g, int storage, const double *fn_ref, void *gout,
+                           const uint32_t *mask2d, float scale, cudaStream_t s);
+void launch_export_lattice(const Geom &g, int storage, const void *gin, const uint32_t *mask2d,
+                           const float *rho, const float *ux, const float *uy, const float *uz,
+                           float inv_scale, double *fn_ref, double *dn, double *un, double *vn,
+                           double *wn, cudaStream_t s);
+void launch_export_force(const Geom &g, const float *Fx, const float *Fy, const float *Fz,
+                         const uint32_t *mask2d, double *out3, cudaStream_t s);
+void launch_fill_f32(float *p, long long n, float v, cudaStream_t s);
+
+struct SpreadArgs {
+    const double *X; long long nv; int V, ncell;
+    const float *Fv;
+    float *Fx, *Fy, *Fz;
+    const uint32_t *mask2d;
+    int *flags;
+};
+int  spread_smem_bytes();
+void launch_spread(const Geom &g, const SpreadArgs &a, cudaStream_t s);
+
+struct AdvectArgs {
+    double *X, *Xd; float *U;
+    const float *ux, *uy, *uz;
+    long long nv;
+    double dtM;                // dt * M
+    int *flags;
+};
+void launch_advect(const Geom &g, const AdvectArgs &a, cudaStream_t s);
+
+struct MembraneArgs {
+    const double *Xd; long long nv, ne;
+    const double *nref;
+    const int *tri, *v2e_off, *v2e;
+    const int16_t *nbr;       // [6][V] local neighbour ids, -1 = none
+    float *Fv;
+    int V, E, ncell;
+    double C, rgs; int law;
+    double LX, LZ;
+    int niter;
+    int *flags;
+};
+int  membrane_smem_bytes(int V);
+void launch_membrane(const MembraneArgs &a, bool fp64, cudaStream_t s);
+
+struct VolumeArgs {
+    double *X; long long nv;
+    const int *tri, *v2e_off, *v2e;
+    const double *vol0;
+    double *gx;               // [3][ncell]
+    double *vol_out, *area_out;
+    double *cen_out;          // [3][ncell] centroid when correct == 0
+    int V, E, ncell;
+    int *flags, *vc_max, *vc_last;
+    int correct;              // 0: metrics only (volume, area, centroid), positions untouched
+};
+int  volume_smem_bytes(int V);
+void launch_volume(const Geom &g, const VolumeArgs &a, cudaStream_t s);
+
+// one-time kernel attribute setup (dynamic shared memory limits); called by
+// rbc_create before any launch or graph capture
+int  setup_kernel_attributes();
+
+void launch_step_begin(int *d_iter, float *d_drive, double P, int flowstart, double freq, double dt,
+                       cudaStream_t s);
+
+// packed vertex -> element incidence: element id (bits 0..23), local position
+// of the vertex in the element (bits 24..25), neighbour slots of the two other
+// vertices (bits 26..28 and 29..31)
+__host__ __device__ __forceinline__ int v2e_elem(int p) { return p & 0xFFFFFF; }
+__host__ __device__ __forceinline__ int v2e_en(int p) { return (p >> 24) & 3; }
+__host__ __device__ __forceinline__ int v2e_sa(int p) { return (p >> 26) & 7; }
+__host__ __device__ __forceinline__ int v2e_sb(int p) { return (p >> 29) & 7; }
+
+}  // namespace rbc

@@ -1,0 +1,178 @@
+// volume.cu -- FP64 per-cell volume correction, one CTA per cell.
+//
+// Replaces volume_correction() (volume_correction.cu:453-524 of the reference)
+// with CapsulePeriodicBefore/After (28-94), CalcEleNormal (138-200), CalcVolume
+// (246-281), CalcLambda1 (378-399), VolumeCorrection_GPU (97-135) and
+// CalcCenter (310-352).  The reference iterates on the host: per iteration one
+// normal kernel, two thrust::reduce calls per cell and a host->device copy of
+// lambda, until every cell has |V - V0| / V0 * 100 < 1e-3 or 1000 iterations.
+// A converged cell gets lambda = 0 and never moves again, so each cell's
+// sequence of moves does not depend on the other cells: one CTA per cell runs
+// that cell's loop on the device with block reductions.  The reference's
+// return value (iterations - 1 of the slowest cell) is kept as an atomic max.
+// Also the step-begin kernel (iteration counter and drive factor, main.cu:75,
+// lbm.cu:1030-1035).
+#include "rbc_internal.cuh"
+
+namespace rbc {
+
+constexpr int VOL_THREADS = 1024;
+constexpr double COEFF_VOL_CHANGE = 0.1;   // volume_correction.cu:14
+constexpr double VC_EPS = 1.0e-3;          // volume_correction.cu:15, percent
+constexpr int VC_ITRMAX = 1000;            // volume_correction.cu:487
+
+int volume_smem_bytes(int V) { return 24 * V; }
+
+__device__ __forceinline__ double block_sum_d(double v, double *red) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    __syncthreads();
+    if (lane == 0) red[wid] = v;
+    __syncthreads();
+    double s = 0.0;
+    for (int k = 0; k < nw; k++) s += red[k];
+    return s;
+}
+
+// unit normal, area and volume contribution of local element e (CalcEleNormal_GPU)
+__device__ __forceinline__ void ele_normal(const double *__restrict__ p, int V, const int *__restrict__ tri, int e,
+                                           double n[3], double &dS, double &vt)
+{
+    const int na = __ldg(&tri[3 * e]), nb = __ldg(&tri[3 * e + 1]), nc = __ldg(&tri[3 * e + 2]);
+    const double ax = p[na], ay = p[V + na], az = p[2 * V + na];
+    const double bx = p[nb], by = p[V + nb], bz = p[2 * V + nb];
+    const double cx = p[nc], cy = p[V + nc], cz = p[2 * V + nc];
+    const double v1x = bx - ax, v1y = by - ay, v1z = bz - az;
+    const double v2x = cx - ax, v2y = cy - ay, v2z = cz - az;
+    const double c0 = v1y * v2z - v1z * v2y, c1 = v1z * v2x - v1x * v2z, c2 = v1x * v2y - v1y * v2x;
+    const double nc_ = sqrt(c0 * c0 + c1 * c1 + c2 * c2);
+    n[0] = c0 / nc_; n[1] = c1 / nc_; n[2] = c2 / nc_;
+    dS = nc_ / 2.0;
+    const double rx = (ax + bx + cx) / 3.0, ry = (ay + by + cy) / 3.0, rz = (az + bz + cz) / 3.0;
+    vt = 1.0 / 3.0 * (rx * n[0] + ry * n[1] + rz * n[2]) * dS;
+}
+
+__global__ void __launch_bounds__(VOL_THREADS)
+volume_kernel(const Geom g, const VolumeArgs a)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ double red[32];
+    double *p = reinterpret_cast<double *>(smem);   // [3][V]
+    const int V = a.V, E = a.E, tid = threadIdx.x, T = blockDim.x, cell = blockIdx.x, N = a.ncell;
+    const long long vb = (long long)cell * V, nv = a.nv;
+    const double gz = a.gx[2 * N + cell];
+    for (int v = tid; v < V; v += T) {
+        p[v] = a.X[vb + v];
+        p[V + v] = a.X[nv + vb + v];
+        double z = a.X[2 * nv + vb + v];
+        const double dz = z - gz;                           // CapsulePeriodicBefore (z only)
+        if (dz > g.LZ * 0.5) z -= g.LZ; else if (dz < -g.LZ * 0.5) z += g.LZ;
+        p[2 * V + v] = z;
+    }
+    __syncthreads();
+
+    const double V0 = a.correct ? a.vol0[cell] : 0.0;
+    double vol = 0.0, area = 0.0;
+    int it = 0;
+    for (;;) {
+        double sv = 0.0, sa = 0.0;
+        for (int e = tid; e < E; e += T) {
+            double n[3], dS, vt;
+            ele_normal(p, V, a.tri, e, n, dS, vt);
+            sv += vt; sa += dS;
+        }
+        vol = block_sum_d(sv, red);
+        area = block_sum_d(sa, red);
+        if (!a.correct) break;
+        it++;
+        if (fabs(vol - V0) / V0 * 100.0 < VC_EPS) break;
+        const double lambda = 18.0 * (vol - V0) / area;
+        double disp[4][3];
+        for (int m = 0; m < 4; m++) {
+            const int v = tid + m * T;
+            disp[m][0] = disp[m][1] = disp[m][2] = 0.0;
+            if (v >= V) continue;
+            const int k0 = __ldg(&a.v2e_off[v]), k1 = __ldg(&a.v2e_off[v + 1]);
+            const int nne = k1 - k0;
+            double nn0 = 0.0, nn1 = 0.0, nn2 = 0.0;
+            for (int k = k0; k < k1; k++) {
+                double n[3], dS, vt;
+                ele_normal(p, V, a.tri, v2e_elem(__ldg(&a.v2e[k])), n, dS, vt);
+                nn0 += n[0] / nne; nn1 += n[1] / nne; nn2 += n[2] / nne;
+            }
+            disp[m][0] = -lambda / 6.0 * nn0 * COEFF_VOL_CHANGE;
+            disp[m][1] = -lambda / 6.0 * nn1 * COEFF_VOL_CHANGE;
+            disp[m][2] = -lambda / 6.0 * nn2 * COEFF_VOL_CHANGE;
+        }
+        __syncthreads();
+        for (int m = 0; m < 4; m++) {
+            const int v = tid + m * T;
+            if (v >= V) continue;
+            p[v] += disp[m][0]; p[V + v] += disp[m][1]; p[2 * V + v] += disp[m][2];
+        }
+        __syncthreads();
+        if (it >= VC_ITRMAX) { if (tid == 0) atomicOr(a.flags, RBC_FLAG_VC_NOT_CONVERGED); break; }
+    }
+    // CalcCenter: vertex mean, wrapped into [zmin, zmax]
+    double sx = 0.0, sy = 0.0, sz = 0.0;
+    for (int v = tid; v < V; v += T) { sx += p[v]; sy += p[V + v]; sz += p[2 * V + v]; }
+    sx = block_sum_d(sx, red) / (double)V;
+    sy = block_sum_d(sy, red) / (double)V;
+    sz = block_sum_d(sz, red) / (double)V;
+    if (sz < g.zmin) sz += g.LZ; else if (sz > g.zmax) sz -= g.LZ;
+    if (tid == 0) {
+        if (a.vol_out) a.vol_out[cell] = vol;
+        if (a.area_out) a.area_out[cell] = area;
+        double *cen = a.correct ? a.gx : a.cen_out;
+        if (cen) { cen[cell] = sx; cen[N + cell] = sy; cen[2 * N + cell] = sz; }
+        if (a.correct) { atomicMax(a.vc_max, it - 1); atomicMax(a.vc_last, it - 1); }
+    }
+    if (!a.correct) return;
+    // CapsulePeriodicAfter, then store
+    for (int v = tid; v < V; v += T) {
+        double z = p[2 * V + v];
+        if (z < g.zmin) z += g.LZ; else if (z > g.zmax) z -= g.LZ;
+        a.X[vb + v] = p[v];
+        a.X[nv + vb + v] = p[V + v];
+        a.X[2 * nv + vb + v] = z;
+    }
+}
+
+void launch_volume(const Geom &g, const VolumeArgs &a, cudaStream_t s)
+{
+    if (a.ncell <= 0) return;
+    const int smem = volume_smem_bytes(a.V);
+    volume_kernel<<<a.ncell, VOL_THREADS, smem, s>>>(g, a);
+}
+
+cudaError_t membrane_setup(int bytes);
+cudaError_t spread_setup();
+
+// Largest dynamic shared memory any launch may ask for (B200: 227 KB per CTA).
+constexpr int MAX_DYN_SMEM = 227 * 1024;
+
+int setup_kernel_attributes()
+{
+    cudaError_t e = cudaFuncSetAttribute(volume_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, MAX_DYN_SMEM);
+    if (e != cudaSuccess) return (int)e;
+    if ((e = membrane_setup(MAX_DYN_SMEM)) != cudaSuccess) return (int)e;
+    if ((e = spread_setup()) != cudaSuccess) return (int)e;
+    return 0;
+}
+
+__global__ void step_begin_kernel(int *iter, float *drive, double P, int flowstart, double freq, double dt)
+{
+    const int it = *iter + 1;
+    *iter = it;
+    const double wi = (it > flowstart) ? 1.0 + 0.5 * sin(M_PI * dt * (double)it / freq) : 0.0;
+    *drive = (float)(P * wi);
+}
+
+void launch_step_begin(int *d_iter, float *d_drive, double P, int flowstart, double freq, double dt,
+                       cudaStream_t s)
+{
+    step_begin_kernel<<<1, 1, 0, s>>>(d_iter, d_drive, P, flowstart, freq, dt);
+}
+
+}  // namespace rbc

@@ -1,0 +1,184 @@
+"""Python mirror of the reference's step modules over the C ABI.
+
+``Simulation`` owns one device handle.  Its methods carry the names of the
+reference entry points they replace and run in the same order inside
+``step()`` (main.cu:73-110 with M = 1):
+
+    stress()            stress.cu:580       membrane FEM nodal forces
+    ibm_st1()           ibm.cu:299          spread forces to the lattice
+    lbm_d3q19()         lbm.cu:1463         collide + stream
+    ibm_st2()           ibm.cu:642          interpolate + RK4 advect
+    volume_correction() volume_correction.cu:453
+
+State moves in and out in the reference's layouts (``import_*``/``export_*``).
+All compute runs in the CUDA library; nothing here computes physics.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _native as N
+from .configs import Case
+
+
+def _dp(a):
+    return None if a is None else a.ctypes.data_as(N._DP)
+
+
+def _f64(a, n=None):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    if n is not None and a.size != n:
+        raise ValueError(f"expected {n} values, got {a.size}")
+    return a
+
+
+class Simulation:
+    def __init__(self, case: Case, **overrides):
+        L = N.lib()
+        self.case = case
+        params = dict(case.params)
+        params.update(overrides)
+        self.params = params
+        self._p = N.params_struct(params)
+        self._bc = np.ascontiguousarray(case.bc, dtype=np.int32)
+        self._tri = np.ascontiguousarray(case.tri, dtype=np.int32).reshape(-1)
+        self._xr = np.ascontiguousarray(case.xr, dtype=np.float64)
+        m = None
+        if case.ncell > 0:
+            m = N.RbcMesh(case.ncell, case.vertex, case.element, self._tri.ctypes.data_as(N._IP),
+                          self._xr.ctypes.data_as(N._DP))
+        h = N._H()
+        N.check(L.rbc_create(C.byref(self._p), C.byref(m) if m is not None else None,
+                             self._bc.ctypes.data_as(N._IP), C.byref(h)))
+        self._h = h
+        self.n = case.n
+        self.nv = case.ncell * case.vertex
+        self.ne = case.ncell * case.element
+
+    # -- lifetime ---------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None):
+            N.lib().rbc_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _call(self, name, *args):
+        N.check(getattr(N.lib(), name)(self._h, *args), self._h)
+
+    # -- the step (reference entry-point names) -----------------------------
+    def stress(self):
+        self._call("rbc_stress")
+
+    def ibm_st1(self):
+        self._call("rbc_ibm_st1")
+
+    def lbm_d3q19(self):
+        self._call("rbc_lbm_d3q19")
+
+    def ibm_st2(self):
+        self._call("rbc_ibm_st2")
+
+    def volume_correction(self) -> int:
+        it = C.c_int(0)
+        self._call("rbc_volume_correction", C.byref(it))
+        return it.value
+
+    def step(self, nsteps: int = 1):
+        self._call("rbc_step", int(nsteps))
+
+    @property
+    def iter(self) -> int:
+        v = C.c_int(0)
+        self._call("rbc_get_iter", C.byref(v))
+        return v.value
+
+    @iter.setter
+    def iter(self, value: int):
+        self._call("rbc_set_iter", int(value))
+
+    # -- state in / out ------------------------------------------------------
+    def import_lattice(self, fn):
+        self._call("rbc_import_ref_lattice", _dp(_f64(fn, self.n * 19)))
+
+    def export_lattice(self, fn=True, macro=True) -> dict:
+        out = {}
+        if fn:
+            out["fn"] = np.empty(self.n * 19)
+        if macro:
+            for k in ("dn", "un", "vn", "wn"):
+                out[k] = np.empty(self.n)
+        self._call("rbc_export_ref_lattice", _dp(out.get("fn")), _dp(out.get("dn")), _dp(out.get("un")),
+                   _dp(out.get("vn")), _dp(out.get("wn")))
+        return out
+
+    def export_force(self) -> dict:
+        out = {k: np.empty(self.n) for k in ("fx", "fy", "fz")}
+        self._call("rbc_export_ref_force", _dp(out["fx"]), _dp(out["fy"]), _dp(out["fz"]))
+        return out
+
+    def import_cells(self, x=None, y=None, z=None, xd=None, nd=None, volume0=None, gx=None):
+        nv, ne, nc = self.nv, self.ne, self.case.ncell
+        args = [None if a is None else _f64(a, n)
+                for a, n in ((x, nv), (y, nv), (z, nv), (xd, 3 * nv), (nd, 4 * ne), (volume0, nc), (gx, 3 * nc))]
+        self._keep = args
+        self._call("rbc_import_ref_cells", *map(_dp, args))
+
+    def import_vertex_force(self, fx, fy, fz):
+        nv = self.nv
+        args = [_f64(fx, nv), _f64(fy, nv), _f64(fz, nv)]
+        self._call("rbc_import_ref_vertex_force", *map(_dp, args))
+
+    def export_cells(self) -> dict:
+        nv, nc = self.nv, self.case.ncell
+        keys = ("x", "y", "z", "xd", "u", "v", "w", "fx", "fy", "fz", "gx")
+        sizes = (nv, nv, nv, 3 * nv, nv, nv, nv, nv, nv, nv, 3 * nc)
+        out = {k: np.empty(s) for k, s in zip(keys, sizes)}
+        self._call("rbc_export_ref_cells", *[_dp(out[k]) for k in keys])
+        return out
+
+    # -- diagnostics ----------------------------------------------------------
+    def status(self) -> tuple[int, int]:
+        f, v = C.c_int(0), C.c_int(0)
+        self._call("rbc_get_status", C.byref(f), C.byref(v))
+        return f.value, v.value
+
+    def cell_metrics(self) -> dict:
+        nc = self.case.ncell
+        out = {"volume": np.empty(nc), "area": np.empty(nc), "centroid": np.empty(3 * nc)}
+        self._call("rbc_cell_metrics", _dp(out["volume"]), _dp(out["area"]), _dp(out["centroid"]))
+        return out
+
+    def profile_steps(self, nsteps: int) -> dict:
+        """Run nsteps with a CUDA event around each kernel; returns the summed
+        device milliseconds per kernel."""
+        ms = np.zeros(N.RBC_NUM_KERNELS)
+        self._call("rbc_profile_steps", int(nsteps), _dp(ms))
+        return dict(zip(N.RBC_KERNEL_NAMES, ms.tolist()))
+
+    @property
+    def stream(self) -> int:
+        v = C.c_void_p()
+        self._call("rbc_get_stream", C.byref(v))
+        return v.value or 0
+
+    def synchronize(self):
+        self._call("rbc_synchronize")
+
+    @property
+    def launches(self) -> int:
+        v = C.c_longlong(0)
+        self._call("rbc_launch_count", C.byref(v))
+        return v.value

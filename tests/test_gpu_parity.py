@@ -1,0 +1,260 @@
+"""Parity of the sm_100a step against the FP64 oracle, through the C ABI.
+
+Each test starts both from the same reference-layout state (a developed flow
+with deformed cells, produced by the oracle), runs the same stage or steps and
+compares the results.  Tolerances (FP32 lattice and IB arithmetic, FP64
+positions and volume correction):
+  velocity field        relative L2 <= 1e-5 per step
+  density               max |d rho| <= 1e-6 per step
+  populations           max |d f|   <= 1e-8 per step (COMP nodes)
+  vertex positions      max |d x|   <= 1e-5 * max|x| per step (and displacement
+                        relative L2 <= 1e-4)
+  membrane forces       relative L2 <= 5e-3 (FP32 mechanics), 1e-6 (FP64 mechanics)
+"""
+import numpy as np
+import pytest
+
+from preprocess_src_b200 import configs
+
+pytestmark = pytest.mark.gpu
+
+
+def rel_l2(a, b):
+    return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / max(np.linalg.norm(b), 1e-300))
+
+
+def parity_case(**kw):
+    """40 x 24 x 24 duct, two subdivision-3 cells of radius 6, one straddling the
+    periodic boundary; a stronger drive than the named workloads so a few steps
+    give a developed flow and deformed cells."""
+    kw.setdefault("g", 4e-5)
+    kw.setdefault("Gs", 2e-3)
+    return configs.duct_case("parity_40x24x24_2c", 40, 24, 24,
+                             centers_duct=[(0.6, 12.2, 11.7), (21.0, 11.6, 12.4)],
+                             subdiv=3, radius=6.0, seed=11, **kw)
+
+
+@pytest.fixture(scope="module")
+def developed(oracle_mod, native_lib):
+    case = parity_case()
+    o = oracle_mod.Oracle(case)
+    o.step(40)
+    return case, o
+
+
+def load(o, **overrides):
+    from preprocess_src_b200.step import Simulation
+    sim = Simulation(o.case, **overrides)
+    sim.import_lattice(o.fn)
+    sim.import_cells(x=o["x"], y=o["y"], z=o["z"], xd=o["xd"], nd=o["nd"], volume0=o["volume0"], gx=o["gx"])
+    sim.iter = o.iter
+    return sim
+
+
+def clone(oracle_mod, o):
+    c = oracle_mod.Oracle(o.case, init_fluid=False)
+    for k in ("dn", "un", "vn", "wn", "dm", "um", "vm", "wm", "fx", "fy", "fz", "x", "y", "z", "u", "v", "w",
+              "cfx", "cfy", "cfz", "xd", "nd", "volume0", "gx"):
+        c.a[k][:] = o.a[k]
+    c.fn[:] = o.fn
+    c.iter = o.iter
+    return c
+
+
+def comp(case):
+    return case.bc == configs.COMP
+
+
+def test_import_export_roundtrip(developed):
+    case, o = developed
+    sim = load(o)
+    out = sim.export_lattice(fn=True, macro=False)
+    m = np.repeat(comp(case), 19)
+    err = np.abs(out["fn"][m] - o.fn[m]).max()
+    assert err <= 1e-9, err
+
+
+def test_stress_matches_oracle(developed, oracle_mod):
+    case, o = developed
+    for fp64, tol in ((0, 5e-3), (1, 1e-6)):
+        sim = load(o, membrane_fp64=fp64)
+        c = clone(oracle_mod, o)
+        assert c.stress() == 0
+        sim.stress()
+        got = sim.export_cells()
+        ref = np.concatenate([c["cfx"], c["cfy"], c["cfz"]])
+        mine = np.concatenate([got["fx"], got["fy"], got["fz"]])
+        err = rel_l2(mine, ref)
+        print(f"membrane_fp64={fp64}: force rel L2 {err:.3e}, max|f| {np.abs(ref).max():.3e}")
+        assert err <= tol, (fp64, err)
+        flags, _ = sim.status()
+        assert flags & 8 == 0, "load solve residual flag"
+
+
+def test_spread_matches_oracle(developed, oracle_mod):
+    case, o = developed
+    c = clone(oracle_mod, o)
+    c.stress()
+    sim = load(o)
+    sim.import_vertex_force(c["cfx"], c["cfy"], c["cfz"])
+    c.ibm_st1()
+    sim.ibm_st1()
+    f = sim.export_force()
+    m = comp(case)
+    ref = np.concatenate([c["fx"][m], c["fy"][m], c["fz"][m]])
+    mine = np.concatenate([f["fx"][m], f["fy"][m], f["fz"][m]])
+    err = rel_l2(mine, ref)
+    print(f"spread rel L2 {err:.3e}, sum ref {ref.sum():.6e} sum gpu {mine.sum():.6e}")
+    assert err <= 1e-6, err
+    flags, _ = sim.status()
+    assert flags & 4 == 0, "spread took the direct-atomic path"
+
+
+def test_lbm_matches_oracle(developed, oracle_mod):
+    case, o = developed
+    c = clone(oracle_mod, o)
+    c.iter += 1
+    c.stress()
+    sim = load(o)
+    sim.iter = c.iter
+    sim.import_vertex_force(c["cfx"], c["cfy"], c["cfz"])
+    c.ibm_st1()
+    sim.ibm_st1()
+    c.lbm_d3q19()
+    sim.lbm_d3q19()
+    out = sim.export_lattice()
+    m = comp(case)
+    mq = np.repeat(m, 19)
+    ferr = np.abs(out["fn"][mq] - c.fn[mq]).max()
+    derr = np.abs(out["dn"][m] - c["dn"][m]).max()
+    uref = np.concatenate([c["un"][m], c["vn"][m], c["wn"][m]])
+    umine = np.concatenate([out["un"][m], out["vn"][m], out["wn"][m]])
+    uerr = rel_l2(umine, uref)
+    print(f"lbm: max|df| {ferr:.3e}  max|drho| {derr:.3e}  u rel L2 {uerr:.3e}  max|u| {np.abs(uref).max():.3e}")
+    assert ferr <= 1e-8 and derr <= 1e-6 and uerr <= 1e-5
+
+
+def test_pure_fluid_lbm_matches_oracle(oracle_mod, native_lib):
+    case = configs.duct_case("fluid_32x20x16", 32, 20, 16, g=1e-4)
+    o = oracle_mod.Oracle(case)
+    o.step(30)
+    sim = load(o)
+    o.step(1)
+    sim.step(1)
+    out = sim.export_lattice()
+    m = comp(case)
+    uref = np.concatenate([o["un"][m], o["vn"][m], o["wn"][m]])
+    umine = np.concatenate([out["un"][m], out["vn"][m], out["wn"][m]])
+    assert rel_l2(umine, uref) <= 1e-5
+    mq = np.repeat(m, 19)
+    assert np.abs(out["fn"][mq] - o.fn[mq]).max() <= 1e-8
+
+
+def test_advect_matches_oracle(developed, oracle_mod):
+    case, o = developed
+    c = clone(oracle_mod, o)
+    sim = load(o)
+    # the oracle's averaged velocity is the last lbm step's; give the GPU the same field
+    c.iter += 1
+    c.stress(); c.ibm_st1(); c.lbm_d3q19()
+    sim.iter = c.iter
+    sim.stress(); sim.ibm_st1(); sim.lbm_d3q19()
+    x0 = np.concatenate([c["x"], c["y"], c["z"]]).copy()
+    c.ibm_st2()
+    sim.ibm_st2()
+    got = sim.export_cells()
+    ref = np.concatenate([c["x"], c["y"], c["z"]])
+    mine = np.concatenate([got["x"], got["y"], got["z"]])
+    perr = np.abs(mine - ref).max()
+    derr = rel_l2(mine - x0, ref - x0)
+    verr = rel_l2(np.concatenate([got["u"], got["v"], got["w"]]), np.concatenate([c["u"], c["v"], c["w"]]))
+    print(f"advect: max|dx| {perr:.3e}  displacement rel L2 {derr:.3e}  vertex u rel L2 {verr:.3e}")
+    assert perr <= 1e-5 * np.abs(ref).max() and derr <= 1e-4 and verr <= 1e-4
+    assert np.abs(got["xd"] - c["xd"]).max() <= 1e-5 * np.abs(ref).max()
+
+
+def test_volume_correction_matches_oracle(developed, oracle_mod):
+    case, o = developed
+    c = clone(oracle_mod, o)
+    rng = np.random.default_rng(5)
+    for k in ("x", "y", "z"):   # shrink each cell a little about its centroid so the loop must iterate
+        c.a[k][:] = c.a[k] * 0.999 + 1e-4 * rng.standard_normal(c.a[k].size)
+    sim = load(c)
+    it_ref = c.volume_correction()
+    it_gpu = sim.volume_correction()
+    got = sim.export_cells()
+    assert it_ref == it_gpu and it_ref > 0, (it_ref, it_gpu)
+    err = max(np.abs(got[k] - c[k]).max() for k in ("x", "y", "z"))
+    assert err <= 1e-9, err
+    assert np.abs(got["gx"] - c["gx"]).max() <= 1e-9
+    vol = sim.cell_metrics()["volume"]
+    assert np.all(np.abs(vol - c["volume0"]) / c["volume0"] < 1e-5)
+
+
+def test_full_steps_match_oracle(developed, oracle_mod):
+    case, o = developed
+    c = clone(oracle_mod, o)
+    sim = load(o)
+    m = comp(case)
+    for nsteps in (1, 2, 5):
+        c.step(nsteps)
+        sim.step(nsteps)
+        out = sim.export_lattice(fn=False)
+        got = sim.export_cells()
+        uref = np.concatenate([c["un"][m], c["vn"][m], c["wn"][m]])
+        umine = np.concatenate([out["un"][m], out["vn"][m], out["wn"][m]])
+        uerr = rel_l2(umine, uref)
+        ref = np.concatenate([c["x"], c["y"], c["z"]])
+        perr = np.abs(np.concatenate([got["x"], got["y"], got["z"]]) - ref).max()
+        print(f"after +{nsteps} steps: u rel L2 {uerr:.3e}  max|dx| {perr:.3e}")
+        assert uerr <= 1e-5 * nsteps and perr <= 1e-5 * np.abs(ref).max()
+    assert sim.iter == c.iter
+
+
+def test_long_run_drift_and_conservation(developed, oracle_mod):
+    case, o = developed
+    c = clone(oracle_mod, o)
+    sim = load(o)
+    m = comp(case)
+    mass0 = sim.export_lattice(fn=False)["dn"][m].sum()
+    c.step(100)
+    sim.step(100)
+    out = sim.export_lattice(fn=False)
+    got = sim.export_cells()
+    uref = np.concatenate([c["un"][m], c["vn"][m], c["wn"][m]])
+    umine = np.concatenate([out["un"][m], out["vn"][m], out["wn"][m]])
+    uerr = rel_l2(umine, uref)
+    perr = np.abs(np.concatenate([got["x"], got["y"], got["z"]]) - np.concatenate([c["x"], c["y"], c["z"]])).max()
+    mass1 = out["dn"][m].sum()
+    vol = sim.cell_metrics()["volume"]
+    print(f"100 steps: u rel L2 {uerr:.3e}  max|dx| {perr:.3e}  mass drift {(mass1 - mass0) / mass0:.3e}  "
+          f"volume drift {np.abs(vol / c['volume0'] - 1).max():.3e}")
+    assert uerr <= 1e-4 and perr <= 1e-4
+    assert abs(mass1 - mass0) / mass0 <= 1e-6
+    assert np.all(np.abs(vol / c["volume0"] - 1) < 1e-5)
+    flags, vcmax = sim.status()
+    assert flags & (1 | 2 | 8) == 0, flags
+
+
+def test_stage_calls_equal_graph_step(developed):
+    case, o = developed
+    a = load(o)
+    b = load(o)
+    a.step(1)
+    b.iter = b.iter + 1
+    b.stress(); b.ibm_st1(); b.lbm_d3q19(); b.ibm_st2(); b.volume_correction()
+    ea, eb = a.export_lattice(fn=False), b.export_lattice(fn=False)
+    m = comp(case)
+    assert np.abs(ea["wn"][m] - eb["wn"][m]).max() <= 1e-9
+    ca, cb = a.export_cells(), b.export_cells()
+    assert np.abs(ca["z"] - cb["z"]).max() <= 1e-10
+
+
+def test_launch_count_and_status(developed):
+    case, o = developed
+    sim = load(o)
+    n0 = sim.launches
+    sim.step(4)
+    assert sim.launches - n0 == 4 * 6
+    flags, _ = sim.status()
+    assert flags == 0, flags
