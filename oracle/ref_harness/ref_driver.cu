@@ -1,0 +1,275 @@
+// ref_driver.cu -- C entry points that run the reference's own step modules.
+//
+// TEST INFRASTRUCTURE ONLY.  Linked with the reference's lbm.cu, ibm.cu,
+// stress.cu, matrix_solver.cu, volume_correction.cu and init2.cu (compiled
+// unmodified from the reference tree) into oracle/_ref/librefstep_<case>.so.
+// It fills the reference's state structs the way cdo_init / flu_init /
+// cel_init / mem_init would (init1.cu:190-235, 413-434, 626-853, 875-1092) from
+// inputs given by the caller instead of mesh files and a clock-seeded
+// rotation, then calls the reference's fem_init (init2.cu:258) and
+// volume_init (volume_correction.cu:427) and steps with the reference's own
+// stress / ibm_st1 / lbm_d3q19 / ibm_st2 / volume_correction in the order of
+// main.cu:73-110 (M = 1; adhesion, THINC/WLIC and front tracking are inactive
+// for CYTOADHESION = false and LAMBDA1 = 1).
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <map>
+#include <utility>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "def.h"
+
+static process g_prc;
+static domain g_cdo;
+static lattice g_ltc;
+static cell g_cel;
+static fem g_fem;
+static int g_err = 0;
+
+void error(int code)
+{
+    if (!g_err) g_err = code;
+    fprintf(stderr, "reference error(%d)\n", code);
+}
+
+int expand2pow2(int n)
+{
+    int p = 1;
+    while (p < n) p *= 2;
+    return p;
+}
+
+template <typename T>
+static T *dnew(size_t count)
+{
+    T *p = nullptr;
+    if (cudaMalloc((void **)&p, sizeof(T) * (count ? count : 1)) != cudaSuccess) { error(100); return nullptr; }
+    cudaMemset(p, 0, sizeof(T) * (count ? count : 1));
+    return p;
+}
+
+template <typename T>
+static void up(T *d, const T *h, size_t count) { cudaMemcpy(d, h, sizeof(T) * count, cudaMemcpyHostToDevice); }
+template <typename T>
+static void down(T *h, const T *d, size_t count) { cudaMemcpy(h, d, sizeof(T) * count, cudaMemcpyDeviceToHost); }
+
+extern "C" {
+
+int ref_error(void) { return g_err; }
+
+// tri_local [E*3] shared connectivity, xr [3*ncell*V] AoS initial positions
+int ref_setup(int nx, int ny, int nz, const int *bc, int ncell, int V, int E, const int *tri_local, const double *xr)
+{
+    g_err = 0;
+    memset(&g_prc, 0, sizeof(g_prc));
+    memset(&g_cdo, 0, sizeof(g_cdo));
+    memset(&g_ltc, 0, sizeof(g_ltc));
+    memset(&g_cel, 0, sizeof(g_cel));
+    memset(&g_fem, 0, sizeof(g_fem));
+    // cdo_init, CapsuleCHANNELFLOW (init1.cu:190-212)
+    g_cdo.dx = Lc / KL;
+    g_cdo.dt = Cr * g_cdo.dx / Uc;
+    g_cdo.tau = (6.0 * Df + 1.0) / 2.0;
+    g_cdo.sr = SR;
+    g_cdo.lambda = LAMBDA1;
+    g_cdo.nx = nx; g_cdo.ny = ny; g_cdo.nz = nz; g_cdo.n = nx * ny * nz;
+    g_cdo.xmin = -LX / 2.0; g_cdo.xmax = LX / 2.0;
+    g_cdo.ymin = -LY / 2.0; g_cdo.ymax = LY / 2.0;
+    g_cdo.zmin = -LZ / 2.0; g_cdo.zmax = LZ / 2.0;
+    const int n = g_cdo.n;
+    // flu_init + mem_init for the lattice (init1.cu:399-434, 894-931)
+    std::vector<double> f(n * (size_t)Q), one(n, 1.0);
+    const double w[Q] = {1.0 / 3, 1.0 / 18, 1.0 / 18, 1.0 / 18, 1.0 / 18, 1.0 / 18, 1.0 / 18,
+                         1.0 / 36, 1.0 / 36, 1.0 / 36, 1.0 / 36, 1.0 / 36, 1.0 / 36,
+                         1.0 / 36, 1.0 / 36, 1.0 / 36, 1.0 / 36, 1.0 / 36, 1.0 / 36};
+    for (int i = 0; i < n; i++) for (int q = 0; q < Q; q++) f[(size_t)i * Q + q] = w[q];
+    g_ltc.fnD = dnew<double>((size_t)n * Q); g_ltc.fmD = dnew<double>((size_t)n * Q);
+    g_ltc.dnD = dnew<double>(n); g_ltc.unD = dnew<double>(n); g_ltc.vnD = dnew<double>(n); g_ltc.wnD = dnew<double>(n);
+    g_ltc.dmD = dnew<double>(n); g_ltc.umD = dnew<double>(n); g_ltc.vmD = dnew<double>(n); g_ltc.wmD = dnew<double>(n);
+    g_ltc.fxD = dnew<double>(n); g_ltc.fyD = dnew<double>(n); g_ltc.fzD = dnew<double>(n);
+    g_ltc.vfD = dnew<double>(n); g_ltc.vfD2 = dnew<double>(n); g_ltc.bcD = dnew<int>(n);
+    up(g_ltc.fnD, f.data(), (size_t)n * Q);
+    up(g_ltc.dnD, one.data(), n); up(g_ltc.dmD, one.data(), n);
+    up(g_ltc.bcD, bc, n);
+    // cells (cel_init 626-853 without the file reads; mem_init 933-1005)
+    cell &c = g_cel;
+    c.n = ncell; c.vertex = V; c.element = E; c.rg = 1.0; c.br = BR; c.gs = GS;
+    const int nv = ncell * V, ne = ncell * E;
+    c.xH = (double *)malloc(sizeof(double) * nv); c.yH = (double *)malloc(sizeof(double) * nv);
+    c.zH = (double *)malloc(sizeof(double) * nv); c.eleH = (int *)malloc(sizeof(int) * ne * TRI);
+    for (int j = 0; j < nv; j++) { c.xH[j] = xr[3 * j]; c.yH[j] = xr[3 * j + 1]; c.zH[j] = xr[3 * j + 2]; }
+    for (int ic = 0; ic < ncell; ic++)
+        for (int e = 0; e < E; e++)
+            for (int k = 0; k < TRI; k++) c.eleH[(ic * E + e) * TRI + k] = tri_local[e * TRI + k] + ic * V;
+    // edge-neighbour elements (cel_init 756-795) for fourpoint_bend, which runs with BR = 0
+    std::vector<int> ec(ne * TRI, 0), ecn(ne, 0);
+    {
+        std::map<std::pair<int, int>, std::vector<int>> edges;   // undirected edge -> elements
+        for (int e = 0; e < ne; e++)
+            for (int s = 0; s < 3; s++) {
+                int a = c.eleH[e * TRI + s], b = c.eleH[e * TRI + (s + 1) % 3];
+                edges[{a < b ? a : b, a < b ? b : a}].push_back(e);
+            }
+        for (const auto &kv : edges)
+            if (kv.second.size() == 2)
+                for (int k = 0; k < 2; k++) {
+                    const int e1 = kv.second[k], e2 = kv.second[1 - k];
+                    if (ecn[e1] < 3) ec[e1 * TRI + ecn[e1]++] = e2;
+                }
+    }
+    std::vector<double> c0(ne * TRI, 1.0), s0(ne * TRI, 0.0), zero(nv, 0.0);   // init1.cu:849-850
+    c.xD = dnew<double>(nv); c.yD = dnew<double>(nv); c.zD = dnew<double>(nv);
+    c.uD = dnew<double>(nv); c.vD = dnew<double>(nv); c.wD = dnew<double>(nv);
+    c.fxD = dnew<double>(nv); c.fyD = dnew<double>(nv); c.fzD = dnew<double>(nv);
+    c.c0D = dnew<double>(ne * TRI); c.s0D = dnew<double>(ne * TRI);
+    c.eleD = dnew<int>(ne * TRI); c.ecD = dnew<int>(ne * TRI);
+    up(c.xD, c.xH, nv); up(c.yD, c.yH, nv); up(c.zD, c.zH, nv);
+    up(c.c0D, c0.data(), ne * TRI); up(c.s0D, s0.data(), ne * TRI);
+    up(c.eleD, c.eleH, ne * TRI); up(c.ecD, ec.data(), ne * TRI);
+    // the reference's fem_init (init2.cu:258-400), then mem_init's fem uploads (1007-1046)
+    fem_init(&g_cel, &g_fem);
+    if (g_err) return g_err;
+    fem &m = g_fem;
+    const int nth = c.n_th, mn = c.mn;
+    m.xd = dnew<double>(nth * 3); m.xrd = dnew<double>(nth * 3);
+    m.qd = dnew<double>((size_t)ncell * mn); m.qid = dnew<double>((size_t)ncell * mn);
+    m.td = dnew<double>(ne * 4); m.tpd = dnew<double>(ne * 2); m.rgd = dnew<double>(ne); m.nd = dnew<double>(ne * 4);
+    m.eled = dnew<int>(ne * 6); m.nlnd = dnew<int>(nth); m.lnd = dnew<int>(nth * 7); m.lod = dnew<int>(nth * 7);
+    m.nled = dnew<int>(nth); m.led = dnew<int>(nth * 6);
+    m.ptrd = dnew<int>(mn); m.indexd = dnew<int>(mn * 7); m.valued = dnew<double>(mn * 7); m.bd = dnew<double>(mn);
+    up(m.xd, m.x, nth * 3); up(m.xrd, m.xr, nth * 3); up(m.nd, m.n, ne * 4);
+    up(m.eled, m.ele, ne * 6); up(m.nlnd, m.nln, nth); up(m.lnd, m.ln, nth * 7); up(m.lod, m.lo, nth * 7);
+    up(m.nled, m.nle, nth); up(m.led, m.le, nth * 6);
+    up(m.ptrd, m.ptr, mn); up(m.indexd, m.index, mn * 7); up(m.valued, m.value, mn * 7);
+    volume_init(&g_cdo, &g_cel);
+    cudaDeviceSynchronize();
+    return g_err ? g_err : (cudaGetLastError() == cudaSuccess ? 0 : 101);
+}
+
+int ref_set_iter(int iter) { g_prc.iter = iter; return 0; }
+int ref_get_iter(void) { return g_prc.iter; }
+
+int ref_set_lattice(const double *fn)
+{
+    up(g_ltc.fnD, fn, (size_t)g_cdo.n * Q);
+    return 0;
+}
+
+int ref_set_cells(const double *x, const double *y, const double *z, const double *xd, const double *nd,
+                  const double *volume0, const double *gx)
+{
+    const int nv = g_cel.n * g_cel.vertex, ne = g_cel.n * g_cel.element;
+    if (x) up(g_cel.xD, x, nv);
+    if (y) up(g_cel.yD, y, nv);
+    if (z) up(g_cel.zD, z, nv);
+    if (xd) up(g_fem.xd, xd, nv * 3);
+    if (nd) up(g_fem.nd, nd, ne * 4);
+    if (volume0) memcpy(g_cel.volume0, volume0, sizeof(double) * g_cel.n);
+    if (gx) memcpy(g_cel.gx, gx, sizeof(double) * 3 * g_cel.n);
+    return 0;
+}
+
+// 0 stress, 1 ibm_st1, 2 lbm_d3q19, 3 ibm_st2, 4 volume_correction (returns its value)
+int ref_stage(int which)
+{
+    int r = 0;
+    switch (which) {
+    case 0: stress(&g_prc, &g_cdo, &g_cel, &g_fem, &g_ltc); break;
+    case 1: ibm_st1(&g_cdo, &g_ltc, &g_cel); break;
+    case 2: lbm_d3q19(&g_prc, &g_cdo, &g_ltc); break;
+    case 3: ibm_st2(&g_cdo, &g_ltc, &g_cel, &g_fem); break;
+    case 4: r = volume_correction(&g_cdo, &g_cel, &g_fem); break;
+    default: return -1;
+    }
+    cudaDeviceSynchronize();
+    return r;
+}
+
+// main.cu:73-110 with M = 1
+int ref_step(int nsteps)
+{
+    for (int k = 0; k < nsteps && !g_err; k++) {
+        g_prc.iter++;
+        stress(&g_prc, &g_cdo, &g_cel, &g_fem, &g_ltc);
+        ibm_st1(&g_cdo, &g_ltc, &g_cel);
+        lbm_d3q19(&g_prc, &g_cdo, &g_ltc);
+        ibm_st2(&g_cdo, &g_ltc, &g_cel, &g_fem);
+        volume_correction(&g_cdo, &g_cel, &g_fem);
+    }
+    cudaDeviceSynchronize();
+    return g_err;
+}
+
+// ms[5]: device time of stress, ibm_st1, lbm_d3q19, ibm_st2, volume_correction
+int ref_time_steps(int nsteps, double *ms)
+{
+    cudaEvent_t ev[6];
+    for (auto &e : ev) cudaEventCreate(&e);
+    for (int k = 0; k < 5; k++) ms[k] = 0.0;
+    for (int s = 0; s < nsteps && !g_err; s++) {
+        g_prc.iter++;
+        cudaEventRecord(ev[0]);
+        stress(&g_prc, &g_cdo, &g_cel, &g_fem, &g_ltc);
+        cudaEventRecord(ev[1]);
+        ibm_st1(&g_cdo, &g_ltc, &g_cel);
+        cudaEventRecord(ev[2]);
+        lbm_d3q19(&g_prc, &g_cdo, &g_ltc);
+        cudaEventRecord(ev[3]);
+        ibm_st2(&g_cdo, &g_ltc, &g_cel, &g_fem);
+        cudaEventRecord(ev[4]);
+        volume_correction(&g_cdo, &g_cel, &g_fem);
+        cudaEventRecord(ev[5]);
+        cudaEventSynchronize(ev[5]);
+        for (int k = 0; k < 5; k++) {
+            float t = 0.f;
+            cudaEventElapsedTime(&t, ev[k], ev[k + 1]);
+            ms[k] += t;
+        }
+    }
+    for (auto &e : ev) cudaEventDestroy(e);
+    return g_err;
+}
+
+// any pointer may be NULL
+int ref_get_lattice(double *fn, double *dn, double *un, double *vn, double *wn, double *fx, double *fy, double *fz)
+{
+    const int n = g_cdo.n;
+    cudaDeviceSynchronize();
+    if (fn) down(fn, g_ltc.fnD, (size_t)n * Q);
+    if (dn) down(dn, g_ltc.dnD, n);
+    if (un) down(un, g_ltc.unD, n);
+    if (vn) down(vn, g_ltc.vnD, n);
+    if (wn) down(wn, g_ltc.wnD, n);
+    if (fx) down(fx, g_ltc.fxD, n);
+    if (fy) down(fy, g_ltc.fyD, n);
+    if (fz) down(fz, g_ltc.fzD, n);
+    return 0;
+}
+
+int ref_get_cells(double *x, double *y, double *z, double *u, double *v, double *w, double *fx, double *fy,
+                  double *fz, double *xd, double *gx, double *volume0, double *nd)
+{
+    const int nv = g_cel.n * g_cel.vertex, ne = g_cel.n * g_cel.element;
+    cudaDeviceSynchronize();
+    if (x) down(x, g_cel.xD, nv);
+    if (y) down(y, g_cel.yD, nv);
+    if (z) down(z, g_cel.zD, nv);
+    if (u) down(u, g_cel.uD, nv);
+    if (v) down(v, g_cel.vD, nv);
+    if (w) down(w, g_cel.wD, nv);
+    if (fx) down(fx, g_cel.fxD, nv);
+    if (fy) down(fy, g_cel.fyD, nv);
+    if (fz) down(fz, g_cel.fzD, nv);
+    if (xd) down(xd, g_fem.xd, nv * 3);
+    if (gx) memcpy(gx, g_cel.gx, sizeof(double) * 3 * g_cel.n);
+    if (volume0) memcpy(volume0, g_cel.volume0, sizeof(double) * g_cel.n);
+    if (nd) down(nd, g_fem.nd, ne * 4);
+    return 0;
+}
+
+}  // extern "C"

@@ -69,14 +69,19 @@ spread_kernel(const Geom g, const double *__restrict__ X, long long nv, int V,
     }
     for (int v = tid; v < V; v += blockDim.x) {
         const double lx = lat_x(g, xs[v]), ly = lat_y(g, ys[v]);
-        const double lz = unwrap_near(lat_z(g, zs[v]), az, g.nzc);
+        const double lzr = lat_z(g, zs[v]);
+        const double lz = unwrap_near(lzr, az, g.nzc);
         const double flx = floor(lx), fly = floor(ly), flz = floor(lz);
         float wx[4], wy[4], wz[4];
         delta4((float)(lx - flx), wx); delta4((float)(ly - fly), wy); delta4((float)(lz - flz), wz);
         const int ix0 = (int)flx - 1, iy0 = (int)fly - 1, iz0 = (int)flz - 1;
+        const int izr0 = iz0 - (int)lrint(lz - lzr);   // stencil start in the vertex's own (unshifted) frame
         const float f0 = fxs[v] * wscale, f1 = fys[v] * wscale, f2 = fzs[v] * wscale;
 #pragma unroll
         for (int c = 0; c < 4; c++) {
+            // the reference's lattice ends two BUFF planes beyond the periodic
+            // range; stencil nodes past them are skipped (ibm.cu:107-110)
+            if (izr0 + c < -2 || izr0 + c >= g.nzc + 2) continue;
 #pragma unroll
             for (int b = 0; b < 4; b++) {
                 const int gy = iy0 + b;
@@ -145,6 +150,7 @@ __device__ __forceinline__ void interp(const Geom &g, const float *__restrict__ 
     float su = 0.f, sv = 0.f, sw = 0.f;
 #pragma unroll
     for (int c = 0; c < 4; c++) {
+        if (iz0 + c < -2 || iz0 + c >= g.nzc + 2) continue;   // beyond the BUFF planes (ibm.cu:453-455)
         const long long zb = (long long)wrap_z(iz0 + c, g.nzc) * g.plane;
 #pragma unroll
         for (int b = 0; b < 4; b++) {

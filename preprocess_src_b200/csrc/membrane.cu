@@ -216,22 +216,24 @@ static void launch_real(const MembraneArgs &a, cudaStream_t s)
     }
 }
 
-template <typename Real>
-static cudaError_t setup_real(int bytes)
-{
-    cudaError_t e = cudaSuccess, r;
-    if ((r = cudaFuncSetAttribute(membrane_kernel<Real, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess) e = r;
-    if ((r = cudaFuncSetAttribute(membrane_kernel<Real, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess) e = r;
-    if ((r = cudaFuncSetAttribute(membrane_kernel<Real, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess) e = r;
-    if ((r = cudaFuncSetAttribute(membrane_kernel<Real, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess) e = r;
-    return e;
-}
+cudaError_t set_max_dyn_smem(const void *kernel, int optin, int *granted);
 
-cudaError_t membrane_setup(int bytes)
+// the smallest limit over all instantiations bounds the vertices per cell
+cudaError_t membrane_setup(int optin, int *max_bytes)
 {
-    cudaError_t e = setup_real<float>(bytes);
-    cudaError_t f = setup_real<double>(bytes);
-    return e != cudaSuccess ? e : f;
+    const void *ks[] = {(const void *)membrane_kernel<float, 1>, (const void *)membrane_kernel<float, 2>,
+                        (const void *)membrane_kernel<float, 3>, (const void *)membrane_kernel<float, 4>,
+                        (const void *)membrane_kernel<double, 1>, (const void *)membrane_kernel<double, 2>,
+                        (const void *)membrane_kernel<double, 3>, (const void *)membrane_kernel<double, 4>};
+    int lo = optin;
+    for (const void *k : ks) {
+        int g = 0;
+        cudaError_t e = set_max_dyn_smem(k, optin, &g);
+        if (e != cudaSuccess) return e;
+        lo = g < lo ? g : lo;
+    }
+    if (max_bytes) *max_bytes = lo;
+    return cudaSuccess;
 }
 
 void launch_membrane(const MembraneArgs &a, bool fp64, cudaStream_t s)

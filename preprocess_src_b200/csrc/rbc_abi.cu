@@ -496,8 +496,13 @@ int rbc_create(const rbc_params *p, const rbc_mesh *mesh, const int *bc, rbc_han
         if (cudaSetDevice(h->device) != cudaSuccess) { h->err = "cudaSetDevice failed"; return bail(RBC_ERR_CUDA); }
     }
     {
-        int e = setup_kernel_attributes();
+        int mem_max = 0;
+        int e = setup_kernel_attributes(&mem_max);
         if (e) { h->err = std::string("kernel attributes: ") + cudaGetErrorString((cudaError_t)e); return bail(RBC_ERR_CUDA); }
+        if (cells && membrane_smem_bytes(mesh->vertex) > mem_max) {
+            h->err = "more vertices per cell than one CTA's shared memory holds";
+            return bail(RBC_ERR_UNSUPPORTED);
+        }
     }
     if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
         h->err = "stream creation failed";

@@ -147,8 +147,9 @@ int  volume_smem_bytes(int V);
 void launch_volume(const Geom &g, const VolumeArgs &a, cudaStream_t s);
 
 // one-time kernel attribute setup (dynamic shared memory limits); called by
-// rbc_create before any launch or graph capture
-int  setup_kernel_attributes();
+// rbc_create before any launch or graph capture.  Returns a cudaError_t value;
+// *membrane_max_smem receives the dynamic shared memory the membrane kernel may use.
+int  setup_kernel_attributes(int *membrane_max_smem);
 
 void launch_step_begin(int *d_iter, float *d_drive, double P, int flowstart, double freq, double dt,
                        cudaStream_t s);

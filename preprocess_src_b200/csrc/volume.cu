@@ -146,17 +146,30 @@ void launch_volume(const Geom &g, const VolumeArgs &a, cudaStream_t s)
     volume_kernel<<<a.ncell, VOL_THREADS, smem, s>>>(g, a);
 }
 
-cudaError_t membrane_setup(int bytes);
+cudaError_t membrane_setup(int optin, int *max_bytes);
 cudaError_t spread_setup();
 
-// Largest dynamic shared memory any launch may ask for (B200: 227 KB per CTA).
-constexpr int MAX_DYN_SMEM = 227 * 1024;
-
-int setup_kernel_attributes()
+// Dynamic shared memory limit of a kernel: the device's per-block opt-in
+// maximum minus the kernel's static shared memory.
+cudaError_t set_max_dyn_smem(const void *kernel, int optin, int *granted)
 {
-    cudaError_t e = cudaFuncSetAttribute(volume_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, MAX_DYN_SMEM);
+    cudaFuncAttributes fa;
+    cudaError_t e = cudaFuncGetAttributes(&fa, kernel);
+    if (e != cudaSuccess) return e;
+    const int bytes = optin - (int)fa.sharedSizeBytes;
+    e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (granted) *granted = bytes;
+    return e;
+}
+
+int setup_kernel_attributes(int *membrane_max_smem)
+{
+    int dev = 0, optin = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     if (e != cudaSuccess) return (int)e;
-    if ((e = membrane_setup(MAX_DYN_SMEM)) != cudaSuccess) return (int)e;
+    if ((e = set_max_dyn_smem((const void *)volume_kernel, optin, nullptr)) != cudaSuccess) return (int)e;
+    if ((e = membrane_setup(optin, membrane_max_smem)) != cudaSuccess) return (int)e;
     if ((e = spread_setup()) != cudaSuccess) return (int)e;
     return 0;
 }

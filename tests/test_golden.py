@@ -1,0 +1,50 @@
+"""The FP64 oracle against golden vectors from the reference's own kernels.
+
+Fixtures in tests/golden/*.npz were produced by tests/golden/make_golden.py,
+which runs the reference's step modules (compiled unmodified from the
+reference sources with oracle/ref_harness) on a GPU from the inputs that
+golden_cases() regenerates here.  FP64 against FP64: the only differences are
+summation order (tree reductions, thrust) and the BiCGSTAB stopping point.
+"""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from tests.golden.make_golden import SNAPSHOTS, golden_cases
+from preprocess_src_b200 import configs
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+
+
+def rel(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def fixtures():
+    return [(name, case) for name, case in golden_cases().items() if (GOLDEN / f"{name}.npz").exists()]
+
+
+@pytest.mark.parametrize("name,case", fixtures() or [pytest.param(None, None, marks=pytest.mark.skip("no fixtures"))])
+def test_oracle_matches_reference_kernels(name, case, oracle_mod):
+    g = np.load(GOLDEN / f"{name}.npz")
+    o = oracle_mod.Oracle(case)
+    assert np.abs(o["nd"] - g["setup_nd"]).max() <= 1e-12 * np.abs(g["setup_nd"]).max()
+    assert np.allclose(o["volume0"], g["setup_volume0"], rtol=1e-13)
+    assert np.allclose(o["gx"], g["setup_gx"], rtol=0, atol=1e-12)
+    m = case.bc == configs.COMP
+    done = 0
+    for s in SNAPSHOTS:
+        o.step(s - done)
+        done = s
+        u = np.concatenate([o["un"][m], o["vn"][m], o["wn"][m]])
+        uref = np.concatenate([g[f"s{s}_un"], g[f"s{s}_vn"], g[f"s{s}_wn"]])
+        assert rel(u, uref) <= 1e-9, (s, rel(u, uref))
+        assert np.abs(o["dn"][m] - g[f"s{s}_dn"]).max() <= 1e-12
+        x = np.concatenate([o[k] for k in ("x", "y", "z")])
+        xref = np.concatenate([g[f"s{s}_{k}"] for k in ("x", "y", "z")])
+        assert np.abs(x - xref).max() <= 1e-11 * np.abs(xref).max(), (s, np.abs(x - xref).max())
+        f = np.concatenate([o[k] for k in ("cfx", "cfy", "cfz")])
+        fref = np.concatenate([g[f"s{s}_{k}"] for k in ("fx", "fy", "fz")])
+        assert rel(f, fref) <= 1e-8, (s, rel(f, fref))
+        assert np.abs(o["gx"] - g[f"s{s}_gx"]).max() <= 1e-10
