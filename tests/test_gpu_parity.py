@@ -46,7 +46,8 @@ def load(o, **overrides):
     from preprocess_src_b200.step import Simulation
     sim = Simulation(o.case, **overrides)
     sim.import_lattice(o.fn)
-    sim.import_cells(x=o["x"], y=o["y"], z=o["z"], xd=o["xd"], nd=o["nd"], volume0=o["volume0"], gx=o["gx"])
+    if o.case.ncell:
+        sim.import_cells(x=o["x"], y=o["y"], z=o["z"], xd=o["xd"], nd=o["nd"], volume0=o["volume0"], gx=o["gx"])
     sim.iter = o.iter
     return sim
 
