@@ -96,7 +96,7 @@ typedef struct rbc_params {
     /* implementation choices */
     int    storage;      /* RBC_STORE_* */
     int    membrane_fp64;/* 1: element mechanics in FP64, 0: FP32 */
-    int    solver_iters; /* Chebyshev iterations of the load solve; 0 = default (20) */
+    int    solver_iters; /* Chebyshev iterations of the load solve; 0 = default (16) */
     int    device;       /* CUDA device ordinal; -1 = device 0 of this library's runtime */
 } rbc_params;
 
@@ -132,10 +132,11 @@ const char *rbc_last_error(const rbc_handle *h);
 /* fn[nx*ny*nz*19]: pre-collision populations as lbm_d3q19 leaves them in
  * ltc->fnD (lbm.cu:1575).  Only COMP nodes are read. */
 int rbc_import_ref_lattice(rbc_handle *h, const double *fn);
-/* Any pointer may be NULL.  fn: COMP nodes written, others untouched.
+/* Any pointer may be NULL.  fn: populations on COMP nodes, 0 elsewhere.
  * dn/un/vn/wn [nx*ny*nz]: density and velocity of the last lbm step with the
- * reference's half-force shift (lbm.cu:1116-1118); COMP and BUFF nodes are
- * written (BUFF by periodic image, lbm.cu:1378-1432), WALL nodes untouched. */
+ * reference's half-force shift (lbm.cu:1116-1118) on COMP nodes, their periodic
+ * images on BUFF nodes (lbm.cu:1378-1432), and rho = 1, u = 0 on WALL nodes
+ * (the values the reference's WALL nodes keep from flu_init). */
 int rbc_export_ref_lattice(rbc_handle *h, double *fn, double *dn, double *un, double *vn, double *wn);
 /* Eulerian spread force ltc->fx/fy/fz [nx*ny*nz] after rbc_ibm_st1 and before
  * rbc_lbm_d3q19 (COMP nodes, folded as ibm.cu:214-296 leaves them). */
@@ -188,6 +189,7 @@ int rbc_get_stream(const rbc_handle *h, void **stream);
 #define RBC_NUM_KERNELS 6
 #define RBC_KERNEL_NAMES {"step_begin", "membrane", "spread", "lbm_collide_stream", "advect", "volume"}
 int rbc_profile_steps(rbc_handle *h, int nsteps, double *kernel_ms);
+
 /* Sizes of the internal lattice and of the cells. */
 int rbc_dims(const rbc_handle *h, int *nx, int *ny, int *nz_periodic, int *ncell, int *vertex, int *element);
 

@@ -67,44 +67,50 @@ spread_kernel(const Geom g, const double *__restrict__ X, long long nv, int V,
         for (int i = tid; i < 3 * nb; i += blockDim.x) sbox[i] = 0.f;
         __syncthreads();
     }
-    for (int v = tid; v < V; v += blockDim.x) {
+    // One warp per vertex: lane l owns stencil nodes k = l and l + 32 with
+    // (a, b, c) = (k & 3, (k >> 2) & 3, k >> 4), so the 32 atomics of one warp
+    // instruction go to 32 different box nodes (lanes working on neighbouring
+    // vertices would collide on the same nodes).
+    const int lane = tid & 31, nwarp = blockDim.x >> 5;
+    for (int v = tid >> 5; v < V; v += nwarp) {
         const double lx = lat_x(g, xs[v]), ly = lat_y(g, ys[v]);
         const double lzr = lat_z(g, zs[v]);
         const double lz = unwrap_near(lzr, az, g.nzc);
         const double flx = floor(lx), fly = floor(ly), flz = floor(lz);
-        float wx[4], wy[4], wz[4];
-        delta4((float)(lx - flx), wx); delta4((float)(ly - fly), wy); delta4((float)(lz - flz), wz);
+        // lanes 0..2 evaluate sin/cos of the three fractions, the warp shares them
+        float sv = 0.f, cv = 0.f;
+        if (lane < 3) sincospif(0.5f * (float)(lane == 0 ? lx - flx : (lane == 1 ? ly - fly : lz - flz)), &sv, &cv);
         const int ix0 = (int)flx - 1, iy0 = (int)fly - 1, iz0 = (int)flz - 1;
         const int izr0 = iz0 - (int)lrint(lz - lzr);   // stencil start in the vertex's own (unshifted) frame
         const float f0 = fxs[v] * wscale, f1 = fys[v] * wscale, f2 = fzs[v] * wscale;
 #pragma unroll
-        for (int c = 0; c < 4; c++) {
+        for (int half = 0; half < 2; half++) {
+            const int k = lane + 32 * half;
+            const int ka = k & 3, kb = (k >> 2) & 3, kc = k >> 4;
+            // phi at offset 0..3 = (1 - s, 1 + c, 1 + s, 1 - c) / 4 (delta4)
+            const float sx = __shfl_sync(0xffffffffu, sv, 0), cx = __shfl_sync(0xffffffffu, cv, 0);
+            const float sy = __shfl_sync(0xffffffffu, sv, 1), cy = __shfl_sync(0xffffffffu, cv, 1);
+            const float sz = __shfl_sync(0xffffffffu, sv, 2), cz = __shfl_sync(0xffffffffu, cv, 2);
+            const float wa = 0.25f * (ka == 0 ? 1.f - sx : ka == 1 ? 1.f + cx : ka == 2 ? 1.f + sx : 1.f - cx);
+            const float wb = 0.25f * (kb == 0 ? 1.f - sy : kb == 1 ? 1.f + cy : kb == 2 ? 1.f + sy : 1.f - cy);
+            const float wc = 0.25f * (kc == 0 ? 1.f - sz : kc == 1 ? 1.f + cz : kc == 2 ? 1.f + sz : 1.f - cz);
+            const int gx = ix0 + ka, gy = iy0 + kb;
             // the reference's lattice ends two BUFF planes beyond the periodic
             // range; stencil nodes past them are skipped (ibm.cu:107-110)
-            if (izr0 + c < -2 || izr0 + c >= g.nzc + 2) continue;
-#pragma unroll
-            for (int b = 0; b < 4; b++) {
-                const int gy = iy0 + b;
-                if (gy < 0 || gy >= g.ny) continue;
-                const float wyz = wy[b] * wz[c];
-#pragma unroll
-                for (int a = 0; a < 4; a++) {
-                    const int gx = ix0 + a;
-                    if (gx < 0 || gx >= g.nx) continue;
-                    if (!(__ldg(&mask2d[gx + g.nx * gy]) & MASK_FLUID)) continue;
-                    const float w = wx[a] * wyz;
-                    if (use_box) {
-                        const long long li = (gx - bx0) + (long long)bx * ((gy - by0) + (long long)by * (iz0 + c - bz0));
-                        atomicAdd(&sbox[li], w * f0);
-                        atomicAdd(&sbox[nb + li], w * f1);
-                        atomicAdd(&sbox[2 * nb + li], w * f2);
-                    } else {
-                        const long long gi = (long long)wrap_z(iz0 + c, g.nzc) * g.plane + gx + (long long)g.nx * gy;
-                        atomicAdd(&Fx[gi], w * f0);
-                        atomicAdd(&Fy[gi], w * f1);
-                        atomicAdd(&Fz[gi], w * f2);
-                    }
-                }
+            if (izr0 + kc < -2 || izr0 + kc >= g.nzc + 2) continue;
+            if (gx < 0 || gx >= g.nx || gy < 0 || gy >= g.ny) continue;
+            if (!(__ldg(&mask2d[gx + g.nx * gy]) & MASK_FLUID)) continue;
+            const float w = wa * wb * wc;
+            if (use_box) {
+                const long long li = (gx - bx0) + (long long)bx * ((gy - by0) + (long long)by * (iz0 + kc - bz0));
+                atomicAdd(&sbox[li], w * f0);
+                atomicAdd(&sbox[nb + li], w * f1);
+                atomicAdd(&sbox[2 * nb + li], w * f2);
+            } else {
+                const long long gi = (long long)wrap_z(iz0 + kc, g.nzc) * g.plane + gx + (long long)g.nx * gy;
+                atomicAdd(&Fx[gi], w * f0);
+                atomicAdd(&Fy[gi], w * f1);
+                atomicAdd(&Fz[gi], w * f2);
             }
         }
     }
@@ -138,51 +144,62 @@ void launch_spread(const Geom &g, const SpreadArgs &a, cudaStream_t s)
 
 // ---- interpolation + RK4 advection ---------------------------------------
 
-__device__ __forceinline__ void interp(const Geom &g, const float *__restrict__ ux, const float *__restrict__ uy,
-                                       const float *__restrict__ uz, double px, double py, double pz,
-                                       float &ur, float &vr, float &wr)
+// Four lanes per vertex: lane c of the group gathers stencil plane c (16 nodes,
+// one float4 (u, v, w, rho) each); the group sums its partial velocities with
+// two butterfly shuffles, so every lane holds the interpolated velocity.
+__device__ __forceinline__ void interp4(const Geom &g, const float4 *__restrict__ uvr, double px, double py,
+                                        double pz, int c, float &ur, float &vr, float &wr)
 {
     const double lx = lat_x(g, px), ly = lat_y(g, py), lz = lat_z(g, pz);
     const double flx = floor(lx), fly = floor(ly), flz = floor(lz);
     float wx[4], wy[4], wz[4];
     delta4((float)(lx - flx), wx); delta4((float)(ly - fly), wy); delta4((float)(lz - flz), wz);
-    const int ix0 = (int)flx - 1, iy0 = (int)fly - 1, iz0 = (int)flz - 1;
+    const int ix0 = (int)flx - 1, iy0 = (int)fly - 1, iz = (int)flz - 1 + c;
     float su = 0.f, sv = 0.f, sw = 0.f;
-#pragma unroll
-    for (int c = 0; c < 4; c++) {
-        if (iz0 + c < -2 || iz0 + c >= g.nzc + 2) continue;   // beyond the BUFF planes (ibm.cu:453-455)
-        const long long zb = (long long)wrap_z(iz0 + c, g.nzc) * g.plane;
+    if (iz >= -2 && iz < g.nzc + 2) {   // beyond the BUFF planes (ibm.cu:453-455)
+        const long long zb = (long long)wrap_z(iz, g.nzc) * g.plane;
+        const float wzc = c == 0 ? wz[0] : c == 1 ? wz[1] : c == 2 ? wz[2] : wz[3];
 #pragma unroll
         for (int b = 0; b < 4; b++) {
             const int gy = iy0 + b;
             if (gy < 0 || gy >= g.ny) continue;
-            const float wyz = wy[b] * wz[c];
+            const float wyz = wy[b] * wzc;
 #pragma unroll
             for (int a = 0; a < 4; a++) {
                 const int gx = ix0 + a;
                 if (gx < 0 || gx >= g.nx) continue;
-                const long long i = zb + gx + (long long)g.nx * gy;
+                const float4 q = __ldg(&uvr[zb + gx + (long long)g.nx * gy]);
                 const float w = wx[a] * wyz;
-                su += w * __ldg(&ux[i]); sv += w * __ldg(&uy[i]); sw += w * __ldg(&uz[i]);
+                su += w * q.x; sv += w * q.y; sw += w * q.z;
             }
         }
+    }
+#pragma unroll
+    for (int o = 1; o <= 2; o <<= 1) {
+        su += __shfl_xor_sync(0xffffffffu, su, o);
+        sv += __shfl_xor_sync(0xffffffffu, sv, o);
+        sw += __shfl_xor_sync(0xffffffffu, sw, o);
     }
     ur = su; vr = sv; wr = sw;
 }
 
-__global__ void __launch_bounds__(128)
+constexpr int ADVECT_THREADS = 256;
+
+__global__ void __launch_bounds__(ADVECT_THREADS, 4)
 advect_kernel(const Geom g, double *__restrict__ X, double *__restrict__ Xd, float *__restrict__ U,
-              const float *__restrict__ ux, const float *__restrict__ uy, const float *__restrict__ uz,
-              long long nv, double dtM, int *__restrict__ flags)
+              const float4 *__restrict__ uvr, long long nv, double dtM, int *__restrict__ flags)
 {
-    const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= nv) return;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int c = (int)(t & 3);
+    const bool live = (t >> 2) < nv;
+    const long long j = live ? (t >> 2) : nv - 1;   // idle lanes shadow the last vertex for the shuffles
     const double xn = X[j], yn = X[nv + j], zn = X[2 * nv + j];
     float u1, v1, w1, u2, v2, w2, u3, v3, w3, u4, v4, w4;
-    interp(g, ux, uy, uz, xn, yn, zn, u1, v1, w1);
-    interp(g, ux, uy, uz, xn + u1 * dtM * 0.5, yn + v1 * dtM * 0.5, zn + w1 * dtM * 0.5, u2, v2, w2);
-    interp(g, ux, uy, uz, xn + u2 * dtM * 0.5, yn + v2 * dtM * 0.5, zn + w2 * dtM * 0.5, u3, v3, w3);
-    interp(g, ux, uy, uz, xn + u3 * dtM, yn + v3 * dtM, zn + w3 * dtM, u4, v4, w4);
+    interp4(g, uvr, xn, yn, zn, c, u1, v1, w1);
+    interp4(g, uvr, xn + u1 * dtM * 0.5, yn + v1 * dtM * 0.5, zn + w1 * dtM * 0.5, c, u2, v2, w2);
+    interp4(g, uvr, xn + u2 * dtM * 0.5, yn + v2 * dtM * 0.5, zn + w2 * dtM * 0.5, c, u3, v3, w3);
+    interp4(g, uvr, xn + u3 * dtM, yn + v3 * dtM, zn + w3 * dtM, c, u4, v4, w4);
+    if (!live || c != 0) return;
     const double um = ((double)u1 + 2.0 * u2 + 2.0 * u3 + u4) / 6.0;
     const double vm = ((double)v1 + 2.0 * v2 + 2.0 * v3 + v4) / 6.0;
     const double wm = ((double)w1 + 2.0 * w2 + 2.0 * w3 + w4) / 6.0;
@@ -200,8 +217,9 @@ advect_kernel(const Geom g, double *__restrict__ X, double *__restrict__ Xd, flo
 void launch_advect(const Geom &g, const AdvectArgs &a, cudaStream_t s)
 {
     if (a.nv <= 0) return;
-    advect_kernel<<<(unsigned)((a.nv + 127) / 128), 128, 0, s>>>(g, a.X, a.Xd, a.U, a.ux, a.uy, a.uz, a.nv,
-                                                                 a.dtM, a.flags);
+    const long long threads = 4 * a.nv;
+    advect_kernel<<<(unsigned)((threads + ADVECT_THREADS - 1) / ADVECT_THREADS), ADVECT_THREADS, 0, s>>>(
+        g, a.X, a.Xd, a.U, a.uvr, a.nv, a.dtM, a.flags);
 }
 
 }  // namespace rbc

@@ -37,7 +37,7 @@ constexpr int LBM_THREADS = 256;
 template <int STORE>
 __global__ void __launch_bounds__(LBM_THREADS)
 lbm_collide_stream(const typename Store<STORE>::T *__restrict__ gin, typename Store<STORE>::T *__restrict__ gout,
-                   float *__restrict__ rho, float *__restrict__ ux, float *__restrict__ uy, float *__restrict__ uz,
+                   float4 *__restrict__ uvr,
                    float *__restrict__ Fx, float *__restrict__ Fy, float *__restrict__ Fz,
                    const uint32_t *__restrict__ mask2d, const float *__restrict__ drive,
                    int nx, int ny, int nzc, long long nint,
@@ -82,7 +82,7 @@ lbm_collide_stream(const typename Store<STORE>::T *__restrict__ gin, typename St
     const float inv = 1.0f / (r * Cr);
     const float u = (jx + Gx) * inv, v = (jy + Gy) * inv, w = (jz + Gz) * inv;
 
-    rho[idx] = r; ux[idx] = u; uy[idx] = v; uz[idx] = w;
+    uvr[idx] = make_float4(u, v, w, r);
     if (fx != 0.f || fy != 0.f || fz != 0.f) { Fx[idx] = 0.f; Fy[idx] = 0.f; Fz[idx] = 0.f; }
 
     // BGK + Guo forcing (lbm.cu:1129-1213): with G the half force above,
@@ -107,11 +107,11 @@ void launch_lbm(const Geom &g, int storage, const LbmArgs &a, cudaStream_t s)
     const unsigned blocks = (unsigned)((g.nint + LBM_THREADS - 1) / LBM_THREADS);
     if (storage == RBC_STORE_F16)
         lbm_collide_stream<RBC_STORE_F16><<<blocks, LBM_THREADS, 0, s>>>(
-            (const __half *)a.gin, (__half *)a.gout, a.rho, a.ux, a.uy, a.uz, a.Fx, a.Fy, a.Fz, a.mask2d,
+            (const __half *)a.gin, (__half *)a.gout, a.uvr, a.Fx, a.Fy, a.Fz, a.mask2d,
             a.drive, g.nx, g.ny, g.nzc, g.nint, a.omega, a.Cr, a.Bc, a.scale, a.inv_scale);
     else
         lbm_collide_stream<RBC_STORE_F32><<<blocks, LBM_THREADS, 0, s>>>(
-            (const float *)a.gin, (float *)a.gout, a.rho, a.ux, a.uy, a.uz, a.Fx, a.Fy, a.Fz, a.mask2d,
+            (const float *)a.gin, (float *)a.gout, a.uvr, a.Fx, a.Fy, a.Fz, a.mask2d,
             a.drive, g.nx, g.ny, g.nzc, g.nint, a.omega, a.Cr, a.Bc, a.scale, a.inv_scale);
 }
 
@@ -154,9 +154,7 @@ __global__ void import_lattice_kernel(const Geom g, const double *__restrict__ f
 // entries to the reference's untouched initial values (rho 1, u 0).
 template <int STORE>
 __global__ void export_lattice_kernel(const Geom g, const typename Store<STORE>::T *__restrict__ gin,
-                                      const uint32_t *__restrict__ mask2d,
-                                      const float *__restrict__ rho, const float *__restrict__ ux,
-                                      const float *__restrict__ uy, const float *__restrict__ uz,
+                                      const uint32_t *__restrict__ mask2d, const float4 *__restrict__ uvr,
                                       float inv_scale, double *__restrict__ fn, double *__restrict__ dn,
                                       double *__restrict__ un, double *__restrict__ vn, double *__restrict__ wn)
 {
@@ -191,7 +189,8 @@ __global__ void export_lattice_kernel(const Geom g, const typename Store<STORE>:
         double r = 1.0, a = 0.0, b = 0.0, c = 0.0;
         if (m & MASK_FLUID) {
             const long long idx = (long long)wrap_z(zr - 2, g.nzc) * g.plane + xy;
-            r = rho[idx]; a = ux[idx]; b = uy[idx]; c = uz[idx];
+            const float4 q = uvr[idx];
+            r = q.w; a = q.x; b = q.y; c = q.z;
         }
         dn[i] = r; un[i] = a; vn[i] = b; wn[i] = c;
     }
@@ -220,6 +219,18 @@ __global__ void fill_f32_kernel(float *p, long long n, float v)
     if (i < n) p[i] = v;
 }
 
+__global__ void fill_f4_kernel(float4 *p, long long n, float4 v)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = v;
+}
+
+void launch_fill_f4(float4 *p, long long n, float4 v, cudaStream_t s)
+{
+    if (n <= 0) return;
+    fill_f4_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(p, n, v);
+}
+
 void launch_import_lattice(const Geom &g, int storage, const double *fn_ref, void *gout,
                            const uint32_t *mask2d, float scale, cudaStream_t s)
 {
@@ -231,17 +242,16 @@ void launch_import_lattice(const Geom &g, int storage, const double *fn_ref, voi
 }
 
 void launch_export_lattice(const Geom &g, int storage, const void *gin, const uint32_t *mask2d,
-                           const float *rho, const float *ux, const float *uy, const float *uz,
-                           float inv_scale, double *fn_ref, double *dn, double *un, double *vn,
-                           double *wn, cudaStream_t s)
+                           const float4 *uvr, float inv_scale, double *fn_ref, double *dn, double *un,
+                           double *vn, double *wn, cudaStream_t s)
 {
     const long long nref = g.plane * g.nzr;
     const unsigned blocks = (unsigned)((nref + 255) / 256);
     if (storage == RBC_STORE_F16)
-        export_lattice_kernel<RBC_STORE_F16><<<blocks, 256, 0, s>>>(g, (const __half *)gin, mask2d, rho, ux, uy, uz,
+        export_lattice_kernel<RBC_STORE_F16><<<blocks, 256, 0, s>>>(g, (const __half *)gin, mask2d, uvr,
                                                                      inv_scale, fn_ref, dn, un, vn, wn);
     else
-        export_lattice_kernel<RBC_STORE_F32><<<blocks, 256, 0, s>>>(g, (const float *)gin, mask2d, rho, ux, uy, uz,
+        export_lattice_kernel<RBC_STORE_F32><<<blocks, 256, 0, s>>>(g, (const float *)gin, mask2d, uvr,
                                                                      inv_scale, fn_ref, dn, un, vn, wn);
 }
 

@@ -25,14 +25,29 @@
 //     (Chebyshev iteration as in Y. Saad, Iterative Methods for Sparse Linear
 //     Systems, 2nd ed., Alg. 12.1.)
 //  4. f_i = -q_i * ds_i is written out.
-// Element mechanics run in FP32 or FP64 (Real); the solve runs in FP32.
+//
+// Tension without cancellation.  The reference evaluates
+//   t = ca n + cb g^-1,  ca = rgs (I1 + 1) / Js,  cb = (C I2 - 1) Js
+// where the two O(1) terms cancel to O(strain); in FP32 that turns round-off
+// into tension noise of order C * 1e-7.  Here the deformed metric enters only
+// through its difference from the reference metric, D = g - G, formed in FP64
+// from FP64 edge vectors, and everything after that works on small numbers:
+//   I1 = n : D,   I2 = det(n) (G11 D22 + G22 D11 - 2 G12 D12 + det D),
+//   Js - 1 = I2 / (Js + 1),
+//   t = (ca - 1) n + (cb + 1) g^-1 + n D g^-1        (n - g^-1 = n D g^-1),
+//   ca - 1 = (rgs I1 + (rgs - 1) - (Js - 1)) / Js,   cb + 1 = C I2 Js - (Js - 1)
+// (neo-Hookean: ca = rgs / Js, cb = -rgs / Js^3), algebraically the same
+// tension as stress.cu:94-99.
+// Element mechanics after the FP64 metric difference run in FP32 or FP64
+// (Real); the solve runs in FP32.
 #include "rbc_internal.cuh"
 
 namespace rbc {
 
 constexpr int MEM_MAX_THREADS = 1024;
 
-int membrane_smem_bytes(int V) { return 60 * V; }   // pos 24V (later 2x3 FP32 d-buffers), coef 24V, nbr 12V
+// pos 24V (then float4 d-buffers 32V), coef 24V, nbr 12V
+int membrane_smem_bytes(int V) { return 68 * V; }
 
 __device__ __forceinline__ double mimage(double d, double L) {
     if (d > L * 0.5) d -= L; else if (d < -L * 0.5) d += L;
@@ -60,9 +75,9 @@ membrane_kernel(const MembraneArgs a)
     __shared__ float red[32];
     const int V = a.V, E = a.E, tid = threadIdx.x, T = blockDim.x;
     double *pos = reinterpret_cast<double *>(smem);                    // [3][V]
-    float *dbuf = reinterpret_cast<float *>(smem);                     // [2][3][V], after assembly
-    float *coef = reinterpret_cast<float *>(smem + 24 * (size_t)V);    // [6][V]
-    int16_t *snbr = reinterpret_cast<int16_t *>(smem + 48 * (size_t)V);// [6][V]
+    float4 *dbuf = reinterpret_cast<float4 *>(smem);                   // [2][V], after assembly
+    float *coef = reinterpret_cast<float *>(smem + 32 * (size_t)V);    // [6][V]
+    int16_t *snbr = reinterpret_cast<int16_t *>(smem + 56 * (size_t)V);// [6][V]
 
     const int cell = blockIdx.x;
     const long long vb = (long long)cell * V, eb = (long long)cell * E, nv = a.nv, ne = a.ne;
@@ -88,25 +103,43 @@ membrane_kernel(const MembraneArgs a)
             const int pk = __ldg(&a.v2e[k]);
             const int e = v2e_elem(pk), en = v2e_en(pk);
             const int ia = __ldg(&a.tri[3 * e]), ib = __ldg(&a.tri[3 * e + 1]), ic = __ldg(&a.tri[3 * e + 2]);
-            const Real v1x = (Real)(pos[ib] - pos[ia]), v1y = (Real)(pos[V + ib] - pos[V + ia]), v1z = (Real)(pos[2 * V + ib] - pos[2 * V + ia]);
-            const Real v2x = (Real)(pos[ic] - pos[ia]), v2y = (Real)(pos[V + ic] - pos[V + ia]), v2z = (Real)(pos[2 * V + ic] - pos[2 * V + ia]);
-            // deformed covariant metric and its inverse (stress.cu:75-88)
-            const Real g11 = v1x * v1x + v1y * v1y + v1z * v1z;
-            const Real g12 = v1x * v2x + v1y * v2y + v1z * v2z;
-            const Real g22 = v2x * v2x + v2y * v2y + v2z * v2z;
+            const double e1x = pos[ib] - pos[ia], e1y = pos[V + ib] - pos[V + ia], e1z = pos[2 * V + ib] - pos[2 * V + ia];
+            const double e2x = pos[ic] - pos[ia], e2y = pos[V + ic] - pos[V + ia], e2z = pos[2 * V + ic] - pos[2 * V + ia];
+            // deformed covariant metric (stress.cu:75-84) and its difference from the reference, in FP64
+            const double g11d = e1x * e1x + e1y * e1y + e1z * e1z;
+            const double g12d = e1x * e2x + e1y * e2y + e1z * e2z;
+            const double g22d = e2x * e2x + e2y * e2y + e2z * e2z;
+            const double G11 = __ldg(&a.gref[eb + e]), G12 = __ldg(&a.gref[ne + eb + e]), G22 = __ldg(&a.gref[2 * ne + eb + e]);
+            const double n00d = __ldg(&a.nref[eb + e]), n01d = __ldg(&a.nref[ne + eb + e]), n11d = __ldg(&a.nref[2 * ne + eb + e]);
+            const Real d11 = (Real)(g11d - G11), d12 = (Real)(g12d - G12), d22 = (Real)(g22d - G22);
+            const Real g11 = (Real)g11d, g12 = (Real)g12d, g22 = (Real)g22d;
+            const Real n00 = (Real)n00d, n01 = (Real)n01d, n11 = (Real)n11d;
+            const Real detn = (Real)(n00d * n11d - n01d * n01d);
             const Real det = g11 * g22 - g12 * g12;
             const Real idet = (Real)1 / det;
-            const Real n00 = (Real)__ldg(&a.nref[eb + e]), n01 = (Real)__ldg(&a.nref[ne + eb + e]), n11 = (Real)__ldg(&a.nref[2 * ne + eb + e]);
-            // invariants (stress.cu:90-93)
-            const Real i1 = n00 * g11 + (Real)2 * n01 * g12 + n11 * g22 - (Real)2;
-            const Real i2 = det * (n00 * n11 - n01 * n01) - (Real)1;
+            // invariants (stress.cu:90-93) from the metric difference
+            const Real i1 = n00 * d11 + (Real)2 * n01 * d12 + n11 * d22;
+            const Real i2 = detn * ((Real)G11 * d22 + (Real)G22 * d11 - (Real)2 * (Real)G12 * d12 + d11 * d22 - d12 * d12);
             const Real js = sqrt(i2 + (Real)1);
-            Real ca, cb;   // t = ca * n_ref + cb * g^-1 (stress.cu:94-99)
-            if (a.law == RBC_LAW_SKALAK) { ca = rgs * (i1 + (Real)1) / js; cb = (C * i2 - (Real)1) * js; }
-            else { ca = rgs / js; cb = -rgs * js / ((i2 + (Real)1) * (i2 + (Real)1)); }
-            const Real t00 = ca * n00 + cb * g22 * idet;
-            const Real t01 = ca * n01 - cb * g12 * idet;
-            const Real t11 = ca * n11 + cb * g11 * idet;
+            const Real jsm1 = i2 / (js + (Real)1);
+            Real al, be;   // ca - 1 and cb + 1 of the law (stress.cu:94-99)
+            if (a.law == RBC_LAW_SKALAK) {
+                al = (rgs * i1 + (rgs - (Real)1) - jsm1) / js;
+                be = C * i2 * js - jsm1;
+            } else {
+                const Real js3 = js * js * js;
+                al = ((rgs - (Real)1) - jsm1) / js;
+                be = (jsm1 * (js * js + js + (Real)1) - (rgs - (Real)1)) / js3;
+            }
+            const Real gi00 = g22 * idet, gi01 = -g12 * idet, gi11 = g11 * idet;
+            // n D g^-1 = n - g^-1, symmetrised
+            const Real p00 = n00 * d11 + n01 * d12, p01 = n00 * d12 + n01 * d22;
+            const Real p10 = n01 * d11 + n11 * d12, p11 = n01 * d12 + n11 * d22;
+            const Real t00 = al * n00 + be * gi00 + (p00 * gi00 + p01 * gi01);
+            const Real t01 = al * n01 + be * gi01 + (Real)0.5 * ((p00 * gi01 + p01 * gi11) + (p10 * gi00 + p11 * gi01));
+            const Real t11 = al * n11 + be * gi11 + (p10 * gi01 + p11 * gi11);
+            const Real v1x = (Real)e1x, v1y = (Real)e1y, v1z = (Real)e1z;
+            const Real v2x = (Real)e2x, v2y = (Real)e2y, v2z = (Real)e2z;
             const Real gab = sqrt(det);
             diag += gab * (Real)(1.0 / 12.0);
             const Real o = gab * (Real)(1.0 / 24.0);
@@ -140,13 +173,13 @@ membrane_kernel(const MembraneArgs a)
         for (int c = 0; c < 3; c++) {
             x[m][c] = 0.f; r[m][c] = rhs[m][c]; d[m][c] = rhs[m][c] / theta;
             bb += rhs[m][c] * rhs[m][c];
-            if (i < V) dbuf[c * V + i] = d[m][c];
         }
+        if (i < V) dbuf[i] = make_float4(d[m][0], d[m][1], d[m][2], 0.f);
     }
     __syncthreads();
     for (int it = 0; it < a.niter; it++) {
-        const float *cur = dbuf + (it & 1) * 3 * V;
-        float *nxt = dbuf + ((it + 1) & 1) * 3 * V;
+        const float4 *cur = dbuf + (it & 1) * V;
+        float4 *nxt = dbuf + ((it + 1) & 1) * V;
         const float rho_n = 1.0f / (2.0f * sigma - rho);
         const float c1 = rho_n * rho, c2 = 2.0f * rho_n / delta;
 #pragma unroll
@@ -159,16 +192,15 @@ membrane_kernel(const MembraneArgs a)
                 const int j = snbr[s * V + i];
                 if (j >= 0) {
                     const float w = coef[s * V + i];
-                    ad0 += w * cur[j]; ad1 += w * cur[V + j]; ad2 += w * cur[2 * V + j];
+                    const float4 dj = cur[j];
+                    ad0 += w * dj.x; ad1 += w * dj.y; ad2 += w * dj.z;
                 }
             }
             x[m][0] += d[m][0]; x[m][1] += d[m][1]; x[m][2] += d[m][2];
             r[m][0] -= ad0; r[m][1] -= ad1; r[m][2] -= ad2;
 #pragma unroll
-            for (int c = 0; c < 3; c++) {
-                d[m][c] = c1 * d[m][c] + c2 * r[m][c];
-                nxt[c * V + i] = d[m][c];
-            }
+            for (int c = 0; c < 3; c++) d[m][c] = c1 * d[m][c] + c2 * r[m][c];
+            nxt[i] = make_float4(d[m][0], d[m][1], d[m][2], 0.f);
         }
         rho = rho_n;
         __syncthreads();

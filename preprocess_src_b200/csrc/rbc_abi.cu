@@ -22,7 +22,7 @@ namespace {
 thread_local std::string g_create_error;
 
 constexpr float F16_SCALE = 32768.0f;     // (f - w) * 2^15 keeps |g| < 2 inside FP16 range
-constexpr int DEFAULT_SOLVER_ITERS = 20;  // Chebyshev error factor <= 2 * 3^-20 ~ 6e-10
+constexpr int DEFAULT_SOLVER_ITERS = 16;  // Chebyshev error factor <= 2 * 3^-16 ~ 4.6e-8 (FP32 solve)
 constexpr int KERNELS_PER_STEP = 6;       // step_begin, membrane, spread, lbm, advect, volume
 
 }  // namespace
@@ -37,11 +37,11 @@ struct rbc_handle {
     void *g[2] = {nullptr, nullptr};
     int cur = 0;
     size_t gbytes = 0;
-    float *rho = nullptr, *ux = nullptr, *uy = nullptr, *uz = nullptr;
+    float4 *uvr = nullptr;
     float *Fx = nullptr, *Fy = nullptr, *Fz = nullptr;
     uint32_t *mask2d = nullptr;
     // cells
-    double *X = nullptr, *Xd = nullptr, *nref = nullptr;
+    double *X = nullptr, *Xd = nullptr, *nref = nullptr, *gref = nullptr;
     float *U = nullptr, *Fv = nullptr;
     int *tri = nullptr, *v2e_off = nullptr, *v2e = nullptr;
     int16_t *nbr = nullptr;
@@ -171,11 +171,14 @@ int build_topology(rbc_handle *h, const int *tri, std::vector<int> &off, std::ve
     return RBC_OK;
 }
 
-// set_contravariant (init2.cu:206-255) on the AoS reference shape; output [3][ne]
-void reference_metric(const rbc_handle *h, const int *tri, const double *xr, std::vector<double> &nref)
+// set_contravariant (init2.cu:206-255) on the AoS reference shape; outputs
+// [3][ne]: the contravariant metric n and the covariant metric G = n^-1
+void reference_metric(const rbc_handle *h, const int *tri, const double *xr, std::vector<double> &nref,
+                      std::vector<double> &gref)
 {
     const long long ne = h->ne;
     nref.assign(3 * ne, 0.0);
+    gref.assign(3 * ne, 0.0);
     for (int c = 0; c < h->ncell; c++)
         for (int e = 0; e < h->E; e++) {
             const long long a = (long long)c * h->V + tri[3 * e], b = (long long)c * h->V + tri[3 * e + 1],
@@ -190,6 +193,9 @@ void reference_metric(const rbc_handle *h, const int *tri, const double *xr, std
             nref[id] = lv2 / dv12;
             nref[ne + id] = -inv12 / dv12;
             nref[2 * ne + id] = lv1 / dv12;
+            gref[id] = lv1;
+            gref[ne + id] = inv12;
+            gref[2 * ne + id] = lv2;
         }
 }
 
@@ -283,8 +289,8 @@ void free_all(rbc_handle *h)
 {
     if (!h) return;
     for (cudaGraphExec_t g : h->graph) if (g) cudaGraphExecDestroy(g);
-    void *ptrs[] = {h->g[0], h->g[1], h->rho, h->ux, h->uy, h->uz, h->Fx, h->Fy, h->Fz, h->mask2d,
-                    h->X, h->Xd, h->nref, h->U, h->Fv, h->tri, h->v2e_off, h->v2e, h->nbr, h->vol0, h->gx,
+    void *ptrs[] = {h->g[0], h->g[1], h->uvr, h->Fx, h->Fy, h->Fz, h->mask2d,
+                    h->X, h->Xd, h->nref, h->gref, h->U, h->Fv, h->tri, h->v2e_off, h->v2e, h->nbr, h->vol0, h->gx,
                     h->vol_out, h->area_out, h->cen_out, h->d_int, h->d_drive, h->staging};
     for (void *q : ptrs) if (q) cudaFree(q);
     if (h->stream) cudaStreamDestroy(h->stream);
@@ -296,7 +302,7 @@ int launch_stress(rbc_handle *h)
 {
     if (h->ncell == 0) return RBC_OK;
     MembraneArgs a{};
-    a.Xd = h->Xd; a.nv = h->nv; a.ne = h->ne; a.nref = h->nref;
+    a.Xd = h->Xd; a.nv = h->nv; a.ne = h->ne; a.nref = h->nref; a.gref = h->gref;
     a.tri = h->tri; a.v2e_off = h->v2e_off; a.v2e = h->v2e; a.nbr = h->nbr; a.Fv = h->Fv;
     a.V = h->V; a.E = h->E; a.ncell = h->ncell;
     a.C = h->p.C; a.rgs = h->p.rgs; a.law = h->p.law; a.LX = h->p.LX; a.LZ = h->p.LZ;
@@ -324,7 +330,7 @@ int launch_lbm_stage(rbc_handle *h)
 {
     LbmArgs a{};
     a.gin = h->g[h->cur]; a.gout = h->g[1 - h->cur];
-    a.rho = h->rho; a.ux = h->ux; a.uy = h->uy; a.uz = h->uz;
+    a.uvr = h->uvr;
     a.Fx = h->Fx; a.Fy = h->Fy; a.Fz = h->Fz; a.mask2d = h->mask2d; a.drive = h->d_drive;
     a.omega = (float)(1.0 / h->p.tau); a.Cr = (float)h->p.Cr; a.Bc = (float)h->p.B;
     a.scale = h->scale; a.inv_scale = h->inv_scale;
@@ -339,7 +345,7 @@ int launch_advect_stage(rbc_handle *h)
 {
     if (h->ncell == 0) return RBC_OK;
     AdvectArgs a{};
-    a.X = h->X; a.Xd = h->Xd; a.U = h->U; a.ux = h->ux; a.uy = h->uy; a.uz = h->uz; a.nv = h->nv;
+    a.X = h->X; a.Xd = h->Xd; a.U = h->U; a.uvr = h->uvr; a.nv = h->nv;
     a.dtM = h->p.dt * h->p.M; a.flags = h->d_flags();
     launch_advect(h->geo, a, h->stream);
     h->launches++;
@@ -473,12 +479,12 @@ int rbc_create(const rbc_params *p, const rbc_mesh *mesh, const int *bc, rbc_han
     // host-side setup first, so argument and mesh errors are reported without a GPU
     std::vector<int> off, packed;
     std::vector<int16_t> nbr6;
-    std::vector<double> nref, vol0, gx, xs;
+    std::vector<double> nref, gref, vol0, gx, xs;
     if (cells) {
         h->ncell = mesh->ncell; h->V = mesh->vertex; h->E = mesh->element;
         h->nv = (long long)h->ncell * h->V; h->ne = (long long)h->ncell * h->E;
         TRY(build_topology(h, mesh->tri, off, packed, nbr6));
-        reference_metric(h, mesh->tri, mesh->xr, nref);
+        reference_metric(h, mesh->tri, mesh->xr, nref, gref);
         initial_volume(h, mesh->tri, mesh->xr, vol0, gx);
         xs.resize(3 * h->nv);
         for (long long j = 0; j < h->nv; j++)
@@ -514,23 +520,22 @@ int rbc_create(const rbc_params *p, const rbc_mesh *mesh, const int *bc, rbc_han
         h->err = "out of device memory for the populations";
         return bail(RBC_ERR_CUDA);
     }
-    TRY(dalloc(h, &h->rho, g.nint)); TRY(dalloc(h, &h->ux, g.nint)); TRY(dalloc(h, &h->uy, g.nint));
-    TRY(dalloc(h, &h->uz, g.nint)); TRY(dalloc(h, &h->Fx, g.nint)); TRY(dalloc(h, &h->Fy, g.nint));
+    TRY(dalloc(h, &h->uvr, g.nint)); TRY(dalloc(h, &h->Fx, g.nint)); TRY(dalloc(h, &h->Fy, g.nint));
     TRY(dalloc(h, &h->Fz, g.nint)); TRY(dalloc(h, &h->mask2d, g.plane));
     TRY(dalloc(h, &h->d_int, 4)); TRY(dalloc(h, &h->d_drive, 1));
     if (cudaMemset(h->g[0], 0, h->gbytes) != cudaSuccess || cudaMemset(h->g[1], 0, h->gbytes) != cudaSuccess ||
-        cudaMemset(h->ux, 0, 4 * g.nint) != cudaSuccess || cudaMemset(h->uy, 0, 4 * g.nint) != cudaSuccess ||
-        cudaMemset(h->uz, 0, 4 * g.nint) != cudaSuccess || cudaMemset(h->Fx, 0, 4 * g.nint) != cudaSuccess ||
+        cudaMemset(h->Fx, 0, 4 * g.nint) != cudaSuccess ||
         cudaMemset(h->Fy, 0, 4 * g.nint) != cudaSuccess || cudaMemset(h->Fz, 0, 4 * g.nint) != cudaSuccess ||
         cudaMemset(h->d_int, 0, 4 * sizeof(int)) != cudaSuccess || cudaMemset(h->d_drive, 0, sizeof(float)) != cudaSuccess ||
         cudaMemcpy(h->mask2d, mask.data(), 4 * g.plane, cudaMemcpyHostToDevice) != cudaSuccess) {
         h->err = "device initialisation failed";
         return bail(RBC_ERR_CUDA);
     }
-    launch_fill_f32(h->rho, g.nint, 1.0f, h->stream);
+    launch_fill_f4(h->uvr, g.nint, make_float4(0.f, 0.f, 0.f, 1.f), h->stream);
 
     if (cells) {
         TRY(dalloc(h, &h->X, 3 * h->nv)); TRY(dalloc(h, &h->Xd, 3 * h->nv)); TRY(dalloc(h, &h->nref, 3 * h->ne));
+        TRY(dalloc(h, &h->gref, 3 * h->ne));
         TRY(dalloc(h, &h->U, 3 * h->nv)); TRY(dalloc(h, &h->Fv, 3 * h->nv));
         TRY(dalloc(h, &h->tri, 3 * h->E)); TRY(dalloc(h, &h->v2e_off, h->V + 1)); TRY(dalloc(h, &h->v2e, packed.size()));
         TRY(dalloc(h, &h->nbr, 6 * h->V));
@@ -539,6 +544,7 @@ int rbc_create(const rbc_params *p, const rbc_mesh *mesh, const int *bc, rbc_han
         if (cudaMemcpy(h->X, xs.data(), 8 * 3 * h->nv, cudaMemcpyHostToDevice) != cudaSuccess ||
             cudaMemcpy(h->Xd, xs.data(), 8 * 3 * h->nv, cudaMemcpyHostToDevice) != cudaSuccess ||
             cudaMemcpy(h->nref, nref.data(), 8 * 3 * h->ne, cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(h->gref, gref.data(), 8 * 3 * h->ne, cudaMemcpyHostToDevice) != cudaSuccess ||
             cudaMemset(h->U, 0, 4 * 3 * h->nv) != cudaSuccess || cudaMemset(h->Fv, 0, 4 * 3 * h->nv) != cudaSuccess ||
             cudaMemcpy(h->tri, mesh->tri, 4 * 3 * h->E, cudaMemcpyHostToDevice) != cudaSuccess ||
             cudaMemcpy(h->v2e_off, off.data(), 4 * (h->V + 1), cudaMemcpyHostToDevice) != cudaSuccess ||
@@ -595,7 +601,7 @@ int rbc_export_ref_lattice(rbc_handle *h, double *fn, double *dn, double *un, do
     if (rc) return rc;
     double *sfn = (double *)h->staging;
     double *smac = fn ? sfn + Q * n : sfn;
-    launch_export_lattice(h->geo, h->p.storage, h->g[h->cur], h->mask2d, h->rho, h->ux, h->uy, h->uz, h->inv_scale,
+    launch_export_lattice(h->geo, h->p.storage, h->g[h->cur], h->mask2d, h->uvr, h->inv_scale,
                           fn ? sfn : nullptr, macro ? smac : nullptr, smac + n, smac + 2 * n, smac + 3 * n, h->stream);
     h->launches++;
     CK_LAUNCH();
@@ -644,9 +650,14 @@ int rbc_import_ref_cells(rbc_handle *h, const double *x, const double *y, const 
         CK(cudaMemcpy(h->Xd, t.data(), 8 * 3 * nv, cudaMemcpyHostToDevice));
     }
     if (nd) {
-        std::vector<double> t(3 * ne);
-        for (long long e = 0; e < ne; e++) { t[e] = nd[4 * e]; t[ne + e] = nd[4 * e + 1]; t[2 * ne + e] = nd[4 * e + 3]; }
+        std::vector<double> t(3 * ne), G(3 * ne);
+        for (long long e = 0; e < ne; e++) {
+            const double n00 = nd[4 * e], n01 = nd[4 * e + 1], n11 = nd[4 * e + 3], det = n00 * n11 - n01 * n01;
+            t[e] = n00; t[ne + e] = n01; t[2 * ne + e] = n11;
+            G[e] = n11 / det; G[ne + e] = -n01 / det; G[2 * ne + e] = n00 / det;
+        }
         CK(cudaMemcpy(h->nref, t.data(), 8 * 3 * ne, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(h->gref, G.data(), 8 * 3 * ne, cudaMemcpyHostToDevice));
     }
     if (volume0) CK(cudaMemcpy(h->vol0, volume0, 8 * N, cudaMemcpyHostToDevice));
     if (gx) {

@@ -5,14 +5,16 @@
 //                x fastest, z = periodic axis without BUFF planes (nzc = nz - 4
 //                planes).  Each value is f_q - w_q of the post-collision state
 //                of the previous step (pull scheme), FP32 or scaled FP16.
-//   macroscopic  rho, ux, uy, uz [z][y][x] FP32 (ux..uz = the reference's
-//                um/vm/wm with M = 1, including the half-force shift).
+//   macroscopic  uvr[z][y][x] float4 (u, v, w, rho): the reference's um/vm/wm
+//                (M = 1, with the half-force shift) and dn, interleaved so one
+//                16-byte load serves an interpolation stencil point.
 //   IB force     Fx, Fy, Fz [z][y][x] FP32; the LBM kernel zeroes what it read.
 //   wall mask    mask2d[y][x] uint32: bit 31 = fluid column, bit q = the pull
 //                source of direction q is a wall (half-way bounce-back).  The
 //                reference channel is z-invariant, so one plane serves all z.
 //   cells        X, Xd [3][nv] FP64 (cel->x/y/z and fem->xd), U, Fv [3][nv]
-//                FP32; nref [3][ne] FP64 reference metric (n00, n01, n11).
+//                FP32; nref, gref [3][ne] FP64 reference metric, contravariant
+//                (n00, n01, n11) and covariant (G11, G12, G22).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -80,7 +82,7 @@ __device__ __forceinline__ void delta4(float f, float w[4]) {
 
 struct LbmArgs {
     const void *gin; void *gout;
-    float *rho, *ux, *uy, *uz;
+    float4 *uvr;
     float *Fx, *Fy, *Fz;
     const uint32_t *mask2d;
     const float *drive;        // device scalar: P * drive factor of this step
@@ -91,12 +93,12 @@ void launch_lbm(const Geom &g, int storage, const LbmArgs &a, cudaStream_t s);
 void launch_import_lattice(const Geom &g, int storage, const double *fn_ref, void *gout,
                            const uint32_t *mask2d, float scale, cudaStream_t s);
 void launch_export_lattice(const Geom &g, int storage, const void *gin, const uint32_t *mask2d,
-                           const float *rho, const float *ux, const float *uy, const float *uz,
-                           float inv_scale, double *fn_ref, double *dn, double *un, double *vn,
-                           double *wn, cudaStream_t s);
+                           const float4 *uvr, float inv_scale, double *fn_ref, double *dn, double *un,
+                           double *vn, double *wn, cudaStream_t s);
 void launch_export_force(const Geom &g, const float *Fx, const float *Fy, const float *Fz,
                          const uint32_t *mask2d, double *out3, cudaStream_t s);
 void launch_fill_f32(float *p, long long n, float v, cudaStream_t s);
+void launch_fill_f4(float4 *p, long long n, float4 v, cudaStream_t s);
 
 struct SpreadArgs {
     const double *X; long long nv; int V, ncell;
@@ -110,7 +112,7 @@ void launch_spread(const Geom &g, const SpreadArgs &a, cudaStream_t s);
 
 struct AdvectArgs {
     double *X, *Xd; float *U;
-    const float *ux, *uy, *uz;
+    const float4 *uvr;
     long long nv;
     double dtM;                // dt * M
     int *flags;
@@ -119,7 +121,8 @@ void launch_advect(const Geom &g, const AdvectArgs &a, cudaStream_t s);
 
 struct MembraneArgs {
     const double *Xd; long long nv, ne;
-    const double *nref;
+    const double *nref;       // [3][ne] reference contravariant metric (n00, n01, n11)
+    const double *gref;       // [3][ne] reference covariant metric (G11, G12, G22)
     const int *tri, *v2e_off, *v2e;
     const int16_t *nbr;       // [6][V] local neighbour ids, -1 = none
     float *Fv;
