@@ -190,6 +190,33 @@ int rbc_get_stream(const rbc_handle *h, void **stream);
 #define RBC_KERNEL_NAMES {"step_begin", "membrane", "spread", "lbm_collide_stream", "advect", "volume"}
 int rbc_profile_steps(rbc_handle *h, int nsteps, double *kernel_ms);
 
+/* ---- without allocation -------------------------------------------------- */
+
+/* No counterpart in the reference.  Per-cell FP64 volume, area and vertex
+ * centroid (the quantities of rbc_cell_metrics) of cells whose positions the
+ * caller already holds on the device, for callers that cannot allocate device
+ * memory: this call needs no handle and calls no allocator.  Its scratch is a
+ * static device array of RBC_NOALLOC_MAX_CELLS cells (160 KB) that every GPU
+ * loading the library keeps until exit.
+ *   x        device, [3][ncell*vertex] SoA positions (x block, y block, z block)
+ *   tri      device, [element*3] local connectivity shared by all cells
+ *   LZ, zmin, zmax  periodic length and range of z (cells are unwrapped along z
+ *            about their first vertex, centroids wrapped into [zmin, zmax])
+ *   device   CUDA device ordinal, or -1 for this library's current device
+ *   stream   cudaStream_t to run on (NULL = default stream)
+ *   volume, area [ncell], centroid [3*ncell]: host outputs
+ * Synchronous.  ncell above RBC_NOALLOC_MAX_CELLS or vertex above
+ * RBC_NOALLOC_MAX_VERTEX returns RBC_ERR_ARG (text in rbc_last_error(NULL)).
+ * The first call on a device looks up the scratch array's device address and
+ * sets the kernel's shared-memory limit; make that first call before any CUDA
+ * graph capture.  All calls share the scratch array: calls that overlap on the
+ * GPU (other streams, other host threads) race and must be serialised. */
+#define RBC_NOALLOC_MAX_CELLS  4096
+#define RBC_NOALLOC_MAX_VERTEX 4096
+int rbc_cell_metrics_noalloc(const double *x, int ncell, int vertex, int element, const int *tri,
+                             double LZ, double zmin, double zmax, int device, void *stream,
+                             double *volume, double *area, double *centroid);
+
 /* Sizes of the internal lattice and of the cells. */
 int rbc_dims(const rbc_handle *h, int *nx, int *ny, int *nz_periodic, int *ncell, int *vertex, int *element);
 

@@ -15,6 +15,7 @@ RBC_OK, RBC_ERR_ARG, RBC_ERR_CUDA, RBC_ERR_UNSUPPORTED = 0, 1, 2, 3
 RBC_ERR_TOPOLOGY, RBC_ERR_NOT_CONVERGED, RBC_ERR_NONFINITE, RBC_ERR_STATE, RBC_ERR_NO_DEVICE = 4, 5, 6, 7, 8
 RBC_COMP, RBC_BUFF, RBC_WALL = 0, 1, 2
 RBC_STORE_F32, RBC_STORE_F16 = 0, 1
+RBC_NOALLOC_MAX_CELLS = 4096
 RBC_NUM_KERNELS = 6
 RBC_KERNEL_NAMES = ("step_begin", "membrane", "spread", "lbm_collide_stream", "advect", "volume")
 RBC_FLAG_VC_NOT_CONVERGED, RBC_FLAG_NONFINITE, RBC_FLAG_SPREAD_OVERFLOW, RBC_FLAG_SOLVE_RESIDUAL = 1, 2, 4, 8
@@ -66,6 +67,8 @@ _SIGS = {
     "rbc_dims": [_H, _IP, _IP, _IP, _IP, _IP, _IP],
     "rbc_get_stream": [_H, C.POINTER(C.c_void_p)],
     "rbc_profile_steps": [_H, C.c_int, _DP],
+    "rbc_cell_metrics_noalloc": [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_double, C.c_double,
+                                 C.c_double, C.c_int, C.c_void_p, _DP, _DP, _DP],
 }
 _RESTYPE = {"rbc_last_error": C.c_char_p}
 

@@ -27,6 +27,11 @@ constexpr int KERNELS_PER_STEP = 6;       // step_begin, membrane, spread, lbm, 
 
 }  // namespace
 
+namespace rbc {
+// text returned by rbc_last_error(NULL), for entry points that take no handle
+void set_last_error(const std::string &msg) { g_create_error = msg; }
+}
+
 struct rbc_handle {
     rbc_params p{};
     Geom geo{};
