@@ -3,12 +3,13 @@
 // Spreading replaces ibm_st1a/ibm_st1b/ibm_st1c (ibm.cu:27-131, 214-296 of the
 // reference).  The reference adds every vertex's 4x4x4 stencil straight into
 // the FP64 lattice with CAS-loop atomics (about 192 contended atomics per
-// vertex) and folds the BUFF planes afterwards.  Here one CTA owns one cell:
-// it finds the cell's lattice bounding box, accumulates the cell's stencils in
-// a shared-memory box with shared atomics, then adds each non-zero box node to
-// the lattice once with a global FP32 atomic (cells may overlap).  z indices
-// wrap periodically, which is what the BUFF planes plus the fold compute.
-// A cell whose box does not fit in shared memory takes a direct-atomic path.
+// vertex) and folds the BUFF planes afterwards.  Here one CTA owns one surface
+// patch of one cell: it finds the patch's lattice bounding box, accumulates
+// the patch's stencils in a shared-memory box with shared atomics, then adds
+// each non-zero box node to the lattice once with a global FP32 atomic
+// (patches and cells overlap).  z indices wrap periodically, which is what the
+// BUFF planes plus the fold compute.  A patch whose box does not fit in shared
+// memory takes a direct-atomic path.
 //
 // Interpolation + advection replaces ibm_st2a (ibm.cu:372-639): four
 // interpolations of the averaged velocity in a frozen field, classical RK4 in
@@ -19,8 +20,8 @@
 
 namespace rbc {
 
-constexpr int SPREAD_THREADS = 512;
-constexpr int SPREAD_SMEM = 100 * 1024;          // two CTAs per SM
+constexpr int SPREAD_THREADS = 256;
+constexpr int SPREAD_SMEM = 48 * 1024;           // up to four CTAs per SM
 constexpr int SPREAD_BOX_CAP = SPREAD_SMEM / (3 * (int)sizeof(float));
 
 int spread_smem_bytes() { return SPREAD_SMEM; }
@@ -31,23 +32,33 @@ __device__ __forceinline__ double unwrap_near(double l, double ref, int n) {
     return l;
 }
 
+// One CTA per (cell, surface patch).  Patches are compact groups of mesh
+// vertices (recursive coordinate bisection of the reference shape, the same
+// for every cell), so a patch's stencils fit a small box and a step has many
+// more CTAs than cells.  Box layout: x fastest, rows of bx, planes of ps >= bx*by
+// with ps = 8 (mod 32) so the four stencil planes of one vertex sit in
+// different shared-memory banks.
 __global__ void __launch_bounds__(SPREAD_THREADS)
 spread_kernel(const Geom g, const double *__restrict__ X, long long nv, int V,
+              const int *__restrict__ patch_off, const int *__restrict__ patch_vtx,
+              const int *__restrict__ patch_stride, int npatch,
               const float *__restrict__ Fv, float *__restrict__ Fx, float *__restrict__ Fy,
               float *__restrict__ Fz, const uint32_t *__restrict__ mask2d, int *__restrict__ flags)
 {
     extern __shared__ float sbox[];
     __shared__ int s_lo[3], s_hi[3];
-    const int cell = blockIdx.x, tid = threadIdx.x;
+    const int cell = blockIdx.x / npatch, patch = blockIdx.x - cell * npatch, tid = threadIdx.x;
+    const int p0 = patch_off[patch], np = patch_off[patch + 1] - p0, vstride = patch_stride[patch];
     const double *xs = X + (long long)cell * V, *ys = X + nv + (long long)cell * V, *zs = X + 2 * nv + (long long)cell * V;
     const float *fxs = Fv + (long long)cell * V, *fys = Fv + nv + (long long)cell * V, *fzs = Fv + 2 * nv + (long long)cell * V;
     const float wscale = (float)(1.0 / (g.dx * g.dx * g.dx));   // 1/(64 dx^3) of ibm.cu:108 with the 1/4s in delta4
-    const double az = lat_z(g, zs[0]);
+    const double az = lat_z(g, zs[0]);   // one anchor per cell: every patch unwraps z the same way
 
     if (tid < 3) { s_lo[tid] = INT_MAX; s_hi[tid] = INT_MIN; }
     __syncthreads();
     int lo0 = INT_MAX, lo1 = INT_MAX, lo2 = INT_MAX, hi0 = INT_MIN, hi1 = INT_MIN, hi2 = INT_MIN;
-    for (int v = tid; v < V; v += blockDim.x) {
+    for (int k = tid; k < np; k += blockDim.x) {
+        const int v = patch_vtx[p0 + k];
         const int ix = (int)floor(lat_x(g, xs[v])), iy = (int)floor(lat_y(g, ys[v]));
         const int iz = (int)floor(unwrap_near(lat_z(g, zs[v]), az, g.nzc));
         lo0 = min(lo0, ix - 1); hi0 = max(hi0, ix + 2);
@@ -59,7 +70,8 @@ spread_kernel(const Geom g, const double *__restrict__ X, long long nv, int V,
     __syncthreads();
     const int bx0 = s_lo[0], by0 = s_lo[1], bz0 = s_lo[2];
     const int bx = s_hi[0] - bx0 + 1, by = s_hi[1] - by0 + 1, bz = s_hi[2] - bz0 + 1;
-    const long long nb = (long long)bx * by * bz;
+    const long long ps = (((long long)bx * by + 31) & ~31LL) + 8;   // plane stride = 8 (mod 32)
+    const long long nb = ps * bz;
     const bool use_box = nb <= SPREAD_BOX_CAP;
     if (!use_box && tid == 0) atomicOr(flags, RBC_FLAG_SPREAD_OVERFLOW);
 
@@ -67,63 +79,68 @@ spread_kernel(const Geom g, const double *__restrict__ X, long long nv, int V,
         for (int i = tid; i < 3 * nb; i += blockDim.x) sbox[i] = 0.f;
         __syncthreads();
     }
-    // One warp per vertex: lane l owns stencil nodes k = l and l + 32 with
-    // (a, b, c) = (k & 3, (k >> 2) & 3, k >> 4), so the 32 atomics of one warp
-    // instruction go to 32 different box nodes (lanes working on neighbouring
-    // vertices would collide on the same nodes).
-    const int lane = tid & 31, nwarp = blockDim.x >> 5;
-    for (int v = tid >> 5; v < V; v += nwarp) {
+    // Four tasks per vertex: task i handles stencil plane c = i & 3 of the
+    // patch's vertex (i >> 2) * vstride mod np.  vstride is coprime with np, so
+    // the lanes of a warp hold vertices spread over the patch and rarely add
+    // to the same box node in one instruction.  The fluid test is applied once
+    // per node at the flush (wall columns accumulate in shared memory and are
+    // dropped there).
+    for (int i = tid; i < 4 * np; i += blockDim.x) {
+        const int c = i & 3;
+        const int v = patch_vtx[p0 + (int)(((long long)(i >> 2) * vstride) % np)];
         const double lx = lat_x(g, xs[v]), ly = lat_y(g, ys[v]);
         const double lzr = lat_z(g, zs[v]);
         const double lz = unwrap_near(lzr, az, g.nzc);
         const double flx = floor(lx), fly = floor(ly), flz = floor(lz);
-        // lanes 0..2 evaluate sin/cos of the three fractions, the warp shares them
-        float sv = 0.f, cv = 0.f;
-        if (lane < 3) sincospif(0.5f * (float)(lane == 0 ? lx - flx : (lane == 1 ? ly - fly : lz - flz)), &sv, &cv);
-        const int ix0 = (int)flx - 1, iy0 = (int)fly - 1, iz0 = (int)flz - 1;
-        const int izr0 = iz0 - (int)lrint(lz - lzr);   // stencil start in the vertex's own (unshifted) frame
-        const float f0 = fxs[v] * wscale, f1 = fys[v] * wscale, f2 = fzs[v] * wscale;
+        const int iz = (int)flz - 1 + c;
+        // the reference's lattice ends two BUFF planes beyond the periodic
+        // range; stencil nodes past them are skipped (ibm.cu:107-110)
+        const int izr = iz - (int)lrint(lz - lzr);
+        if (izr < -2 || izr >= g.nzc + 2) continue;
+        float wx[4], wy[4], wz[4];
+        delta4((float)(lx - flx), wx); delta4((float)(ly - fly), wy); delta4((float)(lz - flz), wz);
+        const float wzc = c == 0 ? wz[0] : c == 1 ? wz[1] : c == 2 ? wz[2] : wz[3];
+        const int ix0 = (int)flx - 1, iy0 = (int)fly - 1;
+        const float sc = wscale * wzc;
+        const float f0 = fxs[v] * sc, f1 = fys[v] * sc, f2 = fzs[v] * sc;
+        const long long zoff = ps * (iz - bz0);
 #pragma unroll
-        for (int half = 0; half < 2; half++) {
-            const int k = lane + 32 * half;
-            const int ka = k & 3, kb = (k >> 2) & 3, kc = k >> 4;
-            // phi at offset 0..3 = (1 - s, 1 + c, 1 + s, 1 - c) / 4 (delta4)
-            const float sx = __shfl_sync(0xffffffffu, sv, 0), cx = __shfl_sync(0xffffffffu, cv, 0);
-            const float sy = __shfl_sync(0xffffffffu, sv, 1), cy = __shfl_sync(0xffffffffu, cv, 1);
-            const float sz = __shfl_sync(0xffffffffu, sv, 2), cz = __shfl_sync(0xffffffffu, cv, 2);
-            const float wa = 0.25f * (ka == 0 ? 1.f - sx : ka == 1 ? 1.f + cx : ka == 2 ? 1.f + sx : 1.f - cx);
-            const float wb = 0.25f * (kb == 0 ? 1.f - sy : kb == 1 ? 1.f + cy : kb == 2 ? 1.f + sy : 1.f - cy);
-            const float wc = 0.25f * (kc == 0 ? 1.f - sz : kc == 1 ? 1.f + cz : kc == 2 ? 1.f + sz : 1.f - cz);
-            const int gx = ix0 + ka, gy = iy0 + kb;
-            // the reference's lattice ends two BUFF planes beyond the periodic
-            // range; stencil nodes past them are skipped (ibm.cu:107-110)
-            if (izr0 + kc < -2 || izr0 + kc >= g.nzc + 2) continue;
-            if (gx < 0 || gx >= g.nx || gy < 0 || gy >= g.ny) continue;
-            if (!(__ldg(&mask2d[gx + g.nx * gy]) & MASK_FLUID)) continue;
-            const float w = wa * wb * wc;
-            if (use_box) {
-                const long long li = (gx - bx0) + (long long)bx * ((gy - by0) + (long long)by * (iz0 + kc - bz0));
-                atomicAdd(&sbox[li], w * f0);
-                atomicAdd(&sbox[nb + li], w * f1);
-                atomicAdd(&sbox[2 * nb + li], w * f2);
-            } else {
-                const long long gi = (long long)wrap_z(iz0 + kc, g.nzc) * g.plane + gx + (long long)g.nx * gy;
-                atomicAdd(&Fx[gi], w * f0);
-                atomicAdd(&Fy[gi], w * f1);
-                atomicAdd(&Fz[gi], w * f2);
+        for (int b = 0; b < 4; b++) {
+            const int gy = iy0 + b;
+            if (gy < 0 || gy >= g.ny) continue;
+            const float wyb = wy[b];
+#pragma unroll
+            for (int a = 0; a < 4; a++) {
+                const int gx = ix0 + a;
+                if (gx < 0 || gx >= g.nx) continue;
+                const float w = wx[a] * wyb;
+                if (use_box) {
+                    const long long li = (gx - bx0) + (long long)bx * (gy - by0) + zoff;
+                    atomicAdd(&sbox[li], w * f0);
+                    atomicAdd(&sbox[nb + li], w * f1);
+                    atomicAdd(&sbox[2 * nb + li], w * f2);
+                } else if (__ldg(&mask2d[gx + g.nx * gy]) & MASK_FLUID) {
+                    const long long gi = (long long)wrap_z(iz, g.nzc) * g.plane + gx + (long long)g.nx * gy;
+                    atomicAdd(&Fx[gi], w * f0);
+                    atomicAdd(&Fy[gi], w * f1);
+                    atomicAdd(&Fz[gi], w * f2);
+                }
             }
         }
     }
     if (!use_box) return;
     __syncthreads();
+    const long long rowplane = (long long)bx * by;
     for (long long li = tid; li < nb; li += blockDim.x) {
+        const long long lz = li / ps, r = li - lz * ps;
+        if (r >= rowplane) continue;   // plane padding
         const float a = sbox[li], b = sbox[nb + li], c = sbox[2 * nb + li];
         if (a == 0.f && b == 0.f && c == 0.f) continue;
-        const int lx = (int)(li % bx), rest = (int)(li / bx);
-        const int ly = rest % by, lz = rest / by;
+        const int ly = (int)(r / bx), lx = (int)(r - (long long)ly * bx);
         const int gx = bx0 + lx, gy = by0 + ly;
         if (gx < 0 || gx >= g.nx || gy < 0 || gy >= g.ny) continue;   // never written; kept as a guard
-        const long long gi = (long long)wrap_z(bz0 + lz, g.nzc) * g.plane + gx + (long long)g.nx * gy;
+        if (!(__ldg(&mask2d[gx + g.nx * gy]) & MASK_FLUID)) continue;   // wall column: the LBM never reads it
+        const long long gi = (long long)wrap_z(bz0 + (int)lz, g.nzc) * g.plane + gx + (long long)g.nx * gy;
         if (a != 0.f) atomicAdd(&Fx[gi], a);
         if (b != 0.f) atomicAdd(&Fy[gi], b);
         if (c != 0.f) atomicAdd(&Fz[gi], c);
@@ -138,40 +155,60 @@ cudaError_t spread_setup()
 void launch_spread(const Geom &g, const SpreadArgs &a, cudaStream_t s)
 {
     if (a.ncell <= 0) return;
-    spread_kernel<<<a.ncell, SPREAD_THREADS, SPREAD_SMEM, s>>>(g, a.X, a.nv, a.V, a.Fv, a.Fx, a.Fy, a.Fz,
-                                                              a.mask2d, a.flags);
+    spread_kernel<<<a.ncell * a.npatch, SPREAD_THREADS, SPREAD_SMEM, s>>>(
+        g, a.X, a.nv, a.V, a.patch_off, a.patch_vtx, a.patch_stride, a.npatch, a.Fv, a.Fx, a.Fy, a.Fz, a.mask2d,
+        a.flags);
 }
 
 // ---- interpolation + RK4 advection ---------------------------------------
 
-// Four lanes per vertex: lane c of the group gathers stencil plane c (16 nodes,
-// one float4 (u, v, w, rho) each); the group sums its partial velocities with
-// two butterfly shuffles, so every lane holds the interpolated velocity.
-__device__ __forceinline__ void interp4(const Geom &g, const float4 *__restrict__ uvr, double px, double py,
-                                        double pz, int c, float &ur, float &vr, float &wr)
+// Four lanes per vertex: lane c of the group owns stencil plane c (16 nodes).
+// The stage-1 stencil is loaded once into registers (u, v, w of 16 nodes) and
+// reused by the later RK stages, whose positions move by u dt / 2 ~ 1e-3 and
+// almost never leave the stage-1 lattice cell; a stage that does re-gathers.
+// The group sums its partial velocities with two butterfly shuffles.
+struct Plane16 {
+    float u[16], v[16], w[16];
+};
+
+__device__ __forceinline__ void gather_plane(const Geom &g, const float4 *__restrict__ uvr, int ix0, int iy0, int iz,
+                                             Plane16 &P)
+{
+    const bool zin = iz >= -2 && iz < g.nzc + 2;   // beyond the BUFF planes (ibm.cu:453-455)
+    const long long zb = (long long)wrap_z(iz, g.nzc) * g.plane;
+#pragma unroll
+    for (int b = 0; b < 4; b++) {
+        const int gy = iy0 + b;
+#pragma unroll
+        for (int a = 0; a < 4; a++) {
+            const int gx = ix0 + a;
+            float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (zin && gy >= 0 && gy < g.ny && gx >= 0 && gx < g.nx) q = __ldg(&uvr[zb + gx + (long long)g.nx * gy]);
+            P.u[4 * b + a] = q.x; P.v[4 * b + a] = q.y; P.w[4 * b + a] = q.z;
+        }
+    }
+}
+
+__device__ __forceinline__ void lattice_cell(const Geom &g, double px, double py, double pz, int &ix0, int &iy0,
+                                             int &iz0, float &fx, float &fy, float &fz)
 {
     const double lx = lat_x(g, px), ly = lat_y(g, py), lz = lat_z(g, pz);
     const double flx = floor(lx), fly = floor(ly), flz = floor(lz);
-    float wx[4], wy[4], wz[4];
-    delta4((float)(lx - flx), wx); delta4((float)(ly - fly), wy); delta4((float)(lz - flz), wz);
-    const int ix0 = (int)flx - 1, iy0 = (int)fly - 1, iz = (int)flz - 1 + c;
+    ix0 = (int)flx - 1; iy0 = (int)fly - 1; iz0 = (int)flz - 1;
+    fx = (float)(lx - flx); fy = (float)(ly - fly); fz = (float)(lz - flz);
+}
+
+__device__ __forceinline__ void contract(const Plane16 &P, const float wx[4], const float wy[4], float wzc,
+                                         float &ur, float &vr, float &wr)
+{
     float su = 0.f, sv = 0.f, sw = 0.f;
-    if (iz >= -2 && iz < g.nzc + 2) {   // beyond the BUFF planes (ibm.cu:453-455)
-        const long long zb = (long long)wrap_z(iz, g.nzc) * g.plane;
-        const float wzc = c == 0 ? wz[0] : c == 1 ? wz[1] : c == 2 ? wz[2] : wz[3];
 #pragma unroll
-        for (int b = 0; b < 4; b++) {
-            const int gy = iy0 + b;
-            if (gy < 0 || gy >= g.ny) continue;
-            const float wyz = wy[b] * wzc;
+    for (int b = 0; b < 4; b++) {
+        const float wyz = wy[b] * wzc;
 #pragma unroll
-            for (int a = 0; a < 4; a++) {
-                const int gx = ix0 + a;
-                if (gx < 0 || gx >= g.nx) continue;
-                const float4 q = __ldg(&uvr[zb + gx + (long long)g.nx * gy]);
-                const float w = wx[a] * wyz;
-                su += w * q.x; sv += w * q.y; sw += w * q.z;
-            }
+        for (int a = 0; a < 4; a++) {
+            const float w = wx[a] * wyz;
+            su += w * P.u[4 * b + a]; sv += w * P.v[4 * b + a]; sw += w * P.w[4 * b + a];
         }
     }
 #pragma unroll
@@ -185,7 +222,7 @@ __device__ __forceinline__ void interp4(const Geom &g, const float4 *__restrict_
 
 constexpr int ADVECT_THREADS = 256;
 
-__global__ void __launch_bounds__(ADVECT_THREADS, 4)
+__global__ void __launch_bounds__(ADVECT_THREADS)
 advect_kernel(const Geom g, double *__restrict__ X, double *__restrict__ Xd, float *__restrict__ U,
               const float4 *__restrict__ uvr, long long nv, double dtM, int *__restrict__ flags)
 {
@@ -194,15 +231,33 @@ advect_kernel(const Geom g, double *__restrict__ X, double *__restrict__ Xd, flo
     const bool live = (t >> 2) < nv;
     const long long j = live ? (t >> 2) : nv - 1;   // idle lanes shadow the last vertex for the shuffles
     const double xn = X[j], yn = X[nv + j], zn = X[2 * nv + j];
-    float u1, v1, w1, u2, v2, w2, u3, v3, w3, u4, v4, w4;
-    interp4(g, uvr, xn, yn, zn, c, u1, v1, w1);
-    interp4(g, uvr, xn + u1 * dtM * 0.5, yn + v1 * dtM * 0.5, zn + w1 * dtM * 0.5, c, u2, v2, w2);
-    interp4(g, uvr, xn + u2 * dtM * 0.5, yn + v2 * dtM * 0.5, zn + w2 * dtM * 0.5, c, u3, v3, w3);
-    interp4(g, uvr, xn + u3 * dtM, yn + v3 * dtM, zn + w3 * dtM, c, u4, v4, w4);
+    Plane16 P;
+    int bx, by, bz;
+    float fx, fy, fz, wx[4], wy[4], wz[4];
+    lattice_cell(g, xn, yn, zn, bx, by, bz, fx, fy, fz);
+    gather_plane(g, uvr, bx, by, bz + c, P);
+    float us[4], vs[4], ws[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        double px = xn, py = yn, pz = zn;
+        if (k > 0) {
+            const double h = (k < 3 ? 0.5 : 1.0) * dtM;   // ibm.cu:474-498
+            px += us[k - 1] * h; py += vs[k - 1] * h; pz += ws[k - 1] * h;
+            int cx, cy, cz;
+            lattice_cell(g, px, py, pz, cx, cy, cz, fx, fy, fz);
+            if (cx != bx || cy != by || cz != bz) {   // uniform across the 4 lanes of the vertex
+                bx = cx; by = cy; bz = cz;
+                gather_plane(g, uvr, bx, by, bz + c, P);
+            }
+        }
+        delta4(fx, wx); delta4(fy, wy); delta4(fz, wz);
+        const float wzc = c == 0 ? wz[0] : c == 1 ? wz[1] : c == 2 ? wz[2] : wz[3];
+        contract(P, wx, wy, wzc, us[k], vs[k], ws[k]);
+    }
     if (!live || c != 0) return;
-    const double um = ((double)u1 + 2.0 * u2 + 2.0 * u3 + u4) / 6.0;
-    const double vm = ((double)v1 + 2.0 * v2 + 2.0 * v3 + v4) / 6.0;
-    const double wm = ((double)w1 + 2.0 * w2 + 2.0 * w3 + w4) / 6.0;
+    const double um = ((double)us[0] + 2.0 * us[1] + 2.0 * us[2] + us[3]) / 6.0;
+    const double vm = ((double)vs[0] + 2.0 * vs[1] + 2.0 * vs[2] + vs[3]) / 6.0;
+    const double wm = ((double)ws[0] + 2.0 * ws[1] + 2.0 * ws[2] + ws[3]) / 6.0;
     double xr = xn + um * dtM, yr = yn + vm * dtM, zr = zn + wm * dtM;
     if (xr < g.xmin) xr += g.LX;   // ibm.cu:629-632
     if (xr > g.xmax) xr -= g.LX;

@@ -35,7 +35,7 @@ constexpr int LBM_THREADS = 256;
 // One thread per internal node (x fastest).  Per fluid node: 19 pulled loads,
 // 12 B of IB force, 19 stores, 16 B of rho/u.
 template <int STORE>
-__global__ void __launch_bounds__(LBM_THREADS)
+__global__ void __launch_bounds__(LBM_THREADS, 5)
 lbm_collide_stream(const typename Store<STORE>::T *__restrict__ gin, typename Store<STORE>::T *__restrict__ gout,
                    float4 *__restrict__ uvr,
                    float *__restrict__ Fx, float *__restrict__ Fy, float *__restrict__ Fz,

@@ -109,12 +109,17 @@ membrane_kernel(const MembraneArgs a)
             const double g11d = e1x * e1x + e1y * e1y + e1z * e1z;
             const double g12d = e1x * e2x + e1y * e2y + e1z * e2z;
             const double g22d = e2x * e2x + e2y * e2y + e2z * e2z;
-            const double G11 = __ldg(&a.gref[eb + e]), G12 = __ldg(&a.gref[ne + eb + e]), G22 = __ldg(&a.gref[2 * ne + eb + e]);
-            const double n00d = __ldg(&a.nref[eb + e]), n01d = __ldg(&a.nref[ne + eb + e]), n11d = __ldg(&a.nref[2 * ne + eb + e]);
+            // reference metric: covariant G (one aligned 32-byte record per element) and
+            // its inverse n, formed as set_contravariant does (init2.cu:241-249)
+            const double2 *gp = reinterpret_cast<const double2 *>(a.gref + eb + e);
+            const double2 Ga = __ldg(gp), Gb = __ldg(gp + 1);
+            const double G11 = Ga.x, G12 = Ga.y, G22 = Gb.x;
+            const double idG = 1.0 / (G11 * G22 - G12 * G12);
+            const double n00d = G22 * idG, n01d = -G12 * idG, n11d = G11 * idG;
             const Real d11 = (Real)(g11d - G11), d12 = (Real)(g12d - G12), d22 = (Real)(g22d - G22);
             const Real g11 = (Real)g11d, g12 = (Real)g12d, g22 = (Real)g22d;
             const Real n00 = (Real)n00d, n01 = (Real)n01d, n11 = (Real)n11d;
-            const Real detn = (Real)(n00d * n11d - n01d * n01d);
+            const Real detn = (Real)idG;
             const Real det = g11 * g22 - g12 * g12;
             const Real idet = (Real)1 / det;
             // invariants (stress.cu:90-93) from the metric difference

@@ -11,7 +11,9 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <algorithm>
 #include <new>
+#include <numeric>
 #include <string>
 #include <vector>
 
@@ -46,7 +48,8 @@ struct rbc_handle {
     float *Fx = nullptr, *Fy = nullptr, *Fz = nullptr;
     uint32_t *mask2d = nullptr;
     // cells
-    double *X = nullptr, *Xd = nullptr, *nref = nullptr, *gref = nullptr;
+    double *X = nullptr, *Xd = nullptr;
+    double4 *gref = nullptr;
     float *U = nullptr, *Fv = nullptr;
     int *tri = nullptr, *v2e_off = nullptr, *v2e = nullptr;
     int16_t *nbr = nullptr;
@@ -64,6 +67,8 @@ struct rbc_handle {
     float scale = 1.0f, inv_scale = 1.0f;
     std::string err;
     int device = 0;
+    int *patch_off = nullptr, *patch_vtx = nullptr, *patch_stride = nullptr;
+    int npatch = 1;
 
     int *d_iter() { return d_int; }
     int *d_flags() { return d_int + 1; }
@@ -176,14 +181,12 @@ int build_topology(rbc_handle *h, const int *tri, std::vector<int> &off, std::ve
     return RBC_OK;
 }
 
-// set_contravariant (init2.cu:206-255) on the AoS reference shape; outputs
-// [3][ne]: the contravariant metric n and the covariant metric G = n^-1
-void reference_metric(const rbc_handle *h, const int *tri, const double *xr, std::vector<double> &nref,
-                      std::vector<double> &gref)
+// The reference metric of set_contravariant (init2.cu:206-255) on the AoS
+// reference shape, kept in covariant form G [ne] (the kernel forms n = G^-1)
+void reference_metric(const rbc_handle *h, const int *tri, const double *xr, std::vector<double4> &gref)
 {
     const long long ne = h->ne;
-    nref.assign(3 * ne, 0.0);
-    gref.assign(3 * ne, 0.0);
+    gref.assign(ne, make_double4(0, 0, 0, 0));
     for (int c = 0; c < h->ncell; c++)
         for (int e = 0; e < h->E; e++) {
             const long long a = (long long)c * h->V + tri[3 * e], b = (long long)c * h->V + tri[3 * e + 1],
@@ -193,14 +196,8 @@ void reference_metric(const rbc_handle *h, const int *tri, const double *xr, std
             const double lv1 = v1[0] * v1[0] + v1[1] * v1[1] + v1[2] * v1[2];
             const double lv2 = v2[0] * v2[0] + v2[1] * v2[1] + v2[2] * v2[2];
             const double inv12 = v1[0] * v2[0] + v1[1] * v2[1] + v1[2] * v2[2];
-            const double dv12 = lv1 * lv2 - inv12 * inv12;
             const long long id = (long long)c * h->E + e;
-            nref[id] = lv2 / dv12;
-            nref[ne + id] = -inv12 / dv12;
-            nref[2 * ne + id] = lv1 / dv12;
-            gref[id] = lv1;
-            gref[ne + id] = inv12;
-            gref[2 * ne + id] = lv2;
+            gref[id] = make_double4(lv1, inv12, lv2, 0.0);
         }
 }
 
@@ -232,6 +229,46 @@ void initial_volume(const rbc_handle *h, const int *tri, const double *xr, std::
         for (int k = 0; k < 3; k++) s[k] /= (double)V;
         if (s[2] < h->p.zmin) s[2] += h->p.LZ; else if (s[2] > h->p.zmax) s[2] -= h->p.LZ;
         gx[c] = s[0]; gx[N + c] = s[1]; gx[2 * N + c] = s[2];
+    }
+}
+
+// Surface patches for the spread kernel: recursive coordinate bisection of the
+// first cell's initial vertex positions (split along the widest axis at the
+// median until a patch has at most 512 vertices).  The same vertex sets serve
+// every cell, since all cells share the mesh and a compact patch of the surface
+// stays compact as the membrane moves.  Also a lane stride per patch, near
+// 0.618 of its size and coprime with it, that scatters neighbours across lanes.
+void surface_patches(int V, const double *xr, std::vector<int> &off, std::vector<int> &vtx, std::vector<int> &stride)
+{
+    constexpr int kMaxPatch = 512;
+    vtx.resize(V);
+    for (int i = 0; i < V; i++) vtx[i] = i;
+    off.assign(1, 0);
+    std::vector<std::pair<int, int>> stack{{0, V}};
+    std::vector<std::pair<int, int>> leaves;
+    while (!stack.empty()) {
+        auto [b, e] = stack.back();
+        stack.pop_back();
+        if (e - b <= kMaxPatch) { leaves.push_back({b, e}); continue; }
+        double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+        for (int k = b; k < e; k++)
+            for (int d = 0; d < 3; d++) { lo[d] = std::min(lo[d], xr[3 * vtx[k] + d]); hi[d] = std::max(hi[d], xr[3 * vtx[k] + d]); }
+        int ax = 0;
+        for (int d = 1; d < 3; d++) if (hi[d] - lo[d] > hi[ax] - lo[ax]) ax = d;
+        const int mid = b + (e - b) / 2;
+        std::nth_element(vtx.begin() + b, vtx.begin() + mid, vtx.begin() + e,
+                         [&](int i, int j) { return xr[3 * i + ax] < xr[3 * j + ax]; });
+        stack.push_back({mid, e});
+        stack.push_back({b, mid});
+    }
+    std::sort(leaves.begin(), leaves.end());
+    stride.clear();
+    for (auto [b, e] : leaves) {
+        off.push_back(e);
+        const int n = e - b;
+        int s = std::max(1, (int)(0.6180339887 * n)) | 1;
+        while (std::gcd(s, n) != 1) s += 2;
+        stride.push_back(s);
     }
 }
 
@@ -295,7 +332,7 @@ void free_all(rbc_handle *h)
     if (!h) return;
     for (cudaGraphExec_t g : h->graph) if (g) cudaGraphExecDestroy(g);
     void *ptrs[] = {h->g[0], h->g[1], h->uvr, h->Fx, h->Fy, h->Fz, h->mask2d,
-                    h->X, h->Xd, h->nref, h->gref, h->U, h->Fv, h->tri, h->v2e_off, h->v2e, h->nbr, h->vol0, h->gx,
+                    h->X, h->Xd, h->gref, h->U, h->Fv, h->tri, h->v2e_off, h->v2e, h->nbr, h->patch_off, h->patch_vtx, h->patch_stride, h->vol0, h->gx,
                     h->vol_out, h->area_out, h->cen_out, h->d_int, h->d_drive, h->staging};
     for (void *q : ptrs) if (q) cudaFree(q);
     if (h->stream) cudaStreamDestroy(h->stream);
@@ -307,7 +344,7 @@ int launch_stress(rbc_handle *h)
 {
     if (h->ncell == 0) return RBC_OK;
     MembraneArgs a{};
-    a.Xd = h->Xd; a.nv = h->nv; a.ne = h->ne; a.nref = h->nref; a.gref = h->gref;
+    a.Xd = h->Xd; a.nv = h->nv; a.ne = h->ne; a.gref = h->gref;
     a.tri = h->tri; a.v2e_off = h->v2e_off; a.v2e = h->v2e; a.nbr = h->nbr; a.Fv = h->Fv;
     a.V = h->V; a.E = h->E; a.ncell = h->ncell;
     a.C = h->p.C; a.rgs = h->p.rgs; a.law = h->p.law; a.LX = h->p.LX; a.LZ = h->p.LZ;
@@ -324,6 +361,8 @@ int launch_spread_stage(rbc_handle *h)
     if (h->ncell == 0) return RBC_OK;
     SpreadArgs a{};
     a.X = h->X; a.nv = h->nv; a.V = h->V; a.ncell = h->ncell; a.Fv = h->Fv;
+    a.patch_off = h->patch_off; a.patch_vtx = h->patch_vtx; a.patch_stride = h->patch_stride;
+    a.npatch = h->npatch;
     a.Fx = h->Fx; a.Fy = h->Fy; a.Fz = h->Fz; a.mask2d = h->mask2d; a.flags = h->d_flags();
     launch_spread(h->geo, a, h->stream);
     h->launches++;
@@ -467,6 +506,7 @@ int rbc_create(const rbc_params *p, const rbc_mesh *mesh, const int *bc, rbc_han
     g.nx = p->nx; g.ny = p->ny; g.nzr = p->nz; g.nzc = p->nz - 4;
     g.plane = (long long)p->nx * p->ny; g.nint = g.plane * g.nzc;
     g.dx = p->dx;
+    g.inv_dx = 1.0 / p->dx;
     g.xoff = (double)(p->nx - 1) * p->dx / 2.0;
     g.yoff = (double)(p->ny - 1) * p->dx / 2.0;
     g.zoff = (double)(p->nz - 1) * p->dx / 2.0;
@@ -484,12 +524,16 @@ int rbc_create(const rbc_params *p, const rbc_mesh *mesh, const int *bc, rbc_han
     // host-side setup first, so argument and mesh errors are reported without a GPU
     std::vector<int> off, packed;
     std::vector<int16_t> nbr6;
-    std::vector<double> nref, gref, vol0, gx, xs;
+    std::vector<double> vol0, gx, xs;
+    std::vector<double4> gref;
+    std::vector<int> poff, pvtx, pstride;
     if (cells) {
         h->ncell = mesh->ncell; h->V = mesh->vertex; h->E = mesh->element;
         h->nv = (long long)h->ncell * h->V; h->ne = (long long)h->ncell * h->E;
         TRY(build_topology(h, mesh->tri, off, packed, nbr6));
-        reference_metric(h, mesh->tri, mesh->xr, nref, gref);
+        surface_patches(h->V, mesh->xr, poff, pvtx, pstride);
+        h->npatch = (int)poff.size() - 1;
+        reference_metric(h, mesh->tri, mesh->xr, gref);
         initial_volume(h, mesh->tri, mesh->xr, vol0, gx);
         xs.resize(3 * h->nv);
         for (long long j = 0; j < h->nv; j++)
@@ -539,22 +583,25 @@ int rbc_create(const rbc_params *p, const rbc_mesh *mesh, const int *bc, rbc_han
     launch_fill_f4(h->uvr, g.nint, make_float4(0.f, 0.f, 0.f, 1.f), h->stream);
 
     if (cells) {
-        TRY(dalloc(h, &h->X, 3 * h->nv)); TRY(dalloc(h, &h->Xd, 3 * h->nv)); TRY(dalloc(h, &h->nref, 3 * h->ne));
-        TRY(dalloc(h, &h->gref, 3 * h->ne));
+        TRY(dalloc(h, &h->X, 3 * h->nv)); TRY(dalloc(h, &h->Xd, 3 * h->nv)); TRY(dalloc(h, &h->gref, h->ne));
         TRY(dalloc(h, &h->U, 3 * h->nv)); TRY(dalloc(h, &h->Fv, 3 * h->nv));
         TRY(dalloc(h, &h->tri, 3 * h->E)); TRY(dalloc(h, &h->v2e_off, h->V + 1)); TRY(dalloc(h, &h->v2e, packed.size()));
         TRY(dalloc(h, &h->nbr, 6 * h->V));
+        TRY(dalloc(h, &h->patch_off, poff.size())); TRY(dalloc(h, &h->patch_vtx, pvtx.size()));
+        TRY(dalloc(h, &h->patch_stride, pstride.size()));
         TRY(dalloc(h, &h->vol0, h->ncell)); TRY(dalloc(h, &h->gx, 3 * h->ncell));
         TRY(dalloc(h, &h->vol_out, h->ncell)); TRY(dalloc(h, &h->area_out, h->ncell)); TRY(dalloc(h, &h->cen_out, 3 * h->ncell));
         if (cudaMemcpy(h->X, xs.data(), 8 * 3 * h->nv, cudaMemcpyHostToDevice) != cudaSuccess ||
             cudaMemcpy(h->Xd, xs.data(), 8 * 3 * h->nv, cudaMemcpyHostToDevice) != cudaSuccess ||
-            cudaMemcpy(h->nref, nref.data(), 8 * 3 * h->ne, cudaMemcpyHostToDevice) != cudaSuccess ||
-            cudaMemcpy(h->gref, gref.data(), 8 * 3 * h->ne, cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(h->gref, gref.data(), sizeof(double4) * h->ne, cudaMemcpyHostToDevice) != cudaSuccess ||
             cudaMemset(h->U, 0, 4 * 3 * h->nv) != cudaSuccess || cudaMemset(h->Fv, 0, 4 * 3 * h->nv) != cudaSuccess ||
             cudaMemcpy(h->tri, mesh->tri, 4 * 3 * h->E, cudaMemcpyHostToDevice) != cudaSuccess ||
             cudaMemcpy(h->v2e_off, off.data(), 4 * (h->V + 1), cudaMemcpyHostToDevice) != cudaSuccess ||
             cudaMemcpy(h->v2e, packed.data(), 4 * packed.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
             cudaMemcpy(h->nbr, nbr6.data(), 2 * 6 * h->V, cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(h->patch_off, poff.data(), 4 * poff.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(h->patch_vtx, pvtx.data(), 4 * pvtx.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(h->patch_stride, pstride.data(), 4 * pstride.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
             cudaMemcpy(h->vol0, vol0.data(), 8 * h->ncell, cudaMemcpyHostToDevice) != cudaSuccess ||
             cudaMemcpy(h->gx, gx.data(), 8 * 3 * h->ncell, cudaMemcpyHostToDevice) != cudaSuccess) {
             h->err = "cell upload failed";
@@ -655,14 +702,12 @@ int rbc_import_ref_cells(rbc_handle *h, const double *x, const double *y, const 
         CK(cudaMemcpy(h->Xd, t.data(), 8 * 3 * nv, cudaMemcpyHostToDevice));
     }
     if (nd) {
-        std::vector<double> t(3 * ne), G(3 * ne);
+        std::vector<double4> G(ne);
         for (long long e = 0; e < ne; e++) {
             const double n00 = nd[4 * e], n01 = nd[4 * e + 1], n11 = nd[4 * e + 3], det = n00 * n11 - n01 * n01;
-            t[e] = n00; t[ne + e] = n01; t[2 * ne + e] = n11;
-            G[e] = n11 / det; G[ne + e] = -n01 / det; G[2 * ne + e] = n00 / det;
+            G[e] = make_double4(n11 / det, -n01 / det, n00 / det, 0.0);
         }
-        CK(cudaMemcpy(h->nref, t.data(), 8 * 3 * ne, cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(h->gref, G.data(), 8 * 3 * ne, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(h->gref, G.data(), sizeof(double4) * ne, cudaMemcpyHostToDevice));
     }
     if (volume0) CK(cudaMemcpy(h->vol0, volume0, 8 * N, cudaMemcpyHostToDevice));
     if (gx) {

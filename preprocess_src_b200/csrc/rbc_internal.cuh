@@ -13,8 +13,8 @@
 //                source of direction q is a wall (half-way bounce-back).  The
 //                reference channel is z-invariant, so one plane serves all z.
 //   cells        X, Xd [3][nv] FP64 (cel->x/y/z and fem->xd), U, Fv [3][nv]
-//                FP32; nref, gref [3][ne] FP64 reference metric, contravariant
-//                (n00, n01, n11) and covariant (G11, G12, G22).
+//                FP32; gref [ne] double4 reference covariant metric
+//                (G11, G12, G22, -); the contravariant metric n = G^-1.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -50,15 +50,16 @@ __host__ __device__ constexpr double wqd(int q) { return q == 0 ? (1.0 / 3.0) : 
 struct Geom {
     int nx, ny, nzc, nzr;      // internal dims; nzr = reference nz (nzc + 4)
     long long plane, nint;     // nx*ny, nx*ny*nzc
-    double dx;
+    double dx, inv_dx;
     double xoff, yoff, zoff;   // lattice coordinate = (pos + off)/dx (ibm.cu:100-102)
     double LX, LZ, xmin, xmax, zmin, zmax;
 };
 
 // Lattice coordinates of a position in the internal frame (z without BUFF).
-__device__ __forceinline__ double lat_x(const Geom &g, double x) { return (x + g.xoff) / g.dx; }
-__device__ __forceinline__ double lat_y(const Geom &g, double y) { return (y + g.yoff) / g.dx; }
-__device__ __forceinline__ double lat_z(const Geom &g, double z) { return (z + g.zoff) / g.dx - 2.0; }
+// (multiplication by 1/dx; exact for the unit lattice spacing the workloads use)
+__device__ __forceinline__ double lat_x(const Geom &g, double x) { return (x + g.xoff) * g.inv_dx; }
+__device__ __forceinline__ double lat_y(const Geom &g, double y) { return (y + g.yoff) * g.inv_dx; }
+__device__ __forceinline__ double lat_z(const Geom &g, double z) { return (z + g.zoff) * g.inv_dx - 2.0; }
 
 __device__ __forceinline__ int wrap_z(int iz, int nzc) {
     iz %= nzc;
@@ -102,6 +103,8 @@ void launch_fill_f4(float4 *p, long long n, float4 v, cudaStream_t s);
 
 struct SpreadArgs {
     const double *X; long long nv; int V, ncell;
+    const int *patch_off, *patch_vtx, *patch_stride;   // surface patches of the shared mesh
+    int npatch;
     const float *Fv;
     float *Fx, *Fy, *Fz;
     const uint32_t *mask2d;
@@ -121,8 +124,7 @@ void launch_advect(const Geom &g, const AdvectArgs &a, cudaStream_t s);
 
 struct MembraneArgs {
     const double *Xd; long long nv, ne;
-    const double *nref;       // [3][ne] reference contravariant metric (n00, n01, n11)
-    const double *gref;       // [3][ne] reference covariant metric (G11, G12, G22)
+    const double4 *gref;      // [ne] reference covariant metric (G11, G12, G22, unused)
     const int *tri, *v2e_off, *v2e;
     const int16_t *nbr;       // [6][V] local neighbour ids, -1 = none
     float *Fv;
