@@ -14,6 +14,7 @@
 // Interpolation + advection replaces ibm_st2a (ibm.cu:372-639): four
 // interpolations of the averaged velocity in a frozen field, classical RK4 in
 // FP64 positions, periodic wrap in x and z as the reference does.
+#include <cfloat>
 #include "rbc_internal.cuh"
 
 #include <climits>
@@ -22,7 +23,7 @@ namespace rbc {
 
 constexpr int SPREAD_THREADS = 256;
 constexpr int SPREAD_SMEM = 48 * 1024;           // up to four CTAs per SM
-constexpr int SPREAD_BOX_CAP = SPREAD_SMEM / (3 * (int)sizeof(float));
+constexpr int SPREAD_BOX_CAP = SPREAD_SMEM / (3 * (int)sizeof(unsigned));
 
 int spread_smem_bytes() { return SPREAD_SMEM; }
 
@@ -45,8 +46,9 @@ spread_kernel(const Geom g, const double *__restrict__ X, long long nv, int V,
               const float *__restrict__ Fv, float *__restrict__ Fx, float *__restrict__ Fy,
               float *__restrict__ Fz, const uint32_t *__restrict__ mask2d, int *__restrict__ flags)
 {
-    extern __shared__ float sbox[];
+    extern __shared__ unsigned sbox[];
     __shared__ int s_lo[3], s_hi[3];
+    __shared__ unsigned s_fmax[3], s_wmax;
     const int cell = blockIdx.x / npatch, patch = blockIdx.x - cell * npatch, tid = threadIdx.x;
     const int p0 = patch_off[patch], np = patch_off[patch + 1] - p0, vstride = patch_stride[patch];
     const double *xs = X + (long long)cell * V, *ys = X + nv + (long long)cell * V, *zs = X + 2 * nv + (long long)cell * V;
@@ -55,10 +57,17 @@ spread_kernel(const Geom g, const double *__restrict__ X, long long nv, int V,
     const double az = lat_z(g, zs[0]);   // one anchor per cell: every patch unwraps z the same way
 
     if (tid < 3) { s_lo[tid] = INT_MAX; s_hi[tid] = INT_MIN; }
+    if (tid < 3) s_fmax[tid] = 0u;
+    if (tid == 0) s_wmax = 0u;
     __syncthreads();
     int lo0 = INT_MAX, lo1 = INT_MAX, lo2 = INT_MAX, hi0 = INT_MIN, hi1 = INT_MIN, hi2 = INT_MIN;
+    float fmax0 = 0.f, fmax1 = 0.f, fmax2 = 0.f;
+    bool nonfinite = false;
     for (int k = tid; k < np; k += blockDim.x) {
         const int v = patch_vtx[p0 + k];
+        const float afx = fabsf(fxs[v]), afy = fabsf(fys[v]), afz = fabsf(fzs[v]);
+        nonfinite |= !(afx <= FLT_MAX && afy <= FLT_MAX && afz <= FLT_MAX);
+        fmax0 = fmaxf(fmax0, afx); fmax1 = fmaxf(fmax1, afy); fmax2 = fmaxf(fmax2, afz);
         const int ix = (int)floor(lat_x(g, xs[v])), iy = (int)floor(lat_y(g, ys[v]));
         const int iz = (int)floor(unwrap_near(lat_z(g, zs[v]), az, g.nzc));
         lo0 = min(lo0, ix - 1); hi0 = max(hi0, ix + 2);
@@ -67,16 +76,76 @@ spread_kernel(const Geom g, const double *__restrict__ X, long long nv, int V,
     }
     atomicMin(&s_lo[0], lo0); atomicMin(&s_lo[1], lo1); atomicMin(&s_lo[2], lo2);
     atomicMax(&s_hi[0], hi0); atomicMax(&s_hi[1], hi1); atomicMax(&s_hi[2], hi2);
-    __syncthreads();
+    // non-negative floats order like their bit patterns
+    atomicMax(&s_fmax[0], __float_as_uint(fmax0));
+    atomicMax(&s_fmax[1], __float_as_uint(fmax1));
+    atomicMax(&s_fmax[2], __float_as_uint(fmax2));
+    if (__syncthreads_or(nonfinite)) {
+        if (tid == 0) atomicOr(flags, RBC_FLAG_NONFINITE);
+        return;
+    }
+    if ((s_fmax[0] | s_fmax[1] | s_fmax[2]) == 0u) return;   // no force on this patch
     const int bx0 = s_lo[0], by0 = s_lo[1], bz0 = s_lo[2];
     const int bx = s_hi[0] - bx0 + 1, by = s_hi[1] - by0 + 1, bz = s_hi[2] - bz0 + 1;
     const long long ps = (((long long)bx * by + 31) & ~31LL) + 8;   // plane stride = 8 (mod 32)
     const long long nb = ps * bz;
     const bool use_box = nb <= SPREAD_BOX_CAP;
     if (!use_box && tid == 0) atomicOr(flags, RBC_FLAG_SPREAD_OVERFLOW);
+    const int psi = use_box ? (int)ps : 0, nbi = use_box ? (int)nb : 0;   // box indices fit in int
 
+    // Box sums in 32-bit fixed point, one power-of-two scale per force
+    // component.  A vertex whose stencil starts at node b - 1 (b = floor of
+    // its lattice position) gives node b - 1 + a a 1-D weight of at most
+    // k[a] = (1, 2, 2, 1) / 4 (the largest values of delta4's weights), so
+    // Wn = sum over base cells b of count(b) * k[ax] * k[ay] * k[az] bounds
+    // the sum of the weights at node n, and no node's force sum exceeds
+    // max(Wn) * fmax.  A scale of at most 2^31 / that keeps every FINAL sum in
+    // range; partial sums may wrap, but the adds are modular (unsigned), so
+    // the final sums are still exact.  Each term is an FP32 product rounded
+    // once to an integer, the integer sums do not depend on the order of the
+    // atomics, and converting back costs one rounding to FP32 (the scale is
+    // capped at 2^126 so that it and its inverse stay normal floats).
+    float qs[3] = {0.f, 0.f, 0.f}, qi[3] = {0.f, 0.f, 0.f};
     if (use_box) {
-        for (int i = tid; i < 3 * nb; i += blockDim.x) sbox[i] = 0.f;
+        // Wn in units of 1/64: each vertex adds 4 k[a] * 4 k[b] to the 16
+        // nodes (x, y) of its stencil in its base plane; a walk down each
+        // column then applies 4 k along z with a sliding window.
+        unsigned *cnt = sbox + 2 * nbi;
+        for (int i = tid; i < nbi; i += SPREAD_THREADS) cnt[i] = 0u;
+        __syncthreads();
+        for (int k = tid; k < np; k += SPREAD_THREADS) {
+            const int v = patch_vtx[p0 + k];
+            const int ix = (int)floor(lat_x(g, xs[v])), iy = (int)floor(lat_y(g, ys[v]));
+            const int iz = (int)floor(unwrap_near(lat_z(g, zs[v]), az, g.nzc));
+            const int li0 = (ix - 1 - bx0) + bx * (iy - 1 - by0) + psi * (iz - bz0);
+#pragma unroll
+            for (int b = 0; b < 4; b++)
+#pragma unroll
+                for (int a = 0; a < 4; a++)
+                    atomicAdd(&cnt[li0 + a + bx * b], (unsigned)((a == 0 || a == 3 ? 1 : 2) * (b == 0 || b == 3 ? 1 : 2)));
+        }
+        __syncthreads();
+        unsigned wmax = 0u;
+        for (int r = tid; r < bx * by; r += SPREAD_THREADS) {
+            unsigned c2 = 0u, c1 = 0u, c0 = 0u, nx1 = cnt[r];   // base planes z-2, z-1, z, z+1
+            for (int z = 0; z < bz; z++) {
+                c2 = c1; c1 = c0; c0 = nx1;
+                nx1 = z + 1 < bz ? cnt[(z + 1) * psi + r] : 0u;
+                wmax = max(wmax, nx1 + 2u * (c0 + c1) + c2);
+            }
+        }
+        atomicMax(&s_wmax, wmax);
+        __syncthreads();
+        const float wb = (float)s_wmax * (1.0f / 64.0f);
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            const float fm = __uint_as_float(s_fmax[k]) * wscale;
+            // 2.147e9 < 2^31 leaves room for the rounding of the terms
+            const float e = fminf(floorf(log2f(2.147e9f / (wb * fm))), 126.f);
+            qs[k] = exp2f(e);
+            qi[k] = exp2f(-e);
+        }
+        for (int i = tid; i < 3 * nbi; i += blockDim.x) sbox[i] = 0u;
         __syncthreads();
     }
     // Four tasks per vertex: task i handles stencil plane c = i & 3 of the
@@ -85,9 +154,16 @@ spread_kernel(const Geom g, const double *__restrict__ X, long long nv, int V,
     // to the same box node in one instruction.  The fluid test is applied once
     // per node at the flush (wall columns accumulate in shared memory and are
     // dropped there).
-    for (int i = tid; i < 4 * np; i += blockDim.x) {
-        const int c = i & 3;
-        const int v = patch_vtx[p0 + (int)(((long long)(i >> 2) * vstride) % np)];
+    // SPREAD_THREADS is a multiple of 4, so a thread keeps one plane c and
+    // steps through j = tid / 4 + k * SPREAD_THREADS / 4, whose patch slot
+    // j * vstride mod np advances by a constant.
+    const int c = tid & 3, jstep = SPREAD_THREADS / 4;
+    const int vstep = (int)(((long long)jstep * vstride) % np);
+    int jv = (int)(((long long)(tid >> 2) * vstride) % np);
+    for (int j = tid >> 2; j < np; j += jstep) {
+        const int v = patch_vtx[p0 + jv];
+        jv += vstep;
+        if (jv >= np) jv -= np;
         const double lx = lat_x(g, xs[v]), ly = lat_y(g, ys[v]);
         const double lzr = lat_z(g, zs[v]);
         const double lz = unwrap_near(lzr, az, g.nzc);
@@ -103,7 +179,8 @@ spread_kernel(const Geom g, const double *__restrict__ X, long long nv, int V,
         const int ix0 = (int)flx - 1, iy0 = (int)fly - 1;
         const float sc = wscale * wzc;
         const float f0 = fxs[v] * sc, f1 = fys[v] * sc, f2 = fzs[v] * sc;
-        const long long zoff = ps * (iz - bz0);
+        const float q0 = f0 * qs[0], q1 = f1 * qs[1], q2 = f2 * qs[2];
+        const int zoff = psi * (iz - bz0);
 #pragma unroll
         for (int b = 0; b < 4; b++) {
             const int gy = iy0 + b;
@@ -115,10 +192,10 @@ spread_kernel(const Geom g, const double *__restrict__ X, long long nv, int V,
                 if (gx < 0 || gx >= g.nx) continue;
                 const float w = wx[a] * wyb;
                 if (use_box) {
-                    const long long li = (gx - bx0) + (long long)bx * (gy - by0) + zoff;
-                    atomicAdd(&sbox[li], w * f0);
-                    atomicAdd(&sbox[nb + li], w * f1);
-                    atomicAdd(&sbox[2 * nb + li], w * f2);
+                    const int li = (gx - bx0) + bx * (gy - by0) + zoff;
+                    atomicAdd(&sbox[li], (unsigned)__float2int_rn(w * q0));
+                    atomicAdd(&sbox[nbi + li], (unsigned)__float2int_rn(w * q1));
+                    atomicAdd(&sbox[2 * nbi + li], (unsigned)__float2int_rn(w * q2));
                 } else if (__ldg(&mask2d[gx + g.nx * gy]) & MASK_FLUID) {
                     const long long gi = (long long)wrap_z(iz, g.nzc) * g.plane + gx + (long long)g.nx * gy;
                     atomicAdd(&Fx[gi], w * f0);
@@ -130,20 +207,21 @@ spread_kernel(const Geom g, const double *__restrict__ X, long long nv, int V,
     }
     if (!use_box) return;
     __syncthreads();
-    const long long rowplane = (long long)bx * by;
-    for (long long li = tid; li < nb; li += blockDim.x) {
-        const long long lz = li / ps, r = li - lz * ps;
+    const int rowplane = bx * by;
+    for (int li = tid; li < nbi; li += SPREAD_THREADS) {
+        const int lz = li / psi, r = li - lz * psi;
         if (r >= rowplane) continue;   // plane padding
-        const float a = sbox[li], b = sbox[nb + li], c = sbox[2 * nb + li];
-        if (a == 0.f && b == 0.f && c == 0.f) continue;
-        const int ly = (int)(r / bx), lx = (int)(r - (long long)ly * bx);
+        const int ia = (int)sbox[li], ib = (int)sbox[nbi + li], ic = (int)sbox[2 * nbi + li];
+        if ((ia | ib | ic) == 0) continue;
+        const int ly = r / bx, lx = r - ly * bx;
         const int gx = bx0 + lx, gy = by0 + ly;
         if (gx < 0 || gx >= g.nx || gy < 0 || gy >= g.ny) continue;   // never written; kept as a guard
         if (!(__ldg(&mask2d[gx + g.nx * gy]) & MASK_FLUID)) continue;   // wall column: the LBM never reads it
-        const long long gi = (long long)wrap_z(bz0 + (int)lz, g.nzc) * g.plane + gx + (long long)g.nx * gy;
-        if (a != 0.f) atomicAdd(&Fx[gi], a);
-        if (b != 0.f) atomicAdd(&Fy[gi], b);
-        if (c != 0.f) atomicAdd(&Fz[gi], c);
+        const long long gi = (long long)wrap_z(bz0 + lz, g.nzc) * g.plane + gx + (long long)g.nx * gy;
+        const float fa = (float)ia * qi[0], fb = (float)ib * qi[1], fc = (float)ic * qi[2];
+        if (ia != 0) atomicAdd(&Fx[gi], fa);
+        if (ib != 0) atomicAdd(&Fy[gi], fb);
+        if (ic != 0) atomicAdd(&Fz[gi], fc);
     }
 }
 
