@@ -32,42 +32,22 @@ template <> struct Store<RBC_STORE_F16> {
 
 constexpr int LBM_THREADS = 256;
 
-// One thread per internal node (x fastest).  Per fluid node: 19 pulled loads,
-// 12 B of IB force, 19 stores, 16 B of rho/u.
-template <int STORE>
-__global__ void __launch_bounds__(LBM_THREADS, 5)
-lbm_collide_stream(const typename Store<STORE>::T *__restrict__ gin, typename Store<STORE>::T *__restrict__ gout,
-                   float4 *__restrict__ uvr,
-                   float *__restrict__ Fx, float *__restrict__ Fy, float *__restrict__ Fz,
-                   const uint32_t *__restrict__ mask2d, const float *__restrict__ drive,
-                   int nx, int ny, int nzc, long long nint,
-                   float omega, float Cr, float Bc, float scale, float inv_scale)
+// BGK + Guo forcing (lbm.cu:1129-1213 of the reference).  With G the half
+// force rho (P drive z^ + B F) (lbm.cu:1116-1118), u = (j + G) / (rho Cr) and
+//   f_eq,q = w_q [drho + rho (3 Cr e.u + 4.5 Cr^2 (e.u)^2 - 1.5 Cr^2 u.u)]
+//   F_q    = (1 - om/2) 2 w_q [3 e.G - 3 Cr u.G + 9 Cr (e.u)(e.G)]
+// the post-collision value (1 - om) g_q + om f_eq,q + F_q is evaluated as
+//   (1 - om) g_q + w_q (A + e.u (B + C e.u + E e.G) + D e.G)
+// with per-node scalars A..E.
+struct Collision {
+    float u, v, w, r;
+    float Gx, Gy, Gz;
+    float A, B, C, D, E;
+};
+
+__device__ __forceinline__ Collision collision_terms(const float (&g)[Q], float fx, float fy, float fz, float pd,
+                                                     float omega, float Cr, float Bc)
 {
-    using S = Store<STORE>;
-    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= nint) return;
-    const int plane = nx * ny;
-    const int z = (int)(idx / plane);
-    const int xy = (int)(idx - (long long)z * plane);
-    const uint32_t m = __ldg(&mask2d[xy]);
-    if (!(m & MASK_FLUID)) return;
-
-    const long long zb0 = (long long)z * plane;
-    const long long zbm = (z == 0) ? (long long)(nzc - 1) * plane : zb0 - plane;       // plane z-1
-    const long long zbp = (z == nzc - 1) ? 0 : zb0 + plane;                             // plane z+1
-
-    float g[Q];
-#pragma unroll
-    for (int q = 0; q < Q; q++) {
-        const long long src = ((ez(q) == 1) ? zbm : (ez(q) == -1) ? zbp : zb0) + xy - ex(q) - nx * ey(q);
-        const bool bb = (m >> q) & 1u;
-        const typename S::T *p = bb ? (gin + (long long)opp(q) * nint + idx) : (gin + (long long)q * nint + src);
-        g[q] = S::ld(p, inv_scale);
-    }
-
-    const float fx = Fx[idx], fy = Fy[idx], fz = Fz[idx];
-    const float pd = __ldg(drive);
-
     float drho = 0.f, jx = 0.f, jy = 0.f, jz = 0.f;
 #pragma unroll
     for (int q = 0; q < Q; q++) {
@@ -76,35 +56,82 @@ lbm_collide_stream(const typename Store<STORE>::T *__restrict__ gin, typename St
         if (ey(q)) jy += ey(q) * g[q];
         if (ez(q)) jz += ez(q) * g[q];
     }
-    const float r = 1.0f + drho;
-    // half of the total force density: rho P drive z^ + rho B F (lbm.cu:1116-1118)
-    const float Gx = r * Bc * fx, Gy = r * Bc * fy, Gz = r * (pd + Bc * fz);
-    const float inv = 1.0f / (r * Cr);
-    const float u = (jx + Gx) * inv, v = (jy + Gy) * inv, w = (jz + Gz) * inv;
-
-    uvr[idx] = make_float4(u, v, w, r);
-    if (fx != 0.f || fy != 0.f || fz != 0.f) { Fx[idx] = 0.f; Fy[idx] = 0.f; Fz[idx] = 0.f; }
-
-    // BGK + Guo forcing (lbm.cu:1129-1213): with G the half force above,
-    // F_q = (1 - om/2) * 2 * w_q * [3 e.G - 3 Cr u.G + 9 Cr (e.u)(e.G)]
-    const float Cr2 = Cr * Cr;
-    const float om1 = 1.0f - omega;
+    Collision c;
+    c.r = 1.0f + drho;
+    c.Gx = c.r * Bc * fx; c.Gy = c.r * Bc * fy; c.Gz = c.r * (pd + Bc * fz);
+    const float inv = 1.0f / (c.r * Cr);
+    c.u = (jx + c.Gx) * inv; c.v = (jy + c.Gy) * inv; c.w = (jz + c.Gz) * inv;
     const float fo = (1.0f - 0.5f * omega) * 2.0f;
-    const float usq = -1.5f * (u * u + v * v + w * w) * Cr2;
-    const float uG = 3.0f * Cr * (u * Gx + v * Gy + w * Gz);
+    const float usq = -1.5f * Cr * Cr * (c.u * c.u + c.v * c.v + c.w * c.w);
+    const float uG = 3.0f * Cr * (c.u * c.Gx + c.v * c.Gy + c.w * c.Gz);
+    c.A = omega * (drho + c.r * usq) - fo * uG;
+    c.B = 3.0f * Cr * omega * c.r;
+    c.C = 4.5f * Cr * Cr * omega * c.r;
+    c.D = 3.0f * fo;
+    c.E = 9.0f * Cr * fo;
+    return c;
+}
+
+__device__ __forceinline__ float post_collision(const Collision &c, int q, float gq, float om1)
+{
+    const float eu = ex(q) * c.u + ey(q) * c.v + ez(q) * c.w;
+    const float eG = ex(q) * c.Gx + ey(q) * c.Gy + ez(q) * c.Gz;
+    return om1 * gq + wq(q) * (c.A + eu * (c.B + c.C * eu + c.E * eG) + c.D * eG);
+}
+
+// One thread per lattice node: blockIdx.x * blockDim.x + threadIdx.x indexes
+// the node in its (x, y) plane, blockIdx.y (+ k gridDim.y) the plane z.  Per
+// fluid node: 19 pulled loads, 12 B of IB force, 19 stores, 16 B of rho/u.
+//
+// Full-sector stores: a warp that holds any fluid node stores all 32 of its
+// nodes in the same store instructions, its wall nodes writing 0 (their
+// populations are never read) and rho 1, u 0 (what the interpolation reads at
+// walls).  Leaving the wall columns of a row unwritten would leave the first
+// and last 32-byte sectors of the row partly written, which the L2 completes
+// with a DRAM read before writing them back.
+template <int STORE>
+__global__ void __launch_bounds__(LBM_THREADS, 4)
+lbm_collide_stream(const typename Store<STORE>::T *__restrict__ gin, typename Store<STORE>::T *__restrict__ gout,
+                   float4 *__restrict__ uvr,
+                   float *__restrict__ Fx, float *__restrict__ Fy, float *__restrict__ Fz,
+                   const uint32_t *__restrict__ mask2d, const float *__restrict__ drive,
+                   int nx, int ny, int nzc, long long nint,
+                   float omega, float Cr, float Bc, float scale, float inv_scale)
+{
+    using S = Store<STORE>;
+    const int plane = nx * ny;
+    const int xy = blockIdx.x * blockDim.x + threadIdx.x;
+    if (xy >= plane) return;
+    const uint32_t m = __ldg(&mask2d[xy]);
+    const bool fluid = (m & MASK_FLUID) != 0;
+    if (!__any_sync(__activemask(), fluid)) return;   // a warp of wall nodes stores nothing
+    const float pd = __ldg(drive), om1 = 1.0f - omega;
+    for (int z = blockIdx.y; z < nzc; z += gridDim.y) {
+        const long long zb0 = (long long)z * plane, idx = zb0 + xy;
+        const long long zbm = (z == 0) ? (long long)(nzc - 1) * plane : zb0 - plane;   // plane z-1
+        const long long zbp = (z == nzc - 1) ? 0 : zb0 + plane;                         // plane z+1
+        float g[Q];
 #pragma unroll
-    for (int q = 0; q < Q; q++) {
-        const float eu = ex(q) * u + ey(q) * v + ez(q) * w;
-        const float eG = ex(q) * Gx + ey(q) * Gy + ez(q) * Gz;
-        const float geq = wq(q) * (drho + r * (3.0f * Cr * eu + 4.5f * Cr2 * eu * eu + usq));
-        const float fq = fo * wq(q) * (3.0f * eG - uG + 9.0f * Cr * eu * eG);
-        S::st(gout + (long long)q * nint + idx, om1 * g[q] + omega * geq + fq, scale);
+        for (int q = 0; q < Q; q++) {
+            const long long src = ((ez(q) == 1) ? zbm : (ez(q) == -1) ? zbp : zb0) + xy - ex(q) - nx * ey(q);
+            const bool bb = (m >> q) & 1u;   // i - e_q is a wall: half-way bounce-back of f*_{opp q}(i)
+            g[q] = fluid ? S::ld(bb ? gin + (long long)opp(q) * nint + idx : gin + (long long)q * nint + src, inv_scale)
+                         : 0.f;
+        }
+        float fx = 0.f, fy = 0.f, fz = 0.f;
+        if (fluid) { fx = Fx[idx]; fy = Fy[idx]; fz = Fz[idx]; }
+        const Collision c = collision_terms(g, fx, fy, fz, pd, omega, Cr, Bc);
+        uvr[idx] = fluid ? make_float4(c.u, c.v, c.w, c.r) : make_float4(0.f, 0.f, 0.f, 1.f);
+        if (fx != 0.f || fy != 0.f || fz != 0.f) { Fx[idx] = 0.f; Fy[idx] = 0.f; Fz[idx] = 0.f; }
+#pragma unroll
+        for (int q = 0; q < Q; q++)
+            S::st(gout + (long long)q * nint + idx, fluid ? post_collision(c, q, g[q], om1) : 0.f, scale);
     }
 }
 
 void launch_lbm(const Geom &g, int storage, const LbmArgs &a, cudaStream_t s)
 {
-    const unsigned blocks = (unsigned)((g.nint + LBM_THREADS - 1) / LBM_THREADS);
+    const dim3 blocks((unsigned)((g.plane + LBM_THREADS - 1) / LBM_THREADS), (unsigned)(g.nzc < 65535 ? g.nzc : 65535));
     if (storage == RBC_STORE_F16)
         lbm_collide_stream<RBC_STORE_F16><<<blocks, LBM_THREADS, 0, s>>>(
             (const __half *)a.gin, (__half *)a.gout, a.uvr, a.Fx, a.Fy, a.Fz, a.mask2d,

@@ -135,20 +135,37 @@ def test_lbm_matches_oracle(developed, oracle_mod):
     assert ferr <= 1e-8 and derr <= 1e-6 and uerr <= 1e-5
 
 
-def test_pure_fluid_lbm_matches_oracle(oracle_mod, native_lib):
-    case = configs.duct_case("fluid_32x20x16", 32, 20, 16, g=1e-4)
+# (duct width = lattice nx, height, storage): rows of 20, 21 and 24 nodes
+# put warps across row ends and wall columns in different lanes; FP16 stores
+# (f - w) * 2^15 in binary16.
+@pytest.mark.parametrize("width,height,storage", [
+    (20, 16, 0),
+    (21, 18, 0),
+    (24, 16, 1),
+    (20, 16, 1),
+])
+def test_pure_fluid_lbm_matches_oracle(oracle_mod, native_lib, width, height, storage):
+    case = configs.duct_case(f"fluid_32x{width}x{height}", 32, width, height, g=1e-4)
     o = oracle_mod.Oracle(case)
     o.step(30)
-    sim = load(o)
-    o.step(1)
-    sim.step(1)
+    sim = load(o, storage=storage)
+    o.step(3)
+    sim.step(3)
     out = sim.export_lattice()
     m = comp(case)
     uref = np.concatenate([o["un"][m], o["vn"][m], o["wn"][m]])
     umine = np.concatenate([out["un"][m], out["vn"][m], out["wn"][m]])
-    assert rel_l2(umine, uref) <= 1e-5
     mq = np.repeat(m, 19)
-    assert np.abs(out["fn"][mq] - o.fn[mq]).max() <= 1e-8
+    uerr = rel_l2(umine, uref)
+    ferr = np.abs(out["fn"][mq] - o.fn[mq]).max()
+    print(f"fluid {width}x{height} storage {storage}: u rel L2 {uerr:.3e}  max|df| {ferr:.3e}")
+    flags, _ = sim.status()
+    assert flags == 0, flags
+    if storage == 0:
+        assert uerr <= 1e-5 and ferr <= 1e-8
+    else:
+        # binary16 keeps 11 significant bits of (f - w) * 2^15
+        assert uerr <= 5e-3 and ferr <= 5e-6
 
 
 def test_advect_matches_oracle(developed, oracle_mod):
