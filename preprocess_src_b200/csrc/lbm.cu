@@ -79,6 +79,27 @@ __device__ __forceinline__ float post_collision(const Collision &c, int q, float
     return om1 * gq + wq(q) * (c.A + eu * (c.B + c.C * eu + c.E * eG) + c.D * eG);
 }
 
+// Collision of one node from its pulled populations g and stores of the
+// post-collision values (0 for wall lanes) at element offset idx of every
+// population array; I is the offset type (int when Q * nint < 2^31).
+template <int STORE, bool ALL_FLUID, typename I>
+__device__ __forceinline__ void collide_store(float (&g)[Q], bool fluid, I idx, I nint,
+                                              typename Store<STORE>::T *__restrict__ gout, float4 *__restrict__ uvr,
+                                              float *__restrict__ Fx, float *__restrict__ Fy, float *__restrict__ Fz,
+                                              float pd, float omega, float om1, float Cr, float Bc, float scale)
+{
+    using S = Store<STORE>;
+    const bool live = ALL_FLUID || fluid;
+    float fx = 0.f, fy = 0.f, fz = 0.f;
+    if (live) { fx = Fx[idx]; fy = Fy[idx]; fz = Fz[idx]; }
+    const Collision c = collision_terms(g, fx, fy, fz, pd, omega, Cr, Bc);
+    uvr[idx] = live ? make_float4(c.u, c.v, c.w, c.r) : make_float4(0.f, 0.f, 0.f, 1.f);
+    if (fx != 0.f || fy != 0.f || fz != 0.f) { Fx[idx] = 0.f; Fy[idx] = 0.f; Fz[idx] = 0.f; }
+#pragma unroll
+    for (int q = 0; q < Q; q++)
+        S::st(gout + ((I)q * nint + idx), live ? post_collision(c, q, g[q], om1) : 0.f, scale);
+}
+
 // One thread per lattice node: blockIdx.x * blockDim.x + threadIdx.x indexes
 // the node in its (x, y) plane, blockIdx.y (+ k gridDim.y) the plane z.  Per
 // fluid node: 19 pulled loads, 12 B of IB force, 19 stores, 16 B of rho/u.
@@ -89,13 +110,21 @@ __device__ __forceinline__ float post_collision(const Collision &c, int q, float
 // walls).  Leaving the wall columns of a row unwritten would leave the first
 // and last 32-byte sectors of the row partly written, which the L2 completes
 // with a DRAM read before writing them back.
-template <int STORE>
-__global__ void __launch_bounds__(LBM_THREADS, 4)
+//
+// A warp none of whose nodes has a wall link takes a path without the
+// bounce-back selects: such a warp holds only fluid nodes, because a wall node
+// next (in x) to a fluid node gives that node a wall link, and the first and
+// last node of every row are walls.
+#ifndef LBM_MIN_BLOCKS
+#define LBM_MIN_BLOCKS 4   // resident CTAs per SM the register allocation must allow
+#endif
+template <int STORE, typename I>
+__global__ void __launch_bounds__(LBM_THREADS, LBM_MIN_BLOCKS)
 lbm_collide_stream(const typename Store<STORE>::T *__restrict__ gin, typename Store<STORE>::T *__restrict__ gout,
                    float4 *__restrict__ uvr,
                    float *__restrict__ Fx, float *__restrict__ Fy, float *__restrict__ Fz,
                    const uint32_t *__restrict__ mask2d, const float *__restrict__ drive,
-                   int nx, int ny, int nzc, long long nint,
+                   int nx, int ny, int nzc, I nint,
                    float omega, float Cr, float Bc, float scale, float inv_scale)
 {
     using S = Store<STORE>;
@@ -104,42 +133,48 @@ lbm_collide_stream(const typename Store<STORE>::T *__restrict__ gin, typename St
     if (xy >= plane) return;
     const uint32_t m = __ldg(&mask2d[xy]);
     const bool fluid = (m & MASK_FLUID) != 0;
-    if (!__any_sync(__activemask(), fluid)) return;   // a warp of wall nodes stores nothing
+    const unsigned act = __activemask();
+    if (!__any_sync(act, fluid)) return;   // a warp of wall nodes stores nothing
+    const bool warp_links = __any_sync(act, (m & ~MASK_FLUID) != 0u);
     const float pd = __ldg(drive), om1 = 1.0f - omega;
     for (int z = blockIdx.y; z < nzc; z += gridDim.y) {
-        const long long zb0 = (long long)z * plane, idx = zb0 + xy;
-        const long long zbm = (z == 0) ? (long long)(nzc - 1) * plane : zb0 - plane;   // plane z-1
-        const long long zbp = (z == nzc - 1) ? 0 : zb0 + plane;                         // plane z+1
+        const I zb0 = (I)z * plane, idx = zb0 + xy;
+        const I zbm = (z == 0) ? (I)(nzc - 1) * plane : zb0 - plane;   // plane z-1
+        const I zbp = (z == nzc - 1) ? (I)0 : zb0 + plane;             // plane z+1
         float g[Q];
+        if (!warp_links) {
 #pragma unroll
-        for (int q = 0; q < Q; q++) {
-            const long long src = ((ez(q) == 1) ? zbm : (ez(q) == -1) ? zbp : zb0) + xy - ex(q) - nx * ey(q);
-            const bool bb = (m >> q) & 1u;   // i - e_q is a wall: half-way bounce-back of f*_{opp q}(i)
-            g[q] = fluid ? S::ld(bb ? gin + (long long)opp(q) * nint + idx : gin + (long long)q * nint + src, inv_scale)
-                         : 0.f;
+            for (int q = 0; q < Q; q++) {
+                const I src = ((ez(q) == 1) ? zbm : (ez(q) == -1) ? zbp : zb0) + (xy - ex(q) - nx * ey(q));
+                g[q] = S::ld(gin + ((I)q * nint + src), inv_scale);
+            }
+            collide_store<STORE, true, I>(g, true, idx, nint, gout, uvr, Fx, Fy, Fz, pd, omega, om1, Cr, Bc, scale);
+        } else {
+#pragma unroll
+            for (int q = 0; q < Q; q++) {
+                const I src = ((ez(q) == 1) ? zbm : (ez(q) == -1) ? zbp : zb0) + (xy - ex(q) - nx * ey(q));
+                const bool bb = (m >> q) & 1u;   // i - e_q is a wall: half-way bounce-back of f*_{opp q}(i)
+                g[q] = fluid ? S::ld(gin + (bb ? (I)opp(q) * nint + idx : (I)q * nint + src), inv_scale) : 0.f;
+            }
+            collide_store<STORE, false, I>(g, fluid, idx, nint, gout, uvr, Fx, Fy, Fz, pd, omega, om1, Cr, Bc, scale);
         }
-        float fx = 0.f, fy = 0.f, fz = 0.f;
-        if (fluid) { fx = Fx[idx]; fy = Fy[idx]; fz = Fz[idx]; }
-        const Collision c = collision_terms(g, fx, fy, fz, pd, omega, Cr, Bc);
-        uvr[idx] = fluid ? make_float4(c.u, c.v, c.w, c.r) : make_float4(0.f, 0.f, 0.f, 1.f);
-        if (fx != 0.f || fy != 0.f || fz != 0.f) { Fx[idx] = 0.f; Fy[idx] = 0.f; Fz[idx] = 0.f; }
-#pragma unroll
-        for (int q = 0; q < Q; q++)
-            S::st(gout + (long long)q * nint + idx, fluid ? post_collision(c, q, g[q], om1) : 0.f, scale);
     }
 }
 
 void launch_lbm(const Geom &g, int storage, const LbmArgs &a, cudaStream_t s)
 {
     const dim3 blocks((unsigned)((g.plane + LBM_THREADS - 1) / LBM_THREADS), (unsigned)(g.nzc < 65535 ? g.nzc : 65535));
-    if (storage == RBC_STORE_F16)
-        lbm_collide_stream<RBC_STORE_F16><<<blocks, LBM_THREADS, 0, s>>>(
-            (const __half *)a.gin, (__half *)a.gout, a.uvr, a.Fx, a.Fy, a.Fz, a.mask2d,
-            a.drive, g.nx, g.ny, g.nzc, g.nint, a.omega, a.Cr, a.Bc, a.scale, a.inv_scale);
-    else
-        lbm_collide_stream<RBC_STORE_F32><<<blocks, LBM_THREADS, 0, s>>>(
-            (const float *)a.gin, (float *)a.gout, a.uvr, a.Fx, a.Fy, a.Fz, a.mask2d,
-            a.drive, g.nx, g.ny, g.nzc, g.nint, a.omega, a.Cr, a.Bc, a.scale, a.inv_scale);
+    const bool off32 = (long long)Q * g.nint < (1LL << 31);   // every element offset fits in an int
+#define LBM_LAUNCH(ST, I)                                                                                     \
+    lbm_collide_stream<ST, I><<<blocks, LBM_THREADS, 0, s>>>(                                                 \
+        (const Store<ST>::T *)a.gin, (Store<ST>::T *)a.gout, a.uvr, a.Fx, a.Fy, a.Fz, a.mask2d, a.drive, g.nx, \
+        g.ny, g.nzc, (I)g.nint, a.omega, a.Cr, a.Bc, a.scale, a.inv_scale)
+    if (storage == RBC_STORE_F16) {
+        if (off32) LBM_LAUNCH(RBC_STORE_F16, int); else LBM_LAUNCH(RBC_STORE_F16, long long);
+    } else {
+        if (off32) LBM_LAUNCH(RBC_STORE_F32, int); else LBM_LAUNCH(RBC_STORE_F32, long long);
+    }
+#undef LBM_LAUNCH
 }
 
 // ---- reference layout <-> internal layout ---------------------------------
