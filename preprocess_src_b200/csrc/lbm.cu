@@ -95,9 +95,9 @@ __device__ __forceinline__ void collide_store(float (&g)[Q], bool fluid, I idx, 
     const Collision c = collision_terms(g, fx, fy, fz, pd, omega, Cr, Bc);
     uvr[idx] = live ? make_float4(c.u, c.v, c.w, c.r) : make_float4(0.f, 0.f, 0.f, 1.f);
     if (fx != 0.f || fy != 0.f || fz != 0.f) { Fx[idx] = 0.f; Fy[idx] = 0.f; Fz[idx] = 0.f; }
+    typename S::T *ob = gout + idx;
 #pragma unroll
-    for (int q = 0; q < Q; q++)
-        S::st(gout + ((I)q * nint + idx), live ? post_collision(c, q, g[q], om1) : 0.f, scale);
+    for (int q = 0; q < Q; q++) S::st(ob + (I)q * nint, live ? post_collision(c, q, g[q], om1) : 0.f, scale);
 }
 
 // One thread per lattice node: blockIdx.x * blockDim.x + threadIdx.x indexes
@@ -138,23 +138,25 @@ lbm_collide_stream(const typename Store<STORE>::T *__restrict__ gin, typename St
     const bool warp_links = __any_sync(act, (m & ~MASK_FLUID) != 0u);
     const float pd = __ldg(drive), om1 = 1.0f - omega;
     for (int z = blockIdx.y; z < nzc; z += gridDim.y) {
-        const I zb0 = (I)z * plane, idx = zb0 + xy;
-        const I zbm = (z == 0) ? (I)(nzc - 1) * plane : zb0 - plane;   // plane z-1
-        const I zbp = (z == nzc - 1) ? (I)0 : zb0 + plane;             // plane z+1
+        // offsets of the source planes z - 1 and z + 1 from plane z (periodic);
+        // with them every pull offset from the node is uniform over the block
+        const I dzm = (z == 0) ? (I)(nzc - 1) * plane : -(I)plane;
+        const I dzp = (z == nzc - 1) ? -(I)(nzc - 1) * plane : (I)plane;
+        const I idx = (I)z * plane + xy;
+        const typename S::T *gb = gin + idx;
         float g[Q];
         if (!warp_links) {
 #pragma unroll
-            for (int q = 0; q < Q; q++) {
-                const I src = ((ez(q) == 1) ? zbm : (ez(q) == -1) ? zbp : zb0) + (xy - ex(q) - nx * ey(q));
-                g[q] = S::ld(gin + ((I)q * nint + src), inv_scale);
-            }
+            for (int q = 0; q < Q; q++)
+                g[q] = S::ld(gb + ((I)q * nint + ((ez(q) == 1) ? dzm : (ez(q) == -1) ? dzp : (I)0) - ex(q) - nx * ey(q)),
+                             inv_scale);
             collide_store<STORE, true, I>(g, true, idx, nint, gout, uvr, Fx, Fy, Fz, pd, omega, om1, Cr, Bc, scale);
         } else {
 #pragma unroll
             for (int q = 0; q < Q; q++) {
-                const I src = ((ez(q) == 1) ? zbm : (ez(q) == -1) ? zbp : zb0) + (xy - ex(q) - nx * ey(q));
+                const I pull = (I)q * nint + ((ez(q) == 1) ? dzm : (ez(q) == -1) ? dzp : (I)0) - ex(q) - nx * ey(q);
                 const bool bb = (m >> q) & 1u;   // i - e_q is a wall: half-way bounce-back of f*_{opp q}(i)
-                g[q] = fluid ? S::ld(gin + (bb ? (I)opp(q) * nint + idx : (I)q * nint + src), inv_scale) : 0.f;
+                g[q] = fluid ? S::ld(gb + (bb ? (I)opp(q) * nint : pull), inv_scale) : 0.f;
             }
             collide_store<STORE, false, I>(g, fluid, idx, nint, gout, uvr, Fx, Fy, Fz, pd, omega, om1, Cr, Bc, scale);
         }
