@@ -13,10 +13,14 @@
 // Here one CTA owns one cell and does all of it on chip:
 //  1. the cell's FP64 positions go to shared memory, unwrapped about vertex 0
 //     (the reference applies the same minimum-image shift per edge);
-//  2. each thread gathers the rows of its vertices through the vertex ->
-//     element incidence list (fixed order, no atomics): tension, matrix row,
+//  2. element pass: each element's tension is evaluated once and its record
+//     (twice the area gab and the load contributions of its second and third
+//     vertex; the first vertex's is minus their sum) goes to an L2-resident
+//     scratch array;
+//  3. vertex pass: each thread gathers the rows of its vertices through the
+//     vertex -> element incidence list (fixed order, no atomics): matrix row,
 //     right-hand side and nodal area;
-//  3. the scaled system is solved by Chebyshev iteration.  For any P1 triangle
+//  4. the scaled system is solved by Chebyshev iteration.  For any P1 triangle
 //     mesh the element mass matrix is (A/12)(1 + delta_ij), so every
 //     eigenvalue of D^-1 M lies in [1/2, 2] (Rayleigh quotients of an assembled
 //     sum of element matrices stay inside the element bounds).  With these
@@ -24,7 +28,7 @@
 //     (sqrt(4)-1)/(sqrt(4)+1) = 1/3 per iteration, one barrier per iteration.
 //     (Chebyshev iteration as in Y. Saad, Iterative Methods for Sparse Linear
 //     Systems, 2nd ed., Alg. 12.1.)
-//  4. f_i = -q_i * ds_i is written out.
+//  5. f_i = -q_i * ds_i is written out.
 //
 // Tension without cancellation.  The reference evaluates
 //   t = ca n + cb g^-1,  ca = rgs (I1 + 1) / Js,  cb = (C I2 - 1) Js
@@ -67,6 +71,28 @@ __device__ __forceinline__ T block_sum(T v, T *red) {
     return s;
 }
 
+// Element records: for each vertex slot en of an element, the load that the
+// element puts on that vertex and the element's gab, one 4-vector per slot.
+template <typename Real> struct Vec4;
+template <> struct Vec4<float> { using T = float4; };
+template <> struct Vec4<double> { using T = double4; };
+
+__device__ __forceinline__ float4 make_vec4(float x, float y, float z, float w) { return make_float4(x, y, z, w); }
+__device__ __forceinline__ double4 make_vec4(double x, double y, double z, double w) { return make_double4(x, y, z, w); }
+__device__ __forceinline__ void store_vec4(float4 *p, const float4 &v) { *p = v; }
+__device__ __forceinline__ void store_vec4(double4 *p, const double4 &v) {
+    double2 *q = reinterpret_cast<double2 *>(p);
+    q[0] = make_double2(v.x, v.y); q[1] = make_double2(v.z, v.w);
+}
+__device__ __forceinline__ float4 load_vec4(const float4 *p) { return *p; }
+__device__ __forceinline__ double4 load_vec4(const double4 *p) {
+    const double2 *q = reinterpret_cast<const double2 *>(p);
+    const double2 x = q[0], y = q[1];
+    return make_double4(x.x, x.y, y.x, y.y);
+}
+
+constexpr int MAX_VALENCE = 6;   // checked when the topology is built
+
 template <typename Real, int VPT>
 __global__ void __launch_bounds__(MEM_MAX_THREADS, 1)
 membrane_kernel(const MembraneArgs a)
@@ -80,7 +106,7 @@ membrane_kernel(const MembraneArgs a)
     int16_t *snbr = reinterpret_cast<int16_t *>(smem + 56 * (size_t)V);// [6][V]
 
     const int cell = blockIdx.x;
-    const long long vb = (long long)cell * V, eb = (long long)cell * E, nv = a.nv, ne = a.ne;
+    const long long vb = (long long)cell * V, eb = (long long)cell * E, nv = a.nv;
     const double ax = a.Xd[vb], ay = a.Xd[nv + vb], az = a.Xd[2 * nv + vb];
     for (int v = tid; v < V; v += T) {
         pos[v] = mimage(a.Xd[vb + v] - ax, a.LX);
@@ -90,7 +116,64 @@ membrane_kernel(const MembraneArgs a)
     for (int k = tid; k < 6 * V; k += T) snbr[k] = a.nbr[k];
     __syncthreads();
 
+    // element pass: tension of each element once (stress.cu:29-110, 195-270)
     const Real C = (Real)a.C, rgs = (Real)a.rgs;
+    using R4 = typename Vec4<Real>::T;
+    R4 *rec = reinterpret_cast<R4 *>(a.erec) + (size_t)eb * 3;   // [E][3 slots]: load on the slot's vertex, gab
+    for (int e = tid; e < E; e += T) {
+        const int ia = __ldg(&a.tri[3 * e]), ib = __ldg(&a.tri[3 * e + 1]), ic = __ldg(&a.tri[3 * e + 2]);
+        const double e1x = pos[ib] - pos[ia], e1y = pos[V + ib] - pos[V + ia], e1z = pos[2 * V + ib] - pos[2 * V + ia];
+        const double e2x = pos[ic] - pos[ia], e2y = pos[V + ic] - pos[V + ia], e2z = pos[2 * V + ic] - pos[2 * V + ia];
+        // deformed covariant metric (stress.cu:75-84) and its difference from the reference, in FP64
+        const double g11d = e1x * e1x + e1y * e1y + e1z * e1z;
+        const double g12d = e1x * e2x + e1y * e2y + e1z * e2z;
+        const double g22d = e2x * e2x + e2y * e2y + e2z * e2z;
+        // reference metric: covariant G and 1 / det G (one aligned 32-byte record per element);
+        // its inverse n as set_contravariant forms it (init2.cu:241-249)
+        const double2 *gp = reinterpret_cast<const double2 *>(a.gref + eb + e);
+        const double2 Ga = __ldg(gp), Gb = __ldg(gp + 1);
+        const double G11 = Ga.x, G12 = Ga.y, G22 = Gb.x, idG = Gb.y;
+        const Real d11 = (Real)(g11d - G11), d12 = (Real)(g12d - G12), d22 = (Real)(g22d - G22);
+        const Real g11 = (Real)g11d, g12 = (Real)g12d, g22 = (Real)g22d;
+        const Real n00 = (Real)(G22 * idG), n01 = (Real)(-G12 * idG), n11 = (Real)(G11 * idG);
+        const Real detn = (Real)idG;
+        const Real det = g11 * g22 - g12 * g12;
+        const Real idet = (Real)1 / det;
+        // invariants (stress.cu:90-93) from the metric difference
+        const Real i1 = n00 * d11 + (Real)2 * n01 * d12 + n11 * d22;
+        const Real i2 = detn * ((Real)G11 * d22 + (Real)G22 * d11 - (Real)2 * (Real)G12 * d12 + d11 * d22 - d12 * d12);
+        const Real js = sqrt(i2 + (Real)1);
+        const Real jsm1 = i2 / (js + (Real)1);
+        Real al, be;   // ca - 1 and cb + 1 of the law (stress.cu:94-99)
+        if (a.law == RBC_LAW_SKALAK) {
+            al = (rgs * i1 + (rgs - (Real)1) - jsm1) / js;
+            be = C * i2 * js - jsm1;
+        } else {
+            const Real js3 = js * js * js;
+            al = ((rgs - (Real)1) - jsm1) / js;
+            be = (jsm1 * (js * js + js + (Real)1) - (rgs - (Real)1)) / js3;
+        }
+        const Real gi00 = g22 * idet, gi01 = -g12 * idet, gi11 = g11 * idet;
+        // n D g^-1 = n - g^-1, symmetrised
+        const Real p00 = n00 * d11 + n01 * d12, p01 = n00 * d12 + n01 * d22;
+        const Real p10 = n01 * d11 + n11 * d12, p11 = n01 * d12 + n11 * d22;
+        const Real t00 = al * n00 + be * gi00 + (p00 * gi00 + p01 * gi01);
+        const Real t01 = al * n01 + be * gi01 + (Real)0.5 * ((p00 * gi01 + p01 * gi11) + (p10 * gi00 + p11 * gi01));
+        const Real t11 = al * n11 + be * gi11 + (p10 * gi01 + p11 * gi11);
+        const Real v1x = (Real)e1x, v1y = (Real)e1y, v1z = (Real)e1z;
+        const Real v2x = (Real)e2x, v2y = (Real)e2y, v2z = (Real)e2z;
+        const Real gab = sqrt(det), h = gab * (Real)0.5;
+        // load of the element's vertex en (stress.cu:204, shape-function gradients
+        // en 0 (-1,-1), 1 (1,0), 2 (0,1)): h (t^{a0} v1 + t^{a1} v2) for en = 1 (a = 0), 2 (a = 1)
+        const Real bx = h * (t00 * v1x + t01 * v2x), by = h * (t00 * v1y + t01 * v2y), bz = h * (t00 * v1z + t01 * v2z);
+        const Real cx = h * (t01 * v1x + t11 * v2x), cy = h * (t01 * v1y + t11 * v2y), cz = h * (t01 * v1z + t11 * v2z);
+        store_vec4(rec + (size_t)3 * e, make_vec4(-(bx + cx), -(by + cy), -(bz + cz), gab));
+        store_vec4(rec + (size_t)3 * e + 1, make_vec4(bx, by, bz, gab));
+        store_vec4(rec + (size_t)3 * e + 2, make_vec4(cx, cy, cz, gab));
+    }
+    __syncthreads();   // the records are written by this CTA and read below (plain loads, not __ldg)
+
+    // vertex pass: matrix row, right-hand side and nodal area of each vertex
     float rhs[VPT][3], ds[VPT];
 #pragma unroll
     for (int m = 0; m < VPT; m++) {
@@ -99,65 +182,24 @@ membrane_kernel(const MembraneArgs a)
         if (i >= V) continue;
         Real diag = 0, off[6] = {0, 0, 0, 0, 0, 0}, b0 = 0, b1 = 0, b2 = 0, dsum = 0;
         const int k0 = __ldg(&a.v2e_off[i]), k1 = __ldg(&a.v2e_off[i + 1]);
-        for (int k = k0; k < k1; k++) {
-            const int pk = __ldg(&a.v2e[k]);
-            const int e = v2e_elem(pk), en = v2e_en(pk);
-            const int ia = __ldg(&a.tri[3 * e]), ib = __ldg(&a.tri[3 * e + 1]), ic = __ldg(&a.tri[3 * e + 2]);
-            const double e1x = pos[ib] - pos[ia], e1y = pos[V + ib] - pos[V + ia], e1z = pos[2 * V + ib] - pos[2 * V + ia];
-            const double e2x = pos[ic] - pos[ia], e2y = pos[V + ic] - pos[V + ia], e2z = pos[2 * V + ic] - pos[2 * V + ia];
-            // deformed covariant metric (stress.cu:75-84) and its difference from the reference, in FP64
-            const double g11d = e1x * e1x + e1y * e1y + e1z * e1z;
-            const double g12d = e1x * e2x + e1y * e2y + e1z * e2z;
-            const double g22d = e2x * e2x + e2y * e2y + e2z * e2z;
-            // reference metric: covariant G (one aligned 32-byte record per element) and
-            // its inverse n, formed as set_contravariant does (init2.cu:241-249)
-            const double2 *gp = reinterpret_cast<const double2 *>(a.gref + eb + e);
-            const double2 Ga = __ldg(gp), Gb = __ldg(gp + 1);
-            const double G11 = Ga.x, G12 = Ga.y, G22 = Gb.x;
-            const double idG = 1.0 / (G11 * G22 - G12 * G12);
-            const double n00d = G22 * idG, n01d = -G12 * idG, n11d = G11 * idG;
-            const Real d11 = (Real)(g11d - G11), d12 = (Real)(g12d - G12), d22 = (Real)(g22d - G22);
-            const Real g11 = (Real)g11d, g12 = (Real)g12d, g22 = (Real)g22d;
-            const Real n00 = (Real)n00d, n01 = (Real)n01d, n11 = (Real)n11d;
-            const Real detn = (Real)idG;
-            const Real det = g11 * g22 - g12 * g12;
-            const Real idet = (Real)1 / det;
-            // invariants (stress.cu:90-93) from the metric difference
-            const Real i1 = n00 * d11 + (Real)2 * n01 * d12 + n11 * d22;
-            const Real i2 = detn * ((Real)G11 * d22 + (Real)G22 * d11 - (Real)2 * (Real)G12 * d12 + d11 * d22 - d12 * d12);
-            const Real js = sqrt(i2 + (Real)1);
-            const Real jsm1 = i2 / (js + (Real)1);
-            Real al, be;   // ca - 1 and cb + 1 of the law (stress.cu:94-99)
-            if (a.law == RBC_LAW_SKALAK) {
-                al = (rgs * i1 + (rgs - (Real)1) - jsm1) / js;
-                be = C * i2 * js - jsm1;
-            } else {
-                const Real js3 = js * js * js;
-                al = ((rgs - (Real)1) - jsm1) / js;
-                be = (jsm1 * (js * js + js + (Real)1) - (rgs - (Real)1)) / js3;
-            }
-            const Real gi00 = g22 * idet, gi01 = -g12 * idet, gi11 = g11 * idet;
-            // n D g^-1 = n - g^-1, symmetrised
-            const Real p00 = n00 * d11 + n01 * d12, p01 = n00 * d12 + n01 * d22;
-            const Real p10 = n01 * d11 + n11 * d12, p11 = n01 * d12 + n11 * d22;
-            const Real t00 = al * n00 + be * gi00 + (p00 * gi00 + p01 * gi01);
-            const Real t01 = al * n01 + be * gi01 + (Real)0.5 * ((p00 * gi01 + p01 * gi11) + (p10 * gi00 + p11 * gi01));
-            const Real t11 = al * n11 + be * gi11 + (p10 * gi01 + p11 * gi11);
-            const Real v1x = (Real)e1x, v1y = (Real)e1y, v1z = (Real)e1z;
-            const Real v2x = (Real)e2x, v2y = (Real)e2y, v2z = (Real)e2z;
-            const Real gab = sqrt(det);
+        // all incidence entries first, then all records, then the sums (in list order)
+        int pk[MAX_VALENCE];
+#pragma unroll
+        for (int j = 0; j < MAX_VALENCE; j++) pk[j] = k0 + j < k1 ? __ldg(&a.v2e[k0 + j]) : 0;
+        R4 r[MAX_VALENCE];
+#pragma unroll
+        for (int j = 0; j < MAX_VALENCE; j++)
+            if (k0 + j < k1) r[j] = load_vec4(rec + (size_t)3 * v2e_elem(pk[j]) + v2e_en(pk[j]));
+#pragma unroll
+        for (int j = 0; j < MAX_VALENCE; j++) {
+            if (k0 + j >= k1) break;
+            const int sa = v2e_sa(pk[j]), sb = v2e_sb(pk[j]);
+            const Real gab = r[j].w;
             diag += gab * (Real)(1.0 / 12.0);
             const Real o = gab * (Real)(1.0 / 24.0);
-            off[v2e_sa(pk)] += o;
-            off[v2e_sb(pk)] += o;
-            // shape-function gradients (stress.cu:204): en 0 (-1,-1), 1 (1,0), 2 (0,1)
-            const Real f0 = en == 1 ? (Real)1 : (en == 0 ? (Real)-1 : (Real)0);
-            const Real f1 = en == 2 ? (Real)1 : (en == 0 ? (Real)-1 : (Real)0);
-            const Real h = gab * (Real)0.5;
-            const Real c0 = h * (t00 * f0 + t01 * f1), c1 = h * (t01 * f0 + t11 * f1);
-            b0 += c0 * v1x + c1 * v2x;
-            b1 += c0 * v1y + c1 * v2y;
-            b2 += c0 * v1z + c1 * v2z;
+#pragma unroll
+            for (int t = 0; t < 6; t++) off[t] += (t == sa ? o : (Real)0) + (t == sb ? o : (Real)0);
+            b0 += r[j].x; b1 += r[j].y; b2 += r[j].z;
             dsum += gab * (Real)(1.0 / 6.0);
         }
         const Real idg = (Real)1 / diag;

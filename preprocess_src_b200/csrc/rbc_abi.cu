@@ -50,6 +50,7 @@ struct rbc_handle {
     // cells
     double *X = nullptr, *Xd = nullptr;
     double4 *gref = nullptr;
+    void *erec = nullptr;   // membrane element records, [ne][3] 4-vectors of float or double
     float *U = nullptr, *Fv = nullptr;
     int *tri = nullptr, *v2e_off = nullptr, *v2e = nullptr;
     int16_t *nbr = nullptr;
@@ -182,7 +183,7 @@ int build_topology(rbc_handle *h, const int *tri, std::vector<int> &off, std::ve
 }
 
 // The reference metric of set_contravariant (init2.cu:206-255) on the AoS
-// reference shape, kept in covariant form G [ne] (the kernel forms n = G^-1)
+// reference shape, kept in covariant form G [ne] with 1 / det G (the kernel forms n = G^-1)
 void reference_metric(const rbc_handle *h, const int *tri, const double *xr, std::vector<double4> &gref)
 {
     const long long ne = h->ne;
@@ -197,7 +198,7 @@ void reference_metric(const rbc_handle *h, const int *tri, const double *xr, std
             const double lv2 = v2[0] * v2[0] + v2[1] * v2[1] + v2[2] * v2[2];
             const double inv12 = v1[0] * v2[0] + v1[1] * v2[1] + v1[2] * v2[2];
             const long long id = (long long)c * h->E + e;
-            gref[id] = make_double4(lv1, inv12, lv2, 0.0);
+            gref[id] = make_double4(lv1, inv12, lv2, 1.0 / (lv1 * lv2 - inv12 * inv12));
         }
 }
 
@@ -332,7 +333,7 @@ void free_all(rbc_handle *h)
     if (!h) return;
     for (cudaGraphExec_t g : h->graph) if (g) cudaGraphExecDestroy(g);
     void *ptrs[] = {h->g[0], h->g[1], h->uvr, h->Fx, h->Fy, h->Fz, h->mask2d,
-                    h->X, h->Xd, h->gref, h->U, h->Fv, h->tri, h->v2e_off, h->v2e, h->nbr, h->patch_off, h->patch_vtx, h->patch_stride, h->vol0, h->gx,
+                    h->X, h->Xd, h->gref, h->erec, h->U, h->Fv, h->tri, h->v2e_off, h->v2e, h->nbr, h->patch_off, h->patch_vtx, h->patch_stride, h->vol0, h->gx,
                     h->vol_out, h->area_out, h->cen_out, h->d_int, h->d_drive, h->staging};
     for (void *q : ptrs) if (q) cudaFree(q);
     if (h->stream) cudaStreamDestroy(h->stream);
@@ -344,7 +345,7 @@ int launch_stress(rbc_handle *h)
 {
     if (h->ncell == 0) return RBC_OK;
     MembraneArgs a{};
-    a.Xd = h->Xd; a.nv = h->nv; a.ne = h->ne; a.gref = h->gref;
+    a.Xd = h->Xd; a.nv = h->nv; a.ne = h->ne; a.gref = h->gref; a.erec = h->erec;
     a.tri = h->tri; a.v2e_off = h->v2e_off; a.v2e = h->v2e; a.nbr = h->nbr; a.Fv = h->Fv;
     a.V = h->V; a.E = h->E; a.ncell = h->ncell;
     a.C = h->p.C; a.rgs = h->p.rgs; a.law = h->p.law; a.LX = h->p.LX; a.LZ = h->p.LZ;
@@ -584,6 +585,10 @@ int rbc_create(const rbc_params *p, const rbc_mesh *mesh, const int *bc, rbc_han
 
     if (cells) {
         TRY(dalloc(h, &h->X, 3 * h->nv)); TRY(dalloc(h, &h->Xd, 3 * h->nv)); TRY(dalloc(h, &h->gref, h->ne));
+        if (cudaMalloc(&h->erec, (size_t)h->ne * 12 * (p->membrane_fp64 ? sizeof(double) : sizeof(float))) != cudaSuccess) {
+            h->err = "out of device memory for the membrane element records";
+            return bail(RBC_ERR_CUDA);
+        }
         TRY(dalloc(h, &h->U, 3 * h->nv)); TRY(dalloc(h, &h->Fv, 3 * h->nv));
         TRY(dalloc(h, &h->tri, 3 * h->E)); TRY(dalloc(h, &h->v2e_off, h->V + 1)); TRY(dalloc(h, &h->v2e, packed.size()));
         TRY(dalloc(h, &h->nbr, 6 * h->V));
@@ -705,7 +710,7 @@ int rbc_import_ref_cells(rbc_handle *h, const double *x, const double *y, const 
         std::vector<double4> G(ne);
         for (long long e = 0; e < ne; e++) {
             const double n00 = nd[4 * e], n01 = nd[4 * e + 1], n11 = nd[4 * e + 3], det = n00 * n11 - n01 * n01;
-            G[e] = make_double4(n11 / det, -n01 / det, n00 / det, 0.0);
+            G[e] = make_double4(n11 / det, -n01 / det, n00 / det, det);   // G = n^-1, 1 / det G = det n
         }
         CK(cudaMemcpy(h->gref, G.data(), sizeof(double4) * ne, cudaMemcpyHostToDevice));
     }

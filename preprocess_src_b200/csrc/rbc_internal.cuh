@@ -124,7 +124,8 @@ void launch_advect(const Geom &g, const AdvectArgs &a, cudaStream_t s);
 
 struct MembraneArgs {
     const double *Xd; long long nv, ne;
-    const double4 *gref;      // [ne] reference covariant metric (G11, G12, G22, unused)
+    const double4 *gref;      // [ne] reference covariant metric (G11, G12, G22, 1 / det G)
+    void *erec;               // [ne][3] element records (Real 4-vectors): scratch written and read by each CTA
     const int *tri, *v2e_off, *v2e;
     const int16_t *nbr;       // [6][V] local neighbour ids, -1 = none
     float *Fv;
