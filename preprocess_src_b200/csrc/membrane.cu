@@ -280,7 +280,19 @@ static void launch_vpt(const MembraneArgs &a, cudaStream_t s)
     auto k = membrane_kernel<Real, VPT>;
     int T = (a.V + VPT - 1) / VPT;
     T = ((T + 31) / 32) * 32;
-    k<<<a.ncell, T, smem, s>>>(a);
+    // launched at the given stream priority: when the previous step's volume
+    // correction runs beside it, the membrane CTAs are dispatched first
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3((unsigned)a.ncell);
+    cfg.blockDim = dim3((unsigned)T);
+    cfg.dynamicSmemBytes = (size_t)smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributePriority;
+    attr[0].val.priority = a.priority;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, k, a);
 }
 
 template <typename Real>

@@ -63,7 +63,14 @@ struct rbc_handle {
     size_t staging_bytes = 0;
     int iter = 0;
     bool force_pending = false;
-    cudaGraphExec_t graph[2] = {nullptr, nullptr};   // one step starting from buffer 0 / buffer 1
+    // CUDA graphs of one step starting from population buffer 0 / 1, in three
+    // forms (StepForm): the whole step; the step without its volume
+    // correction; the step without its correction but with the previous
+    // step's correction beside its membrane pass
+    cudaGraphExec_t graph[3][2] = {{nullptr, nullptr}, {nullptr, nullptr}, {nullptr, nullptr}};
+    cudaStream_t side = nullptr;                      // second branch of the pipelined graphs (capture only)
+    cudaEvent_t fork = nullptr, join = nullptr;
+    int prio_high = 0;                                // greatest stream priority of the device
     long long launches = 0;
     float scale = 1.0f, inv_scale = 1.0f;
     std::string err;
@@ -331,7 +338,11 @@ int build_mask(const rbc_params *p, const int *bc, std::vector<uint32_t> &mask)
 void free_all(rbc_handle *h)
 {
     if (!h) return;
-    for (cudaGraphExec_t g : h->graph) if (g) cudaGraphExecDestroy(g);
+    for (auto &form : h->graph)
+        for (cudaGraphExec_t g : form) if (g) cudaGraphExecDestroy(g);
+    if (h->fork) cudaEventDestroy(h->fork);
+    if (h->join) cudaEventDestroy(h->join);
+    if (h->side) cudaStreamDestroy(h->side);
     void *ptrs[] = {h->g[0], h->g[1], h->uvr, h->Fx, h->Fy, h->Fz, h->mask2d,
                     h->X, h->Xd, h->gref, h->erec, h->U, h->Fv, h->tri, h->v2e_off, h->v2e, h->nbr, h->patch_off, h->patch_vtx, h->patch_stride, h->vol0, h->gx,
                     h->vol_out, h->area_out, h->cen_out, h->d_int, h->d_drive, h->staging};
@@ -351,6 +362,7 @@ int launch_stress(rbc_handle *h)
     a.C = h->p.C; a.rgs = h->p.rgs; a.law = h->p.law; a.LX = h->p.LX; a.LZ = h->p.LZ;
     a.niter = h->p.solver_iters > 0 ? h->p.solver_iters : DEFAULT_SOLVER_ITERS;
     a.flags = h->d_flags();
+    a.priority = h->prio_high;
     launch_membrane(a, h->p.membrane_fp64 != 0, h->stream);
     h->launches++;
     CK_LAUNCH();
@@ -409,49 +421,65 @@ VolumeArgs volume_args(rbc_handle *h, int correct)
     return a;
 }
 
-int launch_volume_stage(rbc_handle *h)
+int launch_volume_stage(rbc_handle *h, cudaStream_t st)
 {
     if (h->ncell == 0) return RBC_OK;
-    CK(cudaMemsetAsync(h->d_vclast(), 0, sizeof(int), h->stream));
-    launch_volume(h->geo, volume_args(h, 1), h->stream);
+    CK(cudaMemsetAsync(h->d_vclast(), 0, sizeof(int), st));
+    launch_volume(h->geo, volume_args(h, 1), st);
     h->launches++;
     CK_LAUNCH();
     return RBC_OK;
 }
 
-// one full step (main.cu:73-110 with M = 1); the device increments iter
-int enqueue_step(rbc_handle *h)
+enum StepForm { STEP_WHOLE = 0, STEP_BODY = 1, STEP_PIPELINED = 2 };
+
+// one step (main.cu:73-110 with M = 1); the device increments iter.
+// STEP_BODY leaves out the step's volume correction; STEP_PIPELINED also runs
+// the previous step's correction on a second branch beside step_begin +
+// membrane (the membrane pass reads fem->xd, which the correction does not
+// touch; the correction writes cel->x, which the spread reads, so the
+// branches join before the spread).
+int enqueue_step(rbc_handle *h, StepForm form = STEP_WHOLE)
 {
     int rc;
+    const bool pipelined = form == STEP_PIPELINED;
+    if (pipelined) {
+        CK(cudaEventRecord(h->fork, h->stream));
+        CK(cudaStreamWaitEvent(h->side, h->fork, 0));
+        if ((rc = launch_volume_stage(h, h->side))) return rc;
+        CK(cudaEventRecord(h->join, h->side));
+    }
     launch_step_begin(h->d_iter(), h->d_drive, h->p.P, h->p.flowstart, h->p.freq, h->p.dt, h->stream);
     h->launches++;
     CK_LAUNCH();
     if ((rc = launch_stress(h))) return rc;
+    if (pipelined) CK(cudaStreamWaitEvent(h->stream, h->join, 0));
     if ((rc = launch_spread_stage(h))) return rc;
     if ((rc = launch_lbm_stage(h))) return rc;
     if ((rc = launch_advect_stage(h))) return rc;
-    if ((rc = launch_volume_stage(h))) return rc;
+    if (form == STEP_WHOLE && (rc = launch_volume_stage(h, h->stream))) return rc;
     return RBC_OK;
 }
 
 // CUDA graph of one step starting from population buffer c (the step flips
 // the buffers, so two graphs alternate)
-int build_graph(rbc_handle *h, int c)
+int build_graph(rbc_handle *h, int c, StepForm form)
 {
     cudaGraph_t graph = nullptr;
     const long long launches0 = h->launches;
     const int cur0 = h->cur;
     h->cur = c;
     CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-    int rc = enqueue_step(h);
+    int rc = enqueue_step(h, form);
     cudaError_t e = cudaStreamEndCapture(h->stream, &graph);
     h->launches = launches0;
     h->cur = cur0;
     if (rc != RBC_OK) { if (graph) cudaGraphDestroy(graph); return rc; }
     if (e != cudaSuccess) { h->err = std::string("graph capture: ") + cudaGetErrorString(e); return RBC_ERR_CUDA; }
-    e = cudaGraphInstantiate(&h->graph[c], graph, 0);
+    cudaGraphExec_t &exec = h->graph[form][c];
+    e = cudaGraphInstantiate(&exec, graph, 0);
     cudaGraphDestroy(graph);
-    if (e != cudaSuccess) { h->graph[c] = nullptr; h->err = std::string("graph instantiate: ") + cudaGetErrorString(e); return RBC_ERR_CUDA; }
+    if (e != cudaSuccess) { exec = nullptr; h->err = std::string("graph instantiate: ") + cudaGetErrorString(e); return RBC_ERR_CUDA; }
     return RBC_OK;
 }
 
@@ -560,9 +588,17 @@ int rbc_create(const rbc_params *p, const rbc_mesh *mesh, const int *bc, rbc_han
             return bail(RBC_ERR_UNSUPPORTED);
         }
     }
-    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
-        h->err = "stream creation failed";
-        return bail(RBC_ERR_CUDA);
+    {
+        int lo = 0, hi = 0;
+        if (cudaDeviceGetStreamPriorityRange(&lo, &hi) != cudaSuccess ||
+            cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&h->fork, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&h->join, cudaEventDisableTiming) != cudaSuccess) {
+            h->err = "stream creation failed";
+            return bail(RBC_ERR_CUDA);
+        }
+        h->prio_high = hi;   // numerically lowest value = greatest priority
     }
     const size_t esz = p->storage == RBC_STORE_F16 ? 2 : 4;
     h->gbytes = esz * (size_t)Q * (size_t)g.nint;
@@ -831,7 +867,7 @@ int rbc_volume_correction(rbc_handle *h, int *iters)
 {
     if (!h) return RBC_ERR_ARG;
     RBC_DEVICE_GUARD(h);
-    int rc = launch_volume_stage(h);
+    int rc = launch_volume_stage(h, h->stream);
     if (rc) return rc;
     if (iters) {
         int v = 0;
@@ -851,12 +887,24 @@ int rbc_step(rbc_handle *h, int nsteps)
     if (nsteps == 0) return RBC_OK;
     int rc;
     if ((rc = prepare_steps(h))) return rc;
-    for (int c = 0; c < 2; c++)
-        if (!h->graph[c] && (rc = build_graph(h, c))) return rc;
+    // one step, or no cells: whole steps.  Otherwise step 1 without its
+    // correction, steps 2..n pipelined with the correction of the step before,
+    // then the correction of step n: the same kernels in the same data order.
+    const bool pipe = nsteps > 1 && h->ncell > 0;
+    for (int c = 0; c < 2; c++) {
+        if (!h->graph[STEP_WHOLE][c] && (rc = build_graph(h, c, STEP_WHOLE))) return rc;
+        if (pipe && !h->graph[STEP_BODY][c] && (rc = build_graph(h, c, STEP_BODY))) return rc;
+        if (pipe && !h->graph[STEP_PIPELINED][c] && (rc = build_graph(h, c, STEP_PIPELINED))) return rc;
+    }
     for (int k = 0; k < nsteps; k++) {
-        CK(cudaGraphLaunch(h->graph[h->cur], h->stream));
+        const StepForm form = !pipe ? STEP_WHOLE : k == 0 ? STEP_BODY : STEP_PIPELINED;
+        CK(cudaGraphLaunch(h->graph[form][h->cur], h->stream));
         h->cur ^= 1;
         h->launches += KERNELS_PER_STEP;
+    }
+    if (pipe) {
+        h->launches -= 1;   // step n's correction, counted with its step, is launched here
+        if ((rc = launch_volume_stage(h, h->stream))) return rc;
     }
     h->iter += nsteps;
     return RBC_OK;
@@ -884,7 +932,7 @@ int rbc_profile_steps(rbc_handle *h, int nsteps, double *kernel_ms)
         cudaEventRecord(ev[4], h->stream);
         if (!rc) rc = launch_advect_stage(h);
         cudaEventRecord(ev[5], h->stream);
-        if (!rc) rc = launch_volume_stage(h);
+        if (!rc) rc = launch_volume_stage(h, h->stream);
         cudaEventRecord(ev[6], h->stream);
         if (cudaEventSynchronize(ev[6]) != cudaSuccess) { rc = RBC_ERR_CUDA; h->err = "profiled step failed"; break; }
         for (int k = 0; k < RBC_NUM_KERNELS; k++) {

@@ -134,6 +134,7 @@ struct MembraneArgs {
     double LX, LZ;
     int niter;
     int *flags;
+    int priority;             // launch priority (cudaLaunchAttributePriority)
 };
 int  membrane_smem_bytes(int V);
 void launch_membrane(const MembraneArgs &a, bool fp64, cudaStream_t s);

@@ -268,6 +268,28 @@ def test_stage_calls_equal_graph_step(developed):
     assert np.abs(ca["z"] - cb["z"]).max() <= 1e-10
 
 
+def test_multi_step_call_equals_stage_calls(developed):
+    """rbc_step(h, 3) runs step 1 without its volume correction, steps 2 and 3
+    with the previous step's correction beside their membrane pass, then the
+    last correction; the result must be that of three stage-by-stage steps."""
+    case, o = developed
+    a = load(o)
+    b = load(o)
+    a.step(3)
+    for _ in range(3):
+        b.iter = b.iter + 1
+        b.stress(); b.ibm_st1(); b.lbm_d3q19(); b.ibm_st2(); b.volume_correction()
+    assert a.iter == b.iter
+    ea, eb = a.export_lattice(fn=False), b.export_lattice(fn=False)
+    m = comp(case)
+    assert np.abs(ea["wn"][m] - eb["wn"][m]).max() <= 1e-9
+    ca, cb = a.export_cells(), b.export_cells()
+    for k in ("x", "y", "z", "xd"):
+        assert np.abs(ca[k] - cb[k]).max() <= 1e-10, k
+    assert np.abs(ca["fx"] - cb["fx"]).max() <= 1e-6 * np.abs(cb["fx"]).max()
+    assert a.status() == b.status()
+
+
 def test_launch_count_and_status(developed):
     case, o = developed
     sim = load(o)
