@@ -299,60 +299,159 @@ __device__ __forceinline__ void contract(const Plane16 &P, const float wx[4], co
 }
 
 constexpr int ADVECT_THREADS = 256;
+constexpr int ADVECT_MAX_PATCH = MAX_PATCH_VERTICES;
+constexpr int ADVECT_BOX_BYTES = 48 * 1024;
+constexpr int ADVECT_BOX_CAP = ADVECT_BOX_BYTES / (int)sizeof(float4);
+constexpr int ADVECT_SMEM = ADVECT_BOX_BYTES + ADVECT_MAX_PATCH * (3 * (int)sizeof(double) + (int)sizeof(int));
 
+// Stage-1 stencil plane of one lane from the patch's shared-memory box; false
+// when the plane is not inside the box (the caller then gathers from global
+// memory).  (xi, yi, zi) = stencil corner relative to the box origin.
+__device__ __forceinline__ bool box_plane(const float4 *box, int bxs, int bys, int bzs, int xi, int yi, int zi,
+                                          bool zin, Plane16 &P)
+{
+    if (xi < 0 || xi + 3 >= bxs || yi < 0 || yi + 3 >= bys || zi < 0 || zi >= bzs) return false;
+    const float4 *row = box + ((long long)zi * bys + yi) * bxs + xi;
+#pragma unroll
+    for (int b = 0; b < 4; b++)
+#pragma unroll
+        for (int a = 0; a < 4; a++) {
+            const float4 q = zin ? row[b * bxs + a] : make_float4(0.f, 0.f, 0.f, 0.f);
+            P.u[4 * b + a] = q.x; P.v[4 * b + a] = q.y; P.w[4 * b + a] = q.z;
+        }
+    return true;
+}
+
+// One CTA per (cell, surface patch), as for the spread.  The CTA loads the
+// lattice box of its patch's stage-1 stencils, widened by one node on every
+// side for the later RK stages, into shared memory with coalesced row reads,
+// so a stencil gather is 16 shared-memory reads instead of 16 scattered L1/L2
+// reads.  Box nodes outside the lattice in x or y hold 0 (the reference reads
+// nothing there); z wraps periodically, and nodes beyond the two BUFF planes
+// of the vertex's own (unwrapped) frame are dropped per vertex as
+// ibm.cu:453-455 does.  A box larger than ADVECT_SMEM, or a later-stage
+// stencil outside the box, gathers from global memory instead.
 __global__ void __launch_bounds__(ADVECT_THREADS)
 advect_kernel(const Geom g, double *__restrict__ X, double *__restrict__ Xd, float *__restrict__ U,
-              const float4 *__restrict__ uvr, long long nv, double dtM, int *__restrict__ flags)
+              const float4 *__restrict__ uvr, long long nv, int V, const int *__restrict__ patch_off,
+              const int *__restrict__ patch_vtx, int npatch, double dtM, int *__restrict__ flags)
 {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const int c = (int)(t & 3);
-    const bool live = (t >> 2) < nv;
-    const long long j = live ? (t >> 2) : nv - 1;   // idle lanes shadow the last vertex for the shuffles
-    const double xn = X[j], yn = X[nv + j], zn = X[2 * nv + j];
-    Plane16 P;
-    int bx, by, bz;
-    float fx, fy, fz, wx[4], wy[4], wz[4];
-    lattice_cell(g, xn, yn, zn, bx, by, bz, fx, fy, fz);
-    gather_plane(g, uvr, bx, by, bz + c, P);
-    float us[4], vs[4], ws[4];
-#pragma unroll
-    for (int k = 0; k < 4; k++) {
-        double px = xn, py = yn, pz = zn;
-        if (k > 0) {
-            const double h = (k < 3 ? 0.5 : 1.0) * dtM;   // ibm.cu:474-498
-            px += us[k - 1] * h; py += vs[k - 1] * h; pz += ws[k - 1] * h;
-            int cx, cy, cz;
-            lattice_cell(g, px, py, pz, cx, cy, cz, fx, fy, fz);
-            if (cx != bx || cy != by || cz != bz) {   // uniform across the 4 lanes of the vertex
-                bx = cx; by = cy; bz = cz;
-                gather_plane(g, uvr, bx, by, bz + c, P);
-            }
-        }
-        delta4(fx, wx); delta4(fy, wy); delta4(fz, wz);
-        const float wzc = c == 0 ? wz[0] : c == 1 ? wz[1] : c == 2 ? wz[2] : wz[3];
-        contract(P, wx, wy, wzc, us[k], vs[k], ws[k]);
+    extern __shared__ float4 abox[];   // [ADVECT_BOX_CAP] box, then the patch's positions and vertex ids
+    double *spos = reinterpret_cast<double *>(abox + ADVECT_BOX_CAP);   // [3][ADVECT_MAX_PATCH]
+    int *svid = reinterpret_cast<int *>(spos + 3 * ADVECT_MAX_PATCH);    // [ADVECT_MAX_PATCH]
+    __shared__ int s_lo[3], s_hi[3];
+    const int cell = blockIdx.x / npatch, patch = blockIdx.x - cell * npatch, tid = threadIdx.x;
+    const int p0 = patch_off[patch], np = patch_off[patch + 1] - p0;
+    const long long vb = (long long)cell * V;
+    const double *xs = X + vb, *ys = X + nv + vb, *zs = X + 2 * nv + vb;
+    const double az = lat_z(g, zs[0]);   // one anchor per cell: every patch unwraps z the same way
+
+    if (tid < 3) { s_lo[tid] = INT_MAX; s_hi[tid] = INT_MIN; }
+    __syncthreads();
+    int lo0 = INT_MAX, lo1 = INT_MAX, lo2 = INT_MAX, hi0 = INT_MIN, hi1 = INT_MIN, hi2 = INT_MIN;
+    for (int k = tid; k < np; k += ADVECT_THREADS) {
+        const int v = patch_vtx[p0 + k];
+        const double px = xs[v], py = ys[v], pz = zs[v];
+        svid[k] = v; spos[k] = px; spos[ADVECT_MAX_PATCH + k] = py; spos[2 * ADVECT_MAX_PATCH + k] = pz;
+        const int ix = (int)floor(lat_x(g, px)), iy = (int)floor(lat_y(g, py));
+        const int iz = (int)floor(unwrap_near(lat_z(g, pz), az, g.nzc));
+        lo0 = min(lo0, ix - 2); hi0 = max(hi0, ix + 3);
+        lo1 = min(lo1, iy - 2); hi1 = max(hi1, iy + 3);
+        lo2 = min(lo2, iz - 2); hi2 = max(hi2, iz + 3);
     }
-    if (!live || c != 0) return;
-    const double um = ((double)us[0] + 2.0 * us[1] + 2.0 * us[2] + us[3]) / 6.0;
-    const double vm = ((double)vs[0] + 2.0 * vs[1] + 2.0 * vs[2] + vs[3]) / 6.0;
-    const double wm = ((double)ws[0] + 2.0 * ws[1] + 2.0 * ws[2] + ws[3]) / 6.0;
-    double xr = xn + um * dtM, yr = yn + vm * dtM, zr = zn + wm * dtM;
-    if (xr < g.xmin) xr += g.LX;   // ibm.cu:629-632
-    if (xr > g.xmax) xr -= g.LX;
-    if (zr < g.zmin) zr += g.LZ;
-    if (zr > g.zmax) zr -= g.LZ;
-    if (!isfinite(xr) || !isfinite(yr) || !isfinite(zr)) atomicOr(flags, RBC_FLAG_NONFINITE);
-    X[j] = xr; X[nv + j] = yr; X[2 * nv + j] = zr;
-    Xd[j] = xr; Xd[nv + j] = yr; Xd[2 * nv + j] = zr;
-    U[j] = (float)um; U[nv + j] = (float)vm; U[2 * nv + j] = (float)wm;
+    atomicMin(&s_lo[0], lo0); atomicMin(&s_lo[1], lo1); atomicMin(&s_lo[2], lo2);
+    atomicMax(&s_hi[0], hi0); atomicMax(&s_hi[1], hi1); atomicMax(&s_hi[2], hi2);
+    __syncthreads();
+    const int bx0 = s_lo[0], by0 = s_lo[1], bz0 = s_lo[2];
+    const long long bxl = (long long)s_hi[0] - bx0 + 1, byl = (long long)s_hi[1] - by0 + 1, bzl = (long long)s_hi[2] - bz0 + 1;
+    const bool use_box = np > 0 && bxl * byl * bzl <= ADVECT_BOX_CAP;
+    const int bxs = use_box ? (int)bxl : 0, bys = use_box ? (int)byl : 0, bzs = use_box ? (int)bzl : 0;
+    if (use_box) {
+        // node li = (z * bys + y) * bxs + x; each thread steps li by ADVECT_THREADS
+        const int nb = bxs * bys * bzs;
+        int x = tid % bxs, y = (tid / bxs) % bys, z = tid / (bxs * bys);
+        const int sx = ADVECT_THREADS % bxs, sy = (ADVECT_THREADS / bxs) % bys, sz = ADVECT_THREADS / (bxs * bys);
+        for (int li = tid; li < nb; li += ADVECT_THREADS) {
+            const int gx = bx0 + x, gy = by0 + y;
+            float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (gx >= 0 && gx < g.nx && gy >= 0 && gy < g.ny)
+                q = __ldg(&uvr[(long long)wrap_z(bz0 + z, g.nzc) * g.plane + gx + (long long)g.nx * gy]);
+            abox[li] = q;
+            x += sx; y += sy; z += sz;
+            if (x >= bxs) { x -= bxs; y++; }
+            if (y >= bys) { y -= bys; z++; }
+        }
+    }
+    __syncthreads();
+
+    // four lanes per vertex (lane c owns stencil plane c), 64 vertices per pass;
+    // every lane of a warp runs the same passes (shuffles), idle lanes shadow vertex 0
+    const int c = tid & 3;
+    const int npass = (np + ADVECT_THREADS / 4 - 1) / (ADVECT_THREADS / 4);
+    for (int pass = 0; pass < npass; pass++) {
+        const int j = pass * (ADVECT_THREADS / 4) + (tid >> 2);
+        const bool live = j < np;
+        const int jj = live ? j : 0;
+        const long long vj = vb + svid[jj];
+        const double xn = spos[jj], yn = spos[ADVECT_MAX_PATCH + jj], zn = spos[2 * ADVECT_MAX_PATCH + jj];
+        Plane16 P;
+        int bx, by, bz;
+        float fx, fy, fz, wx[4], wy[4], wz[4];
+        lattice_cell(g, xn, yn, zn, bx, by, bz, fx, fy, fz);
+        // shift from the raw z frame to the cell's unwrapped frame (a multiple of nzc)
+        const double lzr = lat_z(g, zn);
+        const int zsh = (int)lrint(unwrap_near(lzr, az, g.nzc) - lzr);
+        auto fetch = [&](int cx, int cy, int cz) {
+            const int izr = cz + c;
+            const bool zin = izr >= -2 && izr < g.nzc + 2;   // beyond the BUFF planes (ibm.cu:453-455)
+            if (!use_box || !box_plane(abox, bxs, bys, bzs, cx - bx0, cy - by0, izr + zsh - bz0, zin, P))
+                gather_plane(g, uvr, cx, cy, izr, P);
+        };
+        fetch(bx, by, bz);
+        float us[4], vs[4], ws[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            double px = xn, py = yn, pz = zn;
+            if (k > 0) {
+                const double h = (k < 3 ? 0.5 : 1.0) * dtM;   // ibm.cu:474-498
+                px += us[k - 1] * h; py += vs[k - 1] * h; pz += ws[k - 1] * h;
+                int cx, cy, cz;
+                lattice_cell(g, px, py, pz, cx, cy, cz, fx, fy, fz);
+                if (cx != bx || cy != by || cz != bz) {   // uniform across the 4 lanes of the vertex
+                    bx = cx; by = cy; bz = cz;
+                    fetch(bx, by, bz);
+                }
+            }
+            delta4(fx, wx); delta4(fy, wy); delta4(fz, wz);
+            const float wzc = c == 0 ? wz[0] : c == 1 ? wz[1] : c == 2 ? wz[2] : wz[3];
+            contract(P, wx, wy, wzc, us[k], vs[k], ws[k]);
+        }
+        if (!live || c != 0) continue;
+        const double um = ((double)us[0] + 2.0 * us[1] + 2.0 * us[2] + us[3]) / 6.0;
+        const double vm = ((double)vs[0] + 2.0 * vs[1] + 2.0 * vs[2] + vs[3]) / 6.0;
+        const double wm = ((double)ws[0] + 2.0 * ws[1] + 2.0 * ws[2] + ws[3]) / 6.0;
+        double xr = xn + um * dtM, yr = yn + vm * dtM, zr = zn + wm * dtM;
+        if (xr < g.xmin) xr += g.LX;   // ibm.cu:629-632
+        if (xr > g.xmax) xr -= g.LX;
+        if (zr < g.zmin) zr += g.LZ;
+        if (zr > g.zmax) zr -= g.LZ;
+        if (!isfinite(xr) || !isfinite(yr) || !isfinite(zr)) atomicOr(flags, RBC_FLAG_NONFINITE);
+        X[vj] = xr; X[nv + vj] = yr; X[2 * nv + vj] = zr;
+        Xd[vj] = xr; Xd[nv + vj] = yr; Xd[2 * nv + vj] = zr;
+        U[vj] = (float)um; U[nv + vj] = (float)vm; U[2 * nv + vj] = (float)wm;
+    }
+}
+
+cudaError_t advect_setup()
+{
+    return cudaFuncSetAttribute(advect_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, ADVECT_SMEM);
 }
 
 void launch_advect(const Geom &g, const AdvectArgs &a, cudaStream_t s)
 {
-    if (a.nv <= 0) return;
-    const long long threads = 4 * a.nv;
-    advect_kernel<<<(unsigned)((threads + ADVECT_THREADS - 1) / ADVECT_THREADS), ADVECT_THREADS, 0, s>>>(
-        g, a.X, a.Xd, a.U, a.uvr, a.nv, a.dtM, a.flags);
+    if (a.ncell <= 0) return;
+    advect_kernel<<<a.ncell * a.npatch, ADVECT_THREADS, ADVECT_SMEM, s>>>(
+        g, a.X, a.Xd, a.U, a.uvr, a.nv, a.V, a.patch_off, a.patch_vtx, a.npatch, a.dtM, a.flags);
 }
 
 }  // namespace rbc

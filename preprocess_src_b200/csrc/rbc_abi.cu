@@ -248,7 +248,6 @@ void initial_volume(const rbc_handle *h, const int *tri, const double *xr, std::
 // 0.618 of its size and coprime with it, that scatters neighbours across lanes.
 void surface_patches(int V, const double *xr, std::vector<int> &off, std::vector<int> &vtx, std::vector<int> &stride)
 {
-    constexpr int kMaxPatch = 512;
     vtx.resize(V);
     for (int i = 0; i < V; i++) vtx[i] = i;
     off.assign(1, 0);
@@ -257,7 +256,7 @@ void surface_patches(int V, const double *xr, std::vector<int> &off, std::vector
     while (!stack.empty()) {
         auto [b, e] = stack.back();
         stack.pop_back();
-        if (e - b <= kMaxPatch) { leaves.push_back({b, e}); continue; }
+        if (e - b <= MAX_PATCH_VERTICES) { leaves.push_back({b, e}); continue; }
         double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
         for (int k = b; k < e; k++)
             for (int d = 0; d < 3; d++) { lo[d] = std::min(lo[d], xr[3 * vtx[k] + d]); hi[d] = std::max(hi[d], xr[3 * vtx[k] + d]); }
@@ -403,6 +402,7 @@ int launch_advect_stage(rbc_handle *h)
     if (h->ncell == 0) return RBC_OK;
     AdvectArgs a{};
     a.X = h->X; a.Xd = h->Xd; a.U = h->U; a.uvr = h->uvr; a.nv = h->nv;
+    a.V = h->V; a.ncell = h->ncell; a.patch_off = h->patch_off; a.patch_vtx = h->patch_vtx; a.npatch = h->npatch;
     a.dtM = h->p.dt * h->p.M; a.flags = h->d_flags();
     launch_advect(h->geo, a, h->stream);
     h->launches++;

@@ -101,6 +101,9 @@ void launch_export_force(const Geom &g, const float *Fx, const float *Fy, const 
 void launch_fill_f32(float *p, long long n, float v, cudaStream_t s);
 void launch_fill_f4(float4 *p, long long n, float4 v, cudaStream_t s);
 
+// Surface patches (spread and advection work units) hold at most this many vertices.
+constexpr int MAX_PATCH_VERTICES = 512;
+
 struct SpreadArgs {
     const double *X; long long nv; int V, ncell;
     const int *patch_off, *patch_vtx, *patch_stride;   // surface patches of the shared mesh
@@ -117,6 +120,9 @@ struct AdvectArgs {
     double *X, *Xd; float *U;
     const float4 *uvr;
     long long nv;
+    int V, ncell;
+    const int *patch_off, *patch_vtx;   // surface patches of the shared mesh
+    int npatch;
     double dtM;                // dt * M
     int *flags;
 };
