@@ -93,8 +93,12 @@ __device__ __forceinline__ double4 load_vec4(const double4 *p) {
 
 constexpr int MAX_VALENCE = 6;   // checked when the topology is built
 
+// threads per CTA for VPT vertices per thread: at most 896 for VPT >= 3 (72
+// registers a thread), 1024 otherwise
+template <int VPT> constexpr int mem_max_threads() { return VPT >= 3 ? 896 : MEM_MAX_THREADS; }
+
 template <typename Real, int VPT>
-__global__ void __launch_bounds__(MEM_MAX_THREADS, 1)
+__global__ void __launch_bounds__(mem_max_threads<VPT>(), 1)
 membrane_kernel(const MembraneArgs a)
 {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -223,6 +227,22 @@ membrane_kernel(const MembraneArgs a)
         }
         if (i < V) dbuf[i] = make_float4(d[m][0], d[m][1], d[m][2], 0.f);
     }
+    // each vertex's neighbours and row coefficients stay in registers for the
+    // whole solve (a missing sixth neighbour points at the vertex itself with
+    // coefficient 0)
+    unsigned nb[VPT][3];   // two 16-bit neighbour ids per register
+    float cf[VPT][6];
+#pragma unroll
+    for (int m = 0; m < VPT; m++) {
+        const int i = tid + m * T;
+#pragma unroll
+        for (int s = 0; s < 6; s++) {
+            const int j = i < V ? snbr[s * V + i] : -1;
+            const unsigned id = (unsigned)(j >= 0 ? j : (i < V ? i : 0));
+            if (s & 1) nb[m][s >> 1] |= id << 16; else nb[m][s >> 1] = id;
+            cf[m][s] = j >= 0 ? coef[s * V + i] : 0.f;
+        }
+    }
     __syncthreads();
     for (int it = 0; it < a.niter; it++) {
         const float4 *cur = dbuf + (it & 1) * V;
@@ -236,12 +256,9 @@ membrane_kernel(const MembraneArgs a)
             float ad0 = d[m][0], ad1 = d[m][1], ad2 = d[m][2];
 #pragma unroll
             for (int s = 0; s < 6; s++) {
-                const int j = snbr[s * V + i];
-                if (j >= 0) {
-                    const float w = coef[s * V + i];
-                    const float4 dj = cur[j];
-                    ad0 += w * dj.x; ad1 += w * dj.y; ad2 += w * dj.z;
-                }
+                const float w = cf[m][s];
+                const float4 dj = cur[(s & 1) ? nb[m][s >> 1] >> 16 : nb[m][s >> 1] & 0xFFFFu];
+                ad0 += w * dj.x; ad1 += w * dj.y; ad2 += w * dj.z;
             }
             x[m][0] += d[m][0]; x[m][1] += d[m][1]; x[m][2] += d[m][2];
             r[m][0] -= ad0; r[m][1] -= ad1; r[m][2] -= ad2;
@@ -298,13 +315,12 @@ static void launch_vpt(const MembraneArgs &a, cudaStream_t s)
 template <typename Real>
 static void launch_real(const MembraneArgs &a, cudaStream_t s)
 {
-    const int vpt = (a.V + MEM_MAX_THREADS - 1) / MEM_MAX_THREADS;
-    switch (vpt) {
-    case 1: launch_vpt<Real, 1>(a, s); break;
-    case 2: launch_vpt<Real, 2>(a, s); break;
-    case 3: launch_vpt<Real, 3>(a, s); break;
-    default: launch_vpt<Real, 4>(a, s); break;
-    }
+    // fewest vertices per thread whose CTA (rounded to warps) fits the thread cap
+    auto fits = [&](int vpt, int cap) { return ((a.V + vpt - 1) / vpt + 31) / 32 * 32 <= cap; };
+    if (fits(1, mem_max_threads<1>())) launch_vpt<Real, 1>(a, s);
+    else if (fits(2, mem_max_threads<2>())) launch_vpt<Real, 2>(a, s);
+    else if (fits(3, mem_max_threads<3>())) launch_vpt<Real, 3>(a, s);
+    else launch_vpt<Real, 4>(a, s);   // V <= 3418 (shared-memory limit) fits 4 x 896
 }
 
 cudaError_t set_max_dyn_smem(const void *kernel, int optin, int *granted);
