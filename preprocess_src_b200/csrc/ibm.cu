@@ -27,6 +27,11 @@ constexpr int SPREAD_BOX_CAP = SPREAD_SMEM / (3 * (int)sizeof(unsigned));
 
 int spread_smem_bytes() { return SPREAD_SMEM; }
 
+// A lattice coordinate that the box arithmetic can take: finite and within
+// 2^24 nodes (positions outside are a blown-up state; they raise
+// RBC_FLAG_NONFINITE instead of indexing anything).
+__device__ __forceinline__ bool sane_lattice(double l) { return fabs(l) < 16777216.0; }
+
 __device__ __forceinline__ double unwrap_near(double l, double ref, int n) {
     const double h = 0.5 * n;
     if (l - ref > h) l -= n; else if (l - ref < -h) l += n;
@@ -68,8 +73,10 @@ spread_kernel(const Geom g, const double *__restrict__ X, long long nv, int V,
         const float afx = fabsf(fxs[v]), afy = fabsf(fys[v]), afz = fabsf(fzs[v]);
         nonfinite |= !(afx <= FLT_MAX && afy <= FLT_MAX && afz <= FLT_MAX);
         fmax0 = fmaxf(fmax0, afx); fmax1 = fmaxf(fmax1, afy); fmax2 = fmaxf(fmax2, afz);
-        const int ix = (int)floor(lat_x(g, xs[v])), iy = (int)floor(lat_y(g, ys[v]));
-        const int iz = (int)floor(unwrap_near(lat_z(g, zs[v]), az, g.nzc));
+        const double lxv = lat_x(g, xs[v]), lyv = lat_y(g, ys[v]), lzv = unwrap_near(lat_z(g, zs[v]), az, g.nzc);
+        if (!(sane_lattice(lxv) && sane_lattice(lyv) && sane_lattice(lzv) && sane_lattice(az))) { nonfinite = true; continue; }
+        const int ix = (int)floor(lxv), iy = (int)floor(lyv);
+        const int iz = (int)floor(lzv);
         lo0 = min(lo0, ix - 1); hi0 = max(hi0, ix + 2);
         lo1 = min(lo1, iy - 1); hi1 = max(hi1, iy + 2);
         lo2 = min(lo2, iz - 1); hi2 = max(hi2, iz + 2);
@@ -89,7 +96,7 @@ spread_kernel(const Geom g, const double *__restrict__ X, long long nv, int V,
     const int bx = s_hi[0] - bx0 + 1, by = s_hi[1] - by0 + 1, bz = s_hi[2] - bz0 + 1;
     const long long ps = (((long long)bx * by + 31) & ~31LL) + 8;   // plane stride = 8 (mod 32)
     const long long nb = ps * bz;
-    const bool use_box = nb <= SPREAD_BOX_CAP;
+    const bool use_box = bx >= 4 && by >= 4 && bz >= 4 && nb <= SPREAD_BOX_CAP;
     if (!use_box && tid == 0) atomicOr(flags, RBC_FLAG_SPREAD_OVERFLOW);
     const int psi = use_box ? (int)ps : 0, nbi = use_box ? (int)nb : 0;   // box indices fit in int
 
@@ -349,22 +356,28 @@ advect_kernel(const Geom g, double *__restrict__ X, double *__restrict__ Xd, flo
     if (tid < 3) { s_lo[tid] = INT_MAX; s_hi[tid] = INT_MIN; }
     __syncthreads();
     int lo0 = INT_MAX, lo1 = INT_MAX, lo2 = INT_MAX, hi0 = INT_MIN, hi1 = INT_MIN, hi2 = INT_MIN;
+    bool bad = false;
     for (int k = tid; k < np; k += ADVECT_THREADS) {
         const int v = patch_vtx[p0 + k];
         const double px = xs[v], py = ys[v], pz = zs[v];
         svid[k] = v; spos[k] = px; spos[ADVECT_MAX_PATCH + k] = py; spos[2 * ADVECT_MAX_PATCH + k] = pz;
-        const int ix = (int)floor(lat_x(g, px)), iy = (int)floor(lat_y(g, py));
-        const int iz = (int)floor(unwrap_near(lat_z(g, pz), az, g.nzc));
+        const double lxv = lat_x(g, px), lyv = lat_y(g, py), lzv = unwrap_near(lat_z(g, pz), az, g.nzc);
+        if (!(sane_lattice(lxv) && sane_lattice(lyv) && sane_lattice(lzv) && sane_lattice(az))) { bad = true; continue; }
+        const int ix = (int)floor(lxv), iy = (int)floor(lyv);
+        const int iz = (int)floor(lzv);
         lo0 = min(lo0, ix - 2); hi0 = max(hi0, ix + 3);
         lo1 = min(lo1, iy - 2); hi1 = max(hi1, iy + 3);
         lo2 = min(lo2, iz - 2); hi2 = max(hi2, iz + 3);
     }
     atomicMin(&s_lo[0], lo0); atomicMin(&s_lo[1], lo1); atomicMin(&s_lo[2], lo2);
     atomicMax(&s_hi[0], hi0); atomicMax(&s_hi[1], hi1); atomicMax(&s_hi[2], hi2);
-    __syncthreads();
+    if (__syncthreads_or(bad)) {   // a blown-up patch: flag it, leave its vertices as they are
+        if (tid == 0) atomicOr(flags, RBC_FLAG_NONFINITE);
+        return;
+    }
     const int bx0 = s_lo[0], by0 = s_lo[1], bz0 = s_lo[2];
     const long long bxl = (long long)s_hi[0] - bx0 + 1, byl = (long long)s_hi[1] - by0 + 1, bzl = (long long)s_hi[2] - bz0 + 1;
-    const bool use_box = np > 0 && bxl * byl * bzl <= ADVECT_BOX_CAP;
+    const bool use_box = np > 0 && bxl >= 6 && byl >= 6 && bzl >= 6 && bxl * byl * bzl <= ADVECT_BOX_CAP;
     const int bxs = use_box ? (int)bxl : 0, bys = use_box ? (int)byl : 0, bzs = use_box ? (int)bzl : 0;
     if (use_box) {
         // node li = (z * bys + y) * bxs + x; each thread steps li by ADVECT_THREADS

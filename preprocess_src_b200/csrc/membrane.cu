@@ -11,8 +11,10 @@
 // converts q to forces f_i = -q_i * (area of the one-ring / 3).
 //
 // Here one CTA owns one cell and does all of it on chip:
-//  1. the cell's FP64 positions go to shared memory, unwrapped about vertex 0
-//     (the reference applies the same minimum-image shift per edge);
+//  1. the cell's FP64 positions go to shared memory, relative to vertex 0;
+//     edge vectors take the minimum image in x and z per edge, as the
+//     reference does (stress.cu), so cells of any size relative to LX / 2
+//     and cells across the periodic boundary are handled alike;
 //  2. element pass: each element's tension is evaluated once and its record
 //     (twice the area gab and the load contributions of its second and third
 //     vertex; the first vertex's is minus their sum) goes to an L2-resident
@@ -113,9 +115,9 @@ membrane_kernel(const MembraneArgs a)
     const long long vb = (long long)cell * V, eb = (long long)cell * E, nv = a.nv;
     const double ax = a.Xd[vb], ay = a.Xd[nv + vb], az = a.Xd[2 * nv + vb];
     for (int v = tid; v < V; v += T) {
-        pos[v] = mimage(a.Xd[vb + v] - ax, a.LX);
+        pos[v] = a.Xd[vb + v] - ax;
         pos[V + v] = a.Xd[nv + vb + v] - ay;
-        pos[2 * V + v] = mimage(a.Xd[2 * nv + vb + v] - az, a.LZ);
+        pos[2 * V + v] = a.Xd[2 * nv + vb + v] - az;
     }
     for (int k = tid; k < 6 * V; k += T) snbr[k] = a.nbr[k];
     __syncthreads();
@@ -126,8 +128,10 @@ membrane_kernel(const MembraneArgs a)
     R4 *rec = reinterpret_cast<R4 *>(a.erec) + (size_t)eb * 3;   // [E][3 slots]: load on the slot's vertex, gab
     for (int e = tid; e < E; e += T) {
         const int ia = __ldg(&a.tri[3 * e]), ib = __ldg(&a.tri[3 * e + 1]), ic = __ldg(&a.tri[3 * e + 2]);
-        const double e1x = pos[ib] - pos[ia], e1y = pos[V + ib] - pos[V + ia], e1z = pos[2 * V + ib] - pos[2 * V + ia];
-        const double e2x = pos[ic] - pos[ia], e2y = pos[V + ic] - pos[V + ia], e2z = pos[2 * V + ic] - pos[2 * V + ia];
+        const double e1x = mimage(pos[ib] - pos[ia], a.LX), e1y = pos[V + ib] - pos[V + ia];
+        const double e1z = mimage(pos[2 * V + ib] - pos[2 * V + ia], a.LZ);
+        const double e2x = mimage(pos[ic] - pos[ia], a.LX), e2y = pos[V + ic] - pos[V + ia];
+        const double e2z = mimage(pos[2 * V + ic] - pos[2 * V + ia], a.LZ);
         // deformed covariant metric (stress.cu:75-84) and its difference from the reference, in FP64
         const double g11d = e1x * e1x + e1y * e1y + e1z * e1z;
         const double g12d = e1x * e2x + e1y * e2y + e1z * e2z;

@@ -92,6 +92,26 @@ def test_stress_matches_oracle(developed, oracle_mod):
         assert flags & 8 == 0, "load solve residual flag"
 
 
+def test_narrow_duct_cell_matches_oracle(oracle_mod, native_lib):
+    """A 32-wide duct (the reference's x period LX = 28) with a 15.6-wide cell
+    whose first vertex sits near the cell's edge in x: edge vectors must take
+    the minimum image per edge, not the cell's positions about vertex 0."""
+    from preprocess_src_b200.step import Simulation
+    case = configs.capillary_batch(4, seed=7, lengths=(48, 64))[0]
+    x0 = case.xr[0::3]
+    assert np.ptp(x0) > case.params["LX"] / 2 and abs(x0[0] - x0.mean()) > 4.0
+    o = oracle_mod.Oracle(case)
+    sim = Simulation(case)
+    o.step(3)
+    sim.step(3)
+    got = sim.export_cells()
+    for k in ("x", "y", "z"):
+        assert np.abs(got[k] - o[k]).max() <= 1e-9, k
+    assert np.abs(got["fx"] - o["cfx"]).max() <= 1e-9
+    flags, _ = sim.status()
+    assert flags & 3 == 0, flags
+
+
 def test_spread_matches_oracle(developed, oracle_mod):
     case, o = developed
     c = clone(oracle_mod, o)
