@@ -190,6 +190,34 @@ int rbc_get_stream(const rbc_handle *h, void **stream);
 #define RBC_KERNEL_NAMES {"step_begin", "membrane", "spread", "lbm_collide_stream", "advect", "volume"}
 int rbc_profile_steps(rbc_handle *h, int nsteps, double *kernel_ms);
 
+/* ---- batches of independent simulations ----------------------------------- */
+
+/* Several independent simulations (for instance capillaries of different
+ * sizes and parameters, each its own handle) stepped together: each batch
+ * step is one CUDA graph launch whose nodes are the simulations' whole steps,
+ * so their kernels run concurrently.  The reference runs one simulation per
+ * process; its main.cu:73-110 loop is what each simulation of the batch
+ * executes.  The handles stay owned by the caller and usable (stage calls,
+ * imports, exports, rbc_step) between batch steps; destroy the batch first. */
+typedef struct rbc_batch rbc_batch;
+/* handles: n distinct handles on one device.  Text of errors: rbc_batch_last_error(NULL). */
+int rbc_batch_create(rbc_handle *const *handles, int n, rbc_batch **out);
+int rbc_batch_destroy(rbc_batch *b);
+const char *rbc_batch_last_error(const rbc_batch *b);
+/* nsteps steps of every simulation.  Asynchronous; each handle's later work
+ * is ordered after it, and rbc_batch_synchronize waits for it. */
+int rbc_batch_step(rbc_batch *b, int nsteps);
+int rbc_batch_synchronize(rbc_batch *b);
+/* Simulations per dependency chain of the batch graph (default 1: all
+ * concurrent): simulations i and i + 1 with the same i / chain run one after
+ * the other, chains concurrently. */
+int rbc_batch_set_chain(rbc_batch *b, int chain);
+int rbc_batch_get_chain(const rbc_batch *b, int *chain);
+/* Times chain = 1, 2, 4, ... (up to 64 and the batch size) over 1 +
+ * steps_per_trial batch steps each and keeps the fastest (*chain_out, may be
+ * NULL).  The timed steps are real steps: every simulation advances by them. */
+int rbc_batch_autotune(rbc_batch *b, int steps_per_trial, int *chain_out);
+
 /* ---- without allocation -------------------------------------------------- */
 
 /* No counterpart in the reference.  Per-cell FP64 volume, area and vertex

@@ -69,8 +69,16 @@ _SIGS = {
     "rbc_profile_steps": [_H, C.c_int, _DP],
     "rbc_cell_metrics_noalloc": [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_double, C.c_double,
                                  C.c_double, C.c_int, C.c_void_p, _DP, _DP, _DP],
+    "rbc_batch_create": [C.POINTER(_H), C.c_int, C.POINTER(_H)],
+    "rbc_batch_destroy": [_H],
+    "rbc_batch_last_error": [_H],
+    "rbc_batch_step": [_H, C.c_int],
+    "rbc_batch_synchronize": [_H],
+    "rbc_batch_set_chain": [_H, C.c_int],
+    "rbc_batch_get_chain": [_H, _IP],
+    "rbc_batch_autotune": [_H, C.c_int, _IP],
 }
-_RESTYPE = {"rbc_last_error": C.c_char_p}
+_RESTYPE = {"rbc_last_error": C.c_char_p, "rbc_batch_last_error": C.c_char_p}
 
 # every entry point declared in include/rbc_step.h
 EXPORTED = tuple(_SIGS)

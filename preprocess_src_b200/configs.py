@@ -150,6 +150,23 @@ def single_cell_duct(**kw) -> Case:
                      subdiv=3, steps=1000, **kw)
 
 
+def capillary_batch(n: int = 512, seed: int = 4, lengths=tuple(range(48, 129, 16)), **kw) -> list:
+    """n independent capillaries (config 4): square 32 x 32 ducts of length L
+    drawn uniformly from {48, 64, ..., 128}, one subdivision-3 cell each at the
+    duct centre with a uniform random orientation, Gs log-uniform in
+    [1e-4, 2e-3], g uniform in [5e-7, 2e-6], tau = 1, FP32.  All draws come from
+    one seeded generator in capillary order."""
+    rng = np.random.default_rng(seed)
+    cases = []
+    for i in range(n):
+        L = int(rng.choice(lengths))
+        Gs = float(np.exp(rng.uniform(np.log(1e-4), np.log(2e-3))))
+        g = float(rng.uniform(5e-7, 2e-6))
+        cases.append(duct_case(f"capillary{i:03d}_{L}x32x32", L, 32, 32, centers_duct=[(L / 2.0, 16.0, 16.0)],
+                               subdiv=3, seed=int(rng.integers(1 << 31)), g=g, Gs=Gs, steps=2000, **kw))
+    return cases
+
+
 def dense_suspension(**kw) -> Case:
     """256 x 128 x 128 duct, 200 subdivision-4 cells (2562 vertices, 5120
     triangles each) of radius 7.82 placed by random sequential addition,

@@ -463,19 +463,30 @@ int enqueue_step(rbc_handle *h, StepForm form = STEP_WHOLE)
 
 // CUDA graph of one step starting from population buffer c (the step flips
 // the buffers, so two graphs alternate)
-int build_graph(rbc_handle *h, int c, StepForm form)
+// one step of the given form starting from population buffer c, captured
+// from the handle's stream into *out (not instantiated)
+int capture_step(rbc_handle *h, int c, StepForm form, cudaGraph_t *out)
 {
-    cudaGraph_t graph = nullptr;
+    *out = nullptr;
     const long long launches0 = h->launches;
     const int cur0 = h->cur;
     h->cur = c;
     CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
     int rc = enqueue_step(h, form);
-    cudaError_t e = cudaStreamEndCapture(h->stream, &graph);
+    cudaError_t e = cudaStreamEndCapture(h->stream, out);
     h->launches = launches0;
     h->cur = cur0;
-    if (rc != RBC_OK) { if (graph) cudaGraphDestroy(graph); return rc; }
+    if (rc != RBC_OK) { if (*out) cudaGraphDestroy(*out); *out = nullptr; return rc; }
     if (e != cudaSuccess) { h->err = std::string("graph capture: ") + cudaGetErrorString(e); return RBC_ERR_CUDA; }
+    return RBC_OK;
+}
+
+int build_graph(rbc_handle *h, int c, StepForm form)
+{
+    cudaGraph_t graph = nullptr;
+    int rc = capture_step(h, c, form, &graph);
+    if (rc != RBC_OK) return rc;
+    cudaError_t e;
     cudaGraphExec_t &exec = h->graph[form][c];
     e = cudaGraphInstantiate(&exec, graph, 0);
     cudaGraphDestroy(graph);
@@ -493,6 +504,77 @@ int prepare_steps(rbc_handle *h)
     }
     // the device counter follows the host's prc->iter mirror
     CK(cudaMemcpyAsync(h->d_iter(), &h->iter, sizeof(int), cudaMemcpyHostToDevice, h->stream));
+    return RBC_OK;
+}
+
+}  // namespace
+
+// ---- batches of independent simulations -----------------------------------
+
+struct rbc_batch {
+    std::vector<rbc_handle *> h;
+    std::vector<int> base_cur;          // each handle's buffer parity when the graphs were built
+    std::vector<cudaEvent_t> ready;     // one per handle: its pending work, before a batch step
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t done = nullptr;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    int parity = 0;                     // graph[parity] advances every handle by one step
+    int chain = 1;                      // simulations per dependency chain in the batch graph
+    std::string err;
+};
+
+namespace {
+
+#define CKB(call)                                                                      \
+    do {                                                                               \
+        cudaError_t e_ = (call);                                                       \
+        if (e_ != cudaSuccess) {                                                       \
+            b->err = std::string(#call) + ": " + cudaGetErrorString(e_);               \
+            return RBC_ERR_CUDA;                                                       \
+        }                                                                              \
+    } while (0)
+
+void batch_free_graphs(rbc_batch *b)
+{
+    for (cudaGraphExec_t &g : b->graph) { if (g) cudaGraphExecDestroy(g); g = nullptr; }
+}
+
+// The batch graph for parity k: every simulation's whole step (from buffer
+// base_cur ^ k) as a child graph; simulations i and i + 1 of the same chain
+// (i / chain equal) run one after the other, chains run concurrently.
+int batch_build(rbc_batch *b)
+{
+    batch_free_graphs(b);
+    const int n = (int)b->h.size();
+    for (int i = 0; i < n; i++) b->base_cur[i] = b->h[i]->cur;
+    b->parity = 0;
+    for (int k = 0; k < 2; k++) {
+        cudaGraph_t g = nullptr;
+        CKB(cudaGraphCreate(&g, 0));
+        cudaGraphNode_t prev = nullptr;
+        int rc = RBC_OK;
+        for (int i = 0; i < n && rc == RBC_OK; i++) {
+            cudaGraph_t child = nullptr;
+            rc = capture_step(b->h[i], b->base_cur[i] ^ k, STEP_WHOLE, &child);
+            if (rc != RBC_OK) { b->err = "simulation " + std::to_string(i) + ": " + b->h[i]->err; break; }
+            cudaGraphNode_t node = nullptr;
+            const bool chained = i % b->chain != 0;
+            const cudaError_t e = cudaGraphAddChildGraphNode(&node, g, chained ? &prev : nullptr, chained ? 1 : 0, child);
+            cudaGraphDestroy(child);
+            if (e != cudaSuccess) { b->err = std::string("batch graph: ") + cudaGetErrorString(e); rc = RBC_ERR_CUDA; }
+            prev = node;
+        }
+        cudaError_t e = cudaSuccess;
+        if (rc == RBC_OK) e = cudaGraphInstantiate(&b->graph[k], g, 0);
+        cudaGraphDestroy(g);
+        if (rc != RBC_OK) return rc;
+        if (e != cudaSuccess) {
+            b->graph[k] = nullptr;
+            b->err = std::string("batch graph instantiate: ") + cudaGetErrorString(e);
+            return RBC_ERR_CUDA;
+        }
+    }
     return RBC_OK;
 }
 
@@ -1012,6 +1094,144 @@ int rbc_dims(const rbc_handle *h, int *nx, int *ny, int *nz_periodic, int *ncell
     if (ncell) *ncell = h->ncell;
     if (vertex) *vertex = h->V;
     if (element) *element = h->E;
+    return RBC_OK;
+}
+
+// ---- batches ----------------------------------------------------------------
+
+int rbc_batch_create(rbc_handle *const *handles, int n, rbc_batch **out)
+{
+    g_create_error.clear();
+    if (!out) return fail(nullptr, RBC_ERR_ARG, "out is NULL");
+    *out = nullptr;
+    if (!handles || n <= 0) return fail(nullptr, RBC_ERR_ARG, "a batch needs at least one simulation");
+    for (int i = 0; i < n; i++) {
+        if (!handles[i]) return fail(nullptr, RBC_ERR_ARG, "simulation " + std::to_string(i) + " is NULL");
+        if (handles[i]->device != handles[0]->device)
+            return fail(nullptr, RBC_ERR_ARG, "all simulations of a batch must use the same device");
+        for (int j = 0; j < i; j++)
+            if (handles[j] == handles[i]) return fail(nullptr, RBC_ERR_ARG, "a simulation appears twice in the batch");
+    }
+    rbc_batch *b = new (std::nothrow) rbc_batch();
+    if (!b) return fail(nullptr, RBC_ERR_ARG, "out of host memory");
+    b->h.assign(handles, handles + n);
+    b->base_cur.assign(n, 0);
+    b->device = handles[0]->device;
+    auto bail = [&](int code, const std::string &msg) {
+        g_create_error = msg;
+        rbc_batch_destroy(b);
+        return code;
+    };
+    if (cudaSetDevice(b->device) != cudaSuccess) return bail(RBC_ERR_CUDA, "cudaSetDevice failed");
+    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming) != cudaSuccess)
+        return bail(RBC_ERR_CUDA, "stream creation failed");
+    b->ready.assign(n, nullptr);
+    for (int i = 0; i < n; i++)
+        if (cudaEventCreateWithFlags(&b->ready[i], cudaEventDisableTiming) != cudaSuccess)
+            return bail(RBC_ERR_CUDA, "event creation failed");
+    *out = b;
+    return RBC_OK;
+}
+
+int rbc_batch_destroy(rbc_batch *b)
+{
+    if (!b) return RBC_OK;
+    cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    batch_free_graphs(b);
+    for (cudaEvent_t e : b->ready) if (e) cudaEventDestroy(e);
+    if (b->done) cudaEventDestroy(b->done);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+    return RBC_OK;
+}
+
+const char *rbc_batch_last_error(const rbc_batch *b)
+{
+    return b ? b->err.c_str() : g_create_error.c_str();
+}
+
+int rbc_batch_set_chain(rbc_batch *b, int chain)
+{
+    if (!b || chain < 1) return RBC_ERR_ARG;
+    if (chain != b->chain) { b->chain = chain; batch_free_graphs(b); }
+    return RBC_OK;
+}
+
+int rbc_batch_get_chain(const rbc_batch *b, int *chain)
+{
+    if (!b || !chain) return RBC_ERR_ARG;
+    *chain = b->chain;
+    return RBC_OK;
+}
+
+int rbc_batch_step(rbc_batch *b, int nsteps)
+{
+    if (!b || nsteps < 0) return RBC_ERR_ARG;
+    if (nsteps == 0) return RBC_OK;
+    CKB(cudaSetDevice(b->device));
+    const int n = (int)b->h.size();
+    // a simulation stepped on its own since the graphs were built has another buffer parity
+    bool stale = !b->graph[0] || !b->graph[1];
+    for (int i = 0; i < n && !stale; i++) stale = b->h[i]->cur != (b->base_cur[i] ^ b->parity);
+    int rc;
+    if (stale && (rc = batch_build(b))) return rc;
+    for (int i = 0; i < n; i++) {
+        rbc_handle *h = b->h[i];
+        if ((rc = prepare_steps(h))) { b->err = "simulation " + std::to_string(i) + ": " + h->err; return rc; }
+        CKB(cudaEventRecord(b->ready[i], h->stream));
+        CKB(cudaStreamWaitEvent(b->stream, b->ready[i], 0));
+    }
+    for (int k = 0; k < nsteps; k++) {
+        CKB(cudaGraphLaunch(b->graph[b->parity], b->stream));
+        b->parity ^= 1;
+    }
+    CKB(cudaEventRecord(b->done, b->stream));
+    for (int i = 0; i < n; i++) {
+        rbc_handle *h = b->h[i];
+        if (nsteps & 1) h->cur ^= 1;
+        h->iter += nsteps;
+        h->launches += (long long)KERNELS_PER_STEP * nsteps;
+        CKB(cudaStreamWaitEvent(h->stream, b->done, 0));
+    }
+    return RBC_OK;
+}
+
+int rbc_batch_synchronize(rbc_batch *b)
+{
+    if (!b) return RBC_ERR_ARG;
+    CKB(cudaSetDevice(b->device));
+    CKB(cudaStreamSynchronize(b->stream));
+    return RBC_OK;
+}
+
+int rbc_batch_autotune(rbc_batch *b, int steps_per_trial, int *chain_out)
+{
+    if (!b || steps_per_trial < 1) return RBC_ERR_ARG;
+    CKB(cudaSetDevice(b->device));
+    const int n = (int)b->h.size();
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    CKB(cudaEventCreate(&t0));
+    CKB(cudaEventCreate(&t1));
+    int best = b->chain, rc = RBC_OK;
+    float best_ms = 0.f;
+    for (int chain = 1; chain <= n && rc == RBC_OK; chain *= 2) {
+        if ((rc = rbc_batch_set_chain(b, chain))) break;
+        if ((rc = rbc_batch_step(b, 1))) break;   // builds the graphs and warms them up
+        if (cudaEventRecord(t0, b->stream) != cudaSuccess) { rc = RBC_ERR_CUDA; break; }
+        if ((rc = rbc_batch_step(b, steps_per_trial))) break;
+        float ms = 0.f;
+        if (cudaEventRecord(t1, b->stream) != cudaSuccess || cudaEventSynchronize(t1) != cudaSuccess ||
+            cudaEventElapsedTime(&ms, t0, t1) != cudaSuccess) { rc = RBC_ERR_CUDA; break; }
+        if (chain == 1 || ms < best_ms) { best_ms = ms; best = chain; }
+        if (chain >= 64) break;   // longer chains only serialise more
+    }
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    if (rc != RBC_OK) return rc;
+    if ((rc = rbc_batch_set_chain(b, best))) return rc;
+    if (chain_out) *chain_out = best;
     return RBC_OK;
 }
 

@@ -182,3 +182,60 @@ class Simulation:
         v = C.c_longlong(0)
         self._call("rbc_launch_count", C.byref(v))
         return v.value
+
+
+class Batch:
+    """Independent simulations stepped together (rbc_batch_*): every batch step
+    is one CUDA graph launch whose nodes are the simulations' whole steps.  The
+    simulations stay usable on their own between batch steps."""
+
+    def __init__(self, sims):
+        self.sims = list(sims)   # the handles must outlive the batch
+        arr = (N._H * len(self.sims))(*[s._h.value for s in self.sims])
+        b = N._H()
+        code = N.lib().rbc_batch_create(arr, len(self.sims), C.byref(b))
+        if code != N.RBC_OK:
+            msg = N.lib().rbc_batch_last_error(None)
+            raise N.RbcError(code, msg.decode() if msg else "")
+        self._b = b
+
+    def _call(self, name, *args):
+        code = getattr(N.lib(), name)(self._b, *args)
+        if code != N.RBC_OK:
+            msg = N.lib().rbc_batch_last_error(self._b)
+            raise N.RbcError(code, msg.decode() if msg else "")
+
+    def close(self):
+        if getattr(self, "_b", None):
+            N.lib().rbc_batch_destroy(self._b)
+            self._b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self, nsteps: int = 1):
+        self._call("rbc_batch_step", int(nsteps))
+
+    def synchronize(self):
+        self._call("rbc_batch_synchronize")
+
+    @property
+    def chain(self) -> int:
+        v = C.c_int(0)
+        self._call("rbc_batch_get_chain", C.byref(v))
+        return v.value
+
+    @chain.setter
+    def chain(self, value: int):
+        self._call("rbc_batch_set_chain", int(value))
+
+    def autotune(self, steps_per_trial: int = 3) -> int:
+        """Picks the chain length with the fastest batch step; the timed steps
+        advance every simulation."""
+        v = C.c_int(0)
+        self._call("rbc_batch_autotune", int(steps_per_trial), C.byref(v))
+        return v.value
+
