@@ -50,7 +50,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="dense", choices=["dense", "single"])
+    ap.add_argument("--workload", default="dense", choices=["dense", "single", "capillaries"],
+                    help="dense: config 2 (the headline); single: config 1; capillaries: config 4 "
+                         "(512 uneven capillaries as one batch vs one after another)")
+    ap.add_argument("--capillaries", type=int, default=512, help="number of capillaries (capillaries workload)")
     ap.add_argument("--storage", default="f32", choices=["f32", "f16"])
     ap.add_argument("--profile-steps", type=int, default=20)
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU-baseline sample budget")
@@ -265,6 +268,72 @@ def run_ours(args, world, rank, local):
     return result
 
 
+def run_capillaries(args, world, rank, local):
+    """Config 4: independent capillaries of uneven length stepped as one batch
+    (one CUDA graph launch per step, chain length from the autotuner) against
+    the same capillaries stepped one after another.  value = aggregate MLUPS of
+    the batch; the sequential arm is the sum of each capillary's own
+    event-timed steps."""
+    import torch
+
+    from preprocess_src_b200 import configs
+    from preprocess_src_b200.step import Batch, Simulation
+
+    dev = local
+    torch.cuda.set_device(dev)
+    cases = configs.capillary_batch(args.capillaries, seed=4 + 1000 * rank)
+    sims = [Simulation(c, device=dev) for c in cases]
+    fluid = sum(c.fluid_nodes() for c in cases)
+    batch = Batch(sims)
+    chain = batch.autotune(2)
+    batch.step(args.warmup)
+    batch.synchronize()
+    bstream = torch.cuda.ExternalStream(batch.stream, device=torch.device("cuda", dev))
+    barrier(world)
+    l0 = sum(s.launches for s in sims)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(dev) as clk:
+        time.sleep(0.3)
+        ev0.record(bstream)
+        batch.step(args.steps)
+        ev1.record(bstream)
+        ev1.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    launches = sum(s.launches for s in sims) - l0
+    ms_max = allreduce_max(ms, world)
+    flags = [s.status()[0] for s in sims]
+    # the same capillaries one after another, each timed on its own stream
+    seq_ms = 0.0
+    for s in sims:
+        st = torch.cuda.ExternalStream(s.stream, device=torch.device("cuda", dev))
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        s.step(args.steps)
+        b.record(st)
+        b.synchronize()
+        seq_ms += a.elapsed_time(b)
+    batch.close()
+    for s in sims:
+        s.close()
+    if rank != 0:
+        return None
+    value = world * fluid * args.steps / (ms_max * 1e-3) / 1e6
+    seq = fluid * args.steps / (seq_ms * 1e-3) / 1e6
+    return {"metric": "aggregate MLUPS, %d uneven capillaries in one batch (config 4)" % len(cases),
+            "value": round(value, 2), "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "capillary_batch_%d_32x32xL" % len(cases), "capillaries": len(cases),
+                       "fluid_nodes": fluid, "lengths": "uniform {48, 64, ..., 128}", "cells_per_capillary": 1,
+                       "vertices_per_cell": cases[0].vertex, "chain": chain,
+                       "l2": "inputs larger than L2 (populations %.2f GB), no flush" % (2 * 19 * 4 * sum(c.nx * c.ny * (c.nz - 4) for c in cases) / 1e9)},
+            "sequential": {"value": round(seq, 2), "unit": "MLUPS", "ms_per_step": round(seq_ms / args.steps, 4),
+                           "how": "each capillary stepped alone (rbc_step, CUDA graphs), one after another"},
+            "speedup_vs_sequential": round(value / seq, 2),
+            "gpu_launches": launches, "status_flags_nonzero": int(sum(1 for f in flags if f & 3)),
+            "clocks": clk.summary()}
+
+
 def run_e2e(args, case, dev, world):
     """Public-API run with host buffers (pinned), copies inside the timed region."""
     import numpy as np
@@ -332,9 +401,40 @@ def run_e2e(args, case, dev, world):
                     "rbc_export_ref_cells, pinned host buffers"}
 
 
+def run_reference_capillaries(args):
+    """The FP64 oracle on the config-4 capillaries, one after another, for a
+    bounded sample (about 60 s): aggregate MLUPS over the capillaries run."""
+    from preprocess_src_b200 import configs
+    from oracle.oracle import Oracle, num_threads
+    cases = configs.capillary_batch(args.capillaries, seed=4)
+    steps = max(1, min(args.steps, 20))
+    done_nodes, el, ncap = 0, 0.0, 0
+    for c in cases:
+        o = Oracle(c)
+        o.step(1)
+        t0 = time.perf_counter()
+        o.step(steps)
+        el += time.perf_counter() - t0
+        done_nodes += c.fluid_nodes() * steps
+        ncap += 1
+        if el > 60.0:
+            break
+    value = done_nodes / el / 1e6
+    sample = f"{steps} FP64 oracle steps of each of the first {ncap} of {len(cases)} capillaries, one after another ({el:.1f} s)"
+    return {"metric": "aggregate MLUPS, %d uneven capillaries in one batch (config 4)" % len(cases), "impl": "reference",
+            "value": round(value, 4), "unit": "MLUPS", "n_gpus": 1, "steps": steps, "warmup": 1,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "capillary_batch_%d_32x32xL" % len(cases)},
+            "cpu_baseline": {"value": round(value, 4), "unit": "MLUPS", "cores": num_threads(), "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": round(value, 4), "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
 def run_reference(args, world, rank):
     if rank != 0:
         return None
+    if args.workload == "capillaries":
+        return run_reference_capillaries(args)
     case = make_case(args.workload)
     from oracle.oracle import Oracle, num_threads
     o = Oracle(case)
@@ -371,7 +471,7 @@ def main():
             print(json.dumps(res), flush=True)
         return
     world, rank, local = dist_setup(args)
-    res = run_ours(args, world, rank, local)
+    res = run_capillaries(args, world, rank, local) if args.workload == "capillaries" else run_ours(args, world, rank, local)
     if res is not None:
         print(json.dumps(res), flush=True)
     if world > 1:

@@ -208,6 +208,8 @@ const char *rbc_batch_last_error(const rbc_batch *b);
  * is ordered after it, and rbc_batch_synchronize waits for it. */
 int rbc_batch_step(rbc_batch *b, int nsteps);
 int rbc_batch_synchronize(rbc_batch *b);
+/* The CUDA stream (cudaStream_t) the batch graph launches run on. */
+int rbc_batch_get_stream(const rbc_batch *b, void **stream);
 /* Simulations per dependency chain of the batch graph (default 1: all
  * concurrent): simulations i and i + 1 with the same i / chain run one after
  * the other, chains concurrently. */

@@ -74,6 +74,7 @@ _SIGS = {
     "rbc_batch_last_error": [_H],
     "rbc_batch_step": [_H, C.c_int],
     "rbc_batch_synchronize": [_H],
+    "rbc_batch_get_stream": [_H, C.POINTER(C.c_void_p)],
     "rbc_batch_set_chain": [_H, C.c_int],
     "rbc_batch_get_chain": [_H, _IP],
     "rbc_batch_autotune": [_H, C.c_int, _IP],

@@ -1198,6 +1198,13 @@ int rbc_batch_step(rbc_batch *b, int nsteps)
     return RBC_OK;
 }
 
+int rbc_batch_get_stream(const rbc_batch *b, void **stream)
+{
+    if (!b || !stream) return RBC_ERR_ARG;
+    *stream = (void *)b->stream;
+    return RBC_OK;
+}
+
 int rbc_batch_synchronize(rbc_batch *b)
 {
     if (!b) return RBC_ERR_ARG;

@@ -223,6 +223,12 @@ class Batch:
         self._call("rbc_batch_synchronize")
 
     @property
+    def stream(self) -> int:
+        v = C.c_void_p()
+        self._call("rbc_batch_get_stream", C.byref(v))
+        return v.value or 0
+
+    @property
     def chain(self) -> int:
         v = C.c_int(0)
         self._call("rbc_batch_get_chain", C.byref(v))
