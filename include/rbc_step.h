@@ -90,7 +90,7 @@ typedef struct rbc_params {
     double C;            /* Skalak area-dilation ratio */
     double rgs;          /* tension normalisation cel->rg (1.0 for red cells) */
     int    law;          /* RBC_LAW_* */
-    double br;           /* bending modulus BR; only 0 is implemented */
+    double br;           /* bending modulus BR of fourpoint_bend (stress.cu:448-578); 0 = none */
     int    M;            /* sub-cycling factor; only 1 is implemented */
     int    rk_order;     /* RUNGE_KUTTA; only 4 is implemented */
     /* implementation choices */
@@ -159,6 +159,7 @@ int rbc_get_iter(const rbc_handle *h, int *iter);
 
 /* ---- the step ---------------------------------------------------------- */
 
+/* calc_tension + calc_load + q2f, then fourpoint_bend when BR != 0 */
 int rbc_stress(rbc_handle *h);
 int rbc_ibm_st1(rbc_handle *h);
 int rbc_lbm_d3q19(rbc_handle *h);
@@ -185,7 +186,8 @@ int rbc_launch_count(const rbc_handle *h, long long *count);
 int rbc_get_stream(const rbc_handle *h, void **stream);
 /* Runs nsteps full steps with direct launches (no graph) and a CUDA event
  * around every kernel; kernel_ms[RBC_NUM_KERNELS] receives the summed device
- * time per kernel in the order of RBC_KERNEL_NAMES.  Synchronous. */
+ * time per kernel in the order of RBC_KERNEL_NAMES (with BR != 0 the bending
+ * kernel is timed in the "membrane" slot).  Synchronous. */
 #define RBC_NUM_KERNELS 6
 #define RBC_KERNEL_NAMES {"step_begin", "membrane", "spread", "lbm_collide_stream", "advect", "volume"}
 int rbc_profile_steps(rbc_handle *h, int nsteps, double *kernel_ms);

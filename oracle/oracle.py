@@ -27,7 +27,7 @@ class OrcParams(C.Structure):
                 ("law", C.c_int), ("residual", C.c_double), ("itrmax", C.c_int), ("LX", C.c_double),
                 ("LZ", C.c_double), ("xmin", C.c_double), ("xmax", C.c_double), ("zmin", C.c_double),
                 ("zmax", C.c_double), ("ncell", C.c_int), ("vertex", C.c_int), ("element", C.c_int),
-                ("mn", C.c_int)]
+                ("mn", C.c_int), ("br", C.c_double)]
 
 
 _STATE_D = ["fn", "fm", "dn", "un", "vn", "wn", "dm", "um", "vm", "wm", "fx", "fy", "fz"]
@@ -37,7 +37,7 @@ _STATE_CELL_D = ["x", "y", "z", "u", "v", "w", "cfx", "cfy", "cfz", "xd", "nd", 
 class OrcState(C.Structure):
     _fields_ = ([(k, _DP) for k in _STATE_D] + [("bc", _IP)] + [(k, _DP) for k in _STATE_CELL_D]
                 + [("ele", _IP), ("nln", _IP), ("ln", _IP), ("lo", _IP), ("nle", _IP), ("le", _IP),
-                   ("volume0", _DP), ("gx", _DP), ("iter", C.c_int), ("bicg_iters", C.c_int)])
+                   ("volume0", _DP), ("gx", _DP), ("iter", C.c_int), ("bicg_iters", C.c_int), ("ec", _IP)])
 
 
 _lib = None
@@ -56,7 +56,7 @@ def lib() -> C.CDLL:
         for name in ("orc_fem_init", "orc_stress", "orc_calc_load", "orc_volume_correction", "orc_step"):
             getattr(L, name).restype = C.c_int
         for name in ("orc_flu_init", "orc_volume_init", "orc_ibm_st1", "orc_lbm_d3q19", "orc_ibm_st2",
-                     "orc_calc_tension", "orc_q2f"):
+                     "orc_calc_tension", "orc_q2f", "orc_bend"):
             getattr(L, name).restype = None
         L.orc_num_threads.restype = C.c_int
         L.orc_calc_volume.restype = None
@@ -88,7 +88,7 @@ class Oracle:
                            P=p["P"], B=p["B"], flowstart=p["flowstart"], freq=p["freq"], C=p["C"], rgs=p["rgs"],
                            law=p["law"], residual=p["residual"], itrmax=p["itrmax"], LX=p["LX"], LZ=p["LZ"],
                            xmin=p["xmin"], xmax=p["xmax"], zmin=p["zmin"], zmax=p["zmax"], ncell=self.N,
-                           vertex=self.V, element=self.E, mn=self.mn)
+                           vertex=self.V, element=self.E, mn=self.mn, br=float(p.get("br", 0.0)))
         n = case.n
         self.a = {}
         for k in _STATE_D:
@@ -101,6 +101,7 @@ class Oracle:
         self.a["ele"] = case.ele_global() if self.N else np.zeros(3, np.int32)
         for k, s in dict(nln=nv, ln=7 * nv, lo=7 * nv, nle=nv, le=6 * nv).items():
             self.a[k] = np.zeros(s, dtype=np.int32)
+        self.a["ec"] = np.zeros(3 * ne, dtype=np.int32)
         self.a["volume0"] = np.zeros(max(self.N, 1))
         self.a["gx"] = np.zeros(3 * max(self.N, 1))
         self.s = OrcState()

@@ -142,6 +142,32 @@ static void set_contravariant(const double *xr, double *n, const int *ele, int c
 }
 
 /* init2.cu:258-400 (fem_init, RBC branch) */
+/* init1.cu:755-795: cel->ec, the elements sharing an edge with each element,
+ * in increasing element order (the reference scans all elements of the cell) */
+static void edge_neighbours(const orc_params *p, orc_state *s)
+{
+    const long ne = (long)p->ncell * p->element;
+    for (long e1 = 0; e1 < ne; e1++) {
+        long nb[3] = {-1, -1, -1};
+        int cnt = 0;
+        for (int a = 0; a < 3; a++) {
+            const int ia = s->ele[e1*3 + a], ib = s->ele[e1*3 + (a + 1) % 3];
+            for (int k = 0; k < s->nle[ia]; k++) {
+                const long e2 = s->le[ia*6 + k];
+                if (e2 == e1) continue;
+                if (s->ele[e2*3] == ib || s->ele[e2*3+1] == ib || s->ele[e2*3+2] == ib) {
+                    if (cnt < 3) nb[cnt++] = e2;
+                    break;
+                }
+            }
+        }
+        for (int x = 0; x < cnt; x++)   /* increasing element order */
+            for (int y = x + 1; y < cnt; y++)
+                if (nb[y] < nb[x]) { long t = nb[x]; nb[x] = nb[y]; nb[y] = t; }
+        for (int k = 0; k < 3; k++) s->ec[e1*3 + k] = (int)(k < cnt ? nb[k] : e1);
+    }
+}
+
 int orc_fem_init(const orc_params *p, orc_state *s)
 {
     int V = p->vertex, E = p->element, N = p->ncell;
@@ -172,6 +198,7 @@ int orc_fem_init(const orc_params *p, orc_state *s)
         sort_link_order(s->nln, s->lo, V, i);
     }
     set_contravariant(s->xd, s->nd, s->ele, N, E);
+    if (s->ec) edge_neighbours(p, s);
     return 0;
 }
 
@@ -371,12 +398,75 @@ void orc_q2f(const orc_params *p, orc_state *s)
     }
 }
 
-/* stress.cu:580-659 (bending with BR = 0 contributes nothing and is omitted) */
+/* stress.cu:448-578.  For every element e1 and each of its edge neighbours
+ * e2 (cel->ec order): the shared edge (k2, k3) in e1's winding, e1's third
+ * vertex k1 and e2's vertex k4 off the edge; xi and ze are the two triangle
+ * normals with positions taken as minimum images about k1; pairs with
+ * sin^2 < 1e-6 are skipped; with spontaneous angle 0 (c0 = 1, s0 = 0,
+ * init1.cu:849-850) beta = (2/sqrt 3) BR; k1 receives the whole force of
+ * the pair, k2 and k3 half of theirs (e2's visit of the same pair adds the
+ * rest). */
+void orc_bend(const orc_params *p, orc_state *s)
+{
+    if (p->br == 0.0) return;
+    const long ne = (long)p->ncell * p->element;
+    const double eps = 1.0e-6;
+    for (long e1 = 0; e1 < ne; e1++) {
+        const int i[3] = {s->ele[e1*3], s->ele[e1*3+1], s->ele[e1*3+2]};
+        for (int k = 0; k < 3; k++) {
+            const long e2 = s->ec[e1*3 + k];
+            const int j[3] = {s->ele[e2*3], s->ele[e2*3+1], s->ele[e2*3+2]};
+            int k1 = -1, k2 = -1, k3 = -1, k4 = -1;
+            for (int a = 0; a < 3 && k1 < 0; a++) {
+                const int ia = i[a], ib = i[(a + 1) % 3];
+                int has_a = -1, has_b = -1;
+                for (int b = 0; b < 3; b++) { if (j[b] == ia) has_a = b; if (j[b] == ib) has_b = b; }
+                if (has_a >= 0 && has_b >= 0) {
+                    k1 = i[(a + 2) % 3]; k2 = ia; k3 = ib; k4 = j[3 - has_a - has_b];
+                }
+            }
+            if (k1 < 0) continue;
+            double a1x = s->x[k1], a2x = s->x[k2], a3x = s->x[k3], a4x = s->x[k4];
+            double a1y = s->y[k1], a2y = s->y[k2], a3y = s->y[k3], a4y = s->y[k4];
+            double a1z = s->z[k1], a2z = s->z[k2], a3z = s->z[k3], a4z = s->z[k4];
+            a2x = a1x + min_image(a2x - a1x, p->LX); a3x = a1x + min_image(a3x - a1x, p->LX); a4x = a1x + min_image(a4x - a1x, p->LX);
+            a2z = a1z + min_image(a2z - a1z, p->LZ); a3z = a1z + min_image(a3z - a1z, p->LZ); a4z = a1z + min_image(a4z - a1z, p->LZ);
+            const double a21x = a2x - a1x, a31x = a3x - a1x, a34x = a3x - a4x, a24x = a2x - a4x, a23x = a2x - a3x;
+            const double a21y = a2y - a1y, a31y = a3y - a1y, a34y = a3y - a4y, a24y = a2y - a4y, a23y = a2y - a3y;
+            const double a21z = a2z - a1z, a31z = a3z - a1z, a34z = a3z - a4z, a24z = a2z - a4z, a23z = a2z - a3z;
+            const double xix = a21y*a31z - a21z*a31y, xiy = a21z*a31x - a21x*a31z, xiz = a21x*a31y - a21y*a31x;
+            const double zex = a34y*a24z - a34z*a24y, zey = a34z*a24x - a34x*a24z, zez = a34x*a24y - a34y*a24x;
+            const double t1x = (a1x + a2x + a3x) / 3.0, t2x = (a4x + a2x + a3x) / 3.0;
+            const double t1y = (a1y + a2y + a3y) / 3.0, t2y = (a4y + a2y + a3y) / 3.0;
+            const double t1z = (a1z + a2z + a3z) / 3.0, t2z = (a4z + a2z + a3z) / 3.0;
+            const double nxi = sqrt(xix*xix + xiy*xiy + xiz*xiz), nze = sqrt(zex*zex + zey*zey + zez*zez);
+            const double cost = (xix*zex + xiy*zey + xiz*zez) / nxi / nze;
+            const double cost2 = 1.0 - cost * cost;
+            if (cost2 < eps) continue;
+            const double sgn = ((xix-zex)*(t1x-t2x) + (xiy-zey)*(t1y-t2y) + (xiz-zez)*(t1z-t2z)) >= 0.0 ? 1.0 : -1.0;
+            const double sint = sgn * sqrt(cost2);
+            const double beta = sgn * 2.0 / sqrt(3.0) * p->br * (sint * 1.0 - cost * 0.0) / sqrt(cost2);
+            const double b11 = -beta * cost / (nxi * nxi), b12 = beta / nxi / nze, b22 = -beta * cost / (nze * nze);
+            s->cfx[k1] += b11*(xiy*-a23z - xiz*-a23y) + b12*(zey*-a23z - zez*-a23y);
+            s->cfy[k1] += b11*(xiz*-a23x - xix*-a23z) + b12*(zez*-a23x - zex*-a23z);
+            s->cfz[k1] += b11*(xix*-a23y - xiy*-a23x) + b12*(zex*-a23y - zey*-a23x);
+            s->cfx[k2] += 0.5 * (b11*(xiy*-a31z - xiz*-a31y) + b22*(zey*a34z - zez*a34y) + b12*((xiy*a34z - xiz*a34y) + (zey*-a31z - zez*-a31y)));
+            s->cfy[k2] += 0.5 * (b11*(xiz*-a31x - xix*-a31z) + b22*(zez*a34x - zex*a34z) + b12*((xiz*a34x - xix*a34z) + (zez*-a31x - zex*-a31z)));
+            s->cfz[k2] += 0.5 * (b11*(xix*-a31y - xiy*-a31x) + b22*(zex*a34y - zey*a34x) + b12*((xix*a34y - xiy*a34x) + (zex*-a31y - zey*-a31x)));
+            s->cfx[k3] += 0.5 * (b11*(xiy*a21z - xiz*a21y) + b22*(zey*-a24z - zez*-a24y) + b12*((xiy*-a24z - xiz*-a24y) + (zey*a21z - zez*a21y)));
+            s->cfy[k3] += 0.5 * (b11*(xiz*a21x - xix*a21z) + b22*(zez*-a24x - zex*-a24z) + b12*((xiz*-a24x - xix*-a24z) + (zez*a21x - zex*a21z)));
+            s->cfz[k3] += 0.5 * (b11*(xix*a21y - xiy*a21x) + b22*(zex*-a24y - zey*-a24x) + b12*((xix*-a24y - xiy*-a24x) + (zex*a21y - zey*a21x)));
+        }
+    }
+}
+
+/* stress.cu:580-659 */
 int orc_stress(const orc_params *p, orc_state *s)
 {
     orc_calc_tension(p, s);
     int flag = orc_calc_load(p, s);
     orc_q2f(p, s);
+    orc_bend(p, s);
     return flag;
 }
 

@@ -51,6 +51,7 @@ typedef struct orc_params {
     double xmin, xmax, zmin, zmax;
     /* cells */
     int ncell, vertex, element, mn;
+    double br;           /* BR: bending modulus of fourpoint_bend (0 = no bending) */
 } orc_params;
 
 typedef struct orc_state {
@@ -74,6 +75,7 @@ typedef struct orc_state {
     double *volume0, *gx;                  /* [ncell], [3*ncell] */
     int    iter;                           /* prc->iter */
     int    bicg_iters;                     /* diagnostics: last solve's iterations */
+    int    *ec;                            /* [3*ne] edge-neighbour elements (cel->ec) */
 } orc_state;
 
 /* init2.cu:258-400 (fem_init): link tables and the reference metric from the
@@ -84,8 +86,8 @@ void orc_flu_init(const orc_params *p, orc_state *s);
 /* volume_correction.cu:427-450 (volume_init). */
 void orc_volume_init(const orc_params *p, orc_state *s);
 
-/* stress.cu:580-659 (stress): calc_tension, calc_load (BiCGSTAB), q2f.
- * Bending is zero for the configurations (BR = 0) and is not applied.
+/* stress.cu:580-659 (stress): calc_tension, calc_load (BiCGSTAB), q2f, then
+ * fourpoint_bend when p->br != 0.
  * Returns 0, or the BiCGSTAB flag (1 breakdown, 2 no convergence). */
 int  orc_stress(const orc_params *p, orc_state *s);
 /* ibm.cu:299-369 (ibm_st1): zero, spread, periodic fold. */
@@ -106,6 +108,10 @@ void orc_calc_tension(const orc_params *p, orc_state *s);
 int  orc_calc_load(const orc_params *p, orc_state *s);
 void orc_q2f(const orc_params *p, orc_state *s);
 void orc_calc_volume(const orc_params *p, const orc_state *s, double *volume, double *area);
+/* stress.cu:448-578 (fourpoint_bend): adds the dihedral bending forces of
+ * every edge-neighbour pair to cel->fx/fy/fz (spontaneous angle 0, as
+ * init1.cu:849-850 leaves it). */
+void orc_bend(const orc_params *p, orc_state *s);
 
 int  orc_num_threads(void);
 

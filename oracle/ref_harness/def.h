@@ -11,7 +11,7 @@
  * Case-dependent values (lengths, forcing, moduli, solver tolerance) come
  * from -DREF_* flags (see oracle/Makefile and tests/golden/make_golden.py).
  * Lattice units: Cr = dx = dt = 1, M = 1, RK4, LAMBDA1 = 1 (tau = 3 Df + 1/2),
- * no bending (BR = 0), no adhesion, no white cells.
+ * bending modulus BR from -DREF_BR (default 0), no adhesion, no white cells.
  */
 #ifndef REF_HARNESS_DEF_H
 #define REF_HARNESS_DEF_H
@@ -50,6 +50,9 @@
 #endif
 #ifndef REF_B
 #define REF_B 2.5e-04
+#endif
+#ifndef REF_BR
+#define REF_BR 0.0
 #endif
 #ifndef REF_C
 #define REF_C 100.0
@@ -96,7 +99,7 @@
 #define STANDARDOUTPUT 1000000000
 #define ITRLIMIT    1000000000
 #define CYTOADHESION false
-#define BR          0.0
+#define BR          (REF_BR)
 #define GS          1.0
 #define SR          0.0
 #define Lc          1.0

@@ -106,7 +106,7 @@ int ref_setup(int nx, int ny, int nz, const int *bc, int ncell, int V, int E, co
     for (int ic = 0; ic < ncell; ic++)
         for (int e = 0; e < E; e++)
             for (int k = 0; k < TRI; k++) c.eleH[(ic * E + e) * TRI + k] = tri_local[e * TRI + k] + ic * V;
-    // edge-neighbour elements (cel_init 756-795) for fourpoint_bend, which runs with BR = 0
+    // edge-neighbour elements (cel_init 756-795) for fourpoint_bend
     std::vector<int> ec(ne * TRI, 0), ecn(ne, 0);
     {
         std::map<std::pair<int, int>, std::vector<int>> edges;   // undirected edge -> elements

@@ -25,7 +25,7 @@ thread_local std::string g_create_error;
 
 constexpr float F16_SCALE = 32768.0f;     // (f - w) * 2^15 keeps |g| < 2 inside FP16 range
 constexpr int DEFAULT_SOLVER_ITERS = 16;  // Chebyshev error factor <= 2 * 3^-16 ~ 4.6e-8 (FP32 solve)
-constexpr int KERNELS_PER_STEP = 6;       // step_begin, membrane, spread, lbm, advect, volume
+constexpr int KERNELS_PER_STEP = 6;       // step_begin, membrane, spread, lbm, advect, volume (+ bend when BR != 0)
 
 }  // namespace
 
@@ -54,6 +54,7 @@ struct rbc_handle {
     float *U = nullptr, *Fv = nullptr;
     int *tri = nullptr, *v2e_off = nullptr, *v2e = nullptr;
     int16_t *nbr = nullptr;
+    int4 *visit = nullptr;   // bending visits [E][3], allocated when BR != 0
     double *vol0 = nullptr, *gx = nullptr, *vol_out = nullptr, *area_out = nullptr, *cen_out = nullptr;
     // device scalars: iter, flags, vc_max, vc_last
     int *d_int = nullptr;
@@ -78,6 +79,7 @@ struct rbc_handle {
     int *patch_off = nullptr, *patch_vtx = nullptr, *patch_stride = nullptr;
     int npatch = 1;
 
+    int kernels_per_step() const { return KERNELS_PER_STEP + (p.br != 0.0 && ncell > 0 ? 1 : 0); }
     int *d_iter() { return d_int; }
     int *d_flags() { return d_int + 1; }
     int *d_vcmax() { return d_int + 2; }
@@ -279,6 +281,34 @@ void surface_patches(int V, const double *xr, std::vector<int> &off, std::vector
     }
 }
 
+// Edge-neighbour visits of fourpoint_bend (stress.cu:448-578, cel->ec from
+// init1.cu:755-795): for element e1, its edge neighbours in increasing
+// element order; per neighbour e2 across e1's edge (k2 -> k3 in e1's
+// winding), k1 = e1's third vertex and k4 = e2's vertex off the edge.
+void bend_visits(int V, int E, const int *tri, std::vector<int4> &visit)
+{
+    std::vector<std::vector<int>> el(V);
+    for (int e = 0; e < E; e++) for (int a = 0; a < 3; a++) el[tri[3 * e + a]].push_back(e);
+    visit.assign((size_t)3 * E, make_int4(-1, -1, -1, -1));
+    for (int e1 = 0; e1 < E; e1++) {
+        std::vector<int4> found;   // (e2, k1, k2, k3) ... packed below
+        std::vector<std::pair<int, int4>> nb;
+        for (int a = 0; a < 3; a++) {
+            const int ia = tri[3 * e1 + a], ib = tri[3 * e1 + (a + 1) % 3], ic = tri[3 * e1 + (a + 2) % 3];
+            for (int e2 : el[ia]) {
+                if (e2 == e1) continue;
+                int hb = -1, ha = -1;
+                for (int b = 0; b < 3; b++) { if (tri[3 * e2 + b] == ib) hb = b; if (tri[3 * e2 + b] == ia) ha = b; }
+                if (ha < 0 || hb < 0) continue;
+                nb.push_back({e2, make_int4(ic, ia, ib, tri[3 * e2 + (3 - ha - hb)])});
+                break;
+            }
+        }
+        std::sort(nb.begin(), nb.end(), [](const std::pair<int, int4> &x, const std::pair<int, int4> &y) { return x.first < y.first; });
+        for (size_t k = 0; k < nb.size() && k < 3; k++) visit[(size_t)3 * e1 + k] = nb[k].second;
+    }
+}
+
 int check_params(const rbc_params *p)
 {
     if (!p) return fail(nullptr, RBC_ERR_ARG, "params is NULL");
@@ -291,7 +321,7 @@ int check_params(const rbc_params *p)
     if (!(p->LX > 0) || !(p->LZ > 0)) return fail(nullptr, RBC_ERR_ARG, "LX and LZ must be > 0");
     if (p->M != 1) return fail(nullptr, RBC_ERR_UNSUPPORTED, "only M = 1 (no sub-cycling) is implemented");
     if (p->rk_order != 4) return fail(nullptr, RBC_ERR_UNSUPPORTED, "only RUNGE_KUTTA = 4 is implemented");
-    if (p->br != 0.0) return fail(nullptr, RBC_ERR_UNSUPPORTED, "bending (BR != 0) is not implemented");
+    if (!std::isfinite(p->br)) return fail(nullptr, RBC_ERR_ARG, "BR must be finite");
     if (p->storage != RBC_STORE_F32 && p->storage != RBC_STORE_F16) return fail(nullptr, RBC_ERR_ARG, "unknown storage");
     if (p->law != RBC_LAW_SKALAK && p->law != RBC_LAW_NEOHOOKEAN) return fail(nullptr, RBC_ERR_ARG, "unknown law");
     if (p->solver_iters < 0 || p->solver_iters > 200) return fail(nullptr, RBC_ERR_ARG, "solver_iters out of range");
@@ -343,7 +373,7 @@ void free_all(rbc_handle *h)
     if (h->join) cudaEventDestroy(h->join);
     if (h->side) cudaStreamDestroy(h->side);
     void *ptrs[] = {h->g[0], h->g[1], h->uvr, h->Fx, h->Fy, h->Fz, h->mask2d,
-                    h->X, h->Xd, h->gref, h->erec, h->U, h->Fv, h->tri, h->v2e_off, h->v2e, h->nbr, h->patch_off, h->patch_vtx, h->patch_stride, h->vol0, h->gx,
+                    h->X, h->Xd, h->gref, h->erec, h->U, h->Fv, h->tri, h->v2e_off, h->v2e, h->nbr, h->visit, h->patch_off, h->patch_vtx, h->patch_stride, h->vol0, h->gx,
                     h->vol_out, h->area_out, h->cen_out, h->d_int, h->d_drive, h->staging};
     for (void *q : ptrs) if (q) cudaFree(q);
     if (h->stream) cudaStreamDestroy(h->stream);
@@ -377,6 +407,19 @@ int launch_spread_stage(rbc_handle *h)
     a.npatch = h->npatch;
     a.Fx = h->Fx; a.Fy = h->Fy; a.Fz = h->Fz; a.mask2d = h->mask2d; a.flags = h->d_flags();
     launch_spread(h->geo, a, h->stream);
+    h->launches++;
+    CK_LAUNCH();
+    return RBC_OK;
+}
+
+// fourpoint_bend (stress.cu:621-623) on cel->x, added to the membrane forces
+int launch_bend_stage(rbc_handle *h)
+{
+    if (h->ncell == 0 || h->p.br == 0.0) return RBC_OK;
+    BendArgs a{};
+    a.X = h->X; a.nv = h->nv; a.V = h->V; a.v2e_off = h->v2e_off; a.v2e = h->v2e; a.visit = h->visit;
+    a.LX = h->p.LX; a.LZ = h->p.LZ; a.coef = 2.0 / std::sqrt(3.0) * h->p.br; a.Fv = h->Fv;
+    launch_bend(a, h->stream);
     h->launches++;
     CK_LAUNCH();
     return RBC_OK;
@@ -454,6 +497,7 @@ int enqueue_step(rbc_handle *h, StepForm form = STEP_WHOLE)
     CK_LAUNCH();
     if ((rc = launch_stress(h))) return rc;
     if (pipelined) CK(cudaStreamWaitEvent(h->stream, h->join, 0));
+    if ((rc = launch_bend_stage(h))) return rc;   // reads cel->x, after the correction
     if ((rc = launch_spread_stage(h))) return rc;
     if ((rc = launch_lbm_stage(h))) return rc;
     if ((rc = launch_advect_stage(h))) return rc;
@@ -710,6 +754,15 @@ int rbc_create(const rbc_params *p, const rbc_mesh *mesh, const int *bc, rbc_han
         TRY(dalloc(h, &h->U, 3 * h->nv)); TRY(dalloc(h, &h->Fv, 3 * h->nv));
         TRY(dalloc(h, &h->tri, 3 * h->E)); TRY(dalloc(h, &h->v2e_off, h->V + 1)); TRY(dalloc(h, &h->v2e, packed.size()));
         TRY(dalloc(h, &h->nbr, 6 * h->V));
+        if (p->br != 0.0) {
+            std::vector<int4> visit;
+            bend_visits(h->V, h->E, mesh->tri, visit);
+            TRY(dalloc(h, &h->visit, visit.size()));
+            if (cudaMemcpy(h->visit, visit.data(), sizeof(int4) * visit.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
+                h->err = "device initialisation failed";
+                return bail(RBC_ERR_CUDA);
+            }
+        }
         TRY(dalloc(h, &h->patch_off, poff.size())); TRY(dalloc(h, &h->patch_vtx, pvtx.size()));
         TRY(dalloc(h, &h->patch_stride, pstride.size()));
         TRY(dalloc(h, &h->vol0, h->ncell)); TRY(dalloc(h, &h->gx, 3 * h->ncell));
@@ -910,7 +963,8 @@ int rbc_stress(rbc_handle *h)
 {
     if (!h) return RBC_ERR_ARG;
     RBC_DEVICE_GUARD(h);
-    return launch_stress(h);
+    const int rc = launch_stress(h);
+    return rc ? rc : launch_bend_stage(h);
 }
 
 int rbc_ibm_st1(rbc_handle *h)
@@ -982,7 +1036,7 @@ int rbc_step(rbc_handle *h, int nsteps)
         const StepForm form = !pipe ? STEP_WHOLE : k == 0 ? STEP_BODY : STEP_PIPELINED;
         CK(cudaGraphLaunch(h->graph[form][h->cur], h->stream));
         h->cur ^= 1;
-        h->launches += KERNELS_PER_STEP;
+        h->launches += h->kernels_per_step();
     }
     if (pipe) {
         h->launches -= 1;   // step n's correction, counted with its step, is launched here
@@ -1007,6 +1061,7 @@ int rbc_profile_steps(rbc_handle *h, int nsteps, double *kernel_ms)
         h->launches++;
         cudaEventRecord(ev[1], h->stream);
         if (!rc) rc = launch_stress(h);
+        if (!rc) rc = launch_bend_stage(h);   // timed with the membrane pass
         cudaEventRecord(ev[2], h->stream);
         if (!rc) rc = launch_spread_stage(h);
         cudaEventRecord(ev[3], h->stream);
@@ -1192,7 +1247,7 @@ int rbc_batch_step(rbc_batch *b, int nsteps)
         rbc_handle *h = b->h[i];
         if (nsteps & 1) h->cur ^= 1;
         h->iter += nsteps;
-        h->launches += (long long)KERNELS_PER_STEP * nsteps;
+        h->launches += (long long)h->kernels_per_step() * nsteps;
         CKB(cudaStreamWaitEvent(h->stream, b->done, 0));
     }
     return RBC_OK;

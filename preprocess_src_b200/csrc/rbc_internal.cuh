@@ -143,6 +143,18 @@ struct MembraneArgs {
     int priority;             // launch priority (cudaLaunchAttributePriority)
 };
 int  membrane_smem_bytes(int V);
+
+// fourpoint_bend (stress.cu:448-578): added to Fv after the membrane forces
+struct BendArgs {
+    const double *X; long long nv;   // cel->x, [3][nv]
+    int V;
+    const int *v2e_off, *v2e;        // vertex -> element incidence of the shared mesh
+    const int4 *visit;               // [E][3]: (k1, k2, k3, k4) local ids per edge-neighbour visit, k1 < 0: none
+    double LX, LZ;
+    double coef;                     // (2 / sqrt 3) BR
+    float *Fv;
+};
+void launch_bend(const BendArgs &a, cudaStream_t s);
 void launch_membrane(const MembraneArgs &a, bool fp64, cudaStream_t s);
 
 struct VolumeArgs {

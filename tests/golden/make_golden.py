@@ -53,6 +53,9 @@ def golden_cases():
                                                      centers_duct=[(2.5, 9.6, 9.4), (18.0, 9.3, 9.7)],
                                                      subdiv=3, radius=5.0, seed=22, g=4e-5, Gs=2e-3,
                                                      residual=1e-12),
+        "g3_duct24x20x20_1c_bend": configs.duct_case("g3_duct24x20x20_1c_bend", 24, 20, 20,
+                                                     centers_duct=[(12.3, 9.6, 9.4)], subdiv=3, radius=5.5,
+                                                     seed=23, g=4e-5, Gs=2e-3, br=0.02, residual=1e-12),
     }
 
 
@@ -65,7 +68,7 @@ def ref_defs(case) -> str:
     df = (2.0 * p["tau"] - 1.0) / 6.0
     return (f"-DREF_LX={p['LX']!r} -DREF_LY={float(p['ny'] - 4)!r} -DREF_LZ={p['LZ']!r} -DREF_P={p['P']!r} "
             f"-DREF_B={p['B']!r} -DREF_C={p['C']!r} -DREF_DF={df!r} -DREF_RESIDUAL={p['residual']!r} "
-            f"-DREF_ITRMAX={p['itrmax']}")
+            f"-DREF_ITRMAX={p['itrmax']} -DREF_BR={p['br']!r}")
 
 
 def build():

@@ -55,7 +55,7 @@ def test_rejects_unsupported_options(native_lib):
     case = configs.small_duct()
     assert _create(case, M=2)[0] == N.RBC_ERR_UNSUPPORTED
     assert _create(case, rk_order=2)[0] == N.RBC_ERR_UNSUPPORTED
-    assert _create(case, br=1e-3)[0] == N.RBC_ERR_UNSUPPORTED
+    assert _create(case, br=float("inf"))[0] == N.RBC_ERR_ARG
     assert _create(case, tau=0.5)[0] == N.RBC_ERR_ARG
     assert _create(case, storage=7)[0] == N.RBC_ERR_ARG
 

@@ -92,6 +92,24 @@ def test_stress_matches_oracle(developed, oracle_mod):
         assert flags & 8 == 0, "load solve residual flag"
 
 
+def test_stress_with_bending_matches_oracle(oracle_mod, native_lib):
+    """rbc_stress with BR != 0: the Skalak forces plus fourpoint_bend
+    (stress.cu:448-578) on cel->x, against the oracle after a developed flow."""
+    case = parity_case(br=0.02)
+    o = oracle_mod.Oracle(case)
+    o.step(20)
+    sim = load(o)
+    c = clone(oracle_mod, o)
+    assert c.stress() == 0
+    sim.stress()
+    got = sim.export_cells()
+    ref = np.concatenate([c["cfx"], c["cfy"], c["cfz"]])
+    mine = np.concatenate([got["fx"], got["fy"], got["fz"]])
+    err = rel_l2(mine, ref)
+    print(f"stress + bending: force rel L2 {err:.3e}, max|f| {np.abs(ref).max():.3e}")
+    assert np.abs(ref).max() > 1e-3 and err <= 1e-5
+
+
 def test_narrow_duct_cell_matches_oracle(oracle_mod, native_lib):
     """A 32-wide duct (the reference's x period LX = 28) with a 15.6-wide cell
     whose first vertex sits near the cell's edge in x: edge vectors must take

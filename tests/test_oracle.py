@@ -159,3 +159,46 @@ def test_drive_schedule(oracle_mod):
     assert np.abs(o["wn"]).max() == 0.0
     o.step(1)
     assert o["wn"].max() > 0.0
+
+
+def _bend_energy(x, y, z, tri, br):
+    """(2 / sqrt 3) BR sum over edge-neighbour pairs of (1 - cos theta), theta
+    the angle between the two outward triangle normals."""
+    p = np.stack([x, y, z], axis=1)
+    n = np.cross(p[tri[:, 1]] - p[tri[:, 0]], p[tri[:, 2]] - p[tri[:, 0]])
+    n /= np.linalg.norm(n, axis=1)[:, None]
+    edges = {}
+    for e, t in enumerate(tri):
+        for a in range(3):
+            edges.setdefault(tuple(sorted((t[a], t[(a + 1) % 3]))), []).append(e)
+    pairs = np.array([v for v in edges.values() if len(v) == 2])
+    cos = np.einsum("ij,ij->i", n[pairs[:, 0]], n[pairs[:, 1]])
+    return 2.0 / math.sqrt(3.0) * br * float((1.0 - cos).sum())
+
+
+def test_bending_force_is_energy_gradient(oracle_mod):
+    """stress.cu:448-578 with spontaneous angle 0 (init1.cu:849-850): the
+    four-point forces are minus the gradient of (2/sqrt 3) BR sum (1 - cos
+    theta) over edge-neighbour pairs; they have no net force or torque."""
+    case = configs.small_duct(subdiv=2, radius=5.0, br=0.05, Gs=1e-3)
+    rng = np.random.default_rng(5)
+    o = oracle_mod.Oracle(case)
+    for k in ("x", "y", "z"):   # bending reads cel->x: perturb it after the setup
+        o[k][:] += rng.normal(scale=0.15, size=case.vertex)
+    for k in ("cfx", "cfy", "cfz"):
+        o[k][:] = 0.0
+    oracle_mod.lib().orc_bend(oracle_mod.C.byref(o.p), oracle_mod.C.byref(o.s))
+    f = np.stack([o["cfx"], o["cfy"], o["cfz"]], axis=1)
+    assert np.abs(f).max() > 1e-3
+    assert np.abs(f.sum(axis=0)).max() <= 1e-12 * np.abs(f).max() * case.vertex
+    pos = np.stack([o["x"], o["y"], o["z"]], axis=1)
+    torque = np.cross(pos - pos.mean(axis=0), f).sum(axis=0)
+    assert np.abs(torque).max() <= 1e-10 * np.abs(f).max() * case.vertex
+    h = 1e-6
+    for i in rng.choice(case.vertex, 8, replace=False):
+        for d in range(3):
+            xp, xm = [pos[:, c].copy() for c in range(3)], [pos[:, c].copy() for c in range(3)]
+            xp[d][i] += h
+            xm[d][i] -= h
+            g = (_bend_energy(*xp, case.tri, 0.05) - _bend_energy(*xm, case.tri, 0.05)) / (2 * h)
+            assert abs(-g - f[i, d]) <= 1e-6 * np.abs(f).max(), (i, d, -g, f[i, d])
