@@ -50,11 +50,13 @@ def parse():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="dense", choices=["dense", "single", "capillaries"],
+    ap.add_argument("--workload", default="dense", choices=["dense", "single", "capillaries", "adjoint"],
                     help="dense: config 2 (the headline); single: config 1; capillaries: config 4 "
                          "(512 uneven capillaries as one batch vs one after another)")
     ap.add_argument("--capillaries", type=int, default=512, help="number of capillaries (capillaries workload)")
     ap.add_argument("--storage", default="f32", choices=["f32", "f16"])
+    ap.add_argument("--adjoint-steps", type=int, default=2000, help="steps of the recorded run (adjoint workload)")
+    ap.add_argument("--ckpt", type=int, default=100, help="checkpoint interval (adjoint workload)")
     ap.add_argument("--profile-steps", type=int, default=20)
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU-baseline sample budget")
     ap.add_argument("--no-e2e", action="store_true")
@@ -334,6 +336,65 @@ def run_capillaries(args, world, rank, local):
             "clocks": clk.summary()}
 
 
+def run_adjoint(args, world, rank, local):
+    """Config 5: gradient of the cell-shape loss through --adjoint-steps steps
+    of the single-cell duct with a checkpoint every --ckpt steps.  Times, with
+    CUDA events on the library's stream: plain forward steps (rbc_step), the
+    recorded forward (rbc_adjoint_record) and the reverse sweep
+    (rbc_adjoint_backward, which recomputes each segment once).  value = device
+    milliseconds per step of the reverse sweep."""
+    import numpy as np
+    import torch
+
+    from preprocess_src_b200 import configs
+    from preprocess_src_b200.adjoint import InitialState
+    from preprocess_src_b200.step import Simulation
+
+    dev = local
+    torch.cuda.set_device(dev)
+    n = args.adjoint_steps
+    case = configs.single_cell_duct()
+    sim = Simulation(case, device=dev)
+    init = InitialState(sim)
+    st = torch.cuda.ExternalStream(sim.stream, device=torch.device("cuda", dev))
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    sim.step(args.warmup)
+    init.restore(sim)
+    barrier(world)
+    with ClockSampler(dev) as clk:
+        time.sleep(0.3)
+        ev[0].record(st)
+        sim.step(n)
+        ev[1].record(st)
+        ev[1].synchronize()
+        init.restore(sim)
+        ev[2].record(st)
+        sim.adjoint_record(n, args.ckpt)
+        ev[3].record(st)
+        ev[3].synchronize()
+        c = sim.export_cells()
+        # seed: gradient of the mean squared distance to the initial shape
+        x0 = np.stack([init.x, init.y, init.z])
+        seed = (2.0 / sim.nv) * (np.stack([c["x"], c["y"], c["z"]]) - x0)
+        r = sim.adjoint_backward(seed[0], seed[1], seed[2])
+    fwd_ms, rec_ms, bwd_ms = ev[0].elapsed_time(ev[1]), ev[2].elapsed_time(ev[3]), r["ms"]
+    bwd_max = allreduce_max(bwd_ms, world)
+    sim.close()
+    if rank != 0:
+        return None
+    fluid = case.fluid_nodes()
+    return {"metric": "adjoint ms per step, single-cell duct (config 5)", "value": round(bwd_max / n, 4),
+            "unit": "ms/step", "n_gpus": world, "steps": n, "warmup": args.warmup,
+            "ms_per_step": round(bwd_max / n, 4), "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": case.name, "fluid_nodes": fluid, "vertices": sim.nv, "ckpt_every": args.ckpt,
+                       "l2": "lattice and checkpoints below L2 size: steady-state timing of a small case"},
+            "forward_ms_per_step": round(fwd_ms / n, 4), "record_ms_per_step": round(rec_ms / n, 4),
+            "backward_over_forward": round(bwd_ms / fwd_ms, 2),
+            "grad": {"dL/dP": r["grad"][0], "dL/dB": r["grad"][1], "dL/dC": r["grad"][2]},
+            "adjoint_flags": r["flags"], "clocks": clk.summary()}
+
+
 def run_e2e(args, case, dev, world):
     """Public-API run with host buffers (pinned), copies inside the timed region."""
     import numpy as np
@@ -471,7 +532,8 @@ def main():
             print(json.dumps(res), flush=True)
         return
     world, rank, local = dist_setup(args)
-    res = run_capillaries(args, world, rank, local) if args.workload == "capillaries" else run_ours(args, world, rank, local)
+    runner = {"capillaries": run_capillaries, "adjoint": run_adjoint}.get(args.workload, run_ours)
+    res = runner(args, world, rank, local)
     if res is not None:
         print(json.dumps(res), flush=True)
     if world > 1:

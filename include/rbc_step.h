@@ -222,6 +222,46 @@ int rbc_batch_get_chain(const rbc_batch *b, int *chain);
  * NULL).  The timed steps are real steps: every simulation advances by them. */
 int rbc_batch_autotune(rbc_batch *b, int steps_per_trial, int *chain_out);
 
+/* ---- adjoint (gradients through the step) -------------------------------- */
+
+/* No counterpart in the reference.  Exact discrete adjoint of this library's
+ * own step (membrane, spread, collide-stream, RK4 advection, volume
+ * correction) with checkpointing: gradients of a function L of the final
+ * vertex positions (cel->x) with respect to the coefficients P, B, C and to
+ * the initial positions.  FP32 population storage and BR = 0 only
+ * (RBC_ERR_UNSUPPORTED otherwise).
+ *
+ * rbc_adjoint_record: runs nsteps steps from the current state (as rbc_step
+ * would) and keeps a checkpoint of the state every ckpt_every steps and after
+ * the last.  Device memory: (nsteps / ckpt_every + 1) checkpoints of
+ * 4 Q B per node + 48 B per vertex, and ckpt_every steps of stored stages
+ * (104 B per node + 84 B per vertex) used by the backward sweep.
+ * Synchronous. */
+int rbc_adjoint_record(rbc_handle *h, int nsteps, int ckpt_every);
+/* rbc_adjoint_backward: reverse sweep of the recorded run.
+ *   xbar, ybar, zbar  host [nv] each: dL/d(final cel->x, y, z); NULL = 0
+ *   grad              host [3] out: dL/dP, dL/dB, dL/dC
+ *   dx0, dy0, dz0     host [nv] each, may be NULL: dL/d(initial positions),
+ *                     the sum of the adjoints of the initial cel->x and
+ *                     fem->xd (equal at the start of a run from rbc_create)
+ *   adj_flags         may be NULL: bit 0 set when some step's volume
+ *                     correction moved the vertices more than 16 times (the
+ *                     moves beyond are not differentiated)
+ *   ms                may be NULL: device time of the sweep (recomputation
+ *                     included), milliseconds
+ * Each segment between checkpoints is recomputed once, stage by stage, then
+ * reversed.  The handle is left at the state after the recorded run.  May be
+ * called again with other seeds.  Synchronous.  With the reference's macros:
+ * P = g / 2 and B = Gs / 2 (dx = dt = 1), so dL/dg = dL/dP / 2 and
+ * dL/dGs = dL/dB / 2. */
+int rbc_adjoint_backward(rbc_handle *h, const double *xbar, const double *ybar, const double *zbar,
+                         double *grad, double *dx0, double *dy0, double *dz0, int *adj_flags, float *ms);
+/* Replaces the coefficients P (drive), B (IB force) and C (area dilation) of
+ * a handle.  The handle's step graphs are rebuilt on the next rbc_step and a
+ * recorded adjoint run is dropped; a batch holding the handle must be
+ * destroyed and created again.  Synchronous. */
+int rbc_set_coefficients(rbc_handle *h, double P, double B, double C);
+
 /* ---- without allocation -------------------------------------------------- */
 
 /* No counterpart in the reference.  Per-cell FP64 volume, area and vertex

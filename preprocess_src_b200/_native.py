@@ -78,6 +78,9 @@ _SIGS = {
     "rbc_batch_set_chain": [_H, C.c_int],
     "rbc_batch_get_chain": [_H, _IP],
     "rbc_batch_autotune": [_H, C.c_int, _IP],
+    "rbc_adjoint_record": [_H, C.c_int, C.c_int],
+    "rbc_adjoint_backward": [_H, _DP, _DP, _DP, _DP, _DP, _DP, _DP, _IP, C.POINTER(C.c_float)],
+    "rbc_set_coefficients": [_H, C.c_double, C.c_double, C.c_double],
 }
 _RESTYPE = {"rbc_last_error": C.c_char_p, "rbc_batch_last_error": C.c_char_p}
 

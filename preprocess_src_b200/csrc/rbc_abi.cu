@@ -34,6 +34,9 @@ namespace rbc {
 void set_last_error(const std::string &msg) { g_create_error = msg; }
 }
 
+struct AdjointState;
+void adjoint_free(AdjointState *a);
+
 struct rbc_handle {
     rbc_params p{};
     Geom geo{};
@@ -78,6 +81,7 @@ struct rbc_handle {
     int device = 0;
     int *patch_off = nullptr, *patch_vtx = nullptr, *patch_stride = nullptr;
     int npatch = 1;
+    AdjointState *adj = nullptr;                      // checkpoints and buffers of the adjoint, on first use
 
     int kernels_per_step() const { return KERNELS_PER_STEP + (p.br != 0.0 && ncell > 0 ? 1 : 0); }
     int *d_iter() { return d_int; }
@@ -376,6 +380,8 @@ void free_all(rbc_handle *h)
                     h->X, h->Xd, h->gref, h->erec, h->U, h->Fv, h->tri, h->v2e_off, h->v2e, h->nbr, h->visit, h->patch_off, h->patch_vtx, h->patch_stride, h->vol0, h->gx,
                     h->vol_out, h->area_out, h->cen_out, h->d_int, h->d_drive, h->staging};
     for (void *q : ptrs) if (q) cudaFree(q);
+    adjoint_free(h->adj);
+    h->adj = nullptr;
     if (h->stream) cudaStreamDestroy(h->stream);
 }
 
@@ -1294,6 +1300,336 @@ int rbc_batch_autotune(rbc_batch *b, int steps_per_trial, int *chain_out)
     if (rc != RBC_OK) return rc;
     if ((rc = rbc_batch_set_chain(b, best))) return rc;
     if (chain_out) *chain_out = best;
+    return RBC_OK;
+}
+
+}  // extern "C"
+
+// ---- adjoint: checkpointed reverse sweep -----------------------------------
+//
+// rbc_adjoint_record runs the forward steps with the step graphs and keeps a
+// checkpoint of the state (populations, cel->x, fem->xd, centroids, iter)
+// every K steps, plus the state after the run.  rbc_adjoint_backward then
+// takes the segments in reverse order: it restores the segment's checkpoint,
+// recomputes the segment's steps stage by stage while storing what the
+// reverse stages read (populations, positions, membrane forces, lattice force,
+// velocity field, positions before the correction), and runs the adjoint
+// kernels of adjoint.cu step by step backwards through the segment.  Memory:
+// checkpoints (Q floats per node + 48 B per vertex) per segment, and K steps
+// of stored stages (26 floats per node + 84 B per vertex) for the segment in
+// flight.
+
+struct AdjointState {
+    int K = 0, nseg_cap = 0, K_cap = 0;
+    int nsteps = 0, nseg = 0;
+    bool valid = false;
+    std::vector<int> ck_iter;            // iter at each checkpoint
+    std::vector<void *> bufs;            // every allocation below, for adjoint_free
+    // checkpoints [nseg + 1]
+    float *ck_g = nullptr; double *ck_X = nullptr, *ck_Xd = nullptr, *ck_gx = nullptr;
+    // stored stages of one segment [K]
+    float *sg = nullptr, *sF = nullptr, *sFv = nullptr; float4 *suvr = nullptr;
+    double *sX = nullptr, *sXd = nullptr, *sXa = nullptr, *sgx = nullptr;
+    // adjoint state and scratch
+    float *gbar[2] = {nullptr, nullptr}, *gbar_pre = nullptr, *Fbar = nullptr; float4 *ubar = nullptr;
+    double *Xbar = nullptr, *Xdbar = nullptr, *Xabar = nullptr, *Fvbar = nullptr;
+    double *mscr = nullptr, *hist = nullptr, *escr = nullptr, *pbar = nullptr;
+    int *status = nullptr;
+    // outputs of the last recorded step (velocity field, vertex velocities and forces)
+    float4 *fin_uvr = nullptr; float *fin_U = nullptr, *fin_Fv = nullptr;
+    int kmax = 16;                       // volume-correction moves reversed per step
+};
+
+void adjoint_free(AdjointState *a)
+{
+    if (!a) return;
+    for (void *p : a->bufs) if (p) cudaFree(p);
+    delete a;
+}
+
+namespace {
+
+template <typename T>
+int adj_alloc(rbc_handle *h, T **p, size_t count)
+{
+    CK(cudaMalloc((void **)p, sizeof(T) * (count ? count : 1)));
+    h->adj->bufs.push_back((void *)*p);
+    return RBC_OK;
+}
+
+// checkpoint and segment buffers for nseg segments of K steps
+int adjoint_reserve(rbc_handle *h, int K, int nseg)
+{
+    if (!h->adj) h->adj = new (std::nothrow) AdjointState();
+    if (!h->adj) return fail(h, RBC_ERR_CUDA, "out of host memory");
+    AdjointState *a = h->adj;
+    if (a->K_cap >= K && a->nseg_cap >= nseg) return RBC_OK;
+    for (void *p : a->bufs) if (p) cudaFree(p);
+    a->bufs.clear();
+    const size_t n = (size_t)h->geo.nint, nq = (size_t)Q * n, nv3 = 3 * (size_t)h->nv, N3 = 3 * (size_t)h->ncell;
+    const size_t nck = (size_t)nseg + 1, Kc = (size_t)K;
+    int rc;
+#define TRYA(x) do { if ((rc = (x))) { h->err = "adjoint: out of device memory (" #x ")"; return rc; } } while (0)
+    TRYA(adj_alloc(h, &a->ck_g, nck * nq)); TRYA(adj_alloc(h, &a->ck_X, nck * nv3));
+    TRYA(adj_alloc(h, &a->ck_Xd, nck * nv3)); TRYA(adj_alloc(h, &a->ck_gx, nck * N3));
+    TRYA(adj_alloc(h, &a->sg, Kc * nq)); TRYA(adj_alloc(h, &a->sF, Kc * 3 * n)); TRYA(adj_alloc(h, &a->sFv, Kc * nv3));
+    TRYA(adj_alloc(h, &a->suvr, Kc * n));
+    TRYA(adj_alloc(h, &a->sX, Kc * nv3)); TRYA(adj_alloc(h, &a->sXd, Kc * nv3)); TRYA(adj_alloc(h, &a->sXa, Kc * nv3));
+    TRYA(adj_alloc(h, &a->sgx, Kc * N3));
+    TRYA(adj_alloc(h, &a->gbar[0], nq)); TRYA(adj_alloc(h, &a->gbar[1], nq)); TRYA(adj_alloc(h, &a->gbar_pre, nq));
+    TRYA(adj_alloc(h, &a->Fbar, 3 * n)); TRYA(adj_alloc(h, &a->ubar, n));
+    TRYA(adj_alloc(h, &a->Xbar, nv3)); TRYA(adj_alloc(h, &a->Xdbar, nv3)); TRYA(adj_alloc(h, &a->Xabar, nv3));
+    TRYA(adj_alloc(h, &a->Fvbar, nv3)); TRYA(adj_alloc(h, &a->mscr, 7 * (size_t)h->ne));
+    TRYA(adj_alloc(h, &a->hist, (size_t)a->kmax * nv3)); TRYA(adj_alloc(h, &a->escr, 9 * (size_t)h->ne));
+    TRYA(adj_alloc(h, &a->pbar, 4)); TRYA(adj_alloc(h, &a->status, 1));
+    TRYA(adj_alloc(h, &a->fin_uvr, n)); TRYA(adj_alloc(h, &a->fin_U, nv3)); TRYA(adj_alloc(h, &a->fin_Fv, nv3));
+#undef TRYA
+    a->K_cap = K;
+    a->nseg_cap = nseg;
+    return RBC_OK;
+}
+
+int d2d(rbc_handle *h, void *dst, const void *src, size_t bytes)
+{
+    if (bytes) CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, h->stream));
+    return RBC_OK;
+}
+
+// state <-> checkpoint k
+int adjoint_save(rbc_handle *h, int k)
+{
+    AdjointState *a = h->adj;
+    const size_t nq = (size_t)Q * h->geo.nint, nv3 = 3 * (size_t)h->nv, N3 = 3 * (size_t)h->ncell;
+    int rc;
+    if ((rc = d2d(h, a->ck_g + k * nq, h->g[h->cur], 4 * nq))) return rc;
+    if ((rc = d2d(h, a->ck_X + k * nv3, h->X, 8 * nv3))) return rc;
+    if ((rc = d2d(h, a->ck_Xd + k * nv3, h->Xd, 8 * nv3))) return rc;
+    if ((rc = d2d(h, a->ck_gx + k * N3, h->gx, 8 * N3))) return rc;
+    a->ck_iter[k] = h->iter;
+    return RBC_OK;
+}
+
+int adjoint_restore(rbc_handle *h, int k)
+{
+    AdjointState *a = h->adj;
+    const size_t n = (size_t)h->geo.nint, nq = (size_t)Q * n, nv3 = 3 * (size_t)h->nv, N3 = 3 * (size_t)h->ncell;
+    int rc;
+    if ((rc = d2d(h, h->g[h->cur], a->ck_g + k * nq, 4 * nq))) return rc;
+    if ((rc = d2d(h, h->X, a->ck_X + k * nv3, 8 * nv3))) return rc;
+    if ((rc = d2d(h, h->Xd, a->ck_Xd + k * nv3, 8 * nv3))) return rc;
+    if ((rc = d2d(h, h->gx, a->ck_gx + k * N3, 8 * N3))) return rc;
+    CK(cudaMemsetAsync(h->Fx, 0, 4 * n, h->stream));
+    CK(cudaMemsetAsync(h->Fy, 0, 4 * n, h->stream));
+    CK(cudaMemsetAsync(h->Fz, 0, 4 * n, h->stream));
+    h->force_pending = false;
+    h->iter = a->ck_iter[k];
+    return prepare_steps(h);
+}
+
+// recompute the steps of segment s, storing what the reverse stages read
+int adjoint_recompute(rbc_handle *h, int s, int len)
+{
+    AdjointState *a = h->adj;
+    const size_t n = (size_t)h->geo.nint, nq = (size_t)Q * n, nv3 = 3 * (size_t)h->nv, N3 = 3 * (size_t)h->ncell;
+    int rc;
+    if ((rc = adjoint_restore(h, s))) return rc;
+    for (int t = 0; t < len; t++) {
+        if ((rc = d2d(h, a->sg + t * nq, h->g[h->cur], 4 * nq))) return rc;
+        if ((rc = d2d(h, a->sX + t * nv3, h->X, 8 * nv3))) return rc;
+        if ((rc = d2d(h, a->sXd + t * nv3, h->Xd, 8 * nv3))) return rc;
+        if ((rc = d2d(h, a->sgx + t * N3, h->gx, 8 * N3))) return rc;
+        launch_step_begin(h->d_iter(), h->d_drive, h->p.P, h->p.flowstart, h->p.freq, h->p.dt, h->stream);
+        h->launches++;
+        CK_LAUNCH();
+        if ((rc = launch_stress(h))) return rc;
+        if ((rc = d2d(h, a->sFv + t * nv3, h->Fv, 4 * nv3))) return rc;
+        if ((rc = launch_spread_stage(h))) return rc;
+        if ((rc = d2d(h, a->sF + t * 3 * n, h->Fx, 4 * n))) return rc;
+        if ((rc = d2d(h, a->sF + t * 3 * n + n, h->Fy, 4 * n))) return rc;
+        if ((rc = d2d(h, a->sF + t * 3 * n + 2 * n, h->Fz, 4 * n))) return rc;
+        if ((rc = launch_lbm_stage(h))) return rc;
+        if ((rc = d2d(h, a->suvr + t * n, h->uvr, 16 * n))) return rc;
+        if ((rc = launch_advect_stage(h))) return rc;
+        if ((rc = d2d(h, a->sXa + t * nv3, h->Xd, 8 * nv3))) return rc;
+        if ((rc = launch_volume_stage(h, h->stream))) return rc;
+        h->iter++;
+    }
+    return RBC_OK;
+}
+
+// reverse the steps of segment s (already recomputed); the adjoint of the
+// populations after the segment is in gbar[*gb] and moves to gbar[*gb ^ 1]
+// per step
+int adjoint_reverse(rbc_handle *h, int s, int len, int *gb)
+{
+    AdjointState *a = h->adj;
+    const size_t n = (size_t)h->geo.nint, nq = (size_t)Q * n, nv3 = 3 * (size_t)h->nv, N3 = 3 * (size_t)h->ncell;
+    const Geom &g = h->geo;
+    for (int t = len - 1; t >= 0; t--) {
+        const int it = a->ck_iter[s] + t + 1;   // the iteration number step_begin gave this step
+        const double dfac = drive_factor(h->p, it);
+        if (h->ncell > 0) {
+            VolumeAdjArgs va{};
+            va.Xa = a->sXa + t * nv3; va.gx = a->sgx + t * N3; va.vol0 = h->vol0;
+            va.tri = h->tri; va.v2e_off = h->v2e_off; va.v2e = h->v2e;
+            va.X_bar = a->Xbar; va.Xd_bar = a->Xdbar; va.Xa_bar = a->Xabar;
+            va.hist = a->hist; va.escr = a->escr; va.status = a->status;
+            va.nv = h->nv; va.V = h->V; va.E = h->E; va.ncell = h->ncell; va.kmax = a->kmax;
+            launch_volume_adjoint(g, va, h->stream);
+            CK_LAUNCH();
+        }
+        CK(cudaMemsetAsync(a->ubar, 0, 16 * n, h->stream));
+        if (h->ncell > 0) {
+            launch_advect_adjoint(g, a->sX + t * nv3, a->suvr + t * n, a->Xabar, a->Xbar, (float *)a->ubar, h->nv,
+                                  h->p.dt * h->p.M, h->d_flags(), h->stream);
+            CK_LAUNCH();
+        }
+        LbmAdjArgs la{};
+        la.gin = a->sg + t * nq;
+        la.Fx = a->sF + t * 3 * n; la.Fy = la.Fx + n; la.Fz = la.Fx + 2 * n;
+        la.mask2d = h->mask2d; la.gbar_out = a->gbar[*gb]; la.ubar = a->ubar;
+        la.gbar_pre = a->gbar_pre; la.gbar_in = a->gbar[*gb ^ 1]; la.Fbar = a->Fbar; la.pbar = a->pbar;
+        la.pd = (float)(h->p.P * dfac); la.Bc = (float)h->p.B; la.omega = (float)(1.0 / h->p.tau); la.Cr = (float)h->p.Cr;
+        la.dfac = dfac;
+        launch_lbm_adjoint(g, la, h->stream);
+        CK_LAUNCH();
+        *gb ^= 1;
+        if (h->ncell > 0) {
+            launch_spread_adjoint(g, a->sX + t * nv3, a->sFv + t * nv3, a->Fbar, h->mask2d, a->Fvbar, a->Xbar, h->nv,
+                                  h->stream);
+            CK_LAUNCH();
+            MembraneAdjArgs ma{};
+            ma.Xd = a->sXd + t * nv3; ma.nv = h->nv; ma.gref = h->gref;
+            ma.tri = h->tri; ma.v2e_off = h->v2e_off; ma.v2e = h->v2e; ma.nbr = h->nbr;
+            ma.Fv = a->sFv + t * nv3; ma.Fv_bar = a->Fvbar; ma.Xd_bar = a->Xdbar; ma.scratch = a->mscr;
+            ma.cbar = a->pbar + 2;
+            ma.V = h->V; ma.E = h->E; ma.ncell = h->ncell;
+            ma.C = h->p.C; ma.rgs = h->p.rgs; ma.law = h->p.law; ma.LX = h->p.LX; ma.LZ = h->p.LZ;
+            ma.niter = h->p.solver_iters > 0 ? h->p.solver_iters : DEFAULT_SOLVER_ITERS;
+            launch_membrane_adjoint(ma, h->stream);
+            CK_LAUNCH();
+        }
+    }
+    return RBC_OK;
+}
+
+int adjoint_supported(rbc_handle *h)
+{
+    if (h->p.storage != RBC_STORE_F32) return fail(h, RBC_ERR_UNSUPPORTED, "the adjoint needs FP32 population storage");
+    if (h->p.br != 0.0) return fail(h, RBC_ERR_UNSUPPORTED, "the adjoint does not cover bending (BR != 0)");
+    if (h->geo.nzc > 65535) return fail(h, RBC_ERR_UNSUPPORTED, "the adjoint handles at most 65535 periodic planes");
+    return RBC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int rbc_adjoint_record(rbc_handle *h, int nsteps, int ckpt_every)
+{
+    if (!h || nsteps < 1 || ckpt_every < 1) return RBC_ERR_ARG;
+    RBC_DEVICE_GUARD(h);
+    int rc;
+    if ((rc = adjoint_supported(h))) return rc;
+    const int K = std::min(ckpt_every, nsteps), nseg = (nsteps + K - 1) / K;
+    if ((rc = adjoint_reserve(h, K, nseg))) return rc;
+    AdjointState *a = h->adj;
+    a->valid = false;
+    a->K = K; a->nsteps = nsteps; a->nseg = nseg;
+    a->ck_iter.assign(nseg + 1, 0);
+    CK(cudaStreamSynchronize(h->stream));
+    if (h->force_pending) {   // a spread force left by rbc_ibm_st1 belongs to no step of the run
+        CK(cudaMemsetAsync(h->Fx, 0, 4 * h->geo.nint, h->stream));
+        CK(cudaMemsetAsync(h->Fy, 0, 4 * h->geo.nint, h->stream));
+        CK(cudaMemsetAsync(h->Fz, 0, 4 * h->geo.nint, h->stream));
+        h->force_pending = false;
+    }
+    for (int s = 0; s < nseg; s++) {
+        if ((rc = adjoint_save(h, s))) return rc;
+        if ((rc = rbc_step(h, std::min(K, nsteps - s * K)))) return rc;
+    }
+    if ((rc = adjoint_save(h, nseg))) return rc;
+    const size_t nv3 = 3 * (size_t)h->nv;
+    if ((rc = d2d(h, a->fin_uvr, h->uvr, 16 * (size_t)h->geo.nint))) return rc;
+    if ((rc = d2d(h, a->fin_U, h->U, 4 * nv3))) return rc;
+    if ((rc = d2d(h, a->fin_Fv, h->Fv, 4 * nv3))) return rc;
+    CK(cudaStreamSynchronize(h->stream));
+    a->valid = true;
+    return RBC_OK;
+}
+
+int rbc_adjoint_backward(rbc_handle *h, const double *xbar, const double *ybar, const double *zbar,
+                         double *grad, double *dx0, double *dy0, double *dz0, int *adj_flags, float *ms)
+{
+    if (!h || !grad) return RBC_ERR_ARG;
+    RBC_DEVICE_GUARD(h);
+    AdjointState *a = h->adj;
+    if (!a || !a->valid) return fail(h, RBC_ERR_STATE, "rbc_adjoint_backward before rbc_adjoint_record");
+    const long long nv = h->nv;
+    const size_t n = (size_t)h->geo.nint, nq = (size_t)Q * n, nv3 = 3 * (size_t)nv;
+    int rc;
+    CK(cudaStreamSynchronize(h->stream));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(cudaEventRecord(e0, h->stream));
+    // seeds: adjoint of the final cel->x; nothing depends on the final populations or fem->xd
+    if (nv > 0) {
+        std::vector<double> seed(nv3, 0.0);
+        const double *in[3] = {xbar, ybar, zbar};
+        for (int c = 0; c < 3; c++) if (in[c]) std::copy(in[c], in[c] + nv, seed.begin() + c * nv);
+        CK(cudaMemcpy(a->Xbar, seed.data(), 8 * nv3, cudaMemcpyHostToDevice));
+        CK(cudaMemsetAsync(a->Xdbar, 0, 8 * nv3, h->stream));
+    }
+    int gb = 0;
+    CK(cudaMemsetAsync(a->gbar[0], 0, 4 * nq, h->stream));
+    CK(cudaMemsetAsync(a->pbar, 0, 4 * sizeof(double), h->stream));
+    CK(cudaMemsetAsync(a->status, 0, sizeof(int), h->stream));
+    for (int s = a->nseg - 1; s >= 0; s--) {
+        const int len = std::min(a->K, a->nsteps - s * a->K);
+        if ((rc = adjoint_recompute(h, s, len))) return rc;
+        if ((rc = adjoint_reverse(h, s, len, &gb))) return rc;
+    }
+    CK(cudaEventRecord(e1, h->stream));
+    double pb[4];
+    int st = 0;
+    CK(cudaMemcpyAsync(pb, a->pbar, sizeof(pb), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(&st, a->status, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    std::vector<double> x0(nv > 0 ? 2 * nv3 : 0);
+    if (nv > 0 && (dx0 || dy0 || dz0)) {
+        CK(cudaMemcpyAsync(x0.data(), a->Xbar, 8 * nv3, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaMemcpyAsync(x0.data() + nv3, a->Xdbar, 8 * nv3, cudaMemcpyDeviceToHost, h->stream));
+    }
+    CK(cudaStreamSynchronize(h->stream));
+    float t = 0.f;
+    CK(cudaEventElapsedTime(&t, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    grad[0] = pb[0]; grad[1] = pb[1]; grad[2] = pb[2];
+    double *outs[3] = {dx0, dy0, dz0};
+    for (int c = 0; c < 3; c++)
+        if (outs[c]) for (long long j = 0; j < nv; j++) outs[c][j] = x0[c * nv + j] + x0[nv3 + c * nv + j];
+    if (adj_flags) *adj_flags = st;
+    if (ms) *ms = t;
+    // leave the handle at the end of the recorded run
+    if ((rc = adjoint_restore(h, a->nseg))) return rc;
+    if ((rc = d2d(h, h->uvr, a->fin_uvr, 16 * n))) return rc;
+    if ((rc = d2d(h, h->U, a->fin_U, 4 * nv3))) return rc;
+    if ((rc = d2d(h, h->Fv, a->fin_Fv, 4 * nv3))) return rc;
+    CK(cudaStreamSynchronize(h->stream));
+    return RBC_OK;
+}
+
+int rbc_set_coefficients(rbc_handle *h, double P, double B, double C)
+{
+    if (!h || !std::isfinite(P) || !std::isfinite(B) || !std::isfinite(C)) return RBC_ERR_ARG;
+    RBC_DEVICE_GUARD(h);
+    CK(cudaStreamSynchronize(h->stream));
+    h->p.P = P; h->p.B = B; h->p.C = C;
+    // the step graphs hold the coefficients as kernel arguments
+    for (auto &form : h->graph)
+        for (cudaGraphExec_t &g : form) if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    if (h->adj) h->adj->valid = false;
     return RBC_OK;
 }
 

@@ -179,6 +179,61 @@ int  setup_kernel_attributes(int *membrane_max_smem);
 void launch_step_begin(int *d_iter, float *d_drive, double P, int flowstart, double freq, double dt,
                        cudaStream_t s);
 
+// ---- adjoint of one step (adjoint.cu); FP32 populations ----------------------
+
+struct LbmAdjArgs {
+    const float *gin;          // g_t, [Q][n]
+    const float *Fx, *Fy, *Fz; // spread force of the step
+    const uint32_t *mask2d;
+    const float *gbar_out;     // adjoint of g_t+1, [Q][n]
+    const float4 *ubar;        // adjoint of the velocity, [n]
+    float *gbar_pre;           // out: adjoint of the pulled populations, [Q][n]
+    float *gbar_in;            // out: adjoint of g_t, [Q][n]
+    float *Fbar;               // out: adjoint of the force, [3][n]
+    double *pbar;              // += (dfac dL/dpd, dL/dB)
+    float pd, Bc, omega, Cr;   // drive P * factor of the step, B, 1 / tau, Cr
+    double dfac;               // drive factor of the step (dpd / dP)
+};
+void launch_lbm_adjoint(const Geom &g, const LbmAdjArgs &a, cudaStream_t s);
+void launch_advect_adjoint(const Geom &g, const double *X, const float4 *uvr, const double *xa_bar, double *X_bar,
+                           float *ubar, long long nv, double dtM, int *flags, cudaStream_t s);
+void launch_spread_adjoint(const Geom &g, const double *X, const float *Fv, const float *Fbar, const uint32_t *mask2d,
+                           double *Fv_bar, double *X_bar, long long nv, cudaStream_t s);
+
+struct MembraneAdjArgs {
+    const double *Xd; long long nv;
+    const double4 *gref;
+    const int *tri, *v2e_off, *v2e;
+    const int16_t *nbr;
+    const float *Fv;           // the step's membrane forces
+    const double *Fv_bar;      // their adjoint, [3][nv]
+    double *Xd_bar;            // out, [3][nv]
+    double *scratch;           // [ne][7]
+    double *cbar;              // += dL/dC
+    int V, E, ncell;
+    double C, rgs; int law;
+    double LX, LZ;
+    int niter;
+};
+void launch_membrane_adjoint(const MembraneAdjArgs &a, cudaStream_t s);
+
+struct VolumeAdjArgs {
+    const double *Xa;          // positions before the correction, [3][nv]
+    const double *gx;          // centroids the correction unwraps about, [3][ncell]
+    const double *vol0;
+    const int *tri, *v2e_off, *v2e;
+    const double *X_bar;       // adjoint of the corrected positions
+    const double *Xd_bar;      // adjoint of fem->xd after the step (= Xa)
+    double *Xa_bar;            // out: adjoint of Xa
+    double *hist;              // [ncell][kmax][3][V]
+    double *escr;              // [ne][9]
+    int *status;               // bit 0: more moves than kmax (only kmax reversed)
+    long long nv;
+    int V, E, ncell, kmax;
+};
+int  volume_adjoint_smem_bytes(int V);
+void launch_volume_adjoint(const Geom &g, const VolumeAdjArgs &a, cudaStream_t s);
+
 // packed vertex -> element incidence: element id (bits 0..23), local position
 // of the vertex in the element (bits 24..25), neighbour slots of the two other
 // vertices (bits 26..28 and 29..31)

@@ -149,6 +149,7 @@ void launch_volume(const Geom &g, const VolumeArgs &a, cudaStream_t s)
 cudaError_t membrane_setup(int optin, int *max_bytes);
 cudaError_t spread_setup();
 cudaError_t advect_setup();
+cudaError_t adjoint_setup(int optin);
 
 // Dynamic shared memory limit of a kernel: the device's per-block opt-in
 // maximum minus the kernel's static shared memory.
@@ -173,6 +174,7 @@ int setup_kernel_attributes(int *membrane_max_smem)
     if ((e = membrane_setup(optin, membrane_max_smem)) != cudaSuccess) return (int)e;
     if ((e = spread_setup()) != cudaSuccess) return (int)e;
     if ((e = advect_setup()) != cudaSuccess) return (int)e;
+    if ((e = adjoint_setup(optin)) != cudaSuccess) return (int)e;
     return 0;
 }
 

@@ -149,6 +149,36 @@ class Simulation:
         self._call("rbc_export_ref_cells", *[_dp(out[k]) for k in keys])
         return out
 
+    # -- adjoint ----------------------------------------------------------------
+    def set_coefficients(self, P=None, B=None, C_=None):
+        """Replace the drive P, IB-force B and area-dilation C coefficients."""
+        P = self.params["P"] if P is None else float(P)
+        B = self.params["B"] if B is None else float(B)
+        C_ = self.params["C"] if C_ is None else float(C_)
+        self._call("rbc_set_coefficients", C.c_double(P), C.c_double(B), C.c_double(C_))
+        self.params.update(P=P, B=B, C=C_)
+
+    def adjoint_record(self, nsteps: int, ckpt_every: int = 100):
+        """Run nsteps steps keeping a checkpoint every ckpt_every steps."""
+        self._call("rbc_adjoint_record", int(nsteps), int(ckpt_every))
+
+    def adjoint_backward(self, xbar, ybar, zbar, want_x0: bool = False) -> dict:
+        """Reverse sweep of the recorded run from dL/d(final cel->x, y, z).
+        Returns grad (dL/dP, dL/dB, dL/dC), flags, ms and, with want_x0,
+        dx0 [3, nv] = dL/d(initial positions)."""
+        nv = self.nv
+        seeds = [_f64(a, nv) for a in (xbar, ybar, zbar)]
+        grad = np.zeros(3)
+        x0 = np.zeros((3, nv)) if want_x0 else None
+        flags = C.c_int(0)
+        ms = C.c_float(0.0)
+        outs = [_dp(x0[k]) for k in range(3)] if want_x0 else [None, None, None]
+        self._call("rbc_adjoint_backward", *[_dp(s) for s in seeds], _dp(grad), *outs, C.byref(flags), C.byref(ms))
+        r = dict(grad=grad, flags=flags.value, ms=ms.value)
+        if want_x0:
+            r["dx0"] = x0
+        return r
+
     # -- diagnostics ----------------------------------------------------------
     def status(self) -> tuple[int, int]:
         f, v = C.c_int(0), C.c_int(0)
