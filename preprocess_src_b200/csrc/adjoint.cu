@@ -9,18 +9,18 @@
 //   Xa     = advect(X_t, u)                RK4 in the frozen field
 //   Xd_t+1 = Xa,   X_t+1 = volume_correction(Xa)
 // The kernels below take the adjoints of a stage's outputs and return those of
-// its inputs.  Nonlinear pointwise maps -- the collision of one node, the
-// Skalak loads of one element, the normal / area / volume of one triangle --
-// are written once as templates on the scalar type; a forward-mode dual number
-// (value plus one derivative) seeded on one input at a time gives one column
-// of their Jacobian, which is contracted with the output adjoint.  The linear
-// global operators are transposed explicitly: pull streaming with half-way
-// bounce-back becomes a gather of the downstream nodes' adjoints; spreading
-// and interpolation are each other's transpose (plus the derivative of the
-// delta weights with respect to the vertex position); RK4 runs its stages
-// backwards; the mass-matrix solve M q = b (M symmetric) is reversed with the
-// same Chebyshev solver; the volume correction's iterations are replayed and
-// reversed one by one.
+// its inputs.  The collision of one node is differentiated by hand in reverse
+// mode, and pull streaming with half-way bounce-back, which reads every fluid
+// slot exactly once, is reversed as a conflict-free push in the same kernel.
+// The Skalak loads of one element and the normal / area / volume of one
+// triangle are written once as templates on the scalar type; a forward-mode
+// dual number (value plus one derivative) seeded on one input at a time gives
+// one column of their Jacobian, which is contracted with the output adjoint.
+// Spreading and interpolation are each other's transpose (plus the derivative
+// of the delta weights with respect to the vertex position); RK4 runs its
+// stages backwards; the mass-matrix solve M q = b (M symmetric) is reversed
+// with the same Chebyshev solver; the volume correction's iterations are
+// replayed and reversed one by one.
 #include "rbc_internal.cuh"
 
 namespace rbc {
@@ -76,50 +76,23 @@ __device__ __forceinline__ R block_sum_r(R v, R *red) {
 
 // ---- collide-stream ----------------------------------------------------------
 
-// The collision of one node as lbm.cu computes it (collision_terms +
-// post_collision), generic in the scalar type.  g: pulled populations (f - w);
-// (fx, fy, fz): spread force; pd: drive P of the step; Bc: B.  post: the
-// post-collision populations; u: the velocity with the half-force shift (what
-// the interpolation reads).
-template <typename T, typename R>
-__device__ __forceinline__ void collide_generic(const T (&g)[Q], T fx, T fy, T fz, T pd, T Bc, R omega, R Cr,
-                                                T (&post)[Q], T (&u)[3])
-{
-    T drho = T(R(0)), jx = T(R(0)), jy = T(R(0)), jz = T(R(0));
-#pragma unroll
-    for (int q = 0; q < Q; q++) {
-        drho += g[q];
-        if (ex(q) == 1) jx += g[q]; else if (ex(q) == -1) jx -= g[q];
-        if (ey(q) == 1) jy += g[q]; else if (ey(q) == -1) jy -= g[q];
-        if (ez(q) == 1) jz += g[q]; else if (ez(q) == -1) jz -= g[q];
-    }
-    const T r = drho + R(1);
-    const T Gx = r * Bc * fx, Gy = r * Bc * fy, Gz = r * (pd + Bc * fz);
-    const T inv = R(1) / (r * Cr);
-    u[0] = (jx + Gx) * inv; u[1] = (jy + Gy) * inv; u[2] = (jz + Gz) * inv;
-    const R fo = (R(1) - R(0.5) * omega) * R(2), om1 = R(1) - omega;
-    const T usq = (u[0] * u[0] + u[1] * u[1] + u[2] * u[2]) * (R(-1.5) * Cr * Cr);
-    const T uG = (u[0] * Gx + u[1] * Gy + u[2] * Gz) * (R(3) * Cr);
-    const T A = (drho + r * usq) * omega - uG * fo;
-    const T B = r * (R(3) * Cr * omega), C = r * (R(4.5) * Cr * Cr * omega);
-    const R D = R(3) * fo, E = R(9) * Cr * fo;
-#pragma unroll
-    for (int q = 0; q < Q; q++) {
-        T eu = T(R(0)), eG = T(R(0));
-        if (ex(q) == 1) { eu += u[0]; eG += Gx; } else if (ex(q) == -1) { eu -= u[0]; eG -= Gx; }
-        if (ey(q) == 1) { eu += u[1]; eG += Gy; } else if (ey(q) == -1) { eu -= u[1]; eG -= Gy; }
-        if (ez(q) == 1) { eu += u[2]; eG += Gz; } else if (ez(q) == -1) { eu -= u[2]; eG -= Gz; }
-        post[q] = g[q] * om1 + (A + eu * (B + C * eu + eG * E) + eG * D) * R(wq(q));
-    }
-}
-
 constexpr int LBM_ADJ_THREADS = 128;
 
-// Adjoint of the collision at every fluid node.  gin: g_t (the populations the
-// forward step pulled from); F: the spread force of the step; gbar_out:
-// adjoint of g_t+1; ubar: adjoint of the velocity field ([n] float4, .w
-// unused).  Writes the adjoint of the pulled populations (gbar_pre) and of the
-// force (Fbar, 0 off the fluid), and adds dfac * d/dP and d/dB to pbar[0..1].
+// Adjoint of collide-stream at every fluid node, written out in reverse mode.
+// The forward (lbm.cu) pulls g_q from node i - e_q (or its own opp-q slot
+// across a wall link), forms drho = sum g, j = sum e g, r = 1 + drho,
+// G = (r B fx, r B fy, r (pd + B fz)), u = (j + G) / (r Cr) and stores
+//   post_q = (1 - om) g_q + w_q (A + eu_q (Bq + Cq eu_q + E eG_q) + D eG_q)
+// with eu_q = e_q . u, eG_q = e_q . G, A = om (drho + r usq) - fo uG,
+// usq = -1.5 Cr^2 u.u, uG = 3 Cr u.G, Bq = 3 Cr om r, Cq = 4.5 Cr^2 om r,
+// D = 3 fo, E = 9 Cr fo, fo = 2 - om.  From the adjoints of post (gbar_out at
+// the node) and of u (ubar) the chain rule, taken back through these lines,
+// gives those of g, F, pd and B.  The pulled populations' adjoints go back to
+// the slots they were pulled from: the pull reads every fluid slot exactly
+// once (slot q of node j by node j + e_q when that node is fluid, else by j
+// itself through its opp-q wall link), so the reverse is a conflict-free push
+// and every fluid slot of gbar_in is written once.  Wall slots are never
+// read.  dfac * dL/dpd and dL/dB are added to pbar[0..1].
 __global__ void __launch_bounds__(LBM_ADJ_THREADS)
 lbm_adjoint_kernel(const LbmAdjArgs a, int nx, int ny, int nzc, long long nint)
 {
@@ -134,33 +107,70 @@ lbm_adjoint_kernel(const LbmAdjArgs a, int nx, int ny, int nzc, long long nint)
         if (m & MASK_FLUID) {
             const long long zbm = (z == 0) ? (long long)(nzc - 1) * plane : zb0 - plane;
             const long long zbp = (z == nzc - 1) ? 0 : zb0 + plane;
-            float g[Q], ob[Q];
+            float g[Q];
 #pragma unroll
             for (int q = 0; q < Q; q++) {
                 const long long src = ((ez(q) == 1) ? zbm : (ez(q) == -1) ? zbp : zb0) + xy - ex(q) - nx * ey(q);
                 g[q] = ((m >> q) & 1u) ? a.gin[(long long)opp(q) * nint + idx] : a.gin[(long long)q * nint + src];
-                ob[q] = a.gbar_out[(long long)q * nint + idx];
             }
-            const float f3[3] = {a.Fx[idx], a.Fy[idx], a.Fz[idx]};
+            const float fx = a.Fx[idx], fy = a.Fy[idx], fz = a.Fz[idx];
+            const float om = a.omega, Cr = a.Cr, Bc = a.Bc, pd = __ldg(a.pd);
+            // forward
+            float drho = 0.f, jx = 0.f, jy = 0.f, jz = 0.f;
+#pragma unroll
+            for (int q = 0; q < Q; q++) {
+                drho += g[q];
+                if (ex(q)) jx += ex(q) * g[q];
+                if (ey(q)) jy += ey(q) * g[q];
+                if (ez(q)) jz += ez(q) * g[q];
+            }
+            const float r = 1.0f + drho;
+            const float Gx = r * Bc * fx, Gy = r * Bc * fy, Gz = r * (pd + Bc * fz);
+            const float inv = 1.0f / (r * Cr);
+            const float ux = (jx + Gx) * inv, uy = (jy + Gy) * inv, uz = (jz + Gz) * inv;
+            const float fo = (1.0f - 0.5f * om) * 2.0f;
+            const float usq = -1.5f * Cr * Cr * (ux * ux + uy * uy + uz * uz);
+            const float Bq = 3.0f * Cr * om * r, Cq = 4.5f * Cr * Cr * om * r, D = 3.0f * fo, E = 9.0f * Cr * fo;
+            // reverse: post_q
             const float4 ub = a.ubar[idx];
-            // one Jacobian column per input: 19 populations, 3 force components, P, B
-#pragma unroll 1
-            for (int k = 0; k < Q + 5; k++) {
-                Dual<float> gd[Q], post[Q], u[3];
+            float ob[Q];
+            float Ab = 0.f, Bb = 0.f, Cb = 0.f;
+            float uxb = ub.x, uyb = ub.y, uzb = ub.z, Gxb = 0.f, Gyb = 0.f, Gzb = 0.f;
 #pragma unroll
-                for (int q = 0; q < Q; q++) gd[q] = Dual<float>(g[q], k == q ? 1.f : 0.f);
-                const Dual<float> fx(f3[0], k == Q ? 1.f : 0.f), fy(f3[1], k == Q + 1 ? 1.f : 0.f),
-                    fz(f3[2], k == Q + 2 ? 1.f : 0.f), dp(a.pd, k == Q + 3 ? 1.f : 0.f), db(a.Bc, k == Q + 4 ? 1.f : 0.f);
-                collide_generic<Dual<float>, float>(gd, fx, fy, fz, dp, db, a.omega, a.Cr, post, u);
-                float s = u[0].d * ub.x + u[1].d * ub.y + u[2].d * ub.z;
+            for (int q = 0; q < Q; q++) {
+                ob[q] = a.gbar_out[(long long)q * nint + idx];
+                const float W = wq(q) * ob[q];
+                const float eu = ex(q) * ux + ey(q) * uy + ez(q) * uz;
+                const float eG = ex(q) * Gx + ey(q) * Gy + ez(q) * Gz;
+                Ab += W; Bb += W * eu; Cb += W * eu * eu;
+                const float eub = W * (Bq + 2.0f * Cq * eu + E * eG), eGb = W * (E * eu + D);
+                if (ex(q)) { uxb += ex(q) * eub; Gxb += ex(q) * eGb; }
+                if (ey(q)) { uyb += ey(q) * eub; Gyb += ey(q) * eGb; }
+                if (ez(q)) { uzb += ez(q) * eub; Gzb += ez(q) * eGb; }
+            }
+            // A, Bq, Cq
+            float drhob = om * Ab;
+            float rb = om * usq * Ab + 3.0f * Cr * om * Bb + 4.5f * Cr * Cr * om * Cb;
+            const float ku = -3.0f * Cr * Cr * (om * r * Ab), kG = 3.0f * Cr * (-fo * Ab);
+            uxb += ku * ux + kG * Gx; uyb += ku * uy + kG * Gy; uzb += ku * uz + kG * Gz;
+            Gxb += kG * ux; Gyb += kG * uy; Gzb += kG * uz;
+            // u = (j + G) / (r Cr)
+            const float jxb = uxb * inv, jyb = uyb * inv, jzb = uzb * inv;
+            Gxb += jxb; Gyb += jyb; Gzb += jzb;
+            rb -= (uxb * ux + uyb * uy + uzb * uz) / r;
+            // G
+            rb += Bc * (Gxb * fx + Gyb * fy) + Gzb * (pd + Bc * fz);
+            a.Fbar[idx] = Gxb * r * Bc; a.Fbar[nint + idx] = Gyb * r * Bc; a.Fbar[2 * nint + idx] = Gzb * r * Bc;
+            dP = (double)(Gzb * r);
+            dB = (double)(r * (Gxb * fx + Gyb * fy + Gzb * fz));
+            drhob += rb;
+            const float om1 = 1.0f - om;
 #pragma unroll
-                for (int q = 0; q < Q; q++) s += post[q].d * ob[q];
-                if (k < Q) a.gbar_pre[(long long)k * nint + idx] = s;
-                else if (k == Q) a.Fbar[idx] = s;
-                else if (k == Q + 1) a.Fbar[nint + idx] = s;
-                else if (k == Q + 2) a.Fbar[2 * nint + idx] = s;
-                else if (k == Q + 3) dP = s;
-                else dB = s;
+            for (int q = 0; q < Q; q++) {
+                const float gb = om1 * ob[q] + drhob + ex(q) * jxb + ey(q) * jyb + ez(q) * jzb;
+                const long long src = ((ez(q) == 1) ? zbm : (ez(q) == -1) ? zbp : zb0) + xy - ex(q) - nx * ey(q);
+                if ((m >> q) & 1u) a.gbar_in[(long long)opp(q) * nint + idx] = gb;
+                else a.gbar_in[(long long)q * nint + src] = gb;
             }
         } else {
             a.Fbar[idx] = 0.f; a.Fbar[nint + idx] = 0.f; a.Fbar[2 * nint + idx] = 0.f;
@@ -178,67 +188,64 @@ lbm_adjoint_kernel(const LbmAdjArgs a, int nx, int ny, int nzc, long long nint)
     if (threadIdx.x == 0) {
         double sp = 0.0, sb = 0.0;
         for (int w = 0; w < LBM_ADJ_THREADS / 32; w++) { sp += red[0][w]; sb += red[1][w]; }
-        atomicAdd(&a.pbar[0], a.dfac * sp);
+        atomicAdd(&a.pbar[0], __ldg(a.dfac) * sp);
         atomicAdd(&a.pbar[1], sb);
-    }
-}
-
-// Transpose of the pull.  Population q of fluid node j is read by node
-// j + e_q (direction q; that node's source j is fluid, so it does not bounce
-// back there) when j + e_q is fluid, and by node j itself in direction opp q
-// when j's opp-q source is a wall (half-way bounce-back).  Populations of wall
-// nodes are never read.
-__global__ void lbm_pull_transpose_kernel(const float *__restrict__ gbar_pre, const uint32_t *__restrict__ mask2d,
-                                          float *__restrict__ gbar_in, int nx, int ny, int nzc, long long nint)
-{
-    const int plane = nx * ny;
-    const int xy = blockIdx.x * blockDim.x + threadIdx.x;
-    if (xy >= plane) return;
-    const int z = blockIdx.y;
-    const long long zb0 = (long long)z * plane, idx = zb0 + xy;
-    const uint32_t m = __ldg(&mask2d[xy]);
-    const bool fluid = (m & MASK_FLUID) != 0;
-    const long long zbm = (z == 0) ? (long long)(nzc - 1) * plane : zb0 - plane;
-    const long long zbp = (z == nzc - 1) ? 0 : zb0 + plane;
-#pragma unroll
-    for (int q = 0; q < Q; q++) {
-        float v = 0.f;
-        if (fluid) {
-            const int xyn = xy + ex(q) + nx * ey(q);   // inside the lattice: fluid is never on its edge
-            if (__ldg(&mask2d[xyn]) & MASK_FLUID)
-                v += gbar_pre[(long long)q * nint + ((ez(q) == 1) ? zbp : (ez(q) == -1) ? zbm : zb0) + xyn];
-            if ((m >> opp(q)) & 1u) v += gbar_pre[(long long)opp(q) * nint + idx];
-        }
-        gbar_in[(long long)q * nint + idx] = v;
     }
 }
 
 // ---- delta stencil with position derivatives ------------------------------
 
-// delta4 (rbc_internal.cuh) in FP64 with d/df of each weight.  With
-// s = sin(pi f / 2), c = cos(pi f / 2): w = (1 - s, 1 + c, 1 + s, 1 - c) / 4,
-// dw/df = (pi / 8) (-c, -s, c, s).
-__device__ __forceinline__ void delta4_d(double f, double w[4], double dw[4]) {
-    double s, c;
-    sincospi(0.5 * f, &s, &c);
-    const double k = 0.125 * 3.14159265358979323846;
-    w[0] = 0.25 * (1.0 - s); w[1] = 0.25 * (1.0 + c); w[2] = 0.25 * (1.0 + s); w[3] = 0.25 * (1.0 - c);
-    dw[0] = -k * c; dw[1] = -k * s; dw[2] = k * c; dw[3] = k * s;
+// One warp per vertex for the interpolation and spreading adjoints: lane l
+// owns the stencil nodes k = l and l + 32 of the 64 (k = a + 4 b + 16 c with
+// x offset a, y offset b, z plane c from the node below the position minus 1).
+// delta4 (rbc_internal.cuh) weights in FP64 with their derivatives: with
+// s = sin(pi f / 2), c = cos(pi f / 2), w = (1 - s, 1 + c, 1 + s, 1 - c) / 4
+// and dw/df = (pi / 8) (-c, -s, c, s).
+__device__ __forceinline__ void delta_w(int k, double s, double c, double &w, double &dw)
+{
+    const double pi8 = 0.125 * 3.14159265358979323846;
+    w = k == 0 ? 0.25 * (1.0 - s) : k == 1 ? 0.25 * (1.0 + c) : k == 2 ? 0.25 * (1.0 + s) : 0.25 * (1.0 - c);
+    dw = k == 0 ? -pi8 * c : k == 1 ? -pi8 * s : k == 2 ? pi8 * c : pi8 * s;
 }
 
-struct Stencil {
-    int ix0, iy0, iz0;            // first node on each axis (z in the raw frame of the position)
-    double wx[4], wy[4], wz[4];   // weights
-    double dx[4], dy[4], dz[4];   // d weight / d position
+struct LaneStencil {
+    long long n[2];     // lattice index of the lane's two nodes, -1 = dropped
+    double w[2];        // weights
+    double dw[2][3];    // d weight / d position
 };
 
-__device__ __forceinline__ void stencil_at(const Geom &g, double px, double py, double pz, Stencil &s) {
+// The lane's two nodes of the stencil at p.  Nodes outside x, y or beyond the
+// two BUFF planes of the position's own z frame are dropped, as in the forward
+// spread (ibm.cu:107-110) and interpolation (ibm.cu:453-455).
+__device__ __forceinline__ void lane_stencil(const Geom &g, double px, double py, double pz, int lane, LaneStencil &s)
+{
     const double lx = lat_x(g, px), ly = lat_y(g, py), lz = lat_z(g, pz);
     const double flx = floor(lx), fly = floor(ly), flz = floor(lz);
-    s.ix0 = (int)flx - 1; s.iy0 = (int)fly - 1; s.iz0 = (int)flz - 1;
-    delta4_d(lx - flx, s.wx, s.dx); delta4_d(ly - fly, s.wy, s.dy); delta4_d(lz - flz, s.wz, s.dz);
+    double sx, cx, sy, cy, sz, cz;
+    sincospi(0.5 * (lx - flx), &sx, &cx);
+    sincospi(0.5 * (ly - fly), &sy, &cy);
+    sincospi(0.5 * (lz - flz), &sz, &cz);
 #pragma unroll
-    for (int k = 0; k < 4; k++) { s.dx[k] *= g.inv_dx; s.dy[k] *= g.inv_dx; s.dz[k] *= g.inv_dx; }
+    for (int h = 0; h < 2; h++) {
+        const int k = lane + 32 * h, a = k & 3, b = (k >> 2) & 3, c = k >> 4;
+        const int gx = (int)flx - 1 + a, gy = (int)fly - 1 + b, iz = (int)flz - 1 + c;
+        const bool in = gx >= 0 && gx < g.nx && gy >= 0 && gy < g.ny && iz >= -2 && iz < g.nzc + 2;
+        s.n[h] = in ? (long long)wrap_z(iz, g.nzc) * g.plane + gx + (long long)g.nx * gy : -1LL;
+        double wa, da, wb, db, wc, dc;
+        delta_w(a, sx, cx, wa, da);
+        delta_w(b, sy, cy, wb, db);
+        delta_w(c, sz, cz, wc, dc);
+        s.w[h] = wa * wb * wc;
+        s.dw[h][0] = da * wb * wc * g.inv_dx;
+        s.dw[h][1] = wa * db * wc * g.inv_dx;
+        s.dw[h][2] = wa * wb * dc * g.inv_dx;
+    }
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;   // the butterfly leaves the same sum in every lane
 }
 
 // a lattice coordinate the stencil arithmetic can take (as in ibm.cu)
@@ -248,86 +255,72 @@ __device__ __forceinline__ bool sane_pos(const Geom &g, double px, double py, do
 
 // ---- interpolation + RK4, reversed -----------------------------------------
 
+constexpr int VTX_ADJ_THREADS = 128;   // four vertices per CTA, one warp each
+
 // Velocity of the frozen field at p as the forward advection interpolates it
-// (stencil nodes beyond the two BUFF planes or outside x, y contribute nothing).
-__device__ __forceinline__ void interp(const Geom &g, const float4 *__restrict__ uvr, double px, double py, double pz,
-                                       double u[3]) {
-    Stencil s;
-    stencil_at(g, px, py, pz, s);
-    u[0] = u[1] = u[2] = 0.0;
-    for (int c = 0; c < 4; c++) {
-        const int iz = s.iz0 + c;
-        if (iz < -2 || iz >= g.nzc + 2) continue;
-        const long long zb = (long long)wrap_z(iz, g.nzc) * g.plane;
-        for (int b = 0; b < 4; b++) {
-            const int gy = s.iy0 + b;
-            if (gy < 0 || gy >= g.ny) continue;
-            for (int a = 0; a < 4; a++) {
-                const int gx = s.ix0 + a;
-                if (gx < 0 || gx >= g.nx) continue;
-                const float4 q = __ldg(&uvr[zb + gx + (long long)g.nx * gy]);
-                const double w = s.wx[a] * s.wy[b] * s.wz[c];
-                u[0] += w * q.x; u[1] += w * q.y; u[2] += w * q.z;
-            }
+// (every lane returns the same sum).
+__device__ __forceinline__ void warp_interp(const Geom &g, const float4 *__restrict__ uvr, const double p[3], int lane,
+                                            double u[3]) {
+    LaneStencil s;
+    lane_stencil(g, p[0], p[1], p[2], lane, s);
+    double u0 = 0.0, u1 = 0.0, u2 = 0.0;
+#pragma unroll
+    for (int h = 0; h < 2; h++)
+        if (s.n[h] >= 0) {
+            const float4 q = __ldg(&uvr[s.n[h]]);
+            u0 += s.w[h] * q.x; u1 += s.w[h] * q.y; u2 += s.w[h] * q.z;
         }
-    }
+    u[0] = warp_sum(u0); u[1] = warp_sum(u1); u[2] = warp_sum(u2);
 }
 
 // Adjoint of one interpolation at p with output adjoint kb: adds w_n kb to
-// the velocity adjoint of each stencil node and returns in pb the position
-// adjoint, sum_n (d w_n / d p) (u_n . kb).
-__device__ __forceinline__ void interp_adjoint(const Geom &g, const float4 *__restrict__ uvr, float *__restrict__ ubar,
-                                               double px, double py, double pz, const double kb[3], double pb[3]) {
-    Stencil s;
-    stencil_at(g, px, py, pz, s);
-    pb[0] = pb[1] = pb[2] = 0.0;
-    for (int c = 0; c < 4; c++) {
-        const int iz = s.iz0 + c;
-        if (iz < -2 || iz >= g.nzc + 2) continue;
-        const long long zb = (long long)wrap_z(iz, g.nzc) * g.plane;
-        for (int b = 0; b < 4; b++) {
-            const int gy = s.iy0 + b;
-            if (gy < 0 || gy >= g.ny) continue;
-            for (int a = 0; a < 4; a++) {
-                const int gx = s.ix0 + a;
-                if (gx < 0 || gx >= g.nx) continue;
-                const long long n = zb + gx + (long long)g.nx * gy;
-                const float4 q = __ldg(&uvr[n]);
-                const double w = s.wx[a] * s.wy[b] * s.wz[c];
-                atomicAdd(&ubar[4 * n + 0], (float)(w * kb[0]));
-                atomicAdd(&ubar[4 * n + 1], (float)(w * kb[1]));
-                atomicAdd(&ubar[4 * n + 2], (float)(w * kb[2]));
-                const double uk = q.x * kb[0] + q.y * kb[1] + q.z * kb[2];
-                pb[0] += s.dx[a] * s.wy[b] * s.wz[c] * uk;
-                pb[1] += s.wx[a] * s.dy[b] * s.wz[c] * uk;
-                pb[2] += s.wx[a] * s.wy[b] * s.dz[c] * uk;
-            }
+// the velocity adjoint of each stencil node; returns in pb (every lane) the
+// position adjoint sum_n (d w_n / d p) (u_n . kb).
+__device__ __forceinline__ void warp_interp_adjoint(const Geom &g, const float4 *__restrict__ uvr,
+                                                    float *__restrict__ ubar, const double p[3], const double kb[3],
+                                                    int lane, double pb[3]) {
+    LaneStencil s;
+    lane_stencil(g, p[0], p[1], p[2], lane, s);
+    double b0 = 0.0, b1 = 0.0, b2 = 0.0;
+#pragma unroll
+    for (int h = 0; h < 2; h++)
+        if (s.n[h] >= 0) {
+            const long long n = s.n[h];
+            const float4 q = __ldg(&uvr[n]);
+            atomicAdd(&ubar[4 * n + 0], (float)(s.w[h] * kb[0]));
+            atomicAdd(&ubar[4 * n + 1], (float)(s.w[h] * kb[1]));
+            atomicAdd(&ubar[4 * n + 2], (float)(s.w[h] * kb[2]));
+            const double uk = q.x * kb[0] + q.y * kb[1] + q.z * kb[2];
+            b0 += s.dw[h][0] * uk; b1 += s.dw[h][1] * uk; b2 += s.dw[h][2] * uk;
         }
-    }
+    pb[0] = warp_sum(b0); pb[1] = warp_sum(b1); pb[2] = warp_sum(b2);
 }
 
-// One thread per vertex.  xa_bar: adjoint of the advected positions; writes
+// One warp per vertex.  xa_bar: adjoint of the advected positions; writes
 // X_bar (adjoint of X_t through the advection, overwritten) and adds to ubar.
 // The periodic wrap of the result in x and z is a translation (derivative 1).
-__global__ void advect_adjoint_kernel(const Geom g, const double *__restrict__ X, const float4 *__restrict__ uvr,
-                                      const double *__restrict__ xa_bar, double *__restrict__ X_bar,
-                                      float *__restrict__ ubar, long long nv, double dtM, int *__restrict__ flags)
+__global__ void __launch_bounds__(VTX_ADJ_THREADS)
+advect_adjoint_kernel(const Geom g, const double *__restrict__ X, const float4 *__restrict__ uvr,
+                      const double *__restrict__ xa_bar, double *__restrict__ X_bar, float *__restrict__ ubar,
+                      long long nv, double dtM, int *__restrict__ flags)
 {
-    const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (v >= nv) return;
-    double p[4][3], k[4][3];
+    const long long v = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (v >= nv) return;   // uniform over the warp
+    double p[4][3], k[3][3];
     p[0][0] = X[v]; p[0][1] = X[nv + v]; p[0][2] = X[2 * nv + v];
     if (!sane_pos(g, p[0][0], p[0][1], p[0][2])) {
-        atomicOr(flags, RBC_FLAG_NONFINITE);
-        X_bar[v] = X_bar[nv + v] = X_bar[2 * nv + v] = 0.0;
+        if (lane == 0) {
+            atomicOr(flags, RBC_FLAG_NONFINITE);
+            X_bar[v] = X_bar[nv + v] = X_bar[2 * nv + v] = 0.0;
+        }
         return;
     }
     const double hs[4] = {0.0, 0.5 * dtM, 0.5 * dtM, dtM};   // stage offsets (ibm.cu:474-498)
-    interp(g, uvr, p[0][0], p[0][1], p[0][2], k[0]);
-    for (int s = 1; s < 4; s++) {
+    for (int s = 0; s < 3; s++) {
+        warp_interp(g, uvr, p[s], lane, k[s]);
         // the forward adds the FP32 stage velocity to the FP64 position
-        for (int c = 0; c < 3; c++) p[s][c] = p[0][c] + (double)(float)k[s - 1][c] * hs[s];
-        interp(g, uvr, p[s][0], p[s][1], p[s][2], k[s]);
+        for (int c = 0; c < 3; c++) p[s + 1][c] = p[0][c] + (double)(float)k[s][c] * hs[s + 1];
     }
     double xb[3], kb[4][3];
     for (int c = 0; c < 3; c++) {
@@ -337,60 +330,50 @@ __global__ void advect_adjoint_kernel(const Geom g, const double *__restrict__ X
     }
     for (int s = 3; s >= 0; s--) {
         double pb[3];
-        interp_adjoint(g, uvr, ubar, p[s][0], p[s][1], p[s][2], kb[s], pb);
+        warp_interp_adjoint(g, uvr, ubar, p[s], kb[s], lane, pb);
         for (int c = 0; c < 3; c++) {
             xb[c] += pb[c];
             if (s > 0) kb[s - 1][c] += hs[s] * pb[c];   // p_s = X + h_s k_s-1
         }
     }
-    for (int c = 0; c < 3; c++) X_bar[(long long)c * nv + v] = xb[c];
+    if (lane < 3) X_bar[(long long)lane * nv + v] = xb[lane];
 }
 
 // ---- spreading, reversed --------------------------------------------------
 
-// F(n) = sum_v w_n(X_v) Fv_v / dx^3 over fluid columns, stencil planes beyond
-// the BUFF planes of the vertex's raw frame dropped (ibm.cu:107-110).  One
-// thread per vertex: Fv_bar = sum_n w_n Fbar(n) / dx^3 (overwritten) and
+// F(n) = sum_v w_n(X_v) Fv_v / dx^3 over fluid columns.  One warp per vertex:
+// Fv_bar = sum_n w_n Fbar(n) / dx^3 (overwritten) and
 // X_bar += sum_n (d w_n / d X) (Fv . Fbar(n)) / dx^3.
-__global__ void spread_adjoint_kernel(const Geom g, const double *__restrict__ X, const float *__restrict__ Fv,
-                                      const float *__restrict__ Fbar, const uint32_t *__restrict__ mask2d,
-                                      double *__restrict__ Fv_bar, double *__restrict__ X_bar, long long nv)
+__global__ void __launch_bounds__(VTX_ADJ_THREADS)
+spread_adjoint_kernel(const Geom g, const double *__restrict__ X, const float *__restrict__ Fv,
+                      const float *__restrict__ Fbar, const uint32_t *__restrict__ mask2d,
+                      double *__restrict__ Fv_bar, double *__restrict__ X_bar, long long nv)
 {
-    const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (v >= nv) return;
-    const double px = X[v], py = X[nv + v], pz = X[2 * nv + v];
+    const long long v = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (v >= nv) return;   // uniform over the warp
+    const double p[3] = {X[v], X[nv + v], X[2 * nv + v]};
     double fb[3] = {0.0, 0.0, 0.0}, pb[3] = {0.0, 0.0, 0.0};
-    if (sane_pos(g, px, py, pz)) {
+    if (sane_pos(g, p[0], p[1], p[2])) {
         const double wscale = 1.0 / (g.dx * g.dx * g.dx);
-        Stencil s;
-        stencil_at(g, px, py, pz, s);
         const double f[3] = {Fv[v], Fv[nv + v], Fv[2 * nv + v]};
-        for (int c = 0; c < 4; c++) {
-            const int iz = s.iz0 + c;
-            if (iz < -2 || iz >= g.nzc + 2) continue;
-            const long long zb = (long long)wrap_z(iz, g.nzc) * g.plane;
-            for (int b = 0; b < 4; b++) {
-                const int gy = s.iy0 + b;
-                if (gy < 0 || gy >= g.ny) continue;
-                for (int a = 0; a < 4; a++) {
-                    const int gx = s.ix0 + a;
-                    if (gx < 0 || gx >= g.nx) continue;
-                    if (!(__ldg(&mask2d[gx + g.nx * gy]) & MASK_FLUID)) continue;
-                    const long long n = zb + gx + (long long)g.nx * gy;
-                    const double F0 = Fbar[n], F1 = Fbar[g.nint + n], F2 = Fbar[2 * g.nint + n];
-                    const double w = s.wx[a] * s.wy[b] * s.wz[c] * wscale;
-                    fb[0] += w * F0; fb[1] += w * F1; fb[2] += w * F2;
-                    const double fF = (f[0] * F0 + f[1] * F1 + f[2] * F2) * wscale;
-                    pb[0] += s.dx[a] * s.wy[b] * s.wz[c] * fF;
-                    pb[1] += s.wx[a] * s.dy[b] * s.wz[c] * fF;
-                    pb[2] += s.wx[a] * s.wy[b] * s.dz[c] * fF;
-                }
-            }
+        LaneStencil s;
+        lane_stencil(g, p[0], p[1], p[2], lane, s);
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const long long n = s.n[h];
+            if (n < 0 || !(__ldg(&mask2d[n % g.plane]) & MASK_FLUID)) continue;
+            const double F0 = Fbar[n], F1 = Fbar[g.nint + n], F2 = Fbar[2 * g.nint + n];
+            const double w = s.w[h] * wscale;
+            fb[0] += w * F0; fb[1] += w * F1; fb[2] += w * F2;
+            const double fF = (f[0] * F0 + f[1] * F1 + f[2] * F2) * wscale;
+            pb[0] += s.dw[h][0] * fF; pb[1] += s.dw[h][1] * fF; pb[2] += s.dw[h][2] * fF;
         }
     }
-    for (int c = 0; c < 3; c++) {
-        Fv_bar[(long long)c * nv + v] = fb[c];
-        X_bar[(long long)c * nv + v] += pb[c];
+    for (int c = 0; c < 3; c++) { fb[c] = warp_sum(fb[c]); pb[c] = warp_sum(pb[c]); }
+    if (lane < 3) {
+        Fv_bar[(long long)lane * nv + v] = fb[lane];
+        X_bar[(long long)lane * nv + v] += pb[lane];
     }
 }
 
@@ -456,29 +439,29 @@ __device__ __forceinline__ void edges_of(const MembraneAdjArgs &a, long long vb,
 
 constexpr int MEM_ADJ_THREADS = 1024;
 
-// One CTA per cell.  Fv: the membrane forces of the step (forward output);
-// Fv_bar: their adjoint.  The forward solves M q = b (b = element loads
-// gathered per vertex, M the P1 mass matrix) and sets Fv = -q ds (ds = one-ring
-// area / 3).  Reverse: q_bar = -ds Fv_bar, ds_bar = -q . Fv_bar,
-// lambda = M^-1 q_bar (Chebyshev on D^-1 M as the forward: with M symmetric the
-// transpose of the polynomial solve is the same polynomial solve), b_bar =
-// lambda, M_bar = -lambda q^T.  Per element the adjoints of (load on b, load on
-// c, gab) are contracted with the Jacobian of element_loads (seven dual
-// passes: e1, e2, C) and the edge adjoints gathered to the vertices.  Writes
-// Xd_bar (overwritten) and adds dL/dC to cbar.
+// The forward solves M q = b per cell (b = element loads gathered per vertex,
+// M the P1 mass matrix) and sets Fv = -q ds (ds = one-ring area / 3).  Its
+// reverse, from Fv_bar: q_bar = -ds Fv_bar, ds_bar = -q . Fv_bar,
+// lambda = M^-1 q_bar (Chebyshev on D^-1 M as the forward: with M symmetric
+// the transpose of the polynomial solve is the same polynomial solve),
+// b_bar = lambda, M_bar = -lambda q^T.  Three kernels: the per-cell solve,
+// one thread per element for the element Jacobians, one thread per vertex
+// for the gather.
+
+// One CTA per cell: element areas (scratch[7 e]), rows of D^-1 M, q, ds_bar,
+// and lambda; writes lam, qv, dsb per vertex.
 template <int VPT>
 __global__ void __launch_bounds__(MEM_ADJ_THREADS, 1)
-membrane_adjoint_kernel(const MembraneAdjArgs a)
+membrane_adjoint_solve_kernel(const MembraneAdjArgs a)
 {
     extern __shared__ __align__(16) unsigned char smem[];
-    __shared__ double red[32];
     const int V = a.V, E = a.E, tid = threadIdx.x, T = blockDim.x;
     float4 *dbuf = reinterpret_cast<float4 *>(smem);                    // [2][V]
     float *coef = reinterpret_cast<float *>(smem + 32 * (size_t)V);     // [6][V]
     int16_t *snbr = reinterpret_cast<int16_t *>(smem + 56 * (size_t)V); // [6][V]
     const int cell = blockIdx.x;
     const long long vb = (long long)cell * V, eb = (long long)cell * E, nv = a.nv;
-    double *er = a.scratch + eb * 7;   // per element: gab, then the adjoints of e1 and e2
+    double *er = a.scratch + eb * 7;
     for (int k = tid; k < 6 * V; k += T) snbr[k] = a.nbr[k];
     for (int e = tid; e < E; e += T) {
         double e1[3], e2[3];
@@ -490,7 +473,6 @@ membrane_adjoint_kernel(const MembraneAdjArgs a)
         er[7 * e] = sqrt(g11 * g22 - g12 * g12);
     }
     __syncthreads();
-    // rows of D^-1 M, q, ds_bar and the scaled right-hand side D^-1 q_bar
     float q[VPT][3], rhs[VPT][3], dsb[VPT];
 #pragma unroll
     for (int m = 0; m < VPT; m++) {
@@ -556,33 +538,45 @@ membrane_adjoint_kernel(const MembraneAdjArgs a)
         rho = rho_n;
         __syncthreads();
     }
-    // lambda, q and ds_bar of every vertex to shared memory (the solve's buffers are free)
-    float4 *slam = dbuf, *sq = dbuf + V;
-    float *sdsb = coef;
 #pragma unroll
     for (int m = 0; m < VPT; m++) {
         const int i = tid + m * T;
         if (i >= V) continue;
-        slam[i] = make_float4(x[m][0], x[m][1], x[m][2], 0.f);
-        sq[i] = make_float4(q[m][0], q[m][1], q[m][2], 0.f);
-        sdsb[i] = dsb[m];
+        a.lam[vb + i] = make_float4(x[m][0], x[m][1], x[m][2], 0.f);
+        a.qv[vb + i] = make_float4(q[m][0], q[m][1], q[m][2], 0.f);
+        a.dsb[vb + i] = dsb[m];
     }
-    __syncthreads();
+}
+
+constexpr int MEM_ADJ_ELEM_THREADS = 128;
+
+// One thread per element of any cell: the adjoints of (load on b, load on c,
+// gab) from lambda, q and ds_bar of the element's vertices, contracted with
+// the Jacobian of element_loads (seven dual passes: e1, e2, C).  Writes the
+// edge adjoints to scratch[7 e + 1 .. 6] and adds dL/dC to cbar.
+__global__ void __launch_bounds__(MEM_ADJ_ELEM_THREADS)
+membrane_adjoint_element_kernel(const MembraneAdjArgs a)
+{
+    __shared__ double red[MEM_ADJ_ELEM_THREADS / 32];
+    const long long eg = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     double cb = 0.0;
-    for (int e = tid; e < E; e += T) {
+    if (eg < a.ne) {
+        const int cell = (int)(eg / a.E), e = (int)(eg - (long long)cell * a.E);
+        const long long vb = (long long)cell * a.V;
         double e1[3], e2[3];
         int ia, ib, ic;
         edges_of(a, vb, e, e1, e2, ia, ib, ic);
-        const float4 la = slam[ia], lb = slam[ib], lc = slam[ic], qa = sq[ia], qb = sq[ib], qc = sq[ic];
+        const float4 la = a.lam[vb + ia], lb = a.lam[vb + ib], lc = a.lam[vb + ic];
+        const float4 qa = a.qv[vb + ia], qb = a.qv[vb + ib], qc = a.qv[vb + ic];
         auto dotf = [](float4 u, float4 w) { return (double)u.x * w.x + (double)u.y * w.y + (double)u.z * w.z; };
         // M = sum_e gab (1 + delta_ij) / 24 over the element's vertex pairs; ds_i = sum_e gab / 6
         const double mdiag = -(dotf(la, qa) + dotf(lb, qb) + dotf(lc, qc));
         const double moff = -(dotf(la, qb) + dotf(lb, qa) + dotf(la, qc) + dotf(lc, qa) + dotf(lb, qc) + dotf(lc, qb));
-        const double gb = mdiag / 12.0 + moff / 24.0 + ((double)sdsb[ia] + sdsb[ib] + sdsb[ic]) / 6.0;
+        const double gb = mdiag / 12.0 + moff / 24.0 + ((double)a.dsb[vb + ia] + a.dsb[vb + ib] + a.dsb[vb + ic]) / 6.0;
         const double bBb[3] = {(double)lb.x - la.x, (double)lb.y - la.y, (double)lb.z - la.z};
         const double bCb[3] = {(double)lc.x - la.x, (double)lc.y - la.y, (double)lc.z - la.z};
-        const double4 G = a.gref[eb + e];
-        double res[7];
+        const double4 G = a.gref[eg];
+        double *er = a.scratch + 7 * eg;
 #pragma unroll 1
         for (int k = 0; k < 7; k++) {
             Dual<double> d1[3], d2[3], oB[3], oC[3], og;
@@ -594,32 +588,40 @@ membrane_adjoint_kernel(const MembraneAdjArgs a)
             element_loads<Dual<double>>(d1, d2, G.x, G.y, G.z, G.w, Cd, a.rgs, a.law, oB, oC, og);
             double s = og.d * gb;
             for (int c = 0; c < 3; c++) s += oB[c].d * bBb[c] + oC[c].d * bCb[c];
-            res[k] = s;
+            if (k < 6) er[1 + k] = s; else cb = s;
         }
-        for (int k = 0; k < 6; k++) er[7 * e + 1 + k] = res[k];
-        cb += res[6];
     }
-    cb = block_sum_r(cb, red);
-    if (tid == 0) atomicAdd(a.cbar, cb);
-    __syncthreads();
-    // edge adjoints to the vertices: e1 = x_b - x_a, e2 = x_c - x_a
 #pragma unroll
-    for (int m = 0; m < VPT; m++) {
-        const int i = tid + m * T;
-        if (i >= V) continue;
-        double xb[3] = {0.0, 0.0, 0.0};
-        for (int k = __ldg(&a.v2e_off[i]); k < __ldg(&a.v2e_off[i + 1]); k++) {
-            const int pk = __ldg(&a.v2e[k]);
-            const double *rec = er + 7 * v2e_elem(pk);
-            const int en = v2e_en(pk);
-            for (int c = 0; c < 3; c++) {
-                if (en == 0) xb[c] -= rec[1 + c] + rec[4 + c];
-                else if (en == 1) xb[c] += rec[1 + c];
-                else xb[c] += rec[4 + c];
-            }
-        }
-        for (int c = 0; c < 3; c++) a.Xd_bar[(long long)c * nv + vb + i] = xb[c];
+    for (int o = 16; o > 0; o >>= 1) cb += __shfl_xor_sync(0xffffffffu, cb, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = cb;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int w = 0; w < MEM_ADJ_ELEM_THREADS / 32; w++) s += red[w];
+        atomicAdd(a.cbar, s);
     }
+}
+
+// One thread per vertex of any cell: edge adjoints to the vertices
+// (e1 = x_b - x_a, e2 = x_c - x_a); writes Xd_bar.
+__global__ void membrane_adjoint_vertex_kernel(const MembraneAdjArgs a)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= a.nv) return;
+    const int cell = (int)(t / a.V), i = (int)(t - (long long)cell * a.V);
+    const double *er = a.scratch + 7 * ((long long)cell * a.E);
+    double xb[3] = {0.0, 0.0, 0.0};
+    for (int k = __ldg(&a.v2e_off[i]); k < __ldg(&a.v2e_off[i + 1]); k++) {
+        const int pk = __ldg(&a.v2e[k]);
+        const double *rec = er + 7 * v2e_elem(pk);
+        const int en = v2e_en(pk);
+        for (int c = 0; c < 3; c++) {
+            if (en == 0) xb[c] -= rec[1 + c] + rec[4 + c];
+            else if (en == 1) xb[c] += rec[1 + c];
+            else xb[c] += rec[4 + c];
+        }
+    }
+    for (int c = 0; c < 3; c++) a.Xd_bar[(long long)c * a.nv + t] = xb[c];
 }
 
 // ---- volume correction, reversed ------------------------------------------
@@ -784,30 +786,32 @@ void launch_lbm_adjoint(const Geom &g, const LbmAdjArgs &a, cudaStream_t s)
 {
     const dim3 grid((unsigned)((g.plane + LBM_ADJ_THREADS - 1) / LBM_ADJ_THREADS), (unsigned)g.nzc);
     lbm_adjoint_kernel<<<grid, LBM_ADJ_THREADS, 0, s>>>(a, g.nx, g.ny, g.nzc, g.nint);
-    const dim3 grid2((unsigned)((g.plane + 255) / 256), (unsigned)g.nzc);
-    lbm_pull_transpose_kernel<<<grid2, 256, 0, s>>>(a.gbar_pre, a.mask2d, a.gbar_in, g.nx, g.ny, g.nzc, g.nint);
+}
+
+static unsigned warp_blocks(long long nv) {
+    return (unsigned)((nv * 32 + VTX_ADJ_THREADS - 1) / VTX_ADJ_THREADS);
 }
 
 void launch_advect_adjoint(const Geom &g, const double *X, const float4 *uvr, const double *xa_bar, double *X_bar,
                            float *ubar, long long nv, double dtM, int *flags, cudaStream_t s)
 {
     if (nv <= 0) return;
-    advect_adjoint_kernel<<<(unsigned)((nv + 127) / 128), 128, 0, s>>>(g, X, uvr, xa_bar, X_bar, ubar, nv, dtM, flags);
+    advect_adjoint_kernel<<<warp_blocks(nv), VTX_ADJ_THREADS, 0, s>>>(g, X, uvr, xa_bar, X_bar, ubar, nv, dtM, flags);
 }
 
 void launch_spread_adjoint(const Geom &g, const double *X, const float *Fv, const float *Fbar, const uint32_t *mask2d,
                            double *Fv_bar, double *X_bar, long long nv, cudaStream_t s)
 {
     if (nv <= 0) return;
-    spread_adjoint_kernel<<<(unsigned)((nv + 127) / 128), 128, 0, s>>>(g, X, Fv, Fbar, mask2d, Fv_bar, X_bar, nv);
+    spread_adjoint_kernel<<<warp_blocks(nv), VTX_ADJ_THREADS, 0, s>>>(g, X, Fv, Fbar, mask2d, Fv_bar, X_bar, nv);
 }
 
 int volume_adjoint_smem_bytes(int V) { return 48 * V; }
 
 cudaError_t adjoint_setup(int optin)
 {
-    const void *ks[] = {(const void *)membrane_adjoint_kernel<1>, (const void *)membrane_adjoint_kernel<2>,
-                        (const void *)membrane_adjoint_kernel<3>, (const void *)membrane_adjoint_kernel<4>,
+    const void *ks[] = {(const void *)membrane_adjoint_solve_kernel<1>, (const void *)membrane_adjoint_solve_kernel<2>,
+                        (const void *)membrane_adjoint_solve_kernel<3>, (const void *)membrane_adjoint_solve_kernel<4>,
                         (const void *)volume_adjoint_kernel};
     for (const void *k : ks) {
         cudaFuncAttributes fa{};
@@ -826,11 +830,14 @@ void launch_membrane_adjoint(const MembraneAdjArgs &a, cudaStream_t s)
     const int T = (((a.V + vpt - 1) / vpt) + 31) / 32 * 32;
     const size_t smem = (size_t)membrane_smem_bytes(a.V);
     switch (vpt) {
-    case 1: membrane_adjoint_kernel<1><<<a.ncell, T, smem, s>>>(a); break;
-    case 2: membrane_adjoint_kernel<2><<<a.ncell, T, smem, s>>>(a); break;
-    case 3: membrane_adjoint_kernel<3><<<a.ncell, T, smem, s>>>(a); break;
-    default: membrane_adjoint_kernel<4><<<a.ncell, T, smem, s>>>(a); break;
+    case 1: membrane_adjoint_solve_kernel<1><<<a.ncell, T, smem, s>>>(a); break;
+    case 2: membrane_adjoint_solve_kernel<2><<<a.ncell, T, smem, s>>>(a); break;
+    case 3: membrane_adjoint_solve_kernel<3><<<a.ncell, T, smem, s>>>(a); break;
+    default: membrane_adjoint_solve_kernel<4><<<a.ncell, T, smem, s>>>(a); break;
     }
+    membrane_adjoint_element_kernel<<<(unsigned)((a.ne + MEM_ADJ_ELEM_THREADS - 1) / MEM_ADJ_ELEM_THREADS),
+                                      MEM_ADJ_ELEM_THREADS, 0, s>>>(a);
+    membrane_adjoint_vertex_kernel<<<(unsigned)((a.nv + 127) / 128), 128, 0, s>>>(a);
 }
 
 void launch_volume_adjoint(const Geom &g, const VolumeAdjArgs &a, cudaStream_t s)

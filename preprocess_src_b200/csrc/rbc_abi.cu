@@ -12,6 +12,7 @@
 #include <cstdio>
 #include <cstring>
 #include <algorithm>
+#include <map>
 #include <new>
 #include <numeric>
 #include <string>
@@ -1310,14 +1311,17 @@ int rbc_batch_autotune(rbc_batch *b, int steps_per_trial, int *chain_out)
 // rbc_adjoint_record runs the forward steps with the step graphs and keeps a
 // checkpoint of the state (populations, cel->x, fem->xd, centroids, iter)
 // every K steps, plus the state after the run.  rbc_adjoint_backward then
-// takes the segments in reverse order: it restores the segment's checkpoint,
-// recomputes the segment's steps stage by stage while storing what the
-// reverse stages read (populations, positions, membrane forces, lattice force,
-// velocity field, positions before the correction), and runs the adjoint
-// kernels of adjoint.cu step by step backwards through the segment.  Memory:
-// checkpoints (Q floats per node + 48 B per vertex) per segment, and K steps
-// of stored stages (26 floats per node + 84 B per vertex) for the segment in
-// flight.
+// takes the segments in reverse order: it restores a segment's checkpoint,
+// recomputes the segment stage by stage while storing what the reverse stages
+// read (populations, positions, membrane forces, lattice force, velocity
+// field, positions before the correction, drive), and runs the adjoint
+// kernels of adjoint.cu backwards through the segment.  Two segment stores
+// alternate: the recomputation of segment s - 1 (handle stream) runs while
+// segment s is reversed (adjoint stream), and each segment's recomputation
+// and reversal are CUDA graphs, captured once per (store, buffer parity,
+// length) and replayed.  Device memory: nsteps / K + 1 checkpoints
+// (4 Q B per node + 48 B per vertex) and 2 K steps of stored stages
+// (104 B per node + 84 B per vertex).
 
 struct AdjointState {
     int K = 0, nseg_cap = 0, K_cap = 0;
@@ -1327,23 +1331,38 @@ struct AdjointState {
     std::vector<void *> bufs;            // every allocation below, for adjoint_free
     // checkpoints [nseg + 1]
     float *ck_g = nullptr; double *ck_X = nullptr, *ck_Xd = nullptr, *ck_gx = nullptr;
-    // stored stages of one segment [K]
-    float *sg = nullptr, *sF = nullptr, *sFv = nullptr; float4 *suvr = nullptr;
-    double *sX = nullptr, *sXd = nullptr, *sXa = nullptr, *sgx = nullptr;
+    int *ck_itd = nullptr;               // the device iteration counter at each checkpoint
+    // stored stages of two segments [2][K]
+    float *sg = nullptr, *sF = nullptr, *sFv = nullptr, *sdrv = nullptr; float4 *suvr = nullptr;
+    double *sX = nullptr, *sXd = nullptr, *sXa = nullptr, *sgx = nullptr, *sfac = nullptr;
     // adjoint state and scratch
-    float *gbar[2] = {nullptr, nullptr}, *gbar_pre = nullptr, *Fbar = nullptr; float4 *ubar = nullptr;
+    float *gbar[2] = {nullptr, nullptr}, *Fbar = nullptr; float4 *ubar = nullptr;
+    float4 *lam = nullptr, *qv = nullptr; float *dsb = nullptr;
     double *Xbar = nullptr, *Xdbar = nullptr, *Xabar = nullptr, *Fvbar = nullptr;
     double *mscr = nullptr, *hist = nullptr, *escr = nullptr, *pbar = nullptr;
     int *status = nullptr;
     // outputs of the last recorded step (velocity field, vertex velocities and forces)
     float4 *fin_uvr = nullptr; float *fin_U = nullptr, *fin_Fv = nullptr;
     int kmax = 16;                       // volume-correction moves reversed per step
+    // reverse stream, store events, graphs keyed by (kind, store, parity, length)
+    cudaStream_t rev = nullptr;
+    cudaEvent_t filled[2] = {nullptr, nullptr}, drained[2] = {nullptr, nullptr};
+    std::map<long long, cudaGraphExec_t> graphs;
 };
+
+void adjoint_drop_graphs(AdjointState *a)
+{
+    for (auto &kv : a->graphs) if (kv.second) cudaGraphExecDestroy(kv.second);
+    a->graphs.clear();
+}
 
 void adjoint_free(AdjointState *a)
 {
     if (!a) return;
+    adjoint_drop_graphs(a);
     for (void *p : a->bufs) if (p) cudaFree(p);
+    for (cudaEvent_t e : {a->filled[0], a->filled[1], a->drained[0], a->drained[1]}) if (e) cudaEventDestroy(e);
+    if (a->rev) cudaStreamDestroy(a->rev);
     delete a;
 }
 
@@ -1363,20 +1382,31 @@ int adjoint_reserve(rbc_handle *h, int K, int nseg)
     if (!h->adj) h->adj = new (std::nothrow) AdjointState();
     if (!h->adj) return fail(h, RBC_ERR_CUDA, "out of host memory");
     AdjointState *a = h->adj;
+    if (!a->rev) {
+        CK(cudaStreamCreateWithFlags(&a->rev, cudaStreamNonBlocking));
+        for (int b = 0; b < 2; b++) {
+            CK(cudaEventCreateWithFlags(&a->filled[b], cudaEventDisableTiming));
+            CK(cudaEventCreateWithFlags(&a->drained[b], cudaEventDisableTiming));
+        }
+    }
     if (a->K_cap >= K && a->nseg_cap >= nseg) return RBC_OK;
+    adjoint_drop_graphs(a);
     for (void *p : a->bufs) if (p) cudaFree(p);
     a->bufs.clear();
+    a->K_cap = a->nseg_cap = 0;
     const size_t n = (size_t)h->geo.nint, nq = (size_t)Q * n, nv3 = 3 * (size_t)h->nv, N3 = 3 * (size_t)h->ncell;
-    const size_t nck = (size_t)nseg + 1, Kc = (size_t)K;
+    const size_t nck = (size_t)nseg + 1, S = 2 * (size_t)K;
     int rc;
 #define TRYA(x) do { if ((rc = (x))) { h->err = "adjoint: out of device memory (" #x ")"; return rc; } } while (0)
     TRYA(adj_alloc(h, &a->ck_g, nck * nq)); TRYA(adj_alloc(h, &a->ck_X, nck * nv3));
     TRYA(adj_alloc(h, &a->ck_Xd, nck * nv3)); TRYA(adj_alloc(h, &a->ck_gx, nck * N3));
-    TRYA(adj_alloc(h, &a->sg, Kc * nq)); TRYA(adj_alloc(h, &a->sF, Kc * 3 * n)); TRYA(adj_alloc(h, &a->sFv, Kc * nv3));
-    TRYA(adj_alloc(h, &a->suvr, Kc * n));
-    TRYA(adj_alloc(h, &a->sX, Kc * nv3)); TRYA(adj_alloc(h, &a->sXd, Kc * nv3)); TRYA(adj_alloc(h, &a->sXa, Kc * nv3));
-    TRYA(adj_alloc(h, &a->sgx, Kc * N3));
-    TRYA(adj_alloc(h, &a->gbar[0], nq)); TRYA(adj_alloc(h, &a->gbar[1], nq)); TRYA(adj_alloc(h, &a->gbar_pre, nq));
+    TRYA(adj_alloc(h, &a->ck_itd, nck));
+    TRYA(adj_alloc(h, &a->sg, S * nq)); TRYA(adj_alloc(h, &a->sF, S * 3 * n)); TRYA(adj_alloc(h, &a->sFv, S * nv3));
+    TRYA(adj_alloc(h, &a->suvr, S * n)); TRYA(adj_alloc(h, &a->sdrv, S)); TRYA(adj_alloc(h, &a->sfac, S));
+    TRYA(adj_alloc(h, &a->sX, S * nv3)); TRYA(adj_alloc(h, &a->sXd, S * nv3)); TRYA(adj_alloc(h, &a->sXa, S * nv3));
+    TRYA(adj_alloc(h, &a->sgx, S * N3));
+    TRYA(adj_alloc(h, &a->gbar[0], nq)); TRYA(adj_alloc(h, &a->gbar[1], nq));
+    TRYA(adj_alloc(h, &a->lam, h->nv)); TRYA(adj_alloc(h, &a->qv, h->nv)); TRYA(adj_alloc(h, &a->dsb, h->nv));
     TRYA(adj_alloc(h, &a->Fbar, 3 * n)); TRYA(adj_alloc(h, &a->ubar, n));
     TRYA(adj_alloc(h, &a->Xbar, nv3)); TRYA(adj_alloc(h, &a->Xdbar, nv3)); TRYA(adj_alloc(h, &a->Xabar, nv3));
     TRYA(adj_alloc(h, &a->Fvbar, nv3)); TRYA(adj_alloc(h, &a->mscr, 7 * (size_t)h->ne));
@@ -1389,9 +1419,9 @@ int adjoint_reserve(rbc_handle *h, int K, int nseg)
     return RBC_OK;
 }
 
-int d2d(rbc_handle *h, void *dst, const void *src, size_t bytes)
+int d2d(rbc_handle *h, void *dst, const void *src, size_t bytes, cudaStream_t st = nullptr)
 {
-    if (bytes) CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, h->stream));
+    if (bytes) CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, st ? st : h->stream));
     return RBC_OK;
 }
 
@@ -1405,6 +1435,7 @@ int adjoint_save(rbc_handle *h, int k)
     if ((rc = d2d(h, a->ck_X + k * nv3, h->X, 8 * nv3))) return rc;
     if ((rc = d2d(h, a->ck_Xd + k * nv3, h->Xd, 8 * nv3))) return rc;
     if ((rc = d2d(h, a->ck_gx + k * N3, h->gx, 8 * N3))) return rc;
+    if ((rc = d2d(h, a->ck_itd + k, h->d_iter(), sizeof(int)))) return rc;
     a->ck_iter[k] = h->iter;
     return RBC_OK;
 }
@@ -1423,92 +1454,130 @@ int adjoint_restore(rbc_handle *h, int k)
     CK(cudaMemsetAsync(h->Fz, 0, 4 * n, h->stream));
     h->force_pending = false;
     h->iter = a->ck_iter[k];
-    return prepare_steps(h);
+    return d2d(h, h->d_iter(), a->ck_itd + k, sizeof(int));   // device to device: no host staging
 }
 
-// recompute the steps of segment s, storing what the reverse stages read
-int adjoint_recompute(rbc_handle *h, int s, int len)
+constexpr int ADJ_KERNELS_PER_STEP = 14;   // 7 recomputation + 7 reverse kernels
+
+// Enqueue the recomputation of len steps from the handle's state into store b
+// (stream: the handle's).
+int adjoint_enqueue_recompute(rbc_handle *h, int b, int len)
 {
     AdjointState *a = h->adj;
     const size_t n = (size_t)h->geo.nint, nq = (size_t)Q * n, nv3 = 3 * (size_t)h->nv, N3 = 3 * (size_t)h->ncell;
     int rc;
-    if ((rc = adjoint_restore(h, s))) return rc;
     for (int t = 0; t < len; t++) {
-        if ((rc = d2d(h, a->sg + t * nq, h->g[h->cur], 4 * nq))) return rc;
-        if ((rc = d2d(h, a->sX + t * nv3, h->X, 8 * nv3))) return rc;
-        if ((rc = d2d(h, a->sXd + t * nv3, h->Xd, 8 * nv3))) return rc;
-        if ((rc = d2d(h, a->sgx + t * N3, h->gx, 8 * N3))) return rc;
-        launch_step_begin(h->d_iter(), h->d_drive, h->p.P, h->p.flowstart, h->p.freq, h->p.dt, h->stream);
+        const size_t k = (size_t)b * a->K + t;
+        if ((rc = d2d(h, a->sg + k * nq, h->g[h->cur], 4 * nq))) return rc;
+        if ((rc = d2d(h, a->sX + k * nv3, h->X, 8 * nv3))) return rc;
+        if ((rc = d2d(h, a->sXd + k * nv3, h->Xd, 8 * nv3))) return rc;
+        if ((rc = d2d(h, a->sgx + k * N3, h->gx, 8 * N3))) return rc;
+        launch_step_begin_recorded(h->d_iter(), h->d_drive, h->p.P, h->p.flowstart, h->p.freq, h->p.dt,
+                                   a->sdrv + k, a->sfac + k, h->stream);
         h->launches++;
         CK_LAUNCH();
         if ((rc = launch_stress(h))) return rc;
-        if ((rc = d2d(h, a->sFv + t * nv3, h->Fv, 4 * nv3))) return rc;
+        if ((rc = d2d(h, a->sFv + k * nv3, h->Fv, 4 * nv3))) return rc;
         if ((rc = launch_spread_stage(h))) return rc;
-        if ((rc = d2d(h, a->sF + t * 3 * n, h->Fx, 4 * n))) return rc;
-        if ((rc = d2d(h, a->sF + t * 3 * n + n, h->Fy, 4 * n))) return rc;
-        if ((rc = d2d(h, a->sF + t * 3 * n + 2 * n, h->Fz, 4 * n))) return rc;
+        if ((rc = d2d(h, a->sF + k * 3 * n, h->Fx, 4 * n))) return rc;
+        if ((rc = d2d(h, a->sF + k * 3 * n + n, h->Fy, 4 * n))) return rc;
+        if ((rc = d2d(h, a->sF + k * 3 * n + 2 * n, h->Fz, 4 * n))) return rc;
         if ((rc = launch_lbm_stage(h))) return rc;
-        if ((rc = d2d(h, a->suvr + t * n, h->uvr, 16 * n))) return rc;
+        if ((rc = d2d(h, a->suvr + k * n, h->uvr, 16 * n))) return rc;
         if ((rc = launch_advect_stage(h))) return rc;
-        if ((rc = d2d(h, a->sXa + t * nv3, h->Xd, 8 * nv3))) return rc;
+        if ((rc = d2d(h, a->sXa + k * nv3, h->Xd, 8 * nv3))) return rc;
         if ((rc = launch_volume_stage(h, h->stream))) return rc;
-        h->iter++;
     }
     return RBC_OK;
 }
 
-// reverse the steps of segment s (already recomputed); the adjoint of the
-// populations after the segment is in gbar[*gb] and moves to gbar[*gb ^ 1]
-// per step
-int adjoint_reverse(rbc_handle *h, int s, int len, int *gb)
+// Enqueue the reverse of len steps stored in store b (stream: a->rev); the
+// adjoint of the populations after them is in gbar[gb] and ends in
+// gbar[gb ^ (len & 1)].
+int adjoint_enqueue_reverse(rbc_handle *h, int b, int len, int gb)
 {
     AdjointState *a = h->adj;
     const size_t n = (size_t)h->geo.nint, nq = (size_t)Q * n, nv3 = 3 * (size_t)h->nv, N3 = 3 * (size_t)h->ncell;
     const Geom &g = h->geo;
+    cudaStream_t st = a->rev;
     for (int t = len - 1; t >= 0; t--) {
-        const int it = a->ck_iter[s] + t + 1;   // the iteration number step_begin gave this step
-        const double dfac = drive_factor(h->p, it);
+        const size_t k = (size_t)b * a->K + t;
         if (h->ncell > 0) {
             VolumeAdjArgs va{};
-            va.Xa = a->sXa + t * nv3; va.gx = a->sgx + t * N3; va.vol0 = h->vol0;
+            va.Xa = a->sXa + k * nv3; va.gx = a->sgx + k * N3; va.vol0 = h->vol0;
             va.tri = h->tri; va.v2e_off = h->v2e_off; va.v2e = h->v2e;
             va.X_bar = a->Xbar; va.Xd_bar = a->Xdbar; va.Xa_bar = a->Xabar;
             va.hist = a->hist; va.escr = a->escr; va.status = a->status;
             va.nv = h->nv; va.V = h->V; va.E = h->E; va.ncell = h->ncell; va.kmax = a->kmax;
-            launch_volume_adjoint(g, va, h->stream);
+            launch_volume_adjoint(g, va, st);
             CK_LAUNCH();
         }
-        CK(cudaMemsetAsync(a->ubar, 0, 16 * n, h->stream));
+        CK(cudaMemsetAsync(a->ubar, 0, 16 * n, st));
         if (h->ncell > 0) {
-            launch_advect_adjoint(g, a->sX + t * nv3, a->suvr + t * n, a->Xabar, a->Xbar, (float *)a->ubar, h->nv,
-                                  h->p.dt * h->p.M, h->d_flags(), h->stream);
+            launch_advect_adjoint(g, a->sX + k * nv3, a->suvr + k * n, a->Xabar, a->Xbar, (float *)a->ubar, h->nv,
+                                  h->p.dt * h->p.M, h->d_flags(), st);
             CK_LAUNCH();
         }
         LbmAdjArgs la{};
-        la.gin = a->sg + t * nq;
-        la.Fx = a->sF + t * 3 * n; la.Fy = la.Fx + n; la.Fz = la.Fx + 2 * n;
-        la.mask2d = h->mask2d; la.gbar_out = a->gbar[*gb]; la.ubar = a->ubar;
-        la.gbar_pre = a->gbar_pre; la.gbar_in = a->gbar[*gb ^ 1]; la.Fbar = a->Fbar; la.pbar = a->pbar;
-        la.pd = (float)(h->p.P * dfac); la.Bc = (float)h->p.B; la.omega = (float)(1.0 / h->p.tau); la.Cr = (float)h->p.Cr;
-        la.dfac = dfac;
-        launch_lbm_adjoint(g, la, h->stream);
+        la.gin = a->sg + k * nq;
+        la.Fx = a->sF + k * 3 * n; la.Fy = la.Fx + n; la.Fz = la.Fx + 2 * n;
+        la.mask2d = h->mask2d; la.gbar_out = a->gbar[gb]; la.ubar = a->ubar;
+        la.gbar_in = a->gbar[gb ^ 1]; la.Fbar = a->Fbar; la.pbar = a->pbar;
+        la.pd = a->sdrv + k; la.dfac = a->sfac + k;
+        la.Bc = (float)h->p.B; la.omega = (float)(1.0 / h->p.tau); la.Cr = (float)h->p.Cr;
+        launch_lbm_adjoint(g, la, st);
         CK_LAUNCH();
-        *gb ^= 1;
+        gb ^= 1;
         if (h->ncell > 0) {
-            launch_spread_adjoint(g, a->sX + t * nv3, a->sFv + t * nv3, a->Fbar, h->mask2d, a->Fvbar, a->Xbar, h->nv,
-                                  h->stream);
+            launch_spread_adjoint(g, a->sX + k * nv3, a->sFv + k * nv3, a->Fbar, h->mask2d, a->Fvbar, a->Xbar, h->nv, st);
             CK_LAUNCH();
             MembraneAdjArgs ma{};
-            ma.Xd = a->sXd + t * nv3; ma.nv = h->nv; ma.gref = h->gref;
+            ma.Xd = a->sXd + k * nv3; ma.nv = h->nv; ma.ne = h->ne; ma.gref = h->gref;
             ma.tri = h->tri; ma.v2e_off = h->v2e_off; ma.v2e = h->v2e; ma.nbr = h->nbr;
-            ma.Fv = a->sFv + t * nv3; ma.Fv_bar = a->Fvbar; ma.Xd_bar = a->Xdbar; ma.scratch = a->mscr;
+            ma.Fv = a->sFv + k * nv3; ma.Fv_bar = a->Fvbar; ma.Xd_bar = a->Xdbar; ma.scratch = a->mscr;
+            ma.lam = a->lam; ma.qv = a->qv; ma.dsb = a->dsb;
             ma.cbar = a->pbar + 2;
             ma.V = h->V; ma.E = h->E; ma.ncell = h->ncell;
             ma.C = h->p.C; ma.rgs = h->p.rgs; ma.law = h->p.law; ma.LX = h->p.LX; ma.LZ = h->p.LZ;
             ma.niter = h->p.solver_iters > 0 ? h->p.solver_iters : DEFAULT_SOLVER_ITERS;
-            launch_membrane_adjoint(ma, h->stream);
+            launch_membrane_adjoint(ma, st);
             CK_LAUNCH();
         }
+    }
+    return RBC_OK;
+}
+
+// Launch (capturing on first use) the graph of a segment's recomputation
+// (kind 0, on the handle stream, keyed by store and population buffer) or
+// reversal (kind 1, on the adjoint stream, keyed by store and adjoint buffer).
+int adjoint_launch_graph(rbc_handle *h, int kind, int b, int parity, int len)
+{
+    AdjointState *a = h->adj;
+    const long long key = ((long long)len << 3) | (kind << 2) | (b << 1) | parity;
+    cudaStream_t st = kind == 0 ? h->stream : a->rev;
+    auto it = a->graphs.find(key);
+    if (it == a->graphs.end()) {
+        const long long launches0 = h->launches;
+        const int cur0 = h->cur;
+        cudaGraph_t graph = nullptr;
+        CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        const int rc = kind == 0 ? adjoint_enqueue_recompute(h, b, len) : adjoint_enqueue_reverse(h, b, len, parity);
+        const cudaError_t e = cudaStreamEndCapture(st, &graph);
+        h->launches = launches0;
+        h->cur = cur0;
+        if (rc != RBC_OK) { if (graph) cudaGraphDestroy(graph); return rc; }
+        if (e != cudaSuccess) { h->err = std::string("adjoint graph capture: ") + cudaGetErrorString(e); return RBC_ERR_CUDA; }
+        cudaGraphExec_t exec = nullptr;
+        const cudaError_t ei = cudaGraphInstantiate(&exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ei != cudaSuccess) { h->err = std::string("adjoint graph instantiate: ") + cudaGetErrorString(ei); return RBC_ERR_CUDA; }
+        it = a->graphs.emplace(key, exec).first;
+    }
+    CK(cudaGraphLaunch(it->second, st));
+    h->launches += (long long)len * (ADJ_KERNELS_PER_STEP / 2);
+    if (kind == 0) {   // the recomputation advanced the handle
+        if (len & 1) h->cur ^= 1;
+        h->iter += len;
     }
     return RBC_OK;
 }
@@ -1534,16 +1603,14 @@ int rbc_adjoint_record(rbc_handle *h, int nsteps, int ckpt_every)
     const int K = std::min(ckpt_every, nsteps), nseg = (nsteps + K - 1) / K;
     if ((rc = adjoint_reserve(h, K, nseg))) return rc;
     AdjointState *a = h->adj;
+    if (a->K != K) adjoint_drop_graphs(a);   // the graphs index the stores by K
     a->valid = false;
     a->K = K; a->nsteps = nsteps; a->nseg = nseg;
     a->ck_iter.assign(nseg + 1, 0);
     CK(cudaStreamSynchronize(h->stream));
-    if (h->force_pending) {   // a spread force left by rbc_ibm_st1 belongs to no step of the run
-        CK(cudaMemsetAsync(h->Fx, 0, 4 * h->geo.nint, h->stream));
-        CK(cudaMemsetAsync(h->Fy, 0, 4 * h->geo.nint, h->stream));
-        CK(cudaMemsetAsync(h->Fz, 0, 4 * h->geo.nint, h->stream));
-        h->force_pending = false;
-    }
+    // a spread force left by rbc_ibm_st1 belongs to no step of the run; the
+    // device counter follows the host's
+    if ((rc = prepare_steps(h))) return rc;
     for (int s = 0; s < nseg; s++) {
         if ((rc = adjoint_save(h, s))) return rc;
         if ((rc = rbc_step(h, std::min(K, nsteps - s * K)))) return rc;
@@ -1572,24 +1639,38 @@ int rbc_adjoint_backward(rbc_handle *h, const double *xbar, const double *ybar, 
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
-    CK(cudaEventRecord(e0, h->stream));
     // seeds: adjoint of the final cel->x; nothing depends on the final populations or fem->xd
-    if (nv > 0) {
-        std::vector<double> seed(nv3, 0.0);
-        const double *in[3] = {xbar, ybar, zbar};
-        for (int c = 0; c < 3; c++) if (in[c]) std::copy(in[c], in[c] + nv, seed.begin() + c * nv);
-        CK(cudaMemcpy(a->Xbar, seed.data(), 8 * nv3, cudaMemcpyHostToDevice));
-        CK(cudaMemsetAsync(a->Xdbar, 0, 8 * nv3, h->stream));
-    }
-    int gb = 0;
+    std::vector<double> seed(nv3, 0.0);
+    const double *in[3] = {xbar, ybar, zbar};
+    for (int c = 0; c < 3; c++) if (in[c]) std::copy(in[c], in[c] + nv, seed.begin() + c * nv);
+    if (nv > 0) CK(cudaMemcpy(a->Xbar, seed.data(), 8 * nv3, cudaMemcpyHostToDevice));
+    CK(cudaEventRecord(e0, h->stream));
+    if (nv > 0) CK(cudaMemsetAsync(a->Xdbar, 0, 8 * nv3, h->stream));
     CK(cudaMemsetAsync(a->gbar[0], 0, 4 * nq, h->stream));
     CK(cudaMemsetAsync(a->pbar, 0, 4 * sizeof(double), h->stream));
     CK(cudaMemsetAsync(a->status, 0, sizeof(int), h->stream));
+    // the adjoint stream starts after the initialisation; store 1 starts drained
+    CK(cudaEventRecord(a->drained[1], h->stream));
+    auto seg_len = [&](int s) { return std::min(a->K, a->nsteps - s * a->K); };
+    int gb = 0;
+    // segment s uses store (nseg - 1 - s) & 1
+    if ((rc = adjoint_restore(h, a->nseg - 1))) return rc;
+    if ((rc = adjoint_launch_graph(h, 0, 0, h->cur, seg_len(a->nseg - 1)))) return rc;
+    CK(cudaEventRecord(a->filled[0], h->stream));
     for (int s = a->nseg - 1; s >= 0; s--) {
-        const int len = std::min(a->K, a->nsteps - s * a->K);
-        if ((rc = adjoint_recompute(h, s, len))) return rc;
-        if ((rc = adjoint_reverse(h, s, len, &gb))) return rc;
+        const int b = (a->nseg - 1 - s) & 1;
+        CK(cudaStreamWaitEvent(a->rev, a->filled[b], 0));
+        if ((rc = adjoint_launch_graph(h, 1, b, gb, seg_len(s)))) return rc;
+        gb ^= seg_len(s) & 1;
+        CK(cudaEventRecord(a->drained[b], a->rev));
+        if (s > 0) {   // recompute segment s - 1 into the other store while segment s is reversed
+            CK(cudaStreamWaitEvent(h->stream, a->drained[b ^ 1], 0));
+            if ((rc = adjoint_restore(h, s - 1))) return rc;
+            if ((rc = adjoint_launch_graph(h, 0, b ^ 1, h->cur, seg_len(s - 1)))) return rc;
+            CK(cudaEventRecord(a->filled[b ^ 1], h->stream));
+        }
     }
+    CK(cudaStreamWaitEvent(h->stream, a->drained[(a->nseg - 1) & 1], 0));
     CK(cudaEventRecord(e1, h->stream));
     double pb[4];
     int st = 0;
@@ -1626,10 +1707,13 @@ int rbc_set_coefficients(rbc_handle *h, double P, double B, double C)
     RBC_DEVICE_GUARD(h);
     CK(cudaStreamSynchronize(h->stream));
     h->p.P = P; h->p.B = B; h->p.C = C;
-    // the step graphs hold the coefficients as kernel arguments
+    // the step graphs and the adjoint graphs hold the coefficients as kernel arguments
     for (auto &form : h->graph)
         for (cudaGraphExec_t &g : form) if (g) { cudaGraphExecDestroy(g); g = nullptr; }
-    if (h->adj) h->adj->valid = false;
+    if (h->adj) {
+        h->adj->valid = false;
+        adjoint_drop_graphs(h->adj);
+    }
     return RBC_OK;
 }
 

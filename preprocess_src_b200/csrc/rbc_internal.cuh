@@ -178,6 +178,9 @@ int  setup_kernel_attributes(int *membrane_max_smem);
 
 void launch_step_begin(int *d_iter, float *d_drive, double P, int flowstart, double freq, double dt,
                        cudaStream_t s);
+// the same, also storing the step's drive P * factor and factor (for the adjoint)
+void launch_step_begin_recorded(int *d_iter, float *d_drive, double P, int flowstart, double freq, double dt,
+                                float *drive_rec, double *factor_rec, cudaStream_t s);
 
 // ---- adjoint of one step (adjoint.cu); FP32 populations ----------------------
 
@@ -187,12 +190,12 @@ struct LbmAdjArgs {
     const uint32_t *mask2d;
     const float *gbar_out;     // adjoint of g_t+1, [Q][n]
     const float4 *ubar;        // adjoint of the velocity, [n]
-    float *gbar_pre;           // out: adjoint of the pulled populations, [Q][n]
-    float *gbar_in;            // out: adjoint of g_t, [Q][n]
+    float *gbar_in;            // out: adjoint of g_t, [Q][n] (fluid slots)
     float *Fbar;               // out: adjoint of the force, [3][n]
     double *pbar;              // += (dfac dL/dpd, dL/dB)
-    float pd, Bc, omega, Cr;   // drive P * factor of the step, B, 1 / tau, Cr
-    double dfac;               // drive factor of the step (dpd / dP)
+    const float *pd;           // device: drive P * factor of the step
+    const double *dfac;        // device: drive factor of the step (dpd / dP)
+    float Bc, omega, Cr;       // B, 1 / tau, Cr
 };
 void launch_lbm_adjoint(const Geom &g, const LbmAdjArgs &a, cudaStream_t s);
 void launch_advect_adjoint(const Geom &g, const double *X, const float4 *uvr, const double *xa_bar, double *X_bar,
@@ -201,14 +204,16 @@ void launch_spread_adjoint(const Geom &g, const double *X, const float *Fv, cons
                            double *Fv_bar, double *X_bar, long long nv, cudaStream_t s);
 
 struct MembraneAdjArgs {
-    const double *Xd; long long nv;
+    const double *Xd; long long nv, ne;
     const double4 *gref;
     const int *tri, *v2e_off, *v2e;
     const int16_t *nbr;
     const float *Fv;           // the step's membrane forces
     const double *Fv_bar;      // their adjoint, [3][nv]
     double *Xd_bar;            // out, [3][nv]
-    double *scratch;           // [ne][7]
+    double *scratch;           // [ne][7]: gab, adjoints of the edge vectors
+    float4 *lam, *qv;          // [nv] scratch: lambda = M^-1 q_bar and q per vertex
+    float *dsb;                // [nv] scratch: adjoint of the one-ring area / 3
     double *cbar;              // += dL/dC
     int V, E, ncell;
     double C, rgs; int law;

@@ -178,18 +178,27 @@ int setup_kernel_attributes(int *membrane_max_smem)
     return 0;
 }
 
-__global__ void step_begin_kernel(int *iter, float *drive, double P, int flowstart, double freq, double dt)
+__global__ void step_begin_kernel(int *iter, float *drive, double P, int flowstart, double freq, double dt,
+                                  float *drive_rec, double *factor_rec)
 {
     const int it = *iter + 1;
     *iter = it;
     const double wi = (it > flowstart) ? 1.0 + 0.5 * sin(M_PI * dt * (double)it / freq) : 0.0;
     *drive = (float)(P * wi);
+    if (drive_rec) *drive_rec = (float)(P * wi);   // kept for the adjoint of the step
+    if (factor_rec) *factor_rec = wi;
 }
 
 void launch_step_begin(int *d_iter, float *d_drive, double P, int flowstart, double freq, double dt,
                        cudaStream_t s)
 {
-    step_begin_kernel<<<1, 1, 0, s>>>(d_iter, d_drive, P, flowstart, freq, dt);
+    step_begin_kernel<<<1, 1, 0, s>>>(d_iter, d_drive, P, flowstart, freq, dt, nullptr, nullptr);
+}
+
+void launch_step_begin_recorded(int *d_iter, float *d_drive, double P, int flowstart, double freq, double dt,
+                                float *drive_rec, double *factor_rec, cudaStream_t s)
+{
+    step_begin_kernel<<<1, 1, 0, s>>>(d_iter, d_drive, P, flowstart, freq, dt, drive_rec, factor_rec);
 }
 
 }  // namespace rbc
