@@ -173,17 +173,19 @@ def test_lbm_matches_oracle(developed, oracle_mod):
     assert ferr <= 1e-8 and derr <= 1e-6 and uerr <= 1e-5
 
 
-# (duct width = lattice nx, height, storage): rows of 20, 21 and 24 nodes
-# put warps across row ends and wall columns in different lanes; FP16 stores
-# (f - w) * 2^15 in binary16.
-@pytest.mark.parametrize("width,height,storage", [
-    (20, 16, 0),
-    (21, 18, 0),
-    (24, 16, 1),
-    (20, 16, 1),
+# (duct width = lattice nx, height, storage, length): rows of 20, 21 and 24
+# nodes put warps across row ends and wall columns in different lanes; FP16
+# stores (f - w) * 2^15 in binary16 and pulls two planes per thread, so an odd
+# length (33 planes) leaves one thread a single plane.
+@pytest.mark.parametrize("width,height,storage,flow", [
+    (20, 16, 0, 32),
+    (21, 18, 0, 32),
+    (24, 16, 1, 32),
+    (20, 16, 1, 32),
+    (21, 18, 1, 33),
 ])
-def test_pure_fluid_lbm_matches_oracle(oracle_mod, native_lib, width, height, storage):
-    case = configs.duct_case(f"fluid_32x{width}x{height}", 32, width, height, g=1e-4)
+def test_pure_fluid_lbm_matches_oracle(oracle_mod, native_lib, width, height, storage, flow):
+    case = configs.duct_case(f"fluid_{flow}x{width}x{height}", flow, width, height, g=1e-4)
     o = oracle_mod.Oracle(case)
     o.step(30)
     sim = load(o, storage=storage)
