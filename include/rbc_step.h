@@ -262,6 +262,36 @@ int rbc_adjoint_backward(rbc_handle *h, const double *xbar, const double *ybar, 
  * destroyed and created again.  Synchronous. */
 int rbc_set_coefficients(rbc_handle *h, double P, double B, double C);
 
+/* ---- files in the reference's formats (etc.cu) ---------------------------- */
+
+/* The reference's output_data / restart_file files for a red-cell run (no
+ * white cells, no cytoadhesion), byte for byte: restart.bin (etc.cu:738-766,
+ * read by restart_file etc.cu:164-270), cell%04d.bin (etc.cu:566-590),
+ * prof%04d.bin (etc.cu:547-560) and center.dat (OutputCapsuleCenter /
+ * InputCapsuleCenter etc.cu:110-160).  The caller names the files (the
+ * reference builds the names from prc->fnum).  vf / vf2 (VOF indicator, only
+ * used with a viscosity contrast) are written as 0, the reference's unset
+ * rx / ry / rz as 0; both are ignored when read.  Synchronous. */
+
+/* FILEOUTPUT: from the next step on, fem->qi (the load of the membrane solve)
+ * and fem->tp (the principal tensions of each element) are averaged over
+ * output intervals of fileoutput steps as the reference does (reset in the
+ * first step of an interval, stress.cu:101-118, 280-300); 0 stops it and the
+ * files then hold the last averages, or zeros when none was ever kept. */
+int rbc_set_output_interval(rbc_handle *h, int fileoutput);
+int rbc_write_restart(rbc_handle *h, const char *path, int fnum);
+/* Imports a restart.bin written for this handle's lattice and cells: the
+ * populations, positions (cel->x and fem->xd), the averages and the iteration
+ * counter (0 with fnum 0 when the file's fnum exceeds 100, etc.cu:205).
+ * *fnum (may be NULL) receives the file's output counter.  A file of another
+ * size is RBC_ERR_ARG. */
+int rbc_read_restart(rbc_handle *h, const char *path, int *fnum);
+int rbc_write_cell_file(rbc_handle *h, const char *path);
+int rbc_write_prof_file(rbc_handle *h, const char *path);
+int rbc_write_center_file(rbc_handle *h, const char *path);
+/* cel->gx, the centroids the volume correction unwraps about */
+int rbc_read_center_file(rbc_handle *h, const char *path);
+
 /* ---- without allocation -------------------------------------------------- */
 
 /* No counterpart in the reference.  Per-cell FP64 volume, area and vertex

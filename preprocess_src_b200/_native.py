@@ -81,6 +81,13 @@ _SIGS = {
     "rbc_adjoint_record": [_H, C.c_int, C.c_int],
     "rbc_adjoint_backward": [_H, _DP, _DP, _DP, _DP, _DP, _DP, _DP, _IP, C.POINTER(C.c_float)],
     "rbc_set_coefficients": [_H, C.c_double, C.c_double, C.c_double],
+    "rbc_set_output_interval": [_H, C.c_int],
+    "rbc_write_restart": [_H, C.c_char_p, C.c_int],
+    "rbc_read_restart": [_H, C.c_char_p, _IP],
+    "rbc_write_cell_file": [_H, C.c_char_p],
+    "rbc_write_prof_file": [_H, C.c_char_p],
+    "rbc_write_center_file": [_H, C.c_char_p],
+    "rbc_read_center_file": [_H, C.c_char_p],
 }
 _RESTYPE = {"rbc_last_error": C.c_char_p, "rbc_batch_last_error": C.c_char_p}
 

@@ -83,8 +83,14 @@ struct rbc_handle {
     int *patch_off = nullptr, *patch_vtx = nullptr, *patch_stride = nullptr;
     int npatch = 1;
     AdjointState *adj = nullptr;                      // checkpoints and buffers of the adjoint, on first use
+    // output-interval averages of the load and the principal tensions (fem->qi, fem->tp)
+    int fileoutput = 0;                               // FILEOUTPUT; 0 = not accumulated
+    int mn = 0;                                       // the reference's per-cell vector length (expand2pow2(3 V))
+    double *qi_acc = nullptr, *tp_acc = nullptr;      // [ncell][mn], [ne][2]
 
-    int kernels_per_step() const { return KERNELS_PER_STEP + (p.br != 0.0 && ncell > 0 ? 1 : 0); }
+    int kernels_per_step() const {
+        return KERNELS_PER_STEP + (p.br != 0.0 && ncell > 0 ? 1 : 0) + (fileoutput > 0 && ncell > 0 ? 2 : 0);
+    }
     int *d_iter() { return d_int; }
     int *d_flags() { return d_int + 1; }
     int *d_vcmax() { return d_int + 2; }
@@ -381,6 +387,8 @@ void free_all(rbc_handle *h)
                     h->X, h->Xd, h->gref, h->erec, h->U, h->Fv, h->tri, h->v2e_off, h->v2e, h->nbr, h->visit, h->patch_off, h->patch_vtx, h->patch_stride, h->vol0, h->gx,
                     h->vol_out, h->area_out, h->cen_out, h->d_int, h->d_drive, h->staging};
     for (void *q : ptrs) if (q) cudaFree(q);
+    if (h->qi_acc) cudaFree(h->qi_acc);
+    if (h->tp_acc) cudaFree(h->tp_acc);
     adjoint_free(h->adj);
     h->adj = nullptr;
     if (h->stream) cudaStreamDestroy(h->stream);
@@ -402,6 +410,16 @@ int launch_stress(rbc_handle *h)
     launch_membrane(a, h->p.membrane_fp64 != 0, h->stream);
     h->launches++;
     CK_LAUNCH();
+    if (h->fileoutput > 0) {   // calc_tension's tp and substitute_load's qi (stress.cu:101-118, 280-300)
+        AccumArgs c{};
+        c.Xd = h->Xd; c.Fv = h->Fv; c.gref = h->gref; c.tri = h->tri; c.v2e_off = h->v2e_off; c.v2e = h->v2e;
+        c.iter = h->d_iter(); c.qi = h->qi_acc; c.tp = h->tp_acc; c.nv = h->nv; c.ne = h->ne;
+        c.V = h->V; c.E = h->E; c.ncell = h->ncell; c.fileoutput = h->fileoutput; c.M = h->p.M;
+        c.C = h->p.C; c.LX = h->p.LX; c.LZ = h->p.LZ;
+        launch_output_accum(c, h->stream);
+        h->launches += 2;
+        CK_LAUNCH();
+    }
     return RBC_OK;
 }
 
@@ -1461,7 +1479,19 @@ constexpr int ADJ_KERNELS_PER_STEP = 14;   // 7 recomputation + 7 reverse kernel
 
 // Enqueue the recomputation of len steps from the handle's state into store b
 // (stream: the handle's).
+int adjoint_enqueue_recompute_body(rbc_handle *h, int b, int len);
+
 int adjoint_enqueue_recompute(rbc_handle *h, int b, int len)
+{
+    // the recomputation repeats past steps: it must not add to the output averages again
+    const int f = h->fileoutput;
+    h->fileoutput = 0;
+    const int rc = adjoint_enqueue_recompute_body(h, b, len);
+    h->fileoutput = f;
+    return rc;
+}
+
+int adjoint_enqueue_recompute_body(rbc_handle *h, int b, int len)
 {
     AdjointState *a = h->adj;
     const size_t n = (size_t)h->geo.nint, nq = (size_t)Q * n, nv3 = 3 * (size_t)h->nv, N3 = 3 * (size_t)h->ncell;
@@ -1718,3 +1748,100 @@ int rbc_set_coefficients(rbc_handle *h, double P, double B, double C)
 }
 
 }  // extern "C"
+
+// ---- output-interval averages and the reference bc map (for ref_files.cu) ---
+
+namespace rbc {
+
+// expand2pow2 (etc.cu:425-446): the reference's per-cell vector length for 3 V values
+int reference_mn(int V)
+{
+    int n = 3 * V, cnt = 0;
+    while (n > 1) {
+        if (n % 2 == 1) n += 1;
+        n /= 2;
+        cnt++;
+    }
+    return 1 << cnt;
+}
+
+// fem->qi [ncell * mn] and fem->tp [2 ne] to (set = false) or from (set = true)
+// host arrays; zeros when no output interval is set
+int output_averages(rbc_handle *h, double *qi, double *tp, bool set)
+{
+    RBC_DEVICE_GUARD(h);
+    const size_t nq = (size_t)h->ncell * h->mn, nt = 2 * (size_t)h->ne;
+    CK(cudaStreamSynchronize(h->stream));
+    if (!h->qi_acc) {
+        if (!set) {
+            if (qi) std::fill(qi, qi + nq, 0.0);
+            if (tp) std::fill(tp, tp + nt, 0.0);
+        }
+        return RBC_OK;
+    }
+    if (set) {
+        if (qi) CK(cudaMemcpy(h->qi_acc, qi, 8 * nq, cudaMemcpyHostToDevice));
+        if (tp) CK(cudaMemcpy(h->tp_acc, tp, 8 * nt, cudaMemcpyHostToDevice));
+    } else {
+        if (qi) CK(cudaMemcpy(qi, h->qi_acc, 8 * nq, cudaMemcpyDeviceToHost));
+        if (tp) CK(cudaMemcpy(tp, h->tp_acc, 8 * nt, cudaMemcpyDeviceToHost));
+    }
+    return RBC_OK;
+}
+
+// The reference's bc map [nz][ny][nx] of this handle: WALL off the fluid
+// columns, COMP on them in the periodic planes, BUFF in the two planes at
+// each z end (the structure rbc_create accepted).
+int reference_bc(rbc_handle *h, int *bc)
+{
+    RBC_DEVICE_GUARD(h);
+    const long long plane = h->geo.plane;
+    std::vector<uint32_t> mask(plane);
+    CK(cudaMemcpy(mask.data(), h->mask2d, 4 * plane, cudaMemcpyDeviceToHost));
+    const int nz = h->p.nz;
+    for (int z = 0; z < nz; z++) {
+        const bool buff = z < 2 || z >= nz - 2;
+        for (long long xy = 0; xy < plane; xy++)
+            bc[z * plane + xy] = (mask[xy] & MASK_FLUID) ? (buff ? RBC_BUFF : RBC_COMP) : RBC_WALL;
+    }
+    return RBC_OK;
+}
+
+int reference_ele(rbc_handle *h, int *ele)
+{
+    RBC_DEVICE_GUARD(h);
+    std::vector<int> tri(3 * (size_t)h->E);
+    if (h->E > 0) CK(cudaMemcpy(tri.data(), h->tri, 4 * tri.size(), cudaMemcpyDeviceToHost));
+    for (int c = 0; c < h->ncell; c++)
+        for (size_t k = 0; k < tri.size(); k++) ele[(size_t)c * tri.size() + k] = tri[k] + c * h->V;
+    return RBC_OK;
+}
+
+void set_handle_error(rbc_handle *h, const std::string &msg)
+{
+    if (h) h->err = msg; else g_create_error = msg;
+}
+
+}  // namespace rbc
+
+extern "C" int rbc_set_output_interval(rbc_handle *h, int fileoutput)
+{
+    if (!h || fileoutput < 0) return RBC_ERR_ARG;
+    RBC_DEVICE_GUARD(h);
+    CK(cudaStreamSynchronize(h->stream));
+    if (fileoutput > 0 && h->ncell > 0 && !h->qi_acc) {
+        h->mn = reference_mn(h->V);
+        const size_t nq = (size_t)h->ncell * h->mn, nt = 2 * (size_t)h->ne;
+        CK(cudaMalloc(&h->qi_acc, 8 * nq));
+        CK(cudaMalloc(&h->tp_acc, 8 * nt));
+        CK(cudaMemset(h->qi_acc, 0, 8 * nq));   // as fem_init leaves fem->qi (init2.cu:310)
+        CK(cudaMemset(h->tp_acc, 0, 8 * nt));
+    }
+    if (fileoutput != h->fileoutput) {
+        h->fileoutput = h->ncell > 0 ? fileoutput : 0;
+        // the step graphs hold the accumulation launches (or not)
+        for (auto &form : h->graph)
+            for (cudaGraphExec_t &g : form) if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    }
+    return RBC_OK;
+}

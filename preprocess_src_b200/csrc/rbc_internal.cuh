@@ -21,6 +21,8 @@
 #include <cuda_fp16.h>
 #include <stdint.h>
 
+#include <string>
+
 #include "rbc_step.h"
 
 namespace rbc {
@@ -143,6 +145,28 @@ struct MembraneArgs {
     int priority;             // launch priority (cudaLaunchAttributePriority)
 };
 int  membrane_smem_bytes(int V);
+
+// host helpers of the reference-format files (rbc_abi.cu)
+int reference_mn(int V);
+int output_averages(rbc_handle *h, double *qi, double *tp, bool set);
+int reference_bc(rbc_handle *h, int *bc);
+int reference_ele(rbc_handle *h, int *ele);          // cel->eleH: [ncell * E * 3] global vertex ids
+void set_handle_error(rbc_handle *h, const std::string &msg);
+
+// Output-interval averages of the load and the principal tensions (fem->qi,
+// fem->tp of the reference's output files), after the membrane kernel.
+struct AccumArgs {
+    const double *Xd; const float *Fv;
+    const double4 *gref;
+    const int *tri, *v2e_off, *v2e;
+    const int *iter;                 // device iteration counter of the step
+    double *qi;                      // [ncell][3 V] AoS per vertex (the reference's qd layout)
+    double *tp;                      // [ne][2]
+    long long nv, ne;
+    int V, E, ncell, fileoutput, M;
+    double C, LX, LZ;
+};
+void launch_output_accum(const AccumArgs &a, cudaStream_t s);
 
 // fourpoint_bend (stress.cu:448-578): added to Fv after the membrane forces
 struct BendArgs {

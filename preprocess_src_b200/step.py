@@ -149,6 +149,32 @@ class Simulation:
         self._call("rbc_export_ref_cells", *[_dp(out[k]) for k in keys])
         return out
 
+    # -- files in the reference's formats (etc.cu) -------------------------------
+    def set_output_interval(self, fileoutput: int):
+        """FILEOUTPUT: average fem->qi and fem->tp over intervals of this many steps."""
+        self._call("rbc_set_output_interval", int(fileoutput))
+
+    def write_restart(self, path, fnum: int = 0):
+        self._call("rbc_write_restart", str(path).encode(), int(fnum))
+
+    def read_restart(self, path) -> int:
+        """Returns the file's fnum."""
+        f = C.c_int(0)
+        self._call("rbc_read_restart", str(path).encode(), C.byref(f))
+        return f.value
+
+    def write_cell_file(self, path):
+        self._call("rbc_write_cell_file", str(path).encode())
+
+    def write_prof_file(self, path):
+        self._call("rbc_write_prof_file", str(path).encode())
+
+    def write_center_file(self, path):
+        self._call("rbc_write_center_file", str(path).encode())
+
+    def read_center_file(self, path):
+        self._call("rbc_read_center_file", str(path).encode())
+
     # -- adjoint ----------------------------------------------------------------
     def set_coefficients(self, P=None, B=None, C_=None):
         """Replace the drive P, IB-force B and area-dilation C coefficients."""
