@@ -14,8 +14,7 @@ import numpy as np
 import pytest
 
 from oracle import ref_files as RF
-from preprocess_src_b200 import configs
-from tests.test_gpu_parity import comp, load, parity_case, rel_l2
+from tests.test_gpu_parity import comp, parity_case, rel_l2
 
 pytestmark = pytest.mark.gpu
 
