@@ -63,6 +63,19 @@ extern "C" {
 #define RBC_STORE_F32 0            /* f_i - w_i in FP32: 180 B per lattice update */
 #define RBC_STORE_F16 1            /* (f_i - w_i) * scale in FP16: 104 B per lattice update */
 
+/* flow modes.  CHANNEL: z periodic with two BUFF planes at each end, walls from
+ * the bc map (the same in every z plane), body-force drive P along z.  SHEAR
+ * (init1.cu:133-187, lbm.cu:706-980): a box periodic in x and z (two BUFF
+ * layers at each end of both) between two y walls half a node beyond rows 2
+ * and ny - 3 that move along z (walls: both at -/+ sr LY / 2 or the top at
+ * sr LY, LY = (ny - 4) dx, from iteration FLOWSTART on); no body force
+ * (P = 0); with FLOWSTART = 0 rbc_create starts from the walls' linear
+ * profile as flu_init does. */
+#define RBC_FLOW_CHANNEL 0
+#define RBC_FLOW_SHEAR   1
+#define RBC_WALLS_BOTH   0
+#define RBC_WALLS_TOP    1
+
 /* membrane constitutive law (stress.cu:94-99) */
 #define RBC_LAW_SKALAK     0
 #define RBC_LAW_NEOHOOKEAN 1
@@ -98,6 +111,10 @@ typedef struct rbc_params {
     int    membrane_fp64;/* 1: element mechanics in FP64, 0: FP32 */
     int    solver_iters; /* Chebyshev iterations of the load solve; 0 = default (16) */
     int    device;       /* CUDA device ordinal; -1 = device 0 of this library's runtime */
+    /* flow mode */
+    int    flow;         /* RBC_FLOW_CHANNEL (CapsuleCHANNELFLOW) or RBC_FLOW_SHEAR (CapsuleSHEARFLOW) */
+    double sr;           /* cdo->sr, shear rate of the moving walls (shear mode; lattice units) */
+    int    walls;        /* RBC_WALLS_BOTH (allwall: walls at -/+ sr LY/2) or RBC_WALLS_TOP (topwall: top at sr LY) */
 } rbc_params;
 
 typedef struct rbc_mesh {

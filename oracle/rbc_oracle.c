@@ -205,11 +205,23 @@ int orc_fem_init(const orc_params *p, orc_state *s)
 /* init1.cu:413-434 with td = 1, u = 0 (CapsuleCHANNELFLOW branch 399-407) */
 void orc_flu_init(const orc_params *p, orc_state *s)
 {
-    long n = (long)p->nx * p->ny * p->nz;
+    long n = (long)p->nx * p->ny * p->nz, plane = (long)p->nx * p->ny;
+    double LY = (double)(p->ny - 4) * p->dx, Cr = p->Cr, Cr2 = Cr * Cr;
     for (long i = 0; i < n; i++) {
-        for (int q = 0; q < ORC_Q; q++) { s->fn[i*ORC_Q + q] = WQ[q]; s->fm[i*ORC_Q + q] = 0.0; }
-        s->dn[i] = 1.0; s->un[i] = 0.0; s->vn[i] = 0.0; s->wn[i] = 0.0;
-        s->dm[i] = 1.0; s->um[i] = 0.0; s->vm[i] = 0.0; s->wm[i] = 0.0;
+        double tw = 0.0;
+        if (p->flow == 1 && p->flowstart == 0) {
+            long iy = (i % plane) / p->nx;
+            tw = p->walls == 0 ? p->sr * (-LY / 2.0 - 1.5 * p->dx + (double)iy * p->dx)
+                               : p->sr * (-1.5 * p->dx + (double)iy * p->dx);
+        }
+        double uvw = -1.5 * tw * tw * Cr2;
+        for (int q = 0; q < ORC_Q; q++) {
+            double eu = EZ[q] * tw;
+            s->fn[i*ORC_Q + q] = WQ[q] * (1.0 + 3.0 * eu * Cr + 4.5 * eu * eu * Cr2 + uvw);
+            s->fm[i*ORC_Q + q] = 0.0;
+        }
+        s->dn[i] = 1.0; s->un[i] = 0.0; s->vn[i] = 0.0; s->wn[i] = tw;
+        s->dm[i] = 1.0; s->um[i] = 0.0; s->vm[i] = 0.0; s->wm[i] = tw;
         s->fx[i] = 0.0; s->fy[i] = 0.0; s->fz[i] = 0.0;
     }
 }
@@ -506,13 +518,26 @@ void orc_ibm_st1(const orc_params *p, orc_state *s)
                     s->fz[i] += dlt * s->cfz[jid];
                 }
     }
-    long plane = (long)nx * ny, shift = plane * (nz - 4);
+    long plane = (long)nx * ny, shift = plane * (nz - 4), xs = nx - 4;
 #pragma omp parallel for schedule(static)
     for (long i = 0; i < n; i++) {
         if (s->bc[i] != ORC_COMP) continue;
-        long iz = i / plane;
-        if (iz <= 3) { s->fx[i] += s->fx[i + shift]; s->fy[i] += s->fy[i + shift]; s->fz[i] += s->fz[i + shift]; }
-        if (iz >= nz - 4) { s->fx[i] += s->fx[i - shift]; s->fy[i] += s->fy[i - shift]; s->fz[i] += s->fz[i - shift]; }
+        long iz = i / plane, ix = (i % plane) % nx;
+        /* every COMP node adds the spread force its BUFF images received (ibm.cu:239-294);
+         * the images are not modified, so the order of the adds does not matter */
+        long img[8];
+        int k = 0;
+        if (iz <= 3) img[k++] = i + shift;
+        if (iz >= nz - 4) img[k++] = i - shift;
+        if (p->flow == 1) {
+            if (ix <= 3) img[k++] = i + xs;
+            if (ix >= nx - 4) img[k++] = i - xs;
+            if (ix <= 3 && iz <= 3) img[k++] = i + xs + shift;
+            if (ix >= nx - 4 && iz <= 3) img[k++] = i - xs + shift;
+            if (ix <= 3 && iz >= nz - 4) img[k++] = i + xs - shift;
+            if (ix >= nx - 4 && iz >= nz - 4) img[k++] = i - xs - shift;
+        }
+        for (int t = 0; t < k; t++) { s->fx[i] += s->fx[img[t]]; s->fy[i] += s->fy[img[t]]; s->fz[i] += s->fz[img[t]]; }
     }
 }
 
@@ -609,6 +634,25 @@ void orc_lbm_d3q19(const orc_params *p, orc_state *s)
             }
             f[q] = om1 * f[q] + om * feq + om2 * WQ[q] * sP + om3 * WQ[q] * sB;
         }
+        if (p->flow == 1) {
+            /* lbm.cu:754-826, 922-978: x and z periodic through the COMP range, half-way
+             * bounce-back at the y walls, which move along z (sra = 0 before FLOWSTART) */
+            long iz = i / plane, iy = (i % plane) / nx, ix = (i % plane) % nx;
+            double sra = (iter < p->flowstart) ? 0.0 : p->sr, LY = (double)(ny - 4) * p->dx;
+            double utop = p->walls == 0 ? sra * LY / 2.0 : sra * LY, ubot = p->walls == 0 ? -sra * LY / 2.0 : 0.0;
+            for (int q = 0; q < ORC_Q; q++) {
+                long jx = ix + EX[q], jy = iy + EY[q], jz = iz + EZ[q];
+                if (jx > nx - 3) jx -= nx - 4; else if (jx < 2) jx += nx - 4;
+                if (jz > nz - 3) jz -= nz - 4; else if (jz < 2) jz += nz - 4;
+                if (jy > ny - 3 || jy < 2) {
+                    double uw = jy > ny - 3 ? utop : ubot;
+                    fm[i * ORC_Q + OPP[q]] = f[q] - 6.0 * WQ[q] * td * Cr * EZ[q] * uw;
+                } else {
+                    fm[(jx + (long)nx * jy + plane * jz) * ORC_Q + q] = f[q];
+                }
+            }
+            continue;
+        }
         /* push streaming with half-way bounce-back (lbm.cu:1050-1094, 1272-1310) */
         for (int q = 0; q < ORC_Q; q++) {
             long d = i + EX[q] + (long)nx * EY[q] + plane * EZ[q];
@@ -633,6 +677,11 @@ void orc_lbm_d3q19(const orc_params *p, orc_state *s)
         long iz = i / plane, i2 = i;
         if (iz <= 1) i2 += shift;
         if (iz >= nz - 2) i2 -= shift;
+        if (p->flow == 1) {   /* lbm.cu:1316-1374: x BUFF columns too */
+            long ix = (i % plane) % nx;
+            if (ix <= 1) i2 += nx - 4;
+            if (ix >= nx - 2) i2 -= nx - 4;
+        }
         s->dn[i] = s->dn[i2]; s->un[i] = s->un[i2]; s->vn[i] = s->vn[i2]; s->wn[i] = s->wn[i2];
         s->dm[i] = s->dm[i2]; s->um[i] = s->um[i2]; s->vm[i] = s->vm[i2]; s->wm[i] = s->wm[i2];
     }
@@ -685,6 +734,10 @@ static void calc_center(const orc_params *p, orc_state *s)
         double sx = 0.0, sy = 0.0, sz = 0.0;
         for (int j = 0; j < V; j++) { sx += s->x[c*V + j]; sy += s->y[c*V + j]; sz += s->z[c*V + j]; }
         s->gx[3*c+0] = sx / (double)V; s->gx[3*c+1] = sy / (double)V; s->gx[3*c+2] = sz / (double)V;
+        if (p->flow == 1) {   /* volume_correction.cu:319-325 */
+            if (s->gx[3*c+0] < p->xmin) s->gx[3*c+0] += p->LX;
+            else if (s->gx[3*c+0] > p->xmax) s->gx[3*c+0] -= p->LX;
+        }
         if (s->gx[3*c+2] < p->zmin) s->gx[3*c+2] += p->LZ;
         else if (s->gx[3*c+2] > p->zmax) s->gx[3*c+2] -= p->LZ;
     }
@@ -716,6 +769,10 @@ int orc_volume_correction(const orc_params *p, orc_state *s)
             long id = (long)c * V + j;
             double dz = s->z[id] - s->gx[3*c+2];
             if (dz > p->LZ * 0.5) s->z[id] -= p->LZ; else if (dz < -p->LZ * 0.5) s->z[id] += p->LZ;
+            if (p->flow == 1) {   /* volume_correction.cu:48-57 */
+                double dxx = s->x[id] - s->gx[3*c+0];
+                if (dxx > p->LX * 0.5) s->x[id] -= p->LX; else if (dxx < -p->LX * 0.5) s->x[id] += p->LX;
+            }
         }
     int iter = 0, all_converged;
     do {
@@ -749,6 +806,10 @@ int orc_volume_correction(const orc_params *p, orc_state *s)
     calc_center(p, s);
     /* CapsulePeriodicAfter */
     for (long id = 0; id < nv; id++) {
+        if (p->flow == 1) {   /* volume_correction.cu:88-91 */
+            if (s->x[id] < p->xmin) s->x[id] += p->LX;
+            else if (s->x[id] > p->xmax) s->x[id] -= p->LX;
+        }
         if (s->z[id] < p->zmin) s->z[id] += p->LZ;
         else if (s->z[id] > p->zmax) s->z[id] -= p->LZ;
     }

@@ -52,6 +52,11 @@ typedef struct orc_params {
     /* cells */
     int ncell, vertex, element, mn;
     double br;           /* BR: bending modulus of fourpoint_bend (0 = no bending) */
+    /* flow mode: 0 = CapsuleCHANNELFLOW (z periodic, drive P), 1 = CapsuleSHEARFLOW
+     * (x and z periodic, y walls moving along z; init1.cu:133-187, lbm.cu:706-980) */
+    int flow;
+    double sr;           /* cdo->sr: shear rate (shear mode) */
+    int walls;           /* 0: allwall (walls at -/+ sr LY / 2), 1: topwall (top at sr LY) */
 } orc_params;
 
 typedef struct orc_state {
@@ -81,7 +86,8 @@ typedef struct orc_state {
 /* init2.cu:258-400 (fem_init): link tables and the reference metric from the
  * positions in s->xd.  Returns 0, or 3 as error(3) would. */
 int  orc_fem_init(const orc_params *p, orc_state *s);
-/* init1.cu:413-434 (flu_init): equilibrium at rho = 1, u = 0. */
+/* init1.cu:413-434 (flu_init): equilibrium at rho = 1, u = 0 (shear mode with
+ * FLOWSTART = 0: u = (0, 0, w(y)) of the walls' linear profile, init1.cu:367-381). */
 void orc_flu_init(const orc_params *p, orc_state *s);
 /* volume_correction.cu:427-450 (volume_init). */
 void orc_volume_init(const orc_params *p, orc_state *s);

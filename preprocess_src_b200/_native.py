@@ -15,6 +15,8 @@ RBC_OK, RBC_ERR_ARG, RBC_ERR_CUDA, RBC_ERR_UNSUPPORTED = 0, 1, 2, 3
 RBC_ERR_TOPOLOGY, RBC_ERR_NOT_CONVERGED, RBC_ERR_NONFINITE, RBC_ERR_STATE, RBC_ERR_NO_DEVICE = 4, 5, 6, 7, 8
 RBC_COMP, RBC_BUFF, RBC_WALL = 0, 1, 2
 RBC_STORE_F32, RBC_STORE_F16 = 0, 1
+RBC_FLOW_CHANNEL, RBC_FLOW_SHEAR = 0, 1
+RBC_WALLS_BOTH, RBC_WALLS_TOP = 0, 1
 RBC_NOALLOC_MAX_CELLS = 4096
 RBC_NUM_KERNELS = 6
 RBC_KERNEL_NAMES = ("step_begin", "membrane", "spread", "lbm_collide_stream", "advect", "volume")
@@ -29,7 +31,7 @@ class RbcParams(C.Structure):
                 ("zmin", C.c_double), ("zmax", C.c_double), ("C", C.c_double), ("rgs", C.c_double),
                 ("law", C.c_int), ("br", C.c_double), ("M", C.c_int), ("rk_order", C.c_int),
                 ("storage", C.c_int), ("membrane_fp64", C.c_int), ("solver_iters", C.c_int),
-                ("device", C.c_int)]
+                ("device", C.c_int), ("flow", C.c_int), ("sr", C.c_double), ("walls", C.c_int)]
 
 
 class RbcMesh(C.Structure):

@@ -80,13 +80,14 @@ def duct_bc(nx: int, ny: int, nz: int) -> np.ndarray:
 
 
 def base_params(nx: int, ny: int, nz: int, *, tau=1.0, g=1e-6, Gs=5e-4, C=100.0, br=0.0, storage=0,
-                membrane_fp64=0, solver_iters=0, residual=1e-13, itrmax=2000) -> dict:
+                membrane_fp64=0, solver_iters=0, residual=1e-13, itrmax=2000, flow=0, sr=0.0, walls=0,
+                flowstart=0) -> dict:
     LX, LZ = float(nx - 4), float(nz - 4)
     return dict(nx=nx, ny=ny, nz=nz, dx=1.0, dt=1.0, tau=float(tau), Cr=1.0, P=g / 2.0, B=Gs / 2.0,
-                flowstart=0, freq=math.inf, LX=LX, LZ=LZ, xmin=-LX / 2, xmax=LX / 2, zmin=-LZ / 2,
+                flowstart=int(flowstart), freq=math.inf, LX=LX, LZ=LZ, xmin=-LX / 2, xmax=LX / 2, zmin=-LZ / 2,
                 zmax=LZ / 2, C=float(C), rgs=1.0, law=0, br=float(br), M=1, rk_order=4, storage=storage,
                 membrane_fp64=membrane_fp64, solver_iters=solver_iters, residual=residual,
-                itrmax=itrmax, device=-1)
+                itrmax=itrmax, device=-1, flow=int(flow), sr=float(sr), walls=int(walls))
 
 
 def duct_to_ref(p, nx: int, ny: int, nz: int) -> np.ndarray:
@@ -148,6 +149,34 @@ def single_cell_duct(**kw) -> Case:
     kw.setdefault("seed", 1)
     return duct_case("single_cell_duct_64x32x32", 64, 32, 32, centers_duct=[(32.0, 16.0, 16.0)],
                      subdiv=3, steps=1000, **kw)
+
+
+def shear_bc(nx: int, ny: int, nz: int) -> np.ndarray:
+    """CapsuleSHEARFLOW box (init1.cu:133-187): COMP inside, BUFF in the two x
+    and z layers at each end between the walls, WALL in the two rows beyond
+    each y wall."""
+    bc = np.full((nz, ny, nx), WALL, dtype=np.int32)
+    bc[:, 2:ny - 2, :] = BUFF
+    bc[2:nz - 2, 2:ny - 2, 2:nx - 2] = COMP
+    return bc.reshape(-1)
+
+
+def shear_case(name: str, LX: int, LY: int, LZ: int, *, centers=(), sr=1e-3, walls=0, subdiv=3, radius=6.0,
+               seed=0, steps=1, **kw) -> Case:
+    """Shear flow (CapsuleSHEARFLOW): an LX x LY x LZ box periodic in x and z
+    between y walls moving along z at -/+ sr LY / 2 (walls = 0) or with the top
+    wall at sr LY (walls = 1); cells centred at the given reference-frame
+    positions (origin at the box centre)."""
+    nx, ny, nz = LX + 4, LY + 4, LZ + 4
+    kw.setdefault("g", 0.0)
+    params = base_params(nx, ny, nz, flow=1, sr=sr, walls=walls, **kw)
+    shape, tri = _mesh.rbc_shape(subdiv)
+    rng = np.random.default_rng(seed)
+    cells = [_mesh.place(shape, _mesh.random_rotation(rng), radius, np.asarray(c, dtype=np.float64)) for c in centers]
+    xr = np.concatenate(cells).reshape(-1) if cells else np.zeros(0)
+    return Case(name=name, params=params, bc=shear_bc(nx, ny, nz), tri=tri.astype(np.int32), xr=xr,
+                ncell=len(cells), vertex=len(shape), element=len(tri), steps=steps,
+                meta=dict(seed=seed, subdiv=subdiv, radius=radius, LX=LX, LY=LY, LZ=LZ, sr=sr, walls=walls))
 
 
 def capillary_batch(n: int = 512, seed: int = 4, lengths=tuple(range(48, 129, 16)), **kw) -> list:

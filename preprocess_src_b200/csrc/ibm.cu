@@ -44,6 +44,7 @@ __device__ __forceinline__ double unwrap_near(double l, double ref, int n) {
 // more CTAs than cells.  Box layout: x fastest, rows of bx, planes of ps >= bx*by
 // with ps = 8 (mod 32) so the four stencil planes of one vertex sit in
 // different shared-memory banks.
+template <bool XPER>
 __global__ void __launch_bounds__(SPREAD_THREADS)
 spread_kernel(const Geom g, const double *__restrict__ X, long long nv, int V,
               const int *__restrict__ patch_off, const int *__restrict__ patch_vtx,
@@ -60,6 +61,7 @@ spread_kernel(const Geom g, const double *__restrict__ X, long long nv, int V,
     const float *fxs = Fv + (long long)cell * V, *fys = Fv + nv + (long long)cell * V, *fzs = Fv + 2 * nv + (long long)cell * V;
     const float wscale = (float)(1.0 / (g.dx * g.dx * g.dx));   // 1/(64 dx^3) of ibm.cu:108 with the 1/4s in delta4
     const double az = lat_z(g, zs[0]);   // one anchor per cell: every patch unwraps z the same way
+    const double ax = lat_x(g, xs[0]);   // and x, when x is periodic (shear mode)
 
     if (tid < 3) { s_lo[tid] = INT_MAX; s_hi[tid] = INT_MIN; }
     if (tid < 3) s_fmax[tid] = 0u;
@@ -73,8 +75,9 @@ spread_kernel(const Geom g, const double *__restrict__ X, long long nv, int V,
         const float afx = fabsf(fxs[v]), afy = fabsf(fys[v]), afz = fabsf(fzs[v]);
         nonfinite |= !(afx <= FLT_MAX && afy <= FLT_MAX && afz <= FLT_MAX);
         fmax0 = fmaxf(fmax0, afx); fmax1 = fmaxf(fmax1, afy); fmax2 = fmaxf(fmax2, afz);
-        const double lxv = lat_x(g, xs[v]), lyv = lat_y(g, ys[v]), lzv = unwrap_near(lat_z(g, zs[v]), az, g.nzc);
-        if (!(sane_lattice(lxv) && sane_lattice(lyv) && sane_lattice(lzv) && sane_lattice(az))) { nonfinite = true; continue; }
+        const double lxr = lat_x(g, xs[v]), lxv = XPER ? unwrap_near(lxr, ax, g.nx) : lxr;
+        const double lyv = lat_y(g, ys[v]), lzv = unwrap_near(lat_z(g, zs[v]), az, g.nzc);
+        if (!(sane_lattice(lxv) && sane_lattice(lyv) && sane_lattice(lzv) && sane_lattice(az) && sane_lattice(ax))) { nonfinite = true; continue; }
         const int ix = (int)floor(lxv), iy = (int)floor(lyv);
         const int iz = (int)floor(lzv);
         lo0 = min(lo0, ix - 1); hi0 = max(hi0, ix + 2);
@@ -122,7 +125,8 @@ spread_kernel(const Geom g, const double *__restrict__ X, long long nv, int V,
         __syncthreads();
         for (int k = tid; k < np; k += SPREAD_THREADS) {
             const int v = patch_vtx[p0 + k];
-            const int ix = (int)floor(lat_x(g, xs[v])), iy = (int)floor(lat_y(g, ys[v]));
+            const double lxr = lat_x(g, xs[v]);
+            const int ix = (int)floor(XPER ? unwrap_near(lxr, ax, g.nx) : lxr), iy = (int)floor(lat_y(g, ys[v]));
             const int iz = (int)floor(unwrap_near(lat_z(g, zs[v]), az, g.nzc));
             const int li0 = (ix - 1 - bx0) + bx * (iy - 1 - by0) + psi * (iz - bz0);
 #pragma unroll
@@ -171,7 +175,8 @@ spread_kernel(const Geom g, const double *__restrict__ X, long long nv, int V,
         const int v = patch_vtx[p0 + jv];
         jv += vstep;
         if (jv >= np) jv -= np;
-        const double lx = lat_x(g, xs[v]), ly = lat_y(g, ys[v]);
+        const double lxr = lat_x(g, xs[v]), lx = XPER ? unwrap_near(lxr, ax, g.nx) : lxr, ly = lat_y(g, ys[v]);
+        const int xsh = XPER ? (int)lrint(lx - lxr) : 0;   // unwrapped minus raw frame
         const double lzr = lat_z(g, zs[v]);
         const double lz = unwrap_near(lzr, az, g.nzc);
         const double flx = floor(lx), fly = floor(ly), flz = floor(lz);
@@ -196,15 +201,20 @@ spread_kernel(const Geom g, const double *__restrict__ X, long long nv, int V,
 #pragma unroll
             for (int a = 0; a < 4; a++) {
                 const int gx = ix0 + a;
-                if (gx < 0 || gx >= g.nx) continue;
+                // x: outside the lattice; periodic (shear mode): nodes beyond the two BUFF
+                // columns of the vertex's raw frame are dropped as ibm.cu:107-110 drops them,
+                // the rest fold periodically (ibm.cu:239-294)
+                if (!XPER && (gx < 0 || gx >= g.nx)) continue;
+                if (XPER && (gx - xsh < -g.xb || gx - xsh >= g.nx + g.xb)) continue;
                 const float w = wx[a] * wyb;
+                const int gxw = XPER ? wrap_x(gx, g.nx) : gx;
                 if (use_box) {
                     const int li = (gx - bx0) + bx * (gy - by0) + zoff;
                     atomicAdd(&sbox[li], (unsigned)__float2int_rn(w * q0));
                     atomicAdd(&sbox[nbi + li], (unsigned)__float2int_rn(w * q1));
                     atomicAdd(&sbox[2 * nbi + li], (unsigned)__float2int_rn(w * q2));
-                } else if (__ldg(&mask2d[gx + g.nx * gy]) & MASK_FLUID) {
-                    const long long gi = (long long)wrap_z(iz, g.nzc) * g.plane + gx + (long long)g.nx * gy;
+                } else if (__ldg(&mask2d[gxw + g.nx * gy]) & MASK_FLUID) {
+                    const long long gi = (long long)wrap_z(iz, g.nzc) * g.plane + gxw + (long long)g.nx * gy;
                     atomicAdd(&Fx[gi], w * f0);
                     atomicAdd(&Fy[gi], w * f1);
                     atomicAdd(&Fz[gi], w * f2);
@@ -221,7 +231,7 @@ spread_kernel(const Geom g, const double *__restrict__ X, long long nv, int V,
         const int ia = (int)sbox[li], ib = (int)sbox[nbi + li], ic = (int)sbox[2 * nbi + li];
         if ((ia | ib | ic) == 0) continue;
         const int ly = r / bx, lx = r - ly * bx;
-        const int gx = bx0 + lx, gy = by0 + ly;
+        const int gx = XPER ? wrap_x(bx0 + lx, g.nx) : bx0 + lx, gy = by0 + ly;
         if (gx < 0 || gx >= g.nx || gy < 0 || gy >= g.ny) continue;   // never written; kept as a guard
         if (!(__ldg(&mask2d[gx + g.nx * gy]) & MASK_FLUID)) continue;   // wall column: the LBM never reads it
         const long long gi = (long long)wrap_z(bz0 + lz, g.nzc) * g.plane + gx + (long long)g.nx * gy;
@@ -234,13 +244,16 @@ spread_kernel(const Geom g, const double *__restrict__ X, long long nv, int V,
 
 cudaError_t spread_setup()
 {
-    return cudaFuncSetAttribute(spread_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SPREAD_SMEM);
+    cudaError_t e = cudaFuncSetAttribute(spread_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, SPREAD_SMEM);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(spread_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SPREAD_SMEM);
 }
 
 void launch_spread(const Geom &g, const SpreadArgs &a, cudaStream_t s)
 {
     if (a.ncell <= 0) return;
-    spread_kernel<<<a.ncell * a.npatch, SPREAD_THREADS, SPREAD_SMEM, s>>>(
+    auto k = g.xper ? spread_kernel<true> : spread_kernel<false>;
+    k<<<a.ncell * a.npatch, SPREAD_THREADS, SPREAD_SMEM, s>>>(
         g, a.X, a.nv, a.V, a.patch_off, a.patch_vtx, a.patch_stride, a.npatch, a.Fv, a.Fx, a.Fy, a.Fz, a.mask2d,
         a.flags);
 }
@@ -256,8 +269,10 @@ struct Plane16 {
     float u[16], v[16], w[16];
 };
 
+// xm: bit a = stencil column a is inside the reference lattice (x periodic:
+// within the two BUFF columns of the vertex's raw frame, ibm.cu:453-455)
 __device__ __forceinline__ void gather_plane(const Geom &g, const float4 *__restrict__ uvr, int ix0, int iy0, int iz,
-                                             Plane16 &P)
+                                             unsigned xm, Plane16 &P)
 {
     const bool zin = iz >= -2 && iz < g.nzc + 2;   // beyond the BUFF planes (ibm.cu:453-455)
     const long long zb = (long long)wrap_z(iz, g.nzc) * g.plane;
@@ -268,7 +283,9 @@ __device__ __forceinline__ void gather_plane(const Geom &g, const float4 *__rest
         for (int a = 0; a < 4; a++) {
             const int gx = ix0 + a;
             float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (zin && gy >= 0 && gy < g.ny && gx >= 0 && gx < g.nx) q = __ldg(&uvr[zb + gx + (long long)g.nx * gy]);
+            const int gxw = g.xper ? wrap_x(gx, g.nx) : gx;
+            if (zin && ((xm >> a) & 1u) && gy >= 0 && gy < g.ny && gxw >= 0 && gxw < g.nx)
+                q = __ldg(&uvr[zb + gxw + (long long)g.nx * gy]);
             P.u[4 * b + a] = q.x; P.v[4 * b + a] = q.y; P.w[4 * b + a] = q.z;
         }
     }
@@ -315,7 +332,7 @@ constexpr int ADVECT_SMEM = ADVECT_BOX_BYTES + ADVECT_MAX_PATCH * (3 * (int)size
 // when the plane is not inside the box (the caller then gathers from global
 // memory).  (xi, yi, zi) = stencil corner relative to the box origin.
 __device__ __forceinline__ bool box_plane(const float4 *box, int bxs, int bys, int bzs, int xi, int yi, int zi,
-                                          bool zin, Plane16 &P)
+                                          bool zin, unsigned xm, Plane16 &P)
 {
     if (xi < 0 || xi + 3 >= bxs || yi < 0 || yi + 3 >= bys || zi < 0 || zi >= bzs) return false;
     const float4 *row = box + ((long long)zi * bys + yi) * bxs + xi;
@@ -323,7 +340,7 @@ __device__ __forceinline__ bool box_plane(const float4 *box, int bxs, int bys, i
     for (int b = 0; b < 4; b++)
 #pragma unroll
         for (int a = 0; a < 4; a++) {
-            const float4 q = zin ? row[b * bxs + a] : make_float4(0.f, 0.f, 0.f, 0.f);
+            const float4 q = (zin && ((xm >> a) & 1u)) ? row[b * bxs + a] : make_float4(0.f, 0.f, 0.f, 0.f);
             P.u[4 * b + a] = q.x; P.v[4 * b + a] = q.y; P.w[4 * b + a] = q.z;
         }
     return true;
@@ -338,6 +355,7 @@ __device__ __forceinline__ bool box_plane(const float4 *box, int bxs, int bys, i
 // of the vertex's own (unwrapped) frame are dropped per vertex as
 // ibm.cu:453-455 does.  A box larger than ADVECT_SMEM, or a later-stage
 // stencil outside the box, gathers from global memory instead.
+template <bool XPER>
 __global__ void __launch_bounds__(ADVECT_THREADS)
 advect_kernel(const Geom g, double *__restrict__ X, double *__restrict__ Xd, float *__restrict__ U,
               const float4 *__restrict__ uvr, long long nv, int V, const int *__restrict__ patch_off,
@@ -352,6 +370,7 @@ advect_kernel(const Geom g, double *__restrict__ X, double *__restrict__ Xd, flo
     const long long vb = (long long)cell * V;
     const double *xs = X + vb, *ys = X + nv + vb, *zs = X + 2 * nv + vb;
     const double az = lat_z(g, zs[0]);   // one anchor per cell: every patch unwraps z the same way
+    const double ax = lat_x(g, xs[0]);   // and x, when x is periodic (shear mode)
 
     if (tid < 3) { s_lo[tid] = INT_MAX; s_hi[tid] = INT_MIN; }
     __syncthreads();
@@ -361,8 +380,9 @@ advect_kernel(const Geom g, double *__restrict__ X, double *__restrict__ Xd, flo
         const int v = patch_vtx[p0 + k];
         const double px = xs[v], py = ys[v], pz = zs[v];
         svid[k] = v; spos[k] = px; spos[ADVECT_MAX_PATCH + k] = py; spos[2 * ADVECT_MAX_PATCH + k] = pz;
-        const double lxv = lat_x(g, px), lyv = lat_y(g, py), lzv = unwrap_near(lat_z(g, pz), az, g.nzc);
-        if (!(sane_lattice(lxv) && sane_lattice(lyv) && sane_lattice(lzv) && sane_lattice(az))) { bad = true; continue; }
+        const double lxr = lat_x(g, px), lxv = XPER ? unwrap_near(lxr, ax, g.nx) : lxr;
+        const double lyv = lat_y(g, py), lzv = unwrap_near(lat_z(g, pz), az, g.nzc);
+        if (!(sane_lattice(lxv) && sane_lattice(lyv) && sane_lattice(lzv) && sane_lattice(az) && sane_lattice(ax))) { bad = true; continue; }
         const int ix = (int)floor(lxv), iy = (int)floor(lyv);
         const int iz = (int)floor(lzv);
         lo0 = min(lo0, ix - 2); hi0 = max(hi0, ix + 3);
@@ -385,7 +405,7 @@ advect_kernel(const Geom g, double *__restrict__ X, double *__restrict__ Xd, flo
         int x = tid % bxs, y = (tid / bxs) % bys, z = tid / (bxs * bys);
         const int sx = ADVECT_THREADS % bxs, sy = (ADVECT_THREADS / bxs) % bys, sz = ADVECT_THREADS / (bxs * bys);
         for (int li = tid; li < nb; li += ADVECT_THREADS) {
-            const int gx = bx0 + x, gy = by0 + y;
+            const int gx = XPER ? wrap_x(bx0 + x, g.nx) : bx0 + x, gy = by0 + y;
             float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
             if (gx >= 0 && gx < g.nx && gy >= 0 && gy < g.ny)
                 q = __ldg(&uvr[(long long)wrap_z(bz0 + z, g.nzc) * g.plane + gx + (long long)g.nx * gy]);
@@ -411,14 +431,22 @@ advect_kernel(const Geom g, double *__restrict__ X, double *__restrict__ Xd, flo
         int bx, by, bz;
         float fx, fy, fz, wx[4], wy[4], wz[4];
         lattice_cell(g, xn, yn, zn, bx, by, bz, fx, fy, fz);
-        // shift from the raw z frame to the cell's unwrapped frame (a multiple of nzc)
+        // shift from the raw z (and, periodic, x) frame to the cell's unwrapped frame
         const double lzr = lat_z(g, zn);
         const int zsh = (int)lrint(unwrap_near(lzr, az, g.nzc) - lzr);
+        const double lxr = lat_x(g, xn);
+        const int xsh = XPER ? (int)lrint(unwrap_near(lxr, ax, g.nx) - lxr) : 0;
         auto fetch = [&](int cx, int cy, int cz) {
             const int izr = cz + c;
             const bool zin = izr >= -2 && izr < g.nzc + 2;   // beyond the BUFF planes (ibm.cu:453-455)
-            if (!use_box || !box_plane(abox, bxs, bys, bzs, cx - bx0, cy - by0, izr + zsh - bz0, zin, P))
-                gather_plane(g, uvr, cx, cy, izr, P);
+            unsigned xm = 0xFu;
+            if (XPER) {   // the same rule for the x BUFF columns (cx: raw frame)
+                xm = 0u;
+#pragma unroll
+                for (int a = 0; a < 4; a++) xm |= (cx + a >= -g.xb && cx + a < g.nx + g.xb) ? (1u << a) : 0u;
+            }
+            if (!use_box || !box_plane(abox, bxs, bys, bzs, cx + xsh - bx0, cy - by0, izr + zsh - bz0, zin, xm, P))
+                gather_plane(g, uvr, cx, cy, izr, xm, P);
         };
         fetch(bx, by, bz);
         float us[4], vs[4], ws[4];
@@ -457,13 +485,16 @@ advect_kernel(const Geom g, double *__restrict__ X, double *__restrict__ Xd, flo
 
 cudaError_t advect_setup()
 {
-    return cudaFuncSetAttribute(advect_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, ADVECT_SMEM);
+    cudaError_t e = cudaFuncSetAttribute(advect_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, ADVECT_SMEM);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(advect_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, ADVECT_SMEM);
 }
 
 void launch_advect(const Geom &g, const AdvectArgs &a, cudaStream_t s)
 {
     if (a.ncell <= 0) return;
-    advect_kernel<<<a.ncell * a.npatch, ADVECT_THREADS, ADVECT_SMEM, s>>>(
+    auto k = g.xper ? advect_kernel<true> : advect_kernel<false>;
+    k<<<a.ncell * a.npatch, ADVECT_THREADS, ADVECT_SMEM, s>>>(
         g, a.X, a.Xd, a.U, a.uvr, a.nv, a.V, a.patch_off, a.patch_vtx, a.npatch, a.dtM, a.flags);
 }
 

@@ -124,7 +124,7 @@ lbm_collide_stream(const typename Store<STORE>::T *__restrict__ gin, typename St
                    float4 *__restrict__ uvr,
                    float *__restrict__ Fx, float *__restrict__ Fy, float *__restrict__ Fz,
                    const uint32_t *__restrict__ mask2d, const float *__restrict__ drive,
-                   int nx, int ny, int nzc, I nint,
+                   const float *__restrict__ wall, int nx, int ny, int nzc, I nint,
                    float omega, float Cr, float Bc, float scale, float inv_scale)
 {
     using S = Store<STORE>;
@@ -154,9 +154,23 @@ lbm_collide_stream(const typename Store<STORE>::T *__restrict__ gin, typename St
         } else {
 #pragma unroll
             for (int q = 0; q < Q; q++) {
-                const I pull = (I)q * nint + ((ez(q) == 1) ? dzm : (ez(q) == -1) ? dzp : (I)0) - ex(q) - nx * ey(q);
+                // a periodic x (shear mode) wraps the pull of the first and last column
+                const I xw = (ex(q) == 1 && (m & MASK_XLO)) ? (I)nx : (ex(q) == -1 && (m & MASK_XHI)) ? -(I)nx : (I)0;
+                const I pull = (I)q * nint + ((ez(q) == 1) ? dzm : (ez(q) == -1) ? dzp : (I)0) - ex(q) - nx * ey(q) + xw;
                 const bool bb = (m >> q) & 1u;   // i - e_q is a wall: half-way bounce-back of f*_{opp q}(i)
                 g[q] = fluid ? S::ld(gb + (bb ? (I)opp(q) * nint : pull), inv_scale) : 0.f;
+            }
+            if (fluid && (m & (MASK_TOPW | MASK_BOTW))) {
+                // moving wall (shear mode, lbm.cu:946-964): the bounced population gains
+                // 6 w_q rho Cr (e_q . u_w), rho = the node's density of the previous collision
+                // = 1 + the sum of its own post-collision slots (the collision conserves it)
+                float rho = 1.0f;
+#pragma unroll
+                for (int q = 0; q < Q; q++) rho += S::ld(gb + (I)q * nint, inv_scale);
+                const float uw = __ldg(&wall[(m & MASK_TOPW) ? 0 : 1]);
+#pragma unroll
+                for (int q = 0; q < Q; q++)
+                    if (ez(q) != 0 && ((m >> q) & 1u)) g[q] += 6.0f * wq(q) * rho * Cr * (float)ez(q) * uw;
             }
             collide_store<STORE, false, I>(g, fluid, idx, nint, gout, uvr, Fx, Fy, Fz, pd, omega, om1, Cr, Bc, scale);
         }
@@ -169,7 +183,7 @@ void launch_lbm(const Geom &g, int storage, const LbmArgs &a, cudaStream_t s)
     const bool off32 = (long long)Q * g.nint < (1LL << 31);   // every element offset fits in an int
 #define LBM_LAUNCH(ST, I)                                                                                     \
     lbm_collide_stream<ST, I><<<blocks, LBM_THREADS, 0, s>>>(                                                 \
-        (const Store<ST>::T *)a.gin, (Store<ST>::T *)a.gout, a.uvr, a.Fx, a.Fy, a.Fz, a.mask2d, a.drive, g.nx, \
+        (const Store<ST>::T *)a.gin, (Store<ST>::T *)a.gout, a.uvr, a.Fx, a.Fy, a.Fz, a.mask2d, a.drive, a.wall, g.nx, \
         g.ny, g.nzc, (I)g.nint, a.omega, a.Cr, a.Bc, a.scale, a.inv_scale)
     if (storage == RBC_STORE_F16) {
         if (off32) LBM_LAUNCH(RBC_STORE_F16, int); else LBM_LAUNCH(RBC_STORE_F16, long long);
@@ -181,16 +195,28 @@ void launch_lbm(const Geom &g, int storage, const LbmArgs &a, cudaStream_t s)
 
 // ---- reference layout <-> internal layout ---------------------------------
 
+// reference-layout index of internal node (x, y, z) (x and z without the BUFF layers)
 __device__ __forceinline__ long long ref_index(const Geom &g, int x, int y, int z) {
-    return (long long)x + (long long)g.nx * (y + (long long)g.ny * (z + 2));
+    return (long long)(x + g.xb) + (long long)g.nxr * (y + (long long)g.ny * (z + 2));
+}
+__device__ __forceinline__ int nb_x(const Geom &g, int x, int d) { return g.xper ? wrap_x(x + d, g.nx) : x + d; }
+
+// The moving-wall term of a bounced population in direction q at a node of
+// density rho (shear mode, lbm.cu:946-964): 6 w_q rho Cr (e_q . u_w), u_w along z.
+__device__ __forceinline__ double wall_term(int q, uint32_t m, double rho, const WallVel &w) {
+    const double uw = (m & MASK_TOPW) ? w.top : (m & MASK_BOTW) ? w.bot : 0.0;
+    return 6.0 * wqd(q) * rho * w.Cr * (double)ez(q) * uw;
 }
 
 // Reference fn (pre-collision, AoS FP64) -> internal post-collision g*:
 // f*_q(i) = fn[i + e_q][q] when i + e_q is fluid, else fn[i][opp q]
-// (inverse of the push of lbm.cu:1272-1310).
+// (inverse of the push of lbm.cu:1272-1310).  At a moving wall the bounced
+// value excludes the wall term the next step's pull adds (w: the walls'
+// velocities in that step; rho = 1 + the sum of the node's slots, which the
+// terms leave unchanged since the two linked directions have opposite e_z).
 template <int STORE>
 __global__ void import_lattice_kernel(const Geom g, const double *__restrict__ fn, typename Store<STORE>::T *__restrict__ gout,
-                                      const uint32_t *__restrict__ mask2d, float scale)
+                                      const uint32_t *__restrict__ mask2d, float scale, const WallVel w)
 {
     using S = Store<STORE>;
     const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -199,17 +225,25 @@ __global__ void import_lattice_kernel(const Geom g, const double *__restrict__ f
     const int xy = (int)(idx - (long long)z * g.plane);
     const int y = xy / g.nx, x = xy - y * g.nx;
     const uint32_t m = mask2d[xy];
+    double val[Q];
+    double rho = 1.0;
 #pragma unroll
     for (int q = 0; q < Q; q++) {
-        float val = 0.f;
+        val[q] = 0.0;
         if (m & MASK_FLUID) {
             double f;
             if ((m >> opp(q)) & 1u) f = fn[ref_index(g, x, y, z) * Q + opp(q)];
-            else f = fn[ref_index(g, x + ex(q), y + ey(q), wrap_z(z + ez(q), g.nzc)) * Q + q];
-            val = (float)(f - wqd(q));
+            else f = fn[ref_index(g, nb_x(g, x, ex(q)), y + ey(q), wrap_z(z + ez(q), g.nzc)) * Q + q];
+            val[q] = f - wqd(q);
+            rho += val[q];
         }
-        S::st(gout + (long long)q * g.nint + idx, val, scale);
     }
+    if ((m & MASK_FLUID) && (m & (MASK_TOPW | MASK_BOTW)))
+#pragma unroll
+        for (int q = 0; q < Q; q++)
+            if ((m >> opp(q)) & 1u) val[q] -= wall_term(opp(q), m, rho, w);
+#pragma unroll
+    for (int q = 0; q < Q; q++) S::st(gout + (long long)q * g.nint + idx, (float)val[q], scale);
 }
 
 // Internal g* -> reference pre-collision fn (the pull of the LBM kernel without
@@ -220,18 +254,28 @@ template <int STORE>
 __global__ void export_lattice_kernel(const Geom g, const typename Store<STORE>::T *__restrict__ gin,
                                       const uint32_t *__restrict__ mask2d, const float4 *__restrict__ uvr,
                                       float inv_scale, double *__restrict__ fn, double *__restrict__ dn,
-                                      double *__restrict__ un, double *__restrict__ vn, double *__restrict__ wn)
+                                      double *__restrict__ un, double *__restrict__ vn, double *__restrict__ wn,
+                                      const WallVel w)
 {
     using S = Store<STORE>;
-    const long long nref = g.plane * g.nzr;
+    const long long pref = (long long)g.nxr * g.ny, nref = pref * g.nzr;
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nref) return;
-    const int zr = (int)(i / g.plane);
-    const int xy = (int)(i - (long long)zr * g.plane);
-    const int y = xy / g.nx, x = xy - y * g.nx;
+    const int zr = (int)(i / pref);
+    const int xyr = (int)(i - (long long)zr * pref);
+    const int y = xyr / g.nxr, xr = xyr - y * g.nxr;
+    // internal column; x BUFF columns (shear mode) are periodic images
+    const int x = g.xper ? wrap_x(xr - g.xb, g.nx) : xr;
+    const int xy = x + g.nx * y;
     const uint32_t m = mask2d[xy];
-    const bool comp = (m & MASK_FLUID) && zr >= 2 && zr < g.nzr - 2;
+    const bool comp = (m & MASK_FLUID) && zr >= 2 && zr < g.nzr - 2 && xr >= g.xb && xr < g.nxr - g.xb;
     if (fn) {
+        const bool moving = comp && (m & (MASK_TOPW | MASK_BOTW));
+        double rho = 1.0;   // the node's density: 1 + the sum of its own slots
+        if (moving) {
+            const long long idx = (long long)(zr - 2) * g.plane + xy;
+            for (int q = 0; q < Q; q++) rho += S::ld(gin + (long long)q * g.nint + idx, inv_scale);
+        }
 #pragma unroll
         for (int q = 0; q < Q; q++) {
             double f = 0.0;
@@ -239,12 +283,14 @@ __global__ void export_lattice_kernel(const Geom g, const typename Store<STORE>:
                 const int z = zr - 2;
                 const long long idx = (long long)z * g.plane + xy;
                 float gv;
-                if ((m >> q) & 1u) gv = S::ld(gin + (long long)opp(q) * g.nint + idx, inv_scale);
-                else {
-                    const long long src = (long long)wrap_z(z - ez(q), g.nzc) * g.plane + (x - ex(q)) + (long long)g.nx * (y - ey(q));
+                if ((m >> q) & 1u) {
+                    gv = S::ld(gin + (long long)opp(q) * g.nint + idx, inv_scale);
+                    if (moving) f += wall_term(q, m, rho, w);
+                } else {
+                    const long long src = (long long)wrap_z(z - ez(q), g.nzc) * g.plane + nb_x(g, x, -ex(q)) + (long long)g.nx * (y - ey(q));
                     gv = S::ld(gin + (long long)q * g.nint + src, inv_scale);
                 }
-                f = (double)gv + wqd(q);
+                f += (double)gv + wqd(q);
             }
             fn[i * Q + q] = f;
         }
@@ -264,13 +310,15 @@ __global__ void export_force_kernel(const Geom g, const float *__restrict__ Fx, 
                                     const float *__restrict__ Fz, const uint32_t *__restrict__ mask2d,
                                     double *__restrict__ out)
 {
-    const long long nref = g.plane * g.nzr;
+    const long long pref = (long long)g.nxr * g.ny, nref = pref * g.nzr;
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nref) return;
-    const int zr = (int)(i / g.plane);
-    const int xy = (int)(i - (long long)zr * g.plane);
+    const int zr = (int)(i / pref);
+    const int xyr = (int)(i - (long long)zr * pref);
+    const int y = xyr / g.nxr, xr = xyr - y * g.nxr;
+    const int xy = (xr - g.xb) + g.nx * y;
     double a = 0.0, b = 0.0, c = 0.0;
-    if ((mask2d[xy] & MASK_FLUID) && zr >= 2 && zr < g.nzr - 2) {
+    if (xr >= g.xb && xr < g.nxr - g.xb && (mask2d[xy] & MASK_FLUID) && zr >= 2 && zr < g.nzr - 2) {
         const long long idx = (long long)(zr - 2) * g.plane + xy;
         a = Fx[idx]; b = Fy[idx]; c = Fz[idx];
     }
@@ -296,33 +344,33 @@ void launch_fill_f4(float4 *p, long long n, float4 v, cudaStream_t s)
 }
 
 void launch_import_lattice(const Geom &g, int storage, const double *fn_ref, void *gout,
-                           const uint32_t *mask2d, float scale, cudaStream_t s)
+                           const uint32_t *mask2d, float scale, const WallVel &w, cudaStream_t s)
 {
     const unsigned blocks = (unsigned)((g.nint + 255) / 256);
     if (storage == RBC_STORE_F16)
-        import_lattice_kernel<RBC_STORE_F16><<<blocks, 256, 0, s>>>(g, fn_ref, (__half *)gout, mask2d, scale);
+        import_lattice_kernel<RBC_STORE_F16><<<blocks, 256, 0, s>>>(g, fn_ref, (__half *)gout, mask2d, scale, w);
     else
-        import_lattice_kernel<RBC_STORE_F32><<<blocks, 256, 0, s>>>(g, fn_ref, (float *)gout, mask2d, scale);
+        import_lattice_kernel<RBC_STORE_F32><<<blocks, 256, 0, s>>>(g, fn_ref, (float *)gout, mask2d, scale, w);
 }
 
 void launch_export_lattice(const Geom &g, int storage, const void *gin, const uint32_t *mask2d,
                            const float4 *uvr, float inv_scale, double *fn_ref, double *dn, double *un,
-                           double *vn, double *wn, cudaStream_t s)
+                           double *vn, double *wn, const WallVel &w, cudaStream_t s)
 {
-    const long long nref = g.plane * g.nzr;
+    const long long nref = (long long)g.nxr * g.ny * g.nzr;
     const unsigned blocks = (unsigned)((nref + 255) / 256);
     if (storage == RBC_STORE_F16)
         export_lattice_kernel<RBC_STORE_F16><<<blocks, 256, 0, s>>>(g, (const __half *)gin, mask2d, uvr,
-                                                                     inv_scale, fn_ref, dn, un, vn, wn);
+                                                                     inv_scale, fn_ref, dn, un, vn, wn, w);
     else
         export_lattice_kernel<RBC_STORE_F32><<<blocks, 256, 0, s>>>(g, (const float *)gin, mask2d, uvr,
-                                                                     inv_scale, fn_ref, dn, un, vn, wn);
+                                                                     inv_scale, fn_ref, dn, un, vn, wn, w);
 }
 
 void launch_export_force(const Geom &g, const float *Fx, const float *Fy, const float *Fz,
                          const uint32_t *mask2d, double *out3, cudaStream_t s)
 {
-    const long long nref = g.plane * g.nzr;
+    const long long nref = (long long)g.nxr * g.ny * g.nzr;
     export_force_kernel<<<(unsigned)((nref + 255) / 256), 256, 0, s>>>(g, Fx, Fy, Fz, mask2d, out3);
 }
 

@@ -62,7 +62,7 @@ struct rbc_handle {
     double *vol0 = nullptr, *gx = nullptr, *vol_out = nullptr, *area_out = nullptr, *cen_out = nullptr;
     // device scalars: iter, flags, vc_max, vc_last
     int *d_int = nullptr;
-    float *d_drive = nullptr;
+    float *d_drive = nullptr;                          // [3]: drive P * factor, then the walls' z velocities
     // host<->reference staging
     void *staging = nullptr;
     size_t staging_bytes = 0;
@@ -144,10 +144,37 @@ int ensure_staging(rbc_handle *h, size_t bytes)
     return RBC_OK;
 }
 
+// the step-begin arguments of the handle (the adjoint adds where to keep the drive)
+StepBeginArgs step_begin_args(rbc_handle *h);
+WallVel wall_velocities(const rbc_handle *h, int step);
+
 double drive_factor(const rbc_params &p, int iter)
 {
     // lbm.cu:1030-1035
     return (iter > p.flowstart) ? 1.0 + 0.5 * std::sin(M_PI * p.dt * (double)iter / p.freq) : 0.0;
+}
+
+StepBeginArgs step_begin_args(rbc_handle *h)
+{
+    StepBeginArgs a{};
+    a.iter = h->d_iter(); a.drive = h->d_drive;
+    a.P = h->p.P; a.freq = h->p.freq; a.dt = h->p.dt; a.flowstart = h->p.flowstart;
+    if (h->p.flow == RBC_FLOW_SHEAR) {
+        a.wall = h->d_drive + 1;
+        a.sr = h->p.sr; a.LY = (double)(h->p.ny - 4) * h->p.dx; a.walls = h->p.walls;
+    }
+    return a;
+}
+
+// the walls' z velocities in step `step` as step_begin_kernel sets them (lbm.cu:752, 946-964)
+WallVel wall_velocities(const rbc_handle *h, int step)
+{
+    WallVel w{0.0, 0.0, h->p.Cr};
+    if (h->p.flow != RBC_FLOW_SHEAR) return w;
+    const double sra = step < h->p.flowstart ? 0.0 : h->p.sr, LY = (double)(h->p.ny - 4) * h->p.dx;
+    w.top = (double)(float)(h->p.walls == RBC_WALLS_BOTH ? sra * LY / 2.0 : sra * LY);
+    w.bot = (double)(float)(h->p.walls == RBC_WALLS_BOTH ? -sra * LY / 2.0 : 0.0);
+    return w;
 }
 
 // Link tables of the shared local connectivity (init2.cu:258-400): neighbour
@@ -249,6 +276,7 @@ void initial_volume(const rbc_handle *h, const int *tri, const double *xr, std::
             for (int k = 0; k < 3; k++) s[k] += xr[3 * ((long long)c * V + j) + k];
         for (int k = 0; k < 3; k++) s[k] /= (double)V;
         if (s[2] < h->p.zmin) s[2] += h->p.LZ; else if (s[2] > h->p.zmax) s[2] -= h->p.LZ;
+        if (h->p.flow == RBC_FLOW_SHEAR) { if (s[0] < h->p.xmin) s[0] += h->p.LX; else if (s[0] > h->p.xmax) s[0] -= h->p.LX; }
         gx[c] = s[0]; gx[N + c] = s[1]; gx[2 * N + c] = s[2];
     }
 }
@@ -336,12 +364,53 @@ int check_params(const rbc_params *p)
     if (p->storage != RBC_STORE_F32 && p->storage != RBC_STORE_F16) return fail(nullptr, RBC_ERR_ARG, "unknown storage");
     if (p->law != RBC_LAW_SKALAK && p->law != RBC_LAW_NEOHOOKEAN) return fail(nullptr, RBC_ERR_ARG, "unknown law");
     if (p->solver_iters < 0 || p->solver_iters > 200) return fail(nullptr, RBC_ERR_ARG, "solver_iters out of range");
+    if (p->flow != RBC_FLOW_CHANNEL && p->flow != RBC_FLOW_SHEAR) return fail(nullptr, RBC_ERR_ARG, "unknown flow mode");
+    if (p->flow == RBC_FLOW_SHEAR) {
+        if (p->walls != RBC_WALLS_BOTH && p->walls != RBC_WALLS_TOP) return fail(nullptr, RBC_ERR_ARG, "unknown wall motion");
+        if (!std::isfinite(p->sr)) return fail(nullptr, RBC_ERR_ARG, "shear rate must be finite");
+        if (p->P != 0.0) return fail(nullptr, RBC_ERR_ARG, "the shear mode has no body-force drive (P must be 0, lbm.cu:706-980)");
+        if (p->nx < 8 || p->ny < 6) return fail(nullptr, RBC_ERR_ARG, "shear mode: nx >= 8 (4 periodic columns + 4 BUFF), ny >= 6");
+    }
+    return RBC_OK;
+}
+
+// Shear mode (CapsuleSHEARFLOW, init1.cu:133-187): the bc map must be COMP inside
+// the box, BUFF in the two x and z layers of each end between the walls and WALL
+// in the two rows beyond each y wall.  The internal columns are the periodic x
+// range (BUFF columns stripped); fluid rows are y = 2 .. ny - 3, the walls are
+// half a node beyond them and move along z.
+int build_mask_shear(const rbc_params *p, const int *bc, std::vector<uint32_t> &mask)
+{
+    const int nx = p->nx, ny = p->ny, nz = p->nz, nxi = nx - 4;
+    for (int z = 0; z < nz; z++)
+        for (int y = 0; y < ny; y++)
+            for (int x = 0; x < nx; x++) {
+                const bool rowf = y >= 2 && y < ny - 2, inx = x >= 2 && x < nx - 2, inz = z >= 2 && z < nz - 2;
+                const int want = !rowf ? RBC_WALL : (inx && inz) ? RBC_COMP : RBC_BUFF;
+                if (bc[((long long)z * ny + y) * nx + x] != want)
+                    return fail(nullptr, RBC_ERR_ARG, "bc: not the shear-flow box (COMP inside, BUFF x/z layers, WALL rows beyond y)");
+            }
+    mask.assign((size_t)nxi * ny, 0u);
+    for (int y = 2; y < ny - 2; y++)
+        for (int x = 0; x < nxi; x++) {
+            uint32_t m = MASK_FLUID;
+            for (int q = 1; q < Q; q++) {
+                const int sy = y - ey(q);
+                if (sy < 2 || sy >= ny - 2) m |= (1u << q);
+            }
+            if (x == 0) m |= MASK_XLO;
+            if (x == nxi - 1) m |= MASK_XHI;
+            if (y == ny - 3) m |= MASK_TOPW;
+            else if (y == 2) m |= MASK_BOTW;
+            mask[(size_t)y * nxi + x] = m;
+        }
     return RBC_OK;
 }
 
 // Wall mask of one z plane from the reference bc map; checks z invariance.
 int build_mask(const rbc_params *p, const int *bc, std::vector<uint32_t> &mask)
 {
+    if (p->flow == RBC_FLOW_SHEAR) return build_mask_shear(p, bc, mask);
     const int nx = p->nx, ny = p->ny, nz = p->nz;
     const long long plane = (long long)nx * ny;
     mask.assign(plane, 0u);
@@ -456,6 +525,7 @@ int launch_lbm_stage(rbc_handle *h)
     a.gin = h->g[h->cur]; a.gout = h->g[1 - h->cur];
     a.uvr = h->uvr;
     a.Fx = h->Fx; a.Fy = h->Fy; a.Fz = h->Fz; a.mask2d = h->mask2d; a.drive = h->d_drive;
+    a.wall = h->p.flow == RBC_FLOW_SHEAR ? h->d_drive + 1 : nullptr;
     a.omega = (float)(1.0 / h->p.tau); a.Cr = (float)h->p.Cr; a.Bc = (float)h->p.B;
     a.scale = h->scale; a.inv_scale = h->inv_scale;
     launch_lbm(h->geo, h->p.storage, a, h->stream);
@@ -517,7 +587,7 @@ int enqueue_step(rbc_handle *h, StepForm form = STEP_WHOLE)
         if ((rc = launch_volume_stage(h, h->side))) return rc;
         CK(cudaEventRecord(h->join, h->side));
     }
-    launch_step_begin(h->d_iter(), h->d_drive, h->p.P, h->p.flowstart, h->p.freq, h->p.dt, h->stream);
+    launch_step_begin(step_begin_args(h), h->stream);
     h->launches++;
     CK_LAUNCH();
     if ((rc = launch_stress(h))) return rc;
@@ -683,15 +753,17 @@ int rbc_create(const rbc_params *p, const rbc_mesh *mesh, const int *bc, rbc_han
     h->p = *p;
     if (h->p.solver_iters == 0) h->p.solver_iters = DEFAULT_SOLVER_ITERS;
     Geom &g = h->geo;
-    g.nx = p->nx; g.ny = p->ny; g.nzr = p->nz; g.nzc = p->nz - 4;
-    g.plane = (long long)p->nx * p->ny; g.nint = g.plane * g.nzc;
+    const bool shear = p->flow == RBC_FLOW_SHEAR;
+    g.nxr = p->nx; g.xb = shear ? 2 : 0; g.xper = shear ? 1 : 0;
+    g.nx = p->nx - 2 * g.xb; g.ny = p->ny; g.nzr = p->nz; g.nzc = p->nz - 4;
+    g.plane = (long long)g.nx * p->ny; g.nint = g.plane * g.nzc;
     g.dx = p->dx;
     g.inv_dx = 1.0 / p->dx;
     g.xoff = (double)(p->nx - 1) * p->dx / 2.0;
     g.yoff = (double)(p->ny - 1) * p->dx / 2.0;
     g.zoff = (double)(p->nz - 1) * p->dx / 2.0;
     g.LX = p->LX; g.LZ = p->LZ; g.xmin = p->xmin; g.xmax = p->xmax; g.zmin = p->zmin; g.zmax = p->zmax;
-    h->nref_nodes = g.plane * g.nzr;
+    h->nref_nodes = (long long)g.nxr * g.ny * g.nzr;
     if (p->storage == RBC_STORE_F16) { h->scale = F16_SCALE; h->inv_scale = 1.0f / F16_SCALE; }
 
     auto bail = [&](int code) {
@@ -759,16 +831,47 @@ int rbc_create(const rbc_params *p, const rbc_mesh *mesh, const int *bc, rbc_han
     }
     TRY(dalloc(h, &h->uvr, g.nint)); TRY(dalloc(h, &h->Fx, g.nint)); TRY(dalloc(h, &h->Fy, g.nint));
     TRY(dalloc(h, &h->Fz, g.nint)); TRY(dalloc(h, &h->mask2d, g.plane));
-    TRY(dalloc(h, &h->d_int, 4)); TRY(dalloc(h, &h->d_drive, 1));
+    TRY(dalloc(h, &h->d_int, 4)); TRY(dalloc(h, &h->d_drive, 3));
     if (cudaMemset(h->g[0], 0, h->gbytes) != cudaSuccess || cudaMemset(h->g[1], 0, h->gbytes) != cudaSuccess ||
         cudaMemset(h->Fx, 0, 4 * g.nint) != cudaSuccess ||
         cudaMemset(h->Fy, 0, 4 * g.nint) != cudaSuccess || cudaMemset(h->Fz, 0, 4 * g.nint) != cudaSuccess ||
-        cudaMemset(h->d_int, 0, 4 * sizeof(int)) != cudaSuccess || cudaMemset(h->d_drive, 0, sizeof(float)) != cudaSuccess ||
+        cudaMemset(h->d_int, 0, 4 * sizeof(int)) != cudaSuccess || cudaMemset(h->d_drive, 0, 3 * sizeof(float)) != cudaSuccess ||
         cudaMemcpy(h->mask2d, mask.data(), 4 * g.plane, cudaMemcpyHostToDevice) != cudaSuccess) {
         h->err = "device initialisation failed";
         return bail(RBC_ERR_CUDA);
     }
     launch_fill_f4(h->uvr, g.nint, make_float4(0.f, 0.f, 0.f, 1.f), h->stream);
+    if (shear && p->flowstart == 0) {
+        // flu_init's linear profile between the walls (init1.cu:367-381), as reference-layout
+        // populations imported for the first step
+        const double LY = (double)(p->ny - 4) * p->dx, Cr = p->Cr;
+        const long long pr = (long long)p->nx * p->ny;
+        std::vector<double> fn((size_t)h->nref_nodes * Q);
+        std::vector<float4> uv((size_t)g.nint);
+        auto tw_of = [&](int iy) {
+            return p->walls == RBC_WALLS_BOTH ? p->sr * (-LY / 2.0 - 1.5 * p->dx + iy * p->dx)
+                                              : p->sr * (-1.5 * p->dx + iy * p->dx);
+        };
+        for (long long i = 0; i < h->nref_nodes; i++) {
+            const double tw = tw_of((int)((i % pr) / p->nx)), uvw = -1.5 * tw * tw * Cr * Cr;
+            for (int q = 0; q < Q; q++) {
+                const double eu = ez(q) * tw;
+                fn[(size_t)i * Q + q] = wqd(q) * (1.0 + 3.0 * eu * Cr + 4.5 * eu * eu * Cr * Cr + uvw);
+            }
+        }
+        for (long long i = 0; i < g.nint; i++) {
+            const int y = (int)((i % g.plane) / g.nx);
+            uv[(size_t)i] = (y >= 2 && y < g.ny - 2) ? make_float4(0.f, 0.f, (float)tw_of(y), 1.f) : make_float4(0.f, 0.f, 0.f, 1.f);
+        }
+        if (ensure_staging(h, 8 * fn.size()) != RBC_OK ||
+            cudaMemcpy(h->staging, fn.data(), 8 * fn.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(h->uvr, uv.data(), 16 * uv.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
+            h->err = "initial shear profile upload failed";
+            return bail(RBC_ERR_CUDA);
+        }
+        launch_import_lattice(g, p->storage, (const double *)h->staging, h->g[h->cur], h->mask2d, h->scale,
+                              wall_velocities(h, 1), h->stream);
+    }
 
     if (cells) {
         TRY(dalloc(h, &h->X, 3 * h->nv)); TRY(dalloc(h, &h->Xd, 3 * h->nv)); TRY(dalloc(h, &h->gref, h->ne));
@@ -836,7 +939,8 @@ int rbc_import_ref_lattice(rbc_handle *h, const double *fn)
     int rc = ensure_staging(h, bytes);
     if (rc) return rc;
     CK(cudaMemcpyAsync(h->staging, fn, bytes, cudaMemcpyHostToDevice, h->stream));
-    launch_import_lattice(h->geo, h->p.storage, (const double *)h->staging, h->g[h->cur], h->mask2d, h->scale, h->stream);
+    launch_import_lattice(h->geo, h->p.storage, (const double *)h->staging, h->g[h->cur], h->mask2d, h->scale,
+                          wall_velocities(h, h->iter + 1), h->stream);
     h->launches++;
     CK_LAUNCH();
     CK(cudaStreamSynchronize(h->stream));
@@ -855,7 +959,7 @@ int rbc_export_ref_lattice(rbc_handle *h, double *fn, double *dn, double *un, do
     double *sfn = (double *)h->staging;
     double *smac = fn ? sfn + Q * n : sfn;
     launch_export_lattice(h->geo, h->p.storage, h->g[h->cur], h->mask2d, h->uvr, h->inv_scale,
-                          fn ? sfn : nullptr, macro ? smac : nullptr, smac + n, smac + 2 * n, smac + 3 * n, h->stream);
+                          fn ? sfn : nullptr, macro ? smac : nullptr, smac + n, smac + 2 * n, smac + 3 * n, wall_velocities(h, h->iter + 1), h->stream);
     h->launches++;
     CK_LAUNCH();
     if (fn) CK(cudaMemcpyAsync(fn, sfn, sizeof(double) * Q * n, cudaMemcpyDeviceToHost, h->stream));
@@ -971,9 +1075,11 @@ int rbc_set_iter(rbc_handle *h, int iter)
     RBC_DEVICE_GUARD(h);
     CK(cudaStreamSynchronize(h->stream));
     h->iter = iter;
-    const float drive = (float)(h->p.P * drive_factor(h->p, iter));
+    // the drive and wall velocities of step `iter`, as step_begin leaves them (for stage calls)
+    const WallVel w = wall_velocities(h, iter);
+    const float dv[3] = {(float)(h->p.P * drive_factor(h->p, iter)), (float)w.top, (float)w.bot};
     CK(cudaMemcpy(h->d_iter(), &iter, sizeof(int), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(h->d_drive, &drive, sizeof(float), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(h->d_drive, dv, sizeof(dv), cudaMemcpyHostToDevice));
     return RBC_OK;
 }
 
@@ -1082,7 +1188,7 @@ int rbc_profile_steps(rbc_handle *h, int nsteps, double *kernel_ms)
     for (auto &e : ev) CK(cudaEventCreate(&e));
     for (int s = 0; s < nsteps && rc == RBC_OK; s++) {
         cudaEventRecord(ev[0], h->stream);
-        launch_step_begin(h->d_iter(), h->d_drive, h->p.P, h->p.flowstart, h->p.freq, h->p.dt, h->stream);
+        launch_step_begin(step_begin_args(h), h->stream);
         h->launches++;
         cudaEventRecord(ev[1], h->stream);
         if (!rc) rc = launch_stress(h);
@@ -1168,7 +1274,7 @@ int rbc_launch_count(const rbc_handle *h, long long *count)
 int rbc_dims(const rbc_handle *h, int *nx, int *ny, int *nz_periodic, int *ncell, int *vertex, int *element)
 {
     if (!h) return RBC_ERR_ARG;
-    if (nx) *nx = h->geo.nx;
+    if (nx) *nx = h->geo.nxr;
     if (ny) *ny = h->geo.ny;
     if (nz_periodic) *nz_periodic = h->geo.nzc;
     if (ncell) *ncell = h->ncell;
@@ -1502,8 +1608,10 @@ int adjoint_enqueue_recompute_body(rbc_handle *h, int b, int len)
         if ((rc = d2d(h, a->sX + k * nv3, h->X, 8 * nv3))) return rc;
         if ((rc = d2d(h, a->sXd + k * nv3, h->Xd, 8 * nv3))) return rc;
         if ((rc = d2d(h, a->sgx + k * N3, h->gx, 8 * N3))) return rc;
-        launch_step_begin_recorded(h->d_iter(), h->d_drive, h->p.P, h->p.flowstart, h->p.freq, h->p.dt,
-                                   a->sdrv + k, a->sfac + k, h->stream);
+        StepBeginArgs sb = step_begin_args(h);
+        sb.drive_rec = a->sdrv + k;
+        sb.factor_rec = a->sfac + k;
+        launch_step_begin(sb, h->stream);
         h->launches++;
         CK_LAUNCH();
         if ((rc = launch_stress(h))) return rc;
@@ -1617,6 +1725,7 @@ int adjoint_supported(rbc_handle *h)
     if (h->p.storage != RBC_STORE_F32) return fail(h, RBC_ERR_UNSUPPORTED, "the adjoint needs FP32 population storage");
     if (h->p.br != 0.0) return fail(h, RBC_ERR_UNSUPPORTED, "the adjoint does not cover bending (BR != 0)");
     if (h->geo.nzc > 65535) return fail(h, RBC_ERR_UNSUPPORTED, "the adjoint handles at most 65535 periodic planes");
+    if (h->p.flow != RBC_FLOW_CHANNEL) return fail(h, RBC_ERR_UNSUPPORTED, "the adjoint covers the channel mode only");
     return RBC_OK;
 }
 
@@ -1795,15 +1904,19 @@ int output_averages(rbc_handle *h, double *qi, double *tp, bool set)
 int reference_bc(rbc_handle *h, int *bc)
 {
     RBC_DEVICE_GUARD(h);
-    const long long plane = h->geo.plane;
-    std::vector<uint32_t> mask(plane);
-    CK(cudaMemcpy(mask.data(), h->mask2d, 4 * plane, cudaMemcpyDeviceToHost));
-    const int nz = h->p.nz;
-    for (int z = 0; z < nz; z++) {
-        const bool buff = z < 2 || z >= nz - 2;
-        for (long long xy = 0; xy < plane; xy++)
-            bc[z * plane + xy] = (mask[xy] & MASK_FLUID) ? (buff ? RBC_BUFF : RBC_COMP) : RBC_WALL;
-    }
+    const Geom &g = h->geo;
+    std::vector<uint32_t> mask(g.plane);
+    CK(cudaMemcpy(mask.data(), h->mask2d, 4 * g.plane, cudaMemcpyDeviceToHost));
+    const int nz = h->p.nz, nxr = g.nxr;
+    const long long pr = (long long)nxr * g.ny;
+    for (int z = 0; z < nz; z++)
+        for (int y = 0; y < g.ny; y++)
+            for (int xr = 0; xr < nxr; xr++) {
+                // x BUFF columns (shear mode) are periodic images of the internal columns
+                const int x = g.xper ? ((xr - g.xb) % g.nx + g.nx) % g.nx : xr;
+                const bool buff = z < 2 || z >= nz - 2 || xr < g.xb || xr >= nxr - g.xb;
+                bc[z * pr + (long long)y * nxr + xr] = (mask[(size_t)y * g.nx + x] & MASK_FLUID) ? (buff ? RBC_BUFF : RBC_COMP) : RBC_WALL;
+            }
     return RBC_OK;
 }
 

@@ -29,6 +29,11 @@ namespace rbc {
 
 constexpr int Q = 19;
 constexpr uint32_t MASK_FLUID = 0x80000000u;
+// shear mode (x periodic, moving y walls): column flags beside the link bits 1..18
+constexpr uint32_t MASK_XLO = 1u << 20;    // first column: x - 1 is the last column (periodic)
+constexpr uint32_t MASK_XHI = 1u << 21;    // last column: x + 1 is the first column
+constexpr uint32_t MASK_TOPW = 1u << 22;   // the column's wall links touch the top (+y) wall
+constexpr uint32_t MASK_BOTW = 1u << 23;   // ... the bottom (-y) wall
 
 // D3Q19 in the reference's slot order (lbm.cu:1038-1047):
 // ___ p__ m__ _p_ _m_ __p __m pp_ mm_ mp_ pm_ _pp _mm _mp _pm p_p m_m p_m m_p
@@ -51,6 +56,8 @@ __host__ __device__ constexpr double wqd(int q) { return q == 0 ? (1.0 / 3.0) : 
 // Geometry of one handle, passed by value to kernels.
 struct Geom {
     int nx, ny, nzc, nzr;      // internal dims; nzr = reference nz (nzc + 4)
+    int nxr, xb, xper;         // reference nx; x columns stripped at each end (2 in the shear
+                               // mode, whose x is periodic with BUFF columns; else 0); x periodic
     long long plane, nint;     // nx*ny, nx*ny*nzc
     double dx, inv_dx;
     double xoff, yoff, zoff;   // lattice coordinate = (pos + off)/dx (ibm.cu:100-102)
@@ -59,7 +66,7 @@ struct Geom {
 
 // Lattice coordinates of a position in the internal frame (z without BUFF).
 // (multiplication by 1/dx; exact for the unit lattice spacing the workloads use)
-__device__ __forceinline__ double lat_x(const Geom &g, double x) { return (x + g.xoff) * g.inv_dx; }
+__device__ __forceinline__ double lat_x(const Geom &g, double x) { return (x + g.xoff) * g.inv_dx - g.xb; }
 __device__ __forceinline__ double lat_y(const Geom &g, double y) { return (y + g.yoff) * g.inv_dx; }
 __device__ __forceinline__ double lat_z(const Geom &g, double z) { return (z + g.zoff) * g.inv_dx - 2.0; }
 
@@ -67,6 +74,7 @@ __device__ __forceinline__ int wrap_z(int iz, int nzc) {
     iz %= nzc;
     return iz < 0 ? iz + nzc : iz;
 }
+__device__ __forceinline__ int wrap_x(int ix, int nx) { return wrap_z(ix, nx); }
 
 // 4-point cosine delta, phi(r) = (1 + cos(pi r / 2)) / 4 (ibm.cu:103-128), at the
 // four nodes floor(l)-1 .. floor(l)+2 for fraction f = l - floor(l):
@@ -89,15 +97,18 @@ struct LbmArgs {
     float *Fx, *Fy, *Fz;
     const uint32_t *mask2d;
     const float *drive;        // device scalar: P * drive factor of this step
+    const float *wall;         // device [2]: z velocity of the top and bottom walls (shear mode), else NULL
     float omega, Cr, Bc;
     float scale, inv_scale;    // FP16 storage scale
 };
 void launch_lbm(const Geom &g, int storage, const LbmArgs &a, cudaStream_t s);
+// z velocities of the top and bottom walls in the next step (shear mode; 0 otherwise)
+struct WallVel { double top, bot, Cr; };
 void launch_import_lattice(const Geom &g, int storage, const double *fn_ref, void *gout,
-                           const uint32_t *mask2d, float scale, cudaStream_t s);
+                           const uint32_t *mask2d, float scale, const WallVel &w, cudaStream_t s);
 void launch_export_lattice(const Geom &g, int storage, const void *gin, const uint32_t *mask2d,
                            const float4 *uvr, float inv_scale, double *fn_ref, double *dn, double *un,
-                           double *vn, double *wn, cudaStream_t s);
+                           double *vn, double *wn, const WallVel &w, cudaStream_t s);
 void launch_export_force(const Geom &g, const float *Fx, const float *Fy, const float *Fz,
                          const uint32_t *mask2d, double *out3, cudaStream_t s);
 void launch_fill_f32(float *p, long long n, float v, cudaStream_t s);
@@ -200,11 +211,16 @@ void launch_volume(const Geom &g, const VolumeArgs &a, cudaStream_t s);
 // *membrane_max_smem receives the dynamic shared memory the membrane kernel may use.
 int  setup_kernel_attributes(int *membrane_max_smem);
 
-void launch_step_begin(int *d_iter, float *d_drive, double P, int flowstart, double freq, double dt,
-                       cudaStream_t s);
-// the same, also storing the step's drive P * factor and factor (for the adjoint)
-void launch_step_begin_recorded(int *d_iter, float *d_drive, double P, int flowstart, double freq, double dt,
-                                float *drive_rec, double *factor_rec, cudaStream_t s);
+// Step begin: iteration counter, drive P * factor (lbm.cu:1030-1035) and, in the
+// shear mode, the walls' z velocities (lbm.cu:752, 946-964).
+struct StepBeginArgs {
+    int *iter; float *drive;
+    double P, freq, dt; int flowstart;
+    float *wall;               // [2] top, bottom; NULL outside the shear mode
+    double sr, LY; int walls;  // shear rate, wall distance, 0 both walls / 1 top wall
+    float *drive_rec; double *factor_rec;   // where the adjoint keeps the step's drive (may be NULL)
+};
+void launch_step_begin(const StepBeginArgs &a, cudaStream_t s);
 
 // ---- adjoint of one step (adjoint.cu); FP32 populations ----------------------
 

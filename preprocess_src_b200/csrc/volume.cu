@@ -10,8 +10,8 @@
 // sequence of moves does not depend on the other cells: one CTA per cell runs
 // that cell's loop on the device with block reductions.  The reference's
 // return value (iterations - 1 of the slowest cell) is kept as an atomic max.
-// Also the step-begin kernel (iteration counter and drive factor, main.cu:75,
-// lbm.cu:1030-1035).
+// Also the step-begin kernel (iteration counter, drive factor and wall
+// velocities, main.cu:75, lbm.cu:752, 1030-1035).
 #include "rbc_internal.cuh"
 
 namespace rbc {
@@ -61,12 +61,17 @@ volume_kernel(const Geom g, const VolumeArgs a)
     double *p = reinterpret_cast<double *>(smem);   // [3][V]
     const int V = a.V, E = a.E, tid = threadIdx.x, T = blockDim.x, cell = blockIdx.x, N = a.ncell;
     const long long vb = (long long)cell * V, nv = a.nv;
-    const double gz = a.gx[2 * N + cell];
+    const double gz = a.gx[2 * N + cell], gxx = a.gx[cell];
     for (int v = tid; v < V; v += T) {
-        p[v] = a.X[vb + v];
+        double x = a.X[vb + v];
+        if (g.xper) {                                       // CapsulePeriodicBefore, x (shear mode)
+            const double dxx = x - gxx;
+            if (dxx > g.LX * 0.5) x -= g.LX; else if (dxx < -g.LX * 0.5) x += g.LX;
+        }
+        p[v] = x;
         p[V + v] = a.X[nv + vb + v];
         double z = a.X[2 * nv + vb + v];
-        const double dz = z - gz;                           // CapsulePeriodicBefore (z only)
+        const double dz = z - gz;                           // CapsulePeriodicBefore, z
         if (dz > g.LZ * 0.5) z -= g.LZ; else if (dz < -g.LZ * 0.5) z += g.LZ;
         p[2 * V + v] = z;
     }
@@ -121,6 +126,7 @@ volume_kernel(const Geom g, const VolumeArgs a)
     sy = block_sum_d(sy, red) / (double)V;
     sz = block_sum_d(sz, red) / (double)V;
     if (sz < g.zmin) sz += g.LZ; else if (sz > g.zmax) sz -= g.LZ;
+    if (g.xper) { if (sx < g.xmin) sx += g.LX; else if (sx > g.xmax) sx -= g.LX; }   // volume_correction.cu:319-325
     if (tid == 0) {
         if (a.vol_out) a.vol_out[cell] = vol;
         if (a.area_out) a.area_out[cell] = area;
@@ -131,9 +137,10 @@ volume_kernel(const Geom g, const VolumeArgs a)
     if (!a.correct) return;
     // CapsulePeriodicAfter, then store
     for (int v = tid; v < V; v += T) {
-        double z = p[2 * V + v];
+        double z = p[2 * V + v], x = p[v];
         if (z < g.zmin) z += g.LZ; else if (z > g.zmax) z -= g.LZ;
-        a.X[vb + v] = p[v];
+        if (g.xper) { if (x < g.xmin) x += g.LX; else if (x > g.xmax) x -= g.LX; }   // volume_correction.cu:88-91
+        a.X[vb + v] = x;
         a.X[nv + vb + v] = p[V + v];
         a.X[2 * nv + vb + v] = z;
     }
@@ -178,27 +185,24 @@ int setup_kernel_attributes(int *membrane_max_smem)
     return 0;
 }
 
-__global__ void step_begin_kernel(int *iter, float *drive, double P, int flowstart, double freq, double dt,
-                                  float *drive_rec, double *factor_rec)
+__global__ void step_begin_kernel(const StepBeginArgs a)
 {
-    const int it = *iter + 1;
-    *iter = it;
-    const double wi = (it > flowstart) ? 1.0 + 0.5 * sin(M_PI * dt * (double)it / freq) : 0.0;
-    *drive = (float)(P * wi);
-    if (drive_rec) *drive_rec = (float)(P * wi);   // kept for the adjoint of the step
-    if (factor_rec) *factor_rec = wi;
+    const int it = *a.iter + 1;
+    *a.iter = it;
+    const double wi = (it > a.flowstart) ? 1.0 + 0.5 * sin(M_PI * a.dt * (double)it / a.freq) : 0.0;
+    *a.drive = (float)(a.P * wi);
+    if (a.drive_rec) *a.drive_rec = (float)(a.P * wi);   // kept for the adjoint of the step
+    if (a.factor_rec) *a.factor_rec = wi;
+    if (a.wall) {   // lbm.cu:752 (sra), 946-964: allwall -/+ sra LY/2, topwall sra LY at the top
+        const double sra = (it < a.flowstart) ? 0.0 : a.sr;
+        a.wall[0] = (float)(a.walls == 0 ? sra * a.LY / 2.0 : sra * a.LY);
+        a.wall[1] = (float)(a.walls == 0 ? -sra * a.LY / 2.0 : 0.0);
+    }
 }
 
-void launch_step_begin(int *d_iter, float *d_drive, double P, int flowstart, double freq, double dt,
-                       cudaStream_t s)
+void launch_step_begin(const StepBeginArgs &a, cudaStream_t s)
 {
-    step_begin_kernel<<<1, 1, 0, s>>>(d_iter, d_drive, P, flowstart, freq, dt, nullptr, nullptr);
-}
-
-void launch_step_begin_recorded(int *d_iter, float *d_drive, double P, int flowstart, double freq, double dt,
-                                float *drive_rec, double *factor_rec, cudaStream_t s)
-{
-    step_begin_kernel<<<1, 1, 0, s>>>(d_iter, d_drive, P, flowstart, freq, dt, drive_rec, factor_rec);
+    step_begin_kernel<<<1, 1, 0, s>>>(a);
 }
 
 }  // namespace rbc

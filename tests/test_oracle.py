@@ -202,3 +202,22 @@ def test_bending_force_is_energy_gradient(oracle_mod):
             xm[d][i] -= h
             g = (_bend_energy(*xp, case.tri, 0.05) - _bend_energy(*xm, case.tri, 0.05)) / (2 * h)
             assert abs(-g - f[i, d]) <= 1e-6 * np.abs(f).max(), (i, d, -g, f[i, d])
+
+
+@pytest.mark.parametrize("walls", [0, 1])
+def test_shear_mode_reaches_the_couette_profile(oracle_mod, walls):
+    """CapsuleSHEARFLOW without cells: from rest, walls moving from step 1 on
+    (FLOWSTART = 1), the flow between the half-way walls becomes the linear
+    Couette profile u_z(y) = sr y (both walls at -/+ sr LY/2) or sr (y + LY/2)
+    (top wall at sr LY), which half-way bounce-back holds exactly."""
+    from preprocess_src_b200 import configs
+    case = configs.shear_case("couette_8x16x8", 8, 16, 8, sr=1e-3, walls=walls, flowstart=1)
+    o = oracle_mod.Oracle(case)
+    o.step(4000)
+    nx, ny, nz = case.nx, case.ny, case.nz
+    w = o["wn"].reshape(nz, ny, nx)[2:nz - 2, 2:ny - 2, 2:nx - 2]
+    LY = ny - 4
+    y = -LY / 2 - 1.5 + np.arange(2, ny - 2)
+    exact = 1e-3 * (y if walls == 0 else y + LY / 2)
+    assert np.abs(w - exact[None, :, None]).max() <= 1e-9 * np.abs(exact).max()
+    assert np.abs(o["un"]).max() <= 1e-12 and np.abs(o["vn"]).max() <= 1e-12
