@@ -115,6 +115,9 @@ typedef struct rbc_params {
     int    flow;         /* RBC_FLOW_CHANNEL (CapsuleCHANNELFLOW) or RBC_FLOW_SHEAR (CapsuleSHEARFLOW) */
     double sr;           /* cdo->sr, shear rate of the moving walls (shear mode; lattice units) */
     int    walls;        /* RBC_WALLS_BOTH (allwall: walls at -/+ sr LY/2) or RBC_WALLS_TOP (topwall: top at sr LY) */
+    /* channel mode: > 0 = the walls are the circular tube x^2 + y^2 = tube_r^2 and its links
+     * bounce back by linear interpolation at the circle (lbm_cylinder.cu:61-231); 0 = half-way */
+    double tube_r;
 } rbc_params;
 
 typedef struct rbc_mesh {

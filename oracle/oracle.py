@@ -27,7 +27,8 @@ class OrcParams(C.Structure):
                 ("law", C.c_int), ("residual", C.c_double), ("itrmax", C.c_int), ("LX", C.c_double),
                 ("LZ", C.c_double), ("xmin", C.c_double), ("xmax", C.c_double), ("zmin", C.c_double),
                 ("zmax", C.c_double), ("ncell", C.c_int), ("vertex", C.c_int), ("element", C.c_int),
-                ("mn", C.c_int), ("br", C.c_double), ("flow", C.c_int), ("sr", C.c_double), ("walls", C.c_int)]
+                ("mn", C.c_int), ("br", C.c_double), ("flow", C.c_int), ("sr", C.c_double), ("walls", C.c_int),
+                ("tube_r", C.c_double)]
 
 
 _STATE_D = ["fn", "fm", "dn", "un", "vn", "wn", "dm", "um", "vm", "wm", "fx", "fy", "fz"]
@@ -89,7 +90,8 @@ class Oracle:
                            law=p["law"], residual=p["residual"], itrmax=p["itrmax"], LX=p["LX"], LZ=p["LZ"],
                            xmin=p["xmin"], xmax=p["xmax"], zmin=p["zmin"], zmax=p["zmax"], ncell=self.N,
                            vertex=self.V, element=self.E, mn=self.mn, br=float(p.get("br", 0.0)),
-                           flow=int(p.get("flow", 0)), sr=float(p.get("sr", 0.0)), walls=int(p.get("walls", 0)))
+                           flow=int(p.get("flow", 0)), sr=float(p.get("sr", 0.0)), walls=int(p.get("walls", 0)),
+                           tube_r=float(p.get("tube_r", 0.0)))
         n = case.n
         self.a = {}
         for k in _STATE_D:

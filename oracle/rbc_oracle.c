@@ -670,6 +670,38 @@ void orc_lbm_d3q19(const orc_params *p, orc_state *s)
             fm[j] = f[q];
         }
     }
+    if (p->flow == 0 && p->tube_r > 0.0) {
+        /* lbm_cylinder.cu:116-231: every half-way bounced population of a link that crosses the
+         * circle x^2 + y^2 = R^2 at fraction t of the link is replaced by a linear interpolation
+         * (BounceBackLinearInterpolation_DEV, lbm_cylinder.cu:61-87) of itself (f1), the
+         * population streamed into the node along the link's direction (f2) and the one the
+         * node streamed to its opposite neighbour (f3).  The reference list is built once from
+         * the bc map (SetDistanceFromWall_GPU); the links are z-invariant, so it is recomputed. */
+        const double R = p->tube_r, dxl = p->dx;
+#pragma omp parallel for schedule(static)
+        for (long i = 0; i < n; i++) {
+            if (bc[i] != ORC_COMP) continue;
+            long iz = i / plane, iy = (i % plane) / nx, ix = (i % plane) % nx;
+            const double xi = (ix - (nx - 1) / 2.0) * dxl, yi = (iy - (ny - 1) / 2.0) * dxl;   /* init1.cu:223-224 */
+            for (int q = 1; q < ORC_Q; q++) {
+                long j = i + EX[q] + (long)nx * EY[q] + plane * EZ[q];
+                if (bc[j] != ORC_WALL) continue;
+                double ddx = EX[q] * dxl, ddy = EY[q] * dxl;
+                double a = ddx * ddx + ddy * ddy;
+                double Det = (xi * ddx + yi * ddy) * (xi * ddx + yi * ddy) - a * (xi * xi + yi * yi - R * R);
+                if (Det < 0.0) continue;
+                double t1 = (-xi * ddx - yi * ddy + sqrt(Det)) / a, t2 = (-xi * ddx - yi * ddy - sqrt(Det)) / a, t;
+                if (t1 > 0.0 && t1 < 1.0) t = t1; else if (t2 > 0.0 && t2 < 1.0) t = t2; else continue;
+                int o = OPP[q];
+                long jj = i + EX[o] + (long)nx * EY[o] + plane * EZ[o];
+                if (bc[jj] == ORC_BUFF) jj = i + EX[o] + (long)nx * EY[o] - plane * EZ[o] * (nz - 5);
+                double f1 = fm[i * ORC_Q + o], f2 = fm[i * ORC_Q + q], f3 = fm[jj * ORC_Q + o], f;
+                if (t < 0.5) f = 2.0 * t * f1 + (1.0 - 2.0 * t) * f2;
+                else f = 1.0 / (2.0 * t) * f1 + (2.0 * t - 1.0) / (2.0 * t) * f3;
+                fm[i * ORC_Q + o] = f;
+            }
+        }
+    }
     /* lbm.cu:1378-1432: BUFF planes take their periodic images */
 #pragma omp parallel for schedule(static)
     for (long i = 0; i < n; i++) {

@@ -57,6 +57,8 @@ typedef struct orc_params {
     int flow;
     double sr;           /* cdo->sr: shear rate (shear mode) */
     int walls;           /* 0: allwall (walls at -/+ sr LY / 2), 1: topwall (top at sr LY) */
+    double tube_r;       /* > 0 (channel mode): interpolated bounce-back on the circle x^2 + y^2 = tube_r^2
+                          * after streaming (lbm_cylinder.cu:116-231); 0: half-way bounce-back only */
 } orc_params;
 
 typedef struct orc_state {

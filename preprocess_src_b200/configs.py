@@ -87,7 +87,7 @@ def base_params(nx: int, ny: int, nz: int, *, tau=1.0, g=1e-6, Gs=5e-4, C=100.0,
                 flowstart=int(flowstart), freq=math.inf, LX=LX, LZ=LZ, xmin=-LX / 2, xmax=LX / 2, zmin=-LZ / 2,
                 zmax=LZ / 2, C=float(C), rgs=1.0, law=0, br=float(br), M=1, rk_order=4, storage=storage,
                 membrane_fp64=membrane_fp64, solver_iters=solver_iters, residual=residual,
-                itrmax=itrmax, device=-1, flow=int(flow), sr=float(sr), walls=int(walls))
+                itrmax=itrmax, device=-1, flow=int(flow), sr=float(sr), walls=int(walls), tube_r=0.0)
 
 
 def duct_to_ref(p, nx: int, ny: int, nz: int) -> np.ndarray:
@@ -149,6 +149,40 @@ def single_cell_duct(**kw) -> Case:
     kw.setdefault("seed", 1)
     return duct_case("single_cell_duct_64x32x32", 64, 32, 32, centers_duct=[(32.0, 16.0, 16.0)],
                      subdiv=3, steps=1000, **kw)
+
+
+def tube_bc(nx: int, ny: int, nz: int, R: float) -> np.ndarray:
+    """Circular tube (init1.cu:219-234): COMP where sqrt(x^2 + y^2) <= R in
+    the cross-section, BUFF over those columns in the two end planes at each z
+    end, WALL elsewhere."""
+    x = np.arange(nx) - (nx - 1) / 2.0
+    y = np.arange(ny) - (ny - 1) / 2.0
+    inside = (x[None, :] ** 2 + y[:, None] ** 2) <= R * R
+    bc = np.full((nz, ny, nx), WALL, dtype=np.int32)
+    bc[:, inside] = COMP
+    for z in (0, 1, nz - 2, nz - 1):
+        bc[z][inside] = BUFF
+    return bc.reshape(-1)
+
+
+def tube_case(name: str, flow: int, R: float, *, interp=True, centers=(), subdiv=3, radius=5.0, seed=0,
+              steps=1, **kw) -> Case:
+    """Circular tube of radius R along z (the reference channel's own
+    cross-section, init1.cu:219-234), periodic in z; interp selects the
+    interpolated bounce-back on the circle (lbm_cylinder.cu) instead of
+    half-way bounce-back on the staircase."""
+    n = int(math.ceil(2 * R)) + 3
+    nx = ny = n + (n % 2 == 0)
+    nz = flow + 4
+    params = base_params(nx, ny, nz, **kw)
+    params["tube_r"] = float(R) if interp else 0.0
+    shape, tri = _mesh.rbc_shape(subdiv)
+    rng = np.random.default_rng(seed)
+    cells = [_mesh.place(shape, _mesh.random_rotation(rng), radius, np.asarray(c, dtype=np.float64)) for c in centers]
+    xr = np.concatenate(cells).reshape(-1) if cells else np.zeros(0)
+    return Case(name=name, params=params, bc=tube_bc(nx, ny, nz, R), tri=tri.astype(np.int32), xr=xr,
+                ncell=len(cells), vertex=len(shape), element=len(tri), steps=steps,
+                meta=dict(R=R, interp=interp, flow=flow, seed=seed, subdiv=subdiv, radius=radius))
 
 
 def shear_bc(nx: int, ny: int, nz: int) -> np.ndarray:

@@ -193,6 +193,56 @@ void launch_lbm(const Geom &g, int storage, const LbmArgs &a, cudaStream_t s)
 #undef LBM_LAUNCH
 }
 
+// ---- circular tube: interpolated bounce-back ------------------------------
+
+// lbm_BounceBack_GPU + BounceBackLinearInterpolation_DEV (lbm_cylinder.cu:61-87,
+// 190-231) in pull form, after the collide-stream of a step: for a wall link of
+// node i in pull direction p crossing the circle at fraction t, the slot the
+// next pull bounces back from, f*_{opp p}(i) (read by no other node: its
+// regular reader i - e_p is the wall), becomes
+//   t < 1/2:  2t f1 + (1 - 2t) f2,    t >= 1/2:  f1 / 2t + (2t - 1) / 2t f3
+// with f1 = f*_{opp p}(i) (half-way), f2 = f*_{opp p}(i + e_p) (what i pulls
+// along opp p) and f3 = f*_p(i).  The weights sum to 1, so the same holds for
+// g = f - w.  No listed link reads a slot another one writes (a slot is
+// written only by its own node's link, and links with walls on both sides
+// are not listed).  One thread per (link, plane).
+template <int STORE>
+__global__ void tube_bounce_kernel(const Geom g, typename Store<STORE>::T *__restrict__ gs,
+                                   const int *__restrict__ links, const float *__restrict__ frac, int nlinks,
+                                   float inv_scale, float scale)
+{
+    using S = Store<STORE>;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nlinks) return;
+    const int z = blockIdx.y;
+    const int code = __ldg(&links[k]), xy = code >> 5, p = code & 31, o = opp(p);
+    const float t = __ldg(&frac[k]);
+    const long long zb = (long long)z * g.plane, i = zb + xy;
+    const int zn = wrap_z(z + ez(p), g.nzc), dxy = ex(p) + g.nx * ey(p);   // node i + e_p
+    typename S::T *slot = gs + (long long)o * g.nint + i;
+    const float f1 = S::ld(slot, inv_scale);
+    float f;
+    if (t < 0.5f) {
+        const float f2 = S::ld(gs + (long long)o * g.nint + (long long)zn * g.plane + xy + dxy, inv_scale);
+        f = 2.0f * t * f1 + (1.0f - 2.0f * t) * f2;
+    } else {
+        const float f3 = S::ld(gs + (long long)p * g.nint + i, inv_scale);
+        f = f1 / (2.0f * t) + (2.0f * t - 1.0f) / (2.0f * t) * f3;
+    }
+    S::st(slot, f, scale);
+}
+
+void launch_tube_bounce(const Geom &g, int storage, void *gout, const int *links, const float *frac, int nlinks,
+                        float inv_scale, float scale, cudaStream_t s)
+{
+    if (nlinks <= 0) return;
+    const dim3 grid((unsigned)((nlinks + 127) / 128), (unsigned)g.nzc);
+    if (storage == RBC_STORE_F16)
+        tube_bounce_kernel<RBC_STORE_F16><<<grid, 128, 0, s>>>(g, (__half *)gout, links, frac, nlinks, inv_scale, scale);
+    else
+        tube_bounce_kernel<RBC_STORE_F32><<<grid, 128, 0, s>>>(g, (float *)gout, links, frac, nlinks, inv_scale, scale);
+}
+
 // ---- reference layout <-> internal layout ---------------------------------
 
 // reference-layout index of internal node (x, y, z) (x and z without the BUFF layers)

@@ -51,6 +51,7 @@ struct rbc_handle {
     float4 *uvr = nullptr;
     float *Fx = nullptr, *Fy = nullptr, *Fz = nullptr;
     uint32_t *mask2d = nullptr;
+    int *tube_links = nullptr; float *tube_frac = nullptr; int ntube = 0;   // interpolated wall links (circular tube)
     // cells
     double *X = nullptr, *Xd = nullptr;
     double4 *gref = nullptr;
@@ -89,7 +90,7 @@ struct rbc_handle {
     double *qi_acc = nullptr, *tp_acc = nullptr;      // [ncell][mn], [ne][2]
 
     int kernels_per_step() const {
-        return KERNELS_PER_STEP + (p.br != 0.0 && ncell > 0 ? 1 : 0) + (fileoutput > 0 && ncell > 0 ? 2 : 0);
+        return KERNELS_PER_STEP + (p.br != 0.0 && ncell > 0 ? 1 : 0) + (fileoutput > 0 && ncell > 0 ? 2 : 0) + (ntube > 0 ? 1 : 0);
     }
     int *d_iter() { return d_int; }
     int *d_flags() { return d_int + 1; }
@@ -365,6 +366,8 @@ int check_params(const rbc_params *p)
     if (p->law != RBC_LAW_SKALAK && p->law != RBC_LAW_NEOHOOKEAN) return fail(nullptr, RBC_ERR_ARG, "unknown law");
     if (p->solver_iters < 0 || p->solver_iters > 200) return fail(nullptr, RBC_ERR_ARG, "solver_iters out of range");
     if (p->flow != RBC_FLOW_CHANNEL && p->flow != RBC_FLOW_SHEAR) return fail(nullptr, RBC_ERR_ARG, "unknown flow mode");
+    if (!(p->tube_r >= 0.0) || !std::isfinite(p->tube_r)) return fail(nullptr, RBC_ERR_ARG, "tube_r must be >= 0");
+    if (p->tube_r > 0.0 && p->flow != RBC_FLOW_CHANNEL) return fail(nullptr, RBC_ERR_ARG, "tube_r applies to the channel mode");
     if (p->flow == RBC_FLOW_SHEAR) {
         if (p->walls != RBC_WALLS_BOTH && p->walls != RBC_WALLS_TOP) return fail(nullptr, RBC_ERR_ARG, "unknown wall motion");
         if (!std::isfinite(p->sr)) return fail(nullptr, RBC_ERR_ARG, "shear rate must be finite");
@@ -405,6 +408,37 @@ int build_mask_shear(const rbc_params *p, const int *bc, std::vector<uint32_t> &
             mask[(size_t)y * nxi + x] = m;
         }
     return RBC_OK;
+}
+
+// SetDistanceFromWall_GPU (lbm_cylinder.cu:116-183): every wall link of a fluid
+// column (pull direction p, wall at i - e_p) that crosses the circle
+// x^2 + y^2 = R^2 of the cross-section, with the fraction t in (0, 1) of the
+// link i -> i - e_p at the crossing.  Links are z-invariant: one list per plane.
+void tube_links(const rbc_params *p, const std::vector<uint32_t> &mask, std::vector<int> &links, std::vector<float> &frac)
+{
+    const int nx = p->nx, ny = p->ny;
+    const long long plane = (long long)nx * ny;
+    const double R = p->tube_r, dx = p->dx;
+    links.clear();
+    frac.clear();
+    for (long long xy = 0; xy < plane; xy++) {
+        const uint32_t m = mask[xy];
+        if (!(m & MASK_FLUID)) continue;
+        const int ix = (int)(xy % nx), iy = (int)(xy / nx);
+        const double xi = (ix - (nx - 1) / 2.0) * dx, yi = (iy - (ny - 1) / 2.0) * dx;   // init1.cu:223-224
+        for (int q = 1; q < Q; q++) {
+            if (!((m >> q) & 1u) || ((m >> opp(q)) & 1u)) continue;   // a wall on both sides: half-way
+            const double ddx = -ex(q) * dx, ddy = -ey(q) * dx, a = ddx * ddx + ddy * ddy;
+            if (a == 0.0) continue;
+            const double b = xi * ddx + yi * ddy, det = b * b - a * (xi * xi + yi * yi - R * R);
+            if (det < 0.0) continue;
+            const double t1 = (-b + std::sqrt(det)) / a, t2 = (-b - std::sqrt(det)) / a;
+            double t;
+            if (t1 > 0.0 && t1 < 1.0) t = t1; else if (t2 > 0.0 && t2 < 1.0) t = t2; else continue;
+            links.push_back((int)(xy * 32 + q));
+            frac.push_back((float)t);
+        }
+    }
 }
 
 // Wall mask of one z plane from the reference bc map; checks z invariance.
@@ -452,7 +486,7 @@ void free_all(rbc_handle *h)
     if (h->fork) cudaEventDestroy(h->fork);
     if (h->join) cudaEventDestroy(h->join);
     if (h->side) cudaStreamDestroy(h->side);
-    void *ptrs[] = {h->g[0], h->g[1], h->uvr, h->Fx, h->Fy, h->Fz, h->mask2d,
+    void *ptrs[] = {h->g[0], h->g[1], h->uvr, h->Fx, h->Fy, h->Fz, h->mask2d, h->tube_links, h->tube_frac,
                     h->X, h->Xd, h->gref, h->erec, h->U, h->Fv, h->tri, h->v2e_off, h->v2e, h->nbr, h->visit, h->patch_off, h->patch_vtx, h->patch_stride, h->vol0, h->gx,
                     h->vol_out, h->area_out, h->cen_out, h->d_int, h->d_drive, h->staging};
     for (void *q : ptrs) if (q) cudaFree(q);
@@ -531,6 +565,12 @@ int launch_lbm_stage(rbc_handle *h)
     launch_lbm(h->geo, h->p.storage, a, h->stream);
     h->launches++;
     CK_LAUNCH();
+    if (h->ntube > 0) {   // circular tube: lbm_BounceBack_GPU (lbm_cylinder.cu:190-231) after the stream
+        launch_tube_bounce(h->geo, h->p.storage, h->g[1 - h->cur], h->tube_links, h->tube_frac, h->ntube,
+                           h->inv_scale, h->scale, h->stream);
+        h->launches++;
+        CK_LAUNCH();
+    }
     h->cur ^= 1;
     return RBC_OK;
 }
@@ -841,6 +881,20 @@ int rbc_create(const rbc_params *p, const rbc_mesh *mesh, const int *bc, rbc_han
         return bail(RBC_ERR_CUDA);
     }
     launch_fill_f4(h->uvr, g.nint, make_float4(0.f, 0.f, 0.f, 1.f), h->stream);
+    if (p->tube_r > 0.0) {
+        std::vector<int> links;
+        std::vector<float> frac;
+        tube_links(p, mask, links, frac);
+        h->ntube = (int)links.size();
+        TRY(dalloc(h, &h->tube_links, links.size()));
+        TRY(dalloc(h, &h->tube_frac, frac.size()));
+        if (!links.empty() &&
+            (cudaMemcpy(h->tube_links, links.data(), 4 * links.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+             cudaMemcpy(h->tube_frac, frac.data(), 4 * frac.size(), cudaMemcpyHostToDevice) != cudaSuccess)) {
+            h->err = "device initialisation failed";
+            return bail(RBC_ERR_CUDA);
+        }
+    }
     if (shear && p->flowstart == 0) {
         // flu_init's linear profile between the walls (init1.cu:367-381), as reference-layout
         // populations imported for the first step
@@ -1726,6 +1780,7 @@ int adjoint_supported(rbc_handle *h)
     if (h->p.br != 0.0) return fail(h, RBC_ERR_UNSUPPORTED, "the adjoint does not cover bending (BR != 0)");
     if (h->geo.nzc > 65535) return fail(h, RBC_ERR_UNSUPPORTED, "the adjoint handles at most 65535 periodic planes");
     if (h->p.flow != RBC_FLOW_CHANNEL) return fail(h, RBC_ERR_UNSUPPORTED, "the adjoint covers the channel mode only");
+    if (h->ntube > 0) return fail(h, RBC_ERR_UNSUPPORTED, "the adjoint covers half-way bounce-back walls only (tube_r = 0)");
     return RBC_OK;
 }
 

@@ -109,6 +109,11 @@ void launch_import_lattice(const Geom &g, int storage, const double *fn_ref, voi
 void launch_export_lattice(const Geom &g, int storage, const void *gin, const uint32_t *mask2d,
                            const float4 *uvr, float inv_scale, double *fn_ref, double *dn, double *un,
                            double *vn, double *wn, const WallVel &w, cudaStream_t s);
+// Circular tube: after each collide-stream, the slot each listed wall link bounces
+// back from becomes the interpolated bounce-back value (lbm_cylinder.cu:190-231).
+// links[k] = xy * 32 + p (pull direction p, wall at i - e_p), frac[k] = crossing fraction.
+void launch_tube_bounce(const Geom &g, int storage, void *gout, const int *links, const float *frac, int nlinks,
+                        float inv_scale, float scale, cudaStream_t s);
 void launch_export_force(const Geom &g, const float *Fx, const float *Fy, const float *Fz,
                          const uint32_t *mask2d, double *out3, cudaStream_t s);
 void launch_fill_f32(float *p, long long n, float v, cudaStream_t s);
