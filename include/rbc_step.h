@@ -172,6 +172,26 @@ int rbc_import_ref_vertex_force(rbc_handle *h, const double *fx, const double *f
 int rbc_export_ref_cells(rbc_handle *h, double *x, double *y, double *z, double *xd,
                          double *u, double *v, double *w, double *fx, double *fy, double *fz,
                          double *gx);
+/* ---- white cells (N_W > 0: init3.cu, stress.cu:620-655, ibm.cu:334-360 and
+ * 670-690, volume_correction.cu:260-340) ----------------------------------- */
+
+/* A second cell population stepped with the first: its own mesh, tension
+ * normalisation rgs (cel->rg_w = GSw / GS) and bending modulus br (BRw); the
+ * same law and C as the red cells.  It spreads into and advects with the same
+ * lattice and has its own volume correction.  Replaces wbc_init (init3.cu) for
+ * the step; the mesh's ncell is cel->n_w.  Synchronous; once per handle. */
+int rbc_add_wbc(rbc_handle *h, const rbc_mesh *mesh, double rgs, double br);
+/* cel->n_w, vertex_w, element_w (all 0 without white cells); any pointer may be NULL */
+int rbc_wbc_dims(const rbc_handle *h, int *ncell, int *vertex, int *element);
+/* rbc_import_ref_cells / rbc_export_ref_cells / rbc_cell_metrics for the white
+ * cells (cel->x_w ..., fem->xd_w, fem->nd_w, cel->volume0_w, cel->gx_w) */
+int rbc_import_ref_wbc(rbc_handle *h, const double *x, const double *y, const double *z,
+                       const double *xd, const double *nd, const double *volume0, const double *gx);
+int rbc_export_ref_wbc(rbc_handle *h, double *x, double *y, double *z, double *xd,
+                       double *u, double *v, double *w, double *fx, double *fy, double *fz,
+                       double *gx);
+int rbc_wbc_metrics(rbc_handle *h, double *volume, double *area, double *centroid);
+
 /* prc->iter as the stage entry points see it (rbc_step increments it first,
  * as main.cu:75 does) */
 int rbc_set_iter(rbc_handle *h, int iter);

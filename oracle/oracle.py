@@ -38,7 +38,8 @@ _STATE_CELL_D = ["x", "y", "z", "u", "v", "w", "cfx", "cfy", "cfz", "xd", "nd", 
 class OrcState(C.Structure):
     _fields_ = ([(k, _DP) for k in _STATE_D] + [("bc", _IP)] + [(k, _DP) for k in _STATE_CELL_D]
                 + [("ele", _IP), ("nln", _IP), ("ln", _IP), ("lo", _IP), ("nle", _IP), ("le", _IP),
-                   ("volume0", _DP), ("gx", _DP), ("iter", C.c_int), ("bicg_iters", C.c_int), ("ec", _IP)])
+                   ("volume0", _DP), ("gx", _DP), ("iter", C.c_int), ("bicg_iters", C.c_int), ("ec", _IP),
+                   ("crg", _DP), ("cbr", _DP)])
 
 
 _lib = None
@@ -79,7 +80,9 @@ def expand2pow2(n: int) -> int:
 class Oracle:
     """Reference-layout FP64 state of one case, stepped on the CPU."""
 
-    def __init__(self, case, init_fluid=True):
+    def __init__(self, case, init_fluid=True, cell_rgs=None, cell_br=None):
+        """cell_rgs, cell_br: optional [ncell] per-cell tension normalisation and
+        bending modulus (cells of a second population on the same mesh)."""
         self.case = case
         p = case.params
         self.N, self.V, self.E = case.ncell, case.vertex, case.element
@@ -107,6 +110,11 @@ class Oracle:
         self.a["ec"] = np.zeros(3 * ne, dtype=np.int32)
         self.a["volume0"] = np.zeros(max(self.N, 1))
         self.a["gx"] = np.zeros(3 * max(self.N, 1))
+        for k, v in (("crg", cell_rgs), ("cbr", cell_br)):
+            if v is not None:
+                self.a[k] = np.ascontiguousarray(v, dtype=np.float64).reshape(-1)
+                if self.a[k].size != self.N:
+                    raise ValueError(f"{k}: one value per cell")
         self.s = OrcState()
         for k, arr in self.a.items():
             setattr(self.s, k, arr.ctypes.data_as(_IP if arr.dtype == np.int32 else _DP))

@@ -256,11 +256,12 @@ void orc_calc_tension(const orc_params *p, orc_state *s)
         double i1 = n[4*j+0]*vd[0] + n[4*j+1]*vd[1] + n[4*j+2]*vd[2] + n[4*j+3]*vd[3] - 2.0;
         double i2 = dv12d * dn12 - 1.0;
         double js = sqrt(i2 + 1.0);
+        const double rgs = s->crg ? s->crg[j / p->element] : p->rgs;
         for (int i = 0; i < 4; i++) {
             if (p->law == 0)
-                s->t[4*j + i] = p->rgs * (i1 + 1.0) / js * n[4*j + i] + (p->C * i2 - 1.0) * js * ndf[i];
+                s->t[4*j + i] = rgs * (i1 + 1.0) / js * n[4*j + i] + (p->C * i2 - 1.0) * js * ndf[i];
             else
-                s->t[4*j + i] = p->rgs * (n[4*j + i] / js - ndf[i] * js / (i2 + 1.0) / (i2 + 1.0));
+                s->t[4*j + i] = rgs * (n[4*j + i] / js - ndf[i] * js / (i2 + 1.0) / (i2 + 1.0));
         }
     }
 }
@@ -420,10 +421,12 @@ void orc_q2f(const orc_params *p, orc_state *s)
  * rest). */
 void orc_bend(const orc_params *p, orc_state *s)
 {
-    if (p->br == 0.0) return;
+    if (p->br == 0.0 && !s->cbr) return;
     const long ne = (long)p->ncell * p->element;
     const double eps = 1.0e-6;
     for (long e1 = 0; e1 < ne; e1++) {
+        const double br = s->cbr ? s->cbr[e1 / p->element] : p->br;
+        if (br == 0.0) continue;
         const int i[3] = {s->ele[e1*3], s->ele[e1*3+1], s->ele[e1*3+2]};
         for (int k = 0; k < 3; k++) {
             const long e2 = s->ec[e1*3 + k];
@@ -457,7 +460,7 @@ void orc_bend(const orc_params *p, orc_state *s)
             if (cost2 < eps) continue;
             const double sgn = ((xix-zex)*(t1x-t2x) + (xiy-zey)*(t1y-t2y) + (xiz-zez)*(t1z-t2z)) >= 0.0 ? 1.0 : -1.0;
             const double sint = sgn * sqrt(cost2);
-            const double beta = sgn * 2.0 / sqrt(3.0) * p->br * (sint * 1.0 - cost * 0.0) / sqrt(cost2);
+            const double beta = sgn * 2.0 / sqrt(3.0) * br * (sint * 1.0 - cost * 0.0) / sqrt(cost2);
             const double b11 = -beta * cost / (nxi * nxi), b12 = beta / nxi / nze, b22 = -beta * cost / (nze * nze);
             s->cfx[k1] += b11*(xiy*-a23z - xiz*-a23y) + b12*(zey*-a23z - zez*-a23y);
             s->cfy[k1] += b11*(xiz*-a23x - xix*-a23z) + b12*(zez*-a23x - zex*-a23z);

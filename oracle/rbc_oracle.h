@@ -83,6 +83,10 @@ typedef struct orc_state {
     int    iter;                           /* prc->iter */
     int    bicg_iters;                     /* diagnostics: last solve's iterations */
     int    *ec;                            /* [3*ne] edge-neighbour elements (cel->ec) */
+    /* [ncell] per-cell tension normalisation and bending modulus, or NULL for
+     * p->rgs / p->br in every cell: a run with white cells as well (cel->rg_w
+     * = GSw / GS, cel->br_w = BRw, init3.cu:91-92) on the same mesh */
+    double *crg, *cbr;
 } orc_state;
 
 /* init2.cu:258-400 (fem_init): link tables and the reference metric from the

@@ -2,12 +2,14 @@
 
 TEST INFRASTRUCTURE ONLY: the checker for the library's file writers and
 readers (csrc/ref_files.cu).  Byte layouts follow etc.cu of the reference for
-a red-cell run (N_R > 0, N_W = 0, no cytoadhesion):
+a run with red cells (N_R), white cells (N_W) or both, no cytoadhesion; the
+white cells' fields carry the suffix "_w" as in the reference:
 
-  restart.bin   output_data etc.cu:738-766 / restart_file etc.cu:164-270
-  cell%04d.bin  etc.cu:566-590
+  restart.bin   output_data etc.cu:738-781 / restart_file etc.cu:164-270
+  cell%04d.bin  etc.cu:566-600 (one block per population, red first)
   prof%04d.bin  etc.cu:547-560
   center.dat    OutputCapsuleCenter / InputCapsuleCenter etc.cu:110-160
+                (red cells' lines, then the white cells', each counted from 0)
 
 and the output-interval averages those files carry: fem->tp, the principal
 tensions of calc_tension (stress.cu:76-118), and fem->qi, the load of
@@ -29,16 +31,24 @@ def expand2pow2(n: int) -> int:
     return 2 ** cnt
 
 
-def restart_layout(n: int, N: int, V: int, E: int):
-    """(name, dtype, count) in file order."""
+def _cell_block(N: int, V: int, E: int, sfx: str):
+    mn = expand2pow2(3 * V)
+    lay = [(k + sfx, np.float64, N * V) for k in ("x", "y", "z")]
+    lay += [(k + sfx, np.float64, N) for k in ("rx", "ry", "rz")]
+    lay += [(k + sfx, np.float64, N * V) for k in ("u", "v", "w")]
+    lay += [("qi" + sfx, np.float64, N * mn), ("tp" + sfx, np.float64, N * E * 2)]
+    return lay
+
+
+def restart_layout(n: int, N: int, V: int, E: int, Nw: int = 0, Vw: int = 0, Ew: int = 0):
+    """(name, dtype, count) in file order; N, V, E the red cells', Nw, Vw, Ew
+    the white cells'."""
     lay = [("iter", np.int32, 1), ("fnum", np.int32, 1), ("fn", np.float64, 19 * n)]
     lay += [(k, np.float64, n) for k in ("dm", "um", "vm", "wm", "vf", "vf2")]
     if N > 0:
-        mn = expand2pow2(3 * V)
-        lay += [(k, np.float64, N * V) for k in ("x", "y", "z")]
-        lay += [(k, np.float64, N) for k in ("rx", "ry", "rz")]
-        lay += [(k, np.float64, N * V) for k in ("u", "v", "w")]
-        lay += [("qi", np.float64, N * mn), ("tp", np.float64, N * E * 2)]
+        lay += _cell_block(N, V, E, "")
+    if Nw > 0:
+        lay += _cell_block(Nw, Vw, Ew, "_w")
     return lay
 
 
@@ -65,25 +75,35 @@ def _write(path, lay, fields: dict):
             f.write(a.tobytes())
 
 
-def read_restart(path, n, N, V, E) -> dict:
-    return _read(path, restart_layout(n, N, V, E))
+def read_restart(path, n, N, V, E, Nw=0, Vw=0, Ew=0) -> dict:
+    return _read(path, restart_layout(n, N, V, E, Nw, Vw, Ew))
 
 
-def write_restart(path, n, N, V, E, fields: dict):
+def write_restart(path, n, N, V, E, fields: dict, Nw=0, Vw=0, Ew=0):
     """fields: any subset of the layout's names; the rest are zeros."""
-    _write(path, restart_layout(n, N, V, E), fields)
+    _write(path, restart_layout(n, N, V, E, Nw, Vw, Ew), fields)
 
 
-def cell_layout(N, V, E):
-    return ([("N", np.int32, 1), ("V", np.int32, 1), ("E", np.int32, 1)]
-            + [(k, np.float64, N * V) for k in ("x", "y", "z", "u", "v", "w")]
-            + [("qi", np.float64, N * V * 3), ("tp", np.float64, N * E * 2), ("ele", np.int32, N * E * 3)])
+def cell_layout(N, V, E, sfx=""):
+    return ([(k + sfx, np.int32, 1) for k in ("N", "V", "E")]
+            + [(k + sfx, np.float64, N * V) for k in ("x", "y", "z", "u", "v", "w")]
+            + [("qi" + sfx, np.float64, N * V * 3), ("tp" + sfx, np.float64, N * E * 2),
+               ("ele" + sfx, np.int32, N * E * 3)])
 
 
-def read_cell_file(path) -> dict:
-    head = np.fromfile(path, dtype=np.int32, count=3)
-    N, V, E = (int(v) for v in head)
-    return _read(path, cell_layout(N, V, E))
+def read_cell_file(path, blocks: int = 1) -> dict:
+    """blocks = 2 for a file with red and white cells (the second block's
+    names carry "_w"); a run with white cells only writes one block."""
+    raw_len = len(open(path, "rb").read())
+    lay, off = [], 0
+    for b in range(blocks):
+        N, V, E = (int(v) for v in np.fromfile(path, dtype=np.int32, count=3, offset=off))
+        blk = cell_layout(N, V, E, "_w" if b else "")
+        lay += blk
+        off += sum(np.dtype(dt).itemsize * c for _, dt, c in blk)
+        if off > raw_len:
+            raise ValueError(f"{path}: too short for block {b}")
+    return _read(path, lay)
 
 
 def prof_layout(n):

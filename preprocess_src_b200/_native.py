@@ -91,6 +91,11 @@ _SIGS = {
     "rbc_write_prof_file": [_H, C.c_char_p],
     "rbc_write_center_file": [_H, C.c_char_p],
     "rbc_read_center_file": [_H, C.c_char_p],
+    "rbc_add_wbc": [_H, C.POINTER(RbcMesh), C.c_double, C.c_double],
+    "rbc_wbc_dims": [_H, _IP, _IP, _IP],
+    "rbc_import_ref_wbc": [_H, _DP, _DP, _DP, _DP, _DP, _DP, _DP],
+    "rbc_export_ref_wbc": [_H, _DP, _DP, _DP, _DP, _DP, _DP, _DP, _DP, _DP, _DP, _DP],
+    "rbc_wbc_metrics": [_H, _DP, _DP, _DP],
 }
 _RESTYPE = {"rbc_last_error": C.c_char_p, "rbc_batch_last_error": C.c_char_p}
 

@@ -135,6 +135,34 @@ def suspension_case(name: str, flow: int, Ly: int, Lz: int, ncell: int, *, subdi
                           hematocrit=hct))
 
 
+def split_cells(case: Case, nred: int) -> tuple[Case, Case]:
+    """The first nred cells of case as the red cells and the rest as a white
+    cell population on the same mesh: (red case, white-cell case).  The
+    white-cell case carries only the mesh (its lattice is case's)."""
+    nv = nred * case.vertex
+    red = Case(name=case.name + "_red", params=dict(case.params), bc=case.bc, tri=case.tri,
+               xr=case.xr[:3 * nv].copy(), ncell=nred, vertex=case.vertex, element=case.element,
+               steps=case.steps, meta=dict(case.meta))
+    white = Case(name=case.name + "_white", params=dict(case.params), bc=case.bc, tri=case.tri,
+                 xr=case.xr[3 * nv:].copy(), ncell=case.ncell - nred, vertex=case.vertex,
+                 element=case.element, steps=case.steps, meta=dict(case.meta))
+    return red, white
+
+
+def sphere_cells(case: Case, centers_ref, *, subdiv=2, radius=4.0, seed=0) -> Case:
+    """Spherical cells (init3.cu's SPHERE shape: an icosphere) of the given
+    radius at reference-frame centres, as a white-cell population for case's
+    lattice."""
+    shape, tri = _mesh.icosphere(subdiv)
+    rng = np.random.default_rng(seed)
+    cells = [_mesh.place(shape, _mesh.random_rotation(rng), radius, np.asarray(c, dtype=np.float64))
+             for c in centers_ref]
+    xr = np.concatenate(cells).reshape(-1)
+    return Case(name=case.name + "_spheres", params=dict(case.params), bc=case.bc, tri=tri.astype(np.int32),
+                xr=xr, ncell=len(cells), vertex=len(shape), element=len(tri), steps=case.steps,
+                meta=dict(subdiv=subdiv, radius=radius, seed=seed))
+
+
 def _cell_volume(v: np.ndarray, f: np.ndarray) -> float:
     a, b, c = v[f[:, 0]], v[f[:, 1]], v[f[:, 2]]
     return float(np.einsum("ij,ij->i", (a + b + c) / 3.0, np.cross(b - a, c - a)).sum() / 6.0)

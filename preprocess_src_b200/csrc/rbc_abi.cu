@@ -26,7 +26,6 @@ thread_local std::string g_create_error;
 
 constexpr float F16_SCALE = 32768.0f;     // (f - w) * 2^15 keeps |g| < 2 inside FP16 range
 constexpr int DEFAULT_SOLVER_ITERS = 16;  // Chebyshev error factor <= 2 * 3^-16 ~ 4.6e-8 (FP32 solve)
-constexpr int KERNELS_PER_STEP = 6;       // step_begin, membrane, spread, lbm, advect, volume (+ bend when BR != 0)
 
 }  // namespace
 
@@ -38,11 +37,44 @@ void set_last_error(const std::string &msg) { g_create_error = msg; }
 struct AdjointState;
 void adjoint_free(AdjointState *a);
 
+// One cell population: the red cells (the reference's cel->x ..., fem->...) or
+// the white cells (cel->x_w ..., fem->..._w, init3.cu), each with its own mesh
+// shared by its cells, tension normalisation rg (1 for red cells, GSw / GS for
+// white ones) and bending modulus.
+struct CellGroup {
+    int ncell = 0, V = 0, E = 0;
+    long long nv = 0, ne = 0;
+    double rgs = 1.0, br = 0.0;
+    double *X = nullptr, *Xd = nullptr;
+    double4 *gref = nullptr;
+    void *erec = nullptr;   // membrane element records, [ne][3] 4-vectors of float or double
+    float *U = nullptr, *Fv = nullptr;
+    int *tri = nullptr, *v2e_off = nullptr, *v2e = nullptr;
+    int16_t *nbr = nullptr;
+    int4 *visit = nullptr;   // bending visits [E][3], allocated when BR != 0
+    double *vol0 = nullptr, *gx = nullptr, *vol_out = nullptr, *area_out = nullptr, *cen_out = nullptr;
+    int *patch_off = nullptr, *patch_vtx = nullptr, *patch_stride = nullptr;
+    int npatch = 1;
+    int mn = 0;                                       // the reference's per-cell vector length (expand2pow2(3 V))
+    double *qi_acc = nullptr, *tp_acc = nullptr;      // output-interval averages [ncell][mn], [ne][2]
+};
+
 struct rbc_handle {
     rbc_params p{};
     Geom geo{};
-    int ncell = 0, V = 0, E = 0;
-    long long nv = 0, ne = 0, nref_nodes = 0;
+    // cell populations: cg[0] red cells, cg[1] white cells (rbc_add_wbc)
+    CellGroup cg[2];
+    int ngroups = 1;
+    // the red cells under the names the single-population code uses (the handle is never copied)
+    int &ncell = cg[0].ncell, &V = cg[0].V, &E = cg[0].E;
+    long long &nv = cg[0].nv, &ne = cg[0].ne;
+    double *&X = cg[0].X, *&Xd = cg[0].Xd;
+    double4 *&gref = cg[0].gref;
+    float *&U = cg[0].U, *&Fv = cg[0].Fv;
+    int *&tri = cg[0].tri, *&v2e_off = cg[0].v2e_off, *&v2e = cg[0].v2e;
+    int16_t *&nbr = cg[0].nbr;
+    double *&vol0 = cg[0].vol0, *&gx = cg[0].gx;
+    long long nref_nodes = 0;
     cudaStream_t stream = nullptr;
     // lattice
     void *g[2] = {nullptr, nullptr};
@@ -52,15 +84,6 @@ struct rbc_handle {
     float *Fx = nullptr, *Fy = nullptr, *Fz = nullptr;
     uint32_t *mask2d = nullptr;
     int *tube_links = nullptr; float *tube_frac = nullptr; int ntube = 0;   // interpolated wall links (circular tube)
-    // cells
-    double *X = nullptr, *Xd = nullptr;
-    double4 *gref = nullptr;
-    void *erec = nullptr;   // membrane element records, [ne][3] 4-vectors of float or double
-    float *U = nullptr, *Fv = nullptr;
-    int *tri = nullptr, *v2e_off = nullptr, *v2e = nullptr;
-    int16_t *nbr = nullptr;
-    int4 *visit = nullptr;   // bending visits [E][3], allocated when BR != 0
-    double *vol0 = nullptr, *gx = nullptr, *vol_out = nullptr, *area_out = nullptr, *cen_out = nullptr;
     // device scalars: iter, flags, vc_max, vc_last
     int *d_int = nullptr;
     float *d_drive = nullptr;                          // [3]: drive P * factor, then the walls' z velocities
@@ -81,16 +104,21 @@ struct rbc_handle {
     float scale = 1.0f, inv_scale = 1.0f;
     std::string err;
     int device = 0;
-    int *patch_off = nullptr, *patch_vtx = nullptr, *patch_stride = nullptr;
-    int npatch = 1;
     AdjointState *adj = nullptr;                      // checkpoints and buffers of the adjoint, on first use
-    // output-interval averages of the load and the principal tensions (fem->qi, fem->tp)
-    int fileoutput = 0;                               // FILEOUTPUT; 0 = not accumulated
-    int mn = 0;                                       // the reference's per-cell vector length (expand2pow2(3 V))
-    double *qi_acc = nullptr, *tp_acc = nullptr;      // [ncell][mn], [ne][2]
+    int fileoutput = 0;                               // FILEOUTPUT of the qi / tp averages; 0 = not accumulated
 
     int kernels_per_step() const {
-        return KERNELS_PER_STEP + (p.br != 0.0 && ncell > 0 ? 1 : 0) + (fileoutput > 0 && ncell > 0 ? 2 : 0) + (ntube > 0 ? 1 : 0);
+        int k = 2 + (ntube > 0 ? 1 : 0);   // step_begin, lbm (+ tube bounce-back)
+        for (int g = 0; g < ngroups; g++) {
+            const CellGroup &c = cg[g];
+            if (c.ncell == 0) continue;
+            k += 4 + (c.br != 0.0 ? 1 : 0) + (fileoutput > 0 ? 2 : 0);   // membrane, spread, advect, volume
+        }
+        return k;
+    }
+    bool has_cells() const {
+        for (int g = 0; g < ngroups; g++) if (cg[g].ncell > 0) return true;
+        return false;
     }
     int *d_iter() { return d_int; }
     int *d_flags() { return d_int + 1; }
@@ -182,10 +210,10 @@ WallVel wall_velocities(const rbc_handle *h, int step)
 // lists in the order add_nlink builds them, vertex -> element lists in element
 // order (add_elink), the reference's link-count check, and the packed
 // incidence entries used by the membrane and volume kernels.
-int build_topology(rbc_handle *h, const int *tri, std::vector<int> &off, std::vector<int> &packed,
+int build_topology(rbc_handle *h, const CellGroup &c, const int *tri, std::vector<int> &off, std::vector<int> &packed,
                    std::vector<int16_t> &nbr6)
 {
-    const int V = h->V, E = h->E;
+    const int V = c.V, E = c.E;
     std::vector<std::vector<int>> nl(V), el(V);
     auto add = [&](int a, int b) {
         for (int x : nl[a]) if (x == b) return;
@@ -232,34 +260,34 @@ int build_topology(rbc_handle *h, const int *tri, std::vector<int> &off, std::ve
 
 // The reference metric of set_contravariant (init2.cu:206-255) on the AoS
 // reference shape, kept in covariant form G [ne] with 1 / det G (the kernel forms n = G^-1)
-void reference_metric(const rbc_handle *h, const int *tri, const double *xr, std::vector<double4> &gref)
+void reference_metric(const CellGroup &g, const int *tri, const double *xr, std::vector<double4> &gref)
 {
-    const long long ne = h->ne;
+    const long long ne = g.ne;
     gref.assign(ne, make_double4(0, 0, 0, 0));
-    for (int c = 0; c < h->ncell; c++)
-        for (int e = 0; e < h->E; e++) {
-            const long long a = (long long)c * h->V + tri[3 * e], b = (long long)c * h->V + tri[3 * e + 1],
-                            cc = (long long)c * h->V + tri[3 * e + 2];
+    for (int c = 0; c < g.ncell; c++)
+        for (int e = 0; e < g.E; e++) {
+            const long long a = (long long)c * g.V + tri[3 * e], b = (long long)c * g.V + tri[3 * e + 1],
+                            cc = (long long)c * g.V + tri[3 * e + 2];
             double v1[3], v2[3];
             for (int j = 0; j < 3; j++) { v1[j] = xr[3 * b + j] - xr[3 * a + j]; v2[j] = xr[3 * cc + j] - xr[3 * a + j]; }
             const double lv1 = v1[0] * v1[0] + v1[1] * v1[1] + v1[2] * v1[2];
             const double lv2 = v2[0] * v2[0] + v2[1] * v2[1] + v2[2] * v2[2];
             const double inv12 = v1[0] * v2[0] + v1[1] * v2[1] + v1[2] * v2[2];
-            const long long id = (long long)c * h->E + e;
+            const long long id = (long long)c * g.E + e;
             gref[id] = make_double4(lv1, inv12, lv2, 1.0 / (lv1 * lv2 - inv12 * inv12));
         }
 }
 
 // volume_init (volume_correction.cu:427-450): V0 and the wrapped centroid
-void initial_volume(const rbc_handle *h, const int *tri, const double *xr, std::vector<double> &vol0,
+void initial_volume(const rbc_handle *h, const CellGroup &g, const int *tri, const double *xr, std::vector<double> &vol0,
                     std::vector<double> &gx)
 {
-    const int N = h->ncell, V = h->V;
+    const int N = g.ncell, V = g.V;
     vol0.assign(N, 0.0);
     gx.assign(3 * N, 0.0);
     for (int c = 0; c < N; c++) {
         double vs = 0.0;
-        for (int e = 0; e < h->E; e++) {
+        for (int e = 0; e < g.E; e++) {
             const double *pa = xr + 3 * ((long long)c * V + tri[3 * e]);
             const double *pb = xr + 3 * ((long long)c * V + tri[3 * e + 1]);
             const double *pc = xr + 3 * ((long long)c * V + tri[3 * e + 2]);
@@ -487,11 +515,13 @@ void free_all(rbc_handle *h)
     if (h->join) cudaEventDestroy(h->join);
     if (h->side) cudaStreamDestroy(h->side);
     void *ptrs[] = {h->g[0], h->g[1], h->uvr, h->Fx, h->Fy, h->Fz, h->mask2d, h->tube_links, h->tube_frac,
-                    h->X, h->Xd, h->gref, h->erec, h->U, h->Fv, h->tri, h->v2e_off, h->v2e, h->nbr, h->visit, h->patch_off, h->patch_vtx, h->patch_stride, h->vol0, h->gx,
-                    h->vol_out, h->area_out, h->cen_out, h->d_int, h->d_drive, h->staging};
+                    h->d_int, h->d_drive, h->staging};
     for (void *q : ptrs) if (q) cudaFree(q);
-    if (h->qi_acc) cudaFree(h->qi_acc);
-    if (h->tp_acc) cudaFree(h->tp_acc);
+    for (CellGroup &c : h->cg) {
+        void *cp[] = {c.X, c.Xd, c.gref, c.erec, c.U, c.Fv, c.tri, c.v2e_off, c.v2e, c.nbr, c.visit, c.patch_off,
+                      c.patch_vtx, c.patch_stride, c.vol0, c.gx, c.vol_out, c.area_out, c.cen_out, c.qi_acc, c.tp_acc};
+        for (void *q : cp) if (q) cudaFree(q);
+    }
     adjoint_free(h->adj);
     h->adj = nullptr;
     if (h->stream) cudaStreamDestroy(h->stream);
@@ -499,57 +529,68 @@ void free_all(rbc_handle *h)
 
 // ---- stage launches -------------------------------------------------------
 
+// stress() (stress.cu:580-660) for every cell population
 int launch_stress(rbc_handle *h)
 {
-    if (h->ncell == 0) return RBC_OK;
-    MembraneArgs a{};
-    a.Xd = h->Xd; a.nv = h->nv; a.ne = h->ne; a.gref = h->gref; a.erec = h->erec;
-    a.tri = h->tri; a.v2e_off = h->v2e_off; a.v2e = h->v2e; a.nbr = h->nbr; a.Fv = h->Fv;
-    a.V = h->V; a.E = h->E; a.ncell = h->ncell;
-    a.C = h->p.C; a.rgs = h->p.rgs; a.law = h->p.law; a.LX = h->p.LX; a.LZ = h->p.LZ;
-    a.niter = h->p.solver_iters > 0 ? h->p.solver_iters : DEFAULT_SOLVER_ITERS;
-    a.flags = h->d_flags();
-    a.priority = h->prio_high;
-    launch_membrane(a, h->p.membrane_fp64 != 0, h->stream);
-    h->launches++;
-    CK_LAUNCH();
-    if (h->fileoutput > 0) {   // calc_tension's tp and substitute_load's qi (stress.cu:101-118, 280-300)
-        AccumArgs c{};
-        c.Xd = h->Xd; c.Fv = h->Fv; c.gref = h->gref; c.tri = h->tri; c.v2e_off = h->v2e_off; c.v2e = h->v2e;
-        c.iter = h->d_iter(); c.qi = h->qi_acc; c.tp = h->tp_acc; c.nv = h->nv; c.ne = h->ne;
-        c.V = h->V; c.E = h->E; c.ncell = h->ncell; c.fileoutput = h->fileoutput; c.M = h->p.M;
-        c.C = h->p.C; c.LX = h->p.LX; c.LZ = h->p.LZ;
-        launch_output_accum(c, h->stream);
-        h->launches += 2;
+    for (int k = 0; k < h->ngroups; k++) {
+        CellGroup &g = h->cg[k];
+        if (g.ncell == 0) continue;
+        MembraneArgs a{};
+        a.Xd = g.Xd; a.nv = g.nv; a.ne = g.ne; a.gref = g.gref; a.erec = g.erec;
+        a.tri = g.tri; a.v2e_off = g.v2e_off; a.v2e = g.v2e; a.nbr = g.nbr; a.Fv = g.Fv;
+        a.V = g.V; a.E = g.E; a.ncell = g.ncell;
+        a.C = h->p.C; a.rgs = g.rgs; a.law = h->p.law; a.LX = h->p.LX; a.LZ = h->p.LZ;
+        a.niter = h->p.solver_iters > 0 ? h->p.solver_iters : DEFAULT_SOLVER_ITERS;
+        a.flags = h->d_flags();
+        a.priority = h->prio_high;
+        launch_membrane(a, h->p.membrane_fp64 != 0, h->stream);
+        h->launches++;
+        CK_LAUNCH();
+        if (h->fileoutput > 0) {   // calc_tension's tp and substitute_load's qi (stress.cu:101-118, 280-300)
+            AccumArgs c{};
+            c.Xd = g.Xd; c.Fv = g.Fv; c.gref = g.gref; c.tri = g.tri; c.v2e_off = g.v2e_off; c.v2e = g.v2e;
+            c.iter = h->d_iter(); c.qi = g.qi_acc; c.tp = g.tp_acc; c.nv = g.nv; c.ne = g.ne;
+            c.V = g.V; c.E = g.E; c.ncell = g.ncell; c.fileoutput = h->fileoutput; c.M = h->p.M;
+            c.C = h->p.C; c.LX = h->p.LX; c.LZ = h->p.LZ;
+            launch_output_accum(c, h->stream);
+            h->launches += 2;
+            CK_LAUNCH();
+        }
+    }
+    return RBC_OK;
+}
+
+// ibm_st1's spreading (ibm.cu:299-369) of every population into the same force field
+int launch_spread_stage(rbc_handle *h)
+{
+    for (int k = 0; k < h->ngroups; k++) {
+        CellGroup &g = h->cg[k];
+        if (g.ncell == 0) continue;
+        SpreadArgs a{};
+        a.X = g.X; a.nv = g.nv; a.V = g.V; a.ncell = g.ncell; a.Fv = g.Fv;
+        a.patch_off = g.patch_off; a.patch_vtx = g.patch_vtx; a.patch_stride = g.patch_stride;
+        a.npatch = g.npatch;
+        a.Fx = h->Fx; a.Fy = h->Fy; a.Fz = h->Fz; a.mask2d = h->mask2d; a.flags = h->d_flags();
+        launch_spread(h->geo, a, h->stream);
+        h->launches++;
         CK_LAUNCH();
     }
     return RBC_OK;
 }
 
-int launch_spread_stage(rbc_handle *h)
-{
-    if (h->ncell == 0) return RBC_OK;
-    SpreadArgs a{};
-    a.X = h->X; a.nv = h->nv; a.V = h->V; a.ncell = h->ncell; a.Fv = h->Fv;
-    a.patch_off = h->patch_off; a.patch_vtx = h->patch_vtx; a.patch_stride = h->patch_stride;
-    a.npatch = h->npatch;
-    a.Fx = h->Fx; a.Fy = h->Fy; a.Fz = h->Fz; a.mask2d = h->mask2d; a.flags = h->d_flags();
-    launch_spread(h->geo, a, h->stream);
-    h->launches++;
-    CK_LAUNCH();
-    return RBC_OK;
-}
-
-// fourpoint_bend (stress.cu:621-623) on cel->x, added to the membrane forces
+// fourpoint_bend (stress.cu:621-623, 650-652) on cel->x, added to the membrane forces
 int launch_bend_stage(rbc_handle *h)
 {
-    if (h->ncell == 0 || h->p.br == 0.0) return RBC_OK;
-    BendArgs a{};
-    a.X = h->X; a.nv = h->nv; a.V = h->V; a.v2e_off = h->v2e_off; a.v2e = h->v2e; a.visit = h->visit;
-    a.LX = h->p.LX; a.LZ = h->p.LZ; a.coef = 2.0 / std::sqrt(3.0) * h->p.br; a.Fv = h->Fv;
-    launch_bend(a, h->stream);
-    h->launches++;
-    CK_LAUNCH();
+    for (int k = 0; k < h->ngroups; k++) {
+        CellGroup &g = h->cg[k];
+        if (g.ncell == 0 || g.br == 0.0) continue;
+        BendArgs a{};
+        a.X = g.X; a.nv = g.nv; a.V = g.V; a.v2e_off = g.v2e_off; a.v2e = g.v2e; a.visit = g.visit;
+        a.LX = h->p.LX; a.LZ = h->p.LZ; a.coef = 2.0 / std::sqrt(3.0) * g.br; a.Fv = g.Fv;
+        launch_bend(a, h->stream);
+        h->launches++;
+        CK_LAUNCH();
+    }
     return RBC_OK;
 }
 
@@ -575,37 +616,45 @@ int launch_lbm_stage(rbc_handle *h)
     return RBC_OK;
 }
 
+// ibm_st2 (ibm.cu:642-694) for every population
 int launch_advect_stage(rbc_handle *h)
 {
-    if (h->ncell == 0) return RBC_OK;
-    AdvectArgs a{};
-    a.X = h->X; a.Xd = h->Xd; a.U = h->U; a.uvr = h->uvr; a.nv = h->nv;
-    a.V = h->V; a.ncell = h->ncell; a.patch_off = h->patch_off; a.patch_vtx = h->patch_vtx; a.npatch = h->npatch;
-    a.dtM = h->p.dt * h->p.M; a.flags = h->d_flags();
-    launch_advect(h->geo, a, h->stream);
-    h->launches++;
-    CK_LAUNCH();
+    for (int k = 0; k < h->ngroups; k++) {
+        CellGroup &g = h->cg[k];
+        if (g.ncell == 0) continue;
+        AdvectArgs a{};
+        a.X = g.X; a.Xd = g.Xd; a.U = g.U; a.uvr = h->uvr; a.nv = g.nv;
+        a.V = g.V; a.ncell = g.ncell; a.patch_off = g.patch_off; a.patch_vtx = g.patch_vtx; a.npatch = g.npatch;
+        a.dtM = h->p.dt * h->p.M; a.flags = h->d_flags();
+        launch_advect(h->geo, a, h->stream);
+        h->launches++;
+        CK_LAUNCH();
+    }
     return RBC_OK;
 }
 
-VolumeArgs volume_args(rbc_handle *h, int correct)
+VolumeArgs volume_args(rbc_handle *h, CellGroup &g, int correct)
 {
     VolumeArgs a{};
-    a.X = h->X; a.nv = h->nv; a.tri = h->tri; a.v2e_off = h->v2e_off; a.v2e = h->v2e;
-    a.vol0 = h->vol0; a.gx = h->gx; a.vol_out = h->vol_out; a.area_out = h->area_out; a.cen_out = h->cen_out;
-    a.V = h->V; a.E = h->E; a.ncell = h->ncell;
+    a.X = g.X; a.nv = g.nv; a.tri = g.tri; a.v2e_off = g.v2e_off; a.v2e = g.v2e;
+    a.vol0 = g.vol0; a.gx = g.gx; a.vol_out = g.vol_out; a.area_out = g.area_out; a.cen_out = g.cen_out;
+    a.V = g.V; a.E = g.E; a.ncell = g.ncell;
     a.flags = h->d_flags(); a.vc_max = h->d_vcmax(); a.vc_last = h->d_vclast();
     a.correct = correct;
     return a;
 }
 
+// volume_correction (volume_correction.cu:453-524, both populations) on stream st
 int launch_volume_stage(rbc_handle *h, cudaStream_t st)
 {
-    if (h->ncell == 0) return RBC_OK;
+    if (!h->has_cells()) return RBC_OK;
     CK(cudaMemsetAsync(h->d_vclast(), 0, sizeof(int), st));
-    launch_volume(h->geo, volume_args(h, 1), st);
-    h->launches++;
-    CK_LAUNCH();
+    for (int k = 0; k < h->ngroups; k++) {
+        if (h->cg[k].ncell == 0) continue;
+        launch_volume(h->geo, volume_args(h, h->cg[k], 1), st);
+        h->launches++;
+        CK_LAUNCH();
+    }
     return RBC_OK;
 }
 
@@ -757,6 +806,91 @@ int batch_build(rbc_batch *b)
     return RBC_OK;
 }
 
+// Host-side setup of one cell population from its mesh (init2.cu:258-400,
+// volume_correction.cu:427-450): link tables, reference metric, V0 and
+// centroids, surface patches, bending visits.
+struct GroupPrep {
+    std::vector<int> off, packed, poff, pvtx, pstride;
+    std::vector<int16_t> nbr6;
+    std::vector<double> vol0, gx, xs;
+    std::vector<double4> gref;
+    std::vector<int4> visit;
+};
+
+int prepare_group(rbc_handle *h, CellGroup &c, const rbc_mesh *mesh, GroupPrep &pp)
+{
+    c.ncell = mesh->ncell; c.V = mesh->vertex; c.E = mesh->element;
+    c.nv = (long long)c.ncell * c.V; c.ne = (long long)c.ncell * c.E;
+    int rc = build_topology(h, c, mesh->tri, pp.off, pp.packed, pp.nbr6);
+    if (rc) return rc;
+    surface_patches(c.V, mesh->xr, pp.poff, pp.pvtx, pp.pstride);
+    c.npatch = (int)pp.poff.size() - 1;
+    reference_metric(c, mesh->tri, mesh->xr, pp.gref);
+    initial_volume(h, c, mesh->tri, mesh->xr, pp.vol0, pp.gx);
+    pp.xs.resize(3 * c.nv);
+    for (long long j = 0; j < c.nv; j++)
+        for (int k = 0; k < 3; k++) pp.xs[k * c.nv + j] = mesh->xr[3 * j + k];
+    if (c.br != 0.0) bend_visits(c.V, c.E, mesh->tri, pp.visit);
+    return RBC_OK;
+}
+
+// device arrays of one cell population
+int upload_group(rbc_handle *h, CellGroup &c, const rbc_mesh *mesh, const GroupPrep &pp)
+{
+    int rc;
+#define TRYG(x) do { if ((rc = (x))) return rc; } while (0)
+    TRYG(dalloc(h, &c.X, 3 * c.nv)); TRYG(dalloc(h, &c.Xd, 3 * c.nv)); TRYG(dalloc(h, &c.gref, c.ne));
+    CK(cudaMalloc(&c.erec, (size_t)c.ne * 12 * (h->p.membrane_fp64 ? sizeof(double) : sizeof(float))));
+    TRYG(dalloc(h, &c.U, 3 * c.nv)); TRYG(dalloc(h, &c.Fv, 3 * c.nv));
+    TRYG(dalloc(h, &c.tri, 3 * c.E)); TRYG(dalloc(h, &c.v2e_off, c.V + 1)); TRYG(dalloc(h, &c.v2e, pp.packed.size()));
+    TRYG(dalloc(h, &c.nbr, 6 * c.V));
+    if (!pp.visit.empty()) {
+        TRYG(dalloc(h, &c.visit, pp.visit.size()));
+        CK(cudaMemcpy(c.visit, pp.visit.data(), sizeof(int4) * pp.visit.size(), cudaMemcpyHostToDevice));
+    }
+    TRYG(dalloc(h, &c.patch_off, pp.poff.size())); TRYG(dalloc(h, &c.patch_vtx, pp.pvtx.size()));
+    TRYG(dalloc(h, &c.patch_stride, pp.pstride.size()));
+    TRYG(dalloc(h, &c.vol0, c.ncell)); TRYG(dalloc(h, &c.gx, 3 * c.ncell));
+    TRYG(dalloc(h, &c.vol_out, c.ncell)); TRYG(dalloc(h, &c.area_out, c.ncell)); TRYG(dalloc(h, &c.cen_out, 3 * c.ncell));
+#undef TRYG
+    CK(cudaMemcpy(c.X, pp.xs.data(), 8 * 3 * c.nv, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c.Xd, pp.xs.data(), 8 * 3 * c.nv, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c.gref, pp.gref.data(), sizeof(double4) * c.ne, cudaMemcpyHostToDevice));
+    CK(cudaMemset(c.U, 0, 4 * 3 * c.nv));
+    CK(cudaMemset(c.Fv, 0, 4 * 3 * c.nv));
+    CK(cudaMemcpy(c.tri, mesh->tri, 4 * 3 * c.E, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c.v2e_off, pp.off.data(), 4 * (c.V + 1), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c.v2e, pp.packed.data(), 4 * pp.packed.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c.nbr, pp.nbr6.data(), 2 * 6 * c.V, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c.patch_off, pp.poff.data(), 4 * pp.poff.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c.patch_vtx, pp.pvtx.data(), 4 * pp.pvtx.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c.patch_stride, pp.pstride.data(), 4 * pp.pstride.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c.vol0, pp.vol0.data(), 8 * c.ncell, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c.gx, pp.gx.data(), 8 * 3 * c.ncell, cudaMemcpyHostToDevice));
+    return RBC_OK;
+}
+
+// volume, area, centroid of the cells of population g (synchronous)
+int group_metrics(rbc_handle *h, CellGroup &g, double *volume, double *area, double *centroid)
+{
+    if (g.ncell == 0) return fail(h, RBC_ERR_STATE, "no cells in this population");
+    launch_volume(h->geo, volume_args(h, g, 0), h->stream);
+    h->launches++;
+    CK_LAUNCH();
+    const int N = g.ncell;
+    std::vector<double> t(5 * N);
+    CK(cudaMemcpyAsync(t.data(), g.vol_out, 8 * N, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(t.data() + N, g.area_out, 8 * N, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(t.data() + 2 * N, g.cen_out, 8 * 3 * N, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    for (int c = 0; c < N; c++) {
+        if (volume) volume[c] = t[c];
+        if (area) area[c] = t[N + c];
+        if (centroid) for (int k = 0; k < 3; k++) centroid[3 * c + k] = t[(2 + k) * N + c];
+    }
+    return RBC_OK;
+}
+
 }  // namespace
 
 // ===========================================================================
@@ -814,23 +948,10 @@ int rbc_create(const rbc_params *p, const rbc_mesh *mesh, const int *bc, rbc_han
     };
 #define TRY(x) do { int r_ = (x); if (r_) return bail(r_); } while (0)
     // host-side setup first, so argument and mesh errors are reported without a GPU
-    std::vector<int> off, packed;
-    std::vector<int16_t> nbr6;
-    std::vector<double> vol0, gx, xs;
-    std::vector<double4> gref;
-    std::vector<int> poff, pvtx, pstride;
-    if (cells) {
-        h->ncell = mesh->ncell; h->V = mesh->vertex; h->E = mesh->element;
-        h->nv = (long long)h->ncell * h->V; h->ne = (long long)h->ncell * h->E;
-        TRY(build_topology(h, mesh->tri, off, packed, nbr6));
-        surface_patches(h->V, mesh->xr, poff, pvtx, pstride);
-        h->npatch = (int)poff.size() - 1;
-        reference_metric(h, mesh->tri, mesh->xr, gref);
-        initial_volume(h, mesh->tri, mesh->xr, vol0, gx);
-        xs.resize(3 * h->nv);
-        for (long long j = 0; j < h->nv; j++)
-            for (int k = 0; k < 3; k++) xs[k * h->nv + j] = mesh->xr[3 * j + k];
-    }
+    GroupPrep prep;
+    h->cg[0].rgs = p->rgs;
+    h->cg[0].br = p->br;
+    if (cells) TRY(prepare_group(h, h->cg[0], mesh, prep));
     {
         int ndev = 0;
         if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
@@ -927,45 +1048,7 @@ int rbc_create(const rbc_params *p, const rbc_mesh *mesh, const int *bc, rbc_han
                               wall_velocities(h, 1), h->stream);
     }
 
-    if (cells) {
-        TRY(dalloc(h, &h->X, 3 * h->nv)); TRY(dalloc(h, &h->Xd, 3 * h->nv)); TRY(dalloc(h, &h->gref, h->ne));
-        if (cudaMalloc(&h->erec, (size_t)h->ne * 12 * (p->membrane_fp64 ? sizeof(double) : sizeof(float))) != cudaSuccess) {
-            h->err = "out of device memory for the membrane element records";
-            return bail(RBC_ERR_CUDA);
-        }
-        TRY(dalloc(h, &h->U, 3 * h->nv)); TRY(dalloc(h, &h->Fv, 3 * h->nv));
-        TRY(dalloc(h, &h->tri, 3 * h->E)); TRY(dalloc(h, &h->v2e_off, h->V + 1)); TRY(dalloc(h, &h->v2e, packed.size()));
-        TRY(dalloc(h, &h->nbr, 6 * h->V));
-        if (p->br != 0.0) {
-            std::vector<int4> visit;
-            bend_visits(h->V, h->E, mesh->tri, visit);
-            TRY(dalloc(h, &h->visit, visit.size()));
-            if (cudaMemcpy(h->visit, visit.data(), sizeof(int4) * visit.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
-                h->err = "device initialisation failed";
-                return bail(RBC_ERR_CUDA);
-            }
-        }
-        TRY(dalloc(h, &h->patch_off, poff.size())); TRY(dalloc(h, &h->patch_vtx, pvtx.size()));
-        TRY(dalloc(h, &h->patch_stride, pstride.size()));
-        TRY(dalloc(h, &h->vol0, h->ncell)); TRY(dalloc(h, &h->gx, 3 * h->ncell));
-        TRY(dalloc(h, &h->vol_out, h->ncell)); TRY(dalloc(h, &h->area_out, h->ncell)); TRY(dalloc(h, &h->cen_out, 3 * h->ncell));
-        if (cudaMemcpy(h->X, xs.data(), 8 * 3 * h->nv, cudaMemcpyHostToDevice) != cudaSuccess ||
-            cudaMemcpy(h->Xd, xs.data(), 8 * 3 * h->nv, cudaMemcpyHostToDevice) != cudaSuccess ||
-            cudaMemcpy(h->gref, gref.data(), sizeof(double4) * h->ne, cudaMemcpyHostToDevice) != cudaSuccess ||
-            cudaMemset(h->U, 0, 4 * 3 * h->nv) != cudaSuccess || cudaMemset(h->Fv, 0, 4 * 3 * h->nv) != cudaSuccess ||
-            cudaMemcpy(h->tri, mesh->tri, 4 * 3 * h->E, cudaMemcpyHostToDevice) != cudaSuccess ||
-            cudaMemcpy(h->v2e_off, off.data(), 4 * (h->V + 1), cudaMemcpyHostToDevice) != cudaSuccess ||
-            cudaMemcpy(h->v2e, packed.data(), 4 * packed.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
-            cudaMemcpy(h->nbr, nbr6.data(), 2 * 6 * h->V, cudaMemcpyHostToDevice) != cudaSuccess ||
-            cudaMemcpy(h->patch_off, poff.data(), 4 * poff.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
-            cudaMemcpy(h->patch_vtx, pvtx.data(), 4 * pvtx.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
-            cudaMemcpy(h->patch_stride, pstride.data(), 4 * pstride.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
-            cudaMemcpy(h->vol0, vol0.data(), 8 * h->ncell, cudaMemcpyHostToDevice) != cudaSuccess ||
-            cudaMemcpy(h->gx, gx.data(), 8 * 3 * h->ncell, cudaMemcpyHostToDevice) != cudaSuccess) {
-            h->err = "cell upload failed";
-            return bail(RBC_ERR_CUDA);
-        }
-    }
+    if (cells) TRY(upload_group(h, h->cg[0], mesh, prep));
     if (cudaStreamSynchronize(h->stream) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
         h->err = "initialisation kernels failed";
         return bail(RBC_ERR_CUDA);
@@ -1043,38 +1126,45 @@ int rbc_export_ref_force(rbc_handle *h, double *fx, double *fy, double *fz)
     return RBC_OK;
 }
 
+static int import_cells(rbc_handle *h, CellGroup &G, const double *x, const double *y, const double *z,
+                        const double *xd, const double *nd, const double *volume0, const double *gx)
+{
+    if (!h) return RBC_ERR_ARG;
+    RBC_DEVICE_GUARD(h);
+    if (G.ncell == 0) return fail(h, RBC_ERR_STATE, "no cells in this population");
+    const long long nv = G.nv, ne = G.ne;
+    const int N = G.ncell;
+    CK(cudaStreamSynchronize(h->stream));
+    if (x) CK(cudaMemcpy(G.X, x, 8 * nv, cudaMemcpyHostToDevice));
+    if (y) CK(cudaMemcpy(G.X + nv, y, 8 * nv, cudaMemcpyHostToDevice));
+    if (z) CK(cudaMemcpy(G.X + 2 * nv, z, 8 * nv, cudaMemcpyHostToDevice));
+    if (xd) {
+        std::vector<double> t(3 * nv);
+        for (long long j = 0; j < nv; j++) for (int k = 0; k < 3; k++) t[k * nv + j] = xd[3 * j + k];
+        CK(cudaMemcpy(G.Xd, t.data(), 8 * 3 * nv, cudaMemcpyHostToDevice));
+    }
+    if (nd) {
+        std::vector<double4> gm(ne);
+        for (long long e = 0; e < ne; e++) {
+            const double n00 = nd[4 * e], n01 = nd[4 * e + 1], n11 = nd[4 * e + 3], det = n00 * n11 - n01 * n01;
+            gm[e] = make_double4(n11 / det, -n01 / det, n00 / det, det);   // G = n^-1, 1 / det G = det n
+        }
+        CK(cudaMemcpy(G.gref, gm.data(), sizeof(double4) * ne, cudaMemcpyHostToDevice));
+    }
+    if (volume0) CK(cudaMemcpy(G.vol0, volume0, 8 * N, cudaMemcpyHostToDevice));
+    if (gx) {
+        std::vector<double> t(3 * N);
+        for (int c = 0; c < N; c++) for (int k = 0; k < 3; k++) t[k * N + c] = gx[3 * c + k];
+        CK(cudaMemcpy(G.gx, t.data(), 8 * 3 * N, cudaMemcpyHostToDevice));
+    }
+    return RBC_OK;
+}
+
 int rbc_import_ref_cells(rbc_handle *h, const double *x, const double *y, const double *z,
                          const double *xd, const double *nd, const double *volume0, const double *gx)
 {
     if (!h) return RBC_ERR_ARG;
-    RBC_DEVICE_GUARD(h);
-    if (h->ncell == 0) return fail(h, RBC_ERR_STATE, "handle has no cells");
-    const long long nv = h->nv, ne = h->ne;
-    const int N = h->ncell;
-    CK(cudaStreamSynchronize(h->stream));
-    if (x) CK(cudaMemcpy(h->X, x, 8 * nv, cudaMemcpyHostToDevice));
-    if (y) CK(cudaMemcpy(h->X + nv, y, 8 * nv, cudaMemcpyHostToDevice));
-    if (z) CK(cudaMemcpy(h->X + 2 * nv, z, 8 * nv, cudaMemcpyHostToDevice));
-    if (xd) {
-        std::vector<double> t(3 * nv);
-        for (long long j = 0; j < nv; j++) for (int k = 0; k < 3; k++) t[k * nv + j] = xd[3 * j + k];
-        CK(cudaMemcpy(h->Xd, t.data(), 8 * 3 * nv, cudaMemcpyHostToDevice));
-    }
-    if (nd) {
-        std::vector<double4> G(ne);
-        for (long long e = 0; e < ne; e++) {
-            const double n00 = nd[4 * e], n01 = nd[4 * e + 1], n11 = nd[4 * e + 3], det = n00 * n11 - n01 * n01;
-            G[e] = make_double4(n11 / det, -n01 / det, n00 / det, det);   // G = n^-1, 1 / det G = det n
-        }
-        CK(cudaMemcpy(h->gref, G.data(), sizeof(double4) * ne, cudaMemcpyHostToDevice));
-    }
-    if (volume0) CK(cudaMemcpy(h->vol0, volume0, 8 * N, cudaMemcpyHostToDevice));
-    if (gx) {
-        std::vector<double> t(3 * N);
-        for (int c = 0; c < N; c++) for (int k = 0; k < 3; k++) t[k * N + c] = gx[3 * c + k];
-        CK(cudaMemcpy(h->gx, t.data(), 8 * 3 * N, cudaMemcpyHostToDevice));
-    }
-    return RBC_OK;
+    return import_cells(h, h->cg[0], x, y, z, xd, nd, volume0, gx);
 }
 
 int rbc_import_ref_vertex_force(rbc_handle *h, const double *fx, const double *fy, const double *fz)
@@ -1090,37 +1180,44 @@ int rbc_import_ref_vertex_force(rbc_handle *h, const double *fx, const double *f
     return RBC_OK;
 }
 
-int rbc_export_ref_cells(rbc_handle *h, double *x, double *y, double *z, double *xd,
-                         double *u, double *v, double *w, double *fx, double *fy, double *fz, double *gxo)
+static int export_cells(rbc_handle *h, CellGroup &G, double *x, double *y, double *z, double *xd,
+                        double *u, double *v, double *w, double *fx, double *fy, double *fz, double *gxo)
 {
     if (!h) return RBC_ERR_ARG;
     RBC_DEVICE_GUARD(h);
-    if (h->ncell == 0) return fail(h, RBC_ERR_STATE, "handle has no cells");
-    const long long nv = h->nv;
-    const int N = h->ncell;
+    if (G.ncell == 0) return fail(h, RBC_ERR_STATE, "no cells in this population");
+    const long long nv = G.nv;
+    const int N = G.ncell;
     CK(cudaStreamSynchronize(h->stream));
-    if (x) CK(cudaMemcpy(x, h->X, 8 * nv, cudaMemcpyDeviceToHost));
-    if (y) CK(cudaMemcpy(y, h->X + nv, 8 * nv, cudaMemcpyDeviceToHost));
-    if (z) CK(cudaMemcpy(z, h->X + 2 * nv, 8 * nv, cudaMemcpyDeviceToHost));
+    if (x) CK(cudaMemcpy(x, G.X, 8 * nv, cudaMemcpyDeviceToHost));
+    if (y) CK(cudaMemcpy(y, G.X + nv, 8 * nv, cudaMemcpyDeviceToHost));
+    if (z) CK(cudaMemcpy(z, G.X + 2 * nv, 8 * nv, cudaMemcpyDeviceToHost));
     if (xd) {
         std::vector<double> t(3 * nv);
-        CK(cudaMemcpy(t.data(), h->Xd, 8 * 3 * nv, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(t.data(), G.Xd, 8 * 3 * nv, cudaMemcpyDeviceToHost));
         for (long long j = 0; j < nv; j++) for (int k = 0; k < 3; k++) xd[3 * j + k] = t[k * nv + j];
     }
     if (u || v || w || fx || fy || fz) {
         std::vector<float> t(6 * nv);
-        CK(cudaMemcpy(t.data(), h->U, 4 * 3 * nv, cudaMemcpyDeviceToHost));
-        CK(cudaMemcpy(t.data() + 3 * nv, h->Fv, 4 * 3 * nv, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(t.data(), G.U, 4 * 3 * nv, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(t.data() + 3 * nv, G.Fv, 4 * 3 * nv, cudaMemcpyDeviceToHost));
         double *outs[6] = {u, v, w, fx, fy, fz};
         for (int k = 0; k < 6; k++)
             if (outs[k]) for (long long j = 0; j < nv; j++) outs[k][j] = t[k * nv + j];
     }
     if (gxo) {
         std::vector<double> t(3 * N);
-        CK(cudaMemcpy(t.data(), h->gx, 8 * 3 * N, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(t.data(), G.gx, 8 * 3 * N, cudaMemcpyDeviceToHost));
         for (int c = 0; c < N; c++) for (int k = 0; k < 3; k++) gxo[3 * c + k] = t[k * N + c];
     }
     return RBC_OK;
+}
+
+int rbc_export_ref_cells(rbc_handle *h, double *x, double *y, double *z, double *xd,
+                         double *u, double *v, double *w, double *fx, double *fy, double *fz, double *gxo)
+{
+    if (!h) return RBC_ERR_ARG;
+    return export_cells(h, h->cg[0], x, y, z, xd, u, v, w, fx, fy, fz, gxo);
 }
 
 int rbc_set_iter(rbc_handle *h, int iter)
@@ -1192,7 +1289,7 @@ int rbc_volume_correction(rbc_handle *h, int *iters)
     if (rc) return rc;
     if (iters) {
         int v = 0;
-        if (h->ncell > 0) {
+        if (h->has_cells()) {
             CK(cudaMemcpyAsync(&v, h->d_vclast(), sizeof(int), cudaMemcpyDeviceToHost, h->stream));
             CK(cudaStreamSynchronize(h->stream));
         }
@@ -1211,7 +1308,7 @@ int rbc_step(rbc_handle *h, int nsteps)
     // one step, or no cells: whole steps.  Otherwise step 1 without its
     // correction, steps 2..n pipelined with the correction of the step before,
     // then the correction of step n: the same kernels in the same data order.
-    const bool pipe = nsteps > 1 && h->ncell > 0;
+    const bool pipe = nsteps > 1 && h->has_cells();
     for (int c = 0; c < 2; c++) {
         if (!h->graph[STEP_WHOLE][c] && (rc = build_graph(h, c, STEP_WHOLE))) return rc;
         if (pipe && !h->graph[STEP_BODY][c] && (rc = build_graph(h, c, STEP_BODY))) return rc;
@@ -1224,7 +1321,8 @@ int rbc_step(rbc_handle *h, int nsteps)
         h->launches += h->kernels_per_step();
     }
     if (pipe) {
-        h->launches -= 1;   // step n's correction, counted with its step, is launched here
+        for (int k = 0; k < h->ngroups; k++)   // step n's corrections, counted with its step, are launched here
+            h->launches -= h->cg[k].ncell > 0 ? 1 : 0;
         if ((rc = launch_volume_stage(h, h->stream))) return rc;
     }
     h->iter += nsteps;
@@ -1293,21 +1391,7 @@ int rbc_cell_metrics(rbc_handle *h, double *volume, double *area, double *centro
     if (!h) return RBC_ERR_ARG;
     RBC_DEVICE_GUARD(h);
     if (h->ncell == 0) return fail(h, RBC_ERR_STATE, "handle has no cells");
-    launch_volume(h->geo, volume_args(h, 0), h->stream);
-    h->launches++;
-    CK_LAUNCH();
-    const int N = h->ncell;
-    std::vector<double> t(5 * N);
-    CK(cudaMemcpyAsync(t.data(), h->vol_out, 8 * N, cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaMemcpyAsync(t.data() + N, h->area_out, 8 * N, cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaMemcpyAsync(t.data() + 2 * N, h->cen_out, 8 * 3 * N, cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaStreamSynchronize(h->stream));
-    for (int c = 0; c < N; c++) {
-        if (volume) volume[c] = t[c];
-        if (area) area[c] = t[N + c];
-        if (centroid) for (int k = 0; k < 3; k++) centroid[3 * c + k] = t[(2 + k) * N + c];
-    }
-    return RBC_OK;
+    return group_metrics(h, h->cg[0], volume, area, centroid);
 }
 
 int rbc_synchronize(rbc_handle *h)
@@ -1730,7 +1814,7 @@ int adjoint_enqueue_reverse(rbc_handle *h, int b, int len, int gb)
             ma.lam = a->lam; ma.qv = a->qv; ma.dsb = a->dsb;
             ma.cbar = a->pbar + 2;
             ma.V = h->V; ma.E = h->E; ma.ncell = h->ncell;
-            ma.C = h->p.C; ma.rgs = h->p.rgs; ma.law = h->p.law; ma.LX = h->p.LX; ma.LZ = h->p.LZ;
+            ma.C = h->p.C; ma.rgs = h->cg[0].rgs; ma.law = h->p.law; ma.LX = h->p.LX; ma.LZ = h->p.LZ;
             ma.niter = h->p.solver_iters > 0 ? h->p.solver_iters : DEFAULT_SOLVER_ITERS;
             launch_membrane_adjoint(ma, st);
             CK_LAUNCH();
@@ -1777,7 +1861,8 @@ int adjoint_launch_graph(rbc_handle *h, int kind, int b, int parity, int len)
 int adjoint_supported(rbc_handle *h)
 {
     if (h->p.storage != RBC_STORE_F32) return fail(h, RBC_ERR_UNSUPPORTED, "the adjoint needs FP32 population storage");
-    if (h->p.br != 0.0) return fail(h, RBC_ERR_UNSUPPORTED, "the adjoint does not cover bending (BR != 0)");
+    if (h->cg[0].br != 0.0) return fail(h, RBC_ERR_UNSUPPORTED, "the adjoint does not cover bending (BR != 0)");
+    if (h->ngroups > 1) return fail(h, RBC_ERR_UNSUPPORTED, "the adjoint covers one cell population (no white cells)");
     if (h->geo.nzc > 65535) return fail(h, RBC_ERR_UNSUPPORTED, "the adjoint handles at most 65535 periodic planes");
     if (h->p.flow != RBC_FLOW_CHANNEL) return fail(h, RBC_ERR_UNSUPPORTED, "the adjoint covers the channel mode only");
     if (h->ntube > 0) return fail(h, RBC_ERR_UNSUPPORTED, "the adjoint covers half-way bounce-back walls only (tube_r = 0)");
@@ -1929,14 +2014,15 @@ int reference_mn(int V)
     return 1 << cnt;
 }
 
-// fem->qi [ncell * mn] and fem->tp [2 ne] to (set = false) or from (set = true)
-// host arrays; zeros when no output interval is set
-int output_averages(rbc_handle *h, double *qi, double *tp, bool set)
+// fem->qi [ncell * mn] and fem->tp [2 ne] of population `group` to (set = false)
+// or from (set = true) host arrays; zeros when no output interval is set
+int output_averages(rbc_handle *h, int group, double *qi, double *tp, bool set)
 {
     RBC_DEVICE_GUARD(h);
-    const size_t nq = (size_t)h->ncell * h->mn, nt = 2 * (size_t)h->ne;
+    CellGroup &g = h->cg[group];
+    const size_t nq = (size_t)g.ncell * reference_mn(g.V), nt = 2 * (size_t)g.ne;
     CK(cudaStreamSynchronize(h->stream));
-    if (!h->qi_acc) {
+    if (!g.qi_acc) {
         if (!set) {
             if (qi) std::fill(qi, qi + nq, 0.0);
             if (tp) std::fill(tp, tp + nt, 0.0);
@@ -1944,11 +2030,11 @@ int output_averages(rbc_handle *h, double *qi, double *tp, bool set)
         return RBC_OK;
     }
     if (set) {
-        if (qi) CK(cudaMemcpy(h->qi_acc, qi, 8 * nq, cudaMemcpyHostToDevice));
-        if (tp) CK(cudaMemcpy(h->tp_acc, tp, 8 * nt, cudaMemcpyHostToDevice));
+        if (qi) CK(cudaMemcpy(g.qi_acc, qi, 8 * nq, cudaMemcpyHostToDevice));
+        if (tp) CK(cudaMemcpy(g.tp_acc, tp, 8 * nt, cudaMemcpyHostToDevice));
     } else {
-        if (qi) CK(cudaMemcpy(qi, h->qi_acc, 8 * nq, cudaMemcpyDeviceToHost));
-        if (tp) CK(cudaMemcpy(tp, h->tp_acc, 8 * nt, cudaMemcpyDeviceToHost));
+        if (qi) CK(cudaMemcpy(qi, g.qi_acc, 8 * nq, cudaMemcpyDeviceToHost));
+        if (tp) CK(cudaMemcpy(tp, g.tp_acc, 8 * nt, cudaMemcpyDeviceToHost));
     }
     return RBC_OK;
 }
@@ -1975,13 +2061,22 @@ int reference_bc(rbc_handle *h, int *bc)
     return RBC_OK;
 }
 
-int reference_ele(rbc_handle *h, int *ele)
+int reference_ele(rbc_handle *h, int group, int *ele)
 {
     RBC_DEVICE_GUARD(h);
-    std::vector<int> tri(3 * (size_t)h->E);
-    if (h->E > 0) CK(cudaMemcpy(tri.data(), h->tri, 4 * tri.size(), cudaMemcpyDeviceToHost));
-    for (int c = 0; c < h->ncell; c++)
-        for (size_t k = 0; k < tri.size(); k++) ele[(size_t)c * tri.size() + k] = tri[k] + c * h->V;
+    const CellGroup &g = h->cg[group];
+    std::vector<int> tri(3 * (size_t)g.E);
+    if (g.E > 0) CK(cudaMemcpy(tri.data(), g.tri, 4 * tri.size(), cudaMemcpyDeviceToHost));
+    for (int c = 0; c < g.ncell; c++)
+        for (size_t k = 0; k < tri.size(); k++) ele[(size_t)c * tri.size() + k] = tri[k] + c * g.V;
+    return RBC_OK;
+}
+
+int group_sizes(const rbc_handle *h, int group, int *ncell, int *vertex, int *element)
+{
+    const CellGroup &g = h->cg[group];
+    if (group >= h->ngroups) { *ncell = *vertex = *element = 0; return RBC_OK; }
+    *ncell = g.ncell; *vertex = g.V; *element = g.E;
     return RBC_OK;
 }
 
@@ -1997,19 +2092,100 @@ extern "C" int rbc_set_output_interval(rbc_handle *h, int fileoutput)
     if (!h || fileoutput < 0) return RBC_ERR_ARG;
     RBC_DEVICE_GUARD(h);
     CK(cudaStreamSynchronize(h->stream));
-    if (fileoutput > 0 && h->ncell > 0 && !h->qi_acc) {
-        h->mn = reference_mn(h->V);
-        const size_t nq = (size_t)h->ncell * h->mn, nt = 2 * (size_t)h->ne;
-        CK(cudaMalloc(&h->qi_acc, 8 * nq));
-        CK(cudaMalloc(&h->tp_acc, 8 * nt));
-        CK(cudaMemset(h->qi_acc, 0, 8 * nq));   // as fem_init leaves fem->qi (init2.cu:310)
-        CK(cudaMemset(h->tp_acc, 0, 8 * nt));
+    for (int k = 0; k < h->ngroups; k++) {
+        CellGroup &g = h->cg[k];
+        if (fileoutput <= 0 || g.ncell == 0 || g.qi_acc) continue;
+        g.mn = reference_mn(g.V);
+        const size_t nq = (size_t)g.ncell * g.mn, nt = 2 * (size_t)g.ne;
+        CK(cudaMalloc(&g.qi_acc, 8 * nq));
+        CK(cudaMalloc(&g.tp_acc, 8 * nt));
+        CK(cudaMemset(g.qi_acc, 0, 8 * nq));   // as fem_init leaves fem->qi (init2.cu:310)
+        CK(cudaMemset(g.tp_acc, 0, 8 * nt));
     }
     if (fileoutput != h->fileoutput) {
-        h->fileoutput = h->ncell > 0 ? fileoutput : 0;
+        h->fileoutput = fileoutput;
         // the step graphs hold the accumulation launches (or not)
         for (auto &form : h->graph)
             for (cudaGraphExec_t &g : form) if (g) { cudaGraphExecDestroy(g); g = nullptr; }
     }
     return RBC_OK;
 }
+
+// ---- white cells (init3.cu) -------------------------------------------------
+
+extern "C" {
+
+int rbc_add_wbc(rbc_handle *h, const rbc_mesh *mesh, double rgs, double br)
+{
+    if (!h || !mesh || mesh->ncell <= 0) return RBC_ERR_ARG;
+    RBC_DEVICE_GUARD(h);
+    if (h->ngroups > 1) return fail(h, RBC_ERR_STATE, "the white cells are already set");
+    if (mesh->vertex < 4 || mesh->element < 4 || !mesh->tri || !mesh->xr)
+        return fail(h, RBC_ERR_ARG, "mesh needs vertex, element >= 4, tri and xr");
+    if (membrane_smem_bytes(mesh->vertex) > 227 * 1024 || mesh->vertex > 4096)
+        return fail(h, RBC_ERR_UNSUPPORTED, "more vertices per cell than one CTA holds (max 3874)");
+    if (mesh->element >= (1 << 24)) return fail(h, RBC_ERR_UNSUPPORTED, "too many elements per cell");
+    if (!(rgs > 0.0) || !std::isfinite(rgs) || !std::isfinite(br)) return fail(h, RBC_ERR_ARG, "rgs must be > 0 and br finite");
+    CK(cudaStreamSynchronize(h->stream));
+    CellGroup &c = h->cg[1];
+    c.rgs = rgs;
+    c.br = br;
+    GroupPrep prep;
+    int rc = prepare_group(h, c, mesh, prep);
+    if (!rc) rc = upload_group(h, c, mesh, prep);
+    if (rc) {   // leave the handle with the red cells only
+        void *cp[] = {c.X, c.Xd, c.gref, c.erec, c.U, c.Fv, c.tri, c.v2e_off, c.v2e, c.nbr, c.visit, c.patch_off,
+                      c.patch_vtx, c.patch_stride, c.vol0, c.gx, c.vol_out, c.area_out, c.cen_out};
+        for (void *q : cp) if (q) cudaFree(q);
+        c = CellGroup{};
+        return rc;
+    }
+    h->ngroups = 2;
+    if (h->fileoutput > 0) {
+        const int f = h->fileoutput;
+        h->fileoutput = 0;
+        if ((rc = rbc_set_output_interval(h, f))) return rc;
+    }
+    // the step graphs and the adjoint hold one population
+    for (auto &form : h->graph)
+        for (cudaGraphExec_t &g : form) if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    if (h->adj) h->adj->valid = false;
+    return RBC_OK;
+}
+
+int rbc_wbc_dims(const rbc_handle *h, int *ncell, int *vertex, int *element)
+{
+    if (!h) return RBC_ERR_ARG;
+    int n = 0, v = 0, e = 0;
+    group_sizes(h, 1, &n, &v, &e);
+    if (ncell) *ncell = n;
+    if (vertex) *vertex = v;
+    if (element) *element = e;
+    return RBC_OK;
+}
+
+int rbc_import_ref_wbc(rbc_handle *h, const double *x, const double *y, const double *z,
+                       const double *xd, const double *nd, const double *volume0, const double *gx)
+{
+    if (!h) return RBC_ERR_ARG;
+    if (h->ngroups < 2) return fail(h, RBC_ERR_STATE, "no white cells (rbc_add_wbc)");
+    return import_cells(h, h->cg[1], x, y, z, xd, nd, volume0, gx);
+}
+
+int rbc_export_ref_wbc(rbc_handle *h, double *x, double *y, double *z, double *xd,
+                       double *u, double *v, double *w, double *fx, double *fy, double *fz, double *gx)
+{
+    if (!h) return RBC_ERR_ARG;
+    if (h->ngroups < 2) return fail(h, RBC_ERR_STATE, "no white cells (rbc_add_wbc)");
+    return export_cells(h, h->cg[1], x, y, z, xd, u, v, w, fx, fy, fz, gx);
+}
+
+int rbc_wbc_metrics(rbc_handle *h, double *volume, double *area, double *centroid)
+{
+    if (!h) return RBC_ERR_ARG;
+    RBC_DEVICE_GUARD(h);
+    if (h->ngroups < 2) return fail(h, RBC_ERR_STATE, "no white cells (rbc_add_wbc)");
+    return group_metrics(h, h->cg[1], volume, area, centroid);
+}
+
+}  // extern "C"

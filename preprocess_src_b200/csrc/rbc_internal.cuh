@@ -164,9 +164,10 @@ int  membrane_smem_bytes(int V);
 
 // host helpers of the reference-format files (rbc_abi.cu)
 int reference_mn(int V);
-int output_averages(rbc_handle *h, double *qi, double *tp, bool set);
+int output_averages(rbc_handle *h, int group, double *qi, double *tp, bool set);   // group 0 red, 1 white cells
 int reference_bc(rbc_handle *h, int *bc);
-int reference_ele(rbc_handle *h, int *ele);          // cel->eleH: [ncell * E * 3] global vertex ids
+int reference_ele(rbc_handle *h, int group, int *ele);   // cel->eleH(_w): [ncell * E * 3] global vertex ids
+int group_sizes(const rbc_handle *h, int group, int *ncell, int *vertex, int *element);
 void set_handle_error(rbc_handle *h, const std::string &msg);
 
 // Output-interval averages of the load and the principal tensions (fem->qi,

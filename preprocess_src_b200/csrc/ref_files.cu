@@ -1,18 +1,19 @@
 // ref_files.cu -- the reference's restart and output files.
 //
-// Byte layouts of etc.cu for a red-cell run (N_R > 0, N_W = 0, no
-// cytoadhesion), written and read with this library's state:
-//   restart.bin  (output_data etc.cu:738-766, restart_file etc.cu:164-270)
+// Byte layouts of etc.cu for a run with red cells (N_R), white cells (N_W)
+// or both, no cytoadhesion, written and read with this library's state:
+//   restart.bin  (output_data etc.cu:738-781, restart_file etc.cu:164-270)
 //     int iter, int fnum, double fn[n*19], dm[n], um[n], vm[n], wm[n], vf[n],
-//     vf2[n]; then for cells: double x[N*V], y[N*V], z[N*V], rx[N], ry[N],
-//     rz[N], u[N*V], v[N*V], w[N*V], qi[N*mn], tp[N*E*2]
-//   cell%04d.bin (etc.cu:566-590)
-//     int N, V, E, double x, y, z, u, v, w [N*V], qi[N*V*3], tp[N*E*2],
-//     int ele[N*E*3] (global vertex ids)
+//     vf2[n]; then per population (red, then white): double x[N*V], y[N*V],
+//     z[N*V], rx[N], ry[N], rz[N], u[N*V], v[N*V], w[N*V], qi[N*mn], tp[N*E*2]
+//   cell%04d.bin (etc.cu:566-600)
+//     per population: int N, V, E, double x, y, z, u, v, w [N*V], qi[N*V*3],
+//     tp[N*E*2], int ele[N*E*3] (vertex ids within the population)
 //   prof%04d.bin (etc.cu:547-560)
 //     int iter, double dm, um, vm, wm, vf, vf2 [n], int bc[n]
 //   center.dat   (OutputCapsuleCenter / InputCapsuleCenter, etc.cu:110-160)
-//     one line per cell: "%d %e %e %e \n" (cell, cel->gx[3c + 0..2])
+//     one line per cell, red cells then white cells, each numbered from 0:
+//     "%d %e %e %e \n" (cell, cel->gx[3c + 0..2] or cel->gx_w)
 // n = nx * ny * nz counts the BUFF planes.  vf and vf2 (the VOF indicator,
 // used only with a viscosity contrast) stay at flu_init's 0, and rx, ry, rz are
 // never set by the reference; both are written as 0 and ignored when read.
@@ -33,22 +34,60 @@ using namespace rbc;
 
 namespace {
 
+struct Pop {   // one cell population: 0 red cells (cel->x), 1 white cells (cel->x_w)
+    int N = 0, V = 0, E = 0, mn = 0;
+    long long nv = 0, ne = 0;
+};
+
 struct Dims {
-    int nx = 0, ny = 0, nz = 0, N = 0, V = 0, E = 0, mn = 0;
-    long long n = 0, nv = 0, ne = 0;
+    int nx = 0, ny = 0, nz = 0;
+    long long n = 0;
+    Pop pop[2];
 };
 
 int dims_of(rbc_handle *h, Dims &d)
 {
-    int nzp = 0;
-    int rc = rbc_dims(h, &d.nx, &d.ny, &nzp, &d.N, &d.V, &d.E);
+    int nzp = 0, N = 0, V = 0, E = 0;
+    int rc = rbc_dims(h, &d.nx, &d.ny, &nzp, &N, &V, &E);
     if (rc) return rc;
     d.nz = nzp + 4;
     d.n = (long long)d.nx * d.ny * d.nz;
-    d.nv = (long long)d.N * d.V;
-    d.ne = (long long)d.N * d.E;
-    d.mn = d.N > 0 ? reference_mn(d.V) : 0;
+    for (int k = 0; k < 2; k++) {
+        Pop &p = d.pop[k];
+        group_sizes(h, k, &p.N, &p.V, &p.E);
+        p.nv = (long long)p.N * p.V;
+        p.ne = (long long)p.N * p.E;
+        p.mn = p.N > 0 ? reference_mn(p.V) : 0;
+    }
     return RBC_OK;
+}
+
+int export_pop(rbc_handle *h, int k, double *x, double *y, double *z, double *u, double *v, double *w, double *gx)
+{
+    return k == 0 ? rbc_export_ref_cells(h, x, y, z, nullptr, u, v, w, nullptr, nullptr, nullptr, gx)
+                  : rbc_export_ref_wbc(h, x, y, z, nullptr, u, v, w, nullptr, nullptr, nullptr, gx);
+}
+
+int import_pop(rbc_handle *h, int k, const double *x, const double *y, const double *z, const double *xd,
+               const double *gx)
+{
+    return k == 0 ? rbc_import_ref_cells(h, x, y, z, xd, nullptr, nullptr, gx)
+                  : rbc_import_ref_wbc(h, x, y, z, xd, nullptr, nullptr, gx);
+}
+
+// cel->x, y, z, u, v, w of one population and its fem->qi [N mn] and fem->tp [2 N E]
+struct PopState {
+    std::vector<double> cx, qi, tp;
+};
+
+int pop_state(rbc_handle *h, const Pop &p, int k, PopState &st)
+{
+    st.cx.resize((size_t)p.nv * 6);
+    st.qi.resize((size_t)p.N * p.mn);
+    st.tp.resize((size_t)p.ne * 2);
+    double *x = st.cx.data();
+    int rc = export_pop(h, k, x, x + p.nv, x + 2 * p.nv, x + 3 * p.nv, x + 4 * p.nv, x + 5 * p.nv, nullptr);
+    return rc ? rc : output_averages(h, k, st.qi.data(), st.tp.data(), false);
 }
 
 struct File {
@@ -98,16 +137,10 @@ int rbc_write_restart(rbc_handle *h, const char *path, int fnum)
     std::vector<double> fn, mac;
     std::vector<int> bc;
     if ((rc = lattice_of(h, d, fn, mac, bc))) return rc;
-    std::vector<double> zeros((size_t)std::max<long long>(d.n, d.N), 0.0);
-    std::vector<double> cx, qi, tp;
-    if (d.N > 0) {
-        cx.resize((size_t)d.nv * 6);
-        double *x = cx.data(), *y = x + d.nv, *z = y + d.nv, *u = z + d.nv, *v = u + d.nv, *w = v + d.nv;
-        if ((rc = rbc_export_ref_cells(h, x, y, z, nullptr, u, v, w, nullptr, nullptr, nullptr, nullptr))) return rc;
-        qi.resize((size_t)d.N * d.mn);
-        tp.resize((size_t)d.ne * 2);
-        if ((rc = output_averages(h, qi.data(), tp.data(), false))) return rc;
-    }
+    std::vector<double> zeros((size_t)std::max<long long>({d.n, d.pop[0].N, d.pop[1].N}), 0.0);
+    PopState st[2];
+    for (int k = 0; k < 2; k++)
+        if (d.pop[k].N > 0 && (rc = pop_state(h, d.pop[k], k, st[k]))) return rc;
     int iter = 0;
     rbc_get_iter(h, &iter);
     File f(path, "wb");
@@ -115,12 +148,14 @@ int rbc_write_restart(rbc_handle *h, const char *path, int fnum)
     bool ok = put(f.f, &iter, 1) && put(f.f, &fnum, 1) && put(f.f, fn.data(), fn.size())
            && put(f.f, mac.data(), mac.size())          // dm, um, vm, wm
            && put(f.f, zeros.data(), d.n) && put(f.f, zeros.data(), d.n);   // vf, vf2
-    if (ok && d.N > 0) {
-        const double *x = cx.data();
-        ok = put(f.f, x, 3 * d.nv)                       // x, y, z
-          && put(f.f, zeros.data(), d.N) && put(f.f, zeros.data(), d.N) && put(f.f, zeros.data(), d.N)   // rx, ry, rz
-          && put(f.f, x + 3 * d.nv, 3 * d.nv)            // u, v, w
-          && put(f.f, qi.data(), qi.size()) && put(f.f, tp.data(), tp.size());
+    for (int k = 0; k < 2 && ok; k++) {
+        const Pop &p = d.pop[k];
+        if (p.N == 0) continue;
+        const double *x = st[k].cx.data();
+        ok = put(f.f, x, 3 * p.nv)                       // x, y, z
+          && put(f.f, zeros.data(), p.N) && put(f.f, zeros.data(), p.N) && put(f.f, zeros.data(), p.N)   // rx, ry, rz
+          && put(f.f, x + 3 * p.nv, 3 * p.nv)            // u, v, w
+          && put(f.f, st[k].qi.data(), st[k].qi.size()) && put(f.f, st[k].tp.data(), st[k].tp.size());
     }
     return ok ? RBC_OK : io_error(h, "write failed", path);
 }
@@ -137,27 +172,32 @@ int rbc_read_restart(rbc_handle *h, const char *path, int *fnum)
     std::vector<double> fn((size_t)d.n * Q), skip((size_t)d.n * 6);
     bool ok = get(f.f, &iter, 1) && get(f.f, &fn_, 1) && get(f.f, fn.data(), fn.size())
            && get(f.f, skip.data(), skip.size());     // dm, um, vm, wm, vf, vf2: recomputed by the step / unused
-    std::vector<double> cx, qi, tp;
-    if (ok && d.N > 0) {
-        cx.resize((size_t)d.nv * 6);
-        std::vector<double> r((size_t)d.N * 3);
-        qi.resize((size_t)d.N * d.mn);
-        tp.resize((size_t)d.ne * 2);
-        ok = get(f.f, cx.data(), 3 * d.nv) && get(f.f, r.data(), r.size()) && get(f.f, cx.data() + 3 * d.nv, 3 * d.nv)
-          && get(f.f, qi.data(), qi.size()) && get(f.f, tp.data(), tp.size());
+    PopState st[2];
+    for (int k = 0; k < 2 && ok; k++) {
+        const Pop &p = d.pop[k];
+        if (p.N == 0) continue;
+        st[k].cx.resize((size_t)p.nv * 6);
+        st[k].qi.resize((size_t)p.N * p.mn);
+        st[k].tp.resize((size_t)p.ne * 2);
+        std::vector<double> r((size_t)p.N * 3);
+        double *x = st[k].cx.data();
+        ok = get(f.f, x, 3 * p.nv) && get(f.f, r.data(), r.size()) && get(f.f, x + 3 * p.nv, 3 * p.nv)
+          && get(f.f, st[k].qi.data(), st[k].qi.size()) && get(f.f, st[k].tp.data(), st[k].tp.size());
     }
     if (!ok) return io_error(h, "restart file too short for this lattice and these cells", path);
     if (std::fgetc(f.f) != EOF) return io_error(h, "restart file longer than this lattice and these cells", path);
     if (fn_ > 100) { iter = 0; fn_ = 0; }   // etc.cu:205
     if ((rc = rbc_import_ref_lattice(h, fn.data()))) return rc;
-    if (d.N > 0) {
-        // fem->x (hence fem->xd) is set from cel->x (etc.cu:248-255); the vertex velocities are the
+    for (int k = 0; k < 2; k++) {
+        const Pop &p = d.pop[k];
+        if (p.N == 0) continue;
+        // fem->x (hence fem->xd) is set from cel->x (etc.cu:256-274); the vertex velocities are the
         // next advection's output and are not needed to step
-        const double *x = cx.data(), *y = x + d.nv, *z = y + d.nv;
-        std::vector<double> xd((size_t)d.nv * 3);
-        for (long long j = 0; j < d.nv; j++) { xd[3 * j] = x[j]; xd[3 * j + 1] = y[j]; xd[3 * j + 2] = z[j]; }
-        if ((rc = rbc_import_ref_cells(h, x, y, z, xd.data(), nullptr, nullptr, nullptr))) return rc;
-        if ((rc = output_averages(h, qi.data(), tp.data(), true))) return rc;
+        const double *x = st[k].cx.data(), *y = x + p.nv, *z = y + p.nv;
+        std::vector<double> xd((size_t)p.nv * 3);
+        for (long long j = 0; j < p.nv; j++) { xd[3 * j] = x[j]; xd[3 * j + 1] = y[j]; xd[3 * j + 2] = z[j]; }
+        if ((rc = import_pop(h, k, x, y, z, xd.data(), nullptr))) return rc;
+        if ((rc = output_averages(h, k, st[k].qi.data(), st[k].tp.data(), true))) return rc;
     }
     if ((rc = rbc_set_iter(h, iter))) return rc;
     if (fnum) *fnum = fn_;
@@ -170,18 +210,26 @@ int rbc_write_cell_file(rbc_handle *h, const char *path)
     Dims d;
     int rc = dims_of(h, d);
     if (rc) return rc;
-    if (d.N == 0) return RBC_ERR_STATE;
-    std::vector<double> cx((size_t)d.nv * 6), qi((size_t)d.N * d.mn), tp((size_t)d.ne * 2);
-    double *x = cx.data();
-    if ((rc = rbc_export_ref_cells(h, x, x + d.nv, x + 2 * d.nv, nullptr, x + 3 * d.nv, x + 4 * d.nv, x + 5 * d.nv,
-                                   nullptr, nullptr, nullptr, nullptr))) return rc;
-    if ((rc = output_averages(h, qi.data(), tp.data(), false))) return rc;
-    std::vector<int> ele((size_t)d.ne * 3);
-    if ((rc = reference_ele(h, ele.data()))) return rc;
+    if (d.pop[0].N == 0 && d.pop[1].N == 0) return RBC_ERR_STATE;
+    PopState st[2];
+    std::vector<int> ele[2];
+    for (int k = 0; k < 2; k++) {
+        const Pop &p = d.pop[k];
+        if (p.N == 0) continue;
+        if ((rc = pop_state(h, p, k, st[k]))) return rc;
+        ele[k].resize((size_t)p.ne * 3);
+        if ((rc = reference_ele(h, k, ele[k].data()))) return rc;
+    }
     File f(path, "wb");
     if (!f.f) return io_error(h, "cannot open for writing", path);
-    const bool ok = put(f.f, &d.N, 1) && put(f.f, &d.V, 1) && put(f.f, &d.E, 1) && put(f.f, x, 6 * d.nv)
-                 && put(f.f, qi.data(), 3 * d.nv) && put(f.f, tp.data(), tp.size()) && put(f.f, ele.data(), ele.size());
+    bool ok = true;
+    for (int k = 0; k < 2 && ok; k++) {
+        const Pop &p = d.pop[k];
+        if (p.N == 0) continue;
+        ok = put(f.f, &p.N, 1) && put(f.f, &p.V, 1) && put(f.f, &p.E, 1) && put(f.f, st[k].cx.data(), 6 * p.nv)
+          && put(f.f, st[k].qi.data(), 3 * p.nv) && put(f.f, st[k].tp.data(), st[k].tp.size())
+          && put(f.f, ele[k].data(), ele[k].size());
+    }
     return ok ? RBC_OK : io_error(h, "write failed", path);
 }
 
@@ -210,14 +258,18 @@ int rbc_write_center_file(rbc_handle *h, const char *path)
     Dims d;
     int rc = dims_of(h, d);
     if (rc) return rc;
-    std::vector<double> gx((size_t)d.N * 3 + 1);
-    if (d.N > 0 && (rc = rbc_export_ref_cells(h, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
-                                              nullptr, nullptr, nullptr, gx.data()))) return rc;
+    std::vector<double> gx[2];
+    for (int k = 0; k < 2; k++) {
+        gx[k].resize((size_t)d.pop[k].N * 3 + 1);
+        if (d.pop[k].N > 0 && (rc = export_pop(h, k, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, gx[k].data())))
+            return rc;
+    }
     File f(path, "w");
     if (!f.f) return io_error(h, "cannot open for writing", path);
-    for (int c = 0; c < d.N; c++)
-        if (std::fprintf(f.f, "%d %e %e %e \n", c, gx[3 * c], gx[3 * c + 1], gx[3 * c + 2]) < 0)
-            return io_error(h, "write failed", path);
+    for (int k = 0; k < 2; k++)
+        for (int c = 0; c < d.pop[k].N; c++)
+            if (std::fprintf(f.f, "%d %e %e %e \n", c, gx[k][3 * c], gx[k][3 * c + 1], gx[k][3 * c + 2]) < 0)
+                return io_error(h, "write failed", path);
     return RBC_OK;
 }
 
@@ -227,14 +279,19 @@ int rbc_read_center_file(rbc_handle *h, const char *path)
     Dims d;
     int rc = dims_of(h, d);
     if (rc) return rc;
-    if (d.N == 0) return RBC_ERR_STATE;
+    if (d.pop[0].N == 0 && d.pop[1].N == 0) return RBC_ERR_STATE;
     File f(path, "r");
     if (!f.f) return io_error(h, "cannot open for reading", path);
-    std::vector<double> gx((size_t)d.N * 3);
-    for (int c = 0; c < d.N; c++)
-        if (std::fscanf(f.f, "%*d %lf %lf %lf", &gx[3 * c], &gx[3 * c + 1], &gx[3 * c + 2]) != 3)
-            return io_error(h, "center file has fewer lines than cells", path);
-    return rbc_import_ref_cells(h, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, gx.data());
+    std::vector<double> gx[2];
+    for (int k = 0; k < 2; k++) {
+        gx[k].resize((size_t)d.pop[k].N * 3);
+        for (int c = 0; c < d.pop[k].N; c++)
+            if (std::fscanf(f.f, "%*d %lf %lf %lf", &gx[k][3 * c], &gx[k][3 * c + 1], &gx[k][3 * c + 2]) != 3)
+                return io_error(h, "center file has fewer lines than cells", path);
+    }
+    for (int k = 0; k < 2; k++)
+        if (d.pop[k].N > 0 && (rc = import_pop(h, k, nullptr, nullptr, nullptr, nullptr, gx[k].data()))) return rc;
+    return RBC_OK;
 }
 
 }  // extern "C"

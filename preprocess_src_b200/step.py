@@ -149,6 +149,46 @@ class Simulation:
         self._call("rbc_export_ref_cells", *[_dp(out[k]) for k in keys])
         return out
 
+    # -- white cells (init3.cu) --------------------------------------------------
+    def add_wbc(self, wbc: Case, rgs: float = 1.0, br: float = 0.0):
+        """A second cell population (cel->*_w): wbc's mesh (tri, xr, ncell,
+        vertex, element; its lattice is ignored), tension normalisation rgs =
+        GSw / GS and bending modulus br = BRw."""
+        self._tri_w = np.ascontiguousarray(wbc.tri, dtype=np.int32).reshape(-1)
+        self._xr_w = np.ascontiguousarray(wbc.xr, dtype=np.float64)
+        m = N.RbcMesh(wbc.ncell, wbc.vertex, wbc.element, self._tri_w.ctypes.data_as(N._IP),
+                      self._xr_w.ctypes.data_as(N._DP))
+        self._call("rbc_add_wbc", C.byref(m), C.c_double(rgs), C.c_double(br))
+        self.wbc = wbc
+        self.nv_w = wbc.ncell * wbc.vertex
+        self.ne_w = wbc.ncell * wbc.element
+
+    def wbc_dims(self) -> tuple[int, int, int]:
+        n, v, e = C.c_int(0), C.c_int(0), C.c_int(0)
+        self._call("rbc_wbc_dims", C.byref(n), C.byref(v), C.byref(e))
+        return n.value, v.value, e.value
+
+    def import_wbc(self, x=None, y=None, z=None, xd=None, nd=None, volume0=None, gx=None):
+        nv, ne, nc = self.nv_w, self.ne_w, self.wbc.ncell
+        args = [None if a is None else _f64(a, n)
+                for a, n in ((x, nv), (y, nv), (z, nv), (xd, 3 * nv), (nd, 4 * ne), (volume0, nc), (gx, 3 * nc))]
+        self._keep = args
+        self._call("rbc_import_ref_wbc", *map(_dp, args))
+
+    def export_wbc(self) -> dict:
+        nv, nc = self.nv_w, self.wbc.ncell
+        keys = ("x", "y", "z", "xd", "u", "v", "w", "fx", "fy", "fz", "gx")
+        sizes = (nv, nv, nv, 3 * nv, nv, nv, nv, nv, nv, nv, 3 * nc)
+        out = {k: np.empty(s) for k, s in zip(keys, sizes)}
+        self._call("rbc_export_ref_wbc", *[_dp(out[k]) for k in keys])
+        return out
+
+    def wbc_metrics(self) -> dict:
+        nc = self.wbc.ncell
+        out = {"volume": np.empty(nc), "area": np.empty(nc), "centroid": np.empty(3 * nc)}
+        self._call("rbc_wbc_metrics", _dp(out["volume"]), _dp(out["area"]), _dp(out["centroid"]))
+        return out
+
     # -- files in the reference's formats (etc.cu) -------------------------------
     def set_output_interval(self, fileoutput: int):
         """FILEOUTPUT: average fem->qi and fem->tp over intervals of this many steps."""

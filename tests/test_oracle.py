@@ -4,6 +4,7 @@ The reference ships no tests or golden vectors; these pin the oracle with
 analytic results and conservation laws, and tests/test_golden.py pins it
 against outputs of the reference's own kernels.
 """
+import dataclasses
 import math
 
 import numpy as np
@@ -244,3 +245,36 @@ def test_tube_interpolated_bounce_back_beats_the_staircase(oracle_mod):
         exact = g / (4 * (1.0 / 6.0)) * (R * R - r2)
         errs[interp] = np.sqrt(((w - exact)[m] ** 2).sum() / (exact[m] ** 2).sum())
     assert errs[True] <= 0.015 and errs[True] <= 0.25 * errs[False], errs
+
+
+def test_oracle_per_cell_membrane_coefficients(oracle_mod):
+    """The oracle's per-cell rgs and BR (a second cell population on the same
+    mesh, cel->rg_w and cel->br_w of init3.cu:91-92): each cell's stress()
+    force is the one of a single population with that cell's coefficients."""
+    from preprocess_src_b200 import configs
+    case = configs.duct_case("percell", 24, 20, 20, centers_duct=[(6.0, 9.8, 10.1), (17.0, 10.2, 9.7)],
+                             subdiv=2, radius=4.0, seed=5, g=4e-5, Gs=2e-3)
+    o0 = oracle_mod.Oracle(case)
+    o0.step(4)   # deformed cells
+
+    def forces(o):
+        assert o.stress() == 0
+        return np.stack([o["cfx"], o["cfy"], o["cfz"]])
+
+    def at(rgs=None, br=None, cell_rgs=None, cell_br=None):
+        p = dict(case.params)
+        if rgs is not None:
+            p["rgs"] = rgs
+        if br is not None:
+            p["br"] = br
+        o = oracle_mod.Oracle(dataclasses.replace(case, params=p), init_fluid=False, cell_rgs=cell_rgs,
+                              cell_br=cell_br)
+        for k in ("x", "y", "z", "xd", "nd", "volume0", "gx"):
+            o.a[k][:] = o0.a[k]
+        return forces(o)
+
+    V = case.vertex
+    mixed = at(cell_rgs=[1.0, 2.5], cell_br=[0.0, 0.02])
+    np.testing.assert_array_equal(mixed[:, :V], at(rgs=1.0, br=0.0)[:, :V])
+    np.testing.assert_array_equal(mixed[:, V:], at(rgs=2.5, br=0.02)[:, V:])
+    assert np.abs(mixed[:, V:] - at(rgs=1.0)[:, V:]).max() > 1e-6

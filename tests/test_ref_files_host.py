@@ -26,3 +26,43 @@ def test_center_file_format(tmp_path):
     RF.write_center(tmp_path / "c.dat", [1.0, -2.5, 3.25e-3, 4.0, 5.0, 6.0])
     assert (tmp_path / "c.dat").read_text().splitlines()[0] == "0 1.000000e+00 -2.500000e+00 3.250000e-03 "
     np.testing.assert_allclose(RF.read_center(tmp_path / "c.dat"), [1.0, -2.5, 3.25e-3, 4.0, 5.0, 6.0])
+
+
+def test_restart_layout_with_white_cells(tmp_path):
+    """output_data (etc.cu:738-781): the white cells' block follows the red
+    cells' with the same field order; a run with white cells only has no red
+    block."""
+    n, N, V, E, Nw, Vw, Ew = 30, 2, 12, 20, 3, 42, 80
+    names = [k for k, _, _ in RF.restart_layout(n, N, V, E, Nw, Vw, Ew)]
+    red = ["x", "y", "z", "rx", "ry", "rz", "u", "v", "w", "qi", "tp"]
+    assert names == ["iter", "fnum", "fn", "dm", "um", "vm", "wm", "vf", "vf2"] + red + [k + "_w" for k in red]
+    cnt = dict((k, c) for k, _, c in RF.restart_layout(n, N, V, E, Nw, Vw, Ew))
+    assert cnt["qi_w"] == Nw * RF.expand2pow2(3 * Vw) and cnt["tp_w"] == 2 * Nw * Ew and cnt["rx_w"] == Nw
+    only_w = [k for k, _, _ in RF.restart_layout(n, 0, 0, 0, Nw, Vw, Ew)]
+    assert only_w[9:] == [k + "_w" for k in red]
+    rng = np.random.default_rng(1)
+    f = {k: rng.standard_normal(c) for k, dt, c in RF.restart_layout(n, N, V, E, Nw, Vw, Ew) if dt == np.float64}
+    RF.write_restart(tmp_path / "r.bin", n, N, V, E, f, Nw, Vw, Ew)
+    g = RF.read_restart(tmp_path / "r.bin", n, N, V, E, Nw, Vw, Ew)
+    for k in f:
+        np.testing.assert_array_equal(g[k], f[k])
+
+
+def test_cell_file_blocks(tmp_path):
+    """cell%04d.bin (etc.cu:566-600): one self-describing block per population."""
+    rng = np.random.default_rng(2)
+    blocks = []
+    for (N, V, E), sfx in (((2, 12, 20), ""), ((1, 42, 80), "_w")):
+        lay = RF.cell_layout(N, V, E, sfx)
+        vals = {k: (np.array([dict(N=N, V=V, E=E)[k[0]]], np.int32) if c == 1 and dt == np.int32
+                    else rng.integers(0, 50, c).astype(dt) if dt == np.int32 else rng.standard_normal(c))
+                for k, dt, c in lay}
+        blocks.append((lay, vals))
+    with open(tmp_path / "c.bin", "wb") as fh:
+        for lay, vals in blocks:
+            for k, dt, c in lay:
+                fh.write(np.asarray(vals[k], dtype=dt).tobytes())
+    got = RF.read_cell_file(tmp_path / "c.bin", blocks=2)
+    for _, vals in blocks:
+        for k, v in vals.items():
+            np.testing.assert_array_equal(got[k], v)
