@@ -118,6 +118,11 @@ typedef struct rbc_params {
     /* channel mode: > 0 = the walls are the circular tube x^2 + y^2 = tube_r^2 and its links
      * bounce back by linear interpolation at the circle (lbm_cylinder.cu:61-231); 0 = half-way */
     double tube_r;
+    /* bending (BR != 0) about spontaneous angles: 0 = angle 0 for every edge, as
+     * the reference runs (init1.cu:849-850 overwrite the computed angles with
+     * c0 = 1, s0 = 0); 1 = the initial shape's dihedral angles, the values
+     * init1.cu:797-848 (init3.cu:313-364) compute before that override */
+    int    bend_spont;
 } rbc_params;
 
 typedef struct rbc_mesh {

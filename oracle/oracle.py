@@ -39,7 +39,7 @@ class OrcState(C.Structure):
     _fields_ = ([(k, _DP) for k in _STATE_D] + [("bc", _IP)] + [(k, _DP) for k in _STATE_CELL_D]
                 + [("ele", _IP), ("nln", _IP), ("ln", _IP), ("lo", _IP), ("nle", _IP), ("le", _IP),
                    ("volume0", _DP), ("gx", _DP), ("iter", C.c_int), ("bicg_iters", C.c_int), ("ec", _IP),
-                   ("crg", _DP), ("cbr", _DP)])
+                   ("crg", _DP), ("cbr", _DP), ("c0", _DP), ("s0", _DP)])
 
 
 _lib = None
@@ -58,7 +58,7 @@ def lib() -> C.CDLL:
         for name in ("orc_fem_init", "orc_stress", "orc_calc_load", "orc_volume_correction", "orc_step"):
             getattr(L, name).restype = C.c_int
         for name in ("orc_flu_init", "orc_volume_init", "orc_ibm_st1", "orc_lbm_d3q19", "orc_ibm_st2",
-                     "orc_calc_tension", "orc_q2f", "orc_bend"):
+                     "orc_calc_tension", "orc_q2f", "orc_bend", "orc_bend_reference"):
             getattr(L, name).restype = None
         L.orc_num_threads.restype = C.c_int
         L.orc_calc_volume.restype = None
@@ -80,9 +80,11 @@ def expand2pow2(n: int) -> int:
 class Oracle:
     """Reference-layout FP64 state of one case, stepped on the CPU."""
 
-    def __init__(self, case, init_fluid=True, cell_rgs=None, cell_br=None):
+    def __init__(self, case, init_fluid=True, cell_rgs=None, cell_br=None, bend_spont=None):
         """cell_rgs, cell_br: optional [ncell] per-cell tension normalisation and
-        bending modulus (cells of a second population on the same mesh)."""
+        bending modulus (cells of a second population on the same mesh).
+        bend_spont (default: case.params["bend_spont"]): bending about the
+        spontaneous angles of the initial shape instead of 0."""
         self.case = case
         p = case.params
         self.N, self.V, self.E = case.ncell, case.vertex, case.element
@@ -132,6 +134,14 @@ class Oracle:
             if rc != 0:
                 raise RuntimeError(f"oracle fem_init failed with error({rc})")
             L.orc_volume_init(C.byref(self.p), C.byref(self.s))
+            if bend_spont is None:
+                bend_spont = bool(p.get("bend_spont", 0))
+            if bend_spont:
+                self.a["c0"] = np.zeros(3 * ne)
+                self.a["s0"] = np.zeros(3 * ne)
+                self.s.c0 = self.a["c0"].ctypes.data_as(_DP)
+                self.s.s0 = self.a["s0"].ctypes.data_as(_DP)
+                L.orc_bend_reference(C.byref(self.p), C.byref(self.s))
 
     # the population buffers swap like ltc->fnD / ltc->fmD (lbm.cu:1575)
     @property

@@ -411,14 +411,71 @@ void orc_q2f(const orc_params *p, orc_state *s)
     }
 }
 
+/* The four vertices of element e1's visit of its k-th edge neighbour e2
+ * (cel->ec order): the shared edge (k2, k3) in e1's winding, e1's third
+ * vertex k1 and e2's vertex k4 off the edge (stress.cu:490-502).  Returns 0
+ * when e1 has no k-th neighbour. */
+static int bend_quad(const orc_state *s, long e1, int k, int q[4])
+{
+    const long e2 = s->ec[e1*3 + k];
+    const int i[3] = {s->ele[e1*3], s->ele[e1*3+1], s->ele[e1*3+2]};
+    const int j[3] = {s->ele[e2*3], s->ele[e2*3+1], s->ele[e2*3+2]};
+    for (int a = 0; a < 3; a++) {
+        const int ia = i[a], ib = i[(a + 1) % 3];
+        int has_a = -1, has_b = -1;
+        for (int b = 0; b < 3; b++) { if (j[b] == ia) has_a = b; if (j[b] == ib) has_b = b; }
+        if (e2 != e1 && has_a >= 0 && has_b >= 0) {
+            q[0] = i[(a + 2) % 3]; q[1] = ia; q[2] = ib; q[3] = j[3 - has_a - has_b];
+            return 1;
+        }
+    }
+    return 0;
+}
+
+/* init1.cu:797-848 (init3.cu:313-364 for white cells): cos and sin of each
+ * visit's dihedral angle on the current positions, the sign of sin from the
+ * centroid test, 1 - cos^2 clamped at 0.  The reference computes these from
+ * the initial shape and then overwrites them with c0 = 1, s0 = 0
+ * (init1.cu:849-850); this keeps them (spontaneous angles of the reference
+ * shape).  Positions are minimum images about k1, the same for an unwrapped
+ * initial shape. */
+void orc_bend_reference(const orc_params *p, orc_state *s)
+{
+    const long ne = (long)p->ncell * p->element;
+    for (long e1 = 0; e1 < ne; e1++)
+        for (int k = 0; k < 3; k++) {
+            int q[4];
+            s->c0[e1*3 + k] = 1.0;
+            s->s0[e1*3 + k] = 0.0;
+            if (!bend_quad(s, e1, k, q)) continue;
+            double ax[4], ay[4], az[4];
+            for (int v = 0; v < 4; v++) {
+                ax[v] = s->x[q[0]] + min_image(s->x[q[v]] - s->x[q[0]], p->LX);
+                ay[v] = s->y[q[v]];
+                az[v] = s->z[q[0]] + min_image(s->z[q[v]] - s->z[q[0]], p->LZ);
+            }
+            const double a21x = ax[1] - ax[0], a31x = ax[2] - ax[0], a34x = ax[2] - ax[3], a24x = ax[1] - ax[3];
+            const double a21y = ay[1] - ay[0], a31y = ay[2] - ay[0], a34y = ay[2] - ay[3], a24y = ay[1] - ay[3];
+            const double a21z = az[1] - az[0], a31z = az[2] - az[0], a34z = az[2] - az[3], a24z = az[1] - az[3];
+            const double xix = a21y*a31z - a21z*a31y, xiy = a21z*a31x - a21x*a31z, xiz = a21x*a31y - a21y*a31x;
+            const double zex = a34y*a24z - a34z*a24y, zey = a34z*a24x - a34x*a24z, zez = a34x*a24y - a34y*a24x;
+            const double cost = (xix*zex + xiy*zey + xiz*zez) / sqrt(xix*xix + xiy*xiy + xiz*xiz)
+                              / sqrt(zex*zex + zey*zey + zez*zez);
+            double cost2 = 1.0 - cost * cost;
+            if (cost2 < 0.0) cost2 = 0.0;
+            const double t = (xix - zex) * (ax[0] - ax[3]) + (xiy - zey) * (ay[0] - ay[3]) + (xiz - zez) * (az[0] - az[3]);
+            s->c0[e1*3 + k] = cost;
+            s->s0[e1*3 + k] = t >= 0.0 ? sqrt(cost2) : -sqrt(cost2);
+        }
+}
+
 /* stress.cu:448-578.  For every element e1 and each of its edge neighbours
- * e2 (cel->ec order): the shared edge (k2, k3) in e1's winding, e1's third
- * vertex k1 and e2's vertex k4 off the edge; xi and ze are the two triangle
- * normals with positions taken as minimum images about k1; pairs with
- * sin^2 < 1e-6 are skipped; with spontaneous angle 0 (c0 = 1, s0 = 0,
- * init1.cu:849-850) beta = (2/sqrt 3) BR; k1 receives the whole force of
- * the pair, k2 and k3 half of theirs (e2's visit of the same pair adds the
- * rest). */
+ * (bend_quad): xi and ze are the two triangle normals with positions taken
+ * as minimum images about k1; pairs with sin^2 < 1e-6 are skipped; beta =
+ * (2/sqrt 3) BR sgn (sin c0 - cos s0) / |sin| with the spontaneous angle
+ * (c0, s0) of the visit, (1, 0) as init1.cu:849-850 leaves it unless
+ * s->c0 / s->s0 hold others; k1 receives the whole force of the pair, k2 and
+ * k3 half of theirs (e2's visit of the same pair adds the rest). */
 void orc_bend(const orc_params *p, orc_state *s)
 {
     if (p->br == 0.0 && !s->cbr) return;
@@ -427,20 +484,11 @@ void orc_bend(const orc_params *p, orc_state *s)
     for (long e1 = 0; e1 < ne; e1++) {
         const double br = s->cbr ? s->cbr[e1 / p->element] : p->br;
         if (br == 0.0) continue;
-        const int i[3] = {s->ele[e1*3], s->ele[e1*3+1], s->ele[e1*3+2]};
         for (int k = 0; k < 3; k++) {
-            const long e2 = s->ec[e1*3 + k];
-            const int j[3] = {s->ele[e2*3], s->ele[e2*3+1], s->ele[e2*3+2]};
-            int k1 = -1, k2 = -1, k3 = -1, k4 = -1;
-            for (int a = 0; a < 3 && k1 < 0; a++) {
-                const int ia = i[a], ib = i[(a + 1) % 3];
-                int has_a = -1, has_b = -1;
-                for (int b = 0; b < 3; b++) { if (j[b] == ia) has_a = b; if (j[b] == ib) has_b = b; }
-                if (has_a >= 0 && has_b >= 0) {
-                    k1 = i[(a + 2) % 3]; k2 = ia; k3 = ib; k4 = j[3 - has_a - has_b];
-                }
-            }
-            if (k1 < 0) continue;
+            int q[4];
+            if (!bend_quad(s, e1, k, q)) continue;
+            const int k1 = q[0], k2 = q[1], k3 = q[2], k4 = q[3];
+            const double cost0 = s->c0 ? s->c0[e1*3 + k] : 1.0, sint0 = s->s0 ? s->s0[e1*3 + k] : 0.0;
             double a1x = s->x[k1], a2x = s->x[k2], a3x = s->x[k3], a4x = s->x[k4];
             double a1y = s->y[k1], a2y = s->y[k2], a3y = s->y[k3], a4y = s->y[k4];
             double a1z = s->z[k1], a2z = s->z[k2], a3z = s->z[k3], a4z = s->z[k4];
@@ -460,7 +508,7 @@ void orc_bend(const orc_params *p, orc_state *s)
             if (cost2 < eps) continue;
             const double sgn = ((xix-zex)*(t1x-t2x) + (xiy-zey)*(t1y-t2y) + (xiz-zez)*(t1z-t2z)) >= 0.0 ? 1.0 : -1.0;
             const double sint = sgn * sqrt(cost2);
-            const double beta = sgn * 2.0 / sqrt(3.0) * br * (sint * 1.0 - cost * 0.0) / sqrt(cost2);
+            const double beta = sgn * 2.0 / sqrt(3.0) * br * (sint * cost0 - cost * sint0) / sqrt(cost2);
             const double b11 = -beta * cost / (nxi * nxi), b12 = beta / nxi / nze, b22 = -beta * cost / (nze * nze);
             s->cfx[k1] += b11*(xiy*-a23z - xiz*-a23y) + b12*(zey*-a23z - zez*-a23y);
             s->cfy[k1] += b11*(xiz*-a23x - xix*-a23z) + b12*(zez*-a23x - zex*-a23z);

@@ -87,6 +87,9 @@ typedef struct orc_state {
      * p->rgs / p->br in every cell: a run with white cells as well (cel->rg_w
      * = GSw / GS, cel->br_w = BRw, init3.cu:91-92) on the same mesh */
     double *crg, *cbr;
+    /* [3*ne] spontaneous angle (cos, sin) of each bending visit, or NULL for
+     * (1, 0) as init1.cu:849-850 leaves it; orc_bend_reference fills them */
+    double *c0, *s0;
 } orc_state;
 
 /* init2.cu:258-400 (fem_init): link tables and the reference metric from the
@@ -124,6 +127,9 @@ void orc_calc_volume(const orc_params *p, const orc_state *s, double *volume, do
  * every edge-neighbour pair to cel->fx/fy/fz (spontaneous angle 0, as
  * init1.cu:849-850 leaves it). */
 void orc_bend(const orc_params *p, orc_state *s);
+/* init1.cu:797-848 without the override of 849-850: s->c0 / s->s0 from the
+ * current positions (the reference shape when called after orc_fem_init). */
+void orc_bend_reference(const orc_params *p, orc_state *s);
 
 int  orc_num_threads(void);
 

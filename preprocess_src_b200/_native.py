@@ -32,7 +32,7 @@ class RbcParams(C.Structure):
                 ("law", C.c_int), ("br", C.c_double), ("M", C.c_int), ("rk_order", C.c_int),
                 ("storage", C.c_int), ("membrane_fp64", C.c_int), ("solver_iters", C.c_int),
                 ("device", C.c_int), ("flow", C.c_int), ("sr", C.c_double), ("walls", C.c_int),
-                ("tube_r", C.c_double)]
+                ("tube_r", C.c_double), ("bend_spont", C.c_int)]
 
 
 class RbcMesh(C.Structure):

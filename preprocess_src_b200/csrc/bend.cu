@@ -14,9 +14,10 @@
 // k1 the third vertex of e1, k4 the vertex of e2 off the edge): positions are
 // taken as minimum images about k1 (x with LX, z with LZ), xi and ze are the
 // two outward normals, pairs with 1 - cos^2 < 1e-6 contribute nothing, and
-// with the spontaneous angle 0 the reference leaves (c0 = 1, s0 = 0,
-// init1.cu:849-850) the force is (2 / sqrt 3) BR times the gradient of
-// cos theta.
+// the force is beta times the gradient of cos theta with beta = (2 / sqrt 3)
+// BR sgn (sin c0 - cos s0) / |sin| (stress.cu:531-535): (2 / sqrt 3) BR with
+// the spontaneous angle 0 the reference leaves (c0 = 1, s0 = 0,
+// init1.cu:849-850), or with the initial shape's angle of the visit (cs0).
 #include "rbc_internal.cuh"
 
 namespace rbc {
@@ -58,12 +59,16 @@ bend_kernel(const BendArgs a)
             const double cost = (xix * zex + xiy * zey + xiz * zez) / nxi / nze;
             const double cost2 = 1.0 - cost * cost;
             if (cost2 < 1.0e-6) continue;   // (NaN from a degenerate triangle propagates, as in the reference)
-            // centroid test of stress.cu:527 for the sign of sin theta; with c0 = 1, s0 = 0
-            // beta = sign * coef * sin / |sin| = coef
+            // centroid test of stress.cu:527 for the sign of sin theta
             const double dtx = (a1x - a4x) / 3.0, dty = (a1y - a4y) / 3.0, dtz = (a1z - a4z) / 3.0;
             const double sgn = ((xix - zex) * dtx + (xiy - zey) * dty + (xiz - zez) * dtz) >= 0.0 ? 1.0 : -1.0;
             const double sint = sgn * sqrt(cost2);
-            const double beta = sgn * a.coef * sint / sqrt(cost2);
+            double c0 = 1.0, s0 = 0.0;
+            if (a.cs0) {
+                const double2 cs = __ldg(&a.cs0[((long long)cell * a.E + e1) * 3 + s]);
+                c0 = cs.x; s0 = cs.y;
+            }
+            const double beta = sgn * a.coef * (sint * c0 - cost * s0) / sqrt(cost2);
             const double b11 = -beta * cost / (nxi * nxi), b12 = beta / nxi / nze, b22 = -beta * cost / (nze * nze);
             if (role == 0) {
                 fx += b11 * (xiy * -a23z - xiz * -a23y) + b12 * (zey * -a23z - zez * -a23y);

@@ -52,6 +52,7 @@ struct CellGroup {
     int *tri = nullptr, *v2e_off = nullptr, *v2e = nullptr;
     int16_t *nbr = nullptr;
     int4 *visit = nullptr;   // bending visits [E][3], allocated when BR != 0
+    double2 *cs0 = nullptr;  // spontaneous angle (cos, sin) per visit [ncell][E][3] (bend_spont), else none
     double *vol0 = nullptr, *gx = nullptr, *vol_out = nullptr, *area_out = nullptr, *cen_out = nullptr;
     int *patch_off = nullptr, *patch_vtx = nullptr, *patch_stride = nullptr;
     int npatch = 1;
@@ -377,6 +378,48 @@ void bend_visits(int V, int E, const int *tri, std::vector<int4> &visit)
     }
 }
 
+// init1.cu:797-848 (init3.cu:313-364 for white cells) without the override
+// of 849-850: cos and sin of every visit's dihedral angle on the initial
+// shape xr (AoS [3 ncell V]), the sign of sin from the centroid test, 1 - cos^2
+// clamped at 0; positions as minimum images about k1 like the bending kernel.
+void spontaneous_angles(const rbc_params &p, const CellGroup &c, const double *xr, const std::vector<int4> &visit,
+                        std::vector<double2> &cs0)
+{
+    auto mi = [](double d, double L) { return d > L * 0.5 ? d - L : (d < -L * 0.5 ? d + L : d); };
+    cs0.assign((size_t)c.ncell * c.E * 3, make_double2(1.0, 0.0));
+    for (int cell = 0; cell < c.ncell; cell++) {
+        const double *x = xr + (size_t)3 * cell * c.V;
+        for (size_t k = 0; k < (size_t)3 * c.E; k++) {
+            const int4 q = visit[k];
+            if (q.x < 0) continue;
+            const int id[4] = {q.x, q.y, q.z, q.w};
+            double a[4][3];
+            for (int v = 0; v < 4; v++) {
+                a[v][0] = x[3 * q.x] + mi(x[3 * id[v]] - x[3 * q.x], p.LX);
+                a[v][1] = x[3 * id[v] + 1];
+                a[v][2] = x[3 * q.x + 2] + mi(x[3 * id[v] + 2] - x[3 * q.x + 2], p.LZ);
+            }
+            double r21[3], r31[3], r34[3], r24[3], xi[3], ze[3];
+            for (int d = 0; d < 3; d++) {
+                r21[d] = a[1][d] - a[0][d]; r31[d] = a[2][d] - a[0][d];
+                r34[d] = a[2][d] - a[3][d]; r24[d] = a[1][d] - a[3][d];
+            }
+            for (int d = 0; d < 3; d++) {
+                const int d1 = (d + 1) % 3, d2 = (d + 2) % 3;
+                xi[d] = r21[d1] * r31[d2] - r21[d2] * r31[d1];
+                ze[d] = r34[d1] * r24[d2] - r34[d2] * r24[d1];
+            }
+            const double cost = (xi[0] * ze[0] + xi[1] * ze[1] + xi[2] * ze[2])
+                              / std::sqrt(xi[0] * xi[0] + xi[1] * xi[1] + xi[2] * xi[2])
+                              / std::sqrt(ze[0] * ze[0] + ze[1] * ze[1] + ze[2] * ze[2]);
+            const double cost2 = std::max(1.0 - cost * cost, 0.0);
+            double t = 0.0;   // (xi - ze) . (t1 - t2), t1 - t2 = (x1 - x4) / 3
+            for (int d = 0; d < 3; d++) t += (xi[d] - ze[d]) * (a[0][d] - a[3][d]) / 3.0;
+            cs0[(size_t)cell * c.E * 3 + k] = make_double2(cost, t >= 0.0 ? std::sqrt(cost2) : -std::sqrt(cost2));
+        }
+    }
+}
+
 int check_params(const rbc_params *p)
 {
     if (!p) return fail(nullptr, RBC_ERR_ARG, "params is NULL");
@@ -390,6 +433,7 @@ int check_params(const rbc_params *p)
     if (p->M != 1) return fail(nullptr, RBC_ERR_UNSUPPORTED, "only M = 1 (no sub-cycling) is implemented");
     if (p->rk_order != 4) return fail(nullptr, RBC_ERR_UNSUPPORTED, "only RUNGE_KUTTA = 4 is implemented");
     if (!std::isfinite(p->br)) return fail(nullptr, RBC_ERR_ARG, "BR must be finite");
+    if (p->bend_spont != 0 && p->bend_spont != 1) return fail(nullptr, RBC_ERR_ARG, "bend_spont must be 0 or 1");
     if (p->storage != RBC_STORE_F32 && p->storage != RBC_STORE_F16) return fail(nullptr, RBC_ERR_ARG, "unknown storage");
     if (p->law != RBC_LAW_SKALAK && p->law != RBC_LAW_NEOHOOKEAN) return fail(nullptr, RBC_ERR_ARG, "unknown law");
     if (p->solver_iters < 0 || p->solver_iters > 200) return fail(nullptr, RBC_ERR_ARG, "solver_iters out of range");
@@ -506,6 +550,14 @@ int build_mask(const rbc_params *p, const int *bc, std::vector<uint32_t> &mask)
     return RBC_OK;
 }
 
+void free_group(CellGroup &c)
+{
+    void *cp[] = {c.X, c.Xd, c.gref, c.erec, c.U, c.Fv, c.tri, c.v2e_off, c.v2e, c.nbr, c.visit, c.cs0, c.patch_off,
+                  c.patch_vtx, c.patch_stride, c.vol0, c.gx, c.vol_out, c.area_out, c.cen_out, c.qi_acc, c.tp_acc};
+    for (void *q : cp) if (q) cudaFree(q);
+    c = CellGroup{};
+}
+
 void free_all(rbc_handle *h)
 {
     if (!h) return;
@@ -517,11 +569,7 @@ void free_all(rbc_handle *h)
     void *ptrs[] = {h->g[0], h->g[1], h->uvr, h->Fx, h->Fy, h->Fz, h->mask2d, h->tube_links, h->tube_frac,
                     h->d_int, h->d_drive, h->staging};
     for (void *q : ptrs) if (q) cudaFree(q);
-    for (CellGroup &c : h->cg) {
-        void *cp[] = {c.X, c.Xd, c.gref, c.erec, c.U, c.Fv, c.tri, c.v2e_off, c.v2e, c.nbr, c.visit, c.patch_off,
-                      c.patch_vtx, c.patch_stride, c.vol0, c.gx, c.vol_out, c.area_out, c.cen_out, c.qi_acc, c.tp_acc};
-        for (void *q : cp) if (q) cudaFree(q);
-    }
+    for (CellGroup &c : h->cg) free_group(c);
     adjoint_free(h->adj);
     h->adj = nullptr;
     if (h->stream) cudaStreamDestroy(h->stream);
@@ -585,7 +633,8 @@ int launch_bend_stage(rbc_handle *h)
         CellGroup &g = h->cg[k];
         if (g.ncell == 0 || g.br == 0.0) continue;
         BendArgs a{};
-        a.X = g.X; a.nv = g.nv; a.V = g.V; a.v2e_off = g.v2e_off; a.v2e = g.v2e; a.visit = g.visit;
+        a.X = g.X; a.nv = g.nv; a.V = g.V; a.E = g.E; a.v2e_off = g.v2e_off; a.v2e = g.v2e; a.visit = g.visit;
+        a.cs0 = g.cs0;
         a.LX = h->p.LX; a.LZ = h->p.LZ; a.coef = 2.0 / std::sqrt(3.0) * g.br; a.Fv = g.Fv;
         launch_bend(a, h->stream);
         h->launches++;
@@ -815,6 +864,7 @@ struct GroupPrep {
     std::vector<double> vol0, gx, xs;
     std::vector<double4> gref;
     std::vector<int4> visit;
+    std::vector<double2> cs0;
 };
 
 int prepare_group(rbc_handle *h, CellGroup &c, const rbc_mesh *mesh, GroupPrep &pp)
@@ -831,6 +881,7 @@ int prepare_group(rbc_handle *h, CellGroup &c, const rbc_mesh *mesh, GroupPrep &
     for (long long j = 0; j < c.nv; j++)
         for (int k = 0; k < 3; k++) pp.xs[k * c.nv + j] = mesh->xr[3 * j + k];
     if (c.br != 0.0) bend_visits(c.V, c.E, mesh->tri, pp.visit);
+    if (c.br != 0.0 && h->p.bend_spont) spontaneous_angles(h->p, c, mesh->xr, pp.visit, pp.cs0);
     return RBC_OK;
 }
 
@@ -847,6 +898,10 @@ int upload_group(rbc_handle *h, CellGroup &c, const rbc_mesh *mesh, const GroupP
     if (!pp.visit.empty()) {
         TRYG(dalloc(h, &c.visit, pp.visit.size()));
         CK(cudaMemcpy(c.visit, pp.visit.data(), sizeof(int4) * pp.visit.size(), cudaMemcpyHostToDevice));
+    }
+    if (!pp.cs0.empty()) {
+        TRYG(dalloc(h, &c.cs0, pp.cs0.size()));
+        CK(cudaMemcpy(c.cs0, pp.cs0.data(), sizeof(double2) * pp.cs0.size(), cudaMemcpyHostToDevice));
     }
     TRYG(dalloc(h, &c.patch_off, pp.poff.size())); TRYG(dalloc(h, &c.patch_vtx, pp.pvtx.size()));
     TRYG(dalloc(h, &c.patch_stride, pp.pstride.size()));
@@ -2134,10 +2189,7 @@ int rbc_add_wbc(rbc_handle *h, const rbc_mesh *mesh, double rgs, double br)
     int rc = prepare_group(h, c, mesh, prep);
     if (!rc) rc = upload_group(h, c, mesh, prep);
     if (rc) {   // leave the handle with the red cells only
-        void *cp[] = {c.X, c.Xd, c.gref, c.erec, c.U, c.Fv, c.tri, c.v2e_off, c.v2e, c.nbr, c.visit, c.patch_off,
-                      c.patch_vtx, c.patch_stride, c.vol0, c.gx, c.vol_out, c.area_out, c.cen_out};
-        for (void *q : cp) if (q) cudaFree(q);
-        c = CellGroup{};
+        free_group(c);
         return rc;
     }
     h->ngroups = 2;

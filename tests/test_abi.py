@@ -58,6 +58,7 @@ def test_rejects_unsupported_options(native_lib):
     assert _create(case, br=float("inf"))[0] == N.RBC_ERR_ARG
     assert _create(case, tau=0.5)[0] == N.RBC_ERR_ARG
     assert _create(case, storage=7)[0] == N.RBC_ERR_ARG
+    assert _create(case, bend_spont=2)[0] == N.RBC_ERR_ARG
 
 
 def test_rejects_bad_bc(native_lib):

@@ -110,6 +110,30 @@ def test_stress_with_bending_matches_oracle(oracle_mod, native_lib):
     assert np.abs(ref).max() > 1e-3 and err <= 1e-5
 
 
+def test_spontaneous_bending_matches_oracle(oracle_mod, native_lib):
+    """BR != 0 about the initial shape's dihedral angles (bend_spont = 1,
+    init1.cu:797-848 without the override of 849-850): rbc_stress against the
+    oracle after a developed flow, then five whole steps."""
+    case = parity_case(br=0.02, bend_spont=1)
+    o = oracle_mod.Oracle(case)
+    o.step(20)
+    sim = load(o)
+    c = clone(oracle_mod, o)
+    assert c.stress() == 0
+    sim.stress()
+    got = sim.export_cells()
+    ref = np.concatenate([c["cfx"], c["cfy"], c["cfz"]])
+    err = rel_l2(np.concatenate([got["fx"], got["fy"], got["fz"]]), ref)
+    print(f"stress + spontaneous bending: force rel L2 {err:.3e}")
+    assert err <= 1e-5
+    sim = load(o)
+    o.step(5)
+    sim.step(5)
+    got = sim.export_cells()
+    ref = np.concatenate([o["x"], o["y"], o["z"]])
+    assert np.abs(np.concatenate([got["x"], got["y"], got["z"]]) - ref).max() <= 1e-5 * np.abs(ref).max()
+
+
 def test_narrow_duct_cell_matches_oracle(oracle_mod, native_lib):
     """A 32-wide duct (the reference's x period LX = 28) with a 15.6-wide cell
     whose first vertex sits near the cell's edge in x: edge vectors must take

@@ -205,6 +205,66 @@ def test_bending_force_is_energy_gradient(oracle_mod):
             assert abs(-g - f[i, d]) <= 1e-6 * np.abs(f).max(), (i, d, -g, f[i, d])
 
 
+def _signed_angles(x, y, z, tri):
+    """cos and sin of the dihedral angle of every edge-neighbour pair, sin
+    signed by the centroid test of stress.cu:527 (symmetric in the pair)."""
+    p = np.stack([x, y, z], axis=1)
+    n = np.cross(p[tri[:, 1]] - p[tri[:, 0]], p[tri[:, 2]] - p[tri[:, 0]])
+    t = p[tri].mean(axis=1)
+    edges = {}
+    for e, tr in enumerate(tri):
+        for a in range(3):
+            edges.setdefault(tuple(sorted((tr[a], tr[(a + 1) % 3]))), []).append(e)
+    pairs = np.array([v for v in edges.values() if len(v) == 2])
+    n1, n2 = n[pairs[:, 0]], n[pairs[:, 1]]
+    cos = np.einsum("ij,ij->i", n1, n2) / np.linalg.norm(n1, axis=1) / np.linalg.norm(n2, axis=1)
+    sgn = np.where(np.einsum("ij,ij->i", n1 - n2, t[pairs[:, 0]] - t[pairs[:, 1]]) >= 0.0, 1.0, -1.0)
+    return cos, sgn * np.sqrt(np.clip(1.0 - cos * cos, 0.0, None))
+
+
+def test_spontaneous_bending_angles(oracle_mod):
+    """Bending about the initial shape's dihedral angles (init1.cu:797-848,
+    kept instead of the override of 849-850): no force on the initial shape;
+    on a perturbed shape the four-point forces are minus the gradient of
+    (2/sqrt 3) BR sum (1 - cos(theta - theta0)) over edge-neighbour pairs."""
+    case = configs.small_duct(subdiv=2, radius=5.0, br=0.05, Gs=1e-3, bend_spont=1)
+    o = oracle_mod.Oracle(case)
+    assert o.a["s0"].std() > 0.05   # an RBC shape: the angles differ from edge to edge
+
+    def bend(oo):
+        for k in ("cfx", "cfy", "cfz"):
+            oo[k][:] = 0.0
+        oracle_mod.lib().orc_bend(oracle_mod.C.byref(oo.p), oracle_mod.C.byref(oo.s))
+        return np.stack([oo["cfx"], oo["cfy"], oo["cfz"]], axis=1)
+
+    flat = oracle_mod.Oracle(case, bend_spont=False)
+    f_flat = bend(flat)
+    assert np.abs(bend(o)).max() <= 1e-12 * np.abs(f_flat).max()
+    xr = case.xr.reshape(-1, 3)
+    c0, s0 = _signed_angles(xr[:, 0], xr[:, 1], xr[:, 2], case.tri)
+    rng = np.random.default_rng(6)
+    for k in ("x", "y", "z"):
+        o[k][:] += rng.normal(scale=0.15, size=case.vertex)
+    f = bend(o)
+    assert np.abs(f).max() > 1e-3
+    assert np.abs(f.sum(axis=0)).max() <= 1e-12 * np.abs(f).max() * case.vertex
+    pos = np.stack([o["x"], o["y"], o["z"]], axis=1)
+    coef = 2.0 / math.sqrt(3.0) * 0.05
+
+    def energy(q):
+        cos, sin = _signed_angles(q[0], q[1], q[2], case.tri)
+        return coef * float((1.0 - cos * c0 - sin * s0).sum())
+
+    h = 1e-6
+    for i in rng.choice(case.vertex, 8, replace=False):
+        for d in range(3):
+            xp, xm = [pos[:, c].copy() for c in range(3)], [pos[:, c].copy() for c in range(3)]
+            xp[d][i] += h
+            xm[d][i] -= h
+            g = (energy(xp) - energy(xm)) / (2 * h)
+            assert abs(-g - f[i, d]) <= 1e-6 * np.abs(f).max(), (i, d, -g, f[i, d])
+
+
 @pytest.mark.parametrize("walls", [0, 1])
 def test_shear_mode_reaches_the_couette_profile(oracle_mod, walls):
     """CapsuleSHEARFLOW without cells: from rest, walls moving from step 1 on
