@@ -3,7 +3,7 @@
  *
  * One handle owns the device state of one simulation: a D3Q19 lattice stored
  * as pull-scheme SoA populations (f_i - w_i, FP32 or FP16), the Eulerian IB
- * force and velocity fields, and the red-cell meshes (FP64 positions, shared
+ * force and velocity fields, and the red- and white-cell meshes (FP64 positions, shared
  * triangle connectivity, per-element reference metric).
  *
  * The step entry points replace the reference's step modules one for one and
