@@ -28,7 +28,8 @@ class OrcParams(C.Structure):
                 ("LZ", C.c_double), ("xmin", C.c_double), ("xmax", C.c_double), ("zmin", C.c_double),
                 ("zmax", C.c_double), ("ncell", C.c_int), ("vertex", C.c_int), ("element", C.c_int),
                 ("mn", C.c_int), ("br", C.c_double), ("flow", C.c_int), ("sr", C.c_double), ("walls", C.c_int),
-                ("tube_r", C.c_double)]
+                ("tube_r", C.c_double), ("lambda1", C.c_double), ("vof_k", C.c_int),
+                ("vof_residual", C.c_double), ("vof_itrmax", C.c_int)]
 
 
 _STATE_D = ["fn", "fm", "dn", "un", "vn", "wn", "dm", "um", "vm", "wm", "fx", "fy", "fz"]
@@ -39,7 +40,7 @@ class OrcState(C.Structure):
     _fields_ = ([(k, _DP) for k in _STATE_D] + [("bc", _IP)] + [(k, _DP) for k in _STATE_CELL_D]
                 + [("ele", _IP), ("nln", _IP), ("ln", _IP), ("lo", _IP), ("nle", _IP), ("le", _IP),
                    ("volume0", _DP), ("gx", _DP), ("iter", C.c_int), ("bicg_iters", C.c_int), ("ec", _IP),
-                   ("crg", _DP), ("cbr", _DP), ("c0", _DP), ("s0", _DP)])
+                   ("crg", _DP), ("cbr", _DP), ("c0", _DP), ("s0", _DP), ("vf", _DP), ("vof_iters", C.c_int)])
 
 
 _lib = None
@@ -55,10 +56,11 @@ def lib() -> C.CDLL:
     global _lib
     if _lib is None:
         L = C.CDLL(str(build()))
-        for name in ("orc_fem_init", "orc_stress", "orc_calc_load", "orc_volume_correction", "orc_step"):
+        for name in ("orc_fem_init", "orc_stress", "orc_calc_load", "orc_volume_correction", "orc_step",
+                     "orc_front_tracking"):
             getattr(L, name).restype = C.c_int
         for name in ("orc_flu_init", "orc_volume_init", "orc_ibm_st1", "orc_lbm_d3q19", "orc_ibm_st2",
-                     "orc_calc_tension", "orc_q2f", "orc_bend", "orc_bend_reference"):
+                     "orc_calc_tension", "orc_q2f", "orc_bend", "orc_bend_reference", "orc_thinc_wlic"):
             getattr(L, name).restype = None
         L.orc_num_threads.restype = C.c_int
         L.orc_calc_volume.restype = None
@@ -96,7 +98,9 @@ class Oracle:
                            xmin=p["xmin"], xmax=p["xmax"], zmin=p["zmin"], zmax=p["zmax"], ncell=self.N,
                            vertex=self.V, element=self.E, mn=self.mn, br=float(p.get("br", 0.0)),
                            flow=int(p.get("flow", 0)), sr=float(p.get("sr", 0.0)), walls=int(p.get("walls", 0)),
-                           tube_r=float(p.get("tube_r", 0.0)))
+                           tube_r=float(p.get("tube_r", 0.0)), lambda1=float(p.get("lambda1", 1.0)),
+                           vof_k=int(p.get("vof_k", 0)), vof_residual=float(p.get("vof_residual", 1e-10)),
+                           vof_itrmax=int(p.get("vof_itrmax", 20000)))
         n = case.n
         self.a = {}
         for k in _STATE_D:
@@ -112,6 +116,7 @@ class Oracle:
         self.a["ec"] = np.zeros(3 * ne, dtype=np.int32)
         self.a["volume0"] = np.zeros(max(self.N, 1))
         self.a["gx"] = np.zeros(3 * max(self.N, 1))
+        self.a["vf"] = np.zeros(n)
         for k, v in (("crg", cell_rgs), ("cbr", cell_br)):
             if v is not None:
                 self.a[k] = np.ascontiguousarray(v, dtype=np.float64).reshape(-1)
@@ -142,6 +147,9 @@ class Oracle:
                 self.s.c0 = self.a["c0"].ctypes.data_as(_DP)
                 self.s.s0 = self.a["s0"].ctypes.data_as(_DP)
                 L.orc_bend_reference(C.byref(self.p), C.byref(self.s))
+            if self.p.vof_k > 0 and init_fluid:   # vof_init (init1.cu:1094-1120, main.cu:56)
+                if L.orc_front_tracking(C.byref(self.p), C.byref(self.s)) < 0:
+                    raise RuntimeError("oracle front tracking did not converge")
 
     # the population buffers swap like ltc->fnD / ltc->fmD (lbm.cu:1575)
     @property
@@ -187,6 +195,12 @@ class Oracle:
 
     def calc_tension(self):
         self._c("orc_calc_tension")
+
+    def thinc_wlic(self):
+        self._c("orc_thinc_wlic")
+
+    def front_tracking(self) -> int:
+        return self._c("orc_front_tracking")
 
     def step(self, n: int = 1) -> int:
         rc = lib().orc_step(C.byref(self.p), C.byref(self.s), int(n))

@@ -645,8 +645,9 @@ void orc_ibm_st2(const orc_params *p, orc_state *s)
 /* ------------------------------------------------------------------------ */
 
 /* lbm.cu:983-1313 (lbm_CapsuleCHANNELFLOW) + 1378-1432 (BUFF copy) +
- * 1435-1460 (average, M = 1) + pointer swap (1575).  LAMBDA1 = 1, so the
- * viscosity-ratio term of omega (1131) vanishes. */
+ * 1435-1460 (average, M = 1) + pointer swap (1575).  omega = 1 / (3 (1 +
+ * (LAMBDA1 - 1) vf) Df + 1/2) with Df = (tau - 1/2) / 3 (lbm.cu:1131); with
+ * LAMBDA1 = 1 that is 1 / tau, used as such. */
 void orc_lbm_d3q19(const orc_params *p, orc_state *s)
 {
     int nx = p->nx, ny = p->ny, nz = p->nz, iter = s->iter;
@@ -654,7 +655,8 @@ void orc_lbm_d3q19(const orc_params *p, orc_state *s)
     double Cr = p->Cr, Cr2 = Cr * Cr, P = p->P, B = p->B;
     double t = p->dt * (double)iter;
     double wi = (iter > p->flowstart) ? 1.0 + 0.5 * sin(M_PI * t / p->freq) : 0.0;
-    double om = 1.0 / p->tau;
+    const double om0 = 1.0 / p->tau, Df = (p->tau - 0.5) / 3.0;
+    const int visc = p->lambda1 != 1.0 && s->vf;
     const double *fn = s->fn; double *fm = s->fm;
     const int *bc = s->bc;
 #pragma omp parallel for schedule(static)
@@ -671,6 +673,7 @@ void orc_lbm_d3q19(const orc_params *p, orc_state *s)
         s->dn[i] = td; s->un[i] = tu; s->vn[i] = tv; s->wn[i] = tw;
         /* (iter-1)%M == 0 with M = 1: the averages restart every step */
         s->dm[i] = td; s->um[i] = tu; s->vm[i] = tv; s->wm[i] = tw;
+        const double om = visc ? 1.0 / (3.0 * (1.0 + (p->lambda1 - 1.0) * s->vf[i]) * Df + 0.5) : om0;
         double om1 = 1.0 - om, om2 = (1.0 - om / 2.0) * 2.0 * td * P, om3 = (1.0 - om / 2.0) * 2.0 * td * B;
         double uvw = -1.5 * (tu*tu + tv*tv + tw*tw) * Cr2;
         double gP[3] = {0.0, 0.0, wi}, gB[3] = {tfx, tfy, tfz}, uu[3] = {tu, tv, tw};
@@ -770,6 +773,249 @@ void orc_lbm_d3q19(const orc_params *p, orc_state *s)
     }
     /* lbm.cu:1435-1460 divides by M = 1; lbm.cu:1575 swaps the buffers */
     double *tmp = s->fn; s->fn = s->fm; s->fm = tmp;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Volume fraction: thincwlic.cu, fronttrack.cu, matrix_solver.cu            */
+/* ------------------------------------------------------------------------ */
+
+/* thincwlic.cu:12-106 (normal3d_st1, normal3d_st2): n2, the vf gradient at the
+ * cell corner below-left of every node with ix, iy, iz >= 1, and n1, the
+ * average of the eight corner gradients around every interior node */
+static void vof_normals(const orc_params *p, const double *vf, double *n1[3], double *n2[3])
+{
+    const int nx = p->nx, ny = p->ny, nz = p->nz;
+    const long n = (long)nx * ny * nz, pl = (long)nx * ny;
+    const double dx = p->dx;
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < n; i++) {
+        const long iz = i / pl, iy = i / nx - ny * iz, ix = i - nx * iy - pl * iz;
+        if (ix == 0 || iy == 0 || iz == 0) continue;
+        n2[0][i] = 0.25 / dx * (vf[i] - vf[i-1] + vf[i-nx] - vf[i-1-nx] + vf[i-pl] - vf[i-1-pl] + vf[i-nx-pl] - vf[i-1-nx-pl]);
+        n2[1][i] = 0.25 / dx * (vf[i] - vf[i-nx] + vf[i-1] - vf[i-1-nx] + vf[i-pl] - vf[i-nx-pl] + vf[i-1-pl] - vf[i-1-nx-pl]);
+        n2[2][i] = 0.25 / dx * (vf[i] - vf[i-pl] + vf[i-1] - vf[i-1-pl] + vf[i-nx] - vf[i-nx-pl] + vf[i-1-nx] - vf[i-1-nx-pl]);
+    }
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < n; i++) {
+        const long iz = i / pl, iy = i / nx - ny * iz, ix = i - nx * iy - pl * iz;
+        if (ix == 0 || iy == 0 || iz == 0 || ix == nx - 1 || iy == ny - 1 || iz == nz - 1) continue;
+        for (int d = 0; d < 3; d++) {
+            const double *m = n2[d];
+            n1[d][i] = 0.125 * (m[i] + m[i+pl] + m[i+1] + m[i+1+pl] + m[i+nx] + m[i+nx+pl] + m[i+1+nx] + m[i+1+nx+pl]);
+        }
+    }
+}
+
+void orc_thinc_wlic(const orc_params *p, orc_state *s)
+{
+    const int nx = p->nx, ny = p->ny, nz = p->nz;
+    const long n = (long)nx * ny * nz, pl = (long)nx * ny, shift = pl * (nz - 4);
+    const double dx = p->dx, dt = p->dt, beta = 2.0;
+    double *buf = (double *)calloc((size_t)n * 7, sizeof(double));
+    double *n1[3] = {buf, buf + n, buf + 2 * n}, *n2[3] = {buf + 3 * n, buf + 4 * n, buf + 5 * n}, *flux = buf + 6 * n;
+    double *vf = s->vf;
+    const int *bc = s->bc;
+    const double *u[3] = {s->um, s->vm, s->wm};
+    for (int idr = 0; idr < 3; idr++) {
+        vof_normals(p, vf, n1, n2);
+        const long acs = idr == 0 ? 1 : idr == 1 ? nx : pl;
+        /* wlic1d4md_st1 (thincwlic.cu:108-238): the flux through the face between
+         * i - acs and i, THINC in the upwind node weighted by its normal's share
+         * along the sweep (WLIC), plain upwind in full or empty nodes */
+#pragma omp parallel for schedule(static)
+        for (long i = 0; i < n; i++) {
+            flux[i] = 0.0;
+            const long iz = i / pl, iy = i / nx - ny * iz, ix = i - nx * iy - pl * iz;
+            if (ix == 0 || iy == 0 || iz == 0) continue;
+            if (ix == 1 || iy == 1 || iz == 1) continue;
+            if (ix == nx - 1 || iy == ny - 1 || iz == nz - 1) continue;
+            const double up = u[idr][i], um = u[idr][i - acs], uc = (up + um) / 2.0;
+            int isgn;
+            long ii;
+            if (uc <= 0.0) { isgn = 0; ii = i; } else { isgn = 1; ii = i - acs; }
+            const double nn = fabs(n1[0][ii]) + fabs(n1[1][ii]) + fabs(n1[2][ii]);
+            double f;
+            if (vf[ii] >= 1.0 - 1.0e-6 || vf[ii] <= 1.0e-6) f = vf[ii] * uc * 1.0 * dt;
+            else if (nn <= 1.0e-6) f = vf[ii] * uc * 1.0 * dt;
+            else {
+                /* the reference's three assignments of ib leave ii - acs (ii's z index is >= 1) */
+                const long ib = ii - acs;
+                const double alpha = vf[ib] <= vf[ii + acs] ? 1.0 : -1.0;
+                const double a1 = expf(beta * (2.0 * vf[ii] - 1.0) / alpha);
+                const double a3 = expf(beta);
+                const double xc = 0.5 / beta * log((a3 * a3 - a1 * a3) / (a1 * a3 - 1.0));
+                const double a4 = coshf(beta * ((double)isgn - uc * 1.0 * dt / dx - xc));
+                const double a5 = coshf(beta * ((double)isgn - xc));
+                f = 0.5 * (uc * 1.0 * dt - alpha * dx / beta * log(a4 / a5));
+                const double weight = fabs(n1[idr][ii]) / nn;
+                f = f * weight + vf[ii] * uc * 1.0 * dt * (1.0 - weight);
+            }
+            if (bc[i] == ORC_WALL || bc[i - acs] == ORC_WALL) f = 0.0;
+            flux[i] = f;
+        }
+        /* wlic1d4md_st2 (thincwlic.cu:241-272) */
+#pragma omp parallel for schedule(static)
+        for (long i = 0; i < n; i++)
+            if (bc[i] == ORC_COMP) vf[i] = vf[i] - (flux[i + acs] - flux[i]) / dx;
+        /* wlic1d4md_st3 (thincwlic.cu:275-313): BUFF nodes take their periodic
+         * images, WALL nodes 0 */
+#pragma omp parallel for schedule(static)
+        for (long i = 0; i < n; i++) {
+            if (bc[i] == ORC_COMP) continue;
+            if (bc[i] == ORC_BUFF) {
+                const long iz = i / pl, ix = (i % pl) % nx;
+                long i2 = i;
+                if (p->flow == 1) {
+                    if (ix <= 1) i2 += nx - 4;
+                    if (ix >= nx - 2) i2 -= nx - 4;
+                }
+                if (iz <= 1) i2 += shift;
+                if (iz >= nz - 2) i2 -= shift;
+                vf[i] = vf[i2];
+            } else if (bc[i] == ORC_WALL) {
+                vf[i] = 0.0;
+            }
+        }
+    }
+    free(buf);
+}
+
+static long pow2_at_least(long n)
+{
+    long m = 1;
+    while (m < n) m *= 2;
+    return m;
+}
+
+int orc_front_tracking(const orc_params *p, orc_state *s)
+{
+    const int nx = p->nx, ny = p->ny, nz = p->nz;
+    const long n = (long)nx * ny * nz, pl = (long)nx * ny, mn = pow2_at_least(n);
+    const long ne = (long)p->ncell * p->element;
+    const double dx = p->dx, LX = p->LX, LZ = p->LZ;
+    const int *bc = s->bc;
+    if (p->ncell == 0) {   /* nothing to track (the reference's solve would divide by |b| = 0) */
+        memset(s->vf, 0, sizeof(double) * (size_t)n);
+        return 0;
+    }
+    double *g[3], *dg = (double *)calloc((size_t)mn * 7, sizeof(double));
+    g[0] = dg + mn; g[1] = dg + 2 * mn; g[2] = dg + 3 * mn;
+    double *b = dg + 4 * mn, *x = dg + 5 * mn, *r = dg + 6 * mn;
+    /* front_tracking_source2 (fronttrack.cu:351-455): every triangle spreads
+     * its inward normal times its area with the 4-point cosine delta around
+     * its centroid; nodes outside the lattice are dropped.  Serial, so the sums
+     * run in element order. */
+    for (long e = 0; e < ne; e++) {
+        const int j1 = s->ele[3*e], j2 = s->ele[3*e+1], j3 = s->ele[3*e+2];
+        double tx1 = s->x[j1], tx2 = s->x[j2], tx3 = s->x[j3];
+        double ty1 = s->y[j1], ty2 = s->y[j2], ty3 = s->y[j3];
+        double tz1 = s->z[j1], tz2 = s->z[j2], tz3 = s->z[j3];
+        double xx1 = tx2 - tx1, yy1 = ty2 - ty1, zz1 = tz2 - tz1;
+        if (xx1 > LX * 0.5) { xx1 -= LX; tx1 += LX; } else if (xx1 < -LX * 0.5) { xx1 += LX; tx2 += LX; }
+        if (zz1 > LZ * 0.5) { zz1 -= LZ; tz1 += LZ; } else if (zz1 < -LZ * 0.5) { zz1 += LZ; tz2 += LZ; }
+        double xx2 = tx3 - tx1, yy2 = ty3 - ty1, zz2 = tz3 - tz1;
+        if (xx2 > LX * 0.5) { xx2 -= LX; tx1 += LX; } else if (xx2 < -LX * 0.5) { xx2 += LX; tx3 += LX; }
+        if (zz2 > LZ * 0.5) { zz2 -= LZ; tz1 += LZ; } else if (zz2 < -LZ * 0.5) { zz2 += LZ; tz3 += LZ; }
+        const double xg = (tx1 + tx2 + tx3) / 3.0, yg = (ty1 + ty2 + ty3) / 3.0, zg = (tz1 + tz2 + tz3) / 3.0;
+        const double xtr = xg + (double)(nx - 1) * dx / 2.0, ytr = yg + (double)(ny - 1) * dx / 2.0,
+                     ztr = zg + (double)(nz - 1) * dx / 2.0;
+        const int x1 = (int)floor(xtr / dx) - 1, x2 = (int)ceil(xtr / dx) + 1;
+        const int y1 = (int)floor(ytr / dx) - 1, y2 = (int)ceil(ytr / dx) + 1;
+        const int z1 = (int)floor(ztr / dx) - 1, z2 = (int)ceil(ztr / dx) + 1;
+        double nvx = -(yy1 * zz2 - zz1 * yy2), nvy = -(zz1 * xx2 - xx1 * zz2), nvz = -(xx1 * yy2 - yy1 * xx2);
+        const double nn = sqrt(nvx * nvx + nvy * nvy + nvz * nvz), ds = nn / 2.0;
+        nvx /= nn; nvy /= nn; nvz /= nn;
+        for (int iz = z1; iz <= z2; iz++)
+            for (int iy = y1; iy <= y2; iy++)
+                for (int ix = x1; ix <= x2; ix++) {
+                    if (ix < 0 || ix >= nx || iy < 0 || iy >= ny || iz < 0 || iz >= nz) continue;
+                    const long i = ix + (long)nx * iy + pl * iz;
+                    const double xx = (double)ix * dx - xtr, yy = (double)iy * dx - ytr, zz = (double)iz * dx - ztr;
+                    const double xcos = 1.0 + cos(M_PI * xx / (2.0 * dx)), ycos = 1.0 + cos(M_PI * yy / (2.0 * dx)),
+                                 zcos = 1.0 + cos(M_PI * zz / (2.0 * dx));
+                    const double dlt = xcos * ycos * zcos / (64.0 * dx * dx * dx);
+                    g[0][i] += dlt * nvx * ds;
+                    g[1][i] += dlt * nvy * ds;
+                    g[2][i] += dlt * nvz * ds;
+                }
+    }
+    /* front_tracking_source3 (fronttrack.cu:458-537): COMP nodes within two
+     * planes (columns) of a periodic end add their BUFF images and copy the sum
+     * back to them */
+    for (long i = 0; i < n; i++) {
+        if (bc[i] != ORC_COMP) continue;
+        const long iz = i / pl, iy = i / nx - ny * iz, ix = i - nx * iy - pl * iz;
+        long im[3] = {-1, -1, -1};
+        const long sz = pl * (nz - 4), sx = nx - 4;
+        if (p->flow == 1) {
+            const long dxs = ix <= 3 ? sx : (ix >= nx - 4 ? -sx : 0), dzs = iz <= 3 ? sz : (iz >= nz - 4 ? -sz : 0);
+            if (dxs && dzs) { im[0] = i + dxs; im[1] = i + dzs; im[2] = i + dxs + dzs; }
+            else if (dxs) im[0] = i + dxs;
+            else if (dzs) im[0] = i + dzs;
+        } else {
+            if (iz <= 3) im[0] = i + sz; else if (iz >= nz - 4) im[0] = i - sz;
+        }
+        for (int d = 0; d < 3; d++) {
+            for (int k = 0; k < 3; k++) if (im[k] >= 0) g[d][i] += g[d][im[k]];
+            for (int k = 0; k < 3; k++) if (im[k] >= 0) g[d][im[k]] = g[d][i];
+        }
+    }
+    /* front_tracking_source4 (fronttrack.cu:540-583): divergence on COMP nodes;
+     * jacobi_source: b = dg / diagonal (-6 / dx^2 on COMP rows, 1 elsewhere) */
+    for (long i = 0; i < n; i++) {
+        if (bc[i] != ORC_COMP) continue;
+        const double d = (g[0][i+1] - g[0][i-1] + g[1][i+nx] - g[1][i-nx] + g[2][i+pl] - g[2][i-pl]) / (2.0 * dx);
+        b[i] = d / (-6.0 / (dx * dx));
+    }
+    /* the matrix of front_tracking_matrix (fronttrack.cu:27-238) after
+     * jacobi_matrix: COMP rows the 7-point Laplacian over -6/dx^2 (neighbours
+     * (1/dx^2) / (-6/dx^2), diagonal 1); BUFF rows x_i - x_image = 0; WALL and
+     * padding rows x_i = 0 */
+    const double off = (1.0 / (dx * dx)) / (-6.0 / (dx * dx));
+    double bb = 0.0;
+    for (long i = 0; i < mn; i++) bb += b[i] * b[i];
+    int result = -1;
+    for (int cnt = 0; cnt <= 10 && result < 0; cnt++) {
+        for (long i = 0; i < mn; i++) { x[i] = (double)cnt; r[i] = 0.0; }   /* front_tracking_solution */
+        int iter;
+        for (iter = 0; iter < p->vof_itrmax; iter++) {
+            for (int color = 0; color < 2; color++) {   /* redblacksor_1, redblacksor_2 */
+                for (long t = 0; t < mn; t++) {
+                    long par;
+                    if (t < n) { const long iz = t / pl, iy = t / nx - ny * iz, ix = t - nx * iy - pl * iz; par = ix + iy + iz; }
+                    else par = t;
+                    if (par % 2 != color) continue;
+                    double sum;
+                    if (t >= n || bc[t] == ORC_WALL) sum = 1.0 * x[t];
+                    else if (bc[t] == ORC_COMP) {
+                        sum = 0.0;
+                        sum += off * x[t - pl]; sum += off * x[t - nx]; sum += off * x[t - 1]; sum += 1.0 * x[t];
+                        sum += off * x[t + 1]; sum += off * x[t + nx]; sum += off * x[t + pl];
+                    } else {   /* BUFF: the image of fronttrack.cu:104-124 / 146-150 */
+                        const long iz = t / pl, ix = (t % pl) % nx;
+                        long img = t;
+                        if (p->flow == 1) {
+                            if (ix <= 1) img += nx - 4; else if (ix >= nx - 2) img -= nx - 4;
+                        }
+                        if (iz <= 1) img += pl * (nz - 4); else if (iz >= nz - 2) img -= pl * (nz - 4);
+                        sum = 0.0;
+                        if (t < img) { sum += 1.0 * x[t]; sum += -1.0 * x[img]; }
+                        else { sum += -1.0 * x[img]; sum += 1.0 * x[t]; }
+                    }
+                    r[t] = b[t] - sum;
+                    x[t] += 1.3 * r[t];
+                }
+            }
+            double rr = 0.0;
+            for (long i = 0; i < mn; i++) rr += r[i] * r[i];
+            if (sqrt(rr / bb) < p->vof_residual) break;
+        }
+        if (iter < p->vof_itrmax) result = iter + 1;
+    }
+    s->vof_iters = result;
+    if (result > 0) memcpy(s->vf, x, sizeof(double) * (size_t)n);
+    free(dg);
+    return result;
 }
 
 /* ------------------------------------------------------------------------ */
@@ -901,8 +1147,8 @@ int orc_volume_correction(const orc_params *p, orc_state *s)
     return iter - 1;
 }
 
-/* main.cu:73-110 with M = 1 (adhesion, THINC/WLIC and front tracking are off
- * for LAMBDA1 = 1 and CYTOADHESION = false) */
+/* main.cu:73-110 with M = 1 (no adhesion: CYTOADHESION = false); THINC/WLIC
+ * and front tracking when vof_k > 0 */
 int orc_step(const orc_params *p, orc_state *s, int nsteps)
 {
     for (int k = 0; k < nsteps; k++) {
@@ -913,10 +1159,12 @@ int orc_step(const orc_params *p, orc_state *s, int nsteps)
             orc_ibm_st1(p, s);
         }
         orc_lbm_d3q19(p, s);
-        if (p->ncell > 0) {
-            orc_ibm_st2(p, s);
-            if (orc_volume_correction(p, s) < 0) return 5;
+        if (p->ncell > 0) orc_ibm_st2(p, s);
+        if (p->vof_k > 0 && s->vf) {
+            orc_thinc_wlic(p, s);
+            if (s->iter % p->vof_k == 0 && orc_front_tracking(p, s) < 0) return 6;   /* error(5) */
         }
+        if (p->ncell > 0 && orc_volume_correction(p, s) < 0) return 5;
     }
     return 0;
 }

@@ -59,6 +59,14 @@ typedef struct orc_params {
     int walls;           /* 0: allwall (walls at -/+ sr LY / 2), 1: topwall (top at sr LY) */
     double tube_r;       /* > 0 (channel mode): interpolated bounce-back on the circle x^2 + y^2 = tube_r^2
                           * after streaming (lbm_cylinder.cu:116-231); 0: half-way bounce-back only */
+    /* volume fraction of the cells (VOF): vof_k = K > 0 turns it on (CN != 0):
+     * front tracking at setup (vof_init, init1.cu:1094-1120) and every K steps,
+     * THINC/WLIC advection every step, omega = 1 / (3 (1 + (LAMBDA1 - 1) vf) Df
+     * + 1/2) in the collision (lbm.cu:1131) */
+    double lambda1;      /* LAMBDA1: viscosity ratio inside / outside the cells */
+    int vof_k;           /* K: steps between front-tracking solves; 0 = no VOF (CN = 0) */
+    double vof_residual; /* RESIDUAL of the front-tracking solve (matrix_solver.cu:112-216) */
+    int vof_itrmax;      /* ITRMAX of that solve */
 } orc_params;
 
 typedef struct orc_state {
@@ -90,6 +98,8 @@ typedef struct orc_state {
     /* [3*ne] spontaneous angle (cos, sin) of each bending visit, or NULL for
      * (1, 0) as init1.cu:849-850 leaves it; orc_bend_reference fills them */
     double *c0, *s0;
+    double *vf;                            /* [n] ltc->vf: volume fraction of the cells (VOF) */
+    int    vof_iters;                      /* diagnostics: last front-tracking solve's sweeps */
 } orc_state;
 
 /* init2.cu:258-400 (fem_init): link tables and the reference metric from the
@@ -114,6 +124,15 @@ void orc_ibm_st2(const orc_params *p, orc_state *s);
 /* volume_correction.cu:453-524.  Returns iterations - 1, or -1 when the
  * 1000-iteration cap is hit (the reference calls exit(1) there). */
 int  orc_volume_correction(const orc_params *p, orc_state *s);
+
+/* thincwlic.cu:316-420 (thinc_wlic, red cells): three directional THINC/WLIC
+ * sweeps of s->vf with the step's velocity um, vm, wm. */
+void orc_thinc_wlic(const orc_params *p, orc_state *s);
+/* fronttrack.cu:628-700 (front_tracking, red cells): the indicator gradient
+ * of the cell surfaces, its divergence, and the Poisson solve (red-black SOR,
+ * matrix_solver.cu:112-216) into s->vf.  Returns the sweeps of the converged
+ * attempt, or -1 when 10 attempts did not converge (the reference's error(5)). */
+int  orc_front_tracking(const orc_params *p, orc_state *s);
 
 /* main.cu:73-110 with M = 1: nsteps full steps.  Returns 0 or an error code. */
 int  orc_step(const orc_params *p, orc_state *s, int nsteps);

@@ -10,8 +10,10 @@
  *
  * Case-dependent values (lengths, forcing, moduli, solver tolerance) come
  * from -DREF_* flags (see oracle/Makefile and tests/golden/make_golden.py).
- * Lattice units: Cr = dx = dt = 1, M = 1, RK4, LAMBDA1 = 1 (tau = 3 Df + 1/2),
- * bending modulus BR from -DREF_BR (default 0), no adhesion, no white cells.
+ * Lattice units: Cr = dx = dt = 1, M = 1, RK4, tau = 3 Df + 1/2, bending
+ * modulus BR from -DREF_BR (default 0), viscosity ratio LAMBDA1 and
+ * front-tracking interval K from -DREF_LAMBDA1 / -DREF_K (defaults 1 and
+ * never), CN = 1, no adhesion, no white cells.
  */
 #ifndef REF_HARNESS_DEF_H
 #define REF_HARNESS_DEF_H
@@ -84,10 +86,17 @@
 #define FREQ      (REF_FREQ)
 #define FLOWSTART (REF_FLOWSTART)
 
+#ifndef REF_LAMBDA1
+#define REF_LAMBDA1 1.0
+#endif
+#ifndef REF_K
+#define REF_K 1000000000
+#endif
+
 #define Cr          1.0
 #define M           1
-#define K           1000000000
-#define LAMBDA1     1.0
+#define K           (REF_K)
+#define LAMBDA1     (REF_LAMBDA1)
 #define LAMBDA2     1.0
 #define RUNGE_KUTTA 4
 #define N_R         1
@@ -188,5 +197,9 @@ void lbm_d3q19(process *prc, domain *cdo, lattice *ltc);
 int  volume_correction(domain *cdo, cell *cel, fem *fem);
 void volume_init(domain *cdo, cell *cel);
 void fem_init(cell *cel, fem *fem);
+int redblacksor(int *d_ptr, int *d_index, double *d_value, double *d_x, double *d_b, double *d_r, double *d_o,
+                int n, int nnz, int nx, int ny, int nz, int nn);
+void thinc_wlic(domain *cdo, lattice *ltc);
+void front_tracking(domain *cdo, lattice *ltc, cell *cel);
 
 #endif

@@ -8,9 +8,10 @@
 // inputs given by the caller instead of mesh files and a clock-seeded
 // rotation, then calls the reference's fem_init (init2.cu:258) and
 // volume_init (volume_correction.cu:427) and steps with the reference's own
-// stress / ibm_st1 / lbm_d3q19 / ibm_st2 / volume_correction in the order of
-// main.cu:73-110 (M = 1; adhesion, THINC/WLIC and front tracking are inactive
-// for CYTOADHESION = false and LAMBDA1 = 1).
+// stress / ibm_st1 / lbm_d3q19 / ibm_st2 / thinc_wlic / front_tracking /
+// volume_correction in the order of main.cu:73-110 (M = 1, no adhesion).
+// vof_init's front tracking (init1.cu:1094-1120) runs in ref_vof_init when the
+// library was built with a finite K; with vf = 0 THINC/WLIC changes nothing.
 #include <math.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -96,6 +97,8 @@ int ref_setup(int nx, int ny, int nz, const int *bc, int ncell, int V, int E, co
     up(g_ltc.fnD, f.data(), (size_t)n * Q);
     up(g_ltc.dnD, one.data(), n); up(g_ltc.dmD, one.data(), n);
     up(g_ltc.bcD, bc, n);
+    g_ltc.bcH = (int *)malloc(sizeof(int) * (size_t)n);   // front_tracking_matrix reads the host map
+    memcpy(g_ltc.bcH, bc, sizeof(int) * (size_t)n);
     // cells (cel_init 626-853 without the file reads; mem_init 933-1005)
     cell &c = g_cel;
     c.n = ncell; c.vertex = V; c.element = E; c.rg = 1.0; c.br = BR; c.gs = GS;
@@ -190,6 +193,14 @@ int ref_stage(int which)
     return r;
 }
 
+// vof_init (init1.cu:1094-1120): the volume fraction of the initial cells
+int ref_vof_init(void)
+{
+    front_tracking(&g_cdo, &g_ltc, &g_cel);
+    cudaDeviceSynchronize();
+    return g_err;
+}
+
 // main.cu:73-110 with M = 1
 int ref_step(int nsteps)
 {
@@ -199,10 +210,22 @@ int ref_step(int nsteps)
         ibm_st1(&g_cdo, &g_ltc, &g_cel);
         lbm_d3q19(&g_prc, &g_cdo, &g_ltc);
         ibm_st2(&g_cdo, &g_ltc, &g_cel, &g_fem);
+        if (K < 1000000000) {   // THINC/WLIC and front tracking (main.cu:93-98)
+            thinc_wlic(&g_cdo, &g_ltc);
+            if (g_prc.iter % K == 0) front_tracking(&g_cdo, &g_ltc, &g_cel);
+        }
         volume_correction(&g_cdo, &g_cel, &g_fem);
     }
     cudaDeviceSynchronize();
     return g_err;
+}
+
+// ltc->vfD [n]
+int ref_get_vf(double *vf)
+{
+    cudaDeviceSynchronize();
+    down(vf, g_ltc.vfD, (size_t)g_cdo.n);
+    return 0;
 }
 
 // ms[5]: device time of stress, ibm_st1, lbm_d3q19, ibm_st2, volume_correction

@@ -6,9 +6,13 @@ oracle is pinned against outputs of the reference's own step modules
 compiled unmodified from the reference sources with the project-written
 oracle/ref_harness (def.h stand-in, helper shims, driver).
 
-    python tests/golden/make_golden.py build            # here: nvcc, needs the reference sources
-    python tests/golden/make_golden.py run OUTDIR       # on a GPU: writes OUTDIR/<case>.npz
+    python tests/golden/make_golden.py build [CASE...]          # here: nvcc, needs the reference sources
+    python tests/golden/make_golden.py run OUTDIR [CASE...]     # on a GPU: writes OUTDIR/<case>.npz
     python tests/golden/make_golden.py time-dense       # on a GPU: reference step timing, dense suspension
+
+g4 runs the volume fraction (front tracking every K = 10 steps, THINC/WLIC
+every step) with viscosity ratio LAMBDA1 = 5: fronttrack.cu and thincwlic.cu
+join the compiled modules.
 
 The reference takes lengths and physical constants as compile-time macros, so
 each case gets its own library (oracle/_ref/librefstep_<case>.so).  Inputs are
@@ -56,7 +60,18 @@ def golden_cases():
         "g3_duct24x20x20_1c_bend": configs.duct_case("g3_duct24x20x20_1c_bend", 24, 20, 20,
                                                      centers_duct=[(12.3, 9.6, 9.4)], subdiv=3, radius=5.5,
                                                      seed=23, g=4e-5, Gs=2e-3, br=0.02, residual=1e-12),
+        "g4_duct24x20x20_1c_vof": configs.duct_case("g4_duct24x20x20_1c_vof", 24, 20, 20,
+                                                    centers_duct=[(12.3, 9.6, 9.4)], subdiv=3, radius=5.5,
+                                                    seed=24, g=4e-5, Gs=2e-3, residual=1e-12, itrmax=20000,
+                                                    lambda1=5.0, vof_k=10, vof_residual=1e-12,
+                                                    vof_itrmax=20000),
     }
+
+
+def snapshots(case):
+    """Steps after which a fixture holds the state: with VOF (front tracking
+    every K = 10 steps) also one five steps after a solve."""
+    return (1, 25, 30) if case.params["vof_k"] > 0 else SNAPSHOTS
 
 
 def dense_case():
@@ -68,11 +83,14 @@ def ref_defs(case) -> str:
     df = (2.0 * p["tau"] - 1.0) / 6.0
     return (f"-DREF_LX={p['LX']!r} -DREF_LY={float(p['ny'] - 4)!r} -DREF_LZ={p['LZ']!r} -DREF_P={p['P']!r} "
             f"-DREF_B={p['B']!r} -DREF_C={p['C']!r} -DREF_DF={df!r} -DREF_RESIDUAL={p['residual']!r} "
-            f"-DREF_ITRMAX={p['itrmax']} -DREF_BR={p['br']!r}")
+            f"-DREF_ITRMAX={p['itrmax']} -DREF_BR={p['br']!r} -DREF_LAMBDA1={p['lambda1']!r} "
+            f"-DREF_K={p['vof_k'] if p['vof_k'] > 0 else 1000000000}")
 
 
-def build():
+def build(names=()):
     for name, case in list(golden_cases().items()) + [("dense", dense_case())]:
+        if names and name not in names:
+            continue
         subprocess.run(["make", "-s", "-C", str(ROOT / "oracle"), "ref", f"REFTAG={name}",
                         f"REFDEFS={ref_defs(case)}"], check=True)
         print("built", REF_DIR / f"librefstep_{name}.so")
@@ -91,6 +109,13 @@ class Ref:
                               case.element, tri.ctypes.data_as(C.c_void_p), xr.ctypes.data_as(C.c_void_p))
         if rc:
             raise RuntimeError(f"ref_setup failed: {rc}")
+        if case.params["vof_k"] > 0 and self.L.ref_vof_init():
+            raise RuntimeError("reference vof_init failed")
+
+    def vf(self):
+        out = np.empty(self.case.n)
+        self.L.ref_get_vf(out.ctypes.data_as(C.c_void_p))
+        return out
 
     def step(self, n):
         rc = self.L.ref_step(int(n))
@@ -114,20 +139,27 @@ class Ref:
         return out
 
 
-def run(outdir):
+def run(outdir, names=()):
     outdir = Path(outdir)
     outdir.mkdir(parents=True, exist_ok=True)
     for name, case in golden_cases().items():
+        if names and name not in names:
+            continue
         ref = Ref(name, case)
         m = case.bc == configs.COMP
         data = {}
         c0 = ref.cells()
         data["setup_nd"], data["setup_volume0"], data["setup_gx"] = c0["nd"], c0["volume0"], c0["gx"]
+        vof = case.params["vof_k"] > 0
+        if vof:
+            data["setup_vf"] = ref.vf()[m]
         done = 0
-        for s in SNAPSHOTS:
+        for s in snapshots(case):
             ref.step(s - done)
             done = s
             lat, cel = ref.lattice(), ref.cells()
+            if vof:
+                data[f"s{s}_vf"] = ref.vf()[m]
             for k in ("dn", "un", "vn", "wn"):
                 data[f"s{s}_{k}"] = lat[k][m]
             for k in ("x", "y", "z", "u", "v", "w", "fx", "fy", "fz", "gx"):
@@ -157,9 +189,9 @@ def time_dense(steps=3):
 if __name__ == "__main__":
     cmd = sys.argv[1] if len(sys.argv) > 1 else "build"
     if cmd == "build":
-        build()
+        build(sys.argv[2:])
     elif cmd == "run":
-        run(sys.argv[2] if len(sys.argv) > 2 else ROOT / "gpurun_out" / "golden")
+        run(sys.argv[2] if len(sys.argv) > 2 else ROOT / "gpurun_out" / "golden", sys.argv[3:])
     elif cmd == "time-dense":
         time_dense(int(sys.argv[2]) if len(sys.argv) > 2 else 3)
     else:

@@ -11,7 +11,7 @@ from pathlib import Path
 import numpy as np
 import pytest
 
-from tests.golden.make_golden import SNAPSHOTS, golden_cases
+from tests.golden.make_golden import golden_cases, snapshots
 from preprocess_src_b200 import configs
 
 GOLDEN = Path(__file__).resolve().parent / "golden"
@@ -33,21 +33,33 @@ def test_oracle_matches_reference_kernels(name, case, oracle_mod):
     assert np.allclose(o["volume0"], g["setup_volume0"], rtol=1e-13)
     assert np.allclose(o["gx"], g["setup_gx"], rtol=0, atol=1e-12)
     m = case.bc == configs.COMP
+    vof = case.params["vof_k"] > 0
+    # with the volume fraction, THINC/WLIC rounds through the float expf/coshf
+    # (thincwlic.cu:193-198), whose last bit differs between glibc and CUDA:
+    # ~1e-8 per node and step in vf, and through omega in the flow
+    utol = 1e-7 if vof else 1e-9
+    loose = 1e3 if vof else 1.0   # the same through the flow into the cells
+    if vof:
+        print(f"setup vf max|d| {np.abs(o['vf'][m] - g['setup_vf']).max():.2e}")
+        assert np.abs(o["vf"][m] - g["setup_vf"]).max() <= 1e-9
     done = 0
-    for s in SNAPSHOTS:
+    for s in snapshots(case):
         o.step(s - done)
         done = s
         u = np.concatenate([o["un"][m], o["vn"][m], o["wn"][m]])
         uref = np.concatenate([g[f"s{s}_un"], g[f"s{s}_vn"], g[f"s{s}_wn"]])
-        assert rel(u, uref) <= 1e-9, (s, rel(u, uref))
-        assert np.abs(o["dn"][m] - g[f"s{s}_dn"]).max() <= 1e-12
+        if vof:
+            print(f"step {s}: vf max|d| {np.abs(o['vf'][m] - g[f's{s}_vf']).max():.2e}  u rel {rel(u, uref):.2e}")
+            assert np.abs(o["vf"][m] - g[f"s{s}_vf"]).max() <= 1e-6
+        assert rel(u, uref) <= utol, (s, rel(u, uref))
+        assert np.abs(o["dn"][m] - g[f"s{s}_dn"]).max() <= 1e-12 * loose
         x = np.concatenate([o[k] for k in ("x", "y", "z")])
         xref = np.concatenate([g[f"s{s}_{k}"] for k in ("x", "y", "z")])
-        assert np.abs(x - xref).max() <= 1e-12 * np.abs(xref).max(), (s, np.abs(x - xref).max())
-        assert np.abs(o["u"] - g[f"s{s}_u"]).max() <= 1e-12
+        assert np.abs(x - xref).max() <= 1e-12 * loose * np.abs(xref).max(), (s, np.abs(x - xref).max())
+        assert np.abs(o["u"] - g[f"s{s}_u"]).max() <= 1e-12 * loose
         # at step 1 the cells are still at their stress-free shape and the
         # forces are round-off (~1e-13), hence the absolute floor
         f = np.concatenate([o[k] for k in ("cfx", "cfy", "cfz")])
         fref = np.concatenate([g[f"s{s}_{k}"] for k in ("fx", "fy", "fz")])
-        assert np.abs(f - fref).max() <= 1e-8 * np.abs(fref).max() + 1e-12, (s, np.abs(f - fref).max())
-        assert np.abs(o["gx"] - g[f"s{s}_gx"]).max() <= 1e-10
+        assert np.abs(f - fref).max() <= 1e-8 * loose * np.abs(fref).max() + 1e-12, (s, np.abs(f - fref).max())
+        assert np.abs(o["gx"] - g[f"s{s}_gx"]).max() <= 1e-10 * loose

@@ -9,7 +9,7 @@ from pathlib import Path
 import numpy as np
 import pytest
 
-from tests.golden.make_golden import SNAPSHOTS, golden_cases
+from tests.golden.make_golden import golden_cases, snapshots
 from preprocess_src_b200 import configs
 
 pytestmark = pytest.mark.gpu
@@ -31,7 +31,7 @@ def test_gpu_matches_reference_kernels(name, case, native_lib):
     sim = Simulation(case)
     m = case.bc == configs.COMP
     done = 0
-    for s in SNAPSHOTS:
+    for s in snapshots(case):
         sim.step(s - done)
         done = s
         lat = sim.export_lattice(fn=False)

@@ -338,3 +338,23 @@ def test_oracle_per_cell_membrane_coefficients(oracle_mod):
     np.testing.assert_array_equal(mixed[:, :V], at(rgs=1.0, br=0.0)[:, :V])
     np.testing.assert_array_equal(mixed[:, V:], at(rgs=2.5, br=0.02)[:, V:])
     assert np.abs(mixed[:, V:] - at(rgs=1.0)[:, V:]).max() > 1e-6
+
+
+def test_volume_fraction_invariants(oracle_mod):
+    """Front tracking (fronttrack.cu) gives the cells' indicator: its sum over
+    the fluid is the cell volume, it vanishes on walls and its BUFF planes
+    hold their periodic images; THINC/WLIC (thincwlic.cu) moves it through
+    faces only, so the sum stays."""
+    case = configs.duct_case("vof", 24, 20, 20, centers_duct=[(3.0, 9.5, 9.5)], subdiv=3, radius=5.0, seed=3,
+                             g=4e-5, Gs=2e-3, vof_k=10, lambda1=5.0)
+    o = oracle_mod.Oracle(case)
+    m = case.bc == configs.COMP
+    vf = o["vf"].reshape(case.nz, case.ny, case.nx)
+    assert o.s.vof_iters > 0
+    assert abs(o["vf"][m].sum() - o["volume0"][0]) <= 0.01 * o["volume0"][0]
+    assert not o["vf"][case.bc == configs.WALL].any()
+    np.testing.assert_allclose(vf[:2][:, 1:-1, 1:-1], vf[-4:-2][:, 1:-1, 1:-1], rtol=0, atol=1e-9)   # to the solve's tolerance
+    total = o["vf"][m].sum()
+    o.step(9)   # THINC/WLIC every step, no solve before step 10
+    assert abs(o["vf"][m].sum() - total) <= 1e-11 * total
+    assert np.abs(o["vf"] - vf.reshape(-1)).max() > 1e-4   # it moved
