@@ -349,7 +349,7 @@ def test_volume_fraction_invariants(oracle_mod):
                              g=4e-5, Gs=2e-3, vof_k=10, lambda1=5.0)
     o = oracle_mod.Oracle(case)
     m = case.bc == configs.COMP
-    vf = o["vf"].reshape(case.nz, case.ny, case.nx)
+    vf = o["vf"].reshape(case.nz, case.ny, case.nx).copy()
     assert o.s.vof_iters > 0
     assert abs(o["vf"][m].sum() - o["volume0"][0]) <= 0.01 * o["volume0"][0]
     assert not o["vf"][case.bc == configs.WALL].any()
