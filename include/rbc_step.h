@@ -85,6 +85,7 @@ extern "C" {
 #define RBC_FLAG_NONFINITE         0x2
 #define RBC_FLAG_SPREAD_OVERFLOW   0x4   /* informational: a cell used the direct-atomic spread path */
 #define RBC_FLAG_SOLVE_RESIDUAL    0x8   /* membrane load solve residual above 1e-3 */
+#define RBC_FLAG_VOF_NOT_CONVERGED 0x10  /* a front-tracking solve hit vof_itrmax (the reference's error(5)) */
 
 typedef struct rbc_params {
     /* lattice (reference frame, nz includes the 4 BUFF planes) */
@@ -123,6 +124,14 @@ typedef struct rbc_params {
      * c0 = 1, s0 = 0); 1 = the initial shape's dihedral angles, the values
      * init1.cu:797-848 (init3.cu:313-364) compute before that override */
     int    bend_spont;
+    /* volume fraction of the cells (VOF, fronttrack.cu / thincwlic.cu): vof_k = K > 0
+     * (CN != 0) tracks it, by front tracking at rbc_create (vof_init) and every K steps
+     * and THINC/WLIC advection every step; the collision then relaxes with omega =
+     * 1 / (3 (1 + (LAMBDA1 - 1) vf) Df + 1/2) (lbm.cu:1131).  0 = not tracked (vf = 0). */
+    double lambda1;      /* LAMBDA1: viscosity ratio of the cells' interior */
+    int    vof_k;        /* K */
+    double vof_residual; /* RESIDUAL of the front-tracking solve */
+    int    vof_itrmax;   /* ITRMAX of that solve */
 } rbc_params;
 
 typedef struct rbc_mesh {
@@ -197,6 +206,12 @@ int rbc_export_ref_wbc(rbc_handle *h, double *x, double *y, double *z, double *x
                        double *gx);
 int rbc_wbc_metrics(rbc_handle *h, double *volume, double *area, double *centroid);
 
+/* ltc->vf and ltc->vf2 (red and white cells) [nx*ny*nz] in the reference
+ * layout: BUFF nodes hold their periodic images, WALL nodes 0; import reads
+ * COMP nodes.  Either pointer may be NULL.  RBC_ERR_STATE without vof_k > 0. */
+int rbc_export_ref_vof(rbc_handle *h, double *vf, double *vf2);
+int rbc_import_ref_vof(rbc_handle *h, const double *vf, const double *vf2);
+
 /* prc->iter as the stage entry points see it (rbc_step increments it first,
  * as main.cu:75 does) */
 int rbc_set_iter(rbc_handle *h, int iter);
@@ -212,6 +227,14 @@ int rbc_ibm_st2(rbc_handle *h);
 /* *iters (may be NULL) receives the reference's return value, iterations - 1.
  * Synchronous when iters != NULL. */
 int rbc_volume_correction(rbc_handle *h, int *iters);
+/* thinc_wlic (thincwlic.cu:316): THINC/WLIC advection of the volume fraction
+ * with the last lbm step's velocity; nothing without vof_k > 0. */
+int rbc_thinc_wlic(rbc_handle *h);
+/* front_tracking (fronttrack.cu:628): the volume fraction of the current cells
+ * by the Poisson solve of the indicator; *iters (may be NULL) receives the red
+ * cells' solver sweeps (-1 = not converged, RBC_FLAG_VOF_NOT_CONVERGED).
+ * Synchronous when iters != NULL.  rbc_step runs it every vof_k steps. */
+int rbc_front_tracking(rbc_handle *h, int *iters);
 /* nsteps full steps, each a replay of a CUDA graph of one step.  Asynchronous
  * (rbc_synchronize or any export waits for it). */
 int rbc_step(rbc_handle *h, int nsteps);
@@ -232,9 +255,10 @@ int rbc_get_stream(const rbc_handle *h, void **stream);
 /* Runs nsteps full steps with direct launches (no graph) and a CUDA event
  * around every kernel; kernel_ms[RBC_NUM_KERNELS] receives the summed device
  * time per kernel in the order of RBC_KERNEL_NAMES (with BR != 0 the bending
- * kernel is timed in the "membrane" slot).  Synchronous. */
-#define RBC_NUM_KERNELS 6
-#define RBC_KERNEL_NAMES {"step_begin", "membrane", "spread", "lbm_collide_stream", "advect", "volume"}
+ * kernel is timed in the "membrane" slot; "vof" holds the THINC/WLIC sweeps and
+ * the front tracking of the steps it runs in).  Synchronous. */
+#define RBC_NUM_KERNELS 7
+#define RBC_KERNEL_NAMES {"step_begin", "membrane", "spread", "lbm_collide_stream", "advect", "vof", "volume"}
 int rbc_profile_steps(rbc_handle *h, int nsteps, double *kernel_ms);
 
 /* ---- batches of independent simulations ----------------------------------- */

@@ -18,9 +18,10 @@ RBC_STORE_F32, RBC_STORE_F16 = 0, 1
 RBC_FLOW_CHANNEL, RBC_FLOW_SHEAR = 0, 1
 RBC_WALLS_BOTH, RBC_WALLS_TOP = 0, 1
 RBC_NOALLOC_MAX_CELLS = 4096
-RBC_NUM_KERNELS = 6
-RBC_KERNEL_NAMES = ("step_begin", "membrane", "spread", "lbm_collide_stream", "advect", "volume")
+RBC_NUM_KERNELS = 7
+RBC_KERNEL_NAMES = ("step_begin", "membrane", "spread", "lbm_collide_stream", "advect", "vof", "volume")
 RBC_FLAG_VC_NOT_CONVERGED, RBC_FLAG_NONFINITE, RBC_FLAG_SPREAD_OVERFLOW, RBC_FLAG_SOLVE_RESIDUAL = 1, 2, 4, 8
+RBC_FLAG_VOF_NOT_CONVERGED = 16
 
 
 class RbcParams(C.Structure):
@@ -32,7 +33,8 @@ class RbcParams(C.Structure):
                 ("law", C.c_int), ("br", C.c_double), ("M", C.c_int), ("rk_order", C.c_int),
                 ("storage", C.c_int), ("membrane_fp64", C.c_int), ("solver_iters", C.c_int),
                 ("device", C.c_int), ("flow", C.c_int), ("sr", C.c_double), ("walls", C.c_int),
-                ("tube_r", C.c_double), ("bend_spont", C.c_int)]
+                ("tube_r", C.c_double), ("bend_spont", C.c_int), ("lambda1", C.c_double), ("vof_k", C.c_int),
+                ("vof_residual", C.c_double), ("vof_itrmax", C.c_int)]
 
 
 class RbcMesh(C.Structure):
@@ -91,6 +93,10 @@ _SIGS = {
     "rbc_write_prof_file": [_H, C.c_char_p],
     "rbc_write_center_file": [_H, C.c_char_p],
     "rbc_read_center_file": [_H, C.c_char_p],
+    "rbc_thinc_wlic": [_H],
+    "rbc_front_tracking": [_H, _IP],
+    "rbc_export_ref_vof": [_H, _DP, _DP],
+    "rbc_import_ref_vof": [_H, _DP, _DP],
     "rbc_add_wbc": [_H, C.POINTER(RbcMesh), C.c_double, C.c_double],
     "rbc_wbc_dims": [_H, _IP, _IP, _IP],
     "rbc_import_ref_wbc": [_H, _DP, _DP, _DP, _DP, _DP, _DP, _DP],

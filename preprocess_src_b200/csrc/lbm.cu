@@ -118,13 +118,16 @@ __device__ __forceinline__ void collide_store(float (&g)[Q], bool fluid, I idx, 
 #ifndef LBM_MIN_BLOCKS
 #define LBM_MIN_BLOCKS 4   // resident CTAs per SM the register allocation must allow
 #endif
-template <int STORE, typename I>
+// VISC: omega of each node from the volume fraction, 1 / (df3 (1 + lm1 vf) + 1/2)
+// (lbm.cu:1131 with LAMBDA1 != 1); the omega argument otherwise.
+template <int STORE, typename I, bool VISC>
 __global__ void __launch_bounds__(LBM_THREADS, LBM_MIN_BLOCKS)
 lbm_collide_stream(const typename Store<STORE>::T *__restrict__ gin, typename Store<STORE>::T *__restrict__ gout,
                    float4 *__restrict__ uvr,
                    float *__restrict__ Fx, float *__restrict__ Fy, float *__restrict__ Fz,
                    const uint32_t *__restrict__ mask2d, const float *__restrict__ drive,
-                   const float *__restrict__ wall, int nx, int ny, int nzc, I nint,
+                   const float *__restrict__ wall, const double *__restrict__ vf, float lm1, float df3,
+                   int nx, int ny, int nzc, I nint,
                    float omega, float Cr, float Bc, float scale, float inv_scale)
 {
     using S = Store<STORE>;
@@ -136,13 +139,18 @@ lbm_collide_stream(const typename Store<STORE>::T *__restrict__ gin, typename St
     const unsigned act = __activemask();
     if (!__any_sync(act, fluid)) return;   // a warp of wall nodes stores nothing
     const bool warp_links = __any_sync(act, (m & ~MASK_FLUID) != 0u);
-    const float pd = __ldg(drive), om1 = 1.0f - omega;
+    const float pd = __ldg(drive);
+    float om1 = 1.0f - omega;
     for (int z = blockIdx.y; z < nzc; z += gridDim.y) {
         // offsets of the source planes z - 1 and z + 1 from plane z (periodic);
         // with them every pull offset from the node is uniform over the block
         const I dzm = (z == 0) ? (I)(nzc - 1) * plane : -(I)plane;
         const I dzp = (z == nzc - 1) ? -(I)(nzc - 1) * plane : (I)plane;
         const I idx = (I)z * plane + xy;
+        if (VISC) {
+            omega = 1.0f / (df3 * (1.0f + lm1 * (float)__ldg(&vf[idx])) + 0.5f);
+            om1 = 1.0f - omega;
+        }
         const typename S::T *gb = gin + idx;
         float g[Q];
         if (!warp_links) {
@@ -181,15 +189,17 @@ void launch_lbm(const Geom &g, int storage, const LbmArgs &a, cudaStream_t s)
 {
     const dim3 blocks((unsigned)((g.plane + LBM_THREADS - 1) / LBM_THREADS), (unsigned)(g.nzc < 65535 ? g.nzc : 65535));
     const bool off32 = (long long)Q * g.nint < (1LL << 31);   // every element offset fits in an int
-#define LBM_LAUNCH(ST, I)                                                                                     \
-    lbm_collide_stream<ST, I><<<blocks, LBM_THREADS, 0, s>>>(                                                 \
-        (const Store<ST>::T *)a.gin, (Store<ST>::T *)a.gout, a.uvr, a.Fx, a.Fy, a.Fz, a.mask2d, a.drive, a.wall, g.nx, \
-        g.ny, g.nzc, (I)g.nint, a.omega, a.Cr, a.Bc, a.scale, a.inv_scale)
+#define LBM_LAUNCH(ST, I, V)                                                                                  \
+    lbm_collide_stream<ST, I, V><<<blocks, LBM_THREADS, 0, s>>>(                                              \
+        (const Store<ST>::T *)a.gin, (Store<ST>::T *)a.gout, a.uvr, a.Fx, a.Fy, a.Fz, a.mask2d, a.drive, a.wall, a.vf, \
+        a.lm1, a.df3, g.nx, g.ny, g.nzc, (I)g.nint, a.omega, a.Cr, a.Bc, a.scale, a.inv_scale)
+#define LBM_LAUNCH_V(ST, I) do { if (a.vf) LBM_LAUNCH(ST, I, true); else LBM_LAUNCH(ST, I, false); } while (0)
     if (storage == RBC_STORE_F16) {
-        if (off32) LBM_LAUNCH(RBC_STORE_F16, int); else LBM_LAUNCH(RBC_STORE_F16, long long);
+        if (off32) LBM_LAUNCH_V(RBC_STORE_F16, int); else LBM_LAUNCH_V(RBC_STORE_F16, long long);
     } else {
-        if (off32) LBM_LAUNCH(RBC_STORE_F32, int); else LBM_LAUNCH(RBC_STORE_F32, long long);
+        if (off32) LBM_LAUNCH_V(RBC_STORE_F32, int); else LBM_LAUNCH_V(RBC_STORE_F32, long long);
     }
+#undef LBM_LAUNCH_V
 #undef LBM_LAUNCH
 }
 

@@ -58,6 +58,7 @@ struct CellGroup {
     int npatch = 1;
     int mn = 0;                                       // the reference's per-cell vector length (expand2pow2(3 V))
     double *qi_acc = nullptr, *tp_acc = nullptr;      // output-interval averages [ncell][mn], [ne][2]
+    double *vf = nullptr;                             // volume fraction [nint] (ltc->vf, vf2), VOF only
 };
 
 struct rbc_handle {
@@ -85,8 +86,11 @@ struct rbc_handle {
     float *Fx = nullptr, *Fy = nullptr, *Fz = nullptr;
     uint32_t *mask2d = nullptr;
     int *tube_links = nullptr; float *tube_frac = nullptr; int ntube = 0;   // interpolated wall links (circular tube)
-    // device scalars: iter, flags, vc_max, vc_last
+    // device scalars: iter, flags, vc_max, vc_last, front-tracking sweeps of populations 0 and 1
     int *d_int = nullptr;
+    // volume fraction scratch (vof_k > 0): THINC sweep buffers, indicator gradient / CG vectors,
+    // right-hand side, CG block partials
+    double *vof_s1 = nullptr, *vof_s2 = nullptr, *vof_G = nullptr, *vof_b = nullptr, *vof_partial = nullptr;
     float *d_drive = nullptr;                          // [3]: drive P * factor, then the walls' z velocities
     // host<->reference staging
     void *staging = nullptr;
@@ -114,6 +118,7 @@ struct rbc_handle {
             const CellGroup &c = cg[g];
             if (c.ncell == 0) continue;
             k += 4 + (c.br != 0.0 ? 1 : 0) + (fileoutput > 0 ? 2 : 0);   // membrane, spread, advect, volume
+            if (c.vf) k += 3;                                            // THINC/WLIC sweeps
         }
         return k;
     }
@@ -125,6 +130,8 @@ struct rbc_handle {
     int *d_flags() { return d_int + 1; }
     int *d_vcmax() { return d_int + 2; }
     int *d_vclast() { return d_int + 3; }
+    int *d_vofit() { return d_int + 4; }
+    bool vof() const { return p.vof_k > 0; }
 };
 
 #define CK(call)                                                                       \
@@ -434,6 +441,11 @@ int check_params(const rbc_params *p)
     if (p->rk_order != 4) return fail(nullptr, RBC_ERR_UNSUPPORTED, "only RUNGE_KUTTA = 4 is implemented");
     if (!std::isfinite(p->br)) return fail(nullptr, RBC_ERR_ARG, "BR must be finite");
     if (p->bend_spont != 0 && p->bend_spont != 1) return fail(nullptr, RBC_ERR_ARG, "bend_spont must be 0 or 1");
+    if (p->vof_k < 0) return fail(nullptr, RBC_ERR_ARG, "vof_k must be >= 0");
+    if (!(p->lambda1 > 0.0) || !std::isfinite(p->lambda1)) return fail(nullptr, RBC_ERR_ARG, "lambda1 must be > 0");
+    if (p->vof_k > 0 && (!(p->vof_residual > 0.0) || p->vof_itrmax < 1))
+        return fail(nullptr, RBC_ERR_ARG, "vof_residual must be > 0 and vof_itrmax >= 1");
+    if (p->vof_k > 0 && p->M != 1) return fail(nullptr, RBC_ERR_UNSUPPORTED, "VOF with M = 1 only");
     if (p->storage != RBC_STORE_F32 && p->storage != RBC_STORE_F16) return fail(nullptr, RBC_ERR_ARG, "unknown storage");
     if (p->law != RBC_LAW_SKALAK && p->law != RBC_LAW_NEOHOOKEAN) return fail(nullptr, RBC_ERR_ARG, "unknown law");
     if (p->solver_iters < 0 || p->solver_iters > 200) return fail(nullptr, RBC_ERR_ARG, "solver_iters out of range");
@@ -553,7 +565,8 @@ int build_mask(const rbc_params *p, const int *bc, std::vector<uint32_t> &mask)
 void free_group(CellGroup &c)
 {
     void *cp[] = {c.X, c.Xd, c.gref, c.erec, c.U, c.Fv, c.tri, c.v2e_off, c.v2e, c.nbr, c.visit, c.cs0, c.patch_off,
-                  c.patch_vtx, c.patch_stride, c.vol0, c.gx, c.vol_out, c.area_out, c.cen_out, c.qi_acc, c.tp_acc};
+                  c.patch_vtx, c.patch_stride, c.vol0, c.gx, c.vol_out, c.area_out, c.cen_out, c.qi_acc, c.tp_acc,
+                  c.vf};
     for (void *q : cp) if (q) cudaFree(q);
     c = CellGroup{};
 }
@@ -567,7 +580,7 @@ void free_all(rbc_handle *h)
     if (h->join) cudaEventDestroy(h->join);
     if (h->side) cudaStreamDestroy(h->side);
     void *ptrs[] = {h->g[0], h->g[1], h->uvr, h->Fx, h->Fy, h->Fz, h->mask2d, h->tube_links, h->tube_frac,
-                    h->d_int, h->d_drive, h->staging};
+                    h->d_int, h->d_drive, h->staging, h->vof_s1, h->vof_s2, h->vof_G, h->vof_b, h->vof_partial};
     for (void *q : ptrs) if (q) cudaFree(q);
     for (CellGroup &c : h->cg) free_group(c);
     adjoint_free(h->adj);
@@ -652,6 +665,10 @@ int launch_lbm_stage(rbc_handle *h)
     a.wall = h->p.flow == RBC_FLOW_SHEAR ? h->d_drive + 1 : nullptr;
     a.omega = (float)(1.0 / h->p.tau); a.Cr = (float)h->p.Cr; a.Bc = (float)h->p.B;
     a.scale = h->scale; a.inv_scale = h->inv_scale;
+    // the red cells' volume fraction sets omega (lbm.cu:1131; ltc->vf2 of the white cells does not)
+    a.vf = (h->p.lambda1 != 1.0 && h->cg[0].vf) ? h->cg[0].vf : nullptr;
+    a.lm1 = (float)(h->p.lambda1 - 1.0);
+    a.df3 = (float)(h->p.tau - 0.5);   // 3 Df, tau = 3 Df + 1/2
     launch_lbm(h->geo, h->p.storage, a, h->stream);
     h->launches++;
     CK_LAUNCH();
@@ -679,6 +696,64 @@ int launch_advect_stage(rbc_handle *h)
         h->launches++;
         CK_LAUNCH();
     }
+    return RBC_OK;
+}
+
+// thinc_wlic (thincwlic.cu:316-420) of every population's volume fraction
+int launch_thinc_stage(rbc_handle *h)
+{
+    for (int k = 0; k < h->ngroups; k++) {
+        CellGroup &g = h->cg[k];
+        if (!g.vf || g.ncell == 0) continue;
+        launch_thinc_wlic(h->geo, g.vf, h->vof_s1, h->vof_s2, h->uvr, h->mask2d, h->p.dt * h->p.M, h->stream);
+        h->launches += 3;
+        CK_LAUNCH();
+    }
+    return RBC_OK;
+}
+
+// front_tracking (fronttrack.cu:628-944) of every population into its volume fraction
+int launch_front_tracking_stage(rbc_handle *h)
+{
+    for (int k = 0; k < h->ngroups; k++) {
+        CellGroup &g = h->cg[k];
+        if (!g.vf || g.ncell == 0) continue;
+        FrontArgs a{};
+        a.X = g.X; a.nv = g.nv; a.tri = g.tri; a.V = g.V; a.E = g.E; a.ncell = g.ncell; a.mask2d = h->mask2d;
+        a.G = h->vof_G; a.b = h->vof_b; a.vf = g.vf; a.partial = h->vof_partial;
+        a.tol = h->p.vof_residual; a.itrmax = h->p.vof_itrmax; a.iters = h->d_vofit() + k; a.flags = h->d_flags();
+        CK(launch_front_tracking(h->geo, a, h->stream));
+        h->launches += 3;
+        CK_LAUNCH();
+    }
+    return RBC_OK;
+}
+
+// volume fraction storage of population g and the shared scratch, and vof_init
+// (init1.cu:1094-1120): front tracking of the initial cells (synchronous)
+int vof_init_group(rbc_handle *h, CellGroup &g)
+{
+    const size_t n = (size_t)h->geo.nint;
+    if (!h->vof_s1) {
+        CK(cudaMalloc(&h->vof_s1, 8 * n));
+        CK(cudaMalloc(&h->vof_s2, 8 * n));
+        CK(cudaMalloc(&h->vof_G, 8 * 3 * n));
+        CK(cudaMalloc(&h->vof_b, 8 * n));
+        CK(cudaMalloc(&h->vof_partial, 8 * 4 * (size_t)std::max(vof_cg_blocks(), 1)));
+    }
+    if (!g.vf) {
+        CK(cudaMalloc(&g.vf, 8 * n));
+        CK(cudaMemset(g.vf, 0, 8 * n));   // flu_init's vf = 0 (init1.cu:396-411)
+    }
+    if (g.ncell == 0) return RBC_OK;
+    FrontArgs a{};
+    a.X = g.X; a.nv = g.nv; a.tri = g.tri; a.V = g.V; a.E = g.E; a.ncell = g.ncell; a.mask2d = h->mask2d;
+    a.G = h->vof_G; a.b = h->vof_b; a.vf = g.vf; a.partial = h->vof_partial;
+    a.tol = h->p.vof_residual; a.itrmax = h->p.vof_itrmax; a.iters = h->d_vofit() + (&g == &h->cg[1] ? 1 : 0);
+    a.flags = h->d_flags();
+    CK(launch_front_tracking(h->geo, a, h->stream));
+    h->launches += 3;
+    CK(cudaStreamSynchronize(h->stream));
     return RBC_OK;
 }
 
@@ -734,6 +809,7 @@ int enqueue_step(rbc_handle *h, StepForm form = STEP_WHOLE)
     if ((rc = launch_spread_stage(h))) return rc;
     if ((rc = launch_lbm_stage(h))) return rc;
     if ((rc = launch_advect_stage(h))) return rc;
+    if ((rc = launch_thinc_stage(h))) return rc;   // main.cu:94-95
     if (form == STEP_WHOLE && (rc = launch_volume_stage(h, h->stream))) return rc;
     return RBC_OK;
 }
@@ -1047,11 +1123,11 @@ int rbc_create(const rbc_params *p, const rbc_mesh *mesh, const int *bc, rbc_han
     }
     TRY(dalloc(h, &h->uvr, g.nint)); TRY(dalloc(h, &h->Fx, g.nint)); TRY(dalloc(h, &h->Fy, g.nint));
     TRY(dalloc(h, &h->Fz, g.nint)); TRY(dalloc(h, &h->mask2d, g.plane));
-    TRY(dalloc(h, &h->d_int, 4)); TRY(dalloc(h, &h->d_drive, 3));
+    TRY(dalloc(h, &h->d_int, 6)); TRY(dalloc(h, &h->d_drive, 3));
     if (cudaMemset(h->g[0], 0, h->gbytes) != cudaSuccess || cudaMemset(h->g[1], 0, h->gbytes) != cudaSuccess ||
         cudaMemset(h->Fx, 0, 4 * g.nint) != cudaSuccess ||
         cudaMemset(h->Fy, 0, 4 * g.nint) != cudaSuccess || cudaMemset(h->Fz, 0, 4 * g.nint) != cudaSuccess ||
-        cudaMemset(h->d_int, 0, 4 * sizeof(int)) != cudaSuccess || cudaMemset(h->d_drive, 0, 3 * sizeof(float)) != cudaSuccess ||
+        cudaMemset(h->d_int, 0, 6 * sizeof(int)) != cudaSuccess || cudaMemset(h->d_drive, 0, 3 * sizeof(float)) != cudaSuccess ||
         cudaMemcpy(h->mask2d, mask.data(), 4 * g.plane, cudaMemcpyHostToDevice) != cudaSuccess) {
         h->err = "device initialisation failed";
         return bail(RBC_ERR_CUDA);
@@ -1104,6 +1180,7 @@ int rbc_create(const rbc_params *p, const rbc_mesh *mesh, const int *bc, rbc_han
     }
 
     if (cells) TRY(upload_group(h, h->cg[0], mesh, prep));
+    if (p->vof_k > 0) TRY(vof_init_group(h, h->cg[0]));
     if (cudaStreamSynchronize(h->stream) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
         h->err = "initialisation kernels failed";
         return bail(RBC_ERR_CUDA);
@@ -1336,6 +1413,85 @@ int rbc_ibm_st2(rbc_handle *h)
     return launch_advect_stage(h);
 }
 
+int rbc_thinc_wlic(rbc_handle *h)
+{
+    if (!h) return RBC_ERR_ARG;
+    RBC_DEVICE_GUARD(h);
+    return launch_thinc_stage(h);
+}
+
+int rbc_front_tracking(rbc_handle *h, int *iters)
+{
+    if (!h) return RBC_ERR_ARG;
+    RBC_DEVICE_GUARD(h);
+    int rc = launch_front_tracking_stage(h);
+    if (rc || !iters) return rc;
+    int v[2] = {0, 0};
+    CK(cudaMemcpyAsync(v, h->d_vofit(), sizeof(v), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    iters[0] = v[0];
+    return RBC_OK;
+}
+
+// ltc->vf / vf2 [nx*ny*nz] in the reference layout <-> the populations' internal fields
+static int vof_transfer(rbc_handle *h, double *out0, double *out1, const double *in0, const double *in1)
+{
+    RBC_DEVICE_GUARD(h);
+    if (!h->vof()) return fail(h, RBC_ERR_STATE, "the volume fraction is not tracked (vof_k = 0)");
+    const Geom &g = h->geo;
+    std::vector<uint32_t> mask((size_t)g.plane);
+    CK(cudaStreamSynchronize(h->stream));
+    CK(cudaMemcpy(mask.data(), h->mask2d, 4 * mask.size(), cudaMemcpyDeviceToHost));
+    std::vector<double> in((size_t)g.nint);
+    const long long nref = (long long)g.nxr * g.ny * g.nzr;
+    for (int k = 0; k < 2; k++) {
+        double *out = k ? out1 : out0;
+        const double *src = k ? in1 : in0;
+        CellGroup &cgp = h->cg[k];
+        if (!out && !src) continue;
+        if (k >= h->ngroups || !cgp.vf) {   // no such population: its field is 0
+            if (out) std::fill(out, out + nref, 0.0);
+            continue;
+        }
+        if (out) {
+            CK(cudaMemcpy(in.data(), cgp.vf, 8 * in.size(), cudaMemcpyDeviceToHost));
+            for (int iz = 0; iz < g.nzr; iz++)
+                for (int iy = 0; iy < g.ny; iy++)
+                    for (int ix = 0; ix < g.nxr; ix++) {
+                        int xi = ix - g.xb;
+                        const bool in_x = xi >= 0 && xi < g.nx;
+                        if (g.xper) xi = ((xi % g.nx) + g.nx) % g.nx;
+                        const long long r = ((long long)iz * g.ny + iy) * g.nxr + ix;
+                        if ((!in_x && !g.xper) || !(mask[(size_t)iy * g.nx + xi] & MASK_FLUID)) { out[r] = 0.0; continue; }
+                        const int zc = (((iz - 2) % g.nzc) + g.nzc) % g.nzc;
+                        out[r] = in[(size_t)zc * g.plane + (size_t)iy * g.nx + xi];
+                    }
+        } else {
+            for (int zc = 0; zc < g.nzc; zc++)
+                for (int iy = 0; iy < g.ny; iy++)
+                    for (int xi = 0; xi < g.nx; xi++) {
+                        const bool fl = (mask[(size_t)iy * g.nx + xi] & MASK_FLUID) != 0;
+                        const long long r = ((long long)(zc + 2) * g.ny + iy) * g.nxr + xi + g.xb;
+                        in[(size_t)zc * g.plane + (size_t)iy * g.nx + xi] = fl ? src[r] : 0.0;
+                    }
+            CK(cudaMemcpy(cgp.vf, in.data(), 8 * in.size(), cudaMemcpyHostToDevice));
+        }
+    }
+    return RBC_OK;
+}
+
+int rbc_export_ref_vof(rbc_handle *h, double *vf, double *vf2)
+{
+    if (!h) return RBC_ERR_ARG;
+    return vof_transfer(h, vf, vf2, nullptr, nullptr);
+}
+
+int rbc_import_ref_vof(rbc_handle *h, const double *vf, const double *vf2)
+{
+    if (!h) return RBC_ERR_ARG;
+    return vof_transfer(h, nullptr, nullptr, vf, vf2);
+}
+
 int rbc_volume_correction(rbc_handle *h, int *iters)
 {
     if (!h) return RBC_ERR_ARG;
@@ -1363,7 +1519,10 @@ int rbc_step(rbc_handle *h, int nsteps)
     // one step, or no cells: whole steps.  Otherwise step 1 without its
     // correction, steps 2..n pipelined with the correction of the step before,
     // then the correction of step n: the same kernels in the same data order.
-    const bool pipe = nsteps > 1 && h->has_cells();
+    // with the volume fraction, front tracking (main.cu:97-98) runs between the
+    // step's graph and its volume correction, which the pipelined forms leave
+    // to the next graph
+    const bool pipe = (nsteps > 1 || h->vof()) && h->has_cells();
     for (int c = 0; c < 2; c++) {
         if (!h->graph[STEP_WHOLE][c] && (rc = build_graph(h, c, STEP_WHOLE))) return rc;
         if (pipe && !h->graph[STEP_BODY][c] && (rc = build_graph(h, c, STEP_BODY))) return rc;
@@ -1374,6 +1533,7 @@ int rbc_step(rbc_handle *h, int nsteps)
         CK(cudaGraphLaunch(h->graph[form][h->cur], h->stream));
         h->cur ^= 1;
         h->launches += h->kernels_per_step();
+        if (h->vof() && (h->iter + k + 1) % h->p.vof_k == 0 && (rc = launch_front_tracking_stage(h))) return rc;
     }
     if (pipe) {
         for (int k = 0; k < h->ngroups; k++)   // step n's corrections, counted with its step, are launched here
@@ -1407,9 +1567,12 @@ int rbc_profile_steps(rbc_handle *h, int nsteps, double *kernel_ms)
         cudaEventRecord(ev[4], h->stream);
         if (!rc) rc = launch_advect_stage(h);
         cudaEventRecord(ev[5], h->stream);
-        if (!rc) rc = launch_volume_stage(h, h->stream);
+        if (!rc) rc = launch_thinc_stage(h);
+        if (!rc && h->vof() && (h->iter + s + 1) % h->p.vof_k == 0) rc = launch_front_tracking_stage(h);
         cudaEventRecord(ev[6], h->stream);
-        if (cudaEventSynchronize(ev[6]) != cudaSuccess) { rc = RBC_ERR_CUDA; h->err = "profiled step failed"; break; }
+        if (!rc) rc = launch_volume_stage(h, h->stream);
+        cudaEventRecord(ev[7], h->stream);
+        if (cudaEventSynchronize(ev[7]) != cudaSuccess) { rc = RBC_ERR_CUDA; h->err = "profiled step failed"; break; }
         for (int k = 0; k < RBC_NUM_KERNELS; k++) {
             float ms = 0.f;
             cudaEventElapsedTime(&ms, ev[k], ev[k + 1]);
@@ -1490,6 +1653,8 @@ int rbc_batch_create(rbc_handle *const *handles, int n, rbc_batch **out)
             return fail(nullptr, RBC_ERR_ARG, "all simulations of a batch must use the same device");
         for (int j = 0; j < i; j++)
             if (handles[j] == handles[i]) return fail(nullptr, RBC_ERR_ARG, "a simulation appears twice in the batch");
+        if (handles[i]->vof())
+            return fail(nullptr, RBC_ERR_UNSUPPORTED, "batched simulations do not track the volume fraction (needs vof_k = 0)");
     }
     rbc_batch *b = new (std::nothrow) rbc_batch();
     if (!b) return fail(nullptr, RBC_ERR_ARG, "out of host memory");
@@ -1921,6 +2086,7 @@ int adjoint_supported(rbc_handle *h)
     if (h->geo.nzc > 65535) return fail(h, RBC_ERR_UNSUPPORTED, "the adjoint handles at most 65535 periodic planes");
     if (h->p.flow != RBC_FLOW_CHANNEL) return fail(h, RBC_ERR_UNSUPPORTED, "the adjoint covers the channel mode only");
     if (h->ntube > 0) return fail(h, RBC_ERR_UNSUPPORTED, "the adjoint covers half-way bounce-back walls only (tube_r = 0)");
+    if (h->vof()) return fail(h, RBC_ERR_UNSUPPORTED, "the adjoint does not cover the volume fraction (needs vof_k = 0)");
     return RBC_OK;
 }
 
@@ -2193,6 +2359,7 @@ int rbc_add_wbc(rbc_handle *h, const rbc_mesh *mesh, double rgs, double br)
         return rc;
     }
     h->ngroups = 2;
+    if (h->vof() && (rc = vof_init_group(h, c))) return rc;
     if (h->fileoutput > 0) {
         const int f = h->fileoutput;
         h->fileoutput = 0;

@@ -98,6 +98,8 @@ struct LbmArgs {
     const uint32_t *mask2d;
     const float *drive;        // device scalar: P * drive factor of this step
     const float *wall;         // device [2]: z velocity of the top and bottom walls (shear mode), else NULL
+    const double *vf;          // volume fraction: omega = 1 / (df3 (1 + lm1 vf) + 1/2) per node; NULL: omega
+    float lm1, df3;            // LAMBDA1 - 1 and 3 Df (lbm.cu:1131)
     float omega, Cr, Bc;
     float scale, inv_scale;    // FP16 storage scale
 };
@@ -118,6 +120,25 @@ void launch_export_force(const Geom &g, const float *Fx, const float *Fy, const 
                          const uint32_t *mask2d, double *out3, cudaStream_t s);
 void launch_fill_f32(float *p, long long n, float v, cudaStream_t s);
 void launch_fill_f4(float4 *p, long long n, float4 v, cudaStream_t s);
+
+// Volume fraction (vof.cu).  THINC/WLIC: three sweeps vf -> s1 -> s2 -> vf.
+void launch_thinc_wlic(const Geom &g, double *vf, double *s1, double *s2, const float4 *uvr, const uint32_t *mask2d,
+                       double dt, cudaStream_t s);
+// Front tracking of one cell population into vf (warm start from vf).
+struct FrontArgs {
+    const double *X; long long nv;
+    const int *tri; int V, E, ncell;
+    const uint32_t *mask2d;
+    double *G;                 // [3][nint] scratch: the indicator gradient, then the CG vectors
+    double *b;                 // [nint] scratch: right-hand side
+    double *vf;                // [nint] solution
+    double *partial;           // [4 * vof_cg_blocks()] scratch
+    double tol; int itrmax;
+    int *iters;                // device: sweeps of the solve, -1 = not converged
+    int *flags;
+};
+cudaError_t launch_front_tracking(const Geom &g, const FrontArgs &a, cudaStream_t s);
+int vof_cg_blocks();
 
 // Surface patches (spread and advection work units) hold at most this many vertices.
 constexpr int MAX_PATCH_VERTICES = 512;

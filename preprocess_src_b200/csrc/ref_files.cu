@@ -14,9 +14,9 @@
 //   center.dat   (OutputCapsuleCenter / InputCapsuleCenter, etc.cu:110-160)
 //     one line per cell, red cells then white cells, each numbered from 0:
 //     "%d %e %e %e \n" (cell, cel->gx[3c + 0..2] or cel->gx_w)
-// n = nx * ny * nz counts the BUFF planes.  vf and vf2 (the VOF indicator,
-// used only with a viscosity contrast) stay at flu_init's 0, and rx, ry, rz are
-// never set by the reference; both are written as 0 and ignored when read.
+// n = nx * ny * nz counts the BUFF planes.  vf and vf2 are the red and white
+// cells' volume fractions when they are tracked (vof_k > 0), else flu_init's 0;
+// rx, ry, rz are never set by the reference: written as 0, ignored when read.
 // qi and tp are the output-interval averages of the load and the principal
 // tensions (rbc_set_output_interval; 0 when no interval is set).  The
 // populations of non-COMP nodes are never read by the reference's step: they
@@ -108,6 +108,15 @@ int io_error(rbc_handle *h, const char *what, const char *path)
 }
 
 // the lattice in the reference's layout with non-COMP populations as the reference holds them
+// ltc->vf, vf2 [2][n]: the tracked volume fractions, or 0
+int vof_of(rbc_handle *h, const Dims &d, std::vector<double> &vf)
+{
+    vf.assign((size_t)d.n * 2, 0.0);
+    if (rbc_export_ref_vof(h, vf.data(), vf.data() + d.n) == RBC_OK) return RBC_OK;
+    set_handle_error(h, "");   // not tracked: zeros
+    return RBC_OK;
+}
+
 int lattice_of(rbc_handle *h, const Dims &d, std::vector<double> &fn, std::vector<double> &mac, std::vector<int> &bc)
 {
     fn.resize((size_t)d.n * Q);
@@ -137,6 +146,8 @@ int rbc_write_restart(rbc_handle *h, const char *path, int fnum)
     std::vector<double> fn, mac;
     std::vector<int> bc;
     if ((rc = lattice_of(h, d, fn, mac, bc))) return rc;
+    std::vector<double> vf;
+    if ((rc = vof_of(h, d, vf))) return rc;
     std::vector<double> zeros((size_t)std::max<long long>({d.n, d.pop[0].N, d.pop[1].N}), 0.0);
     PopState st[2];
     for (int k = 0; k < 2; k++)
@@ -147,7 +158,7 @@ int rbc_write_restart(rbc_handle *h, const char *path, int fnum)
     if (!f.f) return io_error(h, "cannot open for writing", path);
     bool ok = put(f.f, &iter, 1) && put(f.f, &fnum, 1) && put(f.f, fn.data(), fn.size())
            && put(f.f, mac.data(), mac.size())          // dm, um, vm, wm
-           && put(f.f, zeros.data(), d.n) && put(f.f, zeros.data(), d.n);   // vf, vf2
+           && put(f.f, vf.data(), 2 * d.n);             // vf, vf2
     for (int k = 0; k < 2 && ok; k++) {
         const Pop &p = d.pop[k];
         if (p.N == 0) continue;
@@ -171,7 +182,7 @@ int rbc_read_restart(rbc_handle *h, const char *path, int *fnum)
     int iter = 0, fn_ = 0;
     std::vector<double> fn((size_t)d.n * Q), skip((size_t)d.n * 6);
     bool ok = get(f.f, &iter, 1) && get(f.f, &fn_, 1) && get(f.f, fn.data(), fn.size())
-           && get(f.f, skip.data(), skip.size());     // dm, um, vm, wm, vf, vf2: recomputed by the step / unused
+           && get(f.f, skip.data(), skip.size());     // dm, um, vm, wm (recomputed by the step), vf, vf2
     PopState st[2];
     for (int k = 0; k < 2 && ok; k++) {
         const Pop &p = d.pop[k];
@@ -188,6 +199,8 @@ int rbc_read_restart(rbc_handle *h, const char *path, int *fnum)
     if (std::fgetc(f.f) != EOF) return io_error(h, "restart file longer than this lattice and these cells", path);
     if (fn_ > 100) { iter = 0; fn_ = 0; }   // etc.cu:205
     if ((rc = rbc_import_ref_lattice(h, fn.data()))) return rc;
+    // the volume fractions when tracked (etc.cu:213-214, 281-282); else unused
+    if (rbc_import_ref_vof(h, skip.data() + 4 * d.n, skip.data() + 5 * d.n) != RBC_OK) set_handle_error(h, "");
     for (int k = 0; k < 2; k++) {
         const Pop &p = d.pop[k];
         if (p.N == 0) continue;
@@ -242,13 +255,14 @@ int rbc_write_prof_file(rbc_handle *h, const char *path)
     std::vector<double> fn, mac;
     std::vector<int> bc;
     if ((rc = lattice_of(h, d, fn, mac, bc))) return rc;
-    std::vector<double> zeros((size_t)d.n, 0.0);
+    std::vector<double> vf;
+    if ((rc = vof_of(h, d, vf))) return rc;
     int iter = 0;
     rbc_get_iter(h, &iter);
     File f(path, "wb");
     if (!f.f) return io_error(h, "cannot open for writing", path);
-    const bool ok = put(f.f, &iter, 1) && put(f.f, mac.data(), mac.size()) && put(f.f, zeros.data(), d.n)
-                 && put(f.f, zeros.data(), d.n) && put(f.f, bc.data(), bc.size());
+    const bool ok = put(f.f, &iter, 1) && put(f.f, mac.data(), mac.size()) && put(f.f, vf.data(), 2 * d.n)
+                 && put(f.f, bc.data(), bc.size());
     return ok ? RBC_OK : io_error(h, "write failed", path);
 }
 

@@ -157,6 +157,7 @@ cudaError_t membrane_setup(int optin, int *max_bytes);
 cudaError_t spread_setup();
 cudaError_t advect_setup();
 cudaError_t adjoint_setup(int optin);
+cudaError_t vof_setup();
 
 // Dynamic shared memory limit of a kernel: the device's per-block opt-in
 // maximum minus the kernel's static shared memory.
@@ -182,6 +183,7 @@ int setup_kernel_attributes(int *membrane_max_smem)
     if ((e = spread_setup()) != cudaSuccess) return (int)e;
     if ((e = advect_setup()) != cudaSuccess) return (int)e;
     if ((e = adjoint_setup(optin)) != cudaSuccess) return (int)e;
+    if ((e = vof_setup()) != cudaSuccess) return (int)e;
     return 0;
 }
 

@@ -8,6 +8,8 @@ reference entry points they replace and run in the same order inside
     ibm_st1()           ibm.cu:299          spread forces to the lattice
     lbm_d3q19()         lbm.cu:1463         collide + stream
     ibm_st2()           ibm.cu:642          interpolate + RK4 advect
+    thinc_wlic()        thincwlic.cu:316    advect the volume fraction (vof_k > 0)
+    front_tracking()    fronttrack.cu:628   volume fraction from the cells (every vof_k steps)
     volume_correction() volume_correction.cu:453
 
 State moves in and out in the reference's layouts (``import_*``/``export_*``).
@@ -96,6 +98,15 @@ class Simulation:
         self._call("rbc_volume_correction", C.byref(it))
         return it.value
 
+    def thinc_wlic(self):
+        self._call("rbc_thinc_wlic")
+
+    def front_tracking(self) -> int:
+        """Solver sweeps of the red cells' solve (-1: not converged)."""
+        it = C.c_int(0)
+        self._call("rbc_front_tracking", C.byref(it))
+        return it.value
+
     def step(self, nsteps: int = 1):
         self._call("rbc_step", int(nsteps))
 
@@ -123,6 +134,16 @@ class Simulation:
         self._call("rbc_export_ref_lattice", _dp(out.get("fn")), _dp(out.get("dn")), _dp(out.get("un")),
                    _dp(out.get("vn")), _dp(out.get("wn")))
         return out
+
+    def export_vof(self) -> tuple[np.ndarray, np.ndarray]:
+        """ltc->vf, ltc->vf2 in the reference layout."""
+        vf, vf2 = np.empty(self.n), np.empty(self.n)
+        self._call("rbc_export_ref_vof", _dp(vf), _dp(vf2))
+        return vf, vf2
+
+    def import_vof(self, vf=None, vf2=None):
+        args = [None if a is None else _f64(a, self.n) for a in (vf, vf2)]
+        self._call("rbc_import_ref_vof", *map(_dp, args))
 
     def export_force(self) -> dict:
         out = {k: np.empty(self.n) for k in ("fx", "fy", "fz")}

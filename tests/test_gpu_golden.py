@@ -30,12 +30,18 @@ def test_gpu_matches_reference_kernels(name, case, native_lib):
     g = np.load(GOLDEN / f"{name}.npz")
     sim = Simulation(case)
     m = case.bc == configs.COMP
+    if case.params["vof_k"] > 0:
+        assert np.abs(sim.export_vof()[0][m] - g["setup_vf"]).max() <= 1e-8
     done = 0
     for s in snapshots(case):
         sim.step(s - done)
         done = s
         lat = sim.export_lattice(fn=False)
         cel = sim.export_cells()
+        if case.params["vof_k"] > 0:   # the reference's volume fraction (fronttrack.cu, thincwlic.cu)
+            verr = np.abs(sim.export_vof()[0][m] - g[f"s{s}_vf"]).max()
+            print(f"{name} step {s}: vf max|d| {verr:.2e}")
+            assert verr <= 2e-6
         u = np.concatenate([lat["un"][m], lat["vn"][m], lat["wn"][m]])
         uref = np.concatenate([g[f"s{s}_un"], g[f"s{s}_vn"], g[f"s{s}_wn"]])
         x = np.concatenate([cel[k] for k in ("x", "y", "z")])

@@ -1,0 +1,152 @@
+"""The volume fraction of the cells (VOF: front tracking, fronttrack.cu, and
+THINC/WLIC, thincwlic.cu) with a viscosity ratio (lbm.cu:1131) on the GPU
+against the FP64 oracle, whose restatement is pinned to the reference's own
+kernels (tests/test_golden.py, case g4).
+
+The front-tracking solve converges to the same field on both sides (CG here,
+red-black SOR in the oracle, both to |r|/|b| < 1e-12).  THINC/WLIC rounds
+through the reference's float expf / coshf, whose last bit differs between
+CUDA and glibc (~1e-7 per node and step in vf); the GPU's FP32 velocity adds
+~1e-8.
+"""
+import numpy as np
+import pytest
+
+from preprocess_src_b200 import configs
+from tests.test_gpu_parity import comp, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+def vof_case(**kw):
+    kw.setdefault("lambda1", 5.0)
+    kw.setdefault("vof_k", 10)
+    kw.setdefault("vof_residual", 1e-12)
+    return configs.duct_case("vof_32x20x20_2c", 32, 20, 20, centers_duct=[(1.5, 9.6, 9.4), (17.0, 9.3, 9.7)],
+                             subdiv=3, radius=5.0, seed=31, g=4e-5, Gs=2e-3, **kw)
+
+
+def _u(lat, m):
+    return np.concatenate([lat["un"][m], lat["vn"][m], lat["wn"][m]])
+
+
+def test_front_tracking_at_create_matches_oracle(oracle_mod, native_lib):
+    from preprocess_src_b200.step import Simulation
+    case = vof_case()
+    o = oracle_mod.Oracle(case)
+    m = comp(case)
+    with Simulation(case) as sim:
+        vf, vf2 = sim.export_vof()
+        err = np.abs(vf - o["vf"]).max()
+        print(f"setup vf max|d| {err:.2e}, oracle SOR sweeps {o.s.vof_iters}, sum {vf[m].sum():.6f}")
+        assert err <= 1e-8
+        assert not vf2.any()
+        assert not vf[case.bc == configs.WALL].any()
+        # a second solve from the converged field takes no sweep
+        assert sim.front_tracking() == 0
+        assert np.abs(sim.export_vof()[0] - vf).max() == 0.0
+
+
+def test_vof_steps_match_oracle(oracle_mod, native_lib):
+    """25 full steps with LAMBDA1 = 5: THINC/WLIC every step, front tracking at
+    steps 10 and 20, omega from vf in the collision."""
+    from preprocess_src_b200.step import Simulation
+    case = vof_case()
+    o = oracle_mod.Oracle(case)
+    m = comp(case)
+    with Simulation(case) as sim:
+        for nsteps in (1, 4, 5, 10, 5):
+            o.step(nsteps)
+            sim.step(nsteps)
+            vf = sim.export_vof()[0]
+            lat = sim.export_lattice(fn=False)
+            c = sim.export_cells()
+            ref = np.concatenate([o["x"], o["y"], o["z"]])
+            perr = np.abs(np.concatenate([c["x"], c["y"], c["z"]]) - ref).max()
+            uerr = rel_l2(_u(lat, m), _u(o.a, m))
+            verr = np.abs(vf - o["vf"]).max()
+            print(f"iter {o.iter}: vf max|d| {verr:.2e}  u rel L2 {uerr:.2e}  max|dx| {perr:.2e}")
+            assert verr <= 2e-6 and uerr <= 1e-5 * o.iter and perr <= 1e-5 * np.abs(ref).max()
+        flags, _ = sim.status()
+        assert flags & (1 | 2 | 16) == 0, flags
+
+
+def test_viscosity_ratio_changes_the_flow(native_lib):
+    """The same run with LAMBDA1 = 1 and 5 differs, and LAMBDA1 = 1 with the
+    volume fraction tracked is the run without it."""
+    from preprocess_src_b200.step import Simulation
+    out = {}
+    for lam, k in ((1.0, 0), (1.0, 10), (5.0, 10)):
+        with Simulation(vof_case(lambda1=lam, vof_k=k)) as sim:
+            sim.step(12)
+            out[(lam, k)] = sim.export_lattice(fn=False)["wn"]
+    assert np.abs(out[(1.0, 10)] - out[(1.0, 0)]).max() == 0.0
+    assert np.abs(out[(5.0, 10)] - out[(1.0, 0)]).max() > 1e-7
+
+
+def test_thinc_conserves_and_front_tracking_restores(native_lib):
+    """THINC/WLIC moves vf through faces only (periodic flow axis, no flux
+    through walls): the fluid sum stays; the next front tracking brings the
+    field back to the cells' indicator (sum = cell volume)."""
+    from preprocess_src_b200.step import Simulation
+    case = vof_case(vof_k=1000)
+    m = comp(case)
+    with Simulation(case) as sim:
+        s0 = sim.export_vof()[0][m].sum()
+        vol = sim.cell_metrics()["volume"].sum()
+        sim.step(20)
+        vf = sim.export_vof()[0]
+        assert abs(vf[m].sum() - s0) <= 1e-10 * s0
+        sim.front_tracking()
+        vf1 = sim.export_vof()[0]
+        assert np.abs(vf1 - vf).max() > 1e-4
+        assert abs(vf1[m].sum() - vol) <= 0.01 * vol
+
+
+def test_shear_mode_vof_matches_oracle(oracle_mod, native_lib):
+    """x-periodic shear box: the indicator gradient, its solve and THINC/WLIC
+    wrap x like z; a cell straddles the x boundary."""
+    from preprocess_src_b200.step import Simulation
+    case = configs.shear_case("vof_shear", 28, 20, 24, centers=[(-12.5, 0.3, 1.0)], sr=2e-3, subdiv=3, radius=5.0,
+                              lambda1=3.0, vof_k=6, vof_residual=1e-12)
+    o = oracle_mod.Oracle(case)
+    m = comp(case)
+    with Simulation(case) as sim:
+        assert np.abs(sim.export_vof()[0] - o["vf"]).max() <= 1e-8
+        for nsteps in (1, 7):
+            o.step(nsteps)
+            sim.step(nsteps)
+            verr = np.abs(sim.export_vof()[0] - o["vf"]).max()
+            uerr = rel_l2(_u(sim.export_lattice(fn=False), m), _u(o.a, m))
+            print(f"iter {o.iter}: vf max|d| {verr:.2e}  u rel L2 {uerr:.2e}")
+            assert verr <= 2e-6 and uerr <= 1e-5 * o.iter
+
+
+def test_white_cells_get_their_own_volume_fraction(native_lib):
+    """ltc->vf2 of white cells equals ltc->vf of the same cells as red cells;
+    it does not enter omega."""
+    from preprocess_src_b200.step import Simulation
+    case = vof_case()
+    red, white = configs.split_cells(case, 1)
+    with Simulation(case) as a, Simulation(red) as b:
+        b.add_wbc(white)
+        vf_a = a.export_vof()[0]
+        vf_r, vf_w = b.export_vof()
+        assert np.abs(vf_r + vf_w - vf_a).max() <= 1e-8   # the Poisson solve is linear in the cells
+        assert vf_w.max() > 0.5 and vf_r.max() > 0.5
+
+
+def test_restart_carries_the_volume_fraction(native_lib, tmp_path):
+    from oracle import ref_files as RF
+    from preprocess_src_b200.step import Simulation
+    case = vof_case()
+    with Simulation(case) as a, Simulation(case) as b:
+        a.step(13)
+        a.write_restart(tmp_path / "restart.bin", fnum=2)
+        r = RF.read_restart(tmp_path / "restart.bin", case.n, case.ncell, case.vertex, case.element)
+        vf, vf2 = a.export_vof()
+        np.testing.assert_array_equal(r["vf"], vf)
+        np.testing.assert_array_equal(r["vf2"], vf2)
+        b.import_vof(np.zeros(case.n))
+        assert b.read_restart(tmp_path / "restart.bin") == 2
+        np.testing.assert_array_equal(b.export_vof()[0], vf)
