@@ -734,6 +734,7 @@ int launch_front_tracking_stage(rbc_handle *h)
 int vof_init_group(rbc_handle *h, CellGroup &g)
 {
     const size_t n = (size_t)h->geo.nint;
+    if (h->geo.nint >= (1LL << 31)) return fail(h, RBC_ERR_UNSUPPORTED, "the volume fraction needs fewer than 2^31 nodes");
     if (!h->vof_s1) {
         CK(cudaMalloc(&h->vof_s1, 8 * n));
         CK(cudaMalloc(&h->vof_s2, 8 * n));

@@ -55,93 +55,107 @@ __device__ __forceinline__ bool fluid_col(const uint32_t *mask2d, int nx, int x,
 
 // ---- THINC/WLIC ---------------------------------------------------------
 
-struct Node { int x, y, z; };
+// A CTA sweeps a tile of TX x TY x TZ nodes.  It stages vf of the tile and a
+// halo of two nodes in shared memory, computes the interface normal
+// (normal3d_st1/st2) once for every node of the tile and its two neighbour
+// layers along the sweep, then each node computes the fluxes through its two
+// faces along the sweep from the staged values.
+constexpr int TX = 32, TY = 4, TZ = 4, HALO = 2;
+constexpr int SX = TX + 2 * HALO, SY = TY + 2 * HALO, SZ = TZ + 2 * HALO;
+constexpr int NMAX = (TX + 2) * TY * TZ > TX * (TY + 2) * TZ ? (TX + 2) * TY * TZ : TX * (TY + 2) * TZ;
 
-// n + s e_D with the periodic axes wrapped (z always, x in the shear mode)
+template <int D> struct NormalRegion {   // the tile extended by one node each way along D
+    static constexpr int nx = TX + (D == 0 ? 2 : 0), ny = TY + (D == 1 ? 2 : 0), nz = TZ + (D == 2 ? 2 : 0);
+    static constexpr int ox = D == 0 ? 1 : 0, oy = D == 1 ? 1 : 0, oz = D == 2 ? 1 : 0;   // region origin = tile - o
+};
+
+// normal at staged node (sx, sy, sz) (shared coordinates, >= 1 and < S - 1).
+// The average over the eight cell corners of normal3d_st1's corner gradients
+// is, per component, the central difference across the node weighted (1, 2,
+// 1) x (1, 2, 1) over the two other axes, divided by 32 dx: the 27 staged
+// values are read once.
+__device__ __forceinline__ void staged_normal(const double (&sv)[SZ][SY][SX], int sx, int sy, int sz, double inv32dx,
+                                              double n[3])
+{
+    double V[3][3][3];
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int b = 0; b < 3; b++)
+#pragma unroll
+            for (int c = 0; c < 3; c++) V[a][b][c] = sv[sz + a - 1][sy + b - 1][sx + c - 1];
+    const double w[3] = {1.0, 2.0, 1.0};
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int b = 0; b < 3; b++) {
+            s0 += w[a] * w[b] * (V[a][b][2] - V[a][b][0]);   // x: weights over (z, y)
+            s1 += w[a] * w[b] * (V[a][2][b] - V[a][0][b]);   // y: weights over (z, x)
+            s2 += w[a] * w[b] * (V[2][a][b] - V[0][a][b]);   // z: weights over (y, x)
+        }
+    n[0] = s0 * inv32dx;
+    n[1] = s1 * inv32dx;
+    n[2] = s2 * inv32dx;
+}
+
+// p wrapped into [0, n) for |p| within a few periods (tile and halo offsets)
+__device__ __forceinline__ int wrap_near(int p, int n)
+{
+    while (p < 0) p += n;
+    while (p >= n) p -= n;
+    return p;
+}
+
+template <int D> struct FaceRegion {   // faces along D: the tile's nodes and one beyond it along D
+    static constexpr int nx = TX + (D == 0), ny = TY + (D == 1), nz = TZ + (D == 2);
+};
+constexpr int FMAX = TX * TY * (TZ + 1) > TX * (TY + 1) * TZ ? TX * TY * (TZ + 1) : TX * (TY + 1) * TZ;
+
+// flux through the face between a = b - e_D and b (wlic1d4md_st1,
+// thincwlic.cu:108-238).  (bx, by, bz): b in lattice coordinates; (tx, ty, tz):
+// b in tile coordinates (the upwind node is b or a, inside the normal region).
 template <int D>
-__device__ __forceinline__ Node step(const Geom &g, Node n, int s)
+__device__ double face_flux(const Geom &g, const double (&sv)[SZ][SY][SX], const double (&sn)[3][NMAX],
+                            const float4 *__restrict__ uvr, const uint32_t *__restrict__ mask2d,
+                            int bx, int by, int bz, int tx, int ty, int tz, double dt)
 {
-    if (D == 0) n.x = g.xper ? wrap_x(n.x + s, g.nx) : n.x + s;
-    if (D == 1) n.y += s;
-    if (D == 2) n.z = wrap_z(n.z + s, g.nzc);
-    return n;
-}
-
-__device__ __forceinline__ long long lin(const Geom &g, Node n) { return (long long)n.z * g.plane + (long long)n.y * g.nx + n.x; }
-
-// vf at n + (ox, oy, oz), o in {-1, 0, 1}; the offsets never leave the lattice
-// along a non-periodic axis for the interior nodes this is called for
-__device__ __forceinline__ double vf_at(const Geom &g, const double *vf, Node n, int ox, int oy, int oz)
-{
-    int x = n.x + ox;
-    if (g.xper) x = wrap_x(x, g.nx);
-    const int z = wrap_z(n.z + oz, g.nzc);
-    return __ldg(&vf[(long long)z * g.plane + (long long)(n.y + oy) * g.nx + x]);
-}
-
-// normal3d_st1 + normal3d_st2 (thincwlic.cu:12-106) at node n
-__device__ void interface_normal(const Geom &g, const double *vf, Node n, double nrm[3])
-{
-    double V[3][3][3];   // V[oz + 1][oy + 1][ox + 1]
-#pragma unroll
-    for (int oz = -1; oz <= 1; oz++)
-#pragma unroll
-        for (int oy = -1; oy <= 1; oy++)
-#pragma unroll
-            for (int ox = -1; ox <= 1; ox++) V[oz + 1][oy + 1][ox + 1] = vf_at(g, vf, n, ox, oy, oz);
-    const double c = 0.25 / g.dx;
-    double s[3] = {0.0, 0.0, 0.0};
-    // corners in the reference's summation order: i, i+z, i+x, i+x+z, i+y, i+y+z, i+x+y, i+x+y+z
-    const int cx[8] = {0, 0, 1, 1, 0, 0, 1, 1}, cy[8] = {0, 0, 0, 0, 1, 1, 1, 1}, cz[8] = {0, 1, 0, 1, 0, 1, 0, 1};
-#pragma unroll
-    for (int k = 0; k < 8; k++) {
-        // W(dx, dy, dz) = vf at corner - (dx, dy, dz); corner (cx, cy, cz) relative to n
-#define W(a, b, d) V[cz[k] - (d) + 1][cy[k] - (b) + 1][cx[k] - (a) + 1]
-        s[0] += c * (W(0, 0, 0) - W(1, 0, 0) + W(0, 1, 0) - W(1, 1, 0) + W(0, 0, 1) - W(1, 0, 1) + W(0, 1, 1) - W(1, 1, 1));
-        s[1] += c * (W(0, 0, 0) - W(0, 1, 0) + W(1, 0, 0) - W(1, 1, 0) + W(0, 0, 1) - W(0, 1, 1) + W(1, 0, 1) - W(1, 1, 1));
-        s[2] += c * (W(0, 0, 0) - W(0, 0, 1) + W(1, 0, 0) - W(1, 0, 1) + W(0, 1, 0) - W(0, 1, 1) + W(1, 1, 0) - W(1, 1, 1));
-#undef W
-    }
-    nrm[0] = 0.125 * s[0];
-    nrm[1] = 0.125 * s[1];
-    nrm[2] = 0.125 * s[2];
-}
-
-// flux through the low face of node b along D (wlic1d4md_st1, thincwlic.cu:108-238)
-template <int D>
-__device__ double face_flux(const Geom &g, const double *vf, const float4 *uvr, const uint32_t *mask2d, Node b,
-                            double dt)
-{
+    using R = NormalRegion<D>;
     // wlic1d4md_st1 returns for raw index 0 or 1 along any axis and for the last
     // raw index; on the periodic axes those nodes are BUFF images whose faces no
     // fluid node uses
-    if (b.y <= 1 || b.y >= g.ny - 1) return 0.0;
-    if (!g.xper && (b.x <= 1 || b.x >= g.nx - 1)) return 0.0;
-    const Node a = step<D>(g, b, -1);
-    if (!fluid_col(mask2d, g.nx, b.x, b.y) || !fluid_col(mask2d, g.nx, a.x, a.y)) return 0.0;
-    const long long ib = lin(g, b), ia = lin(g, a);
-    const float4 qb = __ldg(&uvr[ib]), qa = __ldg(&uvr[ia]);
+    if (by <= 1 || by >= g.ny - 1) return 0.0;
+    if (!g.xper && (bx <= 1 || bx >= g.nx - 1)) return 0.0;
+    int ax = bx, ay = by, az = bz;
+    if (D == 0) ax = g.xper ? wrap_near(bx - 1, g.nx) : bx - 1;
+    if (D == 1) ay = by - 1;
+    if (D == 2) az = wrap_near(bz - 1, g.nzc);
+    if (!fluid_col(mask2d, g.nx, bx, by) || !fluid_col(mask2d, g.nx, ax, ay)) return 0.0;
+    const float4 qb = __ldg(&uvr[(long long)bz * g.plane + (long long)by * g.nx + bx]);
+    const float4 qa = __ldg(&uvr[(long long)az * g.plane + (long long)ay * g.nx + ax]);
     const double up = D == 0 ? qb.x : D == 1 ? qb.y : qb.z;
     const double um = D == 0 ? qa.x : D == 1 ? qa.y : qa.z;
     const double uc = (up + um) / 2.0;
     const int isgn = uc <= 0.0 ? 0 : 1;
-    const Node ii = isgn ? a : b;
-    const double v = __ldg(&vf[isgn ? ia : ib]);
+    // upwind node ii in tile coordinates
+    const int ix = tx - (D == 0 ? isgn : 0), iy = ty - (D == 1 ? isgn : 0), iz = tz - (D == 2 ? isgn : 0);
+    const double v = sv[iz + HALO][iy + HALO][ix + HALO];
     if (v >= 1.0 - 1.0e-6 || v <= 1.0e-6) return v * uc * dt;
-    double nrm[3];
-    interface_normal(g, vf, ii, nrm);
-    const double nn = fabs(nrm[0]) + fabs(nrm[1]) + fabs(nrm[2]);
+    const int ni = ((iz + R::oz) * R::ny + (iy + R::oy)) * R::nx + (ix + R::ox);
+    const double n0 = sn[0][ni], n1 = sn[1][ni], n2 = sn[2][ni];
+    const double nn = fabs(n0) + fabs(n1) + fabs(n2);
     if (nn <= 1.0e-6) return v * uc * dt;
     const double beta = 2.0;
-    const double vlo = __ldg(&vf[lin(g, step<D>(g, ii, -1))]), vhi = __ldg(&vf[lin(g, step<D>(g, ii, 1))]);
+    const double vlo = sv[iz + HALO - (D == 2)][iy + HALO - (D == 1)][ix + HALO - (D == 0)];
+    const double vhi = sv[iz + HALO + (D == 2)][iy + HALO + (D == 1)][ix + HALO + (D == 0)];
     const double alpha = vlo <= vhi ? 1.0 : -1.0;
-    const double a1 = expf(beta * (2.0 * v - 1.0) / alpha);
+    const double a1 = expf(beta * (2.0 * v - 1.0) * alpha);   // / alpha: alpha = +-1, the same value
     const double a3 = expf(beta);
     const double xc = 0.5 / beta * log((a3 * a3 - a1 * a3) / (a1 * a3 - 1.0));
-    const double a4 = coshf(beta * ((double)isgn - uc * dt / g.dx - xc));
+    const double a4 = coshf(beta * ((double)isgn - uc * dt * g.inv_dx - xc));
     const double a5 = coshf(beta * ((double)isgn - xc));
     const double f = 0.5 * (uc * dt - alpha * g.dx / beta * log(a4 / a5));
-    const double w = fabs(nrm[D]) / nn;
+    const double w = fabs(D == 0 ? n0 : D == 1 ? n1 : n2) / nn;
     return f * w + v * uc * dt * (1.0 - w);
 }
 
@@ -150,17 +164,56 @@ __global__ void __launch_bounds__(VOF_THREADS)
 thinc_sweep_kernel(const Geom g, const double *__restrict__ vin, double *__restrict__ vout,
                    const float4 *__restrict__ uvr, const uint32_t *__restrict__ mask2d, double dt)
 {
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= g.nint) return;
-    Node n;
-    n.z = (int)(i / g.plane);
-    const int r = (int)(i - (long long)n.z * g.plane);
-    n.y = r / g.nx;
-    n.x = r - n.y * g.nx;
-    if (!fluid_col(mask2d, g.nx, n.x, n.y)) { vout[i] = 0.0; return; }   // wlic1d4md_st3
-    const double flo = face_flux<D>(g, vin, uvr, mask2d, n, dt);
-    const double fhi = face_flux<D>(g, vin, uvr, mask2d, step<D>(g, n, 1), dt);
-    vout[i] = vin[i] - (fhi - flo) / g.dx;   // wlic1d4md_st2
+    using R = NormalRegion<D>;
+    using F = FaceRegion<D>;
+    __shared__ double sv[SZ][SY][SX];
+    __shared__ double sn[3][NMAX];
+    __shared__ double sf[FMAX];
+    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY, z0 = blockIdx.z * TZ;
+    // stage vf of the tile and its halo; nodes beyond a non-periodic end read 0
+    // (they only enter normals of wall nodes, which no face uses)
+    for (int k = threadIdx.x; k < SX * SY * SZ; k += blockDim.x) {
+        const int lx = k % SX, ly = (k / SX) % SY, lz = k / (SX * SY);
+        int x = x0 + lx - HALO;
+        const int y = y0 + ly - HALO, z = wrap_near(z0 + lz - HALO, g.nzc);
+        double v = 0.0;
+        if (g.xper) x = wrap_near(x, g.nx);
+        if (x >= 0 && x < g.nx && y >= 0 && y < g.ny) v = __ldg(&vin[(long long)z * g.plane + (long long)y * g.nx + x]);
+        sv[lz][ly][lx] = v;
+    }
+    __syncthreads();
+    const double inv32dx = 1.0 / (32.0 * g.dx);
+    for (int k = threadIdx.x; k < R::nx * R::ny * R::nz; k += blockDim.x) {
+        const int rx = k % R::nx, ry = (k / R::nx) % R::ny, rz = k / (R::nx * R::ny);
+        double n[3];
+        staged_normal(sv, rx - R::ox + HALO, ry - R::oy + HALO, rz - R::oz + HALO, inv32dx, n);
+        sn[0][k] = n[0];
+        sn[1][k] = n[1];
+        sn[2][k] = n[2];
+    }
+    __syncthreads();
+    // every face along D of the tile once: the low faces of the tile's nodes and
+    // the high face of its last layer
+    for (int k = threadIdx.x; k < F::nx * F::ny * F::nz; k += blockDim.x) {
+        const int fx = k % F::nx, fy = (k / F::nx) % F::ny, fz = k / (F::nx * F::ny);
+        int x = x0 + fx, y = y0 + fy, z = z0 + fz;
+        double f = 0.0;
+        if (g.xper) x = wrap_near(x, g.nx);
+        z = wrap_near(z, g.nzc);
+        if (x < g.nx && y < g.ny) f = face_flux<D>(g, sv, sn, uvr, mask2d, x, y, z, fx, fy, fz, dt);
+        sf[k] = f;
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < TX * TY * TZ; k += blockDim.x) {
+        const int tx = k % TX, ty = (k / TX) % TY, tz = k / (TX * TY);
+        const int x = x0 + tx, y = y0 + ty, z = z0 + tz;
+        if (x >= g.nx || y >= g.ny || z >= g.nzc) continue;
+        const long long i = (long long)z * g.plane + (long long)y * g.nx + x;
+        if (!fluid_col(mask2d, g.nx, x, y)) { vout[i] = 0.0; continue; }   // wlic1d4md_st3
+        const int lo = (tz * F::ny + ty) * F::nx + tx;
+        const int hi = ((tz + (D == 2)) * F::ny + ty + (D == 1)) * F::nx + tx + (D == 0);
+        vout[i] = sv[tz + HALO][ty + HALO][tx + HALO] - (sf[hi] - sf[lo]) * g.inv_dx;   // wlic1d4md_st2
+    }
 }
 
 // ---- front tracking -------------------------------------------------------
@@ -254,7 +307,7 @@ struct CgArgs {
     const uint32_t *mask2d;
     const double *b;
     double *x, *r, *p, *q;
-    double *partial;          // [2][2 * nblocks]
+    double *partial;          // [2][2 * nblocks]; lattice indices fit 32 bits (checked at setup)
     double tol;
     int itrmax;
     int *iters_out;           // device: sweeps taken, -1 = not converged
@@ -262,27 +315,26 @@ struct CgArgs {
 };
 
 constexpr int CG_THREADS = 256;
+constexpr int CG_BLOCKS_PER_SM = 4;
 
-// A v at node i: v_i - (1/6) sum of the fluid neighbours' v (walls hold 0)
-__device__ __forceinline__ double apply_a(const Geom &g, const uint32_t *mask2d, const double *v, long long i, int x, int y,
+// A v at node i = (x, y, z) of a fluid column: v_i - (1/6) sum of the fluid
+// neighbours' v (walls hold 0)
+__device__ __forceinline__ double apply_a(const Geom &g, const uint32_t *mask2d, const double *v, unsigned i, int x, int y,
                                           int z)
 {
     const double off = (1.0 / (g.dx * g.dx)) / (-6.0 / (g.dx * g.dx));
+    const unsigned pl = (unsigned)g.plane, row = (unsigned)(y * g.nx);
+    const unsigned zo = (unsigned)z * pl;
+    const unsigned zm = (z == 0 ? (unsigned)(g.nzc - 1) * pl : zo - pl), zp = (z == g.nzc - 1 ? 0u : zo + pl);
+    int xm = x - 1, xp = x + 1;
+    if (g.xper) { if (xm < 0) xm += g.nx; if (xp >= g.nx) xp -= g.nx; }
     double s = v[i];
-    auto nb = [&](int xx, int yy, int zz) -> double {
-        if (g.xper) xx = wrap_x(xx, g.nx);
-        else if (xx < 0 || xx >= g.nx) return 0.0;
-        if (yy < 0 || yy >= g.ny) return 0.0;
-        zz = wrap_z(zz, g.nzc);
-        if (!fluid_col(mask2d, g.nx, xx, yy)) return 0.0;
-        return v[(long long)zz * g.plane + (long long)yy * g.nx + xx];
-    };
-    s += off * nb(x, y, z - 1);
-    s += off * nb(x, y - 1, z);
-    s += off * nb(x - 1, y, z);
-    s += off * nb(x + 1, y, z);
-    s += off * nb(x, y + 1, z);
-    s += off * nb(x, y, z + 1);
+    s += off * v[zm + row + x];   // the node's own column is fluid, so are its z neighbours
+    if (y > 0 && fluid_col(mask2d, g.nx, x, y - 1)) s += off * v[zo + row - g.nx + x];
+    if (xm >= 0 && fluid_col(mask2d, g.nx, xm, y)) s += off * v[zo + row + xm];
+    if (xp < g.nx && fluid_col(mask2d, g.nx, xp, y)) s += off * v[zo + row + xp];
+    if (y + 1 < g.ny && fluid_col(mask2d, g.nx, x, y + 1)) s += off * v[zo + row + g.nx + x];
+    s += off * v[zp + row + x];
     return s;
 }
 
@@ -308,11 +360,15 @@ __device__ void grid_sum2(cg::grid_group &grid, double *partial, int bank, doubl
     }
     grid.sync();
     __shared__ double res[2];
-    if (threadIdx.x == 0) {
+    if (threadIdx.x < 32) {   // one warp adds the partials: strided lanes, then a fixed tree
         double ta = 0.0, tb = 0.0;
-        for (unsigned k = 0; k < gridDim.x; k++) { ta += pb[k]; tb += pb[gridDim.x + k]; }
-        res[0] = ta;
-        res[1] = tb;
+        for (unsigned k = threadIdx.x; k < gridDim.x; k += 32) { ta += pb[k]; tb += pb[gridDim.x + k]; }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            ta += __shfl_down_sync(0xffffffffu, ta, o);
+            tb += __shfl_down_sync(0xffffffffu, tb, o);
+        }
+        if (threadIdx.x == 0) { res[0] = ta; res[1] = tb; }
     }
     __syncthreads();
     sa = res[0];
@@ -320,26 +376,24 @@ __device__ void grid_sum2(cg::grid_group &grid, double *partial, int bank, doubl
     __syncthreads();
 }
 
-__global__ void __launch_bounds__(CG_THREADS)
+// Conjugate gradients with the search direction and A p updated in one pass:
+// p = r + beta p and q = A p = A r + beta q, so an iteration is two passes
+// over the lattice and two grid barriers.
+__global__ void __launch_bounds__(CG_THREADS, CG_BLOCKS_PER_SM)
 indicator_cg_kernel(const CgArgs a)
 {
     cg::grid_group grid = cg::this_grid();
     const Geom &g = a.g;
-    const long long stride = (long long)gridDim.x * blockDim.x, first = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    auto coords = [&](long long i, int &x, int &y, int &z) {
-        z = (int)(i / g.plane);
-        const int r = (int)(i - (long long)z * g.plane);
-        y = r / g.nx;
-        x = r - y * g.nx;
-    };
+    const unsigned n = (unsigned)g.nint, pl = (unsigned)g.plane;
+    const unsigned stride = gridDim.x * blockDim.x, first = blockIdx.x * blockDim.x + threadIdx.x;
     double lr = 0.0, lb = 0.0;
-    for (long long i = first; i < g.nint; i += stride) {
-        int x, y, z;
-        coords(i, x, y, z);
-        if (!fluid_col(a.mask2d, g.nx, x, y)) { a.x[i] = 0.0; a.r[i] = 0.0; a.p[i] = 0.0; a.q[i] = 0.0; continue; }
-        const double ri = a.b[i] - apply_a(g, a.mask2d, a.x, i, x, y, z);
+    for (unsigned i = first; i < n; i += stride) {
+        const unsigned z = i / pl, rr = i - z * pl, y = rr / (unsigned)g.nx, x = rr - y * (unsigned)g.nx;
+        a.p[i] = 0.0;
+        a.q[i] = 0.0;
+        if (!fluid_col(a.mask2d, g.nx, (int)x, (int)y)) { a.x[i] = 0.0; a.r[i] = 0.0; continue; }
+        const double ri = a.b[i] - apply_a(g, a.mask2d, a.x, i, (int)x, (int)y, (int)z);
         a.r[i] = ri;
-        a.p[i] = ri;
         lr += ri * ri;
         lb += a.b[i] * a.b[i];
     }
@@ -348,23 +402,25 @@ indicator_cg_kernel(const CgArgs a)
     grid_sum2(grid, a.partial, bank, lr, lb, rr, bb);
     bank ^= 1;
     int it = 0;
+    double beta = 0.0;
     if (bb > 0.0) {
         while (it < a.itrmax && !(sqrt(rr / bb) < a.tol)) {
             double lpq = 0.0;
-            for (long long i = first; i < g.nint; i += stride) {
-                int x, y, z;
-                coords(i, x, y, z);
-                if (!fluid_col(a.mask2d, g.nx, x, y)) continue;
-                const double qi = apply_a(g, a.mask2d, a.p, i, x, y, z);
+            for (unsigned i = first; i < n; i += stride) {
+                const unsigned z = i / pl, rw = i - z * pl, y = rw / (unsigned)g.nx, x = rw - y * (unsigned)g.nx;
+                if (!fluid_col(a.mask2d, g.nx, (int)x, (int)y)) continue;
+                const double pi = a.r[i] + beta * a.p[i];
+                const double qi = apply_a(g, a.mask2d, a.r, i, (int)x, (int)y, (int)z) + beta * a.q[i];
+                a.p[i] = pi;
                 a.q[i] = qi;
-                lpq += a.p[i] * qi;
+                lpq += pi * qi;
             }
             double pq, unused;
             grid_sum2(grid, a.partial, bank, lpq, 0.0, pq, unused);
             bank ^= 1;
             const double alpha = rr / pq;
             double lrr = 0.0;
-            for (long long i = first; i < g.nint; i += stride) {
+            for (unsigned i = first; i < n; i += stride) {
                 const double ri = a.r[i] - alpha * a.q[i];
                 a.x[i] += alpha * a.p[i];
                 a.r[i] = ri;
@@ -373,14 +429,12 @@ indicator_cg_kernel(const CgArgs a)
             double rr_new;
             grid_sum2(grid, a.partial, bank, lrr, 0.0, rr_new, unused);
             bank ^= 1;
-            const double beta = rr_new / rr;
+            beta = rr_new / rr;
             rr = rr_new;
-            for (long long i = first; i < g.nint; i += stride) a.p[i] = a.r[i] + beta * a.p[i];
-            grid.sync();
             it++;
         }
     } else {
-        for (long long i = first; i < g.nint; i += stride) a.x[i] = 0.0;
+        for (unsigned i = first; i < n; i += stride) a.x[i] = 0.0;
     }
     if (first == 0) {
         const bool ok = bb == 0.0 || sqrt(rr / bb) < a.tol;
@@ -404,17 +458,17 @@ cudaError_t vof_setup()
     cudaError_t e = cudaGetDevice(&dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, indicator_cg_kernel, CG_THREADS, 0);
-    if (e == cudaSuccess) g_cg_blocks = sms * (per_sm < 2 ? per_sm : 2);
+    if (e == cudaSuccess) g_cg_blocks = sms * (per_sm < CG_BLOCKS_PER_SM ? per_sm : CG_BLOCKS_PER_SM);
     return e;
 }
 
 void launch_thinc_wlic(const Geom &g, double *vf, double *s1, double *s2, const float4 *uvr, const uint32_t *mask2d,
                        double dt, cudaStream_t s)
 {
-    const unsigned blocks = (unsigned)((g.nint + VOF_THREADS - 1) / VOF_THREADS);
-    thinc_sweep_kernel<0><<<blocks, VOF_THREADS, 0, s>>>(g, vf, s1, uvr, mask2d, dt);
-    thinc_sweep_kernel<1><<<blocks, VOF_THREADS, 0, s>>>(g, s1, s2, uvr, mask2d, dt);
-    thinc_sweep_kernel<2><<<blocks, VOF_THREADS, 0, s>>>(g, s2, vf, uvr, mask2d, dt);
+    const dim3 tiles((unsigned)((g.nx + TX - 1) / TX), (unsigned)((g.ny + TY - 1) / TY), (unsigned)((g.nzc + TZ - 1) / TZ));
+    thinc_sweep_kernel<0><<<tiles, VOF_THREADS, 0, s>>>(g, vf, s1, uvr, mask2d, dt);
+    thinc_sweep_kernel<1><<<tiles, VOF_THREADS, 0, s>>>(g, s1, s2, uvr, mask2d, dt);
+    thinc_sweep_kernel<2><<<tiles, VOF_THREADS, 0, s>>>(g, s2, vf, uvr, mask2d, dt);
 }
 
 cudaError_t launch_front_tracking(const Geom &g, const FrontArgs &a, cudaStream_t s)
