@@ -60,8 +60,14 @@ __device__ __forceinline__ bool fluid_col(const uint32_t *mask2d, int nx, int x,
 // (normal3d_st1/st2) once for every node of the tile and its two neighbour
 // layers along the sweep, then each node computes the fluxes through its two
 // faces along the sweep from the staged values.
+// The staged box: two halo layers along the sweep (a face's upwind node is one
+// beyond the tile and its normal and THINC neighbours one more), one across.
 constexpr int TX = 32, TY = 4, TZ = 4, HALO = 2;
 constexpr int SX = TX + 2 * HALO, SY = TY + 2 * HALO, SZ = TZ + 2 * HALO;
+template <int D> struct Staged {   // the part of the SZ x SY x SX box a sweep along D loads
+    static constexpr int hx = D == 0 ? 2 : 1, hy = D == 1 ? 2 : 1, hz = D == 2 ? 2 : 1;
+    static constexpr int nx = TX + 2 * hx, ny = TY + 2 * hy, nz = TZ + 2 * hz;
+};
 constexpr int NMAX = (TX + 2) * TY * TZ > TX * (TY + 2) * TZ ? (TX + 2) * TY * TZ : TX * (TY + 2) * TZ;
 
 template <int D> struct NormalRegion {   // the tile extended by one node each way along D
@@ -172,8 +178,10 @@ thinc_sweep_kernel(const Geom g, const double *__restrict__ vin, double *__restr
     const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY, z0 = blockIdx.z * TZ;
     // stage vf of the tile and its halo; nodes beyond a non-periodic end read 0
     // (they only enter normals of wall nodes, which no face uses)
-    for (int k = threadIdx.x; k < SX * SY * SZ; k += blockDim.x) {
-        const int lx = k % SX, ly = (k / SX) % SY, lz = k / (SX * SY);
+    using St = Staged<D>;
+    for (int k = threadIdx.x; k < St::nx * St::ny * St::nz; k += blockDim.x) {
+        const int lx = k % St::nx + (HALO - St::hx), ly = (k / St::nx) % St::ny + (HALO - St::hy),
+                  lz = k / (St::nx * St::ny) + (HALO - St::hz);
         int x = x0 + lx - HALO;
         const int y = y0 + ly - HALO, z = wrap_near(z0 + lz - HALO, g.nzc);
         double v = 0.0;
