@@ -104,6 +104,10 @@ struct rbc_handle {
     cudaGraphExec_t graph[3][2] = {{nullptr, nullptr}, {nullptr, nullptr}, {nullptr, nullptr}};
     cudaStream_t side = nullptr;                      // second branch of the pipelined graphs (capture only)
     cudaEvent_t fork = nullptr, join = nullptr;
+    // split membrane pass: the first full wave's spread beside the last wave's membrane (capture only)
+    cudaStream_t side2 = nullptr;
+    cudaEvent_t wave_done = nullptr, spread_done = nullptr;
+    int sms = 0;                                      // multiprocessors of the device
     int prio_high = 0;                                // greatest stream priority of the device
     long long launches = 0;
     float scale = 1.0f, inv_scale = 1.0f;
@@ -114,6 +118,8 @@ struct rbc_handle {
 
     int kernels_per_step() const {
         int k = 2 + (ntube > 0 ? 1 : 0);   // step_begin, lbm (+ tube bounce-back)
+        if (ngroups == 1 && cg[0].br == 0.0 && fileoutput == 0 && sms > 0 && cg[0].ncell > sms && cg[0].ncell % sms)
+            k += 2;                        // the membrane pass and the spread in two launches each
         for (int g = 0; g < ngroups; g++) {
             const CellGroup &c = cg[g];
             if (c.ncell == 0) continue;
@@ -579,6 +585,9 @@ void free_all(rbc_handle *h)
     if (h->fork) cudaEventDestroy(h->fork);
     if (h->join) cudaEventDestroy(h->join);
     if (h->side) cudaStreamDestroy(h->side);
+    if (h->wave_done) cudaEventDestroy(h->wave_done);
+    if (h->spread_done) cudaEventDestroy(h->spread_done);
+    if (h->side2) cudaStreamDestroy(h->side2);
     void *ptrs[] = {h->g[0], h->g[1], h->uvr, h->Fx, h->Fy, h->Fz, h->mask2d, h->tube_links, h->tube_frac,
                     h->d_int, h->d_drive, h->staging, h->vof_s1, h->vof_s2, h->vof_G, h->vof_b, h->vof_partial};
     for (void *q : ptrs) if (q) cudaFree(q);
@@ -589,6 +598,52 @@ void free_all(rbc_handle *h)
 }
 
 // ---- stage launches -------------------------------------------------------
+
+// the membrane pass (stress.cu:580-660) of cells [c0, c1) of population g: the
+// kernel indexes cells from the pointers it is given, so a range is an offset
+int launch_membrane_range(rbc_handle *h, CellGroup &g, int c0, int c1, cudaStream_t st)
+{
+    const size_t rec_bytes = (h->p.membrane_fp64 ? sizeof(double4) : sizeof(float4)) * 3;
+    MembraneArgs a{};
+    a.Xd = g.Xd + (size_t)c0 * g.V; a.nv = g.nv; a.ne = g.ne; a.gref = g.gref + (size_t)c0 * g.E;
+    a.erec = (char *)g.erec + (size_t)c0 * g.E * rec_bytes;
+    a.tri = g.tri; a.v2e_off = g.v2e_off; a.v2e = g.v2e; a.nbr = g.nbr; a.Fv = g.Fv + (size_t)c0 * g.V;
+    a.V = g.V; a.E = g.E; a.ncell = c1 - c0;
+    a.C = h->p.C; a.rgs = g.rgs; a.law = h->p.law; a.LX = h->p.LX; a.LZ = h->p.LZ;
+    a.niter = h->p.solver_iters > 0 ? h->p.solver_iters : DEFAULT_SOLVER_ITERS;
+    a.flags = h->d_flags();
+    a.priority = h->prio_high;
+    launch_membrane(a, h->p.membrane_fp64 != 0, st);
+    h->launches++;
+    CK_LAUNCH();
+    return RBC_OK;
+}
+
+// the spread (ibm.cu:299-369) of cells [c0, c1) of population g
+int launch_spread_range(rbc_handle *h, CellGroup &g, int c0, int c1, cudaStream_t st)
+{
+    SpreadArgs a{};
+    a.X = g.X + (size_t)c0 * g.V; a.nv = g.nv; a.V = g.V; a.ncell = c1 - c0; a.Fv = g.Fv + (size_t)c0 * g.V;
+    a.patch_off = g.patch_off; a.patch_vtx = g.patch_vtx; a.patch_stride = g.patch_stride;
+    a.npatch = g.npatch;
+    a.Fx = h->Fx; a.Fy = h->Fy; a.Fz = h->Fz; a.mask2d = h->mask2d; a.flags = h->d_flags();
+    launch_spread(h->geo, a, st);
+    h->launches++;
+    CK_LAUNCH();
+    return RBC_OK;
+}
+
+// Cells in the full waves of the membrane kernel (one CTA per cell and per
+// multiprocessor) when splitting off the last partial wave pays: one
+// population, no bending and no output averages (both read all the forces
+// of the step), more cells than multiprocessors.  0 = no split.
+int membrane_wave_split(const rbc_handle *h)
+{
+    const CellGroup &g = h->cg[0];
+    if (h->ngroups != 1 || g.br != 0.0 || h->fileoutput > 0 || h->sms <= 0 || g.ncell <= h->sms) return 0;
+    const int full = (g.ncell / h->sms) * h->sms;
+    return full < g.ncell ? full : 0;
+}
 
 // stress() (stress.cu:580-660) for every cell population
 int launch_stress(rbc_handle *h)
@@ -791,6 +846,14 @@ enum StepForm { STEP_WHOLE = 0, STEP_BODY = 1, STEP_PIPELINED = 2 };
 // membrane (the membrane pass reads fem->xd, which the correction does not
 // touch; the correction writes cel->x, which the spread reads, so the
 // branches join before the spread).
+//
+// With more cells than multiprocessors the membrane kernel (one cell per
+// multiprocessor) runs in full waves and a last partial one that leaves most
+// multiprocessors idle.  Then the full waves run as one launch and the last
+// wave as a second, high-priority launch, while a third branch spreads the
+// full waves' cells beside it: each cell's spread needs only its own forces,
+// and the spread adds integer fixed-point values, so the order of the two
+// spreads does not change the force field.
 int enqueue_step(rbc_handle *h, StepForm form = STEP_WHOLE)
 {
     int rc;
@@ -804,10 +867,25 @@ int enqueue_step(rbc_handle *h, StepForm form = STEP_WHOLE)
     launch_step_begin(step_begin_args(h), h->stream);
     h->launches++;
     CK_LAUNCH();
-    if ((rc = launch_stress(h))) return rc;
-    if (pipelined) CK(cudaStreamWaitEvent(h->stream, h->join, 0));
-    if ((rc = launch_bend_stage(h))) return rc;   // reads cel->x, after the correction
-    if ((rc = launch_spread_stage(h))) return rc;
+    const int split = membrane_wave_split(h);
+    if (split > 0) {
+        CellGroup &g = h->cg[0];
+        if ((rc = launch_membrane_range(h, g, 0, split, h->stream))) return rc;
+        CK(cudaEventRecord(h->wave_done, h->stream));
+        if ((rc = launch_membrane_range(h, g, split, g.ncell, h->stream))) return rc;
+        CK(cudaStreamWaitEvent(h->side2, h->wave_done, 0));
+        if (pipelined) CK(cudaStreamWaitEvent(h->side2, h->join, 0));   // the spread reads cel->x
+        if ((rc = launch_spread_range(h, g, 0, split, h->side2))) return rc;
+        CK(cudaEventRecord(h->spread_done, h->side2));
+        if (pipelined) CK(cudaStreamWaitEvent(h->stream, h->join, 0));
+        if ((rc = launch_spread_range(h, g, split, g.ncell, h->stream))) return rc;
+        CK(cudaStreamWaitEvent(h->stream, h->spread_done, 0));
+    } else {
+        if ((rc = launch_stress(h))) return rc;
+        if (pipelined) CK(cudaStreamWaitEvent(h->stream, h->join, 0));
+        if ((rc = launch_bend_stage(h))) return rc;   // reads cel->x, after the correction
+        if ((rc = launch_spread_stage(h))) return rc;
+    }
     if ((rc = launch_lbm_stage(h))) return rc;
     if ((rc = launch_advect_stage(h))) return rc;
     if ((rc = launch_thinc_stage(h))) return rc;   // main.cu:94-95
@@ -1109,8 +1187,12 @@ int rbc_create(const rbc_params *p, const rbc_mesh *mesh, const int *bc, rbc_han
         if (cudaDeviceGetStreamPriorityRange(&lo, &hi) != cudaSuccess ||
             cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
             cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaStreamCreateWithFlags(&h->side2, cudaStreamNonBlocking) != cudaSuccess ||
             cudaEventCreateWithFlags(&h->fork, cudaEventDisableTiming) != cudaSuccess ||
-            cudaEventCreateWithFlags(&h->join, cudaEventDisableTiming) != cudaSuccess) {
+            cudaEventCreateWithFlags(&h->join, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&h->wave_done, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&h->spread_done, cudaEventDisableTiming) != cudaSuccess ||
+            cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, h->device) != cudaSuccess) {
             h->err = "stream creation failed";
             return bail(RBC_ERR_CUDA);
         }

@@ -362,3 +362,29 @@ def test_launch_count_and_status(developed):
     assert sim.launches - n0 == 4 * 6
     flags, _ = sim.status()
     assert flags == 0, flags
+
+
+def test_split_membrane_wave_equals_stage_calls(native_lib):
+    """More cells than multiprocessors: rbc_step runs the membrane pass as its
+    full waves plus the last partial wave, the full waves' spread beside the
+    last wave.  The spread adds integer fixed-point values, so the steps equal
+    the stage-by-stage steps (one membrane and one spread launch) bit for bit."""
+    import torch
+    from preprocess_src_b200.step import Simulation
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    ncell = sms + 12
+    case = configs.suspension_case("many_small_cells", 96, 44, 44, ncell, subdiv=2, radius=2.5, seed=5,
+                                   g=4e-5, Gs=2e-3)
+    with Simulation(case) as a, Simulation(case) as b:
+        n0 = a.launches
+        a.step(3)
+        assert a.launches - n0 == 3 * (6 + 2)   # two more launches per step
+        for _ in range(3):
+            b.iter = b.iter + 1
+            b.stress(); b.ibm_st1(); b.lbm_d3q19(); b.ibm_st2(); b.volume_correction()
+        ca, cb = a.export_cells(), b.export_cells()
+        for k in ("x", "y", "z", "fx", "fy", "fz"):
+            np.testing.assert_array_equal(ca[k], cb[k], err_msg=k)
+        la, lb = a.export_lattice(fn=False), b.export_lattice(fn=False)
+        np.testing.assert_array_equal(la["wn"], lb["wn"])
+        assert a.status() == b.status()
