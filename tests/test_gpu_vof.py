@@ -150,3 +150,36 @@ def test_restart_carries_the_volume_fraction(native_lib, tmp_path):
         b.import_vof(np.zeros(case.n))
         assert b.read_restart(tmp_path / "restart.bin") == 2
         np.testing.assert_array_equal(b.export_vof()[0], vf)
+
+
+def test_vof_in_the_circular_tube_matches_oracle(oracle_mod, native_lib):
+    """The circular tube (interpolated bounce-back) with the volume fraction:
+    wall columns outside the circle keep vf = 0 and no flux."""
+    from preprocess_src_b200.step import Simulation
+    case = configs.tube_case("vof_tube", 32, 9.3, centers=[(0.3, -0.2, 12.0)], subdiv=3, radius=4.5, seed=2,
+                             lambda1=4.0, vof_k=5, vof_residual=1e-12, g=4e-5, Gs=2e-3)
+    o = oracle_mod.Oracle(case)
+    m = comp(case)
+    with Simulation(case) as sim:
+        assert np.abs(sim.export_vof()[0] - o["vf"]).max() <= 1e-8
+        o.step(7)
+        sim.step(7)
+        verr = np.abs(sim.export_vof()[0] - o["vf"]).max()
+        uerr = rel_l2(_u(sim.export_lattice(fn=False), m), _u(o.a, m))
+        print(f"tube: vf max|d| {verr:.2e}  u rel L2 {uerr:.2e}")
+        assert verr <= 2e-6 and uerr <= 1e-4
+
+
+def test_vof_with_fp16_storage(native_lib):
+    """FP16 population storage with the viscosity ratio: the same volume
+    fraction and flow as FP32 storage to the FP16 round-off."""
+    from preprocess_src_b200.step import Simulation
+    m = comp(vof_case())
+    out = {}
+    for st in (0, 1):
+        with Simulation(vof_case(storage=st)) as sim:
+            sim.step(12)
+            out[st] = (sim.export_vof()[0], _u(sim.export_lattice(fn=False), m))
+            assert sim.status()[0] & 3 == 0
+    assert np.abs(out[1][0] - out[0][0]).max() <= 1e-4
+    assert rel_l2(out[1][1], out[0][1]) <= 5e-3
