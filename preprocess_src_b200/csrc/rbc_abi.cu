@@ -115,6 +115,11 @@ struct rbc_handle {
     int device = 0;
     AdjointState *adj = nullptr;                      // checkpoints and buffers of the adjoint, on first use
     int fileoutput = 0;                               // FILEOUTPUT of the qi / tp averages; 0 = not accumulated
+    // the volume correction that ended the last rbc_step left every population's
+    // volume, area (vol_out, area_out) and centroid (gx) of the current state
+    bool metrics_valid = false;
+    double *metrics_host = nullptr;                   // pinned staging of one population's metrics [5][ncell]
+    size_t metrics_host_n = 0;
 
     int kernels_per_step() const {
         int k = 2 + (ntube > 0 ? 1 : 0);   // step_begin, lbm (+ tube bounce-back)
@@ -149,7 +154,15 @@ struct rbc_handle {
         }                                                                              \
     } while (0)
 
+// Entry points that may change the device state drop the record that the
+// cells' metrics on the device are those of the current state; read-only
+// entry points keep it.
 #define RBC_DEVICE_GUARD(h)                                                            \
+    do {                                                                               \
+        if (cudaSetDevice((h)->device) != cudaSuccess) return RBC_ERR_CUDA;            \
+        (h)->metrics_valid = false;                                                    \
+    } while (0)
+#define RBC_DEVICE_GUARD_RO(h)                                                         \
     do {                                                                               \
         if (cudaSetDevice((h)->device) != cudaSuccess) return RBC_ERR_CUDA;            \
     } while (0)
@@ -585,6 +598,7 @@ void free_all(rbc_handle *h)
     if (h->fork) cudaEventDestroy(h->fork);
     if (h->join) cudaEventDestroy(h->join);
     if (h->side) cudaStreamDestroy(h->side);
+    if (h->metrics_host) cudaFreeHost(h->metrics_host);
     if (h->wave_done) cudaEventDestroy(h->wave_done);
     if (h->spread_done) cudaEventDestroy(h->spread_done);
     if (h->side2) cudaStreamDestroy(h->side2);
@@ -1080,18 +1094,29 @@ int upload_group(rbc_handle *h, CellGroup &c, const rbc_mesh *mesh, const GroupP
     return RBC_OK;
 }
 
-// volume, area, centroid of the cells of population g (synchronous)
+// volume, area, centroid of the cells of population g (synchronous): the values
+// the step's volume correction left when the state is that step's, else a
+// launch of the volume kernel in measuring mode
 int group_metrics(rbc_handle *h, CellGroup &g, double *volume, double *area, double *centroid)
 {
     if (g.ncell == 0) return fail(h, RBC_ERR_STATE, "no cells in this population");
-    launch_volume(h->geo, volume_args(h, g, 0), h->stream);
-    h->launches++;
-    CK_LAUNCH();
     const int N = g.ncell;
-    std::vector<double> t(5 * N);
-    CK(cudaMemcpyAsync(t.data(), g.vol_out, 8 * N, cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaMemcpyAsync(t.data() + N, g.area_out, 8 * N, cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaMemcpyAsync(t.data() + 2 * N, g.cen_out, 8 * 3 * N, cudaMemcpyDeviceToHost, h->stream));
+    const double *cen = g.gx;
+    if (!h->metrics_valid) {
+        launch_volume(h->geo, volume_args(h, g, 0), h->stream);
+        h->launches++;
+        CK_LAUNCH();
+        cen = g.cen_out;
+    }
+    if (h->metrics_host_n < (size_t)N) {
+        if (h->metrics_host) { CK(cudaFreeHost(h->metrics_host)); h->metrics_host = nullptr; h->metrics_host_n = 0; }
+        CK(cudaMallocHost(&h->metrics_host, 8 * 5 * (size_t)N));
+        h->metrics_host_n = N;
+    }
+    double *t = h->metrics_host;
+    CK(cudaMemcpyAsync(t, g.vol_out, 8 * N, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(t + N, g.area_out, 8 * N, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(t + 2 * N, cen, 8 * 3 * N, cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
     for (int c = 0; c < N; c++) {
         if (volume) volume[c] = t[c];
@@ -1302,7 +1327,7 @@ int rbc_import_ref_lattice(rbc_handle *h, const double *fn)
 int rbc_export_ref_lattice(rbc_handle *h, double *fn, double *dn, double *un, double *vn, double *wn)
 {
     if (!h) return RBC_ERR_ARG;
-    RBC_DEVICE_GUARD(h);
+    RBC_DEVICE_GUARD_RO(h);
     const bool macro = dn || un || vn || wn;
     if (!fn && !macro) return RBC_OK;
     const size_t n = (size_t)h->nref_nodes;
@@ -1326,7 +1351,7 @@ int rbc_export_ref_lattice(rbc_handle *h, double *fn, double *dn, double *un, do
 int rbc_export_ref_force(rbc_handle *h, double *fx, double *fy, double *fz)
 {
     if (!h) return RBC_ERR_ARG;
-    RBC_DEVICE_GUARD(h);
+    RBC_DEVICE_GUARD_RO(h);
     const size_t n = (size_t)h->nref_nodes;
     int rc = ensure_staging(h, sizeof(double) * 3 * n);
     if (rc) return rc;
@@ -1399,7 +1424,7 @@ static int export_cells(rbc_handle *h, CellGroup &G, double *x, double *y, doubl
                         double *u, double *v, double *w, double *fx, double *fy, double *fz, double *gxo)
 {
     if (!h) return RBC_ERR_ARG;
-    RBC_DEVICE_GUARD(h);
+    RBC_DEVICE_GUARD_RO(h);
     if (G.ncell == 0) return fail(h, RBC_ERR_STATE, "no cells in this population");
     const long long nv = G.nv;
     const int N = G.ncell;
@@ -1519,7 +1544,7 @@ int rbc_front_tracking(rbc_handle *h, int *iters)
 // ltc->vf / vf2 [nx*ny*nz] in the reference layout <-> the populations' internal fields
 static int vof_transfer(rbc_handle *h, double *out0, double *out1, const double *in0, const double *in1)
 {
-    RBC_DEVICE_GUARD(h);
+    if (in0 || in1) RBC_DEVICE_GUARD(h); else RBC_DEVICE_GUARD_RO(h);
     if (!h->vof()) return fail(h, RBC_ERR_STATE, "the volume fraction is not tracked (vof_k = 0)");
     const Geom &g = h->geo;
     std::vector<uint32_t> mask((size_t)g.plane);
@@ -1624,6 +1649,7 @@ int rbc_step(rbc_handle *h, int nsteps)
         if ((rc = launch_volume_stage(h, h->stream))) return rc;
     }
     h->iter += nsteps;
+    h->metrics_valid = h->has_cells();   // the last kernels of every population were its volume correction
     return RBC_OK;
 }
 
@@ -1664,6 +1690,7 @@ int rbc_profile_steps(rbc_handle *h, int nsteps, double *kernel_ms)
     }
     for (auto &e : ev) cudaEventDestroy(e);
     if (rc == RBC_OK) h->iter += nsteps;
+    h->metrics_valid = rc == RBC_OK && nsteps > 0 && h->has_cells();
     return rc;
 }
 
@@ -1677,7 +1704,7 @@ int rbc_get_stream(const rbc_handle *h, void **stream)
 int rbc_get_status(rbc_handle *h, int *flags, int *vc_iters_max)
 {
     if (!h) return RBC_ERR_ARG;
-    RBC_DEVICE_GUARD(h);
+    RBC_DEVICE_GUARD_RO(h);
     int v[4];
     CK(cudaStreamSynchronize(h->stream));
     CK(cudaMemcpy(v, h->d_int, sizeof(v), cudaMemcpyDeviceToHost));
@@ -1690,7 +1717,7 @@ int rbc_get_status(rbc_handle *h, int *flags, int *vc_iters_max)
 int rbc_cell_metrics(rbc_handle *h, double *volume, double *area, double *centroid)
 {
     if (!h) return RBC_ERR_ARG;
-    RBC_DEVICE_GUARD(h);
+    RBC_DEVICE_GUARD_RO(h);
     if (h->ncell == 0) return fail(h, RBC_ERR_STATE, "handle has no cells");
     return group_metrics(h, h->cg[0], volume, area, centroid);
 }
@@ -1698,7 +1725,7 @@ int rbc_cell_metrics(rbc_handle *h, double *volume, double *area, double *centro
 int rbc_synchronize(rbc_handle *h)
 {
     if (!h) return RBC_ERR_ARG;
-    RBC_DEVICE_GUARD(h);
+    RBC_DEVICE_GUARD_RO(h);
     CK(cudaStreamSynchronize(h->stream));
     return RBC_OK;
 }
@@ -1820,6 +1847,7 @@ int rbc_batch_step(rbc_batch *b, int nsteps)
         if (nsteps & 1) h->cur ^= 1;
         h->iter += nsteps;
         h->launches += (long long)h->kernels_per_step() * nsteps;
+        h->metrics_valid = h->has_cells();   // each simulation's step ends with its volume correction
         CKB(cudaStreamWaitEvent(h->stream, b->done, 0));
     }
     return RBC_OK;
@@ -2485,7 +2513,7 @@ int rbc_export_ref_wbc(rbc_handle *h, double *x, double *y, double *z, double *x
 int rbc_wbc_metrics(rbc_handle *h, double *volume, double *area, double *centroid)
 {
     if (!h) return RBC_ERR_ARG;
-    RBC_DEVICE_GUARD(h);
+    RBC_DEVICE_GUARD_RO(h);
     if (h->ngroups < 2) return fail(h, RBC_ERR_STATE, "no white cells (rbc_add_wbc)");
     return group_metrics(h, h->cg[1], volume, area, centroid);
 }

@@ -388,3 +388,21 @@ def test_split_membrane_wave_equals_stage_calls(native_lib):
         la, lb = a.export_lattice(fn=False), b.export_lattice(fn=False)
         np.testing.assert_array_equal(la["wn"], lb["wn"])
         assert a.status() == b.status()
+
+
+def test_cell_metrics_after_a_step_equal_the_measured_ones(developed):
+    """After rbc_step the metrics come from the step's volume correction; after
+    any call that may change the state the volume kernel measures them."""
+    case, o = developed
+    sim = load(o)
+    sim.step(3)
+    cached = sim.cell_metrics()
+    sim.iter = sim.iter   # a state-changing entry point: the next call measures
+    n0 = sim.launches
+    measured = sim.cell_metrics()
+    assert sim.launches == n0 + 1
+    for k in ("volume", "area", "centroid"):
+        np.testing.assert_allclose(cached[k], measured[k], rtol=1e-12, atol=1e-12, err_msg=k)
+    n0 = sim.launches
+    sim.cell_metrics()
+    assert sim.launches == n0 + 1   # still no step since: measured again
