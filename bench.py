@@ -56,6 +56,7 @@ def parse():
                          "with the cells' volume fraction tracked (front tracking every --vof-k steps) and "
                          "viscosity ratio LAMBDA1 = 5")
     ap.add_argument("--vof-k", type=int, default=100, help="front-tracking interval K (vof workload)")
+    ap.add_argument("--br", type=float, default=0.0, help="bending modulus BR (dense and single workloads)")
     ap.add_argument("--capillaries", type=int, default=512, help="number of capillaries (capillaries workload)")
     ap.add_argument("--storage", default="f32", choices=["f32", "f16"])
     ap.add_argument("--adjoint-steps", type=int, default=2000, help="steps of the recorded run (adjoint workload)")
@@ -67,15 +68,15 @@ def parse():
     return ap.parse_args()
 
 
-def make_case(workload, seed_offset=0, storage="f32", vof_k=100):
+def make_case(workload, seed_offset=0, storage="f32", vof_k=100, br=0.0):
     from preprocess_src_b200 import configs
     st = 1 if storage == "f16" else 0
     if workload == "single":
-        return configs.single_cell_duct(seed=1 + seed_offset, storage=st)
+        return configs.single_cell_duct(seed=1 + seed_offset, storage=st, br=br)
     if workload == "vof":
         return configs.dense_suspension(seed=2 + seed_offset, storage=st, lambda1=5.0, vof_k=vof_k,
                                         vof_residual=1e-10)
-    return configs.dense_suspension(seed=2 + seed_offset, storage=st)
+    return configs.dense_suspension(seed=2 + seed_offset, storage=st, br=br)
 
 
 def measured_hbm():
@@ -207,7 +208,7 @@ def run_ours(args, world, rank, local):
 
     from preprocess_src_b200.step import Simulation
 
-    case = make_case(args.workload, seed_offset=rank, storage=args.storage, vof_k=args.vof_k)
+    case = make_case(args.workload, seed_offset=rank, storage=args.storage, vof_k=args.vof_k, br=args.br)
     dev = local
     sim = Simulation(case, device=dev)
     fluid, nv = case.fluid_nodes(), case.ncell * case.vertex
@@ -271,6 +272,8 @@ def run_ours(args, world, rank, local):
         if args.workload == "vof":
             result["config"].update(lambda1=case.params["lambda1"], vof_k=case.params["vof_k"],
                                     vof_residual=case.params["vof_residual"])
+        if args.br:
+            result["config"]["bending_br"] = args.br
         if e2e:
             result["e2e"] = e2e
         if world == 1 and not args.no_cpu and args.workload != "vof":

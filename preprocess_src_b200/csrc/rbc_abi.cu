@@ -53,6 +53,7 @@ struct CellGroup {
     int16_t *nbr = nullptr;
     int4 *visit = nullptr;   // bending visits [E][3], allocated when BR != 0
     double2 *cs0 = nullptr;  // spontaneous angle (cos, sin) per visit [ncell][E][3] (bend_spont), else none
+    double *bend_rec = nullptr;   // bending visit records [ncell][E][3][9], allocated when BR != 0
     double *vol0 = nullptr, *gx = nullptr, *vol_out = nullptr, *area_out = nullptr, *cen_out = nullptr;
     int *patch_off = nullptr, *patch_vtx = nullptr, *patch_stride = nullptr;
     int npatch = 1;
@@ -128,7 +129,7 @@ struct rbc_handle {
         for (int g = 0; g < ngroups; g++) {
             const CellGroup &c = cg[g];
             if (c.ncell == 0) continue;
-            k += 4 + (c.br != 0.0 ? 1 : 0) + (fileoutput > 0 ? 2 : 0);   // membrane, spread, advect, volume
+            k += 4 + (c.br != 0.0 ? 2 : 0) + (fileoutput > 0 ? 2 : 0);   // membrane, spread, advect, volume
             if (c.vf) k += 3;                                            // THINC/WLIC sweeps
         }
         return k;
@@ -585,7 +586,7 @@ void free_group(CellGroup &c)
 {
     void *cp[] = {c.X, c.Xd, c.gref, c.erec, c.U, c.Fv, c.tri, c.v2e_off, c.v2e, c.nbr, c.visit, c.cs0, c.patch_off,
                   c.patch_vtx, c.patch_stride, c.vol0, c.gx, c.vol_out, c.area_out, c.cen_out, c.qi_acc, c.tp_acc,
-                  c.vf};
+                  c.vf, c.bend_rec};
     for (void *q : cp) if (q) cudaFree(q);
     c = CellGroup{};
 }
@@ -716,10 +717,10 @@ int launch_bend_stage(rbc_handle *h)
         if (g.ncell == 0 || g.br == 0.0) continue;
         BendArgs a{};
         a.X = g.X; a.nv = g.nv; a.V = g.V; a.E = g.E; a.v2e_off = g.v2e_off; a.v2e = g.v2e; a.visit = g.visit;
-        a.cs0 = g.cs0;
+        a.cs0 = g.cs0; a.ncell = g.ncell; a.rec = g.bend_rec;
         a.LX = h->p.LX; a.LZ = h->p.LZ; a.coef = 2.0 / std::sqrt(3.0) * g.br; a.Fv = g.Fv;
         launch_bend(a, h->stream);
-        h->launches++;
+        h->launches += 2;   // the visit and gather passes
         CK_LAUNCH();
     }
     return RBC_OK;
@@ -1067,6 +1068,7 @@ int upload_group(rbc_handle *h, CellGroup &c, const rbc_mesh *mesh, const GroupP
     if (!pp.visit.empty()) {
         TRYG(dalloc(h, &c.visit, pp.visit.size()));
         CK(cudaMemcpy(c.visit, pp.visit.data(), sizeof(int4) * pp.visit.size(), cudaMemcpyHostToDevice));
+        TRYG(dalloc(h, &c.bend_rec, (size_t)c.ncell * c.E * 27));
     }
     if (!pp.cs0.empty()) {
         TRYG(dalloc(h, &c.cs0, pp.cs0.size()));

@@ -213,7 +213,8 @@ struct BendArgs {
     const int *v2e_off, *v2e;        // vertex -> element incidence of the shared mesh
     const int4 *visit;               // [E][3]: (k1, k2, k3, k4) local ids per edge-neighbour visit, k1 < 0: none
     const double2 *cs0;              // [ncell][E][3] spontaneous angle (cos, sin) per visit; nullptr: (1, 0)
-    int E;
+    int E, ncell;
+    double *rec;                     // [ncell][E][3][3][3] scratch: each visit's forces on k1, k2, k3
     double LX, LZ;
     double coef;                     // (2 / sqrt 3) BR
     float *Fv;
