@@ -92,6 +92,7 @@ struct rbc_handle {
     // volume fraction scratch (vof_k > 0): THINC sweep buffers, indicator gradient / CG vectors,
     // right-hand side, CG block partials
     double *vof_s1 = nullptr, *vof_s2 = nullptr, *vof_G = nullptr, *vof_b = nullptr, *vof_partial = nullptr;
+    MgHierarchy vof_mg;                               // multigrid levels of the front-tracking solve
     float *d_drive = nullptr;                          // [3]: drive P * factor, then the walls' z velocities
     // host<->reference staging
     void *staging = nullptr;
@@ -607,6 +608,7 @@ void free_all(rbc_handle *h)
                     h->d_int, h->d_drive, h->staging, h->vof_s1, h->vof_s2, h->vof_G, h->vof_b, h->vof_partial};
     for (void *q : ptrs) if (q) cudaFree(q);
     for (CellGroup &c : h->cg) free_group(c);
+    vof_mg_free(h->vof_mg);
     adjoint_free(h->adj);
     h->adj = nullptr;
     if (h->stream) cudaStreamDestroy(h->stream);
@@ -790,7 +792,7 @@ int launch_front_tracking_stage(rbc_handle *h)
         if (!g.vf || g.ncell == 0) continue;
         FrontArgs a{};
         a.X = g.X; a.nv = g.nv; a.tri = g.tri; a.V = g.V; a.E = g.E; a.ncell = g.ncell; a.mask2d = h->mask2d;
-        a.G = h->vof_G; a.b = h->vof_b; a.vf = g.vf; a.partial = h->vof_partial;
+        a.G = h->vof_G; a.b = h->vof_b; a.vf = g.vf; a.partial = h->vof_partial; a.mg = &h->vof_mg;
         a.tol = h->p.vof_residual; a.itrmax = h->p.vof_itrmax; a.iters = h->d_vofit() + k; a.flags = h->d_flags();
         CK(launch_front_tracking(h->geo, a, h->stream));
         h->launches += 3;
@@ -811,6 +813,9 @@ int vof_init_group(rbc_handle *h, CellGroup &g)
         CK(cudaMalloc(&h->vof_G, 8 * 3 * n));
         CK(cudaMalloc(&h->vof_b, 8 * n));
         CK(cudaMalloc(&h->vof_partial, 8 * 4 * (size_t)std::max(vof_cg_blocks(), 1)));
+        std::vector<uint32_t> mask((size_t)h->geo.plane);
+        CK(cudaMemcpy(mask.data(), h->mask2d, 4 * mask.size(), cudaMemcpyDeviceToHost));
+        CK(vof_mg_build(h->geo, mask.data(), h->vof_mg));
     }
     if (!g.vf) {
         CK(cudaMalloc(&g.vf, 8 * n));
@@ -819,7 +824,7 @@ int vof_init_group(rbc_handle *h, CellGroup &g)
     if (g.ncell == 0) return RBC_OK;
     FrontArgs a{};
     a.X = g.X; a.nv = g.nv; a.tri = g.tri; a.V = g.V; a.E = g.E; a.ncell = g.ncell; a.mask2d = h->mask2d;
-    a.G = h->vof_G; a.b = h->vof_b; a.vf = g.vf; a.partial = h->vof_partial;
+    a.G = h->vof_G; a.b = h->vof_b; a.vf = g.vf; a.partial = h->vof_partial; a.mg = &h->vof_mg;
     a.tol = h->p.vof_residual; a.itrmax = h->p.vof_itrmax; a.iters = h->d_vofit() + (&g == &h->cg[1] ? 1 : 0);
     a.flags = h->d_flags();
     CK(launch_front_tracking(h->geo, a, h->stream));

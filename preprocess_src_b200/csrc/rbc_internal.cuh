@@ -124,6 +124,30 @@ void launch_fill_f4(float4 *p, long long n, float4 v, cudaStream_t s);
 // Volume fraction (vof.cu).  THINC/WLIC: three sweeps vf -> s1 -> s2 -> vf.
 void launch_thinc_wlic(const Geom &g, double *vf, double *s1, double *s2, const float4 *uvr, const uint32_t *mask2d,
                        double dt, cudaStream_t s);
+// Multigrid preconditioner of the front-tracking solve: levels of the
+// Jacobi-scaled Poisson operator on the internal lattice, each the Galerkin
+// product with piecewise-constant aggregation of 2 x 2 x 2 nodes (fewer along
+// an axis that is too short or periodic with odd length).  Coefficients per
+// level column [7][nx * ny]: diagonal, x-, x+, y-, y+, z (the z coupling to
+// both neighbours), inverse diagonal; a column with diagonal 0 is a wall column.
+constexpr int MG_MAX_LEVELS = 12;
+struct MgLevel {
+    int nx, ny, nz;          // dimensions
+    int bx, by, bz;          // aggregation factors to the next level
+    int xper;
+    long long n;
+    const double *coef;
+    double *b, *x, *y;       // right-hand side, pre-smoothed iterate, V-cycle result
+};
+struct MgHierarchy {
+    int nlev = 0;
+    MgLevel lev[MG_MAX_LEVELS];
+    void *mem = nullptr;     // one device allocation holding every level's coefficients and vectors
+};
+// mask2d_host: the handle's column mask; level 0's b and y are the CG's r and z
+cudaError_t vof_mg_build(const Geom &g, const uint32_t *mask2d_host, MgHierarchy &mg);
+void vof_mg_free(MgHierarchy &mg);
+
 // Front tracking of one cell population into vf (warm start from vf).
 struct FrontArgs {
     const double *X; long long nv;
@@ -133,12 +157,15 @@ struct FrontArgs {
     double *b;                 // [nint] scratch: right-hand side
     double *vf;                // [nint] solution
     double *partial;           // [4 * vof_cg_blocks()] scratch
+    const MgHierarchy *mg;     // preconditioner levels (nlev >= 2), or nullptr / nlev < 2 for plain CG
     double tol; int itrmax;
     int *iters;                // device: sweeps of the solve, -1 = not converged
     int *flags;
 };
 cudaError_t launch_front_tracking(const Geom &g, const FrontArgs &a, cudaStream_t s);
 int vof_cg_blocks();
+
+
 
 // Surface patches (spread and advection work units) hold at most this many vertices.
 constexpr int MAX_PATCH_VERTICES = 512;

@@ -40,6 +40,8 @@
 
 #include <cooperative_groups.h>
 
+#include <vector>
+
 namespace cg = cooperative_groups;
 
 namespace rbc {
@@ -451,13 +453,216 @@ indicator_cg_kernel(const CgArgs a)
     }
 }
 
-int g_cg_blocks = 0;   // co-resident blocks of the CG kernel on this device
+// ---- multigrid-preconditioned CG ------------------------------------------
+
+// (A_l v)_i at node i = (x, y, z) of level L (0 on wall columns); v(j, c, x, y, z)
+// gives the vector's value at node j = (x, y, z) of column c
+template <typename Val>
+__device__ __forceinline__ double apply_level_fn(const MgLevel &L, int x, int y, int z, Val v)
+{
+    const unsigned ncol = (unsigned)(L.nx * L.ny), col = (unsigned)(y * L.nx + x);
+    const double *c = L.coef;
+    const double d = c[col];
+    if (d == 0.0) return 0.0;
+    const unsigned zo = (unsigned)z * ncol;
+    double s = d * v(zo + col, col, x, y, z);
+    const double cxm = c[ncol + col], cxp = c[2 * ncol + col], cym = c[3 * ncol + col], cyp = c[4 * ncol + col];
+    const double cz = c[5 * ncol + col];
+    if (cxm != 0.0) {
+        const int xl = x > 0 ? x - 1 : L.nx - 1;
+        const unsigned cl = (unsigned)(y * L.nx + xl);
+        s += cxm * v(zo + cl, cl, xl, y, z);
+    }
+    if (cxp != 0.0) {
+        const int xr = x < L.nx - 1 ? x + 1 : 0;
+        const unsigned cr = (unsigned)(y * L.nx + xr);
+        s += cxp * v(zo + cr, cr, xr, y, z);
+    }
+    if (cym != 0.0) s += cym * v(zo + col - (unsigned)L.nx, col - (unsigned)L.nx, x, y - 1, z);
+    if (cyp != 0.0) s += cyp * v(zo + col + (unsigned)L.nx, col + (unsigned)L.nx, x, y + 1, z);
+    if (cz != 0.0) {
+        const int zm = z == 0 ? L.nz - 1 : z - 1, zp = z == L.nz - 1 ? 0 : z + 1;
+        s += cz * (v((unsigned)zm * ncol + col, col, x, y, zm) + v((unsigned)zp * ncol + col, col, x, y, zp));
+    }
+    return s;
+}
+
+__device__ __forceinline__ double apply_level(const MgLevel &L, const double *v, unsigned, int x, int y, int z)
+{
+    return apply_level_fn(L, x, y, z, [v](unsigned j, unsigned, int, int, int) { return v[j]; });
+}
+
+struct PcgArgs {
+    MgHierarchy mg;           // level 0: b = r, y = z
+    const double *b;          // right-hand side of the scaled system
+    double *x, *r, *p, *q;
+    double *partial;
+    double tol;
+    int itrmax;
+    int *iters_out;
+    int *flags;
+};
+
+constexpr double MG_OMEGA = 0.8;   // damped-Jacobi smoothing weight
+constexpr int MG_COARSE_SWEEPS = 40;
+
+// z = M r: one symmetric V-cycle (one damped-Jacobi sweep from 0 before and
+// one after the coarse correction, the coarsest level by Jacobi sweeps in
+// block 0), so M is symmetric positive definite and CG stays CG.  The
+// pre-smoothed iterate x = w D^-1 b is never stored: the restriction of its
+// residual and the post-smoothing (with x = w D^-1 b + P y_coarse) evaluate
+// it at the stencil's nodes, so each level costs one pass and one barrier on
+// the way down and one on the way up.
+__device__ void vcycle(cg::grid_group &grid, const PcgArgs &a, unsigned first, unsigned stride)
+{
+    const int L = a.mg.nlev;
+    for (int l = 0; l < L - 1; l++) {
+        const MgLevel &F = a.mg.lev[l], &C = a.mg.lev[l + 1];
+        const unsigned ncf = (unsigned)(F.nx * F.ny);
+        const double *fb = F.b, *fc = F.coef;
+        auto xpre = [fb, fc, ncf](unsigned j, unsigned c, int, int, int) { return MG_OMEGA * fb[j] * fc[6 * ncf + c]; };
+        const unsigned nc = (unsigned)C.n, ncc = (unsigned)(C.nx * C.ny);
+        for (unsigned I = first; I < nc; I += stride) {
+            const unsigned Z = I / ncc, rc = I - Z * ncc, Y = rc / (unsigned)C.nx, X = rc - Y * (unsigned)C.nx;
+            double s = 0.0;
+            for (int dz = 0; dz < F.bz; dz++)
+                for (int dy = 0; dy < F.by; dy++)
+                    for (int dx = 0; dx < F.bx; dx++) {
+                        const int x = (int)X * F.bx + dx, y = (int)Y * F.by + dy, z = (int)Z * F.bz + dz;
+                        if (x >= F.nx || y >= F.ny) continue;
+                        const unsigned col = (unsigned)(y * F.nx + x), i = (unsigned)z * ncf + col;
+                        if (fc[col] == 0.0) continue;
+                        s += fb[i] - apply_level_fn(F, x, y, z, xpre);
+                    }
+            C.b[I] = s;
+        }
+        grid.sync();
+    }
+    {   // coarsest level: Jacobi sweeps from 0 in block 0 (x and y alternate)
+        const MgLevel &C = a.mg.lev[L - 1];
+        if (blockIdx.x == 0) {
+            const unsigned nc = (unsigned)C.n, ncc = (unsigned)(C.nx * C.ny);
+            for (unsigned i = threadIdx.x; i < nc; i += blockDim.x) C.y[i] = 0.0;
+            __syncthreads();
+            double *src = C.y, *dst = C.x;
+            for (int sw = 0; sw < MG_COARSE_SWEEPS; sw++) {
+                for (unsigned i = threadIdx.x; i < nc; i += blockDim.x) {
+                    const unsigned Z = i / ncc, rc = i - Z * ncc, Y = rc / (unsigned)C.nx, X = rc - Y * (unsigned)C.nx;
+                    const double id = C.coef[6 * ncc + rc];
+                    dst[i] = id != 0.0 ? src[i] + MG_OMEGA * (C.b[i] - apply_level(C, src, i, (int)X, (int)Y, (int)Z)) * id : 0.0;
+                }
+                __syncthreads();
+                double *t = src; src = dst; dst = t;
+            }
+            if (src != C.y)
+                for (unsigned i = threadIdx.x; i < nc; i += blockDim.x) C.y[i] = src[i];
+        }
+        grid.sync();
+    }
+    for (int l = L - 2; l >= 0; l--) {
+        const MgLevel &F = a.mg.lev[l], &C = a.mg.lev[l + 1];
+        const unsigned nf = (unsigned)F.n, ncf = (unsigned)(F.nx * F.ny), ncc = (unsigned)(C.nx * C.ny);
+        const double *fb = F.b, *fc = F.coef, *cy = C.y;
+        const int sx = F.bx >> 1, sy = F.by >> 1, sz = F.bz >> 1, cnx = C.nx;   // aggregation factors are 1 or 2
+        // x = w D^-1 b + P y_coarse at any node of the level
+        auto xcor = [fb, fc, cy, ncf, ncc, sx, sy, sz, cnx](unsigned j, unsigned c, int x, int y, int z) {
+            const double id = fc[6 * ncf + c];
+            if (id == 0.0) return 0.0;
+            return MG_OMEGA * fb[j] * id + cy[(unsigned)(z >> sz) * ncc + (unsigned)((y >> sy) * cnx + (x >> sx))];
+        };
+        for (unsigned i = first; i < nf; i += stride) {
+            const unsigned z = i / ncf, rc = i - z * ncf, y = rc / (unsigned)F.nx, x = rc - y * (unsigned)F.nx;
+            const double id = fc[6 * ncf + rc];
+            F.y[i] = id != 0.0 ? xcor(i, rc, (int)x, (int)y, (int)z)
+                                     + MG_OMEGA * (fb[i] - apply_level_fn(F, (int)x, (int)y, (int)z, xcor)) * id
+                               : 0.0;
+        }
+        grid.sync();
+    }
+}
+
+constexpr int PCG_BLOCKS_PER_SM = 3;
+
+__global__ void __launch_bounds__(CG_THREADS, PCG_BLOCKS_PER_SM)
+indicator_pcg_kernel(const PcgArgs a)
+{
+    cg::grid_group grid = cg::this_grid();
+    const MgLevel &L0 = a.mg.lev[0];
+    const unsigned n = (unsigned)L0.n, ncol = (unsigned)(L0.nx * L0.ny);
+    const unsigned stride = gridDim.x * blockDim.x, first = blockIdx.x * blockDim.x + threadIdx.x;
+    double lr = 0.0, lb = 0.0;
+    for (unsigned i = first; i < n; i += stride) {
+        const unsigned z = i / ncol, rc = i - z * ncol, y = rc / (unsigned)L0.nx, x = rc - y * (unsigned)L0.nx;
+        if (L0.coef[rc] == 0.0) { a.x[i] = 0.0; a.r[i] = 0.0; a.p[i] = 0.0; continue; }
+        const double ri = a.b[i] - apply_level(L0, a.x, i, (int)x, (int)y, (int)z);
+        a.r[i] = ri;
+        lr += ri * ri;
+        lb += a.b[i] * a.b[i];
+    }
+    double rr, bb;
+    int bank = 0;
+    grid_sum2(grid, a.partial, bank, lr, lb, rr, bb);
+    bank ^= 1;
+    int it = 0;
+    if (bb > 0.0 && !(sqrt(rr / bb) < a.tol)) {
+        vcycle(grid, a, first, stride);   // z = M r (level 0's y)
+        double lrz = 0.0;
+        for (unsigned i = first; i < n; i += stride) { a.p[i] = L0.y[i]; lrz += a.r[i] * L0.y[i]; }
+        double rz, unused;
+        grid_sum2(grid, a.partial, bank, lrz, 0.0, rz, unused);
+        bank ^= 1;
+        while (it < a.itrmax) {
+            double lpq = 0.0;
+            for (unsigned i = first; i < n; i += stride) {
+                const unsigned z = i / ncol, rc = i - z * ncol, y = rc / (unsigned)L0.nx, x = rc - y * (unsigned)L0.nx;
+                const double qi = apply_level(L0, a.p, i, (int)x, (int)y, (int)z);
+                a.q[i] = qi;
+                lpq += a.p[i] * qi;
+            }
+            double pq;
+            grid_sum2(grid, a.partial, bank, lpq, 0.0, pq, unused);
+            bank ^= 1;
+            const double alpha = rz / pq;
+            double lrr = 0.0;
+            for (unsigned i = first; i < n; i += stride) {
+                const double ri = a.r[i] - alpha * a.q[i];
+                a.x[i] += alpha * a.p[i];
+                a.r[i] = ri;
+                lrr += ri * ri;
+            }
+            grid_sum2(grid, a.partial, bank, lrr, 0.0, rr, unused);
+            bank ^= 1;
+            it++;
+            if (sqrt(rr / bb) < a.tol) break;
+            vcycle(grid, a, first, stride);
+            double lrz2 = 0.0;
+            for (unsigned i = first; i < n; i += stride) lrz2 += a.r[i] * L0.y[i];
+            double rz_new;
+            grid_sum2(grid, a.partial, bank, lrz2, 0.0, rz_new, unused);
+            bank ^= 1;
+            const double beta = rz_new / rz;
+            rz = rz_new;
+            for (unsigned i = first; i < n; i += stride) a.p[i] = L0.y[i] + beta * a.p[i];
+            grid.sync();
+        }
+    }
+    if (bb == 0.0)
+        for (unsigned i = first; i < n; i += stride) a.x[i] = 0.0;
+    if (first == 0) {
+        const bool ok = bb == 0.0 || sqrt(rr / bb) < a.tol;
+        *a.iters_out = ok ? it : -1;
+        if (!ok) atomicOr(a.flags, RBC_FLAG_VOF_NOT_CONVERGED);
+    }
+}
+
+int g_cg_blocks = 0;    // co-resident blocks of the CG kernel on this device
+int g_pcg_blocks = 0;   // and of the preconditioned one
 
 }  // namespace
 
 int vof_cg_blocks()
 {
-    return g_cg_blocks;
+    return g_cg_blocks > g_pcg_blocks ? g_cg_blocks : g_pcg_blocks;
 }
 
 cudaError_t vof_setup()
@@ -466,7 +671,10 @@ cudaError_t vof_setup()
     cudaError_t e = cudaGetDevice(&dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, indicator_cg_kernel, CG_THREADS, 0);
+    int per_sm2 = 0;
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, indicator_pcg_kernel, CG_THREADS, 0);
     if (e == cudaSuccess) g_cg_blocks = sms * (per_sm < CG_BLOCKS_PER_SM ? per_sm : CG_BLOCKS_PER_SM);
+    if (e == cudaSuccess) g_pcg_blocks = sms * (per_sm2 < PCG_BLOCKS_PER_SM ? per_sm2 : PCG_BLOCKS_PER_SM);
     return e;
 }
 
@@ -477,6 +685,98 @@ void launch_thinc_wlic(const Geom &g, double *vf, double *s1, double *s2, const 
     thinc_sweep_kernel<0><<<tiles, VOF_THREADS, 0, s>>>(g, vf, s1, uvr, mask2d, dt);
     thinc_sweep_kernel<1><<<tiles, VOF_THREADS, 0, s>>>(g, s1, s2, uvr, mask2d, dt);
     thinc_sweep_kernel<2><<<tiles, VOF_THREADS, 0, s>>>(g, s2, vf, uvr, mask2d, dt);
+}
+
+cudaError_t vof_mg_build(const Geom &g, const uint32_t *mask, MgHierarchy &mg)
+{
+    mg = MgHierarchy{};
+    struct HostLevel { int nx, ny, nz, bx = 1, by = 1, bz = 1; std::vector<double> coef; };
+    std::vector<HostLevel> lv(1);
+    HostLevel &l0 = lv[0];
+    l0.nx = g.nx; l0.ny = g.ny; l0.nz = g.nzc;
+    const int nc0 = g.nx * g.ny;
+    l0.coef.assign(7 * (size_t)nc0, 0.0);
+    const double off = (1.0 / (g.dx * g.dx)) / (-6.0 / (g.dx * g.dx));
+    auto fl = [&](int x, int y) { return (mask[(size_t)y * g.nx + x] & MASK_FLUID) != 0; };
+    for (int y = 0; y < g.ny; y++)
+        for (int x = 0; x < g.nx; x++) {
+            if (!fl(x, y)) continue;
+            const int c = y * g.nx + x;
+            l0.coef[c] = 1.0;
+            const int xl = x > 0 ? x - 1 : (g.xper ? g.nx - 1 : -1), xr = x < g.nx - 1 ? x + 1 : (g.xper ? 0 : -1);
+            if (xl >= 0 && fl(xl, y)) l0.coef[nc0 + c] = off;
+            if (xr >= 0 && fl(xr, y)) l0.coef[2 * nc0 + c] = off;
+            if (y > 0 && fl(x, y - 1)) l0.coef[3 * nc0 + c] = off;
+            if (y < g.ny - 1 && fl(x, y + 1)) l0.coef[4 * nc0 + c] = off;
+            l0.coef[5 * nc0 + c] = off;
+        }
+    // Galerkin coarsening with piecewise-constant aggregation
+    while ((int)lv.size() < MG_MAX_LEVELS) {
+        HostLevel &f = lv.back();
+        if ((long long)f.nx * f.ny * f.nz <= 512) break;
+        const int bx = (f.nx >= 4 && !(g.xper && f.nx % 2)) ? 2 : 1, by = f.ny >= 4 ? 2 : 1;
+        const int bz = (f.nz >= 4 && f.nz % 2 == 0) ? 2 : 1;
+        if (bx * by * bz == 1) break;
+        f.bx = bx; f.by = by; f.bz = bz;
+        HostLevel c;
+        c.nx = (f.nx + bx - 1) / bx; c.ny = (f.ny + by - 1) / by; c.nz = f.nz / bz;
+        const int ncf = f.nx * f.ny, ncc = c.nx * c.ny;
+        c.coef.assign(7 * (size_t)ncc, 0.0);
+        for (int y = 0; y < f.ny; y++)
+            for (int x = 0; x < f.nx; x++) {
+                const int col = y * f.nx + x;
+                const double d = f.coef[col];
+                if (d == 0.0) continue;
+                const int X = x / bx, Y = y / by, C = Y * c.nx + X;
+                const double cxm = f.coef[ncf + col], cxp = f.coef[2 * ncf + col];
+                const double cym = f.coef[3 * ncf + col], cyp = f.coef[4 * ncf + col], cz = f.coef[5 * ncf + col];
+                c.coef[C] += bz * d + (bz == 2 ? 2.0 * cz : 0.0);   // the z link inside the block, both ways
+                const int xl = x > 0 ? x - 1 : f.nx - 1, xr = x < f.nx - 1 ? x + 1 : 0;
+                if (cxm != 0.0) { if (xl / bx == X) c.coef[C] += bz * cxm; else c.coef[ncc + C] += bz * cxm; }
+                if (cxp != 0.0) { if (xr / bx == X) c.coef[C] += bz * cxp; else c.coef[2 * ncc + C] += bz * cxp; }
+                if (cym != 0.0) { if ((y - 1) / by == Y) c.coef[C] += bz * cym; else c.coef[3 * ncc + C] += bz * cym; }
+                if (cyp != 0.0) { if ((y + 1) / by == Y) c.coef[C] += bz * cyp; else c.coef[4 * ncc + C] += bz * cyp; }
+                c.coef[5 * ncc + C] += cz;   // one link per fine column crosses each block boundary in z
+            }
+        lv.push_back(std::move(c));
+    }
+    const int L = (int)lv.size();
+    if (L < 2) return cudaSuccess;
+    for (HostLevel &h : lv) {   // row 6: the inverse diagonal (0 on wall columns)
+        const size_t nc = (size_t)h.nx * h.ny;
+        for (size_t c = 0; c < nc; c++) h.coef[6 * nc + c] = h.coef[c] != 0.0 ? 1.0 / h.coef[c] : 0.0;
+    }
+    // one allocation: every level's coefficients, level 0's x and y, the coarse levels' b, x, y
+    size_t words = 0;
+    for (int l = 0; l < L; l++) {
+        const long long n = (long long)lv[l].nx * lv[l].ny * lv[l].nz;
+        words += lv[l].coef.size() + (size_t)n * (l == 0 ? 2 : 3);
+    }
+    double *mem = nullptr;
+    cudaError_t e = cudaMalloc(&mem, 8 * words);
+    if (e != cudaSuccess) return e;
+    mg.mem = mem;
+    double *cur = mem;
+    for (int l = 0; l < L; l++) {
+        MgLevel &d = mg.lev[l];
+        const HostLevel &h = lv[l];
+        d.nx = h.nx; d.ny = h.ny; d.nz = h.nz; d.bx = h.bx; d.by = h.by; d.bz = h.bz; d.xper = g.xper;
+        d.n = (long long)h.nx * h.ny * h.nz;
+        if ((e = cudaMemcpy(cur, h.coef.data(), 8 * h.coef.size(), cudaMemcpyHostToDevice)) != cudaSuccess) return e;
+        d.coef = cur; cur += h.coef.size();
+        d.b = nullptr;
+        if (l > 0) { d.b = cur; cur += d.n; }
+        d.x = cur; cur += d.n;
+        d.y = cur; cur += d.n;
+    }
+    mg.nlev = L;
+    return cudaSuccess;
+}
+
+void vof_mg_free(MgHierarchy &mg)
+{
+    if (mg.mem) cudaFree(mg.mem);
+    mg = MgHierarchy{};
 }
 
 cudaError_t launch_front_tracking(const Geom &g, const FrontArgs &a, cudaStream_t s)
@@ -490,6 +790,16 @@ cudaError_t launch_front_tracking(const Geom &g, const FrontArgs &a, cudaStream_
     const unsigned blocks = (unsigned)((g.nint + VOF_THREADS - 1) / VOF_THREADS);
     indicator_rhs_kernel<<<blocks, VOF_THREADS, 0, s>>>(g, a.G, a.mask2d, a.b);
     // the gradient is consumed: its storage holds the CG vectors r, p, q
+    if (a.mg && a.mg->nlev >= 2) {
+        PcgArgs c{};
+        c.mg = *a.mg;
+        c.mg.lev[0].b = a.G;   // the residual r is level 0's right-hand side
+        c.b = a.b; c.x = a.vf; c.r = a.G; c.p = a.G + g.nint; c.q = a.G + 2 * g.nint;
+        c.partial = a.partial; c.tol = a.tol; c.itrmax = a.itrmax; c.iters_out = a.iters; c.flags = a.flags;
+        void *args[] = {&c};
+        return cudaLaunchCooperativeKernel((const void *)indicator_pcg_kernel, dim3((unsigned)g_pcg_blocks),
+                                           dim3(CG_THREADS), args, 0, s);
+    }
     CgArgs c{};
     c.g = g; c.mask2d = a.mask2d; c.b = a.b; c.x = a.vf;
     c.r = a.G; c.p = a.G + g.nint; c.q = a.G + 2 * g.nint;
