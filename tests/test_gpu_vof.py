@@ -183,3 +183,13 @@ def test_vof_with_fp16_storage(native_lib):
             assert sim.status()[0] & 3 == 0
     assert np.abs(out[1][0] - out[0][0]).max() <= 1e-4
     assert rel_l2(out[1][1], out[0][1]) <= 5e-3
+
+
+def test_vof_handles_refuse_the_adjoint_and_batches(native_lib):
+    from preprocess_src_b200 import _native as N
+    from preprocess_src_b200.step import Batch, Simulation
+    with Simulation(vof_case()) as sim:
+        with pytest.raises(N.RbcError):
+            sim.adjoint_record(2, 1)
+        with pytest.raises(N.RbcError):
+            Batch([sim])

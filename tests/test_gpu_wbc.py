@@ -198,3 +198,25 @@ def test_add_wbc_argument_checks(native_lib):
             s.add_wbc(white)
         s.step(2)
         assert s.status()[0] & 3 == 0
+
+
+def test_white_cells_in_a_batch_and_out_of_the_adjoint(native_lib):
+    """A simulation with white cells steps in a batch as it does alone; the
+    adjoint refuses it (one population only)."""
+    from preprocess_src_b200 import _native as N
+    from preprocess_src_b200.step import Batch, Simulation
+    case = parity_case()
+    red, white = configs.split_cells(case, 1)
+    with Simulation(red) as a, Simulation(red) as b:
+        for s in (a, b):
+            s.add_wbc(white, rgs=2.0)
+        batch = Batch([a])
+        batch.step(3)
+        b.step(3)
+        batch.synchronize()
+        for ea, eb in ((a.export_cells(), b.export_cells()), (a.export_wbc(), b.export_wbc())):
+            for k in ("x", "y", "z"):
+                np.testing.assert_allclose(ea[k], eb[k], rtol=0, atol=1e-12, err_msg=k)
+        batch.close()
+        with pytest.raises(N.RbcError):
+            a.adjoint_record(2, 1)
