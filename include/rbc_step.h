@@ -245,7 +245,11 @@ int rbc_step(rbc_handle *h, int nsteps);
  * by the call); vc_iters_max: largest volume-correction return value seen. */
 int rbc_get_status(rbc_handle *h, int *flags, int *vc_iters_max);
 /* Synchronous.  FP64 per-cell volume, area and vertex centroid ([ncell],
- * [ncell], [3*ncell]); any pointer may be NULL. */
+ * [ncell], [3*ncell]); any pointer may be NULL.  Right after rbc_step (or a
+ * batch step) these are the values the step's volume correction computed for
+ * the final positions (cel->volume, cel->area, cel->gx), read back without a
+ * kernel; after any other call that may change the state a kernel measures
+ * them. */
 int rbc_cell_metrics(rbc_handle *h, double *volume, double *area, double *centroid);
 int rbc_synchronize(rbc_handle *h);
 /* Number of kernel launches issued by this library since creation. */
