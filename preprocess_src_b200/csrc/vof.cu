@@ -195,8 +195,11 @@ thinc_sweep_kernel(const Geom g, const double *__restrict__ vin, double *__restr
     const double inv32dx = 1.0 / (32.0 * g.dx);
     for (int k = threadIdx.x; k < R::nx * R::ny * R::nz; k += blockDim.x) {
         const int rx = k % R::nx, ry = (k / R::nx) % R::ny, rz = k / (R::nx * R::ny);
-        double n[3];
-        staged_normal(sv, rx - R::ox + HALO, ry - R::oy + HALO, rz - R::oz + HALO, inv32dx, n);
+        const int sx = rx - R::ox + HALO, sy = ry - R::oy + HALO, sz = rz - R::oz + HALO;
+        const double v = sv[sz][sy][sx];
+        double n[3] = {0.0, 0.0, 0.0};
+        // a full or empty node's flux is plain upwind: its normal is never read
+        if (v > 1.0e-6 && v < 1.0 - 1.0e-6) staged_normal(sv, sx, sy, sz, inv32dx, n);
         sn[0][k] = n[0];
         sn[1][k] = n[1];
         sn[2][k] = n[2];
