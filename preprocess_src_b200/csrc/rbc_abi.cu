@@ -24,7 +24,6 @@ namespace {
 
 thread_local std::string g_create_error;
 
-constexpr float F16_SCALE = 32768.0f;     // (f - w) * 2^15 keeps |g| < 2 inside FP16 range
 constexpr int DEFAULT_SOLVER_ITERS = 16;  // Chebyshev error factor <= 2 * 3^-16 ~ 4.6e-8 (FP32 solve)
 
 }  // namespace

@@ -28,6 +28,7 @@
 namespace rbc {
 
 constexpr int Q = 19;
+constexpr float F16_SCALE = 32768.0f;   // FP16 storage (f - w) * 2^15 keeps |g| < 2 inside FP16 range
 constexpr uint32_t MASK_FLUID = 0x80000000u;
 // shear mode (x periodic, moving y walls): column flags beside the link bits 1..18
 constexpr uint32_t MASK_XLO = 1u << 20;    // first column: x - 1 is the last column (periodic)
