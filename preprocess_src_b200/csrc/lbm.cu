@@ -205,12 +205,17 @@ lbm_collide_stream(const typename Store<STORE>::T *__restrict__ gin, typename St
 // z planes per thread: the per-thread setup (mask, warp votes, drive) is paid
 // once for that many nodes.  Dense suspension (256 planes of 128 x 128):
 // FP32 0.1352 / 0.1312 / 0.1337 ms and FP16 0.1292 / 0.1209 / 0.1182 ms at
-// 1 / 2 / 4 planes per thread.
+// 1 / 2 / 4 planes per thread.  A lattice that would leave fewer than
+// LBM_MIN_THREADS threads (~3.5 waves of 148 SMs x 1024 resident threads) keeps
+// fewer planes per thread: the single-cell duct (57,600 nodes) takes 0.0086 ms
+// at one plane per thread and 0.0098 ms at two.
 constexpr int LBM_PLANES_F32 = 2, LBM_PLANES_F16 = 4;
+constexpr long long LBM_MIN_THREADS = 1LL << 19;
 
 void launch_lbm(const Geom &g, int storage, const LbmArgs &a, cudaStream_t s)
 {
-    const int zpt = (storage == RBC_STORE_F16) ? LBM_PLANES_F16 : LBM_PLANES_F32;
+    int zpt = (storage == RBC_STORE_F16) ? LBM_PLANES_F16 : LBM_PLANES_F32;
+    while (zpt > 1 && (long long)g.plane * g.nzc / zpt < LBM_MIN_THREADS) zpt >>= 1;
     const int gz = (g.nzc + zpt - 1) / zpt;
     const dim3 blocks((unsigned)((g.plane + LBM_THREADS - 1) / LBM_THREADS), (unsigned)(gz < 65535 ? gz : 65535));
     const bool off32 = (long long)Q * g.nint < (1LL << 31);   // every element offset fits in an int
