@@ -251,6 +251,14 @@ int rbc_get_status(rbc_handle *h, int *flags, int *vc_iters_max);
  * kernel; after any other call that may change the state a kernel measures
  * them. */
 int rbc_cell_metrics(rbc_handle *h, double *volume, double *area, double *centroid);
+/* Asynchronous form of rbc_cell_metrics for a caller that consumes each
+ * step's metrics while the next steps run: enqueues on the handle's stream
+ * the device-to-host copies of the same values into out (5 * ncell doubles:
+ * volume[ncell], area[ncell], then the centroid as x[ncell], y[ncell],
+ * z[ncell]) and returns without waiting.  out must stay valid until the
+ * copies complete (rbc_synchronize, or an event recorded on the handle's
+ * stream after this call); page-locked memory keeps the call asynchronous. */
+int rbc_cell_metrics_async(rbc_handle *h, double *out);
 int rbc_synchronize(rbc_handle *h);
 /* Number of kernel launches issued by this library since creation. */
 int rbc_launch_count(const rbc_handle *h, long long *count);

@@ -67,6 +67,7 @@ _SIGS = {
     "rbc_step": [_H, C.c_int],
     "rbc_get_status": [_H, _IP, _IP],
     "rbc_cell_metrics": [_H, _DP, _DP, _DP],
+    "rbc_cell_metrics_async": [_H, _DP],
     "rbc_synchronize": [_H],
     "rbc_launch_count": [_H, C.POINTER(C.c_longlong)],
     "rbc_dims": [_H, _IP, _IP, _IP, _IP, _IP, _IP],

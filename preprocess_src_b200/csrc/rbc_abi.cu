@@ -1728,6 +1728,26 @@ int rbc_cell_metrics(rbc_handle *h, double *volume, double *area, double *centro
     return group_metrics(h, h->cg[0], volume, area, centroid);
 }
 
+int rbc_cell_metrics_async(rbc_handle *h, double *out)
+{
+    if (!h || !out) return RBC_ERR_ARG;
+    RBC_DEVICE_GUARD_RO(h);
+    CellGroup &g = h->cg[0];
+    if (h->ncell == 0) return fail(h, RBC_ERR_STATE, "handle has no cells");
+    const int N = g.ncell;
+    const double *cen = g.gx;
+    if (!h->metrics_valid) {   // as group_metrics: measure the current positions
+        launch_volume(h->geo, volume_args(h, g, 0), h->stream);
+        h->launches++;
+        CK_LAUNCH();
+        cen = g.cen_out;
+    }
+    CK(cudaMemcpyAsync(out, g.vol_out, 8 * (size_t)N, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(out + N, g.area_out, 8 * (size_t)N, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(out + 2 * N, cen, 8 * 3 * (size_t)N, cudaMemcpyDeviceToHost, h->stream));
+    return RBC_OK;
+}
+
 int rbc_synchronize(rbc_handle *h)
 {
     if (!h) return RBC_ERR_ARG;

@@ -278,6 +278,12 @@ class Simulation:
         self._call("rbc_cell_metrics", _dp(out["volume"]), _dp(out["area"]), _dp(out["centroid"]))
         return out
 
+    def cell_metrics_async(self, out: np.ndarray) -> None:
+        """Enqueue the copies of the metrics into out (5 * ncell float64:
+        volume, area, centroid x, y, z); valid after synchronize()."""
+        assert out.dtype == np.float64 and out.size >= 5 * self.case.ncell and out.flags["C_CONTIGUOUS"]
+        self._call("rbc_cell_metrics_async", _dp(out))
+
     def profile_steps(self, nsteps: int) -> dict:
         """Run nsteps with a CUDA event around each kernel; returns the summed
         device milliseconds per kernel."""

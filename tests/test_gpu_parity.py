@@ -390,6 +390,24 @@ def test_split_membrane_wave_equals_stage_calls(native_lib):
         assert a.status() == b.status()
 
 
+def test_async_cell_metrics_equal_the_synchronous_ones(developed):
+    """rbc_cell_metrics_async: after the stream synchronises, out holds the
+    values rbc_cell_metrics returns (volume, area, then the centroid by axis),
+    both after a step and after an import (measured by a kernel)."""
+    case, o = developed
+    sim = load(o)
+    nc = case.ncell
+    for stepped in (False, True):
+        if stepped:
+            sim.step(2)
+        out = np.full(5 * nc, np.nan)
+        sim.cell_metrics_async(out)
+        sim.synchronize()
+        ref = sim.cell_metrics()
+        assert np.array_equal(out[:nc], ref["volume"]) and np.array_equal(out[nc:2 * nc], ref["area"])
+        assert np.array_equal(out[2 * nc:].reshape(3, nc).T.reshape(-1), ref["centroid"])
+
+
 def test_cell_metrics_after_a_step_equal_the_measured_ones(developed):
     """After rbc_step the metrics come from the step's volume correction; after
     any call that may change the state the volume kernel measures them."""
