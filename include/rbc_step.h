@@ -84,7 +84,8 @@ extern "C" {
 #define RBC_FLAG_VC_NOT_CONVERGED  0x1
 #define RBC_FLAG_NONFINITE         0x2
 #define RBC_FLAG_SPREAD_OVERFLOW   0x4   /* informational: a cell used the direct-atomic spread path */
-#define RBC_FLAG_SOLVE_RESIDUAL    0x8   /* membrane load solve residual above 1e-3 */
+#define RBC_FLAG_SOLVE_RESIDUAL    0x8   /* membrane load solve: |r| / |b| of the Jacobi-scaled
+                                            system above 1e-3 (|r|^2 > 1e-6 |b|^2) */
 #define RBC_FLAG_VOF_NOT_CONVERGED 0x10  /* a front-tracking solve hit vof_itrmax (the reference's error(5)) */
 
 typedef struct rbc_params {
@@ -382,23 +383,33 @@ int rbc_read_center_file(rbc_handle *h, const char *path);
  * static device array of RBC_NOALLOC_MAX_CELLS cells (160 KB) that every GPU
  * loading the library keeps until exit.
  *   x        device, [3][ncell*vertex] SoA positions (x block, y block, z block)
- *   tri      device, [element*3] local connectivity shared by all cells
- *   LZ, zmin, zmax  periodic length and range of z (cells are unwrapped along z
- *            about their first vertex, centroids wrapped into [zmin, zmax])
- *   device   CUDA device ordinal, or -1 for this library's current device
+ *   tri      device, [element*3] local connectivity shared by all cells; every
+ *            entry must lie in 0..vertex-1 (entries outside are skipped with
+ *            their triangles and the call returns RBC_ERR_ARG)
+ *   LX, xmin, xmax  periodic length and range of x when x is periodic (the
+ *            shear mode, RBC_FLOW_SHEAR); LX <= 0 for the channel and the tube,
+ *            whose x is bounded by walls
+ *   LZ, zmin, zmax  periodic length and range of z
+ *            Cells are unwrapped along each periodic axis about their first
+ *            vertex and their centroids wrapped into [min, max], as the
+ *            handle's volume correction does (cells must span less than half
+ *            of each period).
+ *   device   CUDA device ordinal, or -1 for the calling thread's current device;
+ *            the calling thread's current device is the same after the call
  *   stream   cudaStream_t to run on (NULL = default stream)
- *   volume, area [ncell], centroid [3*ncell]: host outputs
- * Synchronous.  ncell above RBC_NOALLOC_MAX_CELLS or vertex above
- * RBC_NOALLOC_MAX_VERTEX returns RBC_ERR_ARG (text in rbc_last_error(NULL)).
- * The first call on a device looks up the scratch array's device address and
- * sets the kernel's shared-memory limit; make that first call before any CUDA
- * graph capture.  All calls share the scratch array: calls that overlap on the
- * GPU (other streams, other host threads) race and must be serialised. */
+ *   volume, area [ncell], centroid [3*ncell] (x, y, z of each cell): host outputs
+ * Synchronous.  ncell above RBC_NOALLOC_MAX_CELLS, vertex above
+ * RBC_NOALLOC_MAX_VERTEX, LZ <= 0 or NULL pointers return RBC_ERR_ARG (text in
+ * rbc_last_error(NULL)).  The first call on a device looks up the scratch
+ * array's device address and sets the kernel's shared-memory limit; make that
+ * first call before any CUDA graph capture.  All calls share the scratch
+ * array: calls that overlap on the GPU (other streams, other host threads)
+ * race and must be serialised. */
 #define RBC_NOALLOC_MAX_CELLS  4096
 #define RBC_NOALLOC_MAX_VERTEX 4096
 int rbc_cell_metrics_noalloc(const double *x, int ncell, int vertex, int element, const int *tri,
-                             double LZ, double zmin, double zmax, int device, void *stream,
-                             double *volume, double *area, double *centroid);
+                             double LX, double xmin, double xmax, double LZ, double zmin, double zmax,
+                             int device, void *stream, double *volume, double *area, double *centroid);
 
 /* Sizes of the internal lattice and of the cells. */
 int rbc_dims(const rbc_handle *h, int *nx, int *ny, int *nz_periodic, int *ncell, int *vertex, int *element);

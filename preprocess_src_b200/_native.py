@@ -74,7 +74,8 @@ _SIGS = {
     "rbc_get_stream": [_H, C.POINTER(C.c_void_p)],
     "rbc_profile_steps": [_H, C.c_int, _DP],
     "rbc_cell_metrics_noalloc": [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_double, C.c_double,
-                                 C.c_double, C.c_int, C.c_void_p, _DP, _DP, _DP],
+                                 C.c_double, C.c_double, C.c_double, C.c_double, C.c_int, C.c_void_p,
+                                 _DP, _DP, _DP],
     "rbc_batch_create": [C.POINTER(_H), C.c_int, C.POINTER(_H)],
     "rbc_batch_destroy": [_H],
     "rbc_batch_last_error": [_H],

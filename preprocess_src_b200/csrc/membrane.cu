@@ -273,7 +273,8 @@ membrane_kernel(const MembraneArgs a)
         rho = rho_n;
         __syncthreads();
     }
-    // residual of the scaled system, relative to its right-hand side
+    // residual of the scaled system, relative to its right-hand side: the flag
+    // is |r| / |b| > 1e-3, compared as squared norms
     float rr = 0.f;
 #pragma unroll
     for (int m = 0; m < VPT; m++)

@@ -24,10 +24,14 @@ constexpr int kMaxDevices = 64;
 constexpr int kThreads = 1024;
 constexpr int kMaxVertex = RBC_NOALLOC_MAX_VERTEX;
 
-// Scratch of the kernel: volume [N], area [N], centroid [3N] (AoS as cel->gx).
-// Every call overwrites the first 5 * ncell entries; nothing accumulates, so
-// nothing needs clearing.  Calls that overlap on the GPU share this array and race.
-static __device__ __align__(256) double g_metrics_scratch[5 * RBC_NOALLOC_MAX_CELLS];
+// Scratch of the kernel: volume [N], area [N], then the centroids [N][3]
+// (x, y, z of each cell in turn, the layout of rbc_cell_metrics' centroid
+// output).  Every call overwrites the first 5 * ncell entries, so nothing
+// there needs clearing.  The last slot counts triangle entries outside
+// [0, vertex); each call clears it before its kernel.  Calls that overlap on
+// the GPU share this array and race.
+constexpr int kFlagSlot = 5 * RBC_NOALLOC_MAX_CELLS;
+static __device__ __align__(256) double g_metrics_scratch[5 * RBC_NOALLOC_MAX_CELLS + 1];
 
 // In host code g_metrics_scratch names a host-side stand-in, not device
 // memory; the device address is looked up once per device with that device
@@ -48,21 +52,31 @@ __device__ __forceinline__ double block_sum(double v, double *red)
     return s;
 }
 
-// One CTA per cell: positions unwrapped along z about the cell's first vertex,
-// then the volume sum (r . n) dS / 3, the area and the vertex mean of
-// CalcEleNormal_GPU / CalcCenter (volume_correction.cu:138-200, 310-352).
+// One CTA per cell: positions unwrapped about the cell's first vertex along z
+// and, when x is periodic (LX > 0, the shear mode), along x; then the volume
+// sum (r . n) dS / 3, the area and the vertex mean of CalcEleNormal_GPU /
+// CalcCenter (volume_correction.cu:138-200, 310-352), the centroid wrapped
+// into [zmin, zmax] (and [xmin, xmax]) as volume_correction.cu:319-325 does.
+// A triangle entry outside [0, V) is skipped and counted in *bad.
 __global__ void __launch_bounds__(kThreads)
 metrics_noalloc_kernel(const double *__restrict__ X, long long nv, const int *__restrict__ tri, int V, int E,
-                       int ncell, double LZ, double zmin, double zmax, double *__restrict__ out)
+                       int ncell, double LX, double xmin, double xmax, double LZ, double zmin, double zmax,
+                       double *__restrict__ out, unsigned int *__restrict__ bad)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ double red[32];
     double *p = reinterpret_cast<double *>(smem);   // [3][V]
     const int cell = blockIdx.x, tid = threadIdx.x, T = blockDim.x;
     const long long vb = (long long)cell * V;
-    const double z0 = X[2 * nv + vb];
+    const double x0 = X[vb], z0 = X[2 * nv + vb];
+    const bool xper = LX > 0.0;
     for (int v = tid; v < V; v += T) {
-        p[v] = X[vb + v];
+        double x = X[vb + v];
+        if (xper) {
+            const double dx = x - x0;
+            if (dx > 0.5 * LX) x -= LX; else if (dx < -0.5 * LX) x += LX;
+        }
+        p[v] = x;
         p[V + v] = X[nv + vb + v];
         double z = X[2 * nv + vb + v];
         const double dz = z - z0;
@@ -71,8 +85,13 @@ metrics_noalloc_kernel(const double *__restrict__ X, long long nv, const int *__
     }
     __syncthreads();
     double sv = 0.0, sa = 0.0;
+    unsigned int nbad = 0;
     for (int e = tid; e < E; e += T) {
         const int na = tri[3 * e], nb = tri[3 * e + 1], nc = tri[3 * e + 2];
+        if ((unsigned)na >= (unsigned)V || (unsigned)nb >= (unsigned)V || (unsigned)nc >= (unsigned)V) {
+            nbad++;
+            continue;
+        }
         const double ax = p[na], ay = p[V + na], az = p[2 * V + na];
         const double bx = p[nb], by = p[V + nb], bz = p[2 * V + nb];
         const double cx = p[nc], cy = p[V + nc], cz = p[2 * V + nc];
@@ -84,6 +103,7 @@ metrics_noalloc_kernel(const double *__restrict__ X, long long nv, const int *__
         sv += 1.0 / 3.0 * (rx * c0 / nn + ry * c1 / nn + rz * c2 / nn) * dS;
         sa += dS;
     }
+    if (nbad) atomicAdd(bad, nbad);
     const double vol = block_sum(sv, red);
     const double area = block_sum(sa, red);
     double sx = 0.0, sy = 0.0, sz = 0.0;
@@ -92,6 +112,7 @@ metrics_noalloc_kernel(const double *__restrict__ X, long long nv, const int *__
     sy = block_sum(sy, red) / (double)V;
     sz = block_sum(sz, red) / (double)V;
     if (sz < zmin) sz += LZ; else if (sz > zmax) sz -= LZ;
+    if (xper) { if (sx < xmin) sx += LX; else if (sx > xmax) sx -= LX; }
     if (tid == 0) {
         out[cell] = vol;
         out[ncell + cell] = area;
@@ -125,9 +146,50 @@ int setup_device(int dev, double **addr)
 
 }  // namespace
 
+namespace {
+
+// Runs the call on device dev (current on entry); the caller restores its own
+// current device afterwards.
+int metrics_on_device(int dev, const double *x, int ncell, int vertex, int element, const int *tri, double LX,
+                      double xmin, double xmax, double LZ, double zmin, double zmax, void *stream, double *volume,
+                      double *area, double *centroid)
+{
+    double *scratch = nullptr;
+    int rc = setup_device(dev, &scratch);
+    if (rc) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    const long long nv = (long long)ncell * vertex;
+    unsigned int *bad = reinterpret_cast<unsigned int *>(scratch + kFlagSlot);
+    unsigned int nbad = 0;
+    cudaError_t e = cudaMemsetAsync(bad, 0, sizeof(unsigned int), s);
+    if (e == cudaSuccess) {
+        metrics_noalloc_kernel<<<ncell, kThreads, 24 * vertex, s>>>(x, nv, tri, vertex, element, ncell, LX, xmin,
+                                                                    xmax, LZ, zmin, zmax, scratch, bad);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(volume, scratch, sizeof(double) * ncell, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(area, scratch + ncell, sizeof(double) * ncell, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(centroid, scratch + 2 * ncell, sizeof(double) * 3 * ncell, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&nbad, bad, sizeof(unsigned int), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+        rbc::set_last_error(std::string("rbc_cell_metrics_noalloc: ") + cudaGetErrorString(e));
+        return RBC_ERR_CUDA;
+    }
+    if (nbad) {
+        rbc::set_last_error("rbc_cell_metrics_noalloc: " + std::to_string(nbad) +
+                            " triangle entries outside 0..vertex-1 (those triangles were skipped)");
+        return RBC_ERR_ARG;
+    }
+    return RBC_OK;
+}
+
+}  // namespace
+
 extern "C" int rbc_cell_metrics_noalloc(const double *x, int ncell, int vertex, int element, const int *tri,
-                                        double LZ, double zmin, double zmax, int device, void *stream,
-                                        double *volume, double *area, double *centroid)
+                                        double LX, double xmin, double xmax, double LZ, double zmin, double zmax,
+                                        int device, void *stream, double *volume, double *area, double *centroid)
 {
     if (!x || !tri || !volume || !area || !centroid) {
         rbc::set_last_error("rbc_cell_metrics_noalloc: NULL pointer argument");
@@ -140,40 +202,35 @@ extern "C" int rbc_cell_metrics_noalloc(const double *x, int ncell, int vertex, 
         return RBC_ERR_ARG;
     }
     if (vertex < 4 || vertex > kMaxVertex || element < 4) {
-        rbc::set_last_error("rbc_cell_metrics_noalloc: vertex must be 4.." + std::to_string(kMaxVertex) +
-                            " and element >= 4");
+        rbc::set_last_error("rbc_cell_metrics_noalloc: vertex = " + std::to_string(vertex) + " must be 4.." +
+                            std::to_string(kMaxVertex) + " and element >= 4");
         return RBC_ERR_ARG;
     }
     if (!(LZ > 0)) {
         rbc::set_last_error("rbc_cell_metrics_noalloc: LZ must be > 0");
         return RBC_ERR_ARG;
     }
-    int dev = device;
-    if (dev < 0 && cudaGetDevice(&dev) != cudaSuccess) return RBC_ERR_NO_DEVICE;
+    if (LX > 0 && !(xmax > xmin)) {
+        rbc::set_last_error("rbc_cell_metrics_noalloc: a periodic x (LX > 0) needs xmin < xmax");
+        return RBC_ERR_ARG;
+    }
+    int prev = 0;
+    cudaError_t e = cudaGetDevice(&prev);
+    if (e != cudaSuccess) {
+        rbc::set_last_error(std::string("rbc_cell_metrics_noalloc: no current CUDA device: ") + cudaGetErrorString(e));
+        return RBC_ERR_NO_DEVICE;
+    }
+    const int dev = device < 0 ? prev : device;
     if (dev >= kMaxDevices) {
         rbc::set_last_error("rbc_cell_metrics_noalloc: device ordinal above 63");
         return RBC_ERR_ARG;
     }
-    if (cudaSetDevice(dev) != cudaSuccess) {
-        rbc::set_last_error("rbc_cell_metrics_noalloc: cannot select the device");
+    if (dev != prev && cudaSetDevice(dev) != cudaSuccess) {
+        rbc::set_last_error("rbc_cell_metrics_noalloc: cannot select device " + std::to_string(dev));
         return RBC_ERR_CUDA;
     }
-    double *scratch = nullptr;
-    int rc = setup_device(dev, &scratch);
-    if (rc) return rc;
-    cudaStream_t s = (cudaStream_t)stream;
-    const long long nv = (long long)ncell * vertex;
-    metrics_noalloc_kernel<<<ncell, kThreads, 24 * vertex, s>>>(x, nv, tri, vertex, element, ncell, LZ, zmin,
-                                                                zmax, scratch);
-    cudaError_t e = cudaGetLastError();
-    if (e == cudaSuccess) e = cudaMemcpyAsync(volume, scratch, sizeof(double) * ncell, cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(area, scratch + ncell, sizeof(double) * ncell, cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess)
-        e = cudaMemcpyAsync(centroid, scratch + 2 * ncell, sizeof(double) * 3 * ncell, cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    if (e != cudaSuccess) {
-        rbc::set_last_error(std::string("rbc_cell_metrics_noalloc: ") + cudaGetErrorString(e));
-        return RBC_ERR_CUDA;
-    }
-    return RBC_OK;
+    const int rc = metrics_on_device(dev, x, ncell, vertex, element, tri, LX > 0 ? LX : 0.0, xmin, xmax, LZ, zmin,
+                                     zmax, stream, volume, area, centroid);
+    if (dev != prev) cudaSetDevice(prev);   // the caller's current device is left as it was
+    return rc;
 }
