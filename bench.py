@@ -520,6 +520,57 @@ def run_reference_capillaries(args):
             "e2e": {"value": round(value, 4), "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+def reference_kernels_b200(args, tag, case):
+    """The reference's own CUDA step modules (lbm.cu, ibm.cu, stress.cu,
+    matrix_solver.cu, volume_correction.cu compiled from the reference sources
+    for sm_100a by oracle/Makefile, lengths and constants as -D macros) on this
+    GPU: main.cu:73-110's step order, each module timed by CUDA events (the
+    reference synchronises the device after every module).  None when the
+    library was not built (no reference sources where the package was built)
+    or there is no GPU."""
+    import ctypes as C
+
+    import numpy as np
+    lib = ROOT / "oracle" / "_ref" / f"librefstep_{tag}.so"
+    if not lib.exists():
+        return None
+    try:
+        import torch
+        if not torch.cuda.is_available():
+            return None
+    except Exception:
+        return None
+    L = C.CDLL(str(lib))
+    p = lambda a: a.ctypes.data_as(C.c_void_p)  # noqa: E731
+    bc = np.ascontiguousarray(case.bc, dtype=np.int32)
+    tri = np.ascontiguousarray(case.tri, dtype=np.int32).reshape(-1)
+    xr = np.ascontiguousarray(case.xr, dtype=np.float64)
+    t0 = time.perf_counter()
+    if L.ref_setup(case.nx, case.ny, case.nz, p(bc), case.ncell, case.vertex, case.element, p(tri), p(xr)):
+        return {"unavailable": "the reference's setup reported an error"}
+    setup_s = time.perf_counter() - t0
+    if L.ref_step(1):
+        return {"unavailable": "the reference's step reported an error"}
+    steps = max(1, min(args.steps, 3 if tag == "dense" else 50))
+    ms = np.zeros(5)
+    with ClockSampler(0) as clk:
+        time.sleep(0.3)
+        rc = L.ref_time_steps(steps, p(ms))
+    if rc:
+        return {"unavailable": "the reference's step reported an error"}
+    per = ms / steps
+    fluid = case.fluid_nodes()
+    return {"value": round(fluid / (per.sum() * 1e-3) / 1e6, 3), "unit": "MLUPS", "steps": steps, "warmup": 1,
+            "ms_per_step": round(float(per.sum()), 3),
+            "ms_per_step_by_module": dict(zip(("stress", "ibm_st1", "lbm_d3q19", "ibm_st2", "volume_correction"),
+                                              [round(float(v), 3) for v in per])),
+            "lbm_module_mlups": round(fluid / (per[2] * 1e-3) / 1e6, 1), "setup_s": round(setup_s, 2),
+            "dtype": "f64", "residual": case.params["residual"],
+            "how": "the reference's own kernels compiled unmodified for sm_100a with a project-written def.h "
+                   "(oracle/ref_harness), CUDA events around each module, FP64 throughout",
+            "clocks": clk.summary()}
+
+
 def run_reference(args, world, rank):
     if rank != 0:
         return None
@@ -544,7 +595,7 @@ def run_reference(args, world, rank):
     value = fluid * steps / el / 1e6
     sample = (f"{steps} full FP64 oracle steps of {case.name} ({el:.1f} s, capped by a {budget:.0f} s budget); "
               "the reference implements the step only as CUDA kernels, so its CPU arm is the oracle port")
-    return {"metric": METRIC, "impl": "reference", "value": round(value, 4), "unit": "MLUPS", "n_gpus": world,
+    res = {"metric": METRIC, "impl": "reference", "value": round(value, 4), "unit": "MLUPS", "n_gpus": world,
             "steps": steps, "warmup": min(args.warmup, 2), "ms_per_step": round(el / steps * 1e3, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": case.name, "fluid_nodes": fluid, "cells": case.ncell,
@@ -553,6 +604,13 @@ def run_reference(args, world, rank):
             "cpu_baseline": {"value": round(value, 4), "unit": "MLUPS", "cores": num_threads(), "kind": "port",
                              "sample": sample},
             "e2e": {"value": round(value, 4), "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    # beside the CPU value: the reference's own CUDA kernels on this GPU
+    if args.workload in ("dense", "single") and not args.br:
+        from tests.golden.make_golden import bench_cases
+        rk = reference_kernels_b200(args, args.workload, bench_cases()[args.workload])
+        if rk is not None:
+            res["reference_kernels_b200"] = rk
+    return res
 
 
 def main():

@@ -320,6 +320,38 @@ int rbc_batch_autotune(rbc_batch *b, int steps_per_trial, int *chain_out);
  * (104 B per node + 84 B per vertex) used by the backward sweep.
  * Synchronous. */
 int rbc_adjoint_record(rbc_handle *h, int nsteps, int ckpt_every);
+/* rbc_adjoint_record_binomial: the same run for a reverse sweep under binomial
+ * (revolve) checkpointing, for lattices whose segments of stored stages would
+ * not fit: the run is cut into units of `unit` steps, and the backward sweep
+ * reverses them under the binomial schedule with `snaps` snapshot slots beside
+ * the initial state (A. Griewank, A. Walther, "Algorithm 799: revolve", ACM
+ * TOMS 26, 2000): each unit is advanced at most r times before it is
+ * recorded, r the least with C(snaps + r + 1, snaps + 1) >= units.  The
+ * forward run keeps the snapshots the schedule takes before its first
+ * recording.  Device memory: snaps + 2 checkpoints of 4 Q B per node + 48 B
+ * per vertex and 2 * unit steps of stored stages (104 B per node + 84 B per
+ * vertex), independent of nsteps.  rbc_adjoint_backward then follows the
+ * schedule (recordings alternate between the two stores, so a unit's
+ * recording overlaps the reversal of the unit after it).  Synchronous. */
+int rbc_adjoint_record_binomial(rbc_handle *h, int nsteps, int unit, int snaps);
+/* The recorded run's schedule: units (segments between checkpoints for
+ * rbc_adjoint_record), steps per unit, checkpoint slots including the initial
+ * state's, and the units one backward sweep advances without recording (0 for
+ * rbc_adjoint_record).  Any pointer may be NULL.  RBC_ERR_STATE before a
+ * record. */
+int rbc_adjoint_schedule(const rbc_handle *h, int *units, int *unit_steps, int *snapshots, long long *advances);
+/* The binomial schedule of `units` units with `snaps` free slots, from the
+ * initial state in slot 0, as actions (needs no device): ops[i] is
+ * 0 advance args[i] units, 1 keep the state in slot args[i], 2 restore slot
+ * args[i], 3 record unit args[i] (the state advances past it), 4 reverse unit
+ * args[i].  *len receives the number of actions; with cap 0 only *len is set,
+ * a cap below it is RBC_ERR_ARG. */
+#define RBC_ADJ_ADVANCE 0
+#define RBC_ADJ_SNAP    1
+#define RBC_ADJ_RESTORE 2
+#define RBC_ADJ_RECORD  3
+#define RBC_ADJ_REVERSE 4
+int rbc_adjoint_binomial_plan(int units, int snaps, int *ops, int *args, int cap, int *len);
 /* rbc_adjoint_backward: reverse sweep of the recorded run.
  *   xbar, ybar, zbar  host [nv] each: dL/d(final cel->x, y, z); NULL = 0
  *   grad              host [3] out: dL/dP, dL/dB, dL/dC
@@ -410,6 +442,18 @@ int rbc_read_center_file(rbc_handle *h, const char *path);
 int rbc_cell_metrics_noalloc(const double *x, int ncell, int vertex, int element, const int *tri,
                              double LX, double xmin, double xmax, double LZ, double zmin, double zmax,
                              int device, void *stream, double *volume, double *area, double *centroid);
+
+/* Launch shapes (no counterpart in the reference, which launches one thread
+ * per node): results do not depend on them, only the speed.
+ *   RBC_SHAPE_LBM_PLANES  z planes each collide-stream thread updates: 1, 2, 4
+ *                         or 8, or 0 to choose from the lattice size (2 with
+ *                         FP32 storage, 4 with FP16, fewer on lattices too
+ *                         small to fill the GPU).
+ * A change takes effect at the next step (the step graphs are rebuilt);
+ * batches built before keep their graphs until they are rebuilt. */
+#define RBC_SHAPE_LBM_PLANES 1
+int rbc_set_launch_shape(rbc_handle *h, int what, int value);
+int rbc_get_launch_shape(const rbc_handle *h, int what, int *value);
 
 /* Sizes of the internal lattice and of the cells. */
 int rbc_dims(const rbc_handle *h, int *nx, int *ny, int *nz_periodic, int *ncell, int *vertex, int *element);

@@ -14,13 +14,32 @@
  * modulus BR from -DREF_BR (default 0), viscosity ratio LAMBDA1 and
  * front-tracking interval K from -DREF_LAMBDA1 / -DREF_K (defaults 1 and
  * never), CN = 1, no adhesion, no white cells.
+ *
+ * -DREF_NW=<n> adds n white cells (N_W) with GSw / GS = -DREF_GSW and bending
+ * modulus BRw = -DREF_BRW; ref_driver.cu sets them up as cel_init_wbc and
+ * mem_init would (init3.cu:12-389, init1.cu:933-1046) from caller inputs.
+ *
+ * -DREF_SHEAR selects the shear-flow mode (CapsuleSHEARFLOW: x and z periodic,
+ * y walls moving along z) with the lattice shear rate -DREF_SR, both walls
+ * moving (allwall) or, with -DREF_TOPWALL, the top wall only (topwall).
  */
 #ifndef REF_HARNESS_DEF_H
 #define REF_HARNESS_DEF_H
 
 #include <stdbool.h>
 
+#ifdef REF_SHEAR
+#define CapsuleSHEARFLOW
+#ifdef REF_TOPWALL
+#define allwall false
+#define topwall true
+#else
+#define allwall true
+#define topwall false
+#endif
+#else
 #define CapsuleCHANNELFLOW
+#endif
 #define SKALAK
 
 /* node types (values shared with include/rbc_step.h and oracle/rbc_oracle.h) */
@@ -74,6 +93,9 @@
 #ifndef REF_FLOWSTART
 #define REF_FLOWSTART 0
 #endif
+#ifndef REF_SR
+#define REF_SR 0.0
+#endif
 #define LX        (REF_LX)
 #define LY        (REF_LY)
 #define LZ        (REF_LZ)
@@ -100,7 +122,18 @@
 #define LAMBDA2     1.0
 #define RUNGE_KUTTA 4
 #define N_R         1
-#define N_W         0
+#ifndef REF_NW
+#define REF_NW 0
+#endif
+#ifndef REF_GSW
+#define REF_GSW 1.0
+#endif
+#ifndef REF_BRW
+#define REF_BRW 0.0
+#endif
+#define N_W         (REF_NW)
+#define GSw         (REF_GSW)
+#define BRw         (REF_BRW)
 #define N_P         0
 #define N_C         0
 #define CN          1
@@ -110,7 +143,7 @@
 #define CYTOADHESION false
 #define BR          (REF_BR)
 #define GS          1.0
-#define SR          0.0
+#define SR          (REF_SR)
 #define Lc          1.0
 #define KL          1.0
 #define Uc          1.0
@@ -157,7 +190,7 @@ typedef struct {
     /* volume correction */
     double *volume0, *volume, *area, *gx, *lambdaH, *normal, *dS, *vtmp, *lambdaD;
     bool *is_converged;
-    /* white-cell fields referenced by code compiled out with N_W = 0 */
+    /* white cells (N_W > 0) */
     int n_w, vertex_w, element_w, mn_w, nnz_w, n_edge_w, n_th_w;
     double rg_w, br_w;
     double *xH_w, *yH_w, *zH_w, *xD_w, *yD_w, *zD_w, *uD_w, *vD_w, *wD_w, *fxD_w, *fyD_w, *fzD_w;
@@ -197,6 +230,7 @@ void lbm_d3q19(process *prc, domain *cdo, lattice *ltc);
 int  volume_correction(domain *cdo, cell *cel, fem *fem);
 void volume_init(domain *cdo, cell *cel);
 void fem_init(cell *cel, fem *fem);
+void fem_init_wbc(cell *cel, fem *fem);
 int redblacksor(int *d_ptr, int *d_index, double *d_value, double *d_x, double *d_b, double *d_r, double *d_o,
                 int n, int nnz, int nx, int ny, int nz, int nn);
 void thinc_wlic(domain *cdo, lattice *ltc);

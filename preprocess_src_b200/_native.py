@@ -18,6 +18,8 @@ RBC_STORE_F32, RBC_STORE_F16 = 0, 1
 RBC_FLOW_CHANNEL, RBC_FLOW_SHEAR = 0, 1
 RBC_WALLS_BOTH, RBC_WALLS_TOP = 0, 1
 RBC_NOALLOC_MAX_CELLS = 4096
+RBC_NOALLOC_MAX_VERTEX = 4096
+RBC_SHAPE_LBM_PLANES = 1
 RBC_NUM_KERNELS = 7
 RBC_KERNEL_NAMES = ("step_begin", "membrane", "spread", "lbm_collide_stream", "advect", "vof", "volume")
 RBC_FLAG_VC_NOT_CONVERGED, RBC_FLAG_NONFINITE, RBC_FLAG_SPREAD_OVERFLOW, RBC_FLAG_SOLVE_RESIDUAL = 1, 2, 4, 8
@@ -73,6 +75,8 @@ _SIGS = {
     "rbc_dims": [_H, _IP, _IP, _IP, _IP, _IP, _IP],
     "rbc_get_stream": [_H, C.POINTER(C.c_void_p)],
     "rbc_profile_steps": [_H, C.c_int, _DP],
+    "rbc_set_launch_shape": [_H, C.c_int, C.c_int],
+    "rbc_get_launch_shape": [_H, C.c_int, _IP],
     "rbc_cell_metrics_noalloc": [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_double, C.c_double,
                                  C.c_double, C.c_double, C.c_double, C.c_double, C.c_int, C.c_void_p,
                                  _DP, _DP, _DP],
@@ -86,6 +90,9 @@ _SIGS = {
     "rbc_batch_get_chain": [_H, _IP],
     "rbc_batch_autotune": [_H, C.c_int, _IP],
     "rbc_adjoint_record": [_H, C.c_int, C.c_int],
+    "rbc_adjoint_record_binomial": [_H, C.c_int, C.c_int, C.c_int],
+    "rbc_adjoint_schedule": [_H, _IP, _IP, _IP, C.POINTER(C.c_longlong)],
+    "rbc_adjoint_binomial_plan": [C.c_int, C.c_int, _IP, _IP, C.c_int, _IP],
     "rbc_adjoint_backward": [_H, _DP, _DP, _DP, _DP, _DP, _DP, _DP, _IP, C.POINTER(C.c_float)],
     "rbc_set_coefficients": [_H, C.c_double, C.c_double, C.c_double],
     "rbc_set_output_interval": [_H, C.c_int],

@@ -44,19 +44,26 @@ class InitialState:
 
 
 class ShapeRun(torch.autograd.Function):
-    """final_positions = ShapeRun.apply(theta, x0, sim, init, nsteps, ckpt_every)
+    """final_positions = ShapeRun.apply(theta, x0, sim, init, nsteps, ckpt_every, binomial)
 
     theta: float64 tensor [3] = (Gs, C, g); x0: float64 tensor [3, nv] of
-    initial positions, or None for the saved ones.  The simulation must not
-    be stepped between this forward and its backward (the backward reads the
-    checkpoints the forward recorded)."""
+    initial positions, or None for the saved ones.  binomial: None for a
+    checkpoint every ckpt_every steps, or (unit, snapshots) for binomial
+    checkpointing over units of that many steps with that many snapshot slots
+    (memory independent of nsteps).  The simulation must not be stepped
+    between this forward and its backward (the backward reads the checkpoints
+    the forward recorded)."""
 
     @staticmethod
-    def forward(ctx, theta, x0, sim: Simulation, init: InitialState, nsteps: int, ckpt_every: int = 100):
+    def forward(ctx, theta, x0, sim: Simulation, init: InitialState, nsteps: int, ckpt_every: int = 100,
+                binomial=None):
         Gs, C_, g = (float(v) for v in theta.detach().cpu().tolist())
         sim.set_coefficients(P=g / 2.0, B=Gs / 2.0, C_=C_)
         init.restore(sim, None if x0 is None else x0.detach().cpu().numpy())
-        sim.adjoint_record(nsteps, ckpt_every)
+        if binomial is None:
+            sim.adjoint_record(nsteps, ckpt_every)
+        else:
+            sim.adjoint_record_binomial(nsteps, *binomial)
         c = sim.export_cells()
         ctx.sim = sim
         ctx.x0_given = x0 is not None
@@ -73,7 +80,7 @@ class ShapeRun(torch.autograd.Function):
         dP, dB, dC = r["grad"]
         dtheta = torch.tensor([dB / 2.0, dC, dP / 2.0], dtype=torch.float64, device=grad_out.device)
         dx0 = torch.from_numpy(r["dx0"]).to(grad_out.device) if ctx.x0_given else None
-        return dtheta, dx0, None, None, None, None
+        return dtheta, dx0, None, None, None, None, None
 
 
 def shape_loss(final: torch.Tensor, target: torch.Tensor, LX: float, LZ: float) -> torch.Tensor:

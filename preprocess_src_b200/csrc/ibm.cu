@@ -6,10 +6,12 @@
 // vertex) and folds the BUFF planes afterwards.  Here one CTA owns one surface
 // patch of one cell: it finds the patch's lattice bounding box, accumulates
 // the patch's stencils in a shared-memory box with shared atomics, then adds
-// each non-zero box node to the lattice once with a global FP32 atomic
-// (patches and cells overlap).  z indices wrap periodically, which is what the
-// BUFF planes plus the fold compute.  A patch whose box does not fit in shared
-// memory takes a direct-atomic path.
+// each non-zero box node to the lattice once with a global 64-bit integer
+// atomic (patches and cells overlap) into the fixed-point force field
+// (ForceField), whose sums do not depend on the order of the atomics.  z
+// indices wrap periodically, which is what the BUFF planes plus the fold
+// compute.  A patch whose box does not fit in shared memory takes a
+// direct-atomic path (into the same fixed point, so it is deterministic too).
 //
 // Interpolation + advection replaces ibm_st2a (ibm.cu:372-639): four
 // interpolations of the averaged velocity in a frozen field, classical RK4 in
@@ -32,6 +34,28 @@ int spread_smem_bytes() { return SPREAD_SMEM; }
 // RBC_FLAG_NONFINITE instead of indexing anything).
 __device__ __forceinline__ bool sane_lattice(double l) { return fabs(l) < 16777216.0; }
 
+// v * 2^shift rounded to the nearest integer (ties to even) into out; false
+// when its magnitude reaches 2^62 (no add is then made).
+__device__ __forceinline__ bool to_fixed(double v, int shift, long long &out) {
+    const double d = ldexp(v, shift);   // exact: a power-of-two scaling
+    if (!(fabs(d) < 4.611686018427387904e18)) return false;
+    out = __double2ll_rn(d);
+    return true;
+}
+
+// Adds one node's fixed-point force (three components; zeros skipped) and sets
+// its occupancy bit.  Returns false if a component was out of range.
+__device__ __forceinline__ bool add_force(const ForceField &F, long long nint, long long gi, int z, long long xy,
+                                          double a, double b, double c, int sa, int sb, int sc) {
+    long long ia = 0, ib = 0, ic = 0;
+    const bool ok = to_fixed(a, sa, ia) & to_fixed(b, sb, ib) & to_fixed(c, sc, ic);
+    if (ia) atomicAdd(reinterpret_cast<unsigned long long *>(&F.F[gi]), (unsigned long long)ia);
+    if (ib) atomicAdd(reinterpret_cast<unsigned long long *>(&F.F[nint + gi]), (unsigned long long)ib);
+    if (ic) atomicAdd(reinterpret_cast<unsigned long long *>(&F.F[2 * nint + gi]), (unsigned long long)ic);
+    if (ia | ib | ic) atomicOr(&F.bits[(long long)z * F.wpp + (xy >> 5)], 1u << (xy & 31));
+    return ok;
+}
+
 __device__ __forceinline__ double unwrap_near(double l, double ref, int n) {
     const double h = 0.5 * n;
     if (l - ref > h) l -= n; else if (l - ref < -h) l += n;
@@ -44,18 +68,19 @@ __device__ __forceinline__ double unwrap_near(double l, double ref, int n) {
 // more CTAs than cells.  Box layout: x fastest, rows of bx, planes of ps >= bx*by
 // with ps = 8 (mod 32) so the four stencil planes of one vertex sit in
 // different shared-memory banks.
+// bid: the block's (cell, patch) index, blockIdx.x of a one-lattice launch
 template <bool XPER>
-__global__ void __launch_bounds__(SPREAD_THREADS)
-spread_kernel(const Geom g, const double *__restrict__ X, long long nv, int V,
-              const int *__restrict__ patch_off, const int *__restrict__ patch_vtx,
-              const int *__restrict__ patch_stride, int npatch,
-              const float *__restrict__ Fv, float *__restrict__ Fx, float *__restrict__ Fy,
-              float *__restrict__ Fz, const uint32_t *__restrict__ mask2d, int *__restrict__ flags)
+__device__ __forceinline__ void
+spread_body(const Geom &g, const double *__restrict__ X, long long nv, int V,
+            const int *__restrict__ patch_off, const int *__restrict__ patch_vtx,
+            const int *__restrict__ patch_stride, int npatch,
+            const float *__restrict__ Fv, const ForceField &F, const uint32_t *__restrict__ mask2d,
+            int *__restrict__ flags, int bid)
 {
     extern __shared__ unsigned sbox[];
     __shared__ int s_lo[3], s_hi[3];
     __shared__ unsigned s_fmax[3], s_wmax;
-    const int cell = blockIdx.x / npatch, patch = blockIdx.x - cell * npatch, tid = threadIdx.x;
+    const int cell = bid / npatch, patch = bid - cell * npatch, tid = threadIdx.x;
     const int p0 = patch_off[patch], np = patch_off[patch + 1] - p0, vstride = patch_stride[patch];
     const double *xs = X + (long long)cell * V, *ys = X + nv + (long long)cell * V, *zs = X + 2 * nv + (long long)cell * V;
     const float *fxs = Fv + (long long)cell * V, *fys = Fv + nv + (long long)cell * V, *fzs = Fv + 2 * nv + (long long)cell * V;
@@ -114,8 +139,12 @@ spread_kernel(const Geom g, const double *__restrict__ X, long long nv, int V,
     // the final sums are still exact.  Each term is an FP32 product rounded
     // once to an integer, the integer sums do not depend on the order of the
     // atomics, and converting back costs one rounding to FP32 (the scale is
-    // capped at 2^126 so that it and its inverse stay normal floats).
-    float qs[3] = {0.f, 0.f, 0.f}, qi[3] = {0.f, 0.f, 0.f};
+    // capped at 2^126 so that it and its inverse stay normal floats).  The
+    // flush converts each box sum exactly (a power-of-two scaling, rounded
+    // only where the box resolves finer than 2^-FORCE_FRAC) to the lattice's
+    // fixed point, whose integer sums are again order independent.
+    float qs[3] = {0.f, 0.f, 0.f};
+    int qe[3] = {0, 0, 0};
     if (use_box) {
         // Wn in units of 1/64: each vertex adds 4 k[a] * 4 k[b] to the 16
         // nodes (x, y) of its stencil in its base plane; a walk down each
@@ -154,7 +183,7 @@ spread_kernel(const Geom g, const double *__restrict__ X, long long nv, int V,
             // 2.147e9 < 2^31 leaves room for the rounding of the terms
             const float e = fminf(floorf(log2f(2.147e9f / (wb * fm))), 126.f);
             qs[k] = exp2f(e);
-            qi[k] = exp2f(-e);
+            qe[k] = (int)e;
         }
         for (int i = tid; i < 3 * nbi; i += blockDim.x) sbox[i] = 0u;
         __syncthreads();
@@ -214,10 +243,11 @@ spread_kernel(const Geom g, const double *__restrict__ X, long long nv, int V,
                     atomicAdd(&sbox[nbi + li], (unsigned)__float2int_rn(w * q1));
                     atomicAdd(&sbox[2 * nbi + li], (unsigned)__float2int_rn(w * q2));
                 } else if (__ldg(&mask2d[gxw + g.nx * gy]) & MASK_FLUID) {
-                    const long long gi = (long long)wrap_z(iz, g.nzc) * g.plane + gxw + (long long)g.nx * gy;
-                    atomicAdd(&Fx[gi], w * f0);
-                    atomicAdd(&Fy[gi], w * f1);
-                    atomicAdd(&Fz[gi], w * f2);
+                    const int zw = wrap_z(iz, g.nzc);
+                    const long long xy = gxw + (long long)g.nx * gy, gi = (long long)zw * g.plane + xy;
+                    if (!add_force(F, g.nint, gi, zw, xy, (double)(w * f0), (double)(w * f1), (double)(w * f2),
+                                   FORCE_FRAC, FORCE_FRAC, FORCE_FRAC))
+                        atomicOr(flags, RBC_FLAG_NONFINITE);
                 }
             }
         }
@@ -234,12 +264,23 @@ spread_kernel(const Geom g, const double *__restrict__ X, long long nv, int V,
         const int gx = XPER ? wrap_x(bx0 + lx, g.nx) : bx0 + lx, gy = by0 + ly;
         if (gx < 0 || gx >= g.nx || gy < 0 || gy >= g.ny) continue;   // never written; kept as a guard
         if (!(__ldg(&mask2d[gx + g.nx * gy]) & MASK_FLUID)) continue;   // wall column: the LBM never reads it
-        const long long gi = (long long)wrap_z(bz0 + lz, g.nzc) * g.plane + gx + (long long)g.nx * gy;
-        const float fa = (float)ia * qi[0], fb = (float)ib * qi[1], fc = (float)ic * qi[2];
-        if (ia != 0) atomicAdd(&Fx[gi], fa);
-        if (ib != 0) atomicAdd(&Fy[gi], fb);
-        if (ic != 0) atomicAdd(&Fz[gi], fc);
+        const int zw = wrap_z(bz0 + lz, g.nzc);
+        const long long xy = gx + (long long)g.nx * gy, gi = (long long)zw * g.plane + xy;
+        if (!add_force(F, g.nint, gi, zw, xy, (double)ia, (double)ib, (double)ic, FORCE_FRAC - qe[0],
+                       FORCE_FRAC - qe[1], FORCE_FRAC - qe[2]))
+            atomicOr(flags, RBC_FLAG_NONFINITE);
     }
+}
+
+template <bool XPER>
+__global__ void __launch_bounds__(SPREAD_THREADS)
+spread_kernel(const Geom g, const double *__restrict__ X, long long nv, int V,
+              const int *__restrict__ patch_off, const int *__restrict__ patch_vtx,
+              const int *__restrict__ patch_stride, int npatch,
+              const float *__restrict__ Fv, const ForceField F, const uint32_t *__restrict__ mask2d,
+              int *__restrict__ flags)
+{
+    spread_body<XPER>(g, X, nv, V, patch_off, patch_vtx, patch_stride, npatch, Fv, F, mask2d, flags, blockIdx.x);
 }
 
 cudaError_t spread_setup()
@@ -254,8 +295,7 @@ void launch_spread(const Geom &g, const SpreadArgs &a, cudaStream_t s)
     if (a.ncell <= 0) return;
     auto k = g.xper ? spread_kernel<true> : spread_kernel<false>;
     k<<<a.ncell * a.npatch, SPREAD_THREADS, SPREAD_SMEM, s>>>(
-        g, a.X, a.nv, a.V, a.patch_off, a.patch_vtx, a.patch_stride, a.npatch, a.Fv, a.Fx, a.Fy, a.Fz, a.mask2d,
-        a.flags);
+        g, a.X, a.nv, a.V, a.patch_off, a.patch_vtx, a.patch_stride, a.npatch, a.Fv, a.F, a.mask2d, a.flags);
 }
 
 // ---- interpolation + RK4 advection ---------------------------------------
@@ -355,17 +395,18 @@ __device__ __forceinline__ bool box_plane(const float4 *box, int bxs, int bys, i
 // of the vertex's own (unwrapped) frame are dropped per vertex as
 // ibm.cu:453-455 does.  A box larger than ADVECT_SMEM, or a later-stage
 // stencil outside the box, gathers from global memory instead.
+// bid: the block's (cell, patch) index, blockIdx.x of a one-lattice launch
 template <bool XPER>
-__global__ void __launch_bounds__(ADVECT_THREADS)
-advect_kernel(const Geom g, double *__restrict__ X, double *__restrict__ Xd, float *__restrict__ U,
-              const float4 *__restrict__ uvr, long long nv, int V, const int *__restrict__ patch_off,
-              const int *__restrict__ patch_vtx, int npatch, double dtM, int *__restrict__ flags)
+__device__ __forceinline__ void
+advect_body(const Geom &g, double *__restrict__ X, double *__restrict__ Xd, float *__restrict__ U,
+            const float4 *__restrict__ uvr, long long nv, int V, const int *__restrict__ patch_off,
+            const int *__restrict__ patch_vtx, int npatch, double dtM, int *__restrict__ flags, int bid)
 {
     extern __shared__ float4 abox[];   // [ADVECT_BOX_CAP] box, then the patch's positions and vertex ids
     double *spos = reinterpret_cast<double *>(abox + ADVECT_BOX_CAP);   // [3][ADVECT_MAX_PATCH]
     int *svid = reinterpret_cast<int *>(spos + 3 * ADVECT_MAX_PATCH);    // [ADVECT_MAX_PATCH]
     __shared__ int s_lo[3], s_hi[3];
-    const int cell = blockIdx.x / npatch, patch = blockIdx.x - cell * npatch, tid = threadIdx.x;
+    const int cell = bid / npatch, patch = bid - cell * npatch, tid = threadIdx.x;
     const int p0 = patch_off[patch], np = patch_off[patch + 1] - p0;
     const long long vb = (long long)cell * V;
     const double *xs = X + vb, *ys = X + nv + vb, *zs = X + 2 * nv + vb;
@@ -483,6 +524,15 @@ advect_kernel(const Geom g, double *__restrict__ X, double *__restrict__ Xd, flo
     }
 }
 
+template <bool XPER>
+__global__ void __launch_bounds__(ADVECT_THREADS)
+advect_kernel(const Geom g, double *__restrict__ X, double *__restrict__ Xd, float *__restrict__ U,
+              const float4 *__restrict__ uvr, long long nv, int V, const int *__restrict__ patch_off,
+              const int *__restrict__ patch_vtx, int npatch, double dtM, int *__restrict__ flags)
+{
+    advect_body<XPER>(g, X, Xd, U, uvr, nv, V, patch_off, patch_vtx, npatch, dtM, flags, blockIdx.x);
+}
+
 cudaError_t advect_setup()
 {
     cudaError_t e = cudaFuncSetAttribute(advect_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, ADVECT_SMEM);
@@ -496,6 +546,59 @@ void launch_advect(const Geom &g, const AdvectArgs &a, cudaStream_t s)
     auto k = g.xper ? advect_kernel<true> : advect_kernel<false>;
     k<<<a.ncell * a.npatch, ADVECT_THREADS, ADVECT_SMEM, s>>>(
         g, a.X, a.Xd, a.U, a.uvr, a.nv, a.V, a.patch_off, a.patch_vtx, a.npatch, a.dtM, a.flags);
+}
+
+// ---- fused batches ---------------------------------------------------------
+
+template <bool XPER>
+__global__ void __launch_bounds__(SPREAD_THREADS)
+spread_fused_kernel(const DomainArgs *__restrict__ dom, const int *__restrict__ boff, int ndom)
+{
+    const int d = fused_domain(boff, ndom, blockIdx.x);
+    const DomainArgs &D = dom[d];
+    const SpreadArgs &a = D.spread;
+    spread_body<XPER>(D.g, a.X, a.nv, a.V, a.patch_off, a.patch_vtx, a.patch_stride, a.npatch, a.Fv, a.F, a.mask2d,
+                      a.flags, blockIdx.x - boff[d]);
+}
+
+template <bool XPER>
+__global__ void __launch_bounds__(ADVECT_THREADS)
+advect_fused_kernel(const DomainArgs *__restrict__ dom, const int *__restrict__ boff, int ndom)
+{
+    const int d = fused_domain(boff, ndom, blockIdx.x);
+    const DomainArgs &D = dom[d];
+    const AdvectArgs &a = D.adv;
+    advect_body<XPER>(D.g, a.X, a.Xd, a.U, a.uvr, a.nv, a.V, a.patch_off, a.patch_vtx, a.npatch, a.dtM, a.flags,
+                      blockIdx.x - boff[d]);
+}
+
+cudaError_t ibm_fused_setup()
+{
+    const void *ks[] = {(const void *)spread_fused_kernel<false>, (const void *)spread_fused_kernel<true>};
+    for (const void *k : ks) {
+        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, SPREAD_SMEM);
+        if (e != cudaSuccess) return e;
+    }
+    const void *ka[] = {(const void *)advect_fused_kernel<false>, (const void *)advect_fused_kernel<true>};
+    for (const void *k : ka) {
+        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, ADVECT_SMEM);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+void launch_spread_fused(const FusedLaunch &f, bool xper, cudaStream_t s)
+{
+    if (f.nblocks <= 0) return;
+    auto k = xper ? spread_fused_kernel<true> : spread_fused_kernel<false>;
+    k<<<f.nblocks, SPREAD_THREADS, SPREAD_SMEM, s>>>(f.dom, f.boff, f.ndom);
+}
+
+void launch_advect_fused(const FusedLaunch &f, bool xper, cudaStream_t s)
+{
+    if (f.nblocks <= 0) return;
+    auto k = xper ? advect_fused_kernel<true> : advect_fused_kernel<false>;
+    k<<<f.nblocks, ADVECT_THREADS, ADVECT_SMEM, s>>>(f.dom, f.boff, f.ndom);
 }
 
 }  // namespace rbc

@@ -95,25 +95,78 @@ __device__ __forceinline__ float post_collision(const Collision &c, int q, float
     return om1 * gq + wq(q) * (c.A + eu * (c.B + c.C * eu + c.E * eG) + c.D * eG);
 }
 
+// FP16 storage rounds stochastically (cvt.rs.f16x2.f32, sm_100a): each stored
+// value goes to one of its two FP16 neighbours with probability proportional to
+// its closeness, so the storage error has zero mean instead of being a fixed
+// function of the value.  A steady flow stores nearly the same values step
+// after step; rounded to nearest, their errors repeat and add up in the flow,
+// while stochastic errors average out (M. Croci et al., "Stochastic rounding:
+// implementation, error analysis and applications", R. Soc. Open Sci. 9, 2022).
+// cvt.rs takes 13 random bits per value: rbits[12:0] for the low half (the
+// value in the second operand), rbits[28:16] for the high half.  The bits come
+// from a hash of the node index and the step counter, so runs are repeatable:
+// one 32-bit hash per node (the murmur3 finaliser), then per pair of
+// populations a 32 x 32 -> 64-bit product with an odd constant, whose high word
+// supplies the low field and whose low word the high field (the well-mixed
+// bits of each word).
+__device__ __forceinline__ uint32_t node_hash(uint32_t idx, uint32_t step) {
+    uint32_t h = idx * 0x9E3779B1u ^ step * 0x85EBCA77u;
+    h ^= h >> 16; h *= 0x85EBCA6Bu;
+    h ^= h >> 13; h *= 0xC2B2AE35u;
+    h ^= h >> 16;
+    return h;
+}
+__device__ __forceinline__ uint32_t pair_bits(uint32_t h, uint32_t mult) {
+    const unsigned long long p = (unsigned long long)h * mult;
+    return ((uint32_t)(p >> 32) & 0x0000FFFFu) | ((uint32_t)p & 0xFFFF0000u);
+}
+__device__ __forceinline__ uint32_t cvt_rs_f16x2(float hi, float lo, uint32_t rbits) {
+    uint32_t d;
+    asm("cvt.rs.f16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(hi), "f"(lo), "r"(rbits));
+    return d;
+}
+__device__ __forceinline__ void st_u16(__half *p, uint32_t v) {
+    __stcs(reinterpret_cast<unsigned short *>(p), (unsigned short)v);
+}
+
 // Collision of one node from its pulled populations g (storage units) and
 // stores of the post-collision values (0 for wall lanes) at element offset idx of every
-// population array; I is the offset type (int when Q * nint < 2^31).
+// population array; I is the offset type (int when Q * nint < 2^31).  has_force:
+// the node's occupancy bit (F holds its IB force, which is read and zeroed here).
 template <int STORE, bool ALL_FLUID, typename I>
-__device__ __forceinline__ void collide_store(float (&g)[Q], bool fluid, I idx, I nint,
+__device__ __forceinline__ void collide_store(float (&g)[Q], bool fluid, bool has_force, I idx, I nint,
                                               typename Store<STORE>::T *__restrict__ gout, float4 *__restrict__ uvr,
-                                              float *__restrict__ Fx, float *__restrict__ Fy, float *__restrict__ Fz,
+                                              long long *__restrict__ F, uint32_t step,
                                               float pd, float omega, float om1, float Cr, float Bc)
 {
     using S = Store<STORE>;
     const bool live = ALL_FLUID || fluid;
     float fx = 0.f, fy = 0.f, fz = 0.f;
-    if (live) { fx = Fx[idx]; fy = Fy[idx]; fz = Fz[idx]; }
+    if (live && has_force) {
+        constexpr float inv = 1.0f / (float)(1ULL << FORCE_FRAC);
+        fx = (float)F[idx] * inv; fy = (float)F[nint + idx] * inv; fz = (float)F[2 * nint + idx] * inv;
+        F[idx] = 0; F[nint + idx] = 0; F[2 * nint + idx] = 0;
+    }
     const Collision c = collision_terms<(int)S::scale>(g, fx, fy, fz, pd, omega, Cr, Bc);
     uvr[idx] = live ? make_float4(c.u, c.v, c.w, c.r) : make_float4(0.f, 0.f, 0.f, 1.f);
-    if (fx != 0.f || fy != 0.f || fz != 0.f) { Fx[idx] = 0.f; Fy[idx] = 0.f; Fz[idx] = 0.f; }
     typename S::T *ob = gout + idx;
+    if constexpr (STORE == RBC_STORE_F16) {
+        const uint32_t h = node_hash((uint32_t)idx, step);
+        // slot 0 alone, then the pairs (1, 2), (3, 4), ..., (17, 18)
+        const uint32_t d0 = cvt_rs_f16x2(0.f, live ? post_collision(c, 0, g[0], om1) : 0.f, pair_bits(h, 0x2545F491u));
+        st_u16(ob, d0);
 #pragma unroll
-    for (int q = 0; q < Q; q++) S::st_raw(ob + (I)q * nint, live ? post_collision(c, q, g[q], om1) : 0.f);
+        for (int q = 1; q < Q; q += 2) {
+            const float lo = live ? post_collision(c, q, g[q], om1) : 0.f;
+            const float hi = live ? post_collision(c, q + 1, g[q + 1], om1) : 0.f;
+            const uint32_t d = cvt_rs_f16x2(hi, lo, pair_bits(h, 0x9E3779B1u + 0x3C6EF372u * (uint32_t)q));
+            st_u16(ob + (I)q * nint, d);
+            st_u16(ob + (I)(q + 1) * nint, d >> 16);
+        }
+    } else {
+#pragma unroll
+        for (int q = 0; q < Q; q++) S::st_raw(ob + (I)q * nint, live ? post_collision(c, q, g[q], om1) : 0.f);
+    }
 }
 
 // One thread per (x, y) column and a few planes: blockIdx.x * blockDim.x +
@@ -137,19 +190,22 @@ __device__ __forceinline__ void collide_store(float (&g)[Q], bool fluid, I idx, 
 #endif
 // VISC: omega of each node from the volume fraction, 1 / (df3 (1 + lm1 vf) + 1/2)
 // (lbm.cu:1131 with LAMBDA1 != 1); the omega argument otherwise.
+// (bx, by, gy): the block's column tile, its first plane and the plane stride
+// (blockIdx.x, blockIdx.y, gridDim.y of a one-lattice launch).
 template <int STORE, typename I, bool VISC>
-__global__ void __launch_bounds__(LBM_THREADS, LBM_MIN_BLOCKS)
-lbm_collide_stream(const typename Store<STORE>::T *__restrict__ gin, typename Store<STORE>::T *__restrict__ gout,
-                   float4 *__restrict__ uvr,
-                   float *__restrict__ Fx, float *__restrict__ Fy, float *__restrict__ Fz,
-                   const uint32_t *__restrict__ mask2d, const float *__restrict__ drive,
-                   const float *__restrict__ wall, const double *__restrict__ vf, float lm1, float df3,
-                   int nx, int ny, int nzc, I nint,
-                   float omega, float Cr, float Bc)
+__device__ __forceinline__ void
+lbm_collide_stream_body(const typename Store<STORE>::T *__restrict__ gin, typename Store<STORE>::T *__restrict__ gout,
+                        float4 *__restrict__ uvr,
+                        long long *__restrict__ F, const uint32_t *__restrict__ Fbits, int wpp,
+                        const uint32_t *__restrict__ mask2d, const float *__restrict__ drive,
+                        const int *__restrict__ iter,
+                        const float *__restrict__ wall, const double *__restrict__ vf, float lm1, float df3,
+                        int nx, int ny, int nzc, I nint,
+                        float omega, float Cr, float Bc, int bx, int by, int gy)
 {
     using S = Store<STORE>;
     const int plane = nx * ny;
-    const int xy = blockIdx.x * blockDim.x + threadIdx.x;
+    const int xy = bx * blockDim.x + threadIdx.x;
     if (xy >= plane) return;
     const uint32_t m = __ldg(&mask2d[xy]);
     const bool fluid = (m & MASK_FLUID) != 0;
@@ -157,8 +213,16 @@ lbm_collide_stream(const typename Store<STORE>::T *__restrict__ gin, typename St
     if (!__any_sync(act, fluid)) return;   // a warp of wall nodes stores nothing
     const bool warp_links = __any_sync(act, (m & ~MASK_FLUID) != 0u);
     const float pd = __ldg(drive);
+    const uint32_t step = (STORE == RBC_STORE_F16) ? (uint32_t)__ldg(iter) : 0u;
     float om1 = 1.0f - omega;
-    for (int z = blockIdx.y; z < nzc; z += gridDim.y) {
+    // a warp's 32 nodes of a plane are the 32 bits of one occupancy word
+    // (blockDim.x is a multiple of 32), read by every lane (one address); the
+    // words are cleared before the next step's spread
+    const int lane = threadIdx.x & 31;
+    const int fword = xy >> 5;
+    for (int z = by; z < nzc; z += gy) {
+        const uint32_t fw = __ldg(Fbits + ((long long)z * wpp + fword));
+        const bool has_force = (fw >> lane) & 1u;
         // offsets of the source planes z - 1 and z + 1 from plane z (periodic);
         // with them every pull offset from the node is uniform over the block
         const I dzm = (z == 0) ? (I)(nzc - 1) * plane : -(I)plane;
@@ -174,7 +238,7 @@ lbm_collide_stream(const typename Store<STORE>::T *__restrict__ gin, typename St
 #pragma unroll
             for (int q = 0; q < Q; q++)
                 g[q] = S::ld_raw(gb + ((I)q * nint + ((ez(q) == 1) ? dzm : (ez(q) == -1) ? dzp : (I)0) - ex(q) - nx * ey(q)));
-            collide_store<STORE, true, I>(g, true, idx, nint, gout, uvr, Fx, Fy, Fz, pd, omega, om1, Cr, Bc);
+            collide_store<STORE, true, I>(g, true, has_force, idx, nint, gout, uvr, F, step, pd, omega, om1, Cr, Bc);
         } else {
 #pragma unroll
             for (int q = 0; q < Q; q++) {
@@ -197,9 +261,23 @@ lbm_collide_stream(const typename Store<STORE>::T *__restrict__ gin, typename St
                 for (int q = 0; q < Q; q++)
                     if (ez(q) != 0 && ((m >> q) & 1u)) g[q] += 6.0f * wq(q) * rho * Cr * (float)ez(q) * uw * S::scale;
             }
-            collide_store<STORE, false, I>(g, fluid, idx, nint, gout, uvr, Fx, Fy, Fz, pd, omega, om1, Cr, Bc);
+            collide_store<STORE, false, I>(g, fluid, has_force, idx, nint, gout, uvr, F, step, pd, omega, om1, Cr, Bc);
         }
     }
+}
+
+template <int STORE, typename I, bool VISC>
+__global__ void __launch_bounds__(LBM_THREADS, LBM_MIN_BLOCKS)
+lbm_collide_stream(const typename Store<STORE>::T *__restrict__ gin, typename Store<STORE>::T *__restrict__ gout,
+                   float4 *__restrict__ uvr,
+                   long long *__restrict__ F, const uint32_t *__restrict__ Fbits, int wpp,
+                   const uint32_t *__restrict__ mask2d, const float *__restrict__ drive, const int *__restrict__ iter,
+                   const float *__restrict__ wall, const double *__restrict__ vf, float lm1, float df3,
+                   int nx, int ny, int nzc, I nint,
+                   float omega, float Cr, float Bc)
+{
+    lbm_collide_stream_body<STORE, I, VISC>(gin, gout, uvr, F, Fbits, wpp, mask2d, drive, iter, wall, vf, lm1, df3,
+                                            nx, ny, nzc, nint, omega, Cr, Bc, blockIdx.x, blockIdx.y, gridDim.y);
 }
 
 // z planes per thread: the per-thread setup (mask, warp votes, drive) is paid
@@ -216,12 +294,14 @@ void launch_lbm(const Geom &g, int storage, const LbmArgs &a, cudaStream_t s)
 {
     int zpt = (storage == RBC_STORE_F16) ? LBM_PLANES_F16 : LBM_PLANES_F32;
     while (zpt > 1 && (long long)g.plane * g.nzc / zpt < LBM_MIN_THREADS) zpt >>= 1;
+    if (a.planes > 0) zpt = a.planes;   // a launch shape set through rbc_set_launch_shape
     const int gz = (g.nzc + zpt - 1) / zpt;
     const dim3 blocks((unsigned)((g.plane + LBM_THREADS - 1) / LBM_THREADS), (unsigned)(gz < 65535 ? gz : 65535));
     const bool off32 = (long long)Q * g.nint < (1LL << 31);   // every element offset fits in an int
 #define LBM_LAUNCH(ST, I, V)                                                                                  \
     lbm_collide_stream<ST, I, V><<<blocks, LBM_THREADS, 0, s>>>(                                              \
-        (const Store<ST>::T *)a.gin, (Store<ST>::T *)a.gout, a.uvr, a.Fx, a.Fy, a.Fz, a.mask2d, a.drive, a.wall, a.vf, \
+        (const Store<ST>::T *)a.gin, (Store<ST>::T *)a.gout, a.uvr, a.F.F, a.F.bits, a.F.wpp, a.mask2d, a.drive, a.iter, \
+        a.wall, a.vf, \
         a.lm1, a.df3, g.nx, g.ny, g.nzc, (I)g.nint, a.omega, a.Cr, a.Bc)
 #define LBM_LAUNCH_V(ST, I) do { if (a.vf) LBM_LAUNCH(ST, I, true); else LBM_LAUNCH(ST, I, false); } while (0)
     if (storage == RBC_STORE_F16) {
@@ -231,6 +311,37 @@ void launch_lbm(const Geom &g, int storage, const LbmArgs &a, cudaStream_t s)
     }
 #undef LBM_LAUNCH_V
 #undef LBM_LAUNCH
+}
+
+// Fused batches: the collide-stream of every domain in one launch of TPB
+// threads per block; domain d's block b is its column tile b % lbm_bx and
+// first plane b / lbm_bx, planes stepping by lbm_gy.
+template <int STORE, typename I, int TPB>
+__global__ void __launch_bounds__(TPB, (LBM_MIN_BLOCKS * LBM_THREADS) / TPB)
+lbm_fused_kernel(const DomainArgs *__restrict__ dom, const int *__restrict__ boff, int ndom)
+{
+    using T = typename Store<STORE>::T;
+    const int d = fused_domain(boff, ndom, blockIdx.x);
+    const DomainArgs &D = dom[d];
+    const LbmArgs &a = D.lbm;
+    const int b = blockIdx.x - boff[d];
+    lbm_collide_stream_body<STORE, I, false>((const T *)a.gin, (T *)a.gout, a.uvr, a.F.F, a.F.bits, a.F.wpp, a.mask2d,
+                                            a.drive, a.iter, a.wall, nullptr, 0.f, 0.f, D.g.nx, D.g.ny, D.g.nzc,
+                                            (I)D.g.nint, a.omega, a.Cr, a.Bc, b % D.lbm_bx, b / D.lbm_bx, D.lbm_gy);
+}
+
+void launch_lbm_fused(const FusedLaunch &f, int storage, bool off32, int threads, cudaStream_t s)
+{
+    if (f.nblocks <= 0) return;
+#define LBM_FUSED(ST, I, TPB) lbm_fused_kernel<ST, I, TPB><<<f.nblocks, TPB, 0, s>>>(f.dom, f.boff, f.ndom)
+#define LBM_FUSED_T(ST, I) do { if (threads == 128) LBM_FUSED(ST, I, 128); else LBM_FUSED(ST, I, 256); } while (0)
+    if (storage == RBC_STORE_F16) {
+        if (off32) LBM_FUSED_T(RBC_STORE_F16, int); else LBM_FUSED_T(RBC_STORE_F16, long long);
+    } else {
+        if (off32) LBM_FUSED_T(RBC_STORE_F32, int); else LBM_FUSED_T(RBC_STORE_F32, long long);
+    }
+#undef LBM_FUSED_T
+#undef LBM_FUSED
 }
 
 // ---- circular tube: interpolated bounce-back ------------------------------
@@ -396,8 +507,10 @@ __global__ void export_lattice_kernel(const Geom g, const typename Store<STORE>:
     }
 }
 
-__global__ void export_force_kernel(const Geom g, const float *__restrict__ Fx, const float *__restrict__ Fy,
-                                    const float *__restrict__ Fz, const uint32_t *__restrict__ mask2d,
+// The spread's result in the reference layout (ltc->fx/fy/fz): the fixed-point
+// sums as FP64 (exact below 2^53 units of 2^-56); the collide-stream kernel
+// rounds them once more, to FP32.
+__global__ void export_force_kernel(const Geom g, const long long *__restrict__ F, const uint32_t *__restrict__ mask2d,
                                     double *__restrict__ out)
 {
     const long long pref = (long long)g.nxr * g.ny, nref = pref * g.nzr;
@@ -410,9 +523,25 @@ __global__ void export_force_kernel(const Geom g, const float *__restrict__ Fx, 
     double a = 0.0, b = 0.0, c = 0.0;
     if (xr >= g.xb && xr < g.nxr - g.xb && (mask2d[xy] & MASK_FLUID) && zr >= 2 && zr < g.nzr - 2) {
         const long long idx = (long long)(zr - 2) * g.plane + xy;
-        a = Fx[idx]; b = Fy[idx]; c = Fz[idx];
+        constexpr double inv = 1.0 / (double)(1ULL << FORCE_FRAC);
+        a = (double)F[idx] * inv; b = (double)F[g.nint + idx] * inv; c = (double)F[2 * g.nint + idx] * inv;
     }
     out[i] = a; out[nref + i] = b; out[2 * nref + i] = c;
+}
+
+// The force each node's collision reads, FP32 [3][nint] (what the adjoint keeps).
+__global__ void force_to_f32_kernel(const long long *__restrict__ F, long long n3, float *__restrict__ out)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n3) return;
+    constexpr float inv = 1.0f / (float)(1ULL << FORCE_FRAC);
+    out[i] = (float)F[i] * inv;
+}
+
+void launch_force_to_f32(const Geom &g, const long long *F, float *out3, cudaStream_t s)
+{
+    const long long n3 = 3 * g.nint;
+    force_to_f32_kernel<<<(unsigned)((n3 + 255) / 256), 256, 0, s>>>(F, n3, out3);
 }
 
 __global__ void fill_f32_kernel(float *p, long long n, float v)
@@ -457,11 +586,10 @@ void launch_export_lattice(const Geom &g, int storage, const void *gin, const ui
                                                                      inv_scale, fn_ref, dn, un, vn, wn, w);
 }
 
-void launch_export_force(const Geom &g, const float *Fx, const float *Fy, const float *Fz,
-                         const uint32_t *mask2d, double *out3, cudaStream_t s)
+void launch_export_force(const Geom &g, const long long *F, const uint32_t *mask2d, double *out3, cudaStream_t s)
 {
     const long long nref = (long long)g.nxr * g.ny * g.nzr;
-    export_force_kernel<<<(unsigned)((nref + 255) / 256), 256, 0, s>>>(g, Fx, Fy, Fz, mask2d, out3);
+    export_force_kernel<<<(unsigned)((nref + 255) / 256), 256, 0, s>>>(g, F, mask2d, out3);
 }
 
 void launch_fill_f32(float *p, long long n, float v, cudaStream_t s)

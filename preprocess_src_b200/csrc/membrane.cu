@@ -99,9 +99,9 @@ constexpr int MAX_VALENCE = 6;   // checked when the topology is built
 // registers a thread), 1024 otherwise
 template <int VPT> constexpr int mem_max_threads() { return VPT >= 3 ? 896 : MEM_MAX_THREADS; }
 
+// cell: the block's cell, blockIdx.x of a one-population launch
 template <typename Real, int VPT>
-__global__ void __launch_bounds__(mem_max_threads<VPT>(), 1)
-membrane_kernel(const MembraneArgs a)
+__device__ __forceinline__ void membrane_body(const MembraneArgs &a, int cell)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ float red[32];
@@ -111,7 +111,6 @@ membrane_kernel(const MembraneArgs a)
     float *coef = reinterpret_cast<float *>(smem + 32 * (size_t)V);    // [6][V]
     int16_t *snbr = reinterpret_cast<int16_t *>(smem + 56 * (size_t)V);// [6][V]
 
-    const int cell = blockIdx.x;
     const long long vb = (long long)cell * V, eb = (long long)cell * E, nv = a.nv;
     const double ax = a.Xd[vb], ay = a.Xd[nv + vb], az = a.Xd[2 * nv + vb];
     for (int v = tid; v < V; v += T) {
@@ -296,6 +295,13 @@ membrane_kernel(const MembraneArgs a)
 }
 
 template <typename Real, int VPT>
+__global__ void __launch_bounds__(mem_max_threads<VPT>(), 1)
+membrane_kernel(const MembraneArgs a)
+{
+    membrane_body<Real, VPT>(a, blockIdx.x);
+}
+
+template <typename Real, int VPT>
 static void launch_vpt(const MembraneArgs &a, cudaStream_t s)
 {
     const int smem = membrane_smem_bytes(a.V);
@@ -353,6 +359,65 @@ void launch_membrane(const MembraneArgs &a, bool fp64, cudaStream_t s)
     if (a.ncell <= 0) return;
     if (fp64) launch_real<double>(a, s);
     else launch_real<float>(a, s);
+}
+
+// ---- fused batches ---------------------------------------------------------
+
+template <typename Real, int VPT>
+__global__ void __launch_bounds__(mem_max_threads<VPT>(), 1)
+membrane_fused_kernel(const DomainArgs *__restrict__ dom, const int *__restrict__ boff, int ndom)
+{
+    const int d = fused_domain(boff, ndom, blockIdx.x);
+    membrane_body<Real, VPT>(dom[d].mem, blockIdx.x - boff[d]);
+}
+
+int membrane_threads(int V, int vpt) { return ((V + vpt - 1) / vpt + 31) / 32 * 32; }
+
+int membrane_default_vpt(int V)
+{
+    if (membrane_threads(V, 1) <= mem_max_threads<1>()) return 1;
+    if (membrane_threads(V, 2) <= mem_max_threads<2>()) return 2;
+    if (membrane_threads(V, 3) <= mem_max_threads<3>()) return 3;
+    return 4;
+}
+
+template <typename Real, int VPT>
+static void launch_fused_vpt(const FusedLaunch &f, int V, cudaStream_t s)
+{
+    membrane_fused_kernel<Real, VPT><<<f.nblocks, membrane_threads(V, VPT), membrane_smem_bytes(V), s>>>(
+        f.dom, f.boff, f.ndom);
+}
+
+template <typename Real>
+static void launch_fused_real(const FusedLaunch &f, int V, int vpt, cudaStream_t s)
+{
+    switch (vpt) {
+    case 1: launch_fused_vpt<Real, 1>(f, V, s); break;
+    case 2: launch_fused_vpt<Real, 2>(f, V, s); break;
+    case 3: launch_fused_vpt<Real, 3>(f, V, s); break;
+    default: launch_fused_vpt<Real, 4>(f, V, s); break;
+    }
+}
+
+void launch_membrane_fused(const FusedLaunch &f, bool fp64, int V, int vpt, cudaStream_t s)
+{
+    if (f.nblocks <= 0) return;
+    if (fp64) launch_fused_real<double>(f, V, vpt, s);
+    else launch_fused_real<float>(f, V, vpt, s);
+}
+
+cudaError_t membrane_fused_setup(int optin)
+{
+    const void *ks[] = {(const void *)membrane_fused_kernel<float, 1>, (const void *)membrane_fused_kernel<float, 2>,
+                        (const void *)membrane_fused_kernel<float, 3>, (const void *)membrane_fused_kernel<float, 4>,
+                        (const void *)membrane_fused_kernel<double, 1>, (const void *)membrane_fused_kernel<double, 2>,
+                        (const void *)membrane_fused_kernel<double, 3>, (const void *)membrane_fused_kernel<double, 4>};
+    for (const void *k : ks) {
+        int g = 0;
+        cudaError_t e = set_max_dyn_smem(k, optin, &g);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 }  // namespace rbc

@@ -83,7 +83,8 @@ struct rbc_handle {
     int cur = 0;
     size_t gbytes = 0;
     float4 *uvr = nullptr;
-    float *Fx = nullptr, *Fy = nullptr, *Fz = nullptr;
+    long long *Fint = nullptr;                        // IB force, fixed point [3][nint] (ForceField)
+    uint32_t *Fbits = nullptr;                        // its occupancy words [nzc][wpp]
     uint32_t *mask2d = nullptr;
     int *tube_links = nullptr; float *tube_frac = nullptr; int ntube = 0;   // interpolated wall links (circular tube)
     // device scalars: iter, flags, vc_max, vc_last, front-tracking sweeps of populations 0 and 1
@@ -116,6 +117,7 @@ struct rbc_handle {
     int device = 0;
     AdjointState *adj = nullptr;                      // checkpoints and buffers of the adjoint, on first use
     int fileoutput = 0;                               // FILEOUTPUT of the qi / tp averages; 0 = not accumulated
+    int lbm_planes = 0;                               // RBC_SHAPE_LBM_PLANES (0 = automatic)
     // the volume correction that ended the last rbc_step left every population's
     // volume, area (vol_out, area_out) and centroid (gx) of the current state
     bool metrics_valid = false;
@@ -134,6 +136,8 @@ struct rbc_handle {
         }
         return k;
     }
+    ForceField force() const { return ForceField{Fint, Fbits, force_words_per_plane(geo.plane)}; }
+    size_t force_bit_bytes() const { return sizeof(uint32_t) * (size_t)geo.nzc * force_words_per_plane(geo.plane); }
     bool has_cells() const {
         for (int g = 0; g < ngroups; g++) if (cg[g].ncell > 0) return true;
         return false;
@@ -603,7 +607,7 @@ void free_all(rbc_handle *h)
     if (h->wave_done) cudaEventDestroy(h->wave_done);
     if (h->spread_done) cudaEventDestroy(h->spread_done);
     if (h->side2) cudaStreamDestroy(h->side2);
-    void *ptrs[] = {h->g[0], h->g[1], h->uvr, h->Fx, h->Fy, h->Fz, h->mask2d, h->tube_links, h->tube_frac,
+    void *ptrs[] = {h->g[0], h->g[1], h->uvr, h->Fint, h->Fbits, h->mask2d, h->tube_links, h->tube_frac,
                     h->d_int, h->d_drive, h->staging, h->vof_s1, h->vof_s2, h->vof_G, h->vof_b, h->vof_partial};
     for (void *q : ptrs) if (q) cudaFree(q);
     for (CellGroup &c : h->cg) free_group(c);
@@ -642,7 +646,7 @@ int launch_spread_range(rbc_handle *h, CellGroup &g, int c0, int c1, cudaStream_
     a.X = g.X + (size_t)c0 * g.V; a.nv = g.nv; a.V = g.V; a.ncell = c1 - c0; a.Fv = g.Fv + (size_t)c0 * g.V;
     a.patch_off = g.patch_off; a.patch_vtx = g.patch_vtx; a.patch_stride = g.patch_stride;
     a.npatch = g.npatch;
-    a.Fx = h->Fx; a.Fy = h->Fy; a.Fz = h->Fz; a.mask2d = h->mask2d; a.flags = h->d_flags();
+    a.F = h->force(); a.mask2d = h->mask2d; a.flags = h->d_flags();
     launch_spread(h->geo, a, st);
     h->launches++;
     CK_LAUNCH();
@@ -692,6 +696,14 @@ int launch_stress(rbc_handle *h)
     return RBC_OK;
 }
 
+// the occupancy words of the lattice force start each step's spread at zero
+// (the collide-stream kernel zeroes the forces it read, not the words)
+int clear_force_bits(rbc_handle *h, cudaStream_t st)
+{
+    CK(cudaMemsetAsync(h->Fbits, 0, h->force_bit_bytes(), st));
+    return RBC_OK;
+}
+
 // ibm_st1's spreading (ibm.cu:299-369) of every population into the same force field
 int launch_spread_stage(rbc_handle *h)
 {
@@ -702,7 +714,7 @@ int launch_spread_stage(rbc_handle *h)
         a.X = g.X; a.nv = g.nv; a.V = g.V; a.ncell = g.ncell; a.Fv = g.Fv;
         a.patch_off = g.patch_off; a.patch_vtx = g.patch_vtx; a.patch_stride = g.patch_stride;
         a.npatch = g.npatch;
-        a.Fx = h->Fx; a.Fy = h->Fy; a.Fz = h->Fz; a.mask2d = h->mask2d; a.flags = h->d_flags();
+        a.F = h->force(); a.mask2d = h->mask2d; a.flags = h->d_flags();
         launch_spread(h->geo, a, h->stream);
         h->launches++;
         CK_LAUNCH();
@@ -732,10 +744,11 @@ int launch_lbm_stage(rbc_handle *h)
     LbmArgs a{};
     a.gin = h->g[h->cur]; a.gout = h->g[1 - h->cur];
     a.uvr = h->uvr;
-    a.Fx = h->Fx; a.Fy = h->Fy; a.Fz = h->Fz; a.mask2d = h->mask2d; a.drive = h->d_drive;
+    a.F = h->force(); a.mask2d = h->mask2d; a.drive = h->d_drive; a.iter = h->d_iter();
     a.wall = h->p.flow == RBC_FLOW_SHEAR ? h->d_drive + 1 : nullptr;
     a.omega = (float)(1.0 / h->p.tau); a.Cr = (float)h->p.Cr; a.Bc = (float)h->p.B;
     a.scale = h->scale; a.inv_scale = h->inv_scale;
+    a.planes = h->lbm_planes;
     // the red cells' volume fraction sets omega (lbm.cu:1131; ltc->vf2 of the white cells does not)
     a.vf = (h->p.lambda1 != 1.0 && h->cg[0].vf) ? h->cg[0].vf : nullptr;
     a.lm1 = (float)(h->p.lambda1 - 1.0);
@@ -886,6 +899,7 @@ int enqueue_step(rbc_handle *h, StepForm form = STEP_WHOLE)
     launch_step_begin(step_begin_args(h), h->stream);
     h->launches++;
     CK_LAUNCH();
+    if ((rc = clear_force_bits(h, h->stream))) return rc;
     const int split = membrane_wave_split(h);
     if (split > 0) {
         CellGroup &g = h->cg[0];
@@ -948,9 +962,8 @@ int build_graph(rbc_handle *h, int c, StepForm form)
 int prepare_steps(rbc_handle *h)
 {
     if (h->force_pending) {
-        CK(cudaMemsetAsync(h->Fx, 0, 4 * h->geo.nint, h->stream));
-        CK(cudaMemsetAsync(h->Fy, 0, 4 * h->geo.nint, h->stream));
-        CK(cudaMemsetAsync(h->Fz, 0, 4 * h->geo.nint, h->stream));
+        CK(cudaMemsetAsync(h->Fint, 0, 24 * h->geo.nint, h->stream));
+        CK(cudaMemsetAsync(h->Fbits, 0, h->force_bit_bytes(), h->stream));
         h->force_pending = false;
     }
     // the device counter follows the host's prc->iter mirror
@@ -1235,12 +1248,11 @@ int rbc_create(const rbc_params *p, const rbc_mesh *mesh, const int *bc, rbc_han
         h->err = "out of device memory for the populations";
         return bail(RBC_ERR_CUDA);
     }
-    TRY(dalloc(h, &h->uvr, g.nint)); TRY(dalloc(h, &h->Fx, g.nint)); TRY(dalloc(h, &h->Fy, g.nint));
-    TRY(dalloc(h, &h->Fz, g.nint)); TRY(dalloc(h, &h->mask2d, g.plane));
+    TRY(dalloc(h, &h->uvr, g.nint)); TRY(dalloc(h, &h->Fint, 3 * g.nint));
+    TRY(dalloc(h, &h->Fbits, h->force_bit_bytes() / sizeof(uint32_t))); TRY(dalloc(h, &h->mask2d, g.plane));
     TRY(dalloc(h, &h->d_int, 6)); TRY(dalloc(h, &h->d_drive, 3));
     if (cudaMemset(h->g[0], 0, h->gbytes) != cudaSuccess || cudaMemset(h->g[1], 0, h->gbytes) != cudaSuccess ||
-        cudaMemset(h->Fx, 0, 4 * g.nint) != cudaSuccess ||
-        cudaMemset(h->Fy, 0, 4 * g.nint) != cudaSuccess || cudaMemset(h->Fz, 0, 4 * g.nint) != cudaSuccess ||
+        cudaMemset(h->Fint, 0, 24 * g.nint) != cudaSuccess || cudaMemset(h->Fbits, 0, h->force_bit_bytes()) != cudaSuccess ||
         cudaMemset(h->d_int, 0, 6 * sizeof(int)) != cudaSuccess || cudaMemset(h->d_drive, 0, 3 * sizeof(float)) != cudaSuccess ||
         cudaMemcpy(h->mask2d, mask.data(), 4 * g.plane, cudaMemcpyHostToDevice) != cudaSuccess) {
         h->err = "device initialisation failed";
@@ -1362,7 +1374,7 @@ int rbc_export_ref_force(rbc_handle *h, double *fx, double *fy, double *fz)
     int rc = ensure_staging(h, sizeof(double) * 3 * n);
     if (rc) return rc;
     double *s = (double *)h->staging;
-    launch_export_force(h->geo, h->Fx, h->Fy, h->Fz, h->mask2d, s, h->stream);
+    launch_export_force(h->geo, h->Fint, h->mask2d, s, h->stream);
     h->launches++;
     CK_LAUNCH();
     if (fx) CK(cudaMemcpyAsync(fx, s, sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream));
@@ -1499,12 +1511,11 @@ int rbc_ibm_st1(rbc_handle *h)
 {
     if (!h) return RBC_ERR_ARG;
     RBC_DEVICE_GUARD(h);
-    if (h->force_pending) {   // ibm_st1a: start from zero (ibm.cu:315-320)
-        CK(cudaMemsetAsync(h->Fx, 0, 4 * h->geo.nint, h->stream));
-        CK(cudaMemsetAsync(h->Fy, 0, 4 * h->geo.nint, h->stream));
-        CK(cudaMemsetAsync(h->Fz, 0, 4 * h->geo.nint, h->stream));
-    }
-    int rc = launch_spread_stage(h);
+    if (h->force_pending)   // ibm_st1a: start from zero (ibm.cu:315-320)
+        CK(cudaMemsetAsync(h->Fint, 0, 24 * h->geo.nint, h->stream));
+    int rc = clear_force_bits(h, h->stream);
+    if (rc) return rc;
+    rc = launch_spread_stage(h);
     if (rc) return rc;
     h->force_pending = true;
     return RBC_OK;
@@ -1942,10 +1953,31 @@ int rbc_batch_autotune(rbc_batch *b, int steps_per_trial, int *chain_out)
 // (4 Q B per node + 48 B per vertex) and 2 K steps of stored stages
 // (104 B per node + 84 B per vertex).
 
+// Binomial checkpointing (rbc_adjoint_record_binomial): the run is cut into
+// units of `unit` steps and reversed unit by unit under the schedule of
+// binomial (revolve) checkpointing with S snapshot slots beside the initial
+// state (A. Griewank, A. Walther, "Algorithm 799: revolve", ACM TOMS 26,
+// 2000).  To reverse units [a, b) from the state at a (held in a slot) with s
+// free slots: one unit is recorded and reversed at once; with no free slot,
+// each unit t from b - 1 down is reached by restoring a and advancing t - a
+// units; otherwise the state is advanced to m = a + N(s, r - 1), kept in a new
+// slot, [m, b) is reversed with s - 1 slots, a is restored and [a, m) is
+// reversed with s slots.  r is the least repetition count with N(s, r) >= b - a,
+// where N(s, r) = C(s + r + 1, s + 1) is the most units that s free slots
+// reverse when no unit is advanced more than r times, so every unit is
+// advanced at most r times before its recording.
+struct AdjAction { int op, arg; };
+enum { ADJ_ADVANCE, ADJ_SNAP, ADJ_RESTORE, ADJ_RECORD, ADJ_REVERSE };
+
 struct AdjointState {
     int K = 0, nseg_cap = 0, K_cap = 0;
     int nsteps = 0, nseg = 0;
     bool valid = false;
+    // schedule: 0 = a checkpoint every K steps; 1 = binomial over units of K steps
+    int mode = 0;
+    int nunits = 0, snaps = 0, final_slot = 0;
+    std::vector<AdjAction> plan;         // binomial: the backward sweep's actions
+    long long advanced_units = 0;        // binomial: units advanced by the last backward sweep
     std::vector<int> ck_iter;            // iter at each checkpoint
     std::vector<void *> bufs;            // every allocation below, for adjoint_free
     // checkpoints [nseg + 1]
@@ -2068,9 +2100,8 @@ int adjoint_restore(rbc_handle *h, int k)
     if ((rc = d2d(h, h->X, a->ck_X + k * nv3, 8 * nv3))) return rc;
     if ((rc = d2d(h, h->Xd, a->ck_Xd + k * nv3, 8 * nv3))) return rc;
     if ((rc = d2d(h, h->gx, a->ck_gx + k * N3, 8 * N3))) return rc;
-    CK(cudaMemsetAsync(h->Fx, 0, 4 * n, h->stream));
-    CK(cudaMemsetAsync(h->Fy, 0, 4 * n, h->stream));
-    CK(cudaMemsetAsync(h->Fz, 0, 4 * n, h->stream));
+    CK(cudaMemsetAsync(h->Fint, 0, 24 * n, h->stream));
+    CK(cudaMemsetAsync(h->Fbits, 0, h->force_bit_bytes(), h->stream));
     h->force_pending = false;
     h->iter = a->ck_iter[k];
     return d2d(h, h->d_iter(), a->ck_itd + k, sizeof(int));   // device to device: no host staging
@@ -2111,10 +2142,11 @@ int adjoint_enqueue_recompute_body(rbc_handle *h, int b, int len)
         CK_LAUNCH();
         if ((rc = launch_stress(h))) return rc;
         if ((rc = d2d(h, a->sFv + k * nv3, h->Fv, 4 * nv3))) return rc;
+        if ((rc = clear_force_bits(h, h->stream))) return rc;
         if ((rc = launch_spread_stage(h))) return rc;
-        if ((rc = d2d(h, a->sF + k * 3 * n, h->Fx, 4 * n))) return rc;
-        if ((rc = d2d(h, a->sF + k * 3 * n + n, h->Fy, 4 * n))) return rc;
-        if ((rc = d2d(h, a->sF + k * 3 * n + 2 * n, h->Fz, 4 * n))) return rc;
+        launch_force_to_f32(h->geo, h->Fint, a->sF + k * 3 * n, h->stream);   // the force the collision reads
+        h->launches++;
+        CK_LAUNCH();
         if ((rc = launch_lbm_stage(h))) return rc;
         if ((rc = d2d(h, a->suvr + k * n, h->uvr, 16 * n))) return rc;
         if ((rc = launch_advect_stage(h))) return rc;
@@ -2215,6 +2247,42 @@ int adjoint_launch_graph(rbc_handle *h, int kind, int b, int parity, int len)
     return RBC_OK;
 }
 
+// N(s, r) = C(s + r + 1, s + 1), saturated at 2^40
+long long binomial_units(int s, int r)
+{
+    long double v = 1.0L;
+    for (int i = 1; i <= s + 1; i++) {
+        v = v * (long double)(r + i) / (long double)i;
+        if (v > 1e12L) return 1LL << 40;
+    }
+    return (long long)(v + 0.5L);
+}
+
+// the actions that reverse units [a, b) when the state at a is the current
+// one and is held in slot sa, with s free slots above sa
+void binomial_plan(int a, int b, int s, int sa, std::vector<AdjAction> &out)
+{
+    const int n = b - a;
+    if (n == 1) { out.push_back({ADJ_RECORD, a}); out.push_back({ADJ_REVERSE, a}); return; }
+    if (s == 0) {
+        for (int t = b - 1; t >= a; t--) {
+            if (t != b - 1) out.push_back({ADJ_RESTORE, sa});
+            if (t > a) out.push_back({ADJ_ADVANCE, t - a});
+            out.push_back({ADJ_RECORD, t});
+            out.push_back({ADJ_REVERSE, t});
+        }
+        return;
+    }
+    int r = 0;
+    while (binomial_units(s, r) < n) r++;
+    const int m = a + (int)binomial_units(s, r - 1);
+    out.push_back({ADJ_ADVANCE, m - a});
+    out.push_back({ADJ_SNAP, sa + 1});
+    binomial_plan(m, b, s - 1, sa + 1, out);
+    out.push_back({ADJ_RESTORE, sa});
+    binomial_plan(a, m, s, sa, out);
+}
+
 int adjoint_supported(rbc_handle *h)
 {
     if (h->p.storage != RBC_STORE_F32) return fail(h, RBC_ERR_UNSUPPORTED, "the adjoint needs FP32 population storage");
@@ -2242,6 +2310,7 @@ int rbc_adjoint_record(rbc_handle *h, int nsteps, int ckpt_every)
     AdjointState *a = h->adj;
     if (a->K != K) adjoint_drop_graphs(a);   // the graphs index the stores by K
     a->valid = false;
+    a->mode = 0;
     a->K = K; a->nsteps = nsteps; a->nseg = nseg;
     a->ck_iter.assign(nseg + 1, 0);
     CK(cudaStreamSynchronize(h->stream));
@@ -2259,6 +2328,92 @@ int rbc_adjoint_record(rbc_handle *h, int nsteps, int ckpt_every)
     if ((rc = d2d(h, a->fin_Fv, h->Fv, 4 * nv3))) return rc;
     CK(cudaStreamSynchronize(h->stream));
     a->valid = true;
+    return RBC_OK;
+}
+
+int rbc_adjoint_record_binomial(rbc_handle *h, int nsteps, int unit, int snaps)
+{
+    if (!h || nsteps < 1 || unit < 1 || snaps < 0) return RBC_ERR_ARG;
+    RBC_DEVICE_GUARD(h);
+    int rc;
+    if ((rc = adjoint_supported(h))) return rc;
+    const int K = std::min(unit, nsteps), U = (nsteps + K - 1) / K;
+    const int S = std::min(snaps, U - 1);
+    // slots 0 (the initial state) .. S, and S + 1 for the state after the run
+    if ((rc = adjoint_reserve(h, K, S + 1))) return rc;
+    AdjointState *a = h->adj;
+    if (a->K != K) adjoint_drop_graphs(a);
+    a->valid = false;
+    a->mode = 1;
+    a->K = K; a->nsteps = nsteps; a->nunits = U; a->snaps = S; a->final_slot = S + 1;
+    a->ck_iter.assign(S + 2, 0);
+    std::vector<AdjAction> full;
+    binomial_plan(0, U, S, 0, full);
+    CK(cudaStreamSynchronize(h->stream));
+    if ((rc = prepare_steps(h))) return rc;
+    // the forward run takes the snapshots the schedule takes before its first
+    // recording, then runs to the end
+    auto steps_of = [&](int u0, int u) { return std::min((long long)(u0 + u) * K, (long long)nsteps) - (long long)u0 * K; };
+    if ((rc = adjoint_save(h, 0))) return rc;
+    int pos = 0, last_snap = 0, snap_pos = 0;
+    size_t i = 0;
+    for (; i < full.size() && full[i].op != ADJ_RECORD; i++) {
+        if (full[i].op == ADJ_ADVANCE) {
+            if ((rc = rbc_step(h, (int)steps_of(pos, full[i].arg)))) return rc;
+            pos += full[i].arg;
+        } else {   // ADJ_SNAP
+            if ((rc = adjoint_save(h, full[i].arg))) return rc;
+            last_snap = full[i].arg;
+            snap_pos = pos;
+        }
+    }
+    if ((rc = rbc_step(h, (int)steps_of(pos, U - pos)))) return rc;
+    if ((rc = adjoint_save(h, a->final_slot))) return rc;
+    // the backward sweep restarts from the last snapshot, replays the advances
+    // taken after it, then follows the schedule
+    a->plan.clear();
+    a->plan.push_back({ADJ_RESTORE, last_snap});
+    for (size_t j = 0; j < i; j++) {
+        if (full[j].op != ADJ_ADVANCE) continue;
+        int before = 0;   // position before this advance
+        for (size_t k2 = 0; k2 < j; k2++) if (full[k2].op == ADJ_ADVANCE) before += full[k2].arg;
+        if (before >= snap_pos) a->plan.push_back(full[j]);
+    }
+    a->plan.insert(a->plan.end(), full.begin() + i, full.end());
+    const size_t nv3 = 3 * (size_t)h->nv;
+    if ((rc = d2d(h, a->fin_uvr, h->uvr, 16 * (size_t)h->geo.nint))) return rc;
+    if ((rc = d2d(h, a->fin_U, h->U, 4 * nv3))) return rc;
+    if ((rc = d2d(h, a->fin_Fv, h->Fv, 4 * nv3))) return rc;
+    CK(cudaStreamSynchronize(h->stream));
+    a->valid = true;
+    return RBC_OK;
+}
+
+int rbc_adjoint_binomial_plan(int units, int snaps, int *ops, int *args, int cap, int *len)
+{
+    if (units < 1 || snaps < 0 || !len || (cap > 0 && (!ops || !args))) return RBC_ERR_ARG;
+    std::vector<AdjAction> plan;
+    plan.push_back({ADJ_SNAP, 0});   // the initial state in slot 0
+    binomial_plan(0, units, std::min(snaps, units - 1), 0, plan);
+    *len = (int)plan.size();
+    if ((int)plan.size() > cap) return cap > 0 ? RBC_ERR_ARG : RBC_OK;
+    for (size_t i = 0; i < plan.size(); i++) { ops[i] = plan[i].op; args[i] = plan[i].arg; }
+    return RBC_OK;
+}
+
+int rbc_adjoint_schedule(const rbc_handle *h, int *units, int *unit_steps, int *snapshots, long long *advances)
+{
+    if (!h || !h->adj || !h->adj->valid) return RBC_ERR_STATE;
+    const AdjointState *a = h->adj;
+    if (units) *units = a->mode == 1 ? a->nunits : a->nseg;
+    if (unit_steps) *unit_steps = a->K;
+    if (snapshots) *snapshots = a->mode == 1 ? a->snaps + 1 : a->nseg + 1;
+    if (advances) {
+        long long adv = 0;
+        if (a->mode == 1)
+            for (const AdjAction &x : a->plan) if (x.op == ADJ_ADVANCE) adv += x.arg;
+        *advances = adv;
+    }
     return RBC_OK;
 }
 
@@ -2286,28 +2441,71 @@ int rbc_adjoint_backward(rbc_handle *h, const double *xbar, const double *ybar, 
     CK(cudaMemsetAsync(a->gbar[0], 0, 4 * nq, h->stream));
     CK(cudaMemsetAsync(a->pbar, 0, 4 * sizeof(double), h->stream));
     CK(cudaMemsetAsync(a->status, 0, sizeof(int), h->stream));
-    // the adjoint stream starts after the initialisation; store 1 starts drained
+    // the adjoint stream starts after the initialisation; both stores start drained
+    CK(cudaEventRecord(a->drained[0], h->stream));
     CK(cudaEventRecord(a->drained[1], h->stream));
-    auto seg_len = [&](int s) { return std::min(a->K, a->nsteps - s * a->K); };
     int gb = 0;
-    // segment s uses store (nseg - 1 - s) & 1
-    if ((rc = adjoint_restore(h, a->nseg - 1))) return rc;
-    if ((rc = adjoint_launch_graph(h, 0, 0, h->cur, seg_len(a->nseg - 1)))) return rc;
-    CK(cudaEventRecord(a->filled[0], h->stream));
-    for (int s = a->nseg - 1; s >= 0; s--) {
-        const int b = (a->nseg - 1 - s) & 1;
-        CK(cudaStreamWaitEvent(a->rev, a->filled[b], 0));
-        if ((rc = adjoint_launch_graph(h, 1, b, gb, seg_len(s)))) return rc;
-        gb ^= seg_len(s) & 1;
-        CK(cudaEventRecord(a->drained[b], a->rev));
-        if (s > 0) {   // recompute segment s - 1 into the other store while segment s is reversed
-            CK(cudaStreamWaitEvent(h->stream, a->drained[b ^ 1], 0));
-            if ((rc = adjoint_restore(h, s - 1))) return rc;
-            if ((rc = adjoint_launch_graph(h, 0, b ^ 1, h->cur, seg_len(s - 1)))) return rc;
-            CK(cudaEventRecord(a->filled[b ^ 1], h->stream));
+    if (a->mode == 1) {
+        // binomial schedule: recordings alternate between the two stores, so the
+        // recording of a unit (handle stream) runs while the unit recorded
+        // before it is reversed (adjoint stream)
+        auto unit_len = [&](int t) { return std::min(a->K, a->nsteps - t * a->K); };
+        int pos = 0, nrec = 0, store = 0, last_store = 0;
+        for (const AdjAction &x : a->plan) {
+            switch (x.op) {
+            case ADJ_RESTORE:
+                if ((rc = adjoint_restore(h, x.arg))) return rc;
+                pos = a->ck_iter[x.arg] - a->ck_iter[0];
+                pos = pos / a->K;
+                break;
+            case ADJ_SNAP:
+                if ((rc = adjoint_save(h, x.arg))) return rc;
+                break;
+            case ADJ_ADVANCE: {
+                const int steps = std::min((pos + x.arg) * a->K, a->nsteps) - pos * a->K;
+                if ((rc = rbc_step(h, steps))) return rc;
+                pos += x.arg;
+                break;
+            }
+            case ADJ_RECORD:
+                store = nrec++ & 1;
+                CK(cudaStreamWaitEvent(h->stream, a->drained[store], 0));
+                if ((rc = adjoint_launch_graph(h, 0, store, h->cur, unit_len(x.arg)))) return rc;
+                CK(cudaEventRecord(a->filled[store], h->stream));
+                pos = x.arg + 1;
+                last_store = store;
+                break;
+            case ADJ_REVERSE:
+                CK(cudaStreamWaitEvent(a->rev, a->filled[last_store], 0));
+                if ((rc = adjoint_launch_graph(h, 1, last_store, gb, unit_len(x.arg)))) return rc;
+                gb ^= unit_len(x.arg) & 1;
+                CK(cudaEventRecord(a->drained[last_store], a->rev));
+                break;
+            }
         }
+        CK(cudaStreamWaitEvent(h->stream, a->drained[0], 0));
+        CK(cudaStreamWaitEvent(h->stream, a->drained[1], 0));
+    } else {
+        auto seg_len = [&](int s) { return std::min(a->K, a->nsteps - s * a->K); };
+        // segment s uses store (nseg - 1 - s) & 1
+        if ((rc = adjoint_restore(h, a->nseg - 1))) return rc;
+        if ((rc = adjoint_launch_graph(h, 0, 0, h->cur, seg_len(a->nseg - 1)))) return rc;
+        CK(cudaEventRecord(a->filled[0], h->stream));
+        for (int s = a->nseg - 1; s >= 0; s--) {
+            const int b = (a->nseg - 1 - s) & 1;
+            CK(cudaStreamWaitEvent(a->rev, a->filled[b], 0));
+            if ((rc = adjoint_launch_graph(h, 1, b, gb, seg_len(s)))) return rc;
+            gb ^= seg_len(s) & 1;
+            CK(cudaEventRecord(a->drained[b], a->rev));
+            if (s > 0) {   // recompute segment s - 1 into the other store while segment s is reversed
+                CK(cudaStreamWaitEvent(h->stream, a->drained[b ^ 1], 0));
+                if ((rc = adjoint_restore(h, s - 1))) return rc;
+                if ((rc = adjoint_launch_graph(h, 0, b ^ 1, h->cur, seg_len(s - 1)))) return rc;
+                CK(cudaEventRecord(a->filled[b ^ 1], h->stream));
+            }
+        }
+        CK(cudaStreamWaitEvent(h->stream, a->drained[(a->nseg - 1) & 1], 0));
     }
-    CK(cudaStreamWaitEvent(h->stream, a->drained[(a->nseg - 1) & 1], 0));
     CK(cudaEventRecord(e1, h->stream));
     double pb[4];
     int st = 0;
@@ -2330,7 +2528,7 @@ int rbc_adjoint_backward(rbc_handle *h, const double *xbar, const double *ybar, 
     if (adj_flags) *adj_flags = st;
     if (ms) *ms = t;
     // leave the handle at the end of the recorded run
-    if ((rc = adjoint_restore(h, a->nseg))) return rc;
+    if ((rc = adjoint_restore(h, a->mode == 1 ? a->final_slot : a->nseg))) return rc;
     if ((rc = d2d(h, h->uvr, a->fin_uvr, 16 * n))) return rc;
     if ((rc = d2d(h, h->U, a->fin_U, 4 * nv3))) return rc;
     if ((rc = d2d(h, h->Fv, a->fin_Fv, 4 * nv3))) return rc;
@@ -2351,6 +2549,30 @@ int rbc_set_coefficients(rbc_handle *h, double P, double B, double C)
         h->adj->valid = false;
         adjoint_drop_graphs(h->adj);
     }
+    return RBC_OK;
+}
+
+int rbc_set_launch_shape(rbc_handle *h, int what, int value)
+{
+    if (!h) return RBC_ERR_ARG;
+    if (what != RBC_SHAPE_LBM_PLANES) return fail(h, RBC_ERR_ARG, "unknown launch shape");
+    if (value != 0 && value != 1 && value != 2 && value != 4 && value != 8)
+        return fail(h, RBC_ERR_ARG, "RBC_SHAPE_LBM_PLANES takes 0 (automatic), 1, 2, 4 or 8");
+    RBC_DEVICE_GUARD_RO(h);
+    if (value == h->lbm_planes) return RBC_OK;
+    CK(cudaStreamSynchronize(h->stream));
+    h->lbm_planes = value;
+    // the step graphs hold the launch configuration
+    for (auto &form : h->graph)
+        for (cudaGraphExec_t &g : form) if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    if (h->adj) adjoint_drop_graphs(h->adj);
+    return RBC_OK;
+}
+
+int rbc_get_launch_shape(const rbc_handle *h, int what, int *value)
+{
+    if (!h || !value || what != RBC_SHAPE_LBM_PLANES) return RBC_ERR_ARG;
+    *value = h->lbm_planes;
     return RBC_OK;
 }
 

@@ -8,7 +8,9 @@
 //   macroscopic  uvr[z][y][x] float4 (u, v, w, rho): the reference's um/vm/wm
 //                (M = 1, with the half-force shift) and dn, interleaved so one
 //                16-byte load serves an interpolation stencil point.
-//   IB force     Fx, Fy, Fz [z][y][x] FP32; the LBM kernel zeroes what it read.
+//   IB force     F[3][z][y][x] int64 fixed point (ForceField) with one
+//                occupancy bit per node; the LBM kernel converts, reads and
+//                zeroes the nodes whose bit is set, and clears the bits.
 //   wall mask    mask2d[y][x] uint32: bit 31 = fluid column, bit q = the pull
 //                source of direction q is a wall (half-way bounce-back).  The
 //                reference channel is z-invariant, so one plane serves all z.
@@ -90,19 +92,40 @@ __device__ __forceinline__ void delta4(float f, float w[4]) {
     w[3] = 0.25f * (1.0f - c);
 }
 
+// IB force on the lattice: the three components as int64 fixed point
+// F * 2^FORCE_FRAC in arrays [3][nint], and one occupancy bit per node in words
+// [nzc][wpp] (word xy / 32 of plane z, bit xy % 32) that the spread sets for every
+// node it adds to.  Integer sums are exact, so the spread's result does not depend
+// on the order of its global atomics (several patches and cells add to a node).
+// The collide-stream kernel reads, converts (one rounding to FP32) and zeroes the
+// nodes whose bit is set, so only nodes near membranes cost force traffic; the
+// words are cleared (a memset) before each step's spread.  Sums are exact while |F| < 2^(63 - FORCE_FRAC) = 128 at
+// every node (partial sums may wrap; the adds are modular); a contribution of
+// 64 or more raises RBC_FLAG_NONFINITE (a lattice force density of that size
+// has long broken the LBM).
+constexpr int FORCE_FRAC = 56;
+struct ForceField {
+    long long *F;              // [3][nint]
+    uint32_t *bits;            // [nzc][wpp]
+    int wpp;                   // occupancy words per plane, ceil(plane / 32)
+};
+__host__ __device__ constexpr int force_words_per_plane(long long plane) { return (int)((plane + 31) / 32); }
+
 // ---- launchers (defined in the .cu files, called by rbc_abi.cu) ----------
 
 struct LbmArgs {
     const void *gin; void *gout;
     float4 *uvr;
-    float *Fx, *Fy, *Fz;
+    ForceField F;              // read, converted and zeroed where the occupancy bit is set
     const uint32_t *mask2d;
     const float *drive;        // device scalar: P * drive factor of this step
+    const int *iter;           // device: the step counter, which seeds the FP16 stochastic rounding
     const float *wall;         // device [2]: z velocity of the top and bottom walls (shear mode), else NULL
     const double *vf;          // volume fraction: omega = 1 / (df3 (1 + lm1 vf) + 1/2) per node; NULL: omega
     float lm1, df3;            // LAMBDA1 - 1 and 3 Df (lbm.cu:1131)
     float omega, Cr, Bc;
     float scale, inv_scale;    // FP16 storage scale
+    int planes;                // z planes per thread; 0 = chosen from the lattice size
 };
 void launch_lbm(const Geom &g, int storage, const LbmArgs &a, cudaStream_t s);
 // z velocities of the top and bottom walls in the next step (shear mode; 0 otherwise)
@@ -117,8 +140,9 @@ void launch_export_lattice(const Geom &g, int storage, const void *gin, const ui
 // links[k] = xy * 32 + p (pull direction p, wall at i - e_p), frac[k] = crossing fraction.
 void launch_tube_bounce(const Geom &g, int storage, void *gout, const int *links, const float *frac, int nlinks,
                         float inv_scale, float scale, cudaStream_t s);
-void launch_export_force(const Geom &g, const float *Fx, const float *Fy, const float *Fz,
-                         const uint32_t *mask2d, double *out3, cudaStream_t s);
+void launch_export_force(const Geom &g, const long long *F, const uint32_t *mask2d, double *out3, cudaStream_t s);
+// the lattice force as FP32 [3][nint] (the value the collide-stream kernel reads)
+void launch_force_to_f32(const Geom &g, const long long *F, float *out3, cudaStream_t s);
 void launch_fill_f32(float *p, long long n, float v, cudaStream_t s);
 void launch_fill_f4(float4 *p, long long n, float4 v, cudaStream_t s);
 
@@ -176,7 +200,7 @@ struct SpreadArgs {
     const int *patch_off, *patch_vtx, *patch_stride;   // surface patches of the shared mesh
     int npatch;
     const float *Fv;
-    float *Fx, *Fy, *Fz;
+    ForceField F;
     const uint32_t *mask2d;
     int *flags;
 };
@@ -344,5 +368,50 @@ __host__ __device__ __forceinline__ int v2e_elem(int p) { return p & 0xFFFFFF; }
 __host__ __device__ __forceinline__ int v2e_en(int p) { return (p >> 24) & 3; }
 __host__ __device__ __forceinline__ int v2e_sa(int p) { return (p >> 26) & 7; }
 __host__ __device__ __forceinline__ int v2e_sb(int p) { return (p >> 29) & 7; }
+
+// ---- fused batches: one launch per stage for many simulations -------------
+//
+// Every simulation of a fused batch is a "domain": its geometry and the
+// arguments of each stage kernel, exactly as its own handle would launch them
+// (one buffer parity).  A fused launch runs the blocks of all domains of one
+// stage: block b belongs to the domain d with boff[d] <= b < boff[d + 1] and is
+// that domain's block b - boff[d].  The kernels run the same device code as the
+// one-simulation launches, so a fused step equals each simulation's own step
+// bit for bit.
+struct DomainArgs {
+    Geom g;
+    StepBeginArgs sb;
+    ForceField F;
+    MembraneArgs mem;
+    SpreadArgs spread;
+    LbmArgs lbm;
+    int lbm_bx, lbm_gy;        // collide-stream: column tiles per plane, plane stride (tiles along z)
+    AdvectArgs adv;
+    VolumeArgs vol;
+};
+struct FusedLaunch {
+    const DomainArgs *dom;     // device [ndom]
+    const int *boff;           // device [ndom + 1]
+    int ndom, nblocks;
+};
+__device__ __forceinline__ int fused_domain(const int *__restrict__ boff, int ndom, int b)
+{
+    int lo = 0, hi = ndom;     // the last domain whose first block is at or before b
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (__ldg(&boff[mid]) <= b) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+constexpr int FUSED_CLEAR_THREADS = 256;
+void launch_step_begin_fused(const FusedLaunch &f, cudaStream_t s);   // one thread per domain
+void launch_clear_bits_fused(const FusedLaunch &f, cudaStream_t s);   // FUSED_CLEAR_THREADS words per block
+void launch_membrane_fused(const FusedLaunch &f, bool fp64, int V, int vpt, cudaStream_t s);   // a block per cell
+void launch_spread_fused(const FusedLaunch &f, bool xper, cudaStream_t s);    // a block per (cell, patch)
+void launch_lbm_fused(const FusedLaunch &f, int storage, bool off32, int threads, cudaStream_t s);
+void launch_advect_fused(const FusedLaunch &f, bool xper, cudaStream_t s);    // a block per (cell, patch)
+void launch_volume_fused(const FusedLaunch &f, int V, cudaStream_t s);        // a block per cell
+int  membrane_threads(int V, int vpt);     // threads of a membrane block with vpt vertices per thread
+int  membrane_default_vpt(int V);          // the vertices per thread of a one-population launch
 
 }  // namespace rbc

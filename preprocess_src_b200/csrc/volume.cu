@@ -53,13 +53,13 @@ __device__ __forceinline__ void ele_normal(const double *__restrict__ p, int V, 
     vt = 1.0 / 3.0 * (rx * n[0] + ry * n[1] + rz * n[2]) * dS;
 }
 
-__global__ void __launch_bounds__(VOL_THREADS)
-volume_kernel(const Geom g, const VolumeArgs a)
+// cell: the block's cell, blockIdx.x of a one-population launch
+__device__ __forceinline__ void volume_body(const Geom &g, const VolumeArgs &a, int cell)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ double red[32];
     double *p = reinterpret_cast<double *>(smem);   // [3][V]
-    const int V = a.V, E = a.E, tid = threadIdx.x, T = blockDim.x, cell = blockIdx.x, N = a.ncell;
+    const int V = a.V, E = a.E, tid = threadIdx.x, T = blockDim.x, N = a.ncell;
     const long long vb = (long long)cell * V, nv = a.nv;
     const double gz = a.gx[2 * N + cell], gxx = a.gx[cell];
     for (int v = tid; v < V; v += T) {
@@ -146,6 +146,12 @@ volume_kernel(const Geom g, const VolumeArgs a)
     }
 }
 
+__global__ void __launch_bounds__(VOL_THREADS)
+volume_kernel(const Geom g, const VolumeArgs a)
+{
+    volume_body(g, a, blockIdx.x);
+}
+
 void launch_volume(const Geom &g, const VolumeArgs &a, cudaStream_t s)
 {
     if (a.ncell <= 0) return;
@@ -158,6 +164,9 @@ cudaError_t spread_setup();
 cudaError_t advect_setup();
 cudaError_t adjoint_setup(int optin);
 cudaError_t vof_setup();
+cudaError_t membrane_fused_setup(int optin);
+cudaError_t ibm_fused_setup();
+cudaError_t volume_fused_setup(int optin);
 
 // Dynamic shared memory limit of a kernel: the device's per-block opt-in
 // maximum minus the kernel's static shared memory.
@@ -184,10 +193,13 @@ int setup_kernel_attributes(int *membrane_max_smem)
     if ((e = advect_setup()) != cudaSuccess) return (int)e;
     if ((e = adjoint_setup(optin)) != cudaSuccess) return (int)e;
     if ((e = vof_setup()) != cudaSuccess) return (int)e;
+    if ((e = membrane_fused_setup(optin)) != cudaSuccess) return (int)e;
+    if ((e = ibm_fused_setup()) != cudaSuccess) return (int)e;
+    if ((e = volume_fused_setup(optin)) != cudaSuccess) return (int)e;
     return 0;
 }
 
-__global__ void step_begin_kernel(const StepBeginArgs a)
+__device__ __forceinline__ void step_begin_body(const StepBeginArgs &a)
 {
     const int it = *a.iter + 1;
     *a.iter = it;
@@ -202,9 +214,61 @@ __global__ void step_begin_kernel(const StepBeginArgs a)
     }
 }
 
+__global__ void step_begin_kernel(const StepBeginArgs a)
+{
+    step_begin_body(a);
+}
+
 void launch_step_begin(const StepBeginArgs &a, cudaStream_t s)
 {
     step_begin_kernel<<<1, 1, 0, s>>>(a);
+}
+
+// ---- fused batches ---------------------------------------------------------
+
+__global__ void step_begin_fused_kernel(const DomainArgs *__restrict__ dom, int ndom)
+{
+    const int d = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d < ndom) step_begin_body(dom[d].sb);
+}
+
+void launch_step_begin_fused(const FusedLaunch &f, cudaStream_t s)
+{
+    step_begin_fused_kernel<<<(f.ndom + 127) / 128, 128, 0, s>>>(f.dom, f.ndom);
+}
+
+// occupancy words of every domain's lattice force to zero (the memset of a
+// one-simulation step)
+__global__ void __launch_bounds__(FUSED_CLEAR_THREADS)
+clear_bits_fused_kernel(const DomainArgs *__restrict__ dom, const int *__restrict__ boff, int ndom)
+{
+    const int d = fused_domain(boff, ndom, blockIdx.x);
+    const DomainArgs &D = dom[d];
+    const long long w = (long long)(blockIdx.x - boff[d]) * FUSED_CLEAR_THREADS + threadIdx.x;
+    if (w < (long long)D.g.nzc * D.F.wpp) D.F.bits[w] = 0u;
+}
+
+void launch_clear_bits_fused(const FusedLaunch &f, cudaStream_t s)
+{
+    if (f.nblocks > 0) clear_bits_fused_kernel<<<f.nblocks, FUSED_CLEAR_THREADS, 0, s>>>(f.dom, f.boff, f.ndom);
+}
+
+__global__ void __launch_bounds__(VOL_THREADS)
+volume_fused_kernel(const DomainArgs *__restrict__ dom, const int *__restrict__ boff, int ndom)
+{
+    const int d = fused_domain(boff, ndom, blockIdx.x);
+    volume_body(dom[d].g, dom[d].vol, blockIdx.x - boff[d]);
+}
+
+cudaError_t volume_fused_setup(int optin)
+{
+    return set_max_dyn_smem((const void *)volume_fused_kernel, optin, nullptr);
+}
+
+void launch_volume_fused(const FusedLaunch &f, int V, cudaStream_t s)
+{
+    if (f.nblocks > 0)
+        volume_fused_kernel<<<f.nblocks, VOL_THREADS, volume_smem_bytes(V), s>>>(f.dom, f.boff, f.ndom);
 }
 
 }  // namespace rbc

@@ -249,6 +249,20 @@ class Simulation:
         """Run nsteps steps keeping a checkpoint every ckpt_every steps."""
         self._call("rbc_adjoint_record", int(nsteps), int(ckpt_every))
 
+    def adjoint_record_binomial(self, nsteps: int, unit: int = 1, snapshots: int = 16):
+        """Run nsteps steps for a reverse sweep under binomial checkpointing:
+        units of `unit` steps, `snapshots` snapshot slots beside the initial
+        state."""
+        self._call("rbc_adjoint_record_binomial", int(nsteps), int(unit), int(snapshots))
+
+    def adjoint_schedule(self) -> dict:
+        """The recorded run's schedule: units, steps per unit, snapshot slots
+        (the initial state's included) and units advanced without recording in
+        one backward sweep (binomial schedule; 0 for the fixed interval)."""
+        u, k, sn, adv = C.c_int(0), C.c_int(0), C.c_int(0), C.c_longlong(0)
+        self._call("rbc_adjoint_schedule", C.byref(u), C.byref(k), C.byref(sn), C.byref(adv))
+        return {"units": u.value, "unit_steps": k.value, "snapshots": sn.value, "advanced_units": adv.value}
+
     def adjoint_backward(self, xbar, ybar, zbar, want_x0: bool = False) -> dict:
         """Reverse sweep of the recorded run from dL/d(final cel->x, y, z).
         Returns grad (dL/dP, dL/dB, dL/dC), flags, ms and, with want_x0,
@@ -265,6 +279,15 @@ class Simulation:
         if want_x0:
             r["dx0"] = x0
         return r
+
+    # -- launch shapes (speed only; results do not depend on them) -------------
+    def set_launch_shape(self, what: int, value: int):
+        self._call("rbc_set_launch_shape", int(what), int(value))
+
+    def launch_shape(self, what: int) -> int:
+        v = C.c_int(0)
+        self._call("rbc_get_launch_shape", int(what), C.byref(v))
+        return v.value
 
     # -- diagnostics ----------------------------------------------------------
     def status(self) -> tuple[int, int]:

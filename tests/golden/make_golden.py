@@ -8,7 +8,15 @@ oracle/ref_harness (def.h stand-in, helper shims, driver).
 
     python tests/golden/make_golden.py build [CASE...]          # here: nvcc, needs the reference sources
     python tests/golden/make_golden.py run OUTDIR [CASE...]     # on a GPU: writes OUTDIR/<case>.npz
+    python tests/golden/make_golden.py run-dense OUTDIR         # on a GPU: OUTDIR/c2_dense_suspension.npz
     python tests/golden/make_golden.py time-dense       # on a GPU: reference step timing, dense suspension
+
+OUTDIR defaults to tests/golden, where the committed fixtures live.
+
+The dense-suspension fixture (256 x 128 x 128, 200 cells) keeps a seeded
+sample of its nodes and vertices (dense_sample), the per-plane sums of the
+velocity over COMP nodes and the per-cell centroids after DENSE_SNAPSHOTS
+steps: the full fields would not fit a repository.
 
 g4 runs the volume fraction (front tracking every K = 10 steps, THINC/WLIC
 every step) with viscosity ratio LAMBDA1 = 5: fronttrack.cu and thincwlic.cu
@@ -65,7 +73,47 @@ def golden_cases():
                                                     seed=24, g=4e-5, Gs=2e-3, residual=1e-12, itrmax=20000,
                                                     lambda1=5.0, vof_k=10, vof_residual=1e-12,
                                                     vof_itrmax=20000),
+        # shear flow (CapsuleSHEARFLOW), both walls moving: one cell across the
+        # periodic x boundary, one inside
+        "g5_shear24x20x24_2c": configs.shear_case("g5_shear24x20x24_2c", 24, 20, 24,
+                                                  centers=[(11.2, 0.4, -3.1), (-2.0, -0.6, 6.3)], sr=4e-3,
+                                                  walls=0, subdiv=3, radius=5.0, seed=25, Gs=2e-3,
+                                                  residual=1e-12),
+        # shear flow with the top wall moving only (topwall)
+        "g6_shear20x16x20_1c_top": configs.shear_case("g6_shear20x16x20_1c_top", 20, 16, 20,
+                                                      centers=[(0.3, -0.4, 0.6)], sr=5e-3, walls=1, subdiv=3,
+                                                      radius=4.5, seed=26, Gs=2e-3, residual=1e-12),
+        # one red cell and one white cell (N_W = 1, GSw / GS = 2.5, BRw = 0.02) on
+        # the same mesh; fixtures hold the red cells' arrays followed by the
+        # white cells' (the layout of the two-cell case)
+        "g7_duct32x20x20_1r1w": _with_wbc(configs.duct_case("g7_duct32x20x20_1r1w", 32, 20, 20,
+                                                            centers_duct=[(8.2, 9.6, 9.4), (23.9, 9.3, 9.7)],
+                                                            subdiv=3, radius=5.0, seed=27, g=4e-5, Gs=2e-3,
+                                                            residual=1e-12), nred=1, rgs=2.5, br=0.02),
     }
+
+
+def _with_wbc(case, nred, rgs, br):
+    """case with its cells after the first nred as white cells (GSw / GS = rgs,
+    BRw = br): case.meta["wbc"] = (nred, rgs, br)."""
+    case.meta["wbc"] = (nred, float(rgs), float(br))
+    return case
+
+
+def wbc_split(case):
+    """(red case, white case, rgs, br) of a golden case with white cells, else None."""
+    if "wbc" not in case.meta:
+        return None
+    nred, rgs, br = case.meta["wbc"]
+    red, white = configs.split_cells(case, nred)
+    return red, white, rgs, br
+
+
+def cell_coefficients(case):
+    """Per-cell (rgs, br) lists of the two-cell oracle run of a white-cell case."""
+    nred, rgs, br = case.meta["wbc"]
+    nw = case.ncell - nred
+    return [1.0] * nred + [rgs] * nw, [case.params["br"]] * nred + [br] * nw
 
 
 def snapshots(case):
@@ -78,22 +126,51 @@ def dense_case():
     return configs.dense_suspension(residual=1e-12)
 
 
+DENSE_SNAPSHOTS = (2, 30)
+
+
+def dense_sample(case, nodes=16384, verts=8192, seed=77):
+    """Seeded sample of COMP node indices and vertex indices of the dense
+    suspension, sorted (the same on every machine: numpy's PCG64)."""
+    rng = np.random.default_rng(seed)
+    comp = np.flatnonzero(case.bc == configs.COMP)
+    n = np.sort(rng.choice(comp, size=nodes, replace=False))
+    v = np.sort(rng.choice(case.ncell * case.vertex, size=verts, replace=False))
+    return n, v
+
+
 def ref_defs(case) -> str:
     p = case.params
     df = (2.0 * p["tau"] - 1.0) / 6.0
-    return (f"-DREF_LX={p['LX']!r} -DREF_LY={float(p['ny'] - 4)!r} -DREF_LZ={p['LZ']!r} -DREF_P={p['P']!r} "
-            f"-DREF_B={p['B']!r} -DREF_C={p['C']!r} -DREF_DF={df!r} -DREF_RESIDUAL={p['residual']!r} "
-            f"-DREF_ITRMAX={p['itrmax']} -DREF_BR={p['br']!r} -DREF_LAMBDA1={p['lambda1']!r} "
-            f"-DREF_K={p['vof_k'] if p['vof_k'] > 0 else 1000000000}")
+    d = (f"-DREF_LX={p['LX']!r} -DREF_LY={float(p['ny'] - 4)!r} -DREF_LZ={p['LZ']!r} -DREF_P={p['P']!r} "
+         f"-DREF_B={p['B']!r} -DREF_C={p['C']!r} -DREF_DF={df!r} -DREF_RESIDUAL={p['residual']!r} "
+         f"-DREF_ITRMAX={p['itrmax']} -DREF_BR={p['br']!r} -DREF_LAMBDA1={p['lambda1']!r} "
+         f"-DREF_K={p['vof_k'] if p['vof_k'] > 0 else 1000000000} -DREF_FLOWSTART={p['flowstart']}")
+    if p["flow"] == 1:   # CapsuleSHEARFLOW
+        d += f" -DREF_SHEAR -DREF_SR={p['sr']!r}" + (" -DREF_TOPWALL" if p["walls"] == 1 else "")
+    if "wbc" in case.meta:
+        nred, rgs, br = case.meta["wbc"]
+        d += f" -DREF_NW={case.ncell - nred} -DREF_GSW={rgs!r} -DREF_BRW={br!r}"
+    return d
 
 
-def build(names=()):
-    for name, case in list(golden_cases().items()) + [("dense", dense_case())]:
+def bench_cases():
+    """The workloads bench.py's reference arm times with the reference's own
+    kernels: the dense suspension and the single-cell duct (tag -> Case)."""
+    return {"dense": dense_case(), "single": configs.single_cell_duct(residual=1e-12)}
+
+
+def build(names=(), if_present=False):
+    """Reference-kernel libraries of the golden and bench cases; if_present:
+    skip quietly when the reference sources are absent (the recipe checks)."""
+    for name, case in list(golden_cases().items()) + list(bench_cases().items()):
         if names and name not in names:
             continue
-        subprocess.run(["make", "-s", "-C", str(ROOT / "oracle"), "ref", f"REFTAG={name}",
+        target = "ref-if-present" if if_present else "ref"
+        subprocess.run(["make", "-s", "-C", str(ROOT / "oracle"), target, f"REFTAG={name}",
                         f"REFDEFS={ref_defs(case)}"], check=True)
-        print("built", REF_DIR / f"librefstep_{name}.so")
+        if (REF_DIR / f"librefstep_{name}.so").exists():
+            print("built", REF_DIR / f"librefstep_{name}.so")
 
 
 class Ref:
@@ -102,13 +179,24 @@ class Ref:
     def __init__(self, name, case):
         self.L = C.CDLL(str(REF_DIR / f"librefstep_{name}.so"))
         self.case = case
+        split = wbc_split(case)
+        self.red, self.white = (split[0], split[1]) if split else (case, None)
+        red = self.red
         bc = np.ascontiguousarray(case.bc, dtype=np.int32)
-        tri = np.ascontiguousarray(case.tri, dtype=np.int32).reshape(-1)
-        xr = np.ascontiguousarray(case.xr, dtype=np.float64)
-        rc = self.L.ref_setup(case.nx, case.ny, case.nz, bc.ctypes.data_as(C.c_void_p), case.ncell, case.vertex,
-                              case.element, tri.ctypes.data_as(C.c_void_p), xr.ctypes.data_as(C.c_void_p))
+        tri = np.ascontiguousarray(red.tri, dtype=np.int32).reshape(-1)
+        xr = np.ascontiguousarray(red.xr, dtype=np.float64)
+        rc = self.L.ref_setup(case.nx, case.ny, case.nz, bc.ctypes.data_as(C.c_void_p), red.ncell, red.vertex,
+                              red.element, tri.ctypes.data_as(C.c_void_p), xr.ctypes.data_as(C.c_void_p))
         if rc:
             raise RuntimeError(f"ref_setup failed: {rc}")
+        if self.white is not None:
+            w = self.white
+            triw = np.ascontiguousarray(w.tri, dtype=np.int32).reshape(-1)
+            xrw = np.ascontiguousarray(w.xr, dtype=np.float64)
+            rc = self.L.ref_setup_wbc(w.ncell, w.vertex, w.element, triw.ctypes.data_as(C.c_void_p),
+                                      xrw.ctypes.data_as(C.c_void_p))
+            if rc:
+                raise RuntimeError(f"ref_setup_wbc failed: {rc}")
         if case.params["vof_k"] > 0 and self.L.ref_vof_init():
             raise RuntimeError("reference vof_init failed")
 
@@ -129,13 +217,21 @@ class Ref:
         self.L.ref_get_lattice(None, p(out["dn"]), p(out["un"]), p(out["vn"]), p(out["wn"]), None, None, None)
         return out
 
-    def cells(self):
-        case = self.case
-        nv, nc = case.ncell * case.vertex, case.ncell
+    def _population(self, pop, getter):
+        nv, nc = pop.ncell * pop.vertex, pop.ncell
         keys = ("x", "y", "z", "u", "v", "w", "fx", "fy", "fz", "xd", "gx", "volume0", "nd")
-        sizes = (nv,) * 9 + (3 * nv, 3 * nc, nc, 4 * case.ncell * case.element)
+        sizes = (nv,) * 9 + (3 * nv, 3 * nc, nc, 4 * pop.ncell * pop.element)
         out = {k: np.empty(s) for k, s in zip(keys, sizes)}
-        self.L.ref_get_cells(*[out[k].ctypes.data_as(C.c_void_p) for k in keys])
+        getter(*[out[k].ctypes.data_as(C.c_void_p) for k in keys])
+        return out
+
+    def cells(self):
+        """Cell arrays of the case: the red cells', followed by the white cells'
+        when there are any."""
+        out = self._population(self.red, self.L.ref_get_cells)
+        if self.white is not None:
+            w = self._population(self.white, self.L.ref_get_wbc)
+            out = {k: np.concatenate([out[k], w[k]]) for k in out}
         return out
 
 
@@ -168,6 +264,32 @@ def run(outdir, names=()):
         print("wrote", outdir / f"{name}.npz")
 
 
+def run_dense(outdir):
+    outdir = Path(outdir)
+    outdir.mkdir(parents=True, exist_ok=True)
+    case = dense_case()
+    ref = Ref("dense", case)
+    m = case.bc == configs.COMP
+    nodes, verts = dense_sample(case)
+    data = {"snapshots": np.array(DENSE_SNAPSHOTS)}
+    done = 0
+    for s in DENSE_SNAPSHOTS:
+        t0 = time.perf_counter()
+        ref.step(s - done)
+        done = s
+        lat, cel = ref.lattice(), ref.cells()
+        for k in ("dn", "un", "vn", "wn"):
+            data[f"s{s}_{k}"] = lat[k][nodes]
+        data[f"s{s}_plane_u"] = np.stack([np.where(m, lat[k], 0.0).reshape(case.nz, -1).sum(axis=1)
+                                          for k in ("un", "vn", "wn")])
+        for k in ("x", "y", "z"):
+            data[f"s{s}_{k}"] = cel[k][verts]
+        data[f"s{s}_gx"] = cel["gx"]
+        print(f"dense: step {s} in {time.perf_counter() - t0:.1f} s", flush=True)
+    np.savez_compressed(outdir / "c2_dense_suspension.npz", **data)
+    print("wrote", outdir / "c2_dense_suspension.npz")
+
+
 def time_dense(steps=3):
     case = dense_case()
     ref = Ref("dense", case)
@@ -191,7 +313,9 @@ if __name__ == "__main__":
     if cmd == "build":
         build(sys.argv[2:])
     elif cmd == "run":
-        run(sys.argv[2] if len(sys.argv) > 2 else ROOT / "gpurun_out" / "golden", sys.argv[3:])
+        run(sys.argv[2] if len(sys.argv) > 2 else ROOT / "tests" / "golden", sys.argv[3:])
+    elif cmd == "run-dense":
+        run_dense(sys.argv[2] if len(sys.argv) > 2 else ROOT / "tests" / "golden")
     elif cmd == "time-dense":
         time_dense(int(sys.argv[2]) if len(sys.argv) > 2 else 3)
     else:

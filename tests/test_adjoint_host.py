@@ -40,3 +40,63 @@ def test_shape_loss_takes_the_minimum_image():
     x[1, 2] = 0.5           # y is not periodic
     L = shape_loss(x, t, 60.0, 64.0)
     assert abs(float(L) - (0.25 + 0.0625 + 0.25) / 4) < 1e-15
+
+
+def _plan(units, snaps):
+    import ctypes as C
+
+    from preprocess_src_b200 import _native as N
+    L = N.lib()
+    n = C.c_int(0)
+    assert L.rbc_adjoint_binomial_plan(units, snaps, None, None, 0, C.byref(n)) == N.RBC_OK
+    ops = (C.c_int * n.value)()
+    args = (C.c_int * n.value)()
+    assert L.rbc_adjoint_binomial_plan(units, snaps, ops, args, n.value, C.byref(n)) == N.RBC_OK
+    assert L.rbc_adjoint_binomial_plan(units, snaps, ops, args, n.value - 1, C.byref(n)) == N.RBC_ERR_ARG
+    return list(zip(ops, args))
+
+
+def _binomial(s, r):
+    from math import comb
+    return comb(s + r + 1, s + 1)
+
+
+@pytest.mark.parametrize("units,snaps", [(1, 4), (2, 0), (7, 0), (20, 1), (20, 3), (2000, 16), (2000, 5),
+                                         (255, 6), (100, 200)])
+def test_binomial_schedule_reverses_every_unit_once(native_lib, units, snaps):
+    """Simulate the schedule of rbc_adjoint_record_binomial: every unit is
+    recorded from its own state and reversed right after, in order from the
+    last to the first; a restore reads a slot that holds a state; at most
+    snaps + 1 slots are used; no unit is advanced more than r times, r the
+    least with C(snaps + r + 1, snaps + 1) >= units."""
+    plan = _plan(units, snaps)
+    s_eff = min(snaps, units - 1)
+    r = 0
+    while _binomial(s_eff, r) < units:
+        r += 1
+    pos, slots, reversed_, advanced = None, {}, [], [0] * units
+    last_recorded = None
+    for op, arg in plan:
+        if op == 1:      # keep the current state in slot arg
+            if pos is None:
+                pos = 0
+            assert 0 <= arg <= s_eff
+            slots[arg] = pos
+        elif op == 2:    # restore
+            assert arg in slots
+            pos = slots[arg]
+        elif op == 0:    # advance
+            assert arg >= 1 and pos + arg < units
+            for t in range(pos, pos + arg):
+                advanced[t] += 1
+            pos += arg
+        elif op == 3:    # record unit arg from the state at arg
+            assert pos == arg and last_recorded is None
+            last_recorded = arg
+            pos = arg + 1
+        else:            # reverse the unit just recorded
+            assert arg == last_recorded
+            reversed_.append(arg)
+            last_recorded = None
+    assert reversed_ == list(range(units - 1, -1, -1))
+    assert max(advanced) <= r, (max(advanced), r)

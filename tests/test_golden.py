@@ -11,7 +11,7 @@ from pathlib import Path
 import numpy as np
 import pytest
 
-from tests.golden.make_golden import golden_cases, snapshots
+from tests.golden.make_golden import cell_coefficients, golden_cases, snapshots
 from preprocess_src_b200 import configs
 
 GOLDEN = Path(__file__).resolve().parent / "golden"
@@ -28,7 +28,11 @@ def fixtures():
 @pytest.mark.parametrize("name,case", fixtures() or [pytest.param(None, None, marks=pytest.mark.skip("no fixtures"))])
 def test_oracle_matches_reference_kernels(name, case, oracle_mod):
     g = np.load(GOLDEN / f"{name}.npz")
-    o = oracle_mod.Oracle(case)
+    if "wbc" in case.meta:   # red and white cells: one oracle run with per-cell coefficients
+        rgs, br = cell_coefficients(case)
+        o = oracle_mod.Oracle(case, cell_rgs=rgs, cell_br=br)
+    else:
+        o = oracle_mod.Oracle(case)
     assert np.abs(o["nd"] - g["setup_nd"]).max() <= 1e-12 * np.abs(g["setup_nd"]).max()
     assert np.allclose(o["volume0"], g["setup_volume0"], rtol=1e-13)
     assert np.allclose(o["gx"], g["setup_gx"], rtol=0, atol=1e-12)

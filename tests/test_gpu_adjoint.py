@@ -211,3 +211,51 @@ def test_c5_shape_gradient_against_differences_and_fp64_reference(native_lib):
                   f"  oracle h=1e-4 {fx['grad_h1e4'][k]:.9e}")
         np.testing.assert_allclose(adj, ref, rtol=1e-4)
         np.testing.assert_allclose(adj, fd, rtol=3e-3)
+
+
+@pytest.mark.parametrize("unit,snaps", [(1, 3), (1, 0), (4, 2), (5, 1)])
+def test_binomial_checkpointing_equals_fixed_interval(native_lib, unit, snaps):
+    """rbc_adjoint_record_binomial (units of `unit` steps, `snaps` slots)
+    against a checkpoint every step: the same recomputed states (the forward
+    is bitwise repeatable), so the gradients agree up to the order of the
+    reverse sweep's FP32 atomics."""
+    from preprocess_src_b200.step import Simulation
+    case = _case()
+    with Simulation(case) as sim:
+        run = _Run(sim, _stretched(case), 23, 1)
+        ref = run.adjoint(want_x0=True)
+        sim.set_coefficients(**run.theta0)
+        run.init.restore(sim, run.x0)
+        sim.adjoint_record_binomial(23, unit, snaps)
+        end = sim.export_cells()
+        sch = sim.adjoint_schedule()
+        got = sim.adjoint_backward(run.r[0], run.r[1], run.r[2], want_x0=True)
+        after = sim.export_cells()
+        print(f"unit {unit} snaps {snaps}: {sch}, grad {got['grad']} vs {ref['grad']}")
+        assert sch["units"] == -(-23 // unit) and sch["snapshots"] == min(snaps, sch["units"] - 1) + 1
+        np.testing.assert_allclose(got["grad"], ref["grad"], rtol=2e-5)
+        np.testing.assert_allclose(got["dx0"], ref["dx0"], rtol=0, atol=2e-5 * np.abs(ref["dx0"]).max())
+        for k in ("x", "y", "z", "xd"):   # the handle is left at the end of the run
+            np.testing.assert_array_equal(after[k], end[k])
+
+
+def test_binomial_checkpointing_on_the_dense_suspension(native_lib):
+    """The adjoint at the dense suspension's size (256 x 128 x 128, 200 cells):
+    binomial checkpointing with units of one step and two snapshot slots
+    (memory independent of the run length) against a checkpoint every 12
+    steps (a store of 24 steps, 11.5 GB), over 12 steps."""
+    from preprocess_src_b200.step import Simulation
+    case = configs.dense_suspension()
+    nsteps = 12
+    with Simulation(case) as sim:
+        run = _Run(sim, None, nsteps, nsteps)
+        ref = run.adjoint()
+        sim.set_coefficients(**run.theta0)
+        run.init.restore(sim)
+        sim.adjoint_record_binomial(nsteps, 1, 2)
+        got = sim.adjoint_backward(run.r[0], run.r[1], run.r[2])
+        print(f"dense: binomial {got['grad']} ({got['ms']:.1f} ms) vs fixed {ref['grad']} ({ref['ms']:.1f} ms)")
+        scale = np.abs(ref["grad"]).max()
+        assert scale > 0
+        np.testing.assert_allclose(got["grad"], ref["grad"], rtol=0, atol=2e-5 * scale)
+        assert got["flags"] == 0
