@@ -287,8 +287,9 @@ def run_ours(args, world, rank, local):
 
 def run_capillaries(args, world, rank, local):
     """Config 4: independent capillaries of uneven length stepped as one batch
-    (one CUDA graph launch per step, chain length from the autotuner) against
-    the same capillaries stepped one after another.  value = aggregate MLUPS of
+    (one CUDA graph launch per step of seven fused launches, one per stage over
+    all capillaries, launch shapes from the autotuner) against the same
+    capillaries stepped one after another.  value = aggregate MLUPS of
     the batch; the sequential arm is the sum of each capillary's own
     event-timed steps."""
     import torch
@@ -303,11 +304,12 @@ def run_capillaries(args, world, rank, local):
     fluid = sum(c.fluid_nodes() for c in cases)
     batch = Batch(sims)
     chain = batch.autotune(2)
+    fused, shape = batch.fused, batch.shape
     batch.step(args.warmup)
     batch.synchronize()
     bstream = torch.cuda.ExternalStream(batch.stream, device=torch.device("cuda", dev))
     barrier(world)
-    l0 = sum(s.launches for s in sims)
+    l0 = batch.launches
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(dev) as clk:
         time.sleep(0.3)
@@ -316,7 +318,7 @@ def run_capillaries(args, world, rank, local):
         ev1.record(bstream)
         ev1.synchronize()
     ms = ev0.elapsed_time(ev1)
-    launches = sum(s.launches for s in sims) - l0
+    launches = batch.launches - l0
     ms_max = allreduce_max(ms, world)
     flags = [s.status()[0] for s in sims]
     # the same capillaries one after another, each timed on its own stream
@@ -342,7 +344,11 @@ def run_capillaries(args, world, rank, local):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": "capillary_batch_%d_32x32xL" % len(cases), "capillaries": len(cases),
                        "fluid_nodes": fluid, "lengths": "uniform {48, 64, ..., 128}", "cells_per_capillary": 1,
-                       "vertices_per_cell": cases[0].vertex, "chain": chain,
+                       "vertices_per_cell": cases[0].vertex,
+                       "form": "fused: one launch per stage over all capillaries" if fused else
+                               "child graphs (chain %d)" % chain,
+                       "autotuned_shape": {"lbm_threads": shape[0], "lbm_planes": shape[1],
+                                           "membrane_vertices_per_thread": shape[2]} if fused else None,
                        "l2": "inputs larger than L2 (populations %.2f GB), no flush" % (2 * 19 * 4 * sum(c.nx * c.ny * (c.nz - 4) for c in cases) / 1e9)},
             "sequential": {"value": round(seq, 2), "unit": "MLUPS", "ms_per_step": round(seq_ms / args.steps, 4),
                            "how": "each capillary stepped alone (rbc_step, CUDA graphs), one after another"},

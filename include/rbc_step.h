@@ -270,19 +270,28 @@ int rbc_get_stream(const rbc_handle *h, void **stream);
  * time per kernel in the order of RBC_KERNEL_NAMES (with BR != 0 the bending
  * kernel is timed in the "membrane" slot; "vof" holds the THINC/WLIC sweeps and
  * the front tracking of the steps it runs in).  Synchronous. */
-#define RBC_NUM_KERNELS 7
-#define RBC_KERNEL_NAMES {"step_begin", "membrane", "spread", "lbm_collide_stream", "advect", "vof", "volume"}
+#define RBC_NUM_KERNELS 8
+#define RBC_KERNEL_NAMES {"step_begin", "membrane", "spread", "lbm_collide_stream", "force_reset", "advect", "vof", "volume"}
 int rbc_profile_steps(rbc_handle *h, int nsteps, double *kernel_ms);
 
 /* ---- batches of independent simulations ----------------------------------- */
 
 /* Several independent simulations (for instance capillaries of different
- * sizes and parameters, each its own handle) stepped together: each batch
- * step is one CUDA graph launch whose nodes are the simulations' whole steps,
- * so their kernels run concurrently.  The reference runs one simulation per
- * process; its main.cu:73-110 loop is what each simulation of the batch
- * executes.  The handles stay owned by the caller and usable (stage calls,
- * imports, exports, rbc_step) between batch steps; destroy the batch first. */
+ * sizes and parameters, each its own handle) stepped together.  The reference
+ * runs one simulation per process; its main.cu:73-110 loop is what each
+ * simulation of the batch executes.  Two forms:
+ *   fused (the default where possible): each batch step is one CUDA graph of
+ *     seven launches -- step begin, the occupancy-word clear, membrane,
+ *     spread, collide-stream, advection, volume correction -- each running
+ *     the blocks of every simulation (a table of per-simulation arguments and
+ *     block offsets), with the same device code as a simulation's own step,
+ *     so the results are the same bit for bit.  Needs simulations that share
+ *     storage, flow mode, membrane precision and vertices per cell, with no
+ *     white cells, bending, output averages, volume fraction or tube;
+ *   child graphs (otherwise, or rbc_batch_set_form(b, 0)): each batch step is
+ *     one graph launch whose nodes are the simulations' whole steps.
+ * The handles stay owned by the caller and usable (stage calls, imports,
+ * exports, rbc_step) between batch steps; destroy the batch first. */
 typedef struct rbc_batch rbc_batch;
 /* handles: n distinct handles on one device.  Text of errors: rbc_batch_last_error(NULL). */
 int rbc_batch_create(rbc_handle *const *handles, int n, rbc_batch **out);
@@ -299,10 +308,27 @@ int rbc_batch_get_stream(const rbc_batch *b, void **stream);
  * the other, chains concurrently. */
 int rbc_batch_set_chain(rbc_batch *b, int chain);
 int rbc_batch_get_chain(const rbc_batch *b, int *chain);
-/* Times chain = 1, 2, 4, ... (up to 64 and the batch size) over 1 +
- * steps_per_trial batch steps each and keeps the fastest (*chain_out, may be
- * NULL).  The timed steps are real steps: every simulation advances by them. */
+/* Autotuner: times each candidate over 1 + steps_per_trial batch steps and
+ * keeps the fastest.  Fused form: the launch shapes (collide-stream threads
+ * per block 128 / 256 and z planes per thread 1 / 2 / 4, membrane vertices per
+ * thread: the one-simulation choice and the next); child graphs: chain = 1, 2,
+ * 4, ... up to 64.  *chain_out (may be NULL) receives the chain.  The timed
+ * steps are real steps: every simulation advances by them. */
 int rbc_batch_autotune(rbc_batch *b, int steps_per_trial, int *chain_out);
+/* fused: 1 (default) for the fused form where the simulations allow it, 0 for
+ * child graphs.  rbc_batch_get_form: *fused = the form the next step uses;
+ * *obstacle (may be NULL) = why the fused form is not possible ("" if it is). */
+int rbc_batch_set_form(rbc_batch *b, int fused);
+int rbc_batch_get_form(const rbc_batch *b, int *fused, const char **obstacle);
+/* Launch shapes of the fused form: collide-stream threads per block (128 or
+ * 256), z planes per thread (0 = 2 with FP32 storage, 4 with FP16; else 1..8)
+ * and membrane vertices per thread (0 = as one simulation; else 1..4 within the
+ * block's thread limit).  Results do not depend on them. */
+int rbc_batch_set_shape(rbc_batch *b, int lbm_threads, int lbm_planes, int membrane_vpt);
+int rbc_batch_get_shape(const rbc_batch *b, int *lbm_threads, int *lbm_planes, int *membrane_vpt);
+/* Kernels the batch launched (fused: 7 per step; child graphs: every
+ * simulation's step kernels). */
+int rbc_batch_launch_count(const rbc_batch *b, long long *count);
 
 /* ---- adjoint (gradients through the step) -------------------------------- */
 

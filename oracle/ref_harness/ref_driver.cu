@@ -32,6 +32,7 @@ static cell g_cel;
 static fem g_fem;
 static int g_err = 0;
 
+#ifndef REF_WITH_ETC   // else the reference's own (etc.cu:325-446)
 void error(int code)
 {
     if (!g_err) g_err = code;
@@ -44,6 +45,7 @@ int expand2pow2(int n)
     while (p < n) p *= 2;
     return p;
 }
+#endif
 
 template <typename T>
 static T *dnew(size_t count)
@@ -404,5 +406,44 @@ int ref_get_cells(double *x, double *y, double *z, double *u, double *v, double 
     if (nd) down(nd, g_fem.nd, ne * 4);
     return 0;
 }
+
+#ifdef REF_WITH_ETC
+// The reference's output_data (etc.cu:449-790) on the current state with
+// prc->fnum = fnum: it writes config.dat, prof%04d.bin (fnum % 50 == 0),
+// cell/cell%04d.bin, restart.bin (restart%04d.bin when fnum % 100 == 0) and
+// center.dat (center%04d.dat when fnum % 50 == 0) under ./result of the
+// caller's working directory, which must hold result/ and result/cell/.  The
+// host copies it writes from are allocated here as mem_init would
+// (init1.cu:875-1092).
+int ref_write_files(int fnum)
+{
+    const int n = g_cdo.n;
+    cell &c = g_cel;
+    const int nv = c.n * c.vertex;
+    if (!g_ltc.fnH) {
+        g_ltc.fnH = (double *)malloc(sizeof(double) * (size_t)n * Q);
+        double **h[] = {&g_ltc.dmH, &g_ltc.umH, &g_ltc.vmH, &g_ltc.wmH, &g_ltc.vfH, &g_ltc.vfH2};
+        for (double **q : h) *q = (double *)malloc(sizeof(double) * (size_t)n);
+        double **hv[] = {&c.uH, &c.vH, &c.wH};
+        for (double **q : hv) *q = (double *)malloc(sizeof(double) * (size_t)nv);
+        double **hc[] = {&c.rxH, &c.ryH, &c.rzH};
+        for (double **q : hc) *q = (double *)malloc(sizeof(double) * (size_t)c.n);
+        c.rxD = dnew<double>(c.n); c.ryD = dnew<double>(c.n); c.rzD = dnew<double>(c.n);
+#if (N_W > 0)
+        const int nw = c.n_w * c.vertex_w;
+        double **hw[] = {&c.uH_w, &c.vH_w, &c.wH_w};
+        for (double **q : hw) *q = (double *)malloc(sizeof(double) * (size_t)nw);
+        double **hcw[] = {&c.rxH_w, &c.ryH_w, &c.rzH_w};
+        for (double **q : hcw) *q = (double *)malloc(sizeof(double) * (size_t)c.n_w);
+        c.rxD_w = dnew<double>(c.n_w); c.ryD_w = dnew<double>(c.n_w); c.rzD_w = dnew<double>(c.n_w);
+#endif
+    }
+    Wall wall{}, wall_host{};
+    g_prc.fnum = fnum;
+    cudaDeviceSynchronize();
+    output_data(&g_prc, &g_cdo, &g_ltc, &g_cel, &g_fem, &wall, &wall_host);
+    return g_err;
+}
+#endif
 
 }  // extern "C"

@@ -20,8 +20,8 @@ RBC_WALLS_BOTH, RBC_WALLS_TOP = 0, 1
 RBC_NOALLOC_MAX_CELLS = 4096
 RBC_NOALLOC_MAX_VERTEX = 4096
 RBC_SHAPE_LBM_PLANES = 1
-RBC_NUM_KERNELS = 7
-RBC_KERNEL_NAMES = ("step_begin", "membrane", "spread", "lbm_collide_stream", "advect", "vof", "volume")
+RBC_NUM_KERNELS = 8
+RBC_KERNEL_NAMES = ("step_begin", "membrane", "spread", "lbm_collide_stream", "force_reset", "advect", "vof", "volume")
 RBC_FLAG_VC_NOT_CONVERGED, RBC_FLAG_NONFINITE, RBC_FLAG_SPREAD_OVERFLOW, RBC_FLAG_SOLVE_RESIDUAL = 1, 2, 4, 8
 RBC_FLAG_VOF_NOT_CONVERGED = 16
 
@@ -82,6 +82,11 @@ _SIGS = {
                                  _DP, _DP, _DP],
     "rbc_batch_create": [C.POINTER(_H), C.c_int, C.POINTER(_H)],
     "rbc_batch_destroy": [_H],
+    "rbc_batch_set_form": [_H, C.c_int],
+    "rbc_batch_get_form": [_H, _IP, C.POINTER(C.c_char_p)],
+    "rbc_batch_set_shape": [_H, C.c_int, C.c_int, C.c_int],
+    "rbc_batch_get_shape": [_H, _IP, _IP, _IP],
+    "rbc_batch_launch_count": [_H, C.POINTER(C.c_longlong)],
     "rbc_batch_last_error": [_H],
     "rbc_batch_step": [_H, C.c_int],
     "rbc_batch_synchronize": [_H],

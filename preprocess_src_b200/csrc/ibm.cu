@@ -43,16 +43,17 @@ __device__ __forceinline__ bool to_fixed(double v, int shift, long long &out) {
     return true;
 }
 
-// Adds one node's fixed-point force (three components; zeros skipped) and sets
-// its occupancy bit.  Returns false if a component was out of range.
-__device__ __forceinline__ bool add_force(const ForceField &F, long long nint, long long gi, int z, long long xy,
-                                          double a, double b, double c, int sa, int sb, int sc) {
+// Adds one node's fixed-point force (three components; zeros skipped).
+// *added: whether anything was added (the node's occupancy bit must be set).
+// Returns false if a component was out of range.
+__device__ __forceinline__ bool add_force(const ForceField &F, long long nint, long long gi, double a, double b,
+                                          double c, int sa, int sb, int sc, bool *added) {
     long long ia = 0, ib = 0, ic = 0;
     const bool ok = to_fixed(a, sa, ia) & to_fixed(b, sb, ib) & to_fixed(c, sc, ic);
     if (ia) atomicAdd(reinterpret_cast<unsigned long long *>(&F.F[gi]), (unsigned long long)ia);
     if (ib) atomicAdd(reinterpret_cast<unsigned long long *>(&F.F[nint + gi]), (unsigned long long)ib);
     if (ic) atomicAdd(reinterpret_cast<unsigned long long *>(&F.F[2 * nint + gi]), (unsigned long long)ic);
-    if (ia | ib | ic) atomicOr(&F.bits[(long long)z * F.wpp + (xy >> 5)], 1u << (xy & 31));
+    *added = (ia | ib | ic) != 0;
     return ok;
 }
 
@@ -245,9 +246,11 @@ spread_body(const Geom &g, const double *__restrict__ X, long long nv, int V,
                 } else if (__ldg(&mask2d[gxw + g.nx * gy]) & MASK_FLUID) {
                     const int zw = wrap_z(iz, g.nzc);
                     const long long xy = gxw + (long long)g.nx * gy, gi = (long long)zw * g.plane + xy;
-                    if (!add_force(F, g.nint, gi, zw, xy, (double)(w * f0), (double)(w * f1), (double)(w * f2),
-                                   FORCE_FRAC, FORCE_FRAC, FORCE_FRAC))
+                    bool added = false;
+                    if (!add_force(F, g.nint, gi, (double)(w * f0), (double)(w * f1), (double)(w * f2),
+                                   FORCE_FRAC, FORCE_FRAC, FORCE_FRAC, &added))
                         atomicOr(flags, RBC_FLAG_NONFINITE);
+                    if (added) atomicOr(&F.bits[(long long)zw * F.wpp + (xy >> 5)], 1u << (xy & 31));
                 }
             }
         }
@@ -266,9 +269,11 @@ spread_body(const Geom &g, const double *__restrict__ X, long long nv, int V,
         if (!(__ldg(&mask2d[gx + g.nx * gy]) & MASK_FLUID)) continue;   // wall column: the LBM never reads it
         const int zw = wrap_z(bz0 + lz, g.nzc);
         const long long xy = gx + (long long)g.nx * gy, gi = (long long)zw * g.plane + xy;
-        if (!add_force(F, g.nint, gi, zw, xy, (double)ia, (double)ib, (double)ic, FORCE_FRAC - qe[0],
-                       FORCE_FRAC - qe[1], FORCE_FRAC - qe[2]))
+        bool added = false;
+        if (!add_force(F, g.nint, gi, (double)ia, (double)ib, (double)ic, FORCE_FRAC - qe[0],
+                       FORCE_FRAC - qe[1], FORCE_FRAC - qe[2], &added))
             atomicOr(flags, RBC_FLAG_NONFINITE);
+        if (added) atomicOr(&F.bits[(long long)zw * F.wpp + (xy >> 5)], 1u << (xy & 31));
     }
 }
 

@@ -88,11 +88,30 @@ __device__ __forceinline__ Collision collision_terms(const float (&g)[Q], float 
     return c;
 }
 
-__device__ __forceinline__ float post_collision(const Collision &c, int q, float gq, float om1)
+// The post-collision values of an opposite pair (q, q + 1 = opp(q)): with
+// e_{q+1} = -e_q the polynomial splits into its even and odd parts,
+//   S = w_q (A + eu (C eu + E eG)),   T = w_q (B eu + D eG),
+//   f*_q = (1 - om) g_q + S + T,   f*_{q+1} = (1 - om) g_{q+1} + S - T,
+// so it is evaluated once per pair.  TAU1 (om = 1, tau = 1 as in every named
+// workload): (1 - om) g = 0 exactly, and the pulled values enter only through
+// the moments (the same results as the general form with om1 = 0).
+template <bool TAU1>
+__device__ __forceinline__ void post_pair(const Collision &c, int q, float gq, float gp, float om1, float &oq,
+                                          float &op)
 {
     const float eu = ex(q) * c.u + ey(q) * c.v + ez(q) * c.w;
     const float eG = ex(q) * c.Gx + ey(q) * c.Gy + ez(q) * c.Gz;
-    return om1 * gq + wq(q) * (c.A + eu * (c.B + c.C * eu + c.E * eG) + c.D * eG);
+    const float w = wq(q);
+    const float S = w * (c.A + eu * (c.C * eu + c.E * eG));
+    const float T = w * (c.B * eu + c.D * eG);
+    oq = TAU1 ? S + T : om1 * gq + (S + T);
+    op = TAU1 ? S - T : om1 * gp + (S - T);
+}
+
+template <bool TAU1>
+__device__ __forceinline__ float post_rest(const Collision &c, float g0, float om1)
+{
+    return TAU1 ? wq(0) * c.A : om1 * g0 + wq(0) * c.A;
 }
 
 // FP16 storage rounds stochastically (cvt.rs.f16x2.f32, sm_100a): each stored
@@ -132,11 +151,11 @@ __device__ __forceinline__ void st_u16(__half *p, uint32_t v) {
 // Collision of one node from its pulled populations g (storage units) and
 // stores of the post-collision values (0 for wall lanes) at element offset idx of every
 // population array; I is the offset type (int when Q * nint < 2^31).  has_force:
-// the node's occupancy bit (F holds its IB force, which is read and zeroed here).
-template <int STORE, bool ALL_FLUID, typename I>
+// the node's occupancy bit (F holds its IB force; read only here).
+template <int STORE, bool ALL_FLUID, bool TAU1, typename I>
 __device__ __forceinline__ void collide_store(float (&g)[Q], bool fluid, bool has_force, I idx, I nint,
                                               typename Store<STORE>::T *__restrict__ gout, float4 *__restrict__ uvr,
-                                              long long *__restrict__ F, uint32_t step,
+                                              const long long *__restrict__ F, uint32_t step,
                                               float pd, float omega, float om1, float Cr, float Bc)
 {
     using S = Store<STORE>;
@@ -144,28 +163,35 @@ __device__ __forceinline__ void collide_store(float (&g)[Q], bool fluid, bool ha
     float fx = 0.f, fy = 0.f, fz = 0.f;
     if (live && has_force) {
         constexpr float inv = 1.0f / (float)(1ULL << FORCE_FRAC);
-        fx = (float)F[idx] * inv; fy = (float)F[nint + idx] * inv; fz = (float)F[2 * nint + idx] * inv;
-        F[idx] = 0; F[nint + idx] = 0; F[2 * nint + idx] = 0;
+        fx = (float)__ldg(&F[idx]) * inv; fy = (float)__ldg(&F[nint + idx]) * inv;
+        fz = (float)__ldg(&F[2 * nint + idx]) * inv;
     }
     const Collision c = collision_terms<(int)S::scale>(g, fx, fy, fz, pd, omega, Cr, Bc);
     uvr[idx] = live ? make_float4(c.u, c.v, c.w, c.r) : make_float4(0.f, 0.f, 0.f, 1.f);
     typename S::T *ob = gout + idx;
     if constexpr (STORE == RBC_STORE_F16) {
         const uint32_t h = node_hash((uint32_t)idx, step);
-        // slot 0 alone, then the pairs (1, 2), (3, 4), ..., (17, 18)
-        const uint32_t d0 = cvt_rs_f16x2(0.f, live ? post_collision(c, 0, g[0], om1) : 0.f, pair_bits(h, 0x2545F491u));
+        // slot 0 alone, then the opposite pairs (1, 2), (3, 4), ..., (17, 18)
+        const uint32_t d0 = cvt_rs_f16x2(0.f, live ? post_rest<TAU1>(c, g[0], om1) : 0.f, pair_bits(h, 0x2545F491u));
         st_u16(ob, d0);
 #pragma unroll
         for (int q = 1; q < Q; q += 2) {
-            const float lo = live ? post_collision(c, q, g[q], om1) : 0.f;
-            const float hi = live ? post_collision(c, q + 1, g[q + 1], om1) : 0.f;
+            float lo, hi;
+            post_pair<TAU1>(c, q, g[q], g[q + 1], om1, lo, hi);
+            if (!live) { lo = 0.f; hi = 0.f; }
             const uint32_t d = cvt_rs_f16x2(hi, lo, pair_bits(h, 0x9E3779B1u + 0x3C6EF372u * (uint32_t)q));
             st_u16(ob + (I)q * nint, d);
             st_u16(ob + (I)(q + 1) * nint, d >> 16);
         }
     } else {
+        S::st_raw(ob, live ? post_rest<TAU1>(c, g[0], om1) : 0.f);
 #pragma unroll
-        for (int q = 0; q < Q; q++) S::st_raw(ob + (I)q * nint, live ? post_collision(c, q, g[q], om1) : 0.f);
+        for (int q = 1; q < Q; q += 2) {
+            float a, b;
+            post_pair<TAU1>(c, q, g[q], g[q + 1], om1, a, b);
+            S::st_raw(ob + (I)q * nint, live ? a : 0.f);
+            S::st_raw(ob + (I)(q + 1) * nint, live ? b : 0.f);
+        }
     }
 }
 
@@ -192,11 +218,11 @@ __device__ __forceinline__ void collide_store(float (&g)[Q], bool fluid, bool ha
 // (lbm.cu:1131 with LAMBDA1 != 1); the omega argument otherwise.
 // (bx, by, gy): the block's column tile, its first plane and the plane stride
 // (blockIdx.x, blockIdx.y, gridDim.y of a one-lattice launch).
-template <int STORE, typename I, bool VISC>
+template <int STORE, typename I, bool VISC, bool TAU1>
 __device__ __forceinline__ void
 lbm_collide_stream_body(const typename Store<STORE>::T *__restrict__ gin, typename Store<STORE>::T *__restrict__ gout,
                         float4 *__restrict__ uvr,
-                        long long *__restrict__ F, const uint32_t *__restrict__ Fbits, int wpp,
+                        const long long *__restrict__ F, const uint32_t *__restrict__ Fbits, int wpp,
                         const uint32_t *__restrict__ mask2d, const float *__restrict__ drive,
                         const int *__restrict__ iter,
                         const float *__restrict__ wall, const double *__restrict__ vf, float lm1, float df3,
@@ -217,7 +243,7 @@ lbm_collide_stream_body(const typename Store<STORE>::T *__restrict__ gin, typena
     float om1 = 1.0f - omega;
     // a warp's 32 nodes of a plane are the 32 bits of one occupancy word
     // (blockDim.x is a multiple of 32), read by every lane (one address); the
-    // words are cleared before the next step's spread
+    // reset before the next step's spread clears them
     const int lane = threadIdx.x & 31;
     const int fword = xy >> 5;
     for (int z = by; z < nzc; z += gy) {
@@ -238,7 +264,7 @@ lbm_collide_stream_body(const typename Store<STORE>::T *__restrict__ gin, typena
 #pragma unroll
             for (int q = 0; q < Q; q++)
                 g[q] = S::ld_raw(gb + ((I)q * nint + ((ez(q) == 1) ? dzm : (ez(q) == -1) ? dzp : (I)0) - ex(q) - nx * ey(q)));
-            collide_store<STORE, true, I>(g, true, has_force, idx, nint, gout, uvr, F, step, pd, omega, om1, Cr, Bc);
+            collide_store<STORE, true, TAU1, I>(g, true, has_force, idx, nint, gout, uvr, F, step, pd, omega, om1, Cr, Bc);
         } else {
 #pragma unroll
             for (int q = 0; q < Q; q++) {
@@ -261,23 +287,24 @@ lbm_collide_stream_body(const typename Store<STORE>::T *__restrict__ gin, typena
                 for (int q = 0; q < Q; q++)
                     if (ez(q) != 0 && ((m >> q) & 1u)) g[q] += 6.0f * wq(q) * rho * Cr * (float)ez(q) * uw * S::scale;
             }
-            collide_store<STORE, false, I>(g, fluid, has_force, idx, nint, gout, uvr, F, step, pd, omega, om1, Cr, Bc);
+            collide_store<STORE, false, TAU1, I>(g, fluid, has_force, idx, nint, gout, uvr, F, step, pd, omega, om1, Cr, Bc);
         }
     }
 }
 
-template <int STORE, typename I, bool VISC>
+template <int STORE, typename I, bool VISC, bool TAU1>
 __global__ void __launch_bounds__(LBM_THREADS, LBM_MIN_BLOCKS)
 lbm_collide_stream(const typename Store<STORE>::T *__restrict__ gin, typename Store<STORE>::T *__restrict__ gout,
                    float4 *__restrict__ uvr,
-                   long long *__restrict__ F, const uint32_t *__restrict__ Fbits, int wpp,
+                   const long long *__restrict__ F, const uint32_t *__restrict__ Fbits, int wpp,
                    const uint32_t *__restrict__ mask2d, const float *__restrict__ drive, const int *__restrict__ iter,
                    const float *__restrict__ wall, const double *__restrict__ vf, float lm1, float df3,
                    int nx, int ny, int nzc, I nint,
                    float omega, float Cr, float Bc)
 {
-    lbm_collide_stream_body<STORE, I, VISC>(gin, gout, uvr, F, Fbits, wpp, mask2d, drive, iter, wall, vf, lm1, df3,
-                                            nx, ny, nzc, nint, omega, Cr, Bc, blockIdx.x, blockIdx.y, gridDim.y);
+    lbm_collide_stream_body<STORE, I, VISC, TAU1>(gin, gout, uvr, F, Fbits, wpp, mask2d, drive, iter, wall, vf, lm1,
+                                                  df3, nx, ny, nzc, nint, omega, Cr, Bc, blockIdx.x, blockIdx.y,
+                                                  gridDim.y);
 }
 
 // z planes per thread: the per-thread setup (mask, warp votes, drive) is paid
@@ -298,12 +325,19 @@ void launch_lbm(const Geom &g, int storage, const LbmArgs &a, cudaStream_t s)
     const int gz = (g.nzc + zpt - 1) / zpt;
     const dim3 blocks((unsigned)((g.plane + LBM_THREADS - 1) / LBM_THREADS), (unsigned)(gz < 65535 ? gz : 65535));
     const bool off32 = (long long)Q * g.nint < (1LL << 31);   // every element offset fits in an int
-#define LBM_LAUNCH(ST, I, V)                                                                                  \
-    lbm_collide_stream<ST, I, V><<<blocks, LBM_THREADS, 0, s>>>(                                              \
+#define LBM_LAUNCH(ST, I, V, T1)                                                                              \
+    lbm_collide_stream<ST, I, V, T1><<<blocks, LBM_THREADS, 0, s>>>(                                          \
         (const Store<ST>::T *)a.gin, (Store<ST>::T *)a.gout, a.uvr, a.F.F, a.F.bits, a.F.wpp, a.mask2d, a.drive, a.iter, \
         a.wall, a.vf, \
         a.lm1, a.df3, g.nx, g.ny, g.nzc, (I)g.nint, a.omega, a.Cr, a.Bc)
-#define LBM_LAUNCH_V(ST, I) do { if (a.vf) LBM_LAUNCH(ST, I, true); else LBM_LAUNCH(ST, I, false); } while (0)
+    // tau = 1 without a viscosity ratio: the om = 1 form of the collision
+    const bool tau1 = !a.vf && a.omega == 1.0f;
+#define LBM_LAUNCH_V(ST, I)                                                                                   \
+    do {                                                                                                      \
+        if (a.vf) LBM_LAUNCH(ST, I, true, false);                                                             \
+        else if (tau1) LBM_LAUNCH(ST, I, false, true);                                                        \
+        else LBM_LAUNCH(ST, I, false, false);                                                                 \
+    } while (0)
     if (storage == RBC_STORE_F16) {
         if (off32) LBM_LAUNCH_V(RBC_STORE_F16, int); else LBM_LAUNCH_V(RBC_STORE_F16, long long);
     } else {
@@ -325,9 +359,16 @@ lbm_fused_kernel(const DomainArgs *__restrict__ dom, const int *__restrict__ bof
     const DomainArgs &D = dom[d];
     const LbmArgs &a = D.lbm;
     const int b = blockIdx.x - boff[d];
-    lbm_collide_stream_body<STORE, I, false>((const T *)a.gin, (T *)a.gout, a.uvr, a.F.F, a.F.bits, a.F.wpp, a.mask2d,
-                                            a.drive, a.iter, a.wall, nullptr, 0.f, 0.f, D.g.nx, D.g.ny, D.g.nzc,
-                                            (I)D.g.nint, a.omega, a.Cr, a.Bc, b % D.lbm_bx, b / D.lbm_bx, D.lbm_gy);
+    if (a.omega == 1.0f)   // uniform over the block: the om = 1 form, as a one-simulation launch takes it
+        lbm_collide_stream_body<STORE, I, false, true>((const T *)a.gin, (T *)a.gout, a.uvr, a.F.F, a.F.bits, a.F.wpp,
+                                                       a.mask2d, a.drive, a.iter, a.wall, nullptr, 0.f, 0.f, D.g.nx,
+                                                       D.g.ny, D.g.nzc, (I)D.g.nint, a.omega, a.Cr, a.Bc,
+                                                       b % D.lbm_bx, b / D.lbm_bx, D.lbm_gy);
+    else
+        lbm_collide_stream_body<STORE, I, false, false>((const T *)a.gin, (T *)a.gout, a.uvr, a.F.F, a.F.bits,
+                                                        a.F.wpp, a.mask2d, a.drive, a.iter, a.wall, nullptr, 0.f,
+                                                        0.f, D.g.nx, D.g.ny, D.g.nzc, (I)D.g.nint, a.omega, a.Cr,
+                                                        a.Bc, b % D.lbm_bx, b / D.lbm_bx, D.lbm_gy);
 }
 
 void launch_lbm_fused(const FusedLaunch &f, int storage, bool off32, int threads, cudaStream_t s)
@@ -342,6 +383,19 @@ void launch_lbm_fused(const FusedLaunch &f, int storage, bool off32, int threads
     }
 #undef LBM_FUSED_T
 #undef LBM_FUSED
+}
+
+// one warp per 32 words (whole warps: every lane takes part in the ballot)
+__global__ void force_reset_kernel(const ForceField F, long long nwords, long long plane, long long nint)
+{
+    const long long w0 = (((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32;
+    if (w0 < nwords) force_reset_words(F.F, F.bits, w0, nwords, F.wpp, plane, nint, threadIdx.x & 31);
+}
+
+void launch_force_reset(const Geom &g, const ForceField &F, cudaStream_t s)
+{
+    const long long nw = (long long)g.nzc * F.wpp;
+    force_reset_kernel<<<(unsigned)((nw + 255) / 256), 256, 0, s>>>(F, nw, g.plane, g.nint);
 }
 
 // ---- circular tube: interpolated bounce-back ------------------------------

@@ -109,6 +109,8 @@ struct rbc_handle {
     // split membrane pass: the first full wave's spread beside the last wave's membrane (capture only)
     cudaStream_t side2 = nullptr;
     cudaEvent_t wave_done = nullptr, spread_done = nullptr;
+    // the force reset beside the advection (capture only; on side2, idle by then)
+    cudaEvent_t lbm_done = nullptr, reset_done = nullptr;
     int sms = 0;                                      // multiprocessors of the device
     int prio_high = 0;                                // greatest stream priority of the device
     long long launches = 0;
@@ -125,7 +127,7 @@ struct rbc_handle {
     size_t metrics_host_n = 0;
 
     int kernels_per_step() const {
-        int k = 2 + (ntube > 0 ? 1 : 0);   // step_begin, lbm (+ tube bounce-back)
+        int k = 2 + (ntube > 0 ? 1 : 0) + (has_cells() ? 1 : 0);   // step_begin, lbm (+ tube bounce-back, force reset)
         if (ngroups == 1 && cg[0].br == 0.0 && fileoutput == 0 && sms > 0 && cg[0].ncell > sms && cg[0].ncell % sms)
             k += 2;                        // the membrane pass and the spread in two launches each
         for (int g = 0; g < ngroups; g++) {
@@ -606,6 +608,8 @@ void free_all(rbc_handle *h)
     if (h->metrics_host) cudaFreeHost(h->metrics_host);
     if (h->wave_done) cudaEventDestroy(h->wave_done);
     if (h->spread_done) cudaEventDestroy(h->spread_done);
+    if (h->lbm_done) cudaEventDestroy(h->lbm_done);
+    if (h->reset_done) cudaEventDestroy(h->reset_done);
     if (h->side2) cudaStreamDestroy(h->side2);
     void *ptrs[] = {h->g[0], h->g[1], h->uvr, h->Fint, h->Fbits, h->mask2d, h->tube_links, h->tube_frac,
                     h->d_int, h->d_drive, h->staging, h->vof_s1, h->vof_s2, h->vof_G, h->vof_b, h->vof_partial};
@@ -665,20 +669,27 @@ int membrane_wave_split(const rbc_handle *h)
     return full < g.ncell ? full : 0;
 }
 
+// the membrane kernel's arguments for population g
+MembraneArgs membrane_args(rbc_handle *h, CellGroup &g)
+{
+    MembraneArgs a{};
+    a.Xd = g.Xd; a.nv = g.nv; a.ne = g.ne; a.gref = g.gref; a.erec = g.erec;
+    a.tri = g.tri; a.v2e_off = g.v2e_off; a.v2e = g.v2e; a.nbr = g.nbr; a.Fv = g.Fv;
+    a.V = g.V; a.E = g.E; a.ncell = g.ncell;
+    a.C = h->p.C; a.rgs = g.rgs; a.law = h->p.law; a.LX = h->p.LX; a.LZ = h->p.LZ;
+    a.niter = h->p.solver_iters > 0 ? h->p.solver_iters : DEFAULT_SOLVER_ITERS;
+    a.flags = h->d_flags();
+    a.priority = h->prio_high;
+    return a;
+}
+
 // stress() (stress.cu:580-660) for every cell population
 int launch_stress(rbc_handle *h)
 {
     for (int k = 0; k < h->ngroups; k++) {
         CellGroup &g = h->cg[k];
         if (g.ncell == 0) continue;
-        MembraneArgs a{};
-        a.Xd = g.Xd; a.nv = g.nv; a.ne = g.ne; a.gref = g.gref; a.erec = g.erec;
-        a.tri = g.tri; a.v2e_off = g.v2e_off; a.v2e = g.v2e; a.nbr = g.nbr; a.Fv = g.Fv;
-        a.V = g.V; a.E = g.E; a.ncell = g.ncell;
-        a.C = h->p.C; a.rgs = g.rgs; a.law = h->p.law; a.LX = h->p.LX; a.LZ = h->p.LZ;
-        a.niter = h->p.solver_iters > 0 ? h->p.solver_iters : DEFAULT_SOLVER_ITERS;
-        a.flags = h->d_flags();
-        a.priority = h->prio_high;
+        const MembraneArgs a = membrane_args(h, g);
         launch_membrane(a, h->p.membrane_fp64 != 0, h->stream);
         h->launches++;
         CK_LAUNCH();
@@ -696,12 +707,29 @@ int launch_stress(rbc_handle *h)
     return RBC_OK;
 }
 
-// the occupancy words of the lattice force start each step's spread at zero
-// (the collide-stream kernel zeroes the forces it read, not the words)
-int clear_force_bits(rbc_handle *h, cudaStream_t st)
+// The force reset after the collide-stream kernel read the field: zero the
+// forces of the nodes whose occupancy bit is set, then the bits, so the next
+// spread starts from zero.  Right after the read the field's set lines are
+// still in L2 (a reset before the next step's spread, with those lines
+// evicted by the rest of the step, took 14 us on the dense suspension).
+int launch_force_reset_stage(rbc_handle *h, cudaStream_t st)
 {
-    CK(cudaMemsetAsync(h->Fbits, 0, h->force_bit_bytes(), st));
+    if (!h->has_cells()) return RBC_OK;   // nothing spreads: the field stays zero
+    launch_force_reset(h->geo, h->force(), st);
+    h->launches++;
+    CK_LAUNCH();
     return RBC_OK;
+}
+
+// the spread kernel's arguments for population g
+SpreadArgs spread_args(rbc_handle *h, CellGroup &g)
+{
+    SpreadArgs a{};
+    a.X = g.X; a.nv = g.nv; a.V = g.V; a.ncell = g.ncell; a.Fv = g.Fv;
+    a.patch_off = g.patch_off; a.patch_vtx = g.patch_vtx; a.patch_stride = g.patch_stride;
+    a.npatch = g.npatch;
+    a.F = h->force(); a.mask2d = h->mask2d; a.flags = h->d_flags();
+    return a;
 }
 
 // ibm_st1's spreading (ibm.cu:299-369) of every population into the same force field
@@ -710,11 +738,7 @@ int launch_spread_stage(rbc_handle *h)
     for (int k = 0; k < h->ngroups; k++) {
         CellGroup &g = h->cg[k];
         if (g.ncell == 0) continue;
-        SpreadArgs a{};
-        a.X = g.X; a.nv = g.nv; a.V = g.V; a.ncell = g.ncell; a.Fv = g.Fv;
-        a.patch_off = g.patch_off; a.patch_vtx = g.patch_vtx; a.patch_stride = g.patch_stride;
-        a.npatch = g.npatch;
-        a.F = h->force(); a.mask2d = h->mask2d; a.flags = h->d_flags();
+        const SpreadArgs a = spread_args(h, g);
         launch_spread(h->geo, a, h->stream);
         h->launches++;
         CK_LAUNCH();
@@ -739,10 +763,11 @@ int launch_bend_stage(rbc_handle *h)
     return RBC_OK;
 }
 
-int launch_lbm_stage(rbc_handle *h)
+// the collide-stream kernel's arguments from population buffer cur
+LbmArgs lbm_args(rbc_handle *h, int cur)
 {
     LbmArgs a{};
-    a.gin = h->g[h->cur]; a.gout = h->g[1 - h->cur];
+    a.gin = h->g[cur]; a.gout = h->g[1 - cur];
     a.uvr = h->uvr;
     a.F = h->force(); a.mask2d = h->mask2d; a.drive = h->d_drive; a.iter = h->d_iter();
     a.wall = h->p.flow == RBC_FLOW_SHEAR ? h->d_drive + 1 : nullptr;
@@ -753,6 +778,14 @@ int launch_lbm_stage(rbc_handle *h)
     a.vf = (h->p.lambda1 != 1.0 && h->cg[0].vf) ? h->cg[0].vf : nullptr;
     a.lm1 = (float)(h->p.lambda1 - 1.0);
     a.df3 = (float)(h->p.tau - 0.5);   // 3 Df, tau = 3 Df + 1/2
+    return a;
+}
+
+// the collide-stream launch (+ the tube's bounce-back) and, with reset, the
+// force reset after it
+int launch_lbm_stage(rbc_handle *h, bool reset = true)
+{
+    LbmArgs a = lbm_args(h, h->cur);
     launch_lbm(h->geo, h->p.storage, a, h->stream);
     h->launches++;
     CK_LAUNCH();
@@ -763,7 +796,17 @@ int launch_lbm_stage(rbc_handle *h)
         CK_LAUNCH();
     }
     h->cur ^= 1;
-    return RBC_OK;
+    return reset ? launch_force_reset_stage(h, h->stream) : RBC_OK;
+}
+
+// the advection kernel's arguments for population g
+AdvectArgs advect_args(rbc_handle *h, CellGroup &g)
+{
+    AdvectArgs a{};
+    a.X = g.X; a.Xd = g.Xd; a.U = g.U; a.uvr = h->uvr; a.nv = g.nv;
+    a.V = g.V; a.ncell = g.ncell; a.patch_off = g.patch_off; a.patch_vtx = g.patch_vtx; a.npatch = g.npatch;
+    a.dtM = h->p.dt * h->p.M; a.flags = h->d_flags();
+    return a;
 }
 
 // ibm_st2 (ibm.cu:642-694) for every population
@@ -772,10 +815,7 @@ int launch_advect_stage(rbc_handle *h)
     for (int k = 0; k < h->ngroups; k++) {
         CellGroup &g = h->cg[k];
         if (g.ncell == 0) continue;
-        AdvectArgs a{};
-        a.X = g.X; a.Xd = g.Xd; a.U = g.U; a.uvr = h->uvr; a.nv = g.nv;
-        a.V = g.V; a.ncell = g.ncell; a.patch_off = g.patch_off; a.patch_vtx = g.patch_vtx; a.npatch = g.npatch;
-        a.dtM = h->p.dt * h->p.M; a.flags = h->d_flags();
+        const AdvectArgs a = advect_args(h, g);
         launch_advect(h->geo, a, h->stream);
         h->launches++;
         CK_LAUNCH();
@@ -899,7 +939,6 @@ int enqueue_step(rbc_handle *h, StepForm form = STEP_WHOLE)
     launch_step_begin(step_begin_args(h), h->stream);
     h->launches++;
     CK_LAUNCH();
-    if ((rc = clear_force_bits(h, h->stream))) return rc;
     const int split = membrane_wave_split(h);
     if (split > 0) {
         CellGroup &g = h->cg[0];
@@ -919,10 +958,17 @@ int enqueue_step(rbc_handle *h, StepForm form = STEP_WHOLE)
         if ((rc = launch_bend_stage(h))) return rc;   // reads cel->x, after the correction
         if ((rc = launch_spread_stage(h))) return rc;
     }
-    if ((rc = launch_lbm_stage(h))) return rc;
+    // the force reset runs beside the advection (which reads neither the
+    // field nor its bits) and joins before the step ends
+    if ((rc = launch_lbm_stage(h, false))) return rc;
+    CK(cudaEventRecord(h->lbm_done, h->stream));
+    CK(cudaStreamWaitEvent(h->side2, h->lbm_done, 0));
+    if ((rc = launch_force_reset_stage(h, h->side2))) return rc;
+    CK(cudaEventRecord(h->reset_done, h->side2));
     if ((rc = launch_advect_stage(h))) return rc;
     if ((rc = launch_thinc_stage(h))) return rc;   // main.cu:94-95
     if (form == STEP_WHOLE && (rc = launch_volume_stage(h, h->stream))) return rc;
+    CK(cudaStreamWaitEvent(h->stream, h->reset_done, 0));
     return RBC_OK;
 }
 
@@ -986,6 +1032,17 @@ struct rbc_batch {
     int parity = 0;                     // graph[parity] advances every handle by one step
     int chain = 1;                      // simulations per dependency chain in the batch graph
     std::string err;
+    // Fused form: every stage of all simulations in one launch (FusedLaunch).
+    // Used when the simulations share what selects the kernels' code (storage,
+    // flow mode, membrane precision, vertices per cell) and have none of the
+    // stages a fused step leaves out (white cells, bending, output averages,
+    // the volume fraction, the circular tube); else each simulation's step is a
+    // child graph of the batch graph.
+    int use_fused = 1;                  // rbc_batch_set_form: 1 fused when possible, 0 child graphs
+    bool fused = false;                 // the graphs are the fused form
+    int lbm_threads = 256, lbm_planes = 0, mem_vpt = 0;   // fused launch shapes (0: as one simulation)
+    void *fmem = nullptr;               // device: descriptors [2][n], block offsets [2][FSTAGES][n + 1]
+    long long launches = 0;             // fused kernel launches
 };
 
 namespace {
@@ -1002,6 +1059,127 @@ namespace {
 void batch_free_graphs(rbc_batch *b)
 {
     for (cudaGraphExec_t &g : b->graph) { if (g) cudaGraphExecDestroy(g); g = nullptr; }
+    if (b->fmem) { cudaFree(b->fmem); b->fmem = nullptr; }
+    b->fused = false;
+}
+
+// stages of a fused step, in order
+enum { FS_CLEAR, FS_MEMBRANE, FS_SPREAD, FS_LBM, FS_ADVECT, FS_VOLUME, FSTAGES };
+constexpr int FUSED_KERNELS_PER_STEP = FSTAGES + 1;   // + step begin
+
+// why the batch's simulations cannot run as one fused step ("" = they can)
+std::string fused_obstacle(const rbc_batch *b)
+{
+    const rbc_handle *h0 = b->h[0];
+    int V = 0;
+    for (size_t i = 0; i < b->h.size(); i++) {
+        const rbc_handle *h = b->h[i];
+        const std::string who = "simulation " + std::to_string(i) + ": ";
+        if (h->p.storage != h0->p.storage || h->p.flow != h0->p.flow || h->p.membrane_fp64 != h0->p.membrane_fp64)
+            return who + "storage, flow mode and membrane precision differ";
+        if (h->ngroups > 1) return who + "white cells";
+        if (h->cg[0].br != 0.0) return who + "bending (BR != 0)";
+        if (h->fileoutput > 0) return who + "output-interval averages";
+        if (h->vof()) return who + "volume fraction";
+        if (h->ntube > 0) return who + "circular tube";
+        if (h->cg[0].ncell > 0) {
+            if (V && h->cg[0].V != V) return who + "another number of vertices per cell";
+            V = h->cg[0].V;
+        }
+    }
+    return "";
+}
+
+// The fused graphs: descriptors of every simulation for both buffer
+// parities, block offsets of every stage, and one graph per parity of
+// step begin, membrane, spread, collide-stream, force reset, advection and
+// volume correction launches.
+int batch_build_fused(rbc_batch *b)
+{
+    const int n = (int)b->h.size();
+    rbc_handle *h0 = b->h[0];
+    int V = 0;
+    bool off32 = true;
+    for (rbc_handle *h : b->h) {
+        if (h->cg[0].ncell > 0) V = h->cg[0].V;
+        off32 = off32 && (long long)Q * h->geo.nint < (1LL << 31);
+    }
+    const int vpt = b->mem_vpt > 0 ? b->mem_vpt : (V > 0 ? membrane_default_vpt(V) : 1);
+    const int tpb = b->lbm_threads;
+    std::vector<DomainArgs> dom(2 * (size_t)n);
+    std::vector<int> boff(2 * (size_t)FSTAGES * (n + 1), 0);
+    int nblocks[FSTAGES] = {};
+    for (int k = 0; k < 2; k++) {
+        int acc[FSTAGES] = {};
+        for (int i = 0; i < n; i++) {
+            rbc_handle *h = b->h[i];
+            CellGroup &g = h->cg[0];
+            DomainArgs &D = dom[(size_t)k * n + i];
+            D.g = h->geo;
+            D.sb = step_begin_args(h);
+            D.sb.vc_last = h->d_vclast();   // the memset before a one-simulation volume stage
+            D.F = h->force();
+            D.mem = membrane_args(h, g);
+            D.spread = spread_args(h, g);
+            D.lbm = lbm_args(h, b->base_cur[i] ^ k);
+            D.adv = advect_args(h, g);
+            D.vol = volume_args(h, g, 1);
+            int zpt = b->lbm_planes > 0 ? b->lbm_planes : (h->p.storage == RBC_STORE_F16 ? 4 : 2);
+            zpt = std::min(zpt, h->geo.nzc);
+            D.lbm_bx = (int)((h->geo.plane + tpb - 1) / tpb);
+            D.lbm_gy = (h->geo.nzc + zpt - 1) / zpt;
+            const long long words = (long long)h->geo.nzc * D.F.wpp;
+            constexpr int words_per_block = FUSED_CLEAR_THREADS;   // a warp per 32 words
+            const long long cnt[FSTAGES] = {(words + words_per_block - 1) / words_per_block, g.ncell,
+                                            (long long)g.ncell * g.npatch, (long long)D.lbm_bx * D.lbm_gy,
+                                            (long long)g.ncell * g.npatch, g.ncell};
+            for (int st = 0; st < FSTAGES; st++) {
+                boff[((size_t)k * FSTAGES + st) * (n + 1) + i] = acc[st];
+                if ((long long)acc[st] + cnt[st] >= (1LL << 31)) {
+                    b->err = "fused batch: more than 2^31 blocks in one stage";
+                    return RBC_ERR_UNSUPPORTED;
+                }
+                acc[st] += (int)cnt[st];
+            }
+        }
+        for (int st = 0; st < FSTAGES; st++) {
+            boff[((size_t)k * FSTAGES + st) * (n + 1) + n] = acc[st];
+            nblocks[st] = acc[st];
+        }
+    }
+    const size_t dbytes = sizeof(DomainArgs) * dom.size(), obytes = sizeof(int) * boff.size();
+    CKB(cudaMalloc(&b->fmem, dbytes + obytes));
+    DomainArgs *d_dom = (DomainArgs *)b->fmem;
+    int *d_boff = (int *)((char *)b->fmem + dbytes);
+    CKB(cudaMemcpy(d_dom, dom.data(), dbytes, cudaMemcpyHostToDevice));
+    CKB(cudaMemcpy(d_boff, boff.data(), obytes, cudaMemcpyHostToDevice));
+    const bool fp64 = h0->p.membrane_fp64 != 0, xper = h0->geo.xper != 0;
+    for (int k = 0; k < 2; k++) {
+        FusedLaunch f[FSTAGES];
+        for (int st = 0; st < FSTAGES; st++)
+            f[st] = FusedLaunch{d_dom + (size_t)k * n, d_boff + ((size_t)k * FSTAGES + st) * (n + 1), n, nblocks[st]};
+        cudaGraph_t graph = nullptr;
+        CKB(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+        launch_step_begin_fused(f[FS_CLEAR], b->stream);
+        launch_membrane_fused(f[FS_MEMBRANE], fp64, V, vpt, b->stream);
+        launch_spread_fused(f[FS_SPREAD], xper, b->stream);
+        launch_lbm_fused(f[FS_LBM], h0->p.storage, off32, tpb, b->stream);
+        launch_clear_bits_fused(f[FS_CLEAR], b->stream);   // the force reset after the read
+        launch_advect_fused(f[FS_ADVECT], xper, b->stream);
+        launch_volume_fused(f[FS_VOLUME], V, b->stream);
+        const cudaError_t le = cudaGetLastError();
+        const cudaError_t e = cudaStreamEndCapture(b->stream, &graph);
+        if (le != cudaSuccess || e != cudaSuccess) {
+            if (graph) cudaGraphDestroy(graph);
+            b->err = std::string("fused batch capture: ") + cudaGetErrorString(le != cudaSuccess ? le : e);
+            return RBC_ERR_CUDA;
+        }
+        const cudaError_t ei = cudaGraphInstantiate(&b->graph[k], graph, 0);
+        cudaGraphDestroy(graph);
+        if (ei != cudaSuccess) { b->graph[k] = nullptr; b->err = std::string("fused batch instantiate: ") + cudaGetErrorString(ei); return RBC_ERR_CUDA; }
+    }
+    b->fused = true;
+    return RBC_OK;
 }
 
 // The batch graph for parity k: every simulation's whole step (from buffer
@@ -1013,6 +1191,11 @@ int batch_build(rbc_batch *b)
     const int n = (int)b->h.size();
     for (int i = 0; i < n; i++) b->base_cur[i] = b->h[i]->cur;
     b->parity = 0;
+    if (b->use_fused && fused_obstacle(b).empty()) {
+        const int rc = batch_build_fused(b);
+        if (rc != RBC_OK) batch_free_graphs(b);
+        return rc;
+    }
     for (int k = 0; k < 2; k++) {
         cudaGraph_t g = nullptr;
         CKB(cudaGraphCreate(&g, 0));
@@ -1236,6 +1419,8 @@ int rbc_create(const rbc_params *p, const rbc_mesh *mesh, const int *bc, rbc_han
             cudaEventCreateWithFlags(&h->join, cudaEventDisableTiming) != cudaSuccess ||
             cudaEventCreateWithFlags(&h->wave_done, cudaEventDisableTiming) != cudaSuccess ||
             cudaEventCreateWithFlags(&h->spread_done, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&h->lbm_done, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&h->reset_done, cudaEventDisableTiming) != cudaSuccess ||
             cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, h->device) != cudaSuccess) {
             h->err = "stream creation failed";
             return bail(RBC_ERR_CUDA);
@@ -1511,11 +1696,11 @@ int rbc_ibm_st1(rbc_handle *h)
 {
     if (!h) return RBC_ERR_ARG;
     RBC_DEVICE_GUARD(h);
-    if (h->force_pending)   // ibm_st1a: start from zero (ibm.cu:315-320)
+    if (h->force_pending) {   // ibm_st1a: start from zero (ibm.cu:315-320)
         CK(cudaMemsetAsync(h->Fint, 0, 24 * h->geo.nint, h->stream));
-    int rc = clear_force_bits(h, h->stream);
-    if (rc) return rc;
-    rc = launch_spread_stage(h);
+        CK(cudaMemsetAsync(h->Fbits, 0, h->force_bit_bytes(), h->stream));
+    }
+    int rc = launch_spread_stage(h);
     if (rc) return rc;
     h->force_pending = true;
     return RBC_OK;
@@ -1689,16 +1874,18 @@ int rbc_profile_steps(rbc_handle *h, int nsteps, double *kernel_ms)
         cudaEventRecord(ev[2], h->stream);
         if (!rc) rc = launch_spread_stage(h);
         cudaEventRecord(ev[3], h->stream);
-        if (!rc) rc = launch_lbm_stage(h);
+        if (!rc) rc = launch_lbm_stage(h, false);
         cudaEventRecord(ev[4], h->stream);
-        if (!rc) rc = launch_advect_stage(h);
+        if (!rc) rc = launch_force_reset_stage(h, h->stream);
         cudaEventRecord(ev[5], h->stream);
+        if (!rc) rc = launch_advect_stage(h);
+        cudaEventRecord(ev[6], h->stream);
         if (!rc) rc = launch_thinc_stage(h);
         if (!rc && h->vof() && (h->iter + s + 1) % h->p.vof_k == 0) rc = launch_front_tracking_stage(h);
-        cudaEventRecord(ev[6], h->stream);
-        if (!rc) rc = launch_volume_stage(h, h->stream);
         cudaEventRecord(ev[7], h->stream);
-        if (cudaEventSynchronize(ev[7]) != cudaSuccess) { rc = RBC_ERR_CUDA; h->err = "profiled step failed"; break; }
+        if (!rc) rc = launch_volume_stage(h, h->stream);
+        cudaEventRecord(ev[8], h->stream);
+        if (cudaEventSynchronize(ev[8]) != cudaSuccess) { rc = RBC_ERR_CUDA; h->err = "profiled step failed"; break; }
         for (int k = 0; k < RBC_NUM_KERNELS; k++) {
             float ms = 0.f;
             cudaEventElapsedTime(&ms, ev[k], ev[k + 1]);
@@ -1879,11 +2066,15 @@ int rbc_batch_step(rbc_batch *b, int nsteps)
         b->parity ^= 1;
     }
     CKB(cudaEventRecord(b->done, b->stream));
+    if (b->fused) b->launches += (long long)FUSED_KERNELS_PER_STEP * nsteps;
     for (int i = 0; i < n; i++) {
         rbc_handle *h = b->h[i];
         if (nsteps & 1) h->cur ^= 1;
         h->iter += nsteps;
-        h->launches += (long long)h->kernels_per_step() * nsteps;
+        if (!b->fused) {   // the batch graph ran each simulation's own step kernels
+            h->launches += (long long)h->kernels_per_step() * nsteps;
+            b->launches += (long long)h->kernels_per_step() * nsteps;
+        }
         h->metrics_valid = h->has_cells();   // each simulation's step ends with its volume correction
         CKB(cudaStreamWaitEvent(h->stream, b->done, 0));
     }
@@ -1905,6 +2096,23 @@ int rbc_batch_synchronize(rbc_batch *b)
     return RBC_OK;
 }
 
+namespace {
+
+// device time of steps_per_trial batch steps after one untimed step (which
+// builds the graphs); -1 on an error
+float batch_trial(rbc_batch *b, int steps_per_trial, cudaEvent_t t0, cudaEvent_t t1, int *rc)
+{
+    if ((*rc = rbc_batch_step(b, 1))) return -1.f;
+    if (cudaEventRecord(t0, b->stream) != cudaSuccess) { *rc = RBC_ERR_CUDA; return -1.f; }
+    if ((*rc = rbc_batch_step(b, steps_per_trial))) return -1.f;
+    float ms = 0.f;
+    if (cudaEventRecord(t1, b->stream) != cudaSuccess || cudaEventSynchronize(t1) != cudaSuccess ||
+        cudaEventElapsedTime(&ms, t0, t1) != cudaSuccess) { *rc = RBC_ERR_CUDA; return -1.f; }
+    return ms;
+}
+
+}  // namespace
+
 int rbc_batch_autotune(rbc_batch *b, int steps_per_trial, int *chain_out)
 {
     if (!b || steps_per_trial < 1) return RBC_ERR_ARG;
@@ -1913,24 +2121,93 @@ int rbc_batch_autotune(rbc_batch *b, int steps_per_trial, int *chain_out)
     cudaEvent_t t0 = nullptr, t1 = nullptr;
     CKB(cudaEventCreate(&t0));
     CKB(cudaEventCreate(&t1));
-    int best = b->chain, rc = RBC_OK;
-    float best_ms = 0.f;
-    for (int chain = 1; chain <= n && rc == RBC_OK; chain *= 2) {
-        if ((rc = rbc_batch_set_chain(b, chain))) break;
-        if ((rc = rbc_batch_step(b, 1))) break;   // builds the graphs and warms them up
-        if (cudaEventRecord(t0, b->stream) != cudaSuccess) { rc = RBC_ERR_CUDA; break; }
-        if ((rc = rbc_batch_step(b, steps_per_trial))) break;
-        float ms = 0.f;
-        if (cudaEventRecord(t1, b->stream) != cudaSuccess || cudaEventSynchronize(t1) != cudaSuccess ||
-            cudaEventElapsedTime(&ms, t0, t1) != cudaSuccess) { rc = RBC_ERR_CUDA; break; }
-        if (chain == 1 || ms < best_ms) { best_ms = ms; best = chain; }
-        if (chain >= 64) break;   // longer chains only serialise more
+    int rc = RBC_OK;
+    if (b->use_fused && fused_obstacle(b).empty()) {
+        // fused form: the launch shapes, each tried for steps_per_trial steps --
+        // collide-stream threads per block and planes per thread, membrane
+        // vertices per thread (the one-simulation choice and the next larger)
+        int V = 0;
+        for (rbc_handle *h : b->h) if (h->cg[0].ncell > 0) V = h->cg[0].V;
+        const int v0 = V > 0 ? membrane_default_vpt(V) : 1;
+        int best[3] = {b->lbm_threads, b->lbm_planes, b->mem_vpt};
+        float best_ms = -1.f;
+        for (int tpb : {128, 256})
+            for (int planes : {1, 2, 4})
+                for (int vpt : {v0, std::min(v0 + 1, 4)}) {
+                    if (vpt != v0 && vpt == std::min(v0 + 1, 4) && v0 == 4) continue;
+                    b->lbm_threads = tpb; b->lbm_planes = planes; b->mem_vpt = vpt;
+                    batch_free_graphs(b);
+                    const float ms = batch_trial(b, steps_per_trial, t0, t1, &rc);
+                    if (rc != RBC_OK) break;
+                    if (best_ms < 0.f || ms < best_ms) { best_ms = ms; best[0] = tpb; best[1] = planes; best[2] = vpt; }
+                }
+        b->lbm_threads = best[0]; b->lbm_planes = best[1]; b->mem_vpt = best[2];
+        batch_free_graphs(b);
+    } else {
+        // child graphs: the simulations per dependency chain
+        int best = b->chain;
+        float best_ms = 0.f;
+        for (int chain = 1; chain <= n && rc == RBC_OK; chain *= 2) {
+            if ((rc = rbc_batch_set_chain(b, chain))) break;
+            const float ms = batch_trial(b, steps_per_trial, t0, t1, &rc);
+            if (rc != RBC_OK) break;
+            if (chain == 1 || ms < best_ms) { best_ms = ms; best = chain; }
+            if (chain >= 64) break;   // longer chains only serialise more
+        }
+        if (rc == RBC_OK) rc = rbc_batch_set_chain(b, best);
     }
     cudaEventDestroy(t0);
     cudaEventDestroy(t1);
     if (rc != RBC_OK) return rc;
-    if ((rc = rbc_batch_set_chain(b, best))) return rc;
-    if (chain_out) *chain_out = best;
+    if (chain_out) *chain_out = b->chain;
+    return RBC_OK;
+}
+
+int rbc_batch_set_form(rbc_batch *b, int fused)
+{
+    if (!b || (fused != 0 && fused != 1)) return RBC_ERR_ARG;
+    if (fused != b->use_fused) { b->use_fused = fused; batch_free_graphs(b); }
+    return RBC_OK;
+}
+
+int rbc_batch_get_form(const rbc_batch *b, int *fused, const char **obstacle)
+{
+    if (!b) return RBC_ERR_ARG;
+    static thread_local std::string why;
+    why = fused_obstacle(b);
+    if (fused) *fused = (b->use_fused && why.empty()) ? 1 : 0;
+    if (obstacle) *obstacle = why.c_str();
+    return RBC_OK;
+}
+
+int rbc_batch_set_shape(rbc_batch *b, int lbm_threads, int lbm_planes, int membrane_vpt)
+{
+    if (!b || (lbm_threads != 128 && lbm_threads != 256) || lbm_planes < 0 || lbm_planes > 8 ||
+        membrane_vpt < 0 || membrane_vpt > 4) return RBC_ERR_ARG;
+    if (membrane_vpt > 0) {   // the membrane block must fit its thread limit
+        for (rbc_handle *h : b->h)
+            if (h->cg[0].ncell > 0 && h->cg[0].V > 0 &&
+                membrane_threads(h->cg[0].V, membrane_vpt) > (membrane_vpt >= 3 ? 896 : 1024))
+                return RBC_ERR_ARG;
+    }
+    b->lbm_threads = lbm_threads; b->lbm_planes = lbm_planes; b->mem_vpt = membrane_vpt;
+    batch_free_graphs(b);
+    return RBC_OK;
+}
+
+int rbc_batch_get_shape(const rbc_batch *b, int *lbm_threads, int *lbm_planes, int *membrane_vpt)
+{
+    if (!b) return RBC_ERR_ARG;
+    if (lbm_threads) *lbm_threads = b->lbm_threads;
+    if (lbm_planes) *lbm_planes = b->lbm_planes;
+    if (membrane_vpt) *membrane_vpt = b->mem_vpt;
+    return RBC_OK;
+}
+
+int rbc_batch_launch_count(const rbc_batch *b, long long *count)
+{
+    if (!b || !count) return RBC_ERR_ARG;
+    *count = b->launches;
     return RBC_OK;
 }
 
@@ -1999,12 +2276,14 @@ struct AdjointState {
     cudaStream_t rev = nullptr;
     cudaEvent_t filled[2] = {nullptr, nullptr}, drained[2] = {nullptr, nullptr};
     std::map<long long, cudaGraphExec_t> graphs;
+    std::map<long long, long long> graph_kernels;   // kernels each graph launches
 };
 
 void adjoint_drop_graphs(AdjointState *a)
 {
     for (auto &kv : a->graphs) if (kv.second) cudaGraphExecDestroy(kv.second);
     a->graphs.clear();
+    a->graph_kernels.clear();
 }
 
 void adjoint_free(AdjointState *a)
@@ -2107,7 +2386,6 @@ int adjoint_restore(rbc_handle *h, int k)
     return d2d(h, h->d_iter(), a->ck_itd + k, sizeof(int));   // device to device: no host staging
 }
 
-constexpr int ADJ_KERNELS_PER_STEP = 14;   // 7 recomputation + 7 reverse kernels
 
 // Enqueue the recomputation of len steps from the handle's state into store b
 // (stream: the handle's).
@@ -2142,7 +2420,6 @@ int adjoint_enqueue_recompute_body(rbc_handle *h, int b, int len)
         CK_LAUNCH();
         if ((rc = launch_stress(h))) return rc;
         if ((rc = d2d(h, a->sFv + k * nv3, h->Fv, 4 * nv3))) return rc;
-        if ((rc = clear_force_bits(h, h->stream))) return rc;
         if ((rc = launch_spread_stage(h))) return rc;
         launch_force_to_f32(h->geo, h->Fint, a->sF + k * 3 * n, h->stream);   // the force the collision reads
         h->launches++;
@@ -2175,12 +2452,14 @@ int adjoint_enqueue_reverse(rbc_handle *h, int b, int len, int gb)
             va.hist = a->hist; va.escr = a->escr; va.status = a->status;
             va.nv = h->nv; va.V = h->V; va.E = h->E; va.ncell = h->ncell; va.kmax = a->kmax;
             launch_volume_adjoint(g, va, st);
+            h->launches++;
             CK_LAUNCH();
         }
         CK(cudaMemsetAsync(a->ubar, 0, 16 * n, st));
         if (h->ncell > 0) {
             launch_advect_adjoint(g, a->sX + k * nv3, a->suvr + k * n, a->Xabar, a->Xbar, (float *)a->ubar, h->nv,
                                   h->p.dt * h->p.M, h->d_flags(), st);
+            h->launches++;
             CK_LAUNCH();
         }
         LbmAdjArgs la{};
@@ -2191,10 +2470,12 @@ int adjoint_enqueue_reverse(rbc_handle *h, int b, int len, int gb)
         la.pd = a->sdrv + k; la.dfac = a->sfac + k;
         la.Bc = (float)h->p.B; la.omega = (float)(1.0 / h->p.tau); la.Cr = (float)h->p.Cr;
         launch_lbm_adjoint(g, la, st);
+        h->launches++;
         CK_LAUNCH();
         gb ^= 1;
         if (h->ncell > 0) {
             launch_spread_adjoint(g, a->sX + k * nv3, a->sFv + k * nv3, a->Fbar, h->mask2d, a->Fvbar, a->Xbar, h->nv, st);
+            h->launches++;
             CK_LAUNCH();
             MembraneAdjArgs ma{};
             ma.Xd = a->sXd + k * nv3; ma.nv = h->nv; ma.ne = h->ne; ma.gref = h->gref;
@@ -2206,6 +2487,7 @@ int adjoint_enqueue_reverse(rbc_handle *h, int b, int len, int gb)
             ma.C = h->p.C; ma.rgs = h->cg[0].rgs; ma.law = h->p.law; ma.LX = h->p.LX; ma.LZ = h->p.LZ;
             ma.niter = h->p.solver_iters > 0 ? h->p.solver_iters : DEFAULT_SOLVER_ITERS;
             launch_membrane_adjoint(ma, st);
+            h->launches += 3;   // the solve, element and vertex passes
             CK_LAUNCH();
         }
     }
@@ -2228,6 +2510,7 @@ int adjoint_launch_graph(rbc_handle *h, int kind, int b, int parity, int len)
         CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
         const int rc = kind == 0 ? adjoint_enqueue_recompute(h, b, len) : adjoint_enqueue_reverse(h, b, len, parity);
         const cudaError_t e = cudaStreamEndCapture(st, &graph);
+        const long long kernels = h->launches - launches0;   // the launches the capture recorded
         h->launches = launches0;
         h->cur = cur0;
         if (rc != RBC_OK) { if (graph) cudaGraphDestroy(graph); return rc; }
@@ -2237,9 +2520,10 @@ int adjoint_launch_graph(rbc_handle *h, int kind, int b, int parity, int len)
         cudaGraphDestroy(graph);
         if (ei != cudaSuccess) { h->err = std::string("adjoint graph instantiate: ") + cudaGetErrorString(ei); return RBC_ERR_CUDA; }
         it = a->graphs.emplace(key, exec).first;
+        a->graph_kernels[key] = kernels;
     }
     CK(cudaGraphLaunch(it->second, st));
-    h->launches += (long long)len * (ADJ_KERNELS_PER_STEP / 2);
+    h->launches += a->graph_kernels[key];
     if (kind == 0) {   // the recomputation advanced the handle
         if (len & 1) h->cur ^= 1;
         h->iter += len;

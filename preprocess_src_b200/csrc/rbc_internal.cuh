@@ -98,8 +98,10 @@ __device__ __forceinline__ void delta4(float f, float w[4]) {
 // node it adds to.  Integer sums are exact, so the spread's result does not depend
 // on the order of its global atomics (several patches and cells add to a node).
 // The collide-stream kernel reads, converts (one rounding to FP32) and zeroes the
-// nodes whose bit is set, so only nodes near membranes cost force traffic; the
-// words are cleared (a memset) before each step's spread.  Sums are exact while |F| < 2^(63 - FORCE_FRAC) = 128 at
+// nodes whose bit is set, so only nodes near membranes cost force traffic.
+// After that read a reset kernel zeroes the forces of the nodes whose bit is
+// set and clears the words (force_reset_words).  The collide-stream kernel only
+// reads the field: zeroing it there made that kernel 2x slower.  Sums are exact while |F| < 2^(63 - FORCE_FRAC) = 128 at
 // every node (partial sums may wrap; the adds are modular); a contribution of
 // 64 or more raises RBC_FLAG_NONFINITE (a lattice force density of that size
 // has long broken the LBM).
@@ -116,7 +118,7 @@ __host__ __device__ constexpr int force_words_per_plane(long long plane) { retur
 struct LbmArgs {
     const void *gin; void *gout;
     float4 *uvr;
-    ForceField F;              // read, converted and zeroed where the occupancy bit is set
+    ForceField F;              // read and converted where the occupancy bit is set
     const uint32_t *mask2d;
     const float *drive;        // device scalar: P * drive factor of this step
     const int *iter;           // device: the step counter, which seeds the FP16 stochastic rounding
@@ -301,8 +303,35 @@ struct StepBeginArgs {
     float *wall;               // [2] top, bottom; NULL outside the shear mode
     double sr, LY; int walls;  // shear rate, wall distance, 0 both walls / 1 top wall
     float *drive_rec; double *factor_rec;   // where the adjoint keeps the step's drive (may be NULL)
+    int *vc_last;              // when set, zeroed (the volume correction's count of this step; fused batches)
 };
 void launch_step_begin(const StepBeginArgs &a, cudaStream_t s);
+
+// The force field's reset after the collide-stream kernel read it: every word
+// of occupancy bits that is set zeroes its nodes' forces (only those: the rest
+// is zero already), then itself.  One warp per 32 consecutive words: lane l
+// loads word w0 + l (one coalesced load), then the warp zeroes the nodes of
+// each set word in turn (lane l owns node xy = 32 ((w0 + j) mod wpp) + l of
+// word j) and every lane clears its own word.
+__device__ __forceinline__ void force_reset_words(long long *__restrict__ F, uint32_t *__restrict__ bits, long long w0,
+                                                  long long nwords, int wpp, long long plane, long long nint, int lane)
+{
+    const long long wl = w0 + lane;
+    const uint32_t mine = wl < nwords ? bits[wl] : 0u;
+    unsigned pending = __ballot_sync(0xffffffffu, mine != 0u);
+    while (pending) {
+        const int j = __ffs(pending) - 1;
+        pending &= pending - 1;
+        const uint32_t word = __shfl_sync(0xffffffffu, mine, j);
+        const long long w = w0 + j, z = w / wpp, xy = (w - z * wpp) * 32 + lane;
+        if (((word >> lane) & 1u) && xy < plane) {
+            const long long idx = z * plane + xy;
+            F[idx] = 0; F[nint + idx] = 0; F[2 * nint + idx] = 0;
+        }
+    }
+    if (mine) bits[wl] = 0u;
+}
+void launch_force_reset(const Geom &g, const ForceField &F, cudaStream_t s);
 
 // ---- adjoint of one step (adjoint.cu); FP32 populations ----------------------
 
@@ -405,7 +434,7 @@ __device__ __forceinline__ int fused_domain(const int *__restrict__ boff, int nd
 }
 constexpr int FUSED_CLEAR_THREADS = 256;
 void launch_step_begin_fused(const FusedLaunch &f, cudaStream_t s);   // one thread per domain
-void launch_clear_bits_fused(const FusedLaunch &f, cudaStream_t s);   // FUSED_CLEAR_THREADS words per block
+void launch_clear_bits_fused(const FusedLaunch &f, cudaStream_t s);   // the force reset, FUSED_CLEAR_THREADS words per block
 void launch_membrane_fused(const FusedLaunch &f, bool fp64, int V, int vpt, cudaStream_t s);   // a block per cell
 void launch_spread_fused(const FusedLaunch &f, bool xper, cudaStream_t s);    // a block per (cell, patch)
 void launch_lbm_fused(const FusedLaunch &f, int storage, bool off32, int threads, cudaStream_t s);

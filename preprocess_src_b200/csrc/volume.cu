@@ -207,6 +207,7 @@ __device__ __forceinline__ void step_begin_body(const StepBeginArgs &a)
     *a.drive = (float)(a.P * wi);
     if (a.drive_rec) *a.drive_rec = (float)(a.P * wi);   // kept for the adjoint of the step
     if (a.factor_rec) *a.factor_rec = wi;
+    if (a.vc_last) *a.vc_last = 0;
     if (a.wall) {   // lbm.cu:752 (sra), 946-964: allwall -/+ sra LY/2, topwall sra LY at the top
         const double sra = (it < a.flowstart) ? 0.0 : a.sr;
         a.wall[0] = (float)(a.walls == 0 ? sra * a.LY / 2.0 : sra * a.LY);
@@ -237,15 +238,16 @@ void launch_step_begin_fused(const FusedLaunch &f, cudaStream_t s)
     step_begin_fused_kernel<<<(f.ndom + 127) / 128, 128, 0, s>>>(f.dom, f.ndom);
 }
 
-// occupancy words of every domain's lattice force to zero (the memset of a
-// one-simulation step)
+// the force reset of every domain after its collide-stream launch, one warp
+// per 32 occupancy words
 __global__ void __launch_bounds__(FUSED_CLEAR_THREADS)
 clear_bits_fused_kernel(const DomainArgs *__restrict__ dom, const int *__restrict__ boff, int ndom)
 {
     const int d = fused_domain(boff, ndom, blockIdx.x);
     const DomainArgs &D = dom[d];
-    const long long w = (long long)(blockIdx.x - boff[d]) * FUSED_CLEAR_THREADS + threadIdx.x;
-    if (w < (long long)D.g.nzc * D.F.wpp) D.F.bits[w] = 0u;
+    const long long nw = (long long)D.g.nzc * D.F.wpp;
+    const long long w0 = (((long long)(blockIdx.x - boff[d]) * FUSED_CLEAR_THREADS + threadIdx.x) >> 5) * 32;
+    if (w0 < nw) force_reset_words(D.F.F, D.F.bits, w0, nw, D.F.wpp, D.g.plane, D.g.nint, threadIdx.x & 31);
 }
 
 void launch_clear_bits_fused(const FusedLaunch &f, cudaStream_t s)

@@ -332,8 +332,10 @@ class Simulation:
 
 class Batch:
     """Independent simulations stepped together (rbc_batch_*): every batch step
-    is one CUDA graph launch whose nodes are the simulations' whole steps.  The
-    simulations stay usable on their own between batch steps."""
+    is one CUDA graph launch -- in the fused form seven launches, one per stage,
+    each over the blocks of all simulations; otherwise the simulations' whole
+    steps as child graphs.  The simulations stay usable on their own between
+    batch steps."""
 
     def __init__(self, sims):
         self.sims = list(sims)   # the handles must outlive the batch
@@ -385,9 +387,42 @@ class Batch:
         self._call("rbc_batch_set_chain", int(value))
 
     def autotune(self, steps_per_trial: int = 3) -> int:
-        """Picks the chain length with the fastest batch step; the timed steps
-        advance every simulation."""
+        """Picks the fastest launch shapes (fused form) or chain length (child
+        graphs); the timed steps advance every simulation.  Returns the chain."""
         v = C.c_int(0)
         self._call("rbc_batch_autotune", int(steps_per_trial), C.byref(v))
+        return v.value
+
+    @property
+    def fused(self) -> bool:
+        """Whether the next step uses the fused form."""
+        v = C.c_int(0)
+        self._call("rbc_batch_get_form", C.byref(v), None)
+        return bool(v.value)
+
+    def obstacle(self) -> str:
+        """Why the simulations cannot run in the fused form ("" if they can)."""
+        v, msg = C.c_int(0), C.c_char_p()
+        self._call("rbc_batch_get_form", C.byref(v), C.byref(msg))
+        return (msg.value or b"").decode()
+
+    def set_form(self, fused: bool):
+        self._call("rbc_batch_set_form", 1 if fused else 0)
+
+    @property
+    def shape(self) -> tuple[int, int, int]:
+        """(collide-stream threads per block, z planes per thread, membrane
+        vertices per thread) of the fused form; 0 = automatic."""
+        a, b, c = C.c_int(0), C.c_int(0), C.c_int(0)
+        self._call("rbc_batch_get_shape", C.byref(a), C.byref(b), C.byref(c))
+        return a.value, b.value, c.value
+
+    def set_shape(self, lbm_threads: int = 256, lbm_planes: int = 0, membrane_vpt: int = 0):
+        self._call("rbc_batch_set_shape", int(lbm_threads), int(lbm_planes), int(membrane_vpt))
+
+    @property
+    def launches(self) -> int:
+        v = C.c_longlong(0)
+        self._call("rbc_batch_launch_count", C.byref(v))
         return v.value
 

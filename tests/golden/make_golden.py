@@ -9,6 +9,7 @@ oracle/ref_harness (def.h stand-in, helper shims, driver).
     python tests/golden/make_golden.py build [CASE...]          # here: nvcc, needs the reference sources
     python tests/golden/make_golden.py run OUTDIR [CASE...]     # on a GPU: writes OUTDIR/<case>.npz
     python tests/golden/make_golden.py run-dense OUTDIR         # on a GPU: OUTDIR/c2_dense_suspension.npz
+    python tests/golden/make_golden.py run-files OUTDIR         # on a GPU: files of the reference's output_data
     python tests/golden/make_golden.py time-dense       # on a GPU: reference step timing, dense suspension
 
 OUTDIR defaults to tests/golden, where the committed fixtures live.
@@ -154,6 +155,22 @@ def ref_defs(case) -> str:
     return d
 
 
+def file_cases():
+    """Cases whose fixture holds the files the reference's own output_data
+    (etc.cu:449-790) wrote: two red cells in a 16 x 12 x 12 duct, after
+    FILE_STEPS steps, fnum = FILE_FNUM.  Red cells only: with N_W > 0 the
+    reference's output_data does not compile (etc.cu:863-866 redeclare tv and
+    leave a declaration list without its ';')."""
+    return {"g8_duct16x12x12_files": configs.duct_case("g8_duct16x12x12_files", 16, 12, 12,
+                                                       centers_duct=[(4.2, 5.6, 5.4), (12.1, 5.3, 5.7)],
+                                                       subdiv=3, radius=3.2, seed=28, g=4e-5, Gs=2e-3,
+                                                       residual=1e-12)}
+
+
+FILE_STEPS, FILE_FNUM = 4, 50
+FILE_NAMES = ("restart.bin", f"prof{FILE_FNUM:04d}.bin", f"cell/cell{FILE_FNUM:04d}.bin", f"center{FILE_FNUM:04d}.dat")
+
+
 def bench_cases():
     """The workloads bench.py's reference arm times with the reference's own
     kernels: the dense suspension and the single-cell duct (tag -> Case)."""
@@ -163,12 +180,14 @@ def bench_cases():
 def build(names=(), if_present=False):
     """Reference-kernel libraries of the golden and bench cases; if_present:
     skip quietly when the reference sources are absent (the recipe checks)."""
-    for name, case in list(golden_cases().items()) + list(bench_cases().items()):
+    files = file_cases()
+    for name, case in list(golden_cases().items()) + list(bench_cases().items()) + list(files.items()):
         if names and name not in names:
             continue
         target = "ref-if-present" if if_present else "ref"
+        extra = ["REFETC=1"] if name in files else []
         subprocess.run(["make", "-s", "-C", str(ROOT / "oracle"), target, f"REFTAG={name}",
-                        f"REFDEFS={ref_defs(case)}"], check=True)
+                        f"REFDEFS={ref_defs(case)}", *extra], check=True)
         if (REF_DIR / f"librefstep_{name}.so").exists():
             print("built", REF_DIR / f"librefstep_{name}.so")
 
@@ -290,6 +309,34 @@ def run_dense(outdir):
     print("wrote", outdir / "c2_dense_suspension.npz")
 
 
+def run_files(outdir):
+    """Run each file case FILE_STEPS steps with the reference's kernels, let its
+    output_data write the files and keep their bytes (uint8 arrays) and the
+    text of center%04d.dat in OUTDIR/<case>.npz."""
+    import os
+    import tempfile
+    outdir = Path(outdir).resolve()
+    outdir.mkdir(parents=True, exist_ok=True)
+    for name, case in file_cases().items():
+        ref = Ref(name, case)
+        ref.step(FILE_STEPS)
+        cwd = os.getcwd()
+        with tempfile.TemporaryDirectory() as tmp:
+            (Path(tmp) / "result" / "cell").mkdir(parents=True)
+            os.chdir(tmp)
+            try:
+                rc = ref.L.ref_write_files(FILE_FNUM)
+            finally:
+                os.chdir(cwd)
+            if rc:
+                raise RuntimeError(f"reference output_data failed: {rc}")
+            data = {f"file_{k}": np.frombuffer((Path(tmp) / "result" / k).read_bytes(), dtype=np.uint8)
+                    for k in FILE_NAMES}
+        data["steps"], data["fnum"] = np.array(FILE_STEPS), np.array(FILE_FNUM)
+        np.savez_compressed(outdir / f"{name}.npz", **data)
+        print("wrote", outdir / f"{name}.npz", {k: v.size for k, v in data.items()})
+
+
 def time_dense(steps=3):
     case = dense_case()
     ref = Ref("dense", case)
@@ -314,6 +361,8 @@ if __name__ == "__main__":
         build(sys.argv[2:])
     elif cmd == "run":
         run(sys.argv[2] if len(sys.argv) > 2 else ROOT / "tests" / "golden", sys.argv[3:])
+    elif cmd == "run-files":
+        run_files(sys.argv[2] if len(sys.argv) > 2 else ROOT / "tests" / "golden")
     elif cmd == "run-dense":
         run_dense(sys.argv[2] if len(sys.argv) > 2 else ROOT / "tests" / "golden")
     elif cmd == "time-dense":

@@ -153,3 +153,56 @@ def test_output_averages_match_the_oracle(native_lib, oracle_mod, tmp_path):
     print(f"tp rel L2 {rel_l2(c['tp'], tp):.3e}  qi rel L2 {rel_l2(c['qi'], qi):.3e}")
     assert rel_l2(c["tp"], tp) <= 1e-4
     assert rel_l2(c["qi"], qi) <= 1e-4
+
+
+def test_reads_and_writes_the_reference_writers_files(native_lib, tmp_path):
+    """restart.bin, cell%04d.bin, prof%04d.bin and center%04d.dat written by the
+    reference's own output_data (etc.cu:449-790) after four steps of its own
+    kernels: rbc_read_restart takes the state from the reference's restart.bin,
+    and the library's writers then write the same layouts with the same values
+    (FP64 positions, averages, centroids and connectivity exact; populations
+    and velocities as the FP32 step stores them)."""
+    from preprocess_src_b200.step import Simulation
+    from tests.test_ref_files_host import _file_golden
+    cases = _file_golden()
+    if not cases:
+        pytest.skip("no output-file fixture")
+    for name, case, g, names in cases:
+        n, N, V, E = case.n, case.ncell, case.vertex, case.element
+        fnum = int(g["fnum"])
+        ref = {}
+        for k in names:
+            p = tmp_path / ("ref_" + k.replace("/", "_"))
+            p.write_bytes(g[f"file_{k}"].tobytes())
+            ref[k] = p
+        with Simulation(case) as sim:
+            sim.set_output_interval(1000000)
+            assert sim.read_restart(ref["restart.bin"]) == fnum
+            assert sim.iter == int(g["steps"])
+            sim.read_center_file(ref[f"center{fnum:04d}.dat"])
+            sim.write_restart(tmp_path / "restart.bin", fnum=fnum)
+            sim.write_cell_file(tmp_path / "cell.bin")
+            sim.write_prof_file(tmp_path / "prof.bin")
+            sim.write_center_file(tmp_path / "center.dat")
+        a = RF.read_restart(ref["restart.bin"], n, N, V, E)
+        b = RF.read_restart(tmp_path / "restart.bin", n, N, V, E)
+        assert (tmp_path / "restart.bin").stat().st_size == ref["restart.bin"].stat().st_size
+        for k in ("iter", "fnum", "x", "y", "z", "qi", "tp", "rx", "ry", "rz"):
+            np.testing.assert_array_equal(b[k], a[k], err_msg=k)
+        m = np.repeat(case.bc == 0, 19)
+        assert np.abs(b["fn"][m] - a["fn"][m]).max() <= 1e-9   # FP32 (f - w): ~1e-10 here
+        for k in ("dm", "um", "vm", "wm", "u", "v", "w"):
+            scale = max(np.abs(a[k]).max(), 1e-30)
+            assert np.abs(b[k] - a[k]).max() <= 1e-6 * scale, k
+        ca, cb = RF.read_cell_file(ref[f"cell/cell{fnum:04d}.bin"]), RF.read_cell_file(tmp_path / "cell.bin")
+        for k in ("N", "V", "E", "x", "y", "z", "qi", "tp", "ele"):
+            np.testing.assert_array_equal(cb[k], ca[k], err_msg=k)
+        for k in ("u", "v", "w"):
+            assert np.abs(cb[k] - ca[k]).max() <= 1e-6 * np.abs(ca[k]).max(), k
+        pa, pb = RF.read_prof_file(ref[f"prof{fnum:04d}.bin"], n), RF.read_prof_file(tmp_path / "prof.bin", n)
+        np.testing.assert_array_equal(pb["iter"], pa["iter"])
+        np.testing.assert_array_equal(pb["bc"], pa["bc"])
+        mc = case.bc == 0
+        for k in ("dm", "um", "vm", "wm"):
+            assert np.abs(pb[k][mc] - pa[k][mc]).max() <= 1e-6 * max(np.abs(pa[k][mc]).max(), 1e-30), k
+        assert (tmp_path / "center.dat").read_text() == ref[f"center{fnum:04d}.dat"].read_text()

@@ -390,7 +390,7 @@ def test_launch_count_and_status(developed):
     sim = load(o)
     n0 = sim.launches
     sim.step(4)
-    assert sim.launches - n0 == 4 * 6
+    assert sim.launches - n0 == 4 * 7   # step begin, membrane, spread, collide-stream, force reset, advect, volume
     flags, _ = sim.status()
     assert flags == 0, flags
 
@@ -412,7 +412,7 @@ def test_split_membrane_wave_equals_stage_calls(native_lib):
     with Simulation(case) as a, Simulation(case) as b:
         n0 = a.launches
         a.step(nsteps)
-        assert a.launches - n0 == nsteps * (6 + 2)   # two more launches per step
+        assert a.launches - n0 == nsteps * (7 + 2)   # two more launches per step
         for _ in range(nsteps):
             b.iter = b.iter + 1
             b.stress(); b.ibm_st1(); b.lbm_d3q19(); b.ibm_st2(); b.volume_correction()

@@ -43,7 +43,7 @@ def test_split_population_equals_one_population(native_lib):
         n0 = b.launches
         a.step(6)
         b.step(6)
-        assert b.launches - n0 == 6 * 10   # step_begin, lbm, and 4 kernels per population
+        assert b.launches - n0 == 6 * 11   # step_begin, lbm, force reset, and 4 kernels per population
         ca, cr, cw = a.export_cells(), b.export_cells(), b.export_wbc()
         scale = np.abs(_xyz(ca)).max()
         assert np.abs(_xyz(cr) - _xyz(ca, slice(0, V))).max() <= 1e-9 * scale

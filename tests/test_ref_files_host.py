@@ -66,3 +66,50 @@ def test_cell_file_blocks(tmp_path):
     for _, vals in blocks:
         for k, v in vals.items():
             np.testing.assert_array_equal(got[k], v)
+
+
+def _file_golden():
+    from pathlib import Path
+
+    from tests.golden.make_golden import FILE_NAMES, file_cases
+    out = []
+    for name, case in file_cases().items():
+        p = Path(__file__).resolve().parent / "golden" / f"{name}.npz"
+        if p.exists():
+            out.append((name, case, np.load(p), FILE_NAMES))
+    return out
+
+
+def test_layouts_match_the_reference_writers_files(tmp_path):
+    """Files written by the reference's own output_data (etc.cu:449-790,
+    compiled from the reference sources; fixture made by make_golden.py
+    run-files): the numpy layouts parse every byte of them, and restart.bin and
+    center%04d.dat written back from the parsed fields are the same bytes."""
+    cases = _file_golden()
+    if not cases:
+        import pytest
+        pytest.skip("no output-file fixture")
+    for name, case, g, names in cases:
+        n, N, V, E = case.n, case.ncell, case.vertex, case.element
+        paths = {}
+        for k in names:
+            paths[k] = tmp_path / k.replace("/", "_")
+            paths[k].write_bytes(g[f"file_{k}"].tobytes())
+        fnum, steps = int(g["fnum"]), int(g["steps"])
+        r = RF.read_restart(paths["restart.bin"], n, N, V, E)
+        assert int(r["iter"][0]) == steps and int(r["fnum"][0]) == fnum
+        RF.write_restart(tmp_path / "again.bin", n, N, V, E, r)
+        assert (tmp_path / "again.bin").read_bytes() == paths["restart.bin"].read_bytes()
+        prof = RF.read_prof_file(paths[f"prof{fnum:04d}.bin"], n)
+        assert int(prof["iter"][0]) == steps
+        np.testing.assert_array_equal(prof["bc"], case.bc)
+        np.testing.assert_array_equal(prof["dm"], r["dm"])   # the same host copies in both files
+        cell = RF.read_cell_file(paths[f"cell/cell{fnum:04d}.bin"])
+        assert (int(cell["N"][0]), int(cell["V"][0]), int(cell["E"][0])) == (N, V, E)
+        np.testing.assert_array_equal(cell["ele"], case.ele_global())
+        for k in ("x", "y", "z", "u", "v", "w"):
+            np.testing.assert_array_equal(cell[k], r[k])
+        gx = RF.read_center(paths[f"center{fnum:04d}.dat"])
+        assert gx.size == 3 * N
+        RF.write_center(tmp_path / "center.dat", gx)
+        assert (tmp_path / "center.dat").read_text() == paths[f"center{fnum:04d}.dat"].read_text()
