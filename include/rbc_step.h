@@ -106,8 +106,8 @@ typedef struct rbc_params {
     double rgs;          /* tension normalisation cel->rg (1.0 for red cells) */
     int    law;          /* RBC_LAW_* */
     double br;           /* bending modulus BR of fourpoint_bend (stress.cu:448-578); 0 = none */
-    int    M;            /* sub-cycling factor; only 1 is implemented */
-    int    rk_order;     /* RUNGE_KUTTA; only 4 is implemented */
+    int    M;            /* sub-cycling factor M >= 1 (main.cu:78-106); no VOF, batch or adjoint with M > 1 */
+    int    rk_order;     /* RUNGE_KUTTA of the advection: 1, 2 or 4 (1 and 2 need dx = dt = 1) */
     /* implementation choices */
     int    storage;      /* RBC_STORE_* */
     int    membrane_fp64;/* 1: element mechanics in FP64, 0: FP32 */
@@ -171,7 +171,10 @@ int rbc_import_ref_lattice(rbc_handle *h, const double *fn);
  * dn/un/vn/wn [nx*ny*nz]: density and velocity of the last lbm step with the
  * reference's half-force shift (lbm.cu:1116-1118) on COMP nodes, their periodic
  * images on BUFF nodes (lbm.cu:1378-1432), and rho = 1, u = 0 on WALL nodes
- * (the values the reference's WALL nodes keep from flu_init). */
+ * (the values the reference's WALL nodes keep from flu_init).  With M > 1 the
+ * density and velocity are those of ltc->dmD / umD: the sums over the steps of
+ * the current cycle, the velocity averaged after its last step (lbm.cu:1097-1126,
+ * 1435-1460). */
 int rbc_export_ref_lattice(rbc_handle *h, double *fn, double *dn, double *un, double *vn, double *wn);
 /* Eulerian spread force ltc->fx/fy/fz [nx*ny*nz] after rbc_ibm_st1 and before
  * rbc_lbm_d3q19 (COMP nodes, folded as ibm.cu:214-296 leaves them). */
@@ -223,6 +226,10 @@ int rbc_get_iter(const rbc_handle *h, int *iter);
 /* calc_tension + calc_load + q2f, then fourpoint_bend when BR != 0 */
 int rbc_stress(rbc_handle *h);
 int rbc_ibm_st1(rbc_handle *h);
+/* With M > 1 the velocity sums and the force reset follow the place of step
+ * prc->iter (rbc_set_iter) among its M: the caller runs rbc_stress and
+ * rbc_ibm_st1 at the first of every M steps and rbc_ibm_st2 and
+ * rbc_volume_correction at the last, as main.cu:78-106 does. */
 int rbc_lbm_d3q19(rbc_handle *h);
 int rbc_ibm_st2(rbc_handle *h);
 /* *iters (may be NULL) receives the reference's return value, iterations - 1.
@@ -237,7 +244,9 @@ int rbc_thinc_wlic(rbc_handle *h);
  * Synchronous when iters != NULL.  rbc_step runs it every vof_k steps. */
 int rbc_front_tracking(rbc_handle *h, int *iters);
 /* nsteps full steps, each a replay of a CUDA graph of one step.  Asynchronous
- * (rbc_synchronize or any export waits for it). */
+ * (rbc_synchronize or any export waits for it).  With M > 1, nsteps lattice
+ * steps: each runs the stages of its place among its M (main.cu:78-106), and a
+ * call may end inside a cycle. */
 int rbc_step(rbc_handle *h, int nsteps);
 
 /* ---- diagnostics ------------------------------------------------------ */

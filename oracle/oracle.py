@@ -29,7 +29,7 @@ class OrcParams(C.Structure):
                 ("zmax", C.c_double), ("ncell", C.c_int), ("vertex", C.c_int), ("element", C.c_int),
                 ("mn", C.c_int), ("br", C.c_double), ("flow", C.c_int), ("sr", C.c_double), ("walls", C.c_int),
                 ("tube_r", C.c_double), ("lambda1", C.c_double), ("vof_k", C.c_int),
-                ("vof_residual", C.c_double), ("vof_itrmax", C.c_int)]
+                ("vof_residual", C.c_double), ("vof_itrmax", C.c_int), ("M", C.c_int), ("rk_order", C.c_int)]
 
 
 _STATE_D = ["fn", "fm", "dn", "un", "vn", "wn", "dm", "um", "vm", "wm", "fx", "fy", "fz"]
@@ -100,7 +100,8 @@ class Oracle:
                            flow=int(p.get("flow", 0)), sr=float(p.get("sr", 0.0)), walls=int(p.get("walls", 0)),
                            tube_r=float(p.get("tube_r", 0.0)), lambda1=float(p.get("lambda1", 1.0)),
                            vof_k=int(p.get("vof_k", 0)), vof_residual=float(p.get("vof_residual", 1e-10)),
-                           vof_itrmax=int(p.get("vof_itrmax", 20000)))
+                           vof_itrmax=int(p.get("vof_itrmax", 20000)), M=int(p.get("M", 1)),
+                           rk_order=int(p.get("rk_order", 4)))
         n = case.n
         self.a = {}
         for k in _STATE_D:

@@ -592,44 +592,72 @@ void orc_ibm_st1(const orc_params *p, orc_state *s)
     }
 }
 
-/* ibm.cu:372-639 (ibm_st2a, RUNGE_KUTTA == 4) */
+static int orc_M(const orc_params *p) { return p->M > 0 ? p->M : 1; }
+static int orc_rk(const orc_params *p) { return p->rk_order > 0 ? p->rk_order : 4; }
+
+/* The interpolated velocity at (xr, yr, zr) (ibm.cu:444-482).  The RUNGE_KUTTA
+ * == 4 branch works in physical units (xtr / dx, cos(pi |ix dx - xtr| / 2 dx));
+ * the 2 and 1 branches (ibm.cu:522-556, 579-612) leave dx out (xtr = xr + (nx -
+ * 1) / 2, cos(pi |ix - xtr| / 2)), the same for dx = 1.  Both visit the 4 x 4 x 4
+ * nodes of nonzero weight (a node at distance 2 has weight 0). */
+static void interp_velocity(const orc_params *p, const orc_state *s, int with_dx, double xr, double yr, double zr,
+                            double *ur, double *vr, double *wr)
+{
+    const int nx = p->nx, ny = p->ny, nz = p->nz;
+    const double dx = with_dx ? p->dx : 1.0;
+    double u = 0.0, v = 0.0, w = 0.0;
+    const double xtr = xr + (double)(nx - 1) * dx / 2.0;
+    const double ytr = yr + (double)(ny - 1) * dx / 2.0;
+    const double ztr = zr + (double)(nz - 1) * dx / 2.0;
+    const int x1 = (int)floor(xtr / dx) - 1, x2 = (int)ceil(xtr / dx) + 1;
+    const int y1 = (int)floor(ytr / dx) - 1, y2 = (int)ceil(ytr / dx) + 1;
+    const int z1 = (int)floor(ztr / dx) - 1, z2 = (int)ceil(ztr / dx) + 1;
+    for (int iz = z1; iz <= z2; iz++)
+        for (int iy = y1; iy <= y2; iy++)
+            for (int ix = x1; ix <= x2; ix++) {
+                if (ix < 0 || ix >= nx || iy < 0 || iy >= ny || iz < 0 || iz >= nz) continue;
+                long i = ix + (long)nx * iy + (long)nx * ny * iz;
+                double xx = fabs((double)ix * dx - xtr), yy = fabs((double)iy * dx - ytr), zz = fabs((double)iz * dx - ztr);
+                double dlt = (1.0 + cos(M_PI * xx / (2.0 * dx))) * (1.0 + cos(M_PI * yy / (2.0 * dx)))
+                           * (1.0 + cos(M_PI * zz / (2.0 * dx))) / 64.0;
+                u += dlt * s->um[i]; v += dlt * s->vm[i]; w += dlt * s->wm[i];
+            }
+    *ur = u; *vr = v; *wr = w;
+}
+
+/* ibm.cu:372-639 (ibm_st2a): RUNGE_KUTTA 4 (ibm.cu:430-517), 2 (518-574) or 1
+ * (575-617) stages over the averaged lattice velocity, then x += u M dt with the
+ * periodic wrap (ibm.cu:625-632) */
 void orc_ibm_st2(const orc_params *p, orc_state *s)
 {
-    int nx = p->nx, ny = p->ny, nz = p->nz;
     long nv = (long)p->ncell * p->vertex;
-    double dx = p->dx, dt = p->dt;
-    const double Md = 1.0; /* M = 1 */
+    double dt = p->dt;
+    const double Md = (double)orc_M(p);
+    const int rk = orc_rk(p);
 #pragma omp parallel for schedule(static)
     for (long jid = 0; jid < nv; jid++) {
         double xn = s->x[jid], yn = s->y[jid], zn = s->z[jid];
-        double xr = xn, yr = yn, zr = zn;
-        double uk[4][3];
-        for (int rk = 0; rk < 4; rk++) {
-            double ur = 0.0, vr = 0.0, wr = 0.0;
-            double xtr = xr + (double)(nx - 1) * dx / 2.0;
-            double ytr = yr + (double)(ny - 1) * dx / 2.0;
-            double ztr = zr + (double)(nz - 1) * dx / 2.0;
-            int x1 = (int)floor(xtr / dx) - 1, x2 = (int)ceil(xtr / dx) + 1;
-            int y1 = (int)floor(ytr / dx) - 1, y2 = (int)ceil(ytr / dx) + 1;
-            int z1 = (int)floor(ztr / dx) - 1, z2 = (int)ceil(ztr / dx) + 1;
-            for (int iz = z1; iz <= z2; iz++)
-                for (int iy = y1; iy <= y2; iy++)
-                    for (int ix = x1; ix <= x2; ix++) {
-                        if (ix < 0 || ix >= nx || iy < 0 || iy >= ny || iz < 0 || iz >= nz) continue;
-                        long i = ix + (long)nx * iy + (long)nx * ny * iz;
-                        double xx = fabs((double)ix * dx - xtr), yy = fabs((double)iy * dx - ytr), zz = fabs((double)iz * dx - ztr);
-                        double dlt = (1.0 + cos(M_PI * xx / (2.0 * dx))) * (1.0 + cos(M_PI * yy / (2.0 * dx)))
-                                   * (1.0 + cos(M_PI * zz / (2.0 * dx))) / 64.0;
-                        ur += dlt * s->um[i]; vr += dlt * s->vm[i]; wr += dlt * s->wm[i];
-                    }
-            uk[rk][0] = ur; uk[rk][1] = vr; uk[rk][2] = wr;
-            double h = (rk < 2) ? Md * dt / 2.0 : Md * dt;
-            xr = xn + ur * h; yr = yn + vr * h; zr = zn + wr * h;
+        double um, vm, wm;
+        if (rk == 4) {
+            double xr = xn, yr = yn, zr = zn, uk[4][3];
+            for (int k = 0; k < 4; k++) {
+                interp_velocity(p, s, 1, xr, yr, zr, &uk[k][0], &uk[k][1], &uk[k][2]);
+                double h = (k < 2) ? Md * dt / 2.0 : Md * dt;
+                xr = xn + uk[k][0] * h; yr = yn + uk[k][1] * h; zr = zn + uk[k][2] * h;
+            }
+            um = (uk[0][0] + 2.0 * uk[1][0] + 2.0 * uk[2][0] + uk[3][0]) / 6.0;
+            vm = (uk[0][1] + 2.0 * uk[1][1] + 2.0 * uk[2][1] + uk[3][1]) / 6.0;
+            wm = (uk[0][2] + 2.0 * uk[1][2] + 2.0 * uk[2][2] + uk[3][2]) / 6.0;
+        } else if (rk == 2) {
+            double u1, v1, w1, u2, v2, w2;
+            interp_velocity(p, s, 0, xn, yn, zn, &u1, &v1, &w1);
+            /* ibm.cu:560-562: the second stage at x + u1 M (no dt) */
+            interp_velocity(p, s, 0, xn + u1 * Md, yn + v1 * Md, zn + w1 * Md, &u2, &v2, &w2);
+            um = (u1 + u2) / 2.0; vm = (v1 + v2) / 2.0; wm = (w1 + w2) / 2.0;
+        } else {
+            interp_velocity(p, s, 0, xn, yn, zn, &um, &vm, &wm);
         }
-        double um = (uk[0][0] + 2.0 * uk[1][0] + 2.0 * uk[2][0] + uk[3][0]) / 6.0;
-        double vm = (uk[0][1] + 2.0 * uk[1][1] + 2.0 * uk[2][1] + uk[3][1]) / 6.0;
-        double wm = (uk[0][2] + 2.0 * uk[1][2] + 2.0 * uk[2][2] + uk[3][2]) / 6.0;
-        xr = xn + um * Md * dt; yr = yn + vm * Md * dt; zr = zn + wm * Md * dt;
+        double xr = xn + um * Md * dt, yr = yn + vm * Md * dt, zr = zn + wm * Md * dt;
         if (xr < p->xmin) xr += p->LX;
         if (xr > p->xmax) xr -= p->LX;
         if (zr < p->zmin) zr += p->LZ;
@@ -645,7 +673,7 @@ void orc_ibm_st2(const orc_params *p, orc_state *s)
 /* ------------------------------------------------------------------------ */
 
 /* lbm.cu:983-1313 (lbm_CapsuleCHANNELFLOW) + 1378-1432 (BUFF copy) +
- * 1435-1460 (average, M = 1) + pointer swap (1575).  omega = 1 / (3 (1 +
+ * 1435-1460 (the sums of the M sub-steps divided by M) + pointer swap (1575).  omega = 1 / (3 (1 +
  * (LAMBDA1 - 1) vf) Df + 1/2) with Df = (tau - 1/2) / 3 (lbm.cu:1131); with
  * LAMBDA1 = 1 that is 1 / tau, used as such. */
 void orc_lbm_d3q19(const orc_params *p, orc_state *s)
@@ -657,6 +685,7 @@ void orc_lbm_d3q19(const orc_params *p, orc_state *s)
     double wi = (iter > p->flowstart) ? 1.0 + 0.5 * sin(M_PI * t / p->freq) : 0.0;
     const double om0 = 1.0 / p->tau, Df = (p->tau - 0.5) / 3.0;
     const int visc = p->lambda1 != 1.0 && s->vf;
+    const int Ms = orc_M(p);
     const double *fn = s->fn; double *fm = s->fm;
     const int *bc = s->bc;
 #pragma omp parallel for schedule(static)
@@ -671,8 +700,9 @@ void orc_lbm_d3q19(const orc_params *p, orc_state *s)
         double tv = (jy + td * P * 0.0 + td * B * tfy) / (td * Cr);
         double tw = (jz + td * P * wi + td * B * tfz) / (td * Cr);
         s->dn[i] = td; s->un[i] = tu; s->vn[i] = tv; s->wn[i] = tw;
-        /* (iter-1)%M == 0 with M = 1: the averages restart every step */
-        s->dm[i] = td; s->um[i] = tu; s->vm[i] = tv; s->wm[i] = tw;
+        /* lbm.cu:1097-1102, 1122-1126: the sums restart at the first of every M steps */
+        if ((iter - 1) % Ms == 0) { s->dm[i] = 0.0; s->um[i] = 0.0; s->vm[i] = 0.0; s->wm[i] = 0.0; }
+        s->dm[i] += td; s->um[i] += tu; s->vm[i] += tv; s->wm[i] += tw;
         const double om = visc ? 1.0 / (3.0 * (1.0 + (p->lambda1 - 1.0) * s->vf[i]) * Df + 0.5) : om0;
         double om1 = 1.0 - om, om2 = (1.0 - om / 2.0) * 2.0 * td * P, om3 = (1.0 - om / 2.0) * 2.0 * td * B;
         double uvw = -1.5 * (tu*tu + tv*tv + tw*tw) * Cr2;
@@ -771,7 +801,13 @@ void orc_lbm_d3q19(const orc_params *p, orc_state *s)
         s->dn[i] = s->dn[i2]; s->un[i] = s->un[i2]; s->vn[i] = s->vn[i2]; s->wn[i] = s->wn[i2];
         s->dm[i] = s->dm[i2]; s->um[i] = s->um[i2]; s->vm[i] = s->vm[i2]; s->wm[i] = s->wm[i2];
     }
-    /* lbm.cu:1435-1460 divides by M = 1; lbm.cu:1575 swaps the buffers */
+    /* lbm.cu:1545-1548, 1435-1460: at the last of every M steps the velocity sums
+     * become averages (every node, as lbm_AVERAGE does) */
+    if (iter % Ms == 0) {
+#pragma omp parallel for schedule(static)
+        for (long i = 0; i < n; i++) { s->um[i] /= (double)Ms; s->vm[i] /= (double)Ms; s->wm[i] /= (double)Ms; }
+    }
+    /* lbm.cu:1575 swaps the buffers */
     double *tmp = s->fn; s->fn = s->fm; s->fm = tmp;
 }
 
@@ -816,6 +852,7 @@ void orc_thinc_wlic(const orc_params *p, orc_state *s)
     double *vf = s->vf;
     const int *bc = s->bc;
     const double *u[3] = {s->um, s->vm, s->wm};
+    const double Mt = (double)orc_M(p);   /* thincwlic.cu:179-207: the flux over M steps */
     for (int idr = 0; idr < 3; idr++) {
         vof_normals(p, vf, n1, n2);
         const long acs = idr == 0 ? 1 : idr == 1 ? nx : pl;
@@ -835,8 +872,8 @@ void orc_thinc_wlic(const orc_params *p, orc_state *s)
             if (uc <= 0.0) { isgn = 0; ii = i; } else { isgn = 1; ii = i - acs; }
             const double nn = fabs(n1[0][ii]) + fabs(n1[1][ii]) + fabs(n1[2][ii]);
             double f;
-            if (vf[ii] >= 1.0 - 1.0e-6 || vf[ii] <= 1.0e-6) f = vf[ii] * uc * 1.0 * dt;
-            else if (nn <= 1.0e-6) f = vf[ii] * uc * 1.0 * dt;
+            if (vf[ii] >= 1.0 - 1.0e-6 || vf[ii] <= 1.0e-6) f = vf[ii] * uc * Mt * dt;
+            else if (nn <= 1.0e-6) f = vf[ii] * uc * Mt * dt;
             else {
                 /* the reference's three assignments of ib leave ii - acs (ii's z index is >= 1) */
                 const long ib = ii - acs;
@@ -844,11 +881,11 @@ void orc_thinc_wlic(const orc_params *p, orc_state *s)
                 const double a1 = expf(beta * (2.0 * vf[ii] - 1.0) / alpha);
                 const double a3 = expf(beta);
                 const double xc = 0.5 / beta * log((a3 * a3 - a1 * a3) / (a1 * a3 - 1.0));
-                const double a4 = coshf(beta * ((double)isgn - uc * 1.0 * dt / dx - xc));
+                const double a4 = coshf(beta * ((double)isgn - uc * Mt * dt / dx - xc));
                 const double a5 = coshf(beta * ((double)isgn - xc));
-                f = 0.5 * (uc * 1.0 * dt - alpha * dx / beta * log(a4 / a5));
+                f = 0.5 * (uc * Mt * dt - alpha * dx / beta * log(a4 / a5));
                 const double weight = fabs(n1[idr][ii]) / nn;
-                f = f * weight + vf[ii] * uc * 1.0 * dt * (1.0 - weight);
+                f = f * weight + vf[ii] * uc * Mt * dt * (1.0 - weight);
             }
             if (bc[i] == ORC_WALL || bc[i - acs] == ORC_WALL) f = 0.0;
             flux[i] = f;
@@ -1147,24 +1184,28 @@ int orc_volume_correction(const orc_params *p, orc_state *s)
     return iter - 1;
 }
 
-/* main.cu:73-110 with M = 1 (no adhesion: CYTOADHESION = false); THINC/WLIC
- * and front tracking when vof_k > 0 */
+/* main.cu:73-110 (no adhesion: CYTOADHESION = false): the membrane and the
+ * spread at the first of every M steps ((iter - 1) % M == 0), the advection,
+ * THINC/WLIC and the volume correction at the last (iter % M == 0), front
+ * tracking every vof_k steps when vof_k > 0 */
 int orc_step(const orc_params *p, orc_state *s, int nsteps)
 {
+    const int Ms = orc_M(p);
     for (int k = 0; k < nsteps; k++) {
         s->iter++;
-        if (p->ncell > 0) {
+        const int first = (s->iter - 1) % Ms == 0, last = s->iter % Ms == 0;
+        if (p->ncell > 0 && first) {
             int flag = orc_stress(p, s);
             if (flag != 0) return 4;          /* error(4) in stress.cu:366 */
             orc_ibm_st1(p, s);
         }
         orc_lbm_d3q19(p, s);
-        if (p->ncell > 0) orc_ibm_st2(p, s);
+        if (p->ncell > 0 && last) orc_ibm_st2(p, s);
         if (p->vof_k > 0 && s->vf) {
-            orc_thinc_wlic(p, s);
+            if (last) orc_thinc_wlic(p, s);
             if (s->iter % p->vof_k == 0 && orc_front_tracking(p, s) < 0) return 6;   /* error(5) */
         }
-        if (p->ncell > 0 && orc_volume_correction(p, s) < 0) return 5;
+        if (p->ncell > 0 && last && orc_volume_correction(p, s) < 0) return 5;
     }
     return 0;
 }

@@ -67,6 +67,14 @@ typedef struct orc_params {
     int vof_k;           /* K: steps between front-tracking solves; 0 = no VOF (CN = 0) */
     double vof_residual; /* RESIDUAL of the front-tracking solve (matrix_solver.cu:112-216) */
     int vof_itrmax;      /* ITRMAX of that solve */
+    /* sub-cycling and the advection's order (main.cu:78-106, ibm.cu:430-627):
+     * the membrane and the spread run at the first of every M steps, the
+     * advection and the volume correction at the last, and the advection moves
+     * the vertices by the velocity averaged over the M steps (lbm.cu:1097-1126,
+     * 1435-1460) times M dt; rk_order = RUNGE_KUTTA (1, 2 or 4).  0 means the
+     * default (M = 1, RUNGE_KUTTA = 4). */
+    int M;
+    int rk_order;
 } orc_params;
 
 typedef struct orc_state {
@@ -134,7 +142,7 @@ void orc_thinc_wlic(const orc_params *p, orc_state *s);
  * attempt, or -1 when 10 attempts did not converge (the reference's error(5)). */
 int  orc_front_tracking(const orc_params *p, orc_state *s);
 
-/* main.cu:73-110 with M = 1: nsteps full steps.  Returns 0 or an error code. */
+/* main.cu:73-110: nsteps steps (sub-steps when M > 1).  Returns 0 or an error code. */
 int  orc_step(const orc_params *p, orc_state *s, int nsteps);
 
 /* Pieces used by the tests on their own. */

@@ -10,7 +10,8 @@
  *
  * Case-dependent values (lengths, forcing, moduli, solver tolerance) come
  * from -DREF_* flags (see oracle/Makefile and tests/golden/make_golden.py).
- * Lattice units: Cr = dx = dt = 1, M = 1, RK4, tau = 3 Df + 1/2, bending
+ * Lattice units: Cr = dx = dt = 1, tau = 3 Df + 1/2, sub-cycling M and
+ * RUNGE_KUTTA from -DREF_M / -DREF_RK (defaults 1 and 4), bending
  * modulus BR from -DREF_BR (default 0), viscosity ratio LAMBDA1 and
  * front-tracking interval K from -DREF_LAMBDA1 / -DREF_K (defaults 1 and
  * never), CN = 1, no adhesion, no white cells.
@@ -115,12 +116,18 @@
 #define REF_K 1000000000
 #endif
 
+#ifndef REF_M
+#define REF_M 1
+#endif
+#ifndef REF_RK
+#define REF_RK 4
+#endif
 #define Cr          1.0
-#define M           1
+#define M           (REF_M)
 #define K           (REF_K)
 #define LAMBDA1     (REF_LAMBDA1)
 #define LAMBDA2     1.0
-#define RUNGE_KUTTA 4
+#define RUNGE_KUTTA REF_RK
 #define N_R         1
 #ifndef REF_NW
 #define REF_NW 0

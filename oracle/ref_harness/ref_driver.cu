@@ -313,22 +313,36 @@ int ref_vof_init(void)
     return g_err;
 }
 
-// main.cu:73-110 with M = 1
+// main.cu:73-110 (no adhesion): the stages at the sub-steps main.cu gives them
 int ref_step(int nsteps)
 {
     for (int k = 0; k < nsteps && !g_err; k++) {
         g_prc.iter++;
-        stress(&g_prc, &g_cdo, &g_cel, &g_fem, &g_ltc);
-        ibm_st1(&g_cdo, &g_ltc, &g_cel);
+        if ((g_prc.iter - 1) % M == 0) stress(&g_prc, &g_cdo, &g_cel, &g_fem, &g_ltc);
+        if ((g_prc.iter - 1) % M == 0) ibm_st1(&g_cdo, &g_ltc, &g_cel);
         lbm_d3q19(&g_prc, &g_cdo, &g_ltc);
-        ibm_st2(&g_cdo, &g_ltc, &g_cel, &g_fem);
+        if (g_prc.iter % M == 0) ibm_st2(&g_cdo, &g_ltc, &g_cel, &g_fem);
         if (K < 1000000000) {   // THINC/WLIC and front tracking (main.cu:93-98)
-            thinc_wlic(&g_cdo, &g_ltc);
+            if (g_prc.iter % M == 0) thinc_wlic(&g_cdo, &g_ltc);
             if (g_prc.iter % K == 0) front_tracking(&g_cdo, &g_ltc, &g_cel);
         }
-        volume_correction(&g_cdo, &g_cel, &g_fem);
+        if (g_prc.iter % M == 0) volume_correction(&g_cdo, &g_cel, &g_fem);
     }
     cudaDeviceSynchronize();
+    return g_err;
+}
+
+// ltc->dmD, umD, vmD, wmD [n]: the sums over the sub-steps of the current
+// cycle (averaged velocity after its last sub-step, lbm.cu:1545-1548); any
+// pointer may be NULL
+int ref_get_lattice_m(double *dm, double *um, double *vm, double *wm)
+{
+    const int n = g_cdo.n;
+    cudaDeviceSynchronize();
+    if (dm) down(dm, g_ltc.dmD, n);
+    if (um) down(um, g_ltc.umD, n);
+    if (vm) down(vm, g_ltc.vmD, n);
+    if (wm) down(wm, g_ltc.wmD, n);
     return g_err;
 }
 

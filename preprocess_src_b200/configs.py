@@ -81,11 +81,13 @@ def duct_bc(nx: int, ny: int, nz: int) -> np.ndarray:
 
 def base_params(nx: int, ny: int, nz: int, *, tau=1.0, g=1e-6, Gs=5e-4, C=100.0, br=0.0, storage=0,
                 membrane_fp64=0, solver_iters=0, residual=1e-13, itrmax=2000, flow=0, sr=0.0, walls=0,
-                flowstart=0, bend_spont=0, lambda1=1.0, vof_k=0, vof_residual=1e-10, vof_itrmax=20000) -> dict:
+                flowstart=0, bend_spont=0, lambda1=1.0, vof_k=0, vof_residual=1e-10, vof_itrmax=20000, M=1,
+                rk_order=4) -> dict:
     LX, LZ = float(nx - 4), float(nz - 4)
     return dict(nx=nx, ny=ny, nz=nz, dx=1.0, dt=1.0, tau=float(tau), Cr=1.0, P=g / 2.0, B=Gs / 2.0,
                 flowstart=int(flowstart), freq=math.inf, LX=LX, LZ=LZ, xmin=-LX / 2, xmax=LX / 2, zmin=-LZ / 2,
-                zmax=LZ / 2, C=float(C), rgs=1.0, law=0, br=float(br), M=1, rk_order=4, storage=storage,
+                zmax=LZ / 2, C=float(C), rgs=1.0, law=0, br=float(br), M=int(M), rk_order=int(rk_order),
+                storage=storage,
                 membrane_fp64=membrane_fp64, solver_iters=solver_iters, residual=residual,
                 itrmax=itrmax, device=-1, flow=int(flow), sr=float(sr), walls=int(walls), tube_r=0.0,
                 bend_spont=int(bend_spont), lambda1=float(lambda1), vof_k=int(vof_k),

@@ -400,8 +400,9 @@ __device__ __forceinline__ bool box_plane(const float4 *box, int bxs, int bys, i
 // of the vertex's own (unwrapped) frame are dropped per vertex as
 // ibm.cu:453-455 does.  A box larger than ADVECT_SMEM, or a later-stage
 // stencil outside the box, gathers from global memory instead.
-// bid: the block's (cell, patch) index, blockIdx.x of a one-lattice launch
-template <bool XPER>
+// bid: the block's (cell, patch) index, blockIdx.x of a one-lattice launch.
+// RK: RUNGE_KUTTA, the stages of ibm.cu:430-517 (4), 518-574 (2) or 575-617 (1).
+template <bool XPER, int RK>
 __device__ __forceinline__ void
 advect_body(const Geom &g, double *__restrict__ X, double *__restrict__ Xd, float *__restrict__ U,
             const float4 *__restrict__ uvr, long long nv, int V, const int *__restrict__ patch_off,
@@ -495,12 +496,14 @@ advect_body(const Geom &g, double *__restrict__ X, double *__restrict__ Xd, floa
                 gather_plane(g, uvr, cx, cy, izr, xm, P);
         };
         fetch(bx, by, bz);
-        float us[4], vs[4], ws[4];
+        float us[RK], vs[RK], ws[RK];
 #pragma unroll
-        for (int k = 0; k < 4; k++) {
+        for (int k = 0; k < RK; k++) {
             double px = xn, py = yn, pz = zn;
             if (k > 0) {
-                const double h = (k < 3 ? 0.5 : 1.0) * dtM;   // ibm.cu:474-498
+                // RK4: x + u1 M dt / 2, x + u2 M dt / 2, x + u3 M dt (ibm.cu:487-505);
+                // RK2: x + u1 M (ibm.cu:560-562; dt = 1 there)
+                const double h = (RK == 4 && k < 3 ? 0.5 : 1.0) * dtM;
                 px += us[k - 1] * h; py += vs[k - 1] * h; pz += ws[k - 1] * h;
                 int cx, cy, cz;
                 lattice_cell(g, px, py, pz, cx, cy, cz, fx, fy, fz);
@@ -514,9 +517,18 @@ advect_body(const Geom &g, double *__restrict__ X, double *__restrict__ Xd, floa
             contract(P, wx, wy, wzc, us[k], vs[k], ws[k]);
         }
         if (!live || c != 0) continue;
-        const double um = ((double)us[0] + 2.0 * us[1] + 2.0 * us[2] + us[3]) / 6.0;
-        const double vm = ((double)vs[0] + 2.0 * vs[1] + 2.0 * vs[2] + vs[3]) / 6.0;
-        const double wm = ((double)ws[0] + 2.0 * ws[1] + 2.0 * ws[2] + ws[3]) / 6.0;
+        double um, vm, wm;
+        if constexpr (RK == 4) {
+            um = ((double)us[0] + 2.0 * us[1] + 2.0 * us[2] + us[3]) / 6.0;
+            vm = ((double)vs[0] + 2.0 * vs[1] + 2.0 * vs[2] + vs[3]) / 6.0;
+            wm = ((double)ws[0] + 2.0 * ws[1] + 2.0 * ws[2] + ws[3]) / 6.0;
+        } else if constexpr (RK == 2) {   // ibm.cu:570-572
+            um = ((double)us[0] + (double)us[1]) / 2.0;
+            vm = ((double)vs[0] + (double)vs[1]) / 2.0;
+            wm = ((double)ws[0] + (double)ws[1]) / 2.0;
+        } else {                          // ibm.cu:614-616
+            um = us[0]; vm = vs[0]; wm = ws[0];
+        }
         double xr = xn + um * dtM, yr = yn + vm * dtM, zr = zn + wm * dtM;
         if (xr < g.xmin) xr += g.LX;   // ibm.cu:629-632
         if (xr > g.xmax) xr -= g.LX;
@@ -529,26 +541,33 @@ advect_body(const Geom &g, double *__restrict__ X, double *__restrict__ Xd, floa
     }
 }
 
-template <bool XPER>
+template <bool XPER, int RK>
 __global__ void __launch_bounds__(ADVECT_THREADS)
 advect_kernel(const Geom g, double *__restrict__ X, double *__restrict__ Xd, float *__restrict__ U,
               const float4 *__restrict__ uvr, long long nv, int V, const int *__restrict__ patch_off,
               const int *__restrict__ patch_vtx, int npatch, double dtM, int *__restrict__ flags)
 {
-    advect_body<XPER>(g, X, Xd, U, uvr, nv, V, patch_off, patch_vtx, npatch, dtM, flags, blockIdx.x);
+    advect_body<XPER, RK>(g, X, Xd, U, uvr, nv, V, patch_off, patch_vtx, npatch, dtM, flags, blockIdx.x);
 }
 
 cudaError_t advect_setup()
 {
-    cudaError_t e = cudaFuncSetAttribute(advect_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, ADVECT_SMEM);
-    if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(advect_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, ADVECT_SMEM);
+    const void *ks[] = {(const void *)advect_kernel<false, 4>, (const void *)advect_kernel<true, 4>,
+                        (const void *)advect_kernel<false, 2>, (const void *)advect_kernel<true, 2>,
+                        (const void *)advect_kernel<false, 1>, (const void *)advect_kernel<true, 1>};
+    for (const void *k : ks) {
+        const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, ADVECT_SMEM);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 void launch_advect(const Geom &g, const AdvectArgs &a, cudaStream_t s)
 {
     if (a.ncell <= 0) return;
-    auto k = g.xper ? advect_kernel<true> : advect_kernel<false>;
+    auto k = a.rk == 1 ? (g.xper ? advect_kernel<true, 1> : advect_kernel<false, 1>)
+           : a.rk == 2 ? (g.xper ? advect_kernel<true, 2> : advect_kernel<false, 2>)
+                       : (g.xper ? advect_kernel<true, 4> : advect_kernel<false, 4>);
     k<<<a.ncell * a.npatch, ADVECT_THREADS, ADVECT_SMEM, s>>>(
         g, a.X, a.Xd, a.U, a.uvr, a.nv, a.V, a.patch_off, a.patch_vtx, a.npatch, a.dtM, a.flags);
 }
@@ -573,7 +592,7 @@ advect_fused_kernel(const DomainArgs *__restrict__ dom, const int *__restrict__ 
     const int d = fused_domain(boff, ndom, blockIdx.x);
     const DomainArgs &D = dom[d];
     const AdvectArgs &a = D.adv;
-    advect_body<XPER>(D.g, a.X, a.Xd, a.U, a.uvr, a.nv, a.V, a.patch_off, a.patch_vtx, a.npatch, a.dtM, a.flags,
+    advect_body<XPER, 4>(D.g, a.X, a.Xd, a.U, a.uvr, a.nv, a.V, a.patch_off, a.patch_vtx, a.npatch, a.dtM, a.flags,
                       blockIdx.x - boff[d]);
 }
 

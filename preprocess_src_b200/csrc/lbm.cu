@@ -57,6 +57,10 @@ struct Collision {
     float A, B, C, D, E;
 };
 
+// Every product-sum below is an explicit __fmaf_rn / __fmul_rn / __fadd_rn, so
+// no step is left to the compiler's contraction: the kernels that inline this
+// code (one simulation, the fused batch, each with the om = 1 and general
+// forms) round every node the same way, bit for bit.
 template <int SCALE>
 __device__ __forceinline__ Collision collision_terms(const float (&g)[Q], float fx, float fy, float fz, float pd,
                                                      float omega, float Cr, float Bc)
@@ -66,26 +70,39 @@ __device__ __forceinline__ Collision collision_terms(const float (&g)[Q], float 
 #pragma unroll
     for (int q = 0; q < Q; q++) {
         drho += g[q];
-        if (ex(q)) jx += ex(q) * g[q];
-        if (ey(q)) jy += ey(q) * g[q];
-        if (ez(q)) jz += ez(q) * g[q];
+        if (ex(q) == 1) jx += g[q]; else if (ex(q) == -1) jx -= g[q];
+        if (ey(q) == 1) jy += g[q]; else if (ey(q) == -1) jy -= g[q];
+        if (ez(q) == 1) jz += g[q]; else if (ez(q) == -1) jz -= g[q];
     }
     if (SCALE != 1) { drho *= inv_scale; jx *= inv_scale; jy *= inv_scale; jz *= inv_scale; }
     Collision c;
     c.r = 1.0f + drho;
-    c.Gx = c.r * Bc * fx; c.Gy = c.r * Bc * fy; c.Gz = c.r * (pd + Bc * fz);
-    const float inv = 1.0f / (c.r * Cr);
-    c.u = (jx + c.Gx) * inv; c.v = (jy + c.Gy) * inv; c.w = (jz + c.Gz) * inv;
-    const float fo = (1.0f - 0.5f * omega) * 2.0f;
-    const float usq = -1.5f * Cr * Cr * (c.u * c.u + c.v * c.v + c.w * c.w);
-    const float uG = 3.0f * Cr * (c.u * c.Gx + c.v * c.Gy + c.w * c.Gz);
-    c.A = omega * (drho + c.r * usq) - fo * uG;
-    c.B = 3.0f * Cr * omega * c.r;
-    c.C = 4.5f * Cr * Cr * omega * c.r;
-    c.D = 3.0f * fo;
-    c.E = 9.0f * Cr * fo;
+    const float rB = __fmul_rn(c.r, Bc);
+    c.Gx = __fmul_rn(rB, fx); c.Gy = __fmul_rn(rB, fy); c.Gz = __fmul_rn(c.r, __fmaf_rn(Bc, fz, pd));
+    const float inv = 1.0f / __fmul_rn(c.r, Cr);
+    c.u = __fmul_rn(__fadd_rn(jx, c.Gx), inv); c.v = __fmul_rn(__fadd_rn(jy, c.Gy), inv);
+    c.w = __fmul_rn(__fadd_rn(jz, c.Gz), inv);
+    const float fo = __fmul_rn(__fmaf_rn(-0.5f, omega, 1.0f), 2.0f);
+    const float uu = __fmaf_rn(c.w, c.w, __fmaf_rn(c.v, c.v, __fmul_rn(c.u, c.u)));
+    const float usq = __fmul_rn(-1.5f * Cr * Cr, uu);
+    const float uG = __fmul_rn(3.0f * Cr, __fmaf_rn(c.w, c.Gz, __fmaf_rn(c.v, c.Gy, __fmul_rn(c.u, c.Gx))));
+    c.A = __fmaf_rn(-fo, uG, __fmul_rn(omega, __fmaf_rn(c.r, usq, drho)));
+    c.B = __fmul_rn(3.0f * Cr * omega, c.r);
+    c.C = __fmul_rn(4.5f * Cr * Cr * omega, c.r);
+    c.D = __fmul_rn(3.0f, fo);
+    c.E = __fmul_rn(9.0f * Cr, fo);
     if (SCALE != 1) { c.A *= scale; c.B *= scale; c.C *= scale; c.D *= scale; c.E *= scale; }
     return c;
+}
+
+// e_q . (x, y, z) for the lattice directions (components 0 or +-1): additions only
+__device__ __forceinline__ float edot(int q, float x, float y, float z)
+{
+    float d = 0.f;
+    if (ex(q) == 1) d = x; else if (ex(q) == -1) d = -x;
+    if (ey(q) == 1) d = __fadd_rn(d, y); else if (ey(q) == -1) d = __fsub_rn(d, y);
+    if (ez(q) == 1) d = __fadd_rn(d, z); else if (ez(q) == -1) d = __fsub_rn(d, z);
+    return d;
 }
 
 // The post-collision values of an opposite pair (q, q + 1 = opp(q)): with
@@ -99,19 +116,21 @@ template <bool TAU1>
 __device__ __forceinline__ void post_pair(const Collision &c, int q, float gq, float gp, float om1, float &oq,
                                           float &op)
 {
-    const float eu = ex(q) * c.u + ey(q) * c.v + ez(q) * c.w;
-    const float eG = ex(q) * c.Gx + ey(q) * c.Gy + ez(q) * c.Gz;
+    const float eu = edot(q, c.u, c.v, c.w);
+    const float eG = edot(q, c.Gx, c.Gy, c.Gz);
     const float w = wq(q);
-    const float S = w * (c.A + eu * (c.C * eu + c.E * eG));
-    const float T = w * (c.B * eu + c.D * eG);
-    oq = TAU1 ? S + T : om1 * gq + (S + T);
-    op = TAU1 ? S - T : om1 * gp + (S - T);
+    const float S = __fmul_rn(w, __fmaf_rn(eu, __fmaf_rn(c.C, eu, __fmul_rn(c.E, eG)), c.A));
+    const float T = __fmul_rn(w, __fmaf_rn(c.B, eu, __fmul_rn(c.D, eG)));
+    const float sp = __fadd_rn(S, T), sm = __fsub_rn(S, T);
+    oq = TAU1 ? sp : __fmaf_rn(om1, gq, sp);
+    op = TAU1 ? sm : __fmaf_rn(om1, gp, sm);
 }
 
 template <bool TAU1>
 __device__ __forceinline__ float post_rest(const Collision &c, float g0, float om1)
 {
-    return TAU1 ? wq(0) * c.A : om1 * g0 + wq(0) * c.A;
+    const float a = __fmul_rn(wq(0), c.A);
+    return TAU1 ? a : __fmaf_rn(om1, g0, a);
 }
 
 // FP16 storage rounds stochastically (cvt.rs.f16x2.f32, sm_100a): each stored
@@ -152,11 +171,13 @@ __device__ __forceinline__ void st_u16(__half *p, uint32_t v) {
 // stores of the post-collision values (0 for wall lanes) at element offset idx of every
 // population array; I is the offset type (int when Q * nint < 2^31).  has_force:
 // the node's occupancy bit (F holds its IB force; read only here).
-template <int STORE, bool ALL_FLUID, bool TAU1, typename I>
+// SUB: the rho / u store follows acc (LBM_ACC_*, sub-cycling) instead of
+// overwriting.
+template <int STORE, bool ALL_FLUID, bool TAU1, bool SUB, typename I>
 __device__ __forceinline__ void collide_store(float (&g)[Q], bool fluid, bool has_force, I idx, I nint,
                                               typename Store<STORE>::T *__restrict__ gout, float4 *__restrict__ uvr,
                                               const long long *__restrict__ F, uint32_t step,
-                                              float pd, float omega, float om1, float Cr, float Bc)
+                                              float pd, float omega, float om1, float Cr, float Bc, int acc, float Mf)
 {
     using S = Store<STORE>;
     const bool live = ALL_FLUID || fluid;
@@ -167,7 +188,15 @@ __device__ __forceinline__ void collide_store(float (&g)[Q], bool fluid, bool ha
         fz = (float)__ldg(&F[2 * nint + idx]) * inv;
     }
     const Collision c = collision_terms<(int)S::scale>(g, fx, fy, fz, pd, omega, Cr, Bc);
-    uvr[idx] = live ? make_float4(c.u, c.v, c.w, c.r) : make_float4(0.f, 0.f, 0.f, 1.f);
+    float4 m = live ? make_float4(c.u, c.v, c.w, c.r) : make_float4(0.f, 0.f, 0.f, 1.f);
+    if (SUB && live && acc != LBM_ACC_WRITE) {
+        // um += tu (lbm.cu:1122-1126), then um /= M at the last step (lbm.cu:1455-1457);
+        // the density sum dm is not averaged
+        const float4 o = uvr[idx];
+        m.x += o.x; m.y += o.y; m.z += o.z; m.w += o.w;
+        if (acc == LBM_ACC_AVERAGE) { m.x = __fdiv_rn(m.x, Mf); m.y = __fdiv_rn(m.y, Mf); m.z = __fdiv_rn(m.z, Mf); }
+    }
+    uvr[idx] = m;
     typename S::T *ob = gout + idx;
     if constexpr (STORE == RBC_STORE_F16) {
         const uint32_t h = node_hash((uint32_t)idx, step);
@@ -218,7 +247,7 @@ __device__ __forceinline__ void collide_store(float (&g)[Q], bool fluid, bool ha
 // (lbm.cu:1131 with LAMBDA1 != 1); the omega argument otherwise.
 // (bx, by, gy): the block's column tile, its first plane and the plane stride
 // (blockIdx.x, blockIdx.y, gridDim.y of a one-lattice launch).
-template <int STORE, typename I, bool VISC, bool TAU1>
+template <int STORE, typename I, bool VISC, bool TAU1, bool SUB = false>
 __device__ __forceinline__ void
 lbm_collide_stream_body(const typename Store<STORE>::T *__restrict__ gin, typename Store<STORE>::T *__restrict__ gout,
                         float4 *__restrict__ uvr,
@@ -227,7 +256,7 @@ lbm_collide_stream_body(const typename Store<STORE>::T *__restrict__ gin, typena
                         const int *__restrict__ iter,
                         const float *__restrict__ wall, const double *__restrict__ vf, float lm1, float df3,
                         int nx, int ny, int nzc, I nint,
-                        float omega, float Cr, float Bc, int bx, int by, int gy)
+                        float omega, float Cr, float Bc, int bx, int by, int gy, int acc = 0, float Mf = 1.f)
 {
     using S = Store<STORE>;
     const int plane = nx * ny;
@@ -255,7 +284,7 @@ lbm_collide_stream_body(const typename Store<STORE>::T *__restrict__ gin, typena
         const I dzp = (z == nzc - 1) ? -(I)(nzc - 1) * plane : (I)plane;
         const I idx = (I)z * plane + xy;
         if (VISC) {
-            omega = 1.0f / (df3 * (1.0f + lm1 * (float)__ldg(&vf[idx])) + 0.5f);
+            omega = 1.0f / __fmaf_rn(df3, __fmaf_rn(lm1, (float)__ldg(&vf[idx]), 1.0f), 0.5f);
             om1 = 1.0f - omega;
         }
         const typename S::T *gb = gin + idx;
@@ -264,7 +293,8 @@ lbm_collide_stream_body(const typename Store<STORE>::T *__restrict__ gin, typena
 #pragma unroll
             for (int q = 0; q < Q; q++)
                 g[q] = S::ld_raw(gb + ((I)q * nint + ((ez(q) == 1) ? dzm : (ez(q) == -1) ? dzp : (I)0) - ex(q) - nx * ey(q)));
-            collide_store<STORE, true, TAU1, I>(g, true, has_force, idx, nint, gout, uvr, F, step, pd, omega, om1, Cr, Bc);
+            collide_store<STORE, true, TAU1, SUB, I>(g, true, has_force, idx, nint, gout, uvr, F, step, pd, omega, om1,
+                                                     Cr, Bc, acc, Mf);
         } else {
 #pragma unroll
             for (int q = 0; q < Q; q++) {
@@ -285,14 +315,19 @@ lbm_collide_stream_body(const typename Store<STORE>::T *__restrict__ gin, typena
                 const float uw = __ldg(&wall[(m & MASK_TOPW) ? 0 : 1]);
 #pragma unroll
                 for (int q = 0; q < Q; q++)
-                    if (ez(q) != 0 && ((m >> q) & 1u)) g[q] += 6.0f * wq(q) * rho * Cr * (float)ez(q) * uw * S::scale;
+                    if (ez(q) != 0 && ((m >> q) & 1u)) {
+                        const float t = __fmul_rn(__fmul_rn(__fmul_rn(__fmul_rn(6.0f * wq(q), rho), Cr) * (float)ez(q), uw),
+                                                  S::scale);
+                        g[q] = __fadd_rn(g[q], t);
+                    }
             }
-            collide_store<STORE, false, TAU1, I>(g, fluid, has_force, idx, nint, gout, uvr, F, step, pd, omega, om1, Cr, Bc);
+            collide_store<STORE, false, TAU1, SUB, I>(g, fluid, has_force, idx, nint, gout, uvr, F, step, pd, omega,
+                                                      om1, Cr, Bc, acc, Mf);
         }
     }
 }
 
-template <int STORE, typename I, bool VISC, bool TAU1>
+template <int STORE, typename I, bool VISC, bool TAU1, bool SUB>
 __global__ void __launch_bounds__(LBM_THREADS, LBM_MIN_BLOCKS)
 lbm_collide_stream(const typename Store<STORE>::T *__restrict__ gin, typename Store<STORE>::T *__restrict__ gout,
                    float4 *__restrict__ uvr,
@@ -300,11 +335,11 @@ lbm_collide_stream(const typename Store<STORE>::T *__restrict__ gin, typename St
                    const uint32_t *__restrict__ mask2d, const float *__restrict__ drive, const int *__restrict__ iter,
                    const float *__restrict__ wall, const double *__restrict__ vf, float lm1, float df3,
                    int nx, int ny, int nzc, I nint,
-                   float omega, float Cr, float Bc)
+                   float omega, float Cr, float Bc, int acc, float Mf)
 {
-    lbm_collide_stream_body<STORE, I, VISC, TAU1>(gin, gout, uvr, F, Fbits, wpp, mask2d, drive, iter, wall, vf, lm1,
-                                                  df3, nx, ny, nzc, nint, omega, Cr, Bc, blockIdx.x, blockIdx.y,
-                                                  gridDim.y);
+    lbm_collide_stream_body<STORE, I, VISC, TAU1, SUB>(gin, gout, uvr, F, Fbits, wpp, mask2d, drive, iter, wall, vf,
+                                                       lm1, df3, nx, ny, nzc, nint, omega, Cr, Bc, blockIdx.x,
+                                                       blockIdx.y, gridDim.y, acc, Mf);
 }
 
 // z planes per thread: the per-thread setup (mask, warp votes, drive) is paid
@@ -325,18 +360,21 @@ void launch_lbm(const Geom &g, int storage, const LbmArgs &a, cudaStream_t s)
     const int gz = (g.nzc + zpt - 1) / zpt;
     const dim3 blocks((unsigned)((g.plane + LBM_THREADS - 1) / LBM_THREADS), (unsigned)(gz < 65535 ? gz : 65535));
     const bool off32 = (long long)Q * g.nint < (1LL << 31);   // every element offset fits in an int
-#define LBM_LAUNCH(ST, I, V, T1)                                                                              \
-    lbm_collide_stream<ST, I, V, T1><<<blocks, LBM_THREADS, 0, s>>>(                                          \
+#define LBM_LAUNCH(ST, I, V, T1, SB)                                                                          \
+    lbm_collide_stream<ST, I, V, T1, SB><<<blocks, LBM_THREADS, 0, s>>>(                                      \
         (const Store<ST>::T *)a.gin, (Store<ST>::T *)a.gout, a.uvr, a.F.F, a.F.bits, a.F.wpp, a.mask2d, a.drive, a.iter, \
         a.wall, a.vf, \
-        a.lm1, a.df3, g.nx, g.ny, g.nzc, (I)g.nint, a.omega, a.Cr, a.Bc)
-    // tau = 1 without a viscosity ratio: the om = 1 form of the collision
+        a.lm1, a.df3, g.nx, g.ny, g.nzc, (I)g.nint, a.omega, a.Cr, a.Bc, a.acc, a.Mf)
+    // tau = 1 without a viscosity ratio: the om = 1 form of the collision.  The
+    // sums of a sub-cycled step take the general form (with om = 1 it gives the
+    // same values: (1 - om) g = 0 exactly); the volume fraction runs with M = 1.
     const bool tau1 = !a.vf && a.omega == 1.0f;
 #define LBM_LAUNCH_V(ST, I)                                                                                   \
     do {                                                                                                      \
-        if (a.vf) LBM_LAUNCH(ST, I, true, false);                                                             \
-        else if (tau1) LBM_LAUNCH(ST, I, false, true);                                                        \
-        else LBM_LAUNCH(ST, I, false, false);                                                                 \
+        if (a.vf) LBM_LAUNCH(ST, I, true, false, false);                                                      \
+        else if (a.acc != LBM_ACC_WRITE) LBM_LAUNCH(ST, I, false, false, true);                               \
+        else if (tau1) LBM_LAUNCH(ST, I, false, true, false);                                                 \
+        else LBM_LAUNCH(ST, I, false, false, false);                                                          \
     } while (0)
     if (storage == RBC_STORE_F16) {
         if (off32) LBM_LAUNCH_V(RBC_STORE_F16, int); else LBM_LAUNCH_V(RBC_STORE_F16, long long);

@@ -98,12 +98,17 @@ struct rbc_handle {
     void *staging = nullptr;
     size_t staging_bytes = 0;
     int iter = 0;
+    // the IB force field may hold nonzero values: a spread not yet cleared (a
+    // stage call, or a sub-cycled step ended before the last step of its M)
     bool force_pending = false;
     // CUDA graphs of one step starting from population buffer 0 / 1, in three
     // forms (StepForm): the whole step; the step without its volume
     // correction; the step without its correction but with the previous
     // step's correction beside its membrane pass
-    cudaGraphExec_t graph[3][2] = {{nullptr, nullptr}, {nullptr, nullptr}, {nullptr, nullptr}};
+    // (and three more, StepForm STEP_SUB_*, for the first, middle and last of
+    // M sub-cycled steps), with the kernels each launches
+    cudaGraphExec_t graph[6][2] = {};
+    int graph_kernels[6] = {};
     cudaStream_t side = nullptr;                      // second branch of the pipelined graphs (capture only)
     cudaEvent_t fork = nullptr, join = nullptr;
     // split membrane pass: the first full wave's spread beside the last wave's membrane (capture only)
@@ -463,8 +468,14 @@ int check_params(const rbc_params *p)
     if (!(p->dx > 0) || !(p->dt > 0) || !(p->tau > 0.5) || !(p->Cr > 0))
         return fail(nullptr, RBC_ERR_ARG, "dx, dt, Cr must be > 0 and tau > 1/2");
     if (!(p->LX > 0) || !(p->LZ > 0)) return fail(nullptr, RBC_ERR_ARG, "LX and LZ must be > 0");
-    if (p->M != 1) return fail(nullptr, RBC_ERR_UNSUPPORTED, "only M = 1 (no sub-cycling) is implemented");
-    if (p->rk_order != 4) return fail(nullptr, RBC_ERR_UNSUPPORTED, "only RUNGE_KUTTA = 4 is implemented");
+    if (p->M < 1) return fail(nullptr, RBC_ERR_ARG, "M must be >= 1");
+    if (p->rk_order != 1 && p->rk_order != 2 && p->rk_order != 4)
+        return fail(nullptr, RBC_ERR_ARG, "rk_order must be 1, 2 or 4 (RUNGE_KUTTA)");
+    // the reference's RUNGE_KUTTA 2 and 1 branches interpolate in lattice units
+    // without dx and take the midpoint at x + u M without dt (ibm.cu:522-562),
+    // the RUNGE_KUTTA 4 form only for dx = dt = 1
+    if (p->rk_order != 4 && (p->dx != 1.0 || p->dt != 1.0))
+        return fail(nullptr, RBC_ERR_UNSUPPORTED, "RUNGE_KUTTA 1 and 2 need dx = dt = 1");
     if (!std::isfinite(p->br)) return fail(nullptr, RBC_ERR_ARG, "BR must be finite");
     if (p->bend_spont != 0 && p->bend_spont != 1) return fail(nullptr, RBC_ERR_ARG, "bend_spont must be 0 or 1");
     if (p->vof_k < 0) return fail(nullptr, RBC_ERR_ARG, "vof_k must be >= 0");
@@ -764,9 +775,10 @@ int launch_bend_stage(rbc_handle *h)
 }
 
 // the collide-stream kernel's arguments from population buffer cur
-LbmArgs lbm_args(rbc_handle *h, int cur)
+LbmArgs lbm_args(rbc_handle *h, int cur, int acc = LBM_ACC_WRITE)
 {
     LbmArgs a{};
+    a.acc = acc; a.Mf = (float)h->p.M;
     a.gin = h->g[cur]; a.gout = h->g[1 - cur];
     a.uvr = h->uvr;
     a.F = h->force(); a.mask2d = h->mask2d; a.drive = h->d_drive; a.iter = h->d_iter();
@@ -782,10 +794,10 @@ LbmArgs lbm_args(rbc_handle *h, int cur)
 }
 
 // the collide-stream launch (+ the tube's bounce-back) and, with reset, the
-// force reset after it
-int launch_lbm_stage(rbc_handle *h, bool reset = true)
+// force reset after it; acc: the velocity sums of a sub-cycled step (LBM_ACC_*)
+int launch_lbm_stage(rbc_handle *h, bool reset = true, int acc = LBM_ACC_WRITE)
 {
-    LbmArgs a = lbm_args(h, h->cur);
+    LbmArgs a = lbm_args(h, h->cur, acc);
     launch_lbm(h->geo, h->p.storage, a, h->stream);
     h->launches++;
     CK_LAUNCH();
@@ -805,7 +817,7 @@ AdvectArgs advect_args(rbc_handle *h, CellGroup &g)
     AdvectArgs a{};
     a.X = g.X; a.Xd = g.Xd; a.U = g.U; a.uvr = h->uvr; a.nv = g.nv;
     a.V = g.V; a.ncell = g.ncell; a.patch_off = g.patch_off; a.patch_vtx = g.patch_vtx; a.npatch = g.npatch;
-    a.dtM = h->p.dt * h->p.M; a.flags = h->d_flags();
+    a.dtM = h->p.dt * h->p.M; a.rk = h->p.rk_order; a.flags = h->d_flags();
     return a;
 }
 
@@ -910,7 +922,23 @@ int launch_volume_stage(rbc_handle *h, cudaStream_t st)
     return RBC_OK;
 }
 
-enum StepForm { STEP_WHOLE = 0, STEP_BODY = 1, STEP_PIPELINED = 2 };
+enum StepForm { STEP_WHOLE = 0, STEP_BODY = 1, STEP_PIPELINED = 2, STEP_SUB_FIRST = 3, STEP_SUB_MID = 4,
+                STEP_SUB_LAST = 5 };
+
+// Sub-cycling (M > 1, main.cu:78-106): step iter runs the membrane pass and
+// the spread when (iter - 1) % M == 0 and the advection, THINC/WLIC and the
+// volume correction when iter % M == 0; the force field persists over the M
+// collide-streams between them, and the velocity they store is summed, then
+// averaged at the last (lbm.cu:1097-1126, 1435-1460).
+StepForm sub_form(const rbc_handle *h, int iter)
+{
+    const int M = h->p.M, ph = (iter - 1) % M;
+    return ph == 0 ? STEP_SUB_FIRST : ph == M - 1 ? STEP_SUB_LAST : STEP_SUB_MID;
+}
+int lbm_acc(StepForm f)
+{
+    return f == STEP_SUB_MID ? LBM_ACC_ADD : f == STEP_SUB_LAST ? LBM_ACC_AVERAGE : LBM_ACC_WRITE;
+}
 
 // one step (main.cu:73-110 with M = 1); the device increments iter.
 // STEP_BODY leaves out the step's volume correction; STEP_PIPELINED also runs
@@ -930,6 +958,8 @@ int enqueue_step(rbc_handle *h, StepForm form = STEP_WHOLE)
 {
     int rc;
     const bool pipelined = form == STEP_PIPELINED;
+    const bool sub = form >= STEP_SUB_FIRST;
+    const bool first = !sub || form == STEP_SUB_FIRST, last = !sub || form == STEP_SUB_LAST;
     if (pipelined) {
         CK(cudaEventRecord(h->fork, h->stream));
         CK(cudaStreamWaitEvent(h->side, h->fork, 0));
@@ -939,8 +969,10 @@ int enqueue_step(rbc_handle *h, StepForm form = STEP_WHOLE)
     launch_step_begin(step_begin_args(h), h->stream);
     h->launches++;
     CK_LAUNCH();
-    const int split = membrane_wave_split(h);
-    if (split > 0) {
+    const int split = first ? membrane_wave_split(h) : 0;
+    if (!first) {
+        // a middle or last sub-cycled step: the cycle's force is in the field
+    } else if (split > 0) {
         CellGroup &g = h->cg[0];
         if ((rc = launch_membrane_range(h, g, 0, split, h->stream))) return rc;
         CK(cudaEventRecord(h->wave_done, h->stream));
@@ -960,14 +992,15 @@ int enqueue_step(rbc_handle *h, StepForm form = STEP_WHOLE)
     }
     // the force reset runs beside the advection (which reads neither the
     // field nor its bits) and joins before the step ends
-    if ((rc = launch_lbm_stage(h, false))) return rc;
+    if ((rc = launch_lbm_stage(h, false, lbm_acc(form)))) return rc;
+    if (!last) return RBC_OK;
     CK(cudaEventRecord(h->lbm_done, h->stream));
     CK(cudaStreamWaitEvent(h->side2, h->lbm_done, 0));
     if ((rc = launch_force_reset_stage(h, h->side2))) return rc;
     CK(cudaEventRecord(h->reset_done, h->side2));
     if ((rc = launch_advect_stage(h))) return rc;
     if ((rc = launch_thinc_stage(h))) return rc;   // main.cu:94-95
-    if (form == STEP_WHOLE && (rc = launch_volume_stage(h, h->stream))) return rc;
+    if ((form == STEP_WHOLE || form == STEP_SUB_LAST) && (rc = launch_volume_stage(h, h->stream))) return rc;
     CK(cudaStreamWaitEvent(h->stream, h->reset_done, 0));
     return RBC_OK;
 }
@@ -985,6 +1018,7 @@ int capture_step(rbc_handle *h, int c, StepForm form, cudaGraph_t *out)
     CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
     int rc = enqueue_step(h, form);
     cudaError_t e = cudaStreamEndCapture(h->stream, out);
+    h->graph_kernels[form] = (int)(h->launches - launches0);
     h->launches = launches0;
     h->cur = cur0;
     if (rc != RBC_OK) { if (*out) cudaGraphDestroy(*out); *out = nullptr; return rc; }
@@ -1007,7 +1041,10 @@ int build_graph(rbc_handle *h, int c, StepForm form)
 
 int prepare_steps(rbc_handle *h)
 {
-    if (h->force_pending) {
+    // a step that spreads starts from a zero field; a middle or last sub-cycled
+    // step uses the field its cycle's first step spread
+    const bool spreads = h->p.M == 1 || (h->iter % h->p.M) == 0;
+    if (h->force_pending && spreads) {
         CK(cudaMemsetAsync(h->Fint, 0, 24 * h->geo.nint, h->stream));
         CK(cudaMemsetAsync(h->Fbits, 0, h->force_bit_bytes(), h->stream));
         h->force_pending = false;
@@ -1082,6 +1119,7 @@ std::string fused_obstacle(const rbc_batch *b)
         if (h->fileoutput > 0) return who + "output-interval averages";
         if (h->vof()) return who + "volume fraction";
         if (h->ntube > 0) return who + "circular tube";
+        if (h->p.rk_order != 4) return who + "RUNGE_KUTTA != 4";
         if (h->cg[0].ncell > 0) {
             if (V && h->cg[0].V != V) return who + "another number of vertices per cell";
             V = h->cg[0].V;
@@ -1710,9 +1748,13 @@ int rbc_lbm_d3q19(rbc_handle *h)
 {
     if (!h) return RBC_ERR_ARG;
     RBC_DEVICE_GUARD(h);
-    int rc = launch_lbm_stage(h);
+    // sub-cycled: the step h->iter's place among the M (as set by rbc_set_iter);
+    // the force is cleared after the last
+    const StepForm f = h->p.M == 1 ? STEP_WHOLE : sub_form(h, h->iter);
+    const bool last = f == STEP_WHOLE || f == STEP_SUB_LAST;
+    int rc = launch_lbm_stage(h, last, lbm_acc(f));
     if (rc) return rc;
-    h->force_pending = false;   // the LBM kernel consumed and cleared the force
+    if (last) h->force_pending = false;   // the reset cleared the force
     return RBC_OK;
 }
 
@@ -1826,6 +1868,21 @@ int rbc_step(rbc_handle *h, int nsteps)
     if (nsteps == 0) return RBC_OK;
     int rc;
     if ((rc = prepare_steps(h))) return rc;
+    if (h->p.M > 1) {   // sub-cycled: each step's graph by its place among the M
+        bool ended = false;
+        for (int k = 0; k < nsteps; k++) {
+            const StepForm f = sub_form(h, h->iter + k + 1);
+            if (!h->graph[f][h->cur] && (rc = build_graph(h, h->cur, f))) return rc;
+            CK(cudaGraphLaunch(h->graph[f][h->cur], h->stream));
+            h->cur ^= 1;
+            h->launches += h->graph_kernels[f];
+            ended = f == STEP_SUB_LAST;
+        }
+        h->iter += nsteps;
+        h->force_pending = h->iter % h->p.M != 0;   // the cycle's force stays for its remaining steps
+        if (ended) h->metrics_valid = h->has_cells();
+        return RBC_OK;
+    }
     // one step, or no cells: whole steps.  Otherwise step 1 without its
     // correction, steps 2..n pipelined with the correction of the step before,
     // then the correction of step n: the same kernels in the same data order.
@@ -1864,26 +1921,31 @@ int rbc_profile_steps(rbc_handle *h, int nsteps, double *kernel_ms)
     if ((rc = prepare_steps(h))) return rc;
     cudaEvent_t ev[RBC_NUM_KERNELS + 1];
     for (auto &e : ev) CK(cudaEventCreate(&e));
+    bool ended = false;
     for (int s = 0; s < nsteps && rc == RBC_OK; s++) {
+        // the stages of this step's place among M sub-cycled steps (all of them for M = 1)
+        const StepForm f = h->p.M == 1 ? STEP_WHOLE : sub_form(h, h->iter + s + 1);
+        const bool first = f == STEP_WHOLE || f == STEP_SUB_FIRST, last = f == STEP_WHOLE || f == STEP_SUB_LAST;
+        ended = last;
         cudaEventRecord(ev[0], h->stream);
         launch_step_begin(step_begin_args(h), h->stream);
         h->launches++;
         cudaEventRecord(ev[1], h->stream);
-        if (!rc) rc = launch_stress(h);
-        if (!rc) rc = launch_bend_stage(h);   // timed with the membrane pass
+        if (!rc && first) rc = launch_stress(h);
+        if (!rc && first) rc = launch_bend_stage(h);   // timed with the membrane pass
         cudaEventRecord(ev[2], h->stream);
-        if (!rc) rc = launch_spread_stage(h);
+        if (!rc && first) rc = launch_spread_stage(h);
         cudaEventRecord(ev[3], h->stream);
-        if (!rc) rc = launch_lbm_stage(h, false);
+        if (!rc) rc = launch_lbm_stage(h, false, lbm_acc(f));
         cudaEventRecord(ev[4], h->stream);
-        if (!rc) rc = launch_force_reset_stage(h, h->stream);
+        if (!rc && last) rc = launch_force_reset_stage(h, h->stream);
         cudaEventRecord(ev[5], h->stream);
-        if (!rc) rc = launch_advect_stage(h);
+        if (!rc && last) rc = launch_advect_stage(h);
         cudaEventRecord(ev[6], h->stream);
-        if (!rc) rc = launch_thinc_stage(h);
+        if (!rc && last) rc = launch_thinc_stage(h);
         if (!rc && h->vof() && (h->iter + s + 1) % h->p.vof_k == 0) rc = launch_front_tracking_stage(h);
         cudaEventRecord(ev[7], h->stream);
-        if (!rc) rc = launch_volume_stage(h, h->stream);
+        if (!rc && last) rc = launch_volume_stage(h, h->stream);
         cudaEventRecord(ev[8], h->stream);
         if (cudaEventSynchronize(ev[8]) != cudaSuccess) { rc = RBC_ERR_CUDA; h->err = "profiled step failed"; break; }
         for (int k = 0; k < RBC_NUM_KERNELS; k++) {
@@ -1893,8 +1955,11 @@ int rbc_profile_steps(rbc_handle *h, int nsteps, double *kernel_ms)
         }
     }
     for (auto &e : ev) cudaEventDestroy(e);
-    if (rc == RBC_OK) h->iter += nsteps;
-    h->metrics_valid = rc == RBC_OK && nsteps > 0 && h->has_cells();
+    if (rc == RBC_OK) {
+        h->iter += nsteps;
+        h->force_pending = h->p.M > 1 && h->iter % h->p.M != 0;
+    }
+    if (ended || rc != RBC_OK) h->metrics_valid = rc == RBC_OK && nsteps > 0 && h->has_cells();
     return rc;
 }
 
@@ -1989,6 +2054,8 @@ int rbc_batch_create(rbc_handle *const *handles, int n, rbc_batch **out)
             if (handles[j] == handles[i]) return fail(nullptr, RBC_ERR_ARG, "a simulation appears twice in the batch");
         if (handles[i]->vof())
             return fail(nullptr, RBC_ERR_UNSUPPORTED, "batched simulations do not track the volume fraction (needs vof_k = 0)");
+        if (handles[i]->p.M != 1)
+            return fail(nullptr, RBC_ERR_UNSUPPORTED, "batched simulations step with M = 1 (no sub-cycling)");
     }
     rbc_batch *b = new (std::nothrow) rbc_batch();
     if (!b) return fail(nullptr, RBC_ERR_ARG, "out of host memory");
@@ -2576,6 +2643,8 @@ int adjoint_supported(rbc_handle *h)
     if (h->p.flow != RBC_FLOW_CHANNEL) return fail(h, RBC_ERR_UNSUPPORTED, "the adjoint covers the channel mode only");
     if (h->ntube > 0) return fail(h, RBC_ERR_UNSUPPORTED, "the adjoint covers half-way bounce-back walls only (tube_r = 0)");
     if (h->vof()) return fail(h, RBC_ERR_UNSUPPORTED, "the adjoint does not cover the volume fraction (needs vof_k = 0)");
+    if (h->p.M != 1 || h->p.rk_order != 4)
+        return fail(h, RBC_ERR_UNSUPPORTED, "the adjoint covers M = 1 and RUNGE_KUTTA = 4 only");
     return RBC_OK;
 }
 
@@ -2922,6 +2991,40 @@ int reference_bc(rbc_handle *h, int *bc)
                 const bool buff = z < 2 || z >= nz - 2 || xr < g.xb || xr >= nxr - g.xb;
                 bc[z * pr + (long long)y * nxr + xr] = (mask[(size_t)y * g.nx + x] & MASK_FLUID) ? (buff ? RBC_BUFF : RBC_COMP) : RBC_WALL;
             }
+    return RBC_OK;
+}
+
+// ltc->dmD, umD, vmD, wmD [nx*ny*nz] (reference layout, COMP nodes read) into
+// the rho / u field the collide-stream stores (the cycle's sums with M > 1);
+// other fluid nodes of the field are unused, wall columns hold rho 1, u 0 as
+// the kernel leaves them
+int import_macro(rbc_handle *h, const double *dm, const double *um, const double *vm, const double *wm)
+{
+    RBC_DEVICE_GUARD(h);
+    const Geom &g = h->geo;
+    std::vector<uint32_t> mask((size_t)g.plane);
+    CK(cudaStreamSynchronize(h->stream));
+    CK(cudaMemcpy(mask.data(), h->mask2d, 4 * mask.size(), cudaMemcpyDeviceToHost));
+    std::vector<float4> f((size_t)g.nint);
+    for (int zc = 0; zc < g.nzc; zc++)
+        for (int iy = 0; iy < g.ny; iy++)
+            for (int xi = 0; xi < g.nx; xi++) {
+                const size_t i = (size_t)zc * g.plane + (size_t)iy * g.nx + xi;
+                if (!(mask[(size_t)iy * g.nx + xi] & MASK_FLUID)) { f[i] = make_float4(0.f, 0.f, 0.f, 1.f); continue; }
+                const long long r = ((long long)(zc + 2) * g.ny + iy) * g.nxr + xi + g.xb;
+                f[i] = make_float4((float)um[r], (float)vm[r], (float)wm[r], (float)dm[r]);
+            }
+    CK(cudaMemcpy(h->uvr, f.data(), sizeof(float4) * f.size(), cudaMemcpyHostToDevice));
+    return RBC_OK;
+}
+
+// a zero IB force field, as a freshly set-up reference lattice holds it
+int clear_force(rbc_handle *h)
+{
+    RBC_DEVICE_GUARD(h);
+    CK(cudaMemsetAsync(h->Fint, 0, 24 * h->geo.nint, h->stream));
+    CK(cudaMemsetAsync(h->Fbits, 0, h->force_bit_bytes(), h->stream));
+    h->force_pending = false;
     return RBC_OK;
 }
 

@@ -128,7 +128,14 @@ struct LbmArgs {
     float omega, Cr, Bc;
     float scale, inv_scale;    // FP16 storage scale
     int planes;                // z planes per thread; 0 = chosen from the lattice size
+    // sub-cycling (M > 1, lbm.cu:1097-1126, 1435-1460): LBM_ACC_WRITE stores the
+    // node's u and rho (every step of M = 1, the first of M), LBM_ACC_ADD adds
+    // them to the stored sums, LBM_ACC_AVERAGE adds and divides the velocity sum
+    // by Mf (the last of M)
+    int acc;
+    float Mf;
 };
+enum { LBM_ACC_WRITE = 0, LBM_ACC_ADD = 1, LBM_ACC_AVERAGE = 2 };
 void launch_lbm(const Geom &g, int storage, const LbmArgs &a, cudaStream_t s);
 // z velocities of the top and bottom walls in the next step (shear mode; 0 otherwise)
 struct WallVel { double top, bot, Cr; };
@@ -217,6 +224,7 @@ struct AdvectArgs {
     const int *patch_off, *patch_vtx;   // surface patches of the shared mesh
     int npatch;
     double dtM;                // dt * M
+    int rk;                    // RUNGE_KUTTA: 1, 2 or 4 stages
     int *flags;
 };
 void launch_advect(const Geom &g, const AdvectArgs &a, cudaStream_t s);
@@ -241,6 +249,8 @@ int  membrane_smem_bytes(int V);
 int reference_mn(int V);
 int output_averages(rbc_handle *h, int group, double *qi, double *tp, bool set);   // group 0 red, 1 white cells
 int reference_bc(rbc_handle *h, int *bc);
+int import_macro(rbc_handle *h, const double *dm, const double *um, const double *vm, const double *wm);
+int clear_force(rbc_handle *h);
 int reference_ele(rbc_handle *h, int group, int *ele);   // cel->eleH(_w): [ncell * E * 3] global vertex ids
 int group_sizes(const rbc_handle *h, int group, int *ncell, int *vertex, int *element);
 void set_handle_error(rbc_handle *h, const std::string &msg);

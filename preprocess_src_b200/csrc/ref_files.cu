@@ -182,7 +182,7 @@ int rbc_read_restart(rbc_handle *h, const char *path, int *fnum)
     int iter = 0, fn_ = 0;
     std::vector<double> fn((size_t)d.n * Q), skip((size_t)d.n * 6);
     bool ok = get(f.f, &iter, 1) && get(f.f, &fn_, 1) && get(f.f, fn.data(), fn.size())
-           && get(f.f, skip.data(), skip.size());     // dm, um, vm, wm (recomputed by the step), vf, vf2
+           && get(f.f, skip.data(), skip.size());     // dm, um, vm, wm, vf, vf2
     PopState st[2];
     for (int k = 0; k < 2 && ok; k++) {
         const Pop &p = d.pop[k];
@@ -199,6 +199,13 @@ int rbc_read_restart(rbc_handle *h, const char *path, int *fnum)
     if (std::fgetc(f.f) != EOF) return io_error(h, "restart file longer than this lattice and these cells", path);
     if (fn_ > 100) { iter = 0; fn_ = 0; }   // etc.cu:205
     if ((rc = rbc_import_ref_lattice(h, fn.data()))) return rc;
+    // the density and velocity sums (etc.cu:277-280): what the advection reads
+    // when the file ends inside a sub-cycle, and what the next write repeats
+    if ((rc = import_macro(h, skip.data(), skip.data() + d.n, skip.data() + 2 * d.n, skip.data() + 3 * d.n))) return rc;
+    // the file holds no IB force: the reference resumes with the ltc->fx of its
+    // set-up, 0 (init1.cu:394-409, 923), which matters only for a file written
+    // inside a sub-cycle
+    if ((rc = clear_force(h))) return rc;
     // the volume fractions when tracked (etc.cu:213-214, 281-282); else unused
     if (rbc_import_ref_vof(h, skip.data() + 4 * d.n, skip.data() + 5 * d.n) != RBC_OK) set_handle_error(h, "");
     for (int k = 0; k < 2; k++) {

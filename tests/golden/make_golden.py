@@ -91,6 +91,14 @@ def golden_cases():
                                                             centers_duct=[(8.2, 9.6, 9.4), (23.9, 9.3, 9.7)],
                                                             subdiv=3, radius=5.0, seed=27, g=4e-5, Gs=2e-3,
                                                             residual=1e-12), nred=1, rgs=2.5, br=0.02),
+        # sub-cycling: the membrane and the spread every M steps, the advection
+        # with the velocity averaged over them, RUNGE_KUTTA 2 and 1
+        "g9_duct24x20x20_1c_m2rk2": configs.duct_case("g9_duct24x20x20_1c_m2rk2", 24, 20, 20,
+                                                      centers_duct=[(12.3, 9.6, 9.4)], subdiv=3, radius=5.5,
+                                                      seed=29, g=4e-5, Gs=2e-3, residual=1e-12, M=2, rk_order=2),
+        "g10_duct24x20x20_1c_m3rk1": configs.duct_case("g10_duct24x20x20_1c_m3rk1", 24, 20, 20,
+                                                       centers_duct=[(12.3, 9.6, 9.4)], subdiv=3, radius=5.5,
+                                                       seed=30, g=4e-5, Gs=2e-3, residual=1e-12, M=3, rk_order=1),
     }
 
 
@@ -119,8 +127,13 @@ def cell_coefficients(case):
 
 def snapshots(case):
     """Steps after which a fixture holds the state: with VOF (front tracking
-    every K = 10 steps) also one five steps after a solve."""
-    return (1, 25, 30) if case.params["vof_k"] > 0 else SNAPSHOTS
+    every K = 10 steps) also one five steps after a solve; with M > 1 every
+    place in the first cycle."""
+    if case.params["vof_k"] > 0:
+        return (1, 25, 30)
+    if case.params["M"] > 1:
+        return tuple(range(1, case.params["M"] + 1)) + (30,)
+    return SNAPSHOTS
 
 
 def dense_case():
@@ -152,6 +165,8 @@ def ref_defs(case) -> str:
     if "wbc" in case.meta:
         nred, rgs, br = case.meta["wbc"]
         d += f" -DREF_NW={case.ncell - nred} -DREF_GSW={rgs!r} -DREF_BRW={br!r}"
+    if p["M"] != 1 or p["rk_order"] != 4:
+        d += f" -DREF_M={p['M']} -DREF_RK={p['rk_order']}"
     return d
 
 
@@ -230,10 +245,15 @@ class Ref:
             raise RuntimeError(f"reference step failed with error({rc})")
 
     def lattice(self):
+        """dn/un/vn/wn, and with M > 1 also dm/um/vm/wm: the sums of the cycle
+        (velocity averaged after its last step)."""
         n = self.case.n
         out = {k: np.empty(n) for k in ("dn", "un", "vn", "wn")}
         p = lambda a: a.ctypes.data_as(C.c_void_p)  # noqa: E731
         self.L.ref_get_lattice(None, p(out["dn"]), p(out["un"]), p(out["vn"]), p(out["wn"]), None, None, None)
+        if self.case.params["M"] > 1:
+            out.update({k: np.empty(n) for k in ("dm", "um", "vm", "wm")})
+            self.L.ref_get_lattice_m(p(out["dm"]), p(out["um"]), p(out["vm"]), p(out["wm"]))
         return out
 
     def _population(self, pop, getter):
@@ -275,8 +295,9 @@ def run(outdir, names=()):
             lat, cel = ref.lattice(), ref.cells()
             if vof:
                 data[f"s{s}_vf"] = ref.vf()[m]
-            for k in ("dn", "un", "vn", "wn"):
-                data[f"s{s}_{k}"] = lat[k][m]
+            for k in ("dn", "un", "vn", "wn", "dm", "um", "vm", "wm"):
+                if k in lat:
+                    data[f"s{s}_{k}"] = lat[k][m]
             for k in ("x", "y", "z", "u", "v", "w", "fx", "fy", "fz", "gx"):
                 data[f"s{s}_{k}"] = cel[k]
         np.savez_compressed(outdir / f"{name}.npz", **data)

@@ -53,8 +53,12 @@ def _cuda_present():
 
 def test_rejects_unsupported_options(native_lib):
     case = configs.small_duct()
-    assert _create(case, M=2)[0] == N.RBC_ERR_UNSUPPORTED
-    assert _create(case, rk_order=2)[0] == N.RBC_ERR_UNSUPPORTED
+    assert _create(case, M=0)[0] == N.RBC_ERR_ARG
+    assert _create(case, rk_order=3)[0] == N.RBC_ERR_ARG
+    # the reference's RUNGE_KUTTA 1 / 2 branches drop dx and dt (ibm.cu:522-562)
+    rc, msg = _create(case, rk_order=2, dx=0.5)
+    assert rc == N.RBC_ERR_UNSUPPORTED and "dx = dt = 1" in msg
+    assert _create(case, M=2, vof_k=10)[0] == N.RBC_ERR_UNSUPPORTED
     assert _create(case, br=float("inf"))[0] == N.RBC_ERR_ARG
     assert _create(case, tau=0.5)[0] == N.RBC_ERR_ARG
     assert _create(case, storage=7)[0] == N.RBC_ERR_ARG

@@ -57,6 +57,11 @@ def test_oracle_matches_reference_kernels(name, case, oracle_mod):
             assert np.abs(o["vf"][m] - g[f"s{s}_vf"]).max() <= 1e-6
         assert rel(u, uref) <= utol, (s, rel(u, uref))
         assert np.abs(o["dn"][m] - g[f"s{s}_dn"]).max() <= 1e-12 * loose
+        if f"s{s}_um" in g:   # sub-cycled: the sums of the cycle (averaged velocity at its end)
+            um = np.concatenate([o["um"][m], o["vm"][m], o["wm"][m]])
+            umref = np.concatenate([g[f"s{s}_um"], g[f"s{s}_vm"], g[f"s{s}_wm"]])
+            assert rel(um, umref) <= utol, (s, rel(um, umref))
+            assert np.abs(o["dm"][m] - g[f"s{s}_dm"]).max() <= 1e-12 * case.params["M"]
         x = np.concatenate([o[k] for k in ("x", "y", "z")])
         xref = np.concatenate([g[f"s{s}_{k}"] for k in ("x", "y", "z")])
         assert np.abs(x - xref).max() <= 1e-12 * loose * np.abs(xref).max(), (s, np.abs(x - xref).max())
