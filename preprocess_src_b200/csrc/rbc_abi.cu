@@ -50,6 +50,8 @@ struct CellGroup {
     float *U = nullptr, *Fv = nullptr;
     int *tri = nullptr, *v2e_off = nullptr, *v2e = nullptr;
     int16_t *nbr = nullptr;
+    int16_t *nbrp = nullptr;  // neighbours by solve position ([6][V]) and the vertex at each position ([V])
+    int *vord = nullptr;
     int4 *visit = nullptr;   // bending visits [E][3], allocated when BR != 0
     double2 *cs0 = nullptr;  // spontaneous angle (cos, sin) per visit [ncell][E][3] (bend_spont), else none
     double *bend_rec = nullptr;   // bending visit records [ncell][E][3][9], allocated when BR != 0
@@ -246,11 +248,12 @@ WallVel wall_velocities(const rbc_handle *h, int step)
 }
 
 // Link tables of the shared local connectivity (init2.cu:258-400): neighbour
-// lists in the order add_nlink builds them, vertex -> element lists in element
-// order (add_elink), the reference's link-count check, and the packed
-// incidence entries used by the membrane and volume kernels.
+// lists (the vertices add_nlink collects, kept in the membrane solve's order
+// below), vertex -> element lists in element order (add_elink), the
+// reference's link-count check, and the packed incidence entries used by the
+// membrane and volume kernels.
 int build_topology(rbc_handle *h, const CellGroup &c, const int *tri, std::vector<int> &off, std::vector<int> &packed,
-                   std::vector<int16_t> &nbr6)
+                   std::vector<int16_t> &nbr6, std::vector<int16_t> &nbrp6, std::vector<int> &vord)
 {
     const int V = c.V, E = c.E;
     std::vector<std::vector<int>> nl(V), el(V);
@@ -275,6 +278,35 @@ int build_topology(rbc_handle *h, const CellGroup &c, const int *tri, std::vecto
     }
     if (links != 2LL * (V + E - 2))   // init2.cu:369-370
         return fail(h, RBC_ERR_TOPOLOGY, "link count check failed (closed genus-0 mesh expected)");
+    // Solve order of the membrane kernel: breadth first from a vertex of least
+    // valence, each vertex's unvisited neighbours in the order of their
+    // valence, so the positions run ring by ring around the surface; each
+    // neighbour list is then sorted by position.  Consecutive positions (the
+    // lanes of a warp) then gather neighbours at nearby positions in every slot,
+    // which spreads their shared-memory loads over the banks.
+    vord.clear();
+    {
+        std::vector<int> pos(V, -1);
+        for (int root = 0; root < V; root++) {
+            if (pos[root] >= 0) continue;
+            int best = root;
+            for (int i = root; i < V; i++) if (pos[i] < 0 && nl[i].size() < nl[best].size()) best = i;
+            size_t head = vord.size();
+            pos[best] = (int)vord.size(); vord.push_back(best);
+            while (head < vord.size()) {
+                const int u = vord[head++];
+                std::vector<int> nx;
+                for (int x : nl[u]) if (pos[x] < 0) nx.push_back(x);
+                std::stable_sort(nx.begin(), nx.end(), [&](int a, int b) { return nl[a].size() < nl[b].size(); });
+                for (int x : nx) { pos[x] = (int)vord.size(); vord.push_back(x); }
+            }
+        }
+        for (int i = 0; i < V; i++)
+            std::sort(nl[i].begin(), nl[i].end(), [&](int a, int b) { return pos[a] < pos[b]; });
+        nbrp6.assign((size_t)6 * V, (int16_t)-1);
+        for (int p = 0; p < V; p++)
+            for (size_t s = 0; s < nl[vord[p]].size(); s++) nbrp6[s * V + p] = (int16_t)pos[nl[vord[p]][s]];
+    }
     off.assign(V + 1, 0);
     packed.clear();
     nbr6.assign((size_t)6 * V, (int16_t)-1);
@@ -601,7 +633,7 @@ int build_mask(const rbc_params *p, const int *bc, std::vector<uint32_t> &mask)
 
 void free_group(CellGroup &c)
 {
-    void *cp[] = {c.X, c.Xd, c.gref, c.erec, c.U, c.Fv, c.tri, c.v2e_off, c.v2e, c.nbr, c.visit, c.cs0, c.patch_off,
+    void *cp[] = {c.X, c.Xd, c.gref, c.erec, c.U, c.Fv, c.tri, c.v2e_off, c.v2e, c.nbr, c.nbrp, c.vord, c.visit, c.cs0, c.patch_off,
                   c.patch_vtx, c.patch_stride, c.vol0, c.gx, c.vol_out, c.area_out, c.cen_out, c.qi_acc, c.tp_acc,
                   c.vf, c.bend_rec};
     for (void *q : cp) if (q) cudaFree(q);
@@ -642,7 +674,7 @@ int launch_membrane_range(rbc_handle *h, CellGroup &g, int c0, int c1, cudaStrea
     MembraneArgs a{};
     a.Xd = g.Xd + (size_t)c0 * g.V; a.nv = g.nv; a.ne = g.ne; a.gref = g.gref + (size_t)c0 * g.E;
     a.erec = (char *)g.erec + (size_t)c0 * g.E * rec_bytes;
-    a.tri = g.tri; a.v2e_off = g.v2e_off; a.v2e = g.v2e; a.nbr = g.nbr; a.Fv = g.Fv + (size_t)c0 * g.V;
+    a.tri = g.tri; a.v2e_off = g.v2e_off; a.v2e = g.v2e; a.nbr = g.nbr; a.nbrp = g.nbrp; a.vord = g.vord; a.Fv = g.Fv + (size_t)c0 * g.V;
     a.V = g.V; a.E = g.E; a.ncell = c1 - c0;
     a.C = h->p.C; a.rgs = g.rgs; a.law = h->p.law; a.LX = h->p.LX; a.LZ = h->p.LZ;
     a.niter = h->p.solver_iters > 0 ? h->p.solver_iters : DEFAULT_SOLVER_ITERS;
@@ -685,7 +717,7 @@ MembraneArgs membrane_args(rbc_handle *h, CellGroup &g)
 {
     MembraneArgs a{};
     a.Xd = g.Xd; a.nv = g.nv; a.ne = g.ne; a.gref = g.gref; a.erec = g.erec;
-    a.tri = g.tri; a.v2e_off = g.v2e_off; a.v2e = g.v2e; a.nbr = g.nbr; a.Fv = g.Fv;
+    a.tri = g.tri; a.v2e_off = g.v2e_off; a.v2e = g.v2e; a.nbr = g.nbr; a.nbrp = g.nbrp; a.vord = g.vord; a.Fv = g.Fv;
     a.V = g.V; a.E = g.E; a.ncell = g.ncell;
     a.C = h->p.C; a.rgs = g.rgs; a.law = h->p.law; a.LX = h->p.LX; a.LZ = h->p.LZ;
     a.niter = h->p.solver_iters > 0 ? h->p.solver_iters : DEFAULT_SOLVER_ITERS;
@@ -1268,7 +1300,8 @@ int batch_build(rbc_batch *b)
 // centroids, surface patches, bending visits.
 struct GroupPrep {
     std::vector<int> off, packed, poff, pvtx, pstride;
-    std::vector<int16_t> nbr6;
+    std::vector<int16_t> nbr6, nbrp6;
+    std::vector<int> vord;
     std::vector<double> vol0, gx, xs;
     std::vector<double4> gref;
     std::vector<int4> visit;
@@ -1279,7 +1312,7 @@ int prepare_group(rbc_handle *h, CellGroup &c, const rbc_mesh *mesh, GroupPrep &
 {
     c.ncell = mesh->ncell; c.V = mesh->vertex; c.E = mesh->element;
     c.nv = (long long)c.ncell * c.V; c.ne = (long long)c.ncell * c.E;
-    int rc = build_topology(h, c, mesh->tri, pp.off, pp.packed, pp.nbr6);
+    int rc = build_topology(h, c, mesh->tri, pp.off, pp.packed, pp.nbr6, pp.nbrp6, pp.vord);
     if (rc) return rc;
     surface_patches(c.V, mesh->xr, pp.poff, pp.pvtx, pp.pstride);
     c.npatch = (int)pp.poff.size() - 1;
@@ -1302,7 +1335,7 @@ int upload_group(rbc_handle *h, CellGroup &c, const rbc_mesh *mesh, const GroupP
     CK(cudaMalloc(&c.erec, (size_t)c.ne * 12 * (h->p.membrane_fp64 ? sizeof(double) : sizeof(float))));
     TRYG(dalloc(h, &c.U, 3 * c.nv)); TRYG(dalloc(h, &c.Fv, 3 * c.nv));
     TRYG(dalloc(h, &c.tri, 3 * c.E)); TRYG(dalloc(h, &c.v2e_off, c.V + 1)); TRYG(dalloc(h, &c.v2e, pp.packed.size()));
-    TRYG(dalloc(h, &c.nbr, 6 * c.V));
+    TRYG(dalloc(h, &c.nbr, 6 * c.V)); TRYG(dalloc(h, &c.nbrp, 6 * c.V)); TRYG(dalloc(h, &c.vord, c.V));
     if (!pp.visit.empty()) {
         TRYG(dalloc(h, &c.visit, pp.visit.size()));
         CK(cudaMemcpy(c.visit, pp.visit.data(), sizeof(int4) * pp.visit.size(), cudaMemcpyHostToDevice));
@@ -1326,6 +1359,8 @@ int upload_group(rbc_handle *h, CellGroup &c, const rbc_mesh *mesh, const GroupP
     CK(cudaMemcpy(c.v2e_off, pp.off.data(), 4 * (c.V + 1), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(c.v2e, pp.packed.data(), 4 * pp.packed.size(), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(c.nbr, pp.nbr6.data(), 2 * 6 * c.V, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c.nbrp, pp.nbrp6.data(), 2 * 6 * c.V, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c.vord, pp.vord.data(), 4 * c.V, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(c.patch_off, pp.poff.data(), 4 * pp.poff.size(), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(c.patch_vtx, pp.pvtx.data(), 4 * pp.pvtx.size(), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(c.patch_stride, pp.pstride.data(), 4 * pp.pstride.size(), cudaMemcpyHostToDevice));
@@ -3015,6 +3050,23 @@ int import_macro(rbc_handle *h, const double *dm, const double *um, const double
                 f[i] = make_float4((float)um[r], (float)vm[r], (float)wm[r], (float)dm[r]);
             }
     CK(cudaMemcpy(h->uvr, f.data(), sizeof(float4) * f.size(), cudaMemcpyHostToDevice));
+    return RBC_OK;
+}
+
+// cel->u, v, w [ncell * vertex] of population `group` (the last advection's
+// vertex velocities; FP32 in the handle)
+int import_vertex_velocity(rbc_handle *h, int group, const double *u, const double *v, const double *w)
+{
+    RBC_DEVICE_GUARD(h);
+    if (group >= h->ngroups) return RBC_OK;
+    CellGroup &g = h->cg[group];
+    if (g.nv == 0) return RBC_OK;
+    std::vector<float> f(3 * (size_t)g.nv);
+    for (long long j = 0; j < g.nv; j++) {
+        f[j] = (float)u[j]; f[g.nv + j] = (float)v[j]; f[2 * g.nv + j] = (float)w[j];
+    }
+    CK(cudaStreamSynchronize(h->stream));
+    CK(cudaMemcpy(g.U, f.data(), 4 * f.size(), cudaMemcpyHostToDevice));
     return RBC_OK;
 }
 

@@ -235,6 +235,8 @@ struct MembraneArgs {
     void *erec;               // [ne][3] element records (Real 4-vectors): scratch written and read by each CTA
     const int *tri, *v2e_off, *v2e;
     const int16_t *nbr;       // [6][V] local neighbour ids, -1 = none
+    const int16_t *nbrp;      // [6][V] the same neighbours as positions in the solve order, by position
+    const int *vord;          // [V] solve order: the vertex at each position
     float *Fv;
     int V, E, ncell;
     double C, rgs; int law;
@@ -251,6 +253,7 @@ int output_averages(rbc_handle *h, int group, double *qi, double *tp, bool set);
 int reference_bc(rbc_handle *h, int *bc);
 int import_macro(rbc_handle *h, const double *dm, const double *um, const double *vm, const double *wm);
 int clear_force(rbc_handle *h);
+int import_vertex_velocity(rbc_handle *h, int group, const double *u, const double *v, const double *w);
 int reference_ele(rbc_handle *h, int group, int *ele);   // cel->eleH(_w): [ncell * E * 3] global vertex ids
 int group_sizes(const rbc_handle *h, int group, int *ncell, int *vertex, int *element);
 void set_handle_error(rbc_handle *h, const std::string &msg);

@@ -211,12 +211,13 @@ int rbc_read_restart(rbc_handle *h, const char *path, int *fnum)
     for (int k = 0; k < 2; k++) {
         const Pop &p = d.pop[k];
         if (p.N == 0) continue;
-        // fem->x (hence fem->xd) is set from cel->x (etc.cu:256-274); the vertex velocities are the
-        // next advection's output and are not needed to step
+        // fem->x (hence fem->xd) is set from cel->x (etc.cu:256-274); the vertex velocities (the
+        // last advection's, which the next one overwrites) are kept for the next file write
         const double *x = st[k].cx.data(), *y = x + p.nv, *z = y + p.nv;
         std::vector<double> xd((size_t)p.nv * 3);
         for (long long j = 0; j < p.nv; j++) { xd[3 * j] = x[j]; xd[3 * j + 1] = y[j]; xd[3 * j + 2] = z[j]; }
         if ((rc = import_pop(h, k, x, y, z, xd.data(), nullptr))) return rc;
+        if ((rc = import_vertex_velocity(h, k, x + 3 * p.nv, x + 4 * p.nv, x + 5 * p.nv))) return rc;
         if ((rc = output_averages(h, k, st[k].qi.data(), st[k].tp.data(), true))) return rc;
     }
     if ((rc = rbc_set_iter(h, iter))) return rc;
