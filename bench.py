@@ -185,8 +185,9 @@ def barrier(world):
         dist.barrier()
 
 
-def cpu_sample(case, budget_s, warm=1):
-    """FP64 CPU oracle on the same workload: whole steps until the budget."""
+def cpu_sample(case, budget_s, warm=1, keep=None):
+    """FP64 CPU oracle on the same workload: whole steps until the budget.
+    keep: a list that receives the oracle (for the FP64 error of the step)."""
     from oracle.oracle import Oracle, num_threads
     o = Oracle(case)
     o.step(warm)
@@ -198,9 +199,35 @@ def cpu_sample(case, budget_s, warm=1):
         el = time.perf_counter() - t0
         if el >= budget_s:
             break
+    if keep is not None:
+        keep.append(o)
     fl = case.fluid_nodes()
     return {"value": fl * n / el / 1e6, "unit": "MLUPS", "cores": num_threads(), "kind": "port",
             "sample": f"{n} full FP64 oracle steps of {case.name} after {warm} warm-up step(s), {el:.1f} s"}
+
+
+def fp64_error(case, o, dev):
+    """The error the metric is stated at: a fresh simulation of the workload
+    stepped as many steps as the FP64 oracle o (pinned to the reference's own
+    kernels), from the same initial state, against it."""
+    import numpy as np
+    from preprocess_src_b200 import configs
+    from preprocess_src_b200.step import Simulation
+    sim = Simulation(case, device=dev)
+    sim.step(o.iter)
+    lat = sim.export_lattice(fn=False)
+    cel = sim.export_cells()
+    sim.close()
+    m = case.bc == configs.COMP
+    u = np.concatenate([lat[k][m] for k in ("un", "vn", "wn")])
+    uref = np.concatenate([o[k][m] for k in ("un", "vn", "wn")])
+    x = np.concatenate([cel[k] for k in ("x", "y", "z")])
+    xref = np.concatenate([o[k] for k in ("x", "y", "z")])
+    return {"steps": int(o.iter), "velocity_rel_l2": float(np.linalg.norm(u - uref) / np.linalg.norm(uref)),
+            "density_max_abs": float(np.abs(lat["dn"][m] - o["dn"][m]).max()),
+            "position_max_abs": float(np.abs(x - xref).max()),
+            "against": "the FP64 CPU oracle (pinned to the reference's kernels by the golden tests), "
+                       "same initial state, same number of steps"}
 
 
 def run_ours(args, world, rank, local):
@@ -280,7 +307,9 @@ def run_ours(args, world, rank, local):
         if e2e:
             result["e2e"] = e2e
         if world == 1 and not args.no_cpu and args.workload != "vof":
-            result["cpu_baseline"] = cpu_sample(case, args.cpu_seconds)
+            keep = []
+            result["cpu_baseline"] = cpu_sample(case, args.cpu_seconds, keep=keep)
+            result["fp64_error"] = fp64_error(case, keep[0], dev)
     sim.close()
     return result
 
