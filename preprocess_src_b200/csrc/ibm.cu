@@ -285,6 +285,7 @@ spread_kernel(const Geom g, const double *__restrict__ X, long long nv, int V,
               const float *__restrict__ Fv, const ForceField F, const uint32_t *__restrict__ mask2d,
               int *__restrict__ flags)
 {
+    pdl_start();
     spread_body<XPER>(g, X, nv, V, patch_off, patch_vtx, patch_stride, npatch, Fv, F, mask2d, flags, blockIdx.x);
 }
 
@@ -299,8 +300,8 @@ void launch_spread(const Geom &g, const SpreadArgs &a, cudaStream_t s)
 {
     if (a.ncell <= 0) return;
     auto k = g.xper ? spread_kernel<true> : spread_kernel<false>;
-    k<<<a.ncell * a.npatch, SPREAD_THREADS, SPREAD_SMEM, s>>>(
-        g, a.X, a.nv, a.V, a.patch_off, a.patch_vtx, a.patch_stride, a.npatch, a.Fv, a.F, a.mask2d, a.flags);
+    launch_pdl(k, dim3(a.ncell * a.npatch), dim3(SPREAD_THREADS), SPREAD_SMEM, s,
+               g, a.X, a.nv, a.V, a.patch_off, a.patch_vtx, a.patch_stride, a.npatch, a.Fv, a.F, a.mask2d, a.flags);
 }
 
 // ---- interpolation + RK4 advection ---------------------------------------
@@ -547,6 +548,7 @@ advect_kernel(const Geom g, double *__restrict__ X, double *__restrict__ Xd, flo
               const float4 *__restrict__ uvr, long long nv, int V, const int *__restrict__ patch_off,
               const int *__restrict__ patch_vtx, int npatch, double dtM, int *__restrict__ flags)
 {
+    pdl_start();
     advect_body<XPER, RK>(g, X, Xd, U, uvr, nv, V, patch_off, patch_vtx, npatch, dtM, flags, blockIdx.x);
 }
 
@@ -568,8 +570,8 @@ void launch_advect(const Geom &g, const AdvectArgs &a, cudaStream_t s)
     auto k = a.rk == 1 ? (g.xper ? advect_kernel<true, 1> : advect_kernel<false, 1>)
            : a.rk == 2 ? (g.xper ? advect_kernel<true, 2> : advect_kernel<false, 2>)
                        : (g.xper ? advect_kernel<true, 4> : advect_kernel<false, 4>);
-    k<<<a.ncell * a.npatch, ADVECT_THREADS, ADVECT_SMEM, s>>>(
-        g, a.X, a.Xd, a.U, a.uvr, a.nv, a.V, a.patch_off, a.patch_vtx, a.npatch, a.dtM, a.flags);
+    launch_pdl(k, dim3(a.ncell * a.npatch), dim3(ADVECT_THREADS), ADVECT_SMEM, s,
+               g, a.X, a.Xd, a.U, a.uvr, a.nv, a.V, a.patch_off, a.patch_vtx, a.npatch, a.dtM, a.flags);
 }
 
 // ---- fused batches ---------------------------------------------------------

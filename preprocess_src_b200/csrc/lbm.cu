@@ -337,6 +337,7 @@ lbm_collide_stream(const typename Store<STORE>::T *__restrict__ gin, typename St
                    int nx, int ny, int nzc, I nint,
                    float omega, float Cr, float Bc, int acc, float Mf)
 {
+    pdl_start();
     lbm_collide_stream_body<STORE, I, VISC, TAU1, SUB>(gin, gout, uvr, F, Fbits, wpp, mask2d, drive, iter, wall, vf,
                                                        lm1, df3, nx, ny, nzc, nint, omega, Cr, Bc, blockIdx.x,
                                                        blockIdx.y, gridDim.y, acc, Mf);
@@ -361,7 +362,7 @@ void launch_lbm(const Geom &g, int storage, const LbmArgs &a, cudaStream_t s)
     const dim3 blocks((unsigned)((g.plane + LBM_THREADS - 1) / LBM_THREADS), (unsigned)(gz < 65535 ? gz : 65535));
     const bool off32 = (long long)Q * g.nint < (1LL << 31);   // every element offset fits in an int
 #define LBM_LAUNCH(ST, I, V, T1, SB)                                                                          \
-    lbm_collide_stream<ST, I, V, T1, SB><<<blocks, LBM_THREADS, 0, s>>>(                                      \
+    launch_pdl(lbm_collide_stream<ST, I, V, T1, SB>, blocks, dim3(LBM_THREADS), 0, s,                            \
         (const Store<ST>::T *)a.gin, (Store<ST>::T *)a.gout, a.uvr, a.F.F, a.F.bits, a.F.wpp, a.mask2d, a.drive, a.iter, \
         a.wall, a.vf, \
         a.lm1, a.df3, g.nx, g.ny, g.nzc, (I)g.nint, a.omega, a.Cr, a.Bc, a.acc, a.Mf)
@@ -426,6 +427,7 @@ void launch_lbm_fused(const FusedLaunch &f, int storage, bool off32, int threads
 // one warp per 32 words (whole warps: every lane takes part in the ballot)
 __global__ void force_reset_kernel(const ForceField F, long long nwords, long long plane, long long nint)
 {
+    pdl_start();
     const long long w0 = (((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32;
     if (w0 < nwords) force_reset_words(F.F, F.bits, w0, nwords, F.wpp, plane, nint, threadIdx.x & 31);
 }
@@ -433,7 +435,8 @@ __global__ void force_reset_kernel(const ForceField F, long long nwords, long lo
 void launch_force_reset(const Geom &g, const ForceField &F, cudaStream_t s)
 {
     const long long nw = (long long)g.nzc * F.wpp;
-    force_reset_kernel<<<(unsigned)((nw + 255) / 256), 256, 0, s>>>(F, nw, g.plane, g.nint);
+    launch_pdl(force_reset_kernel, dim3((unsigned)((nw + 255) / 256)), dim3(256), 0, s, F, nw, (long long)g.plane,
+               (long long)g.nint);
 }
 
 // ---- circular tube: interpolated bounce-back ------------------------------

@@ -308,6 +308,7 @@ template <typename Real, int VPT>
 __global__ void __launch_bounds__(mem_max_threads<VPT>(), 1)
 membrane_kernel(const MembraneArgs a)
 {
+    pdl_start();
     membrane_body<Real, VPT>(a, blockIdx.x);
 }
 
@@ -325,11 +326,13 @@ static void launch_vpt(const MembraneArgs &a, cudaStream_t s)
     cfg.blockDim = dim3((unsigned)T);
     cfg.dynamicSmemBytes = (size_t)smem;
     cfg.stream = s;
-    cudaLaunchAttribute attr[1];
+    cudaLaunchAttribute attr[2];
     attr[0].id = cudaLaunchAttributePriority;
     attr[0].val.priority = a.priority;
+    attr[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[1].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
-    cfg.numAttrs = 1;
+    cfg.numAttrs = 2;
     cudaLaunchKernelEx(&cfg, k, a);
 }
 

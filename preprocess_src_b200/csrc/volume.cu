@@ -149,6 +149,7 @@ __device__ __forceinline__ void volume_body(const Geom &g, const VolumeArgs &a, 
 __global__ void __launch_bounds__(VOL_THREADS)
 volume_kernel(const Geom g, const VolumeArgs a)
 {
+    pdl_start();
     volume_body(g, a, blockIdx.x);
 }
 
@@ -156,7 +157,7 @@ void launch_volume(const Geom &g, const VolumeArgs &a, cudaStream_t s)
 {
     if (a.ncell <= 0) return;
     const int smem = volume_smem_bytes(a.V);
-    volume_kernel<<<a.ncell, VOL_THREADS, smem, s>>>(g, a);
+    launch_pdl(volume_kernel, dim3(a.ncell), dim3(VOL_THREADS), smem, s, g, a);
 }
 
 cudaError_t membrane_setup(int optin, int *max_bytes);
@@ -217,12 +218,13 @@ __device__ __forceinline__ void step_begin_body(const StepBeginArgs &a)
 
 __global__ void step_begin_kernel(const StepBeginArgs a)
 {
+    pdl_start();
     step_begin_body(a);
 }
 
 void launch_step_begin(const StepBeginArgs &a, cudaStream_t s)
 {
-    step_begin_kernel<<<1, 1, 0, s>>>(a);
+    launch_pdl(step_begin_kernel, dim3(1), dim3(1), 0, s, a);
 }
 
 // ---- fused batches ---------------------------------------------------------
