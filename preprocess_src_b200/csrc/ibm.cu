@@ -310,7 +310,11 @@ void launch_spread(const Geom &g, const SpreadArgs &a, cudaStream_t s)
 // The stage-1 stencil is loaded once into registers (u, v, w of 16 nodes) and
 // reused by the later RK stages, whose positions move by u dt / 2 ~ 1e-3 and
 // almost never leave the stage-1 lattice cell; a stage that does re-gathers.
-// The group sums its partial velocities with two butterfly shuffles.
+// The group sums its partial velocities with two butterfly shuffles.  Stage 1
+// locates the vertex in FP64 (positions ~100 lattice units); the later stages'
+// fractions are the stage-1 fraction plus the move u h / dx in FP32 (one more
+// FP32 rounding of a number below 1, where the FP64 position would round the
+// same move to about 1e-14).
 struct Plane16 {
     float u[16], v[16], w[16];
 };
@@ -452,15 +456,22 @@ advect_body(const Geom &g, double *__restrict__ X, double *__restrict__ Xd, floa
         const int nb = bxs * bys * bzs;
         int x = tid % bxs, y = (tid / bxs) % bys, z = tid / (bxs * bys);
         const int sx = ADVECT_THREADS % bxs, sy = (ADVECT_THREADS / bxs) % bys, sz = ADVECT_THREADS / (bxs * bys);
-        for (int li = tid; li < nb; li += ADVECT_THREADS) {
-            const int gx = XPER ? wrap_x(bx0 + x, g.nx) : bx0 + x, gy = by0 + y;
-            float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (gx >= 0 && gx < g.nx && gy >= 0 && gy < g.ny)
-                q = __ldg(&uvr[(long long)wrap_z(bz0 + z, g.nzc) * g.plane + gx + (long long)g.nx * gy]);
-            abox[li] = q;
-            x += sx; y += sy; z += sz;
-            if (x >= bxs) { x -= bxs; y++; }
-            if (y >= bys) { y -= bys; z++; }
+        // four nodes per thread and round: their loads are issued before any store
+        for (int li = tid; li < nb; li += 4 * ADVECT_THREADS) {
+            float4 q[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const int gx = XPER ? wrap_x(bx0 + x, g.nx) : bx0 + x, gy = by0 + y;
+                q[u] = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (li + u * ADVECT_THREADS < nb && gx >= 0 && gx < g.nx && gy >= 0 && gy < g.ny)
+                    q[u] = __ldg(&uvr[(long long)wrap_z(bz0 + z, g.nzc) * g.plane + gx + (long long)g.nx * gy]);
+                x += sx; y += sy; z += sz;
+                if (x >= bxs) { x -= bxs; y++; }
+                if (y >= bys) { y -= bys; z++; }
+            }
+#pragma unroll
+            for (int u = 0; u < 4; u++)
+                if (li + u * ADVECT_THREADS < nb) abox[li + u * ADVECT_THREADS] = q[u];
         }
     }
     __syncthreads();
@@ -497,17 +508,21 @@ advect_body(const Geom &g, double *__restrict__ X, double *__restrict__ Xd, floa
                 gather_plane(g, uvr, cx, cy, izr, xm, P);
         };
         fetch(bx, by, bz);
+        // the later stages' lattice positions relative to the stage-1 cell, in FP32:
+        // x_k = x_n + u_{k-1} h moves the vertex by u h / dx lattice units (~1e-2)
+        const int bx1 = bx, by1 = by, bz1 = bz;
+        const float f1x = fx, f1y = fy, f1z = fz;
         float us[RK], vs[RK], ws[RK];
 #pragma unroll
         for (int k = 0; k < RK; k++) {
-            double px = xn, py = yn, pz = zn;
             if (k > 0) {
                 // RK4: x + u1 M dt / 2, x + u2 M dt / 2, x + u3 M dt (ibm.cu:487-505);
                 // RK2: x + u1 M (ibm.cu:560-562; dt = 1 there)
-                const double h = (RK == 4 && k < 3 ? 0.5 : 1.0) * dtM;
-                px += us[k - 1] * h; py += vs[k - 1] * h; pz += ws[k - 1] * h;
-                int cx, cy, cz;
-                lattice_cell(g, px, py, pz, cx, cy, cz, fx, fy, fz);
+                const float hs = (float)((RK == 4 && k < 3 ? 0.5 : 1.0) * dtM * g.inv_dx);
+                const float gxs = fmaf(us[k - 1], hs, f1x), gys = fmaf(vs[k - 1], hs, f1y), gzs = fmaf(ws[k - 1], hs, f1z);
+                const float sx = floorf(gxs), sy = floorf(gys), sz = floorf(gzs);
+                fx = gxs - sx; fy = gys - sy; fz = gzs - sz;
+                const int cx = bx1 + (int)sx, cy = by1 + (int)sy, cz = bz1 + (int)sz;
                 if (cx != bx || cy != by || cz != bz) {   // uniform across the 4 lanes of the vertex
                     bx = cx; by = cy; bz = cz;
                     fetch(bx, by, bz);
