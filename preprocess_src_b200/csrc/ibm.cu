@@ -43,6 +43,24 @@ __device__ __forceinline__ bool to_fixed(double v, int shift, long long &out) {
     return true;
 }
 
+// v * 2^shift rounded to the nearest integer, ties to even (as __double2ll_rn
+// of the exact FP64 product, in integer arithmetic); false beyond 2^62 in
+// magnitude.  v: a box sum (|v| < 2^31).
+__device__ __forceinline__ bool box_to_fixed(int v, int shift, long long &out) {
+    if (shift >= 0) {
+        if (shift > 62) { out = 0; return v == 0; }
+        const long long lim = 1LL << (62 - shift);
+        if (v >= lim || -(long long)v >= lim) return false;
+        out = (long long)v << shift;
+        return true;
+    }
+    const int k = -shift;
+    if (k > 32) { out = 0; return true; }
+    const long long x = v, q = x >> k, r = x - (q << k), half = 1LL << (k - 1);
+    out = (r > half || (r == half && (q & 1))) ? q + 1 : q;
+    return true;
+}
+
 // Adds one node's fixed-point force (three components; zeros skipped).
 // *added: whether anything was added (the node's occupancy bit must be set).
 // Returns false if a component was out of range.
@@ -79,6 +97,9 @@ spread_body(const Geom &g, const double *__restrict__ X, long long nv, int V,
             int *__restrict__ flags, int bid)
 {
     extern __shared__ unsigned sbox[];
+    // each patch vertex's lattice cell, unwrap shifts and fractions, from the bounds pass
+    __shared__ int4 s_cell[MAX_PATCH_VERTICES];      // floor(lx), floor(ly), floor(lz), z unwrap shift
+    __shared__ float4 s_frac[MAX_PATCH_VERTICES];    // lx - floor(lx), ly - floor(ly), lz - floor(lz), x shift
     __shared__ int s_lo[3], s_hi[3];
     __shared__ unsigned s_fmax[3], s_wmax;
     const int cell = bid / npatch, patch = bid - cell * npatch, tid = threadIdx.x;
@@ -102,10 +123,15 @@ spread_body(const Geom &g, const double *__restrict__ X, long long nv, int V,
         nonfinite |= !(afx <= FLT_MAX && afy <= FLT_MAX && afz <= FLT_MAX);
         fmax0 = fmaxf(fmax0, afx); fmax1 = fmaxf(fmax1, afy); fmax2 = fmaxf(fmax2, afz);
         const double lxr = lat_x(g, xs[v]), lxv = XPER ? unwrap_near(lxr, ax, g.nx) : lxr;
-        const double lyv = lat_y(g, ys[v]), lzv = unwrap_near(lat_z(g, zs[v]), az, g.nzc);
+        const double lzr = lat_z(g, zs[v]);
+        const double lyv = lat_y(g, ys[v]), lzv = unwrap_near(lzr, az, g.nzc);
         if (!(sane_lattice(lxv) && sane_lattice(lyv) && sane_lattice(lzv) && sane_lattice(az) && sane_lattice(ax))) { nonfinite = true; continue; }
-        const int ix = (int)floor(lxv), iy = (int)floor(lyv);
-        const int iz = (int)floor(lzv);
+        const double flx = floor(lxv), fly = floor(lyv), flz = floor(lzv);
+        const int ix = (int)flx, iy = (int)fly;
+        const int iz = (int)flz;
+        const int xsh = XPER ? (int)lrint(lxv - lxr) : 0, zsh = (int)lrint(lzv - lzr);   // unwrapped minus raw frame
+        s_cell[k] = make_int4(ix, iy, iz, zsh);
+        s_frac[k] = make_float4((float)(lxv - flx), (float)(lyv - fly), (float)(lzv - flz), (float)xsh);
         lo0 = min(lo0, ix - 1); hi0 = max(hi0, ix + 2);
         lo1 = min(lo1, iy - 1); hi1 = max(hi1, iy + 2);
         lo2 = min(lo2, iz - 1); hi2 = max(hi2, iz + 2);
@@ -154,11 +180,8 @@ spread_body(const Geom &g, const double *__restrict__ X, long long nv, int V,
         for (int i = tid; i < nbi; i += SPREAD_THREADS) cnt[i] = 0u;
         __syncthreads();
         for (int k = tid; k < np; k += SPREAD_THREADS) {
-            const int v = patch_vtx[p0 + k];
-            const double lxr = lat_x(g, xs[v]);
-            const int ix = (int)floor(XPER ? unwrap_near(lxr, ax, g.nx) : lxr), iy = (int)floor(lat_y(g, ys[v]));
-            const int iz = (int)floor(unwrap_near(lat_z(g, zs[v]), az, g.nzc));
-            const int li0 = (ix - 1 - bx0) + bx * (iy - 1 - by0) + psi * (iz - bz0);
+            const int4 cl = s_cell[k];
+            const int li0 = (cl.x - 1 - bx0) + bx * (cl.y - 1 - by0) + psi * (cl.z - bz0);
 #pragma unroll
             for (int b = 0; b < 4; b++)
 #pragma unroll
@@ -203,22 +226,20 @@ spread_body(const Geom &g, const double *__restrict__ X, long long nv, int V,
     int jv = (int)(((long long)(tid >> 2) * vstride) % np);
     for (int j = tid >> 2; j < np; j += jstep) {
         const int v = patch_vtx[p0 + jv];
+        const int4 cl = s_cell[jv];
+        const float4 fr = s_frac[jv];
         jv += vstep;
         if (jv >= np) jv -= np;
-        const double lxr = lat_x(g, xs[v]), lx = XPER ? unwrap_near(lxr, ax, g.nx) : lxr, ly = lat_y(g, ys[v]);
-        const int xsh = XPER ? (int)lrint(lx - lxr) : 0;   // unwrapped minus raw frame
-        const double lzr = lat_z(g, zs[v]);
-        const double lz = unwrap_near(lzr, az, g.nzc);
-        const double flx = floor(lx), fly = floor(ly), flz = floor(lz);
-        const int iz = (int)flz - 1 + c;
+        const int xsh = (int)fr.w, zsh = cl.w;   // unwrapped minus raw frame (x shift exact in FP32: |x| < 2^24)
+        const int iz = cl.z - 1 + c;
         // the reference's lattice ends two BUFF planes beyond the periodic
         // range; stencil nodes past them are skipped (ibm.cu:107-110)
-        const int izr = iz - (int)lrint(lz - lzr);
+        const int izr = iz - zsh;
         if (izr < -2 || izr >= g.nzc + 2) continue;
         float wx[4], wy[4], wz[4];
-        delta4((float)(lx - flx), wx); delta4((float)(ly - fly), wy); delta4((float)(lz - flz), wz);
+        delta4(fr.x, wx); delta4(fr.y, wy); delta4(fr.z, wz);
         const float wzc = c == 0 ? wz[0] : c == 1 ? wz[1] : c == 2 ? wz[2] : wz[3];
-        const int ix0 = (int)flx - 1, iy0 = (int)fly - 1;
+        const int ix0 = cl.x - 1, iy0 = cl.y - 1;
         const float sc = wscale * wzc;
         const float f0 = fxs[v] * sc, f1 = fys[v] * sc, f2 = fzs[v] * sc;
         const float q0 = f0 * qs[0], q1 = f1 * qs[1], q2 = f2 * qs[2];
@@ -269,11 +290,14 @@ spread_body(const Geom &g, const double *__restrict__ X, long long nv, int V,
         if (!(__ldg(&mask2d[gx + g.nx * gy]) & MASK_FLUID)) continue;   // wall column: the LBM never reads it
         const int zw = wrap_z(bz0 + lz, g.nzc);
         const long long xy = gx + (long long)g.nx * gy, gi = (long long)zw * g.plane + xy;
-        bool added = false;
-        if (!add_force(F, g.nint, gi, (double)ia, (double)ib, (double)ic, FORCE_FRAC - qe[0],
-                       FORCE_FRAC - qe[1], FORCE_FRAC - qe[2], &added))
-            atomicOr(flags, RBC_FLAG_NONFINITE);
-        if (added) atomicOr(&F.bits[(long long)zw * F.wpp + (xy >> 5)], 1u << (xy & 31));
+        long long fa = 0, fb = 0, fc = 0;
+        const bool ok = box_to_fixed(ia, FORCE_FRAC - qe[0], fa) & box_to_fixed(ib, FORCE_FRAC - qe[1], fb) &
+                        box_to_fixed(ic, FORCE_FRAC - qe[2], fc);
+        if (!ok) atomicOr(flags, RBC_FLAG_NONFINITE);
+        if (fa) atomicAdd(reinterpret_cast<unsigned long long *>(&F.F[gi]), (unsigned long long)fa);
+        if (fb) atomicAdd(reinterpret_cast<unsigned long long *>(&F.F[g.nint + gi]), (unsigned long long)fb);
+        if (fc) atomicAdd(reinterpret_cast<unsigned long long *>(&F.F[2 * g.nint + gi]), (unsigned long long)fc);
+        if (fa | fb | fc) atomicOr(&F.bits[(long long)zw * F.wpp + (xy >> 5)], 1u << (xy & 31));
     }
 }
 
