@@ -57,7 +57,9 @@ namespace rbc {
 
 constexpr int MEM_MAX_THREADS = 1024;
 
-// pos 24V (then float4 d-buffers 32V), coef 24V, nbr 12V
+// pos 24V (then float4 d-buffers 32V), coef 24V, and 12V that the adjoint's
+// membrane pass uses for its neighbour table (this kernel reads its neighbours
+// from global memory once, into registers)
 int membrane_smem_bytes(int V) { return 68 * V; }
 
 __device__ __forceinline__ double mimage(double d, double L) {
@@ -114,7 +116,6 @@ __device__ __forceinline__ void membrane_body(const MembraneArgs &a, int cell)
     double *pos = reinterpret_cast<double *>(smem);                    // [3][V]
     float4 *dbuf = reinterpret_cast<float4 *>(smem);                   // [2][V], after assembly
     float *coef = reinterpret_cast<float *>(smem + 32 * (size_t)V);    // [6][V]
-    int16_t *snbr = reinterpret_cast<int16_t *>(smem + 56 * (size_t)V);// [6][V]
 
     const long long vb = (long long)cell * V, eb = (long long)cell * E, nv = a.nv;
     const double ax = a.Xd[vb], ay = a.Xd[nv + vb], az = a.Xd[2 * nv + vb];
@@ -123,7 +124,6 @@ __device__ __forceinline__ void membrane_body(const MembraneArgs &a, int cell)
         pos[V + v] = a.Xd[nv + vb + v] - ay;
         pos[2 * V + v] = a.Xd[2 * nv + vb + v] - az;
     }
-    for (int k = tid; k < 6 * V; k += T) snbr[k] = a.nbrp[k];   // neighbours by solve position
     __syncthreads();
 
     // element pass: tension of each element once (stress.cu:29-110, 195-270)
@@ -250,7 +250,7 @@ __device__ __forceinline__ void membrane_body(const MembraneArgs &a, int cell)
         const int p = tid + m * T;
 #pragma unroll
         for (int s = 0; s < 6; s++) {
-            const int j = p < V ? snbr[s * V + p] : -1;
+            const int j = p < V ? (int)__ldg(&a.nbrp[s * V + p]) : -1;   // neighbours by solve position
             const unsigned id = (unsigned)(j >= 0 ? j : (p < V ? p : 0));
             if (s & 1) nb[m][s >> 1] |= id << 16; else nb[m][s >> 1] = id;
             cf[m][s] = j >= 0 ? coef[s * V + p] : 0.f;
