@@ -57,7 +57,7 @@ namespace rbc {
 
 constexpr int MEM_MAX_THREADS = 1024;
 
-// pos 24V (then float4 d-buffers 32V), coef 24V, and 12V that the adjoint's
+// pos 24V (then the solve's two d-buffers, 3 x V floats each), coef 24V, and 12V that the adjoint's
 // membrane pass uses for its neighbour table (this kernel reads its neighbours
 // from global memory once, into registers)
 int membrane_smem_bytes(int V) { return 68 * V; }
@@ -114,7 +114,7 @@ __device__ __forceinline__ void membrane_body(const MembraneArgs &a, int cell)
     __shared__ float red[32];
     const int V = a.V, E = a.E, tid = threadIdx.x, T = blockDim.x;
     double *pos = reinterpret_cast<double *>(smem);                    // [3][V]
-    float4 *dbuf = reinterpret_cast<float4 *>(smem);                   // [2][V], after assembly
+    float *dbuf = reinterpret_cast<float *>(smem);                     // [2][3][V], after assembly
     float *coef = reinterpret_cast<float *>(smem + 32 * (size_t)V);    // [6][V]
 
     const long long vb = (long long)cell * V, eb = (long long)cell * E, nv = a.nv;
@@ -238,7 +238,7 @@ __device__ __forceinline__ void membrane_body(const MembraneArgs &a, int cell)
             x[m][c] = 0.f; r[m][c] = rhs[m][c]; d[m][c] = rhs[m][c] / theta;
             bb += rhs[m][c] * rhs[m][c];
         }
-        if (p < V) dbuf[p] = make_float4(d[m][0], d[m][1], d[m][2], 0.f);
+        if (p < V) { dbuf[p] = d[m][0]; dbuf[V + p] = d[m][1]; dbuf[2 * V + p] = d[m][2]; }
     }
     // each vertex's neighbours and row coefficients stay in registers for the
     // whole solve (a missing sixth neighbour points at the vertex itself with
@@ -258,8 +258,10 @@ __device__ __forceinline__ void membrane_body(const MembraneArgs &a, int cell)
     }
     __syncthreads();
     for (int it = 0; it < a.niter; it++) {
-        const float4 *cur = dbuf + (it & 1) * V;
-        float4 *nxt = dbuf + ((it + 1) & 1) * V;
+        // one array per component: three 4-byte gathers per neighbour, whose
+        // warp-wide reads of nearby positions take one wavefront each
+        const float *cur = dbuf + (it & 1) * 3 * V;
+        float *nxt = dbuf + ((it + 1) & 1) * 3 * V;
         const float rho_n = 1.0f / (2.0f * sigma - rho);
         const float c1 = rho_n * rho, c2 = 2.0f * rho_n / delta;
 #pragma unroll
@@ -270,14 +272,14 @@ __device__ __forceinline__ void membrane_body(const MembraneArgs &a, int cell)
 #pragma unroll
             for (int s = 0; s < 6; s++) {
                 const float w = cf[m][s];
-                const float4 dj = cur[(s & 1) ? nb[m][s >> 1] >> 16 : nb[m][s >> 1] & 0xFFFFu];
-                ad0 += w * dj.x; ad1 += w * dj.y; ad2 += w * dj.z;
+                const unsigned j = (s & 1) ? nb[m][s >> 1] >> 16 : nb[m][s >> 1] & 0xFFFFu;
+                ad0 += w * cur[j]; ad1 += w * cur[V + j]; ad2 += w * cur[2 * V + j];
             }
             x[m][0] += d[m][0]; x[m][1] += d[m][1]; x[m][2] += d[m][2];
             r[m][0] -= ad0; r[m][1] -= ad1; r[m][2] -= ad2;
 #pragma unroll
             for (int c = 0; c < 3; c++) d[m][c] = c1 * d[m][c] + c2 * r[m][c];
-            nxt[p] = make_float4(d[m][0], d[m][1], d[m][2], 0.f);
+            nxt[p] = d[m][0]; nxt[V + p] = d[m][1]; nxt[2 * V + p] = d[m][2];
         }
         rho = rho_n;
         __syncthreads();
