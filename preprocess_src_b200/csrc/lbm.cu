@@ -491,10 +491,6 @@ void launch_tube_bounce(const Geom &g, int storage, void *gout, const int *links
 
 // ---- reference layout <-> internal layout ---------------------------------
 
-// reference-layout index of internal node (x, y, z) (x and z without the BUFF layers)
-__device__ __forceinline__ long long ref_index(const Geom &g, int x, int y, int z) {
-    return (long long)(x + g.xb) + (long long)g.nxr * (y + (long long)g.ny * (z + 2));
-}
 __device__ __forceinline__ int nb_x(const Geom &g, int x, int d) { return g.xper ? wrap_x(x + d, g.nx) : x + d; }
 
 // The moving-wall term of a bounced population in direction q at a node of
@@ -511,16 +507,26 @@ __device__ __forceinline__ double wall_term(int q, uint32_t m, double rho, const
 // velocities in that step; rho = 1 + the sum of the node's slots, which the
 // terms leave unchanged since the two linked directions have opposite e_z).
 template <int STORE>
-__global__ void import_lattice_kernel(const Geom g, const double *__restrict__ fn, typename Store<STORE>::T *__restrict__ gout,
-                                      const uint32_t *__restrict__ mask2d, float scale, const WallVel w)
+__global__ void import_lattice_kernel(const Geom g, const ImportPlanes src, typename Store<STORE>::T *__restrict__ gout,
+                                      const uint32_t *__restrict__ mask2d, float scale, const WallVel w, int z0, int z1)
 {
     using S = Store<STORE>;
-    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= g.nint) return;
+    const long long idx = (long long)z0 * g.plane + (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long long)z1 * g.plane) return;
     const int z = (int)(idx / g.plane);
     const int xy = (int)(idx - (long long)z * g.plane);
     const int y = xy / g.nx, x = xy - y * g.nx;
     const uint32_t m = mask2d[xy];
+    // reference plane of internal plane zz in [-1, nzc] (the periodic images -1 -> nzc - 1, nzc -> 0
+    // are the two edge planes)
+    auto plane = [&](int zz) -> const double * {
+        if (zz < 0) return src.edge;
+        if (zz >= g.nzc) return src.edge + src.plane_vals;
+        return src.ring + (long long)(zz % src.ring_planes) * src.plane_vals;
+    };
+    auto at = [&](const double *pl, int xx, int yy) -> const double * {
+        return pl + ((long long)(xx + g.xb) + (long long)g.nxr * yy) * Q;
+    };
     double val[Q];
     double rho = 1.0;
 #pragma unroll
@@ -528,8 +534,8 @@ __global__ void import_lattice_kernel(const Geom g, const double *__restrict__ f
         val[q] = 0.0;
         if (m & MASK_FLUID) {
             double f;
-            if ((m >> opp(q)) & 1u) f = fn[ref_index(g, x, y, z) * Q + opp(q)];
-            else f = fn[ref_index(g, nb_x(g, x, ex(q)), y + ey(q), wrap_z(z + ez(q), g.nzc)) * Q + q];
+            if ((m >> opp(q)) & 1u) f = at(plane(z), x, y)[opp(q)];
+            else f = at(plane(z + ez(q)), nb_x(g, x, ex(q)), y + ey(q))[q];
             val[q] = f - wqd(q);
             rho += val[q];
         }
@@ -657,14 +663,26 @@ void launch_fill_f4(float4 *p, long long n, float4 v, cudaStream_t s)
     fill_f4_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(p, n, v);
 }
 
-void launch_import_lattice(const Geom &g, int storage, const double *fn_ref, void *gout,
-                           const uint32_t *mask2d, float scale, const WallVel &w, cudaStream_t s)
+cudaError_t lattice_io_setup()
 {
-    const unsigned blocks = (unsigned)((g.nint + 255) / 256);
+    // load the import and export kernels now (lazy module loading would load each in its first call)
+    cudaFuncAttributes fa;
+    cudaError_t e = cudaFuncGetAttributes(&fa, (const void *)import_lattice_kernel<RBC_STORE_F32>);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, (const void *)import_lattice_kernel<RBC_STORE_F16>);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, (const void *)export_lattice_kernel<RBC_STORE_F32>);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, (const void *)export_lattice_kernel<RBC_STORE_F16>);
+    return e;
+}
+
+void launch_import_lattice(const Geom &g, int storage, const ImportPlanes &src, void *gout, const uint32_t *mask2d,
+                           float scale, const WallVel &w, int z0, int z1, cudaStream_t s)
+{
+    const unsigned blocks = (unsigned)(((long long)(z1 - z0) * g.plane + 255) / 256);
+    if (blocks == 0) return;
     if (storage == RBC_STORE_F16)
-        import_lattice_kernel<RBC_STORE_F16><<<blocks, 256, 0, s>>>(g, fn_ref, (__half *)gout, mask2d, scale, w);
+        import_lattice_kernel<RBC_STORE_F16><<<blocks, 256, 0, s>>>(g, src, (__half *)gout, mask2d, scale, w, z0, z1);
     else
-        import_lattice_kernel<RBC_STORE_F32><<<blocks, 256, 0, s>>>(g, fn_ref, (float *)gout, mask2d, scale, w);
+        import_lattice_kernel<RBC_STORE_F32><<<blocks, 256, 0, s>>>(g, src, (float *)gout, mask2d, scale, w, z0, z1);
 }
 
 void launch_export_lattice(const Geom &g, int storage, const void *gin, const uint32_t *mask2d,

@@ -99,6 +99,11 @@ struct rbc_handle {
     // host<->reference staging
     void *staging = nullptr;
     size_t staging_bytes = 0;
+    // lattice import: IMPORT_SLOTS chunks of imp_planes reference planes in a ring, then the two
+    // periodic edge planes; a copy and a conversion event per slot (allocated on first use)
+    double *imp_ring = nullptr;
+    int imp_planes = 0;
+    cudaEvent_t imp_copied[4] = {}, imp_freed[4] = {};
     int iter = 0;
     // the IB force field may hold nonzero values: a spread not yet cleared (a
     // stage call, or a sub-cycled step ended before the last step of its M)
@@ -654,8 +659,13 @@ void free_all(rbc_handle *h)
     if (h->lbm_done) cudaEventDestroy(h->lbm_done);
     if (h->reset_done) cudaEventDestroy(h->reset_done);
     if (h->side2) cudaStreamDestroy(h->side2);
+    for (int k = 0; k < 4; k++) {
+        if (h->imp_copied[k]) cudaEventDestroy(h->imp_copied[k]);
+        if (h->imp_freed[k]) cudaEventDestroy(h->imp_freed[k]);
+    }
     void *ptrs[] = {h->g[0], h->g[1], h->uvr, h->Fint, h->Fbits, h->mask2d, h->tube_links, h->tube_frac,
-                    h->d_int, h->d_drive, h->staging, h->vof_s1, h->vof_s2, h->vof_G, h->vof_b, h->vof_partial};
+                    h->d_int, h->d_drive, h->staging, h->vof_s1, h->vof_s2, h->vof_G, h->vof_b, h->vof_partial,
+                    h->imp_ring};
     for (void *q : ptrs) if (q) cudaFree(q);
     for (CellGroup &c : h->cg) free_group(c);
     vof_mg_free(h->vof_mg);
@@ -1414,6 +1424,37 @@ const char *rbc_last_error(const rbc_handle *h)
     return h ? h->err.c_str() : g_create_error.c_str();
 }
 
+constexpr int IMPORT_SLOTS = 4;
+constexpr size_t IMPORT_CHUNK_BYTES = size_t(16) << 20;
+
+// reference planes per import chunk: about IMPORT_CHUNK_BYTES, at most the whole lattice
+static int import_chunk_planes(const Geom &g)
+{
+    const size_t plane_bytes = sizeof(double) * (size_t)g.nxr * g.ny * Q;
+    return std::max(1, std::min(g.nzc, (int)(IMPORT_CHUNK_BYTES / plane_bytes)));
+}
+
+// the import ring (IMPORT_SLOTS chunks and the two edge planes) and its events
+static int ensure_import_ring(rbc_handle *h)
+{
+    const Geom &g = h->geo;
+    const int P = import_chunk_planes(g);
+    if (h->imp_ring && h->imp_planes == P) return RBC_OK;
+    const size_t plane_bytes = sizeof(double) * (size_t)g.nxr * g.ny * Q;
+    if (h->imp_ring) { CK(cudaFree(h->imp_ring)); h->imp_ring = nullptr; }
+    CK(cudaMalloc(&h->imp_ring, plane_bytes * (size_t)(IMPORT_SLOTS * P + 2)));
+    h->imp_planes = P;
+    for (int k = 0; k < IMPORT_SLOTS; k++) {
+        if (!h->imp_copied[k]) CK(cudaEventCreateWithFlags(&h->imp_copied[k], cudaEventDisableTiming));
+        if (!h->imp_freed[k]) CK(cudaEventCreateWithFlags(&h->imp_freed[k], cudaEventDisableTiming));
+    }
+    return RBC_OK;
+}
+
+static int import_lattice_pipelined(rbc_handle *h, const double *fn, const WallVel &w);
+static cudaError_t cell_io_setup();
+static int ensure_cell_staging(rbc_handle *h, const CellGroup &G);
+
 int rbc_create(const rbc_params *p, const rbc_mesh *mesh, const int *bc, rbc_handle **out)
 {
     g_create_error.clear();
@@ -1476,6 +1517,8 @@ int rbc_create(const rbc_params *p, const rbc_mesh *mesh, const int *bc, rbc_han
     {
         int mem_max = 0;
         int e = setup_kernel_attributes(&mem_max);
+        if (!e) e = (int)lattice_io_setup();
+        if (!e) e = (int)cell_io_setup();
         if (e) { h->err = std::string("kernel attributes: ") + cudaGetErrorString((cudaError_t)e); return bail(RBC_ERR_CUDA); }
         if (cells && membrane_smem_bytes(mesh->vertex) > mem_max) {
             h->err = "more vertices per cell than one CTA's shared memory holds";
@@ -1553,18 +1596,20 @@ int rbc_create(const rbc_params *p, const rbc_mesh *mesh, const int *bc, rbc_han
             const int y = (int)((i % g.plane) / g.nx);
             uv[(size_t)i] = (y >= 2 && y < g.ny - 2) ? make_float4(0.f, 0.f, (float)tw_of(y), 1.f) : make_float4(0.f, 0.f, 0.f, 1.f);
         }
-        if (ensure_staging(h, 8 * fn.size()) != RBC_OK ||
-            cudaMemcpy(h->staging, fn.data(), 8 * fn.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
-            cudaMemcpy(h->uvr, uv.data(), 16 * uv.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
+        if (cudaMemcpy(h->uvr, uv.data(), 16 * uv.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+            import_lattice_pipelined(h, fn.data(), wall_velocities(h, 1)) != RBC_OK) {
             h->err = "initial shear profile upload failed";
             return bail(RBC_ERR_CUDA);
         }
-        launch_import_lattice(g, p->storage, (const double *)h->staging, h->g[h->cur], h->mask2d, h->scale,
-                              wall_velocities(h, 1), h->stream);
     }
 
     if (cells) TRY(upload_group(h, h->cg[0], mesh, prep));
     if (p->vof_k > 0) TRY(vof_init_group(h, h->cg[0]));
+    // buffers of the reference-layout imports and exports, allocated here rather than in the first
+    // call: the cells' layout conversions, and the lattice import's ring where the ring is a
+    // bounded part of the lattice (more chunks than slots; smaller lattices allocate it on use)
+    if (cells) TRY(ensure_cell_staging(h, h->cg[0]));
+    if ((g.nzc + import_chunk_planes(g) - 1) / import_chunk_planes(g) > IMPORT_SLOTS) TRY(ensure_import_ring(h));
     if (cudaStreamSynchronize(h->stream) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
         h->err = "initialisation kernels failed";
         return bail(RBC_ERR_CUDA);
@@ -1584,20 +1629,62 @@ int rbc_destroy(rbc_handle *h)
     return RBC_OK;
 }
 
+// Reference fn (host, AoS FP64, all nzc + 4 planes) -> population buffer g[cur], as a pipeline:
+// the copy stream brings chunks of IMPORT_CHUNK_BYTES into a ring of IMPORT_SLOTS slots while the
+// main stream converts each internal slab once the chunk after it has arrived (a slab reads one
+// plane of each neighbouring chunk).  The BUFF planes are not copied; the periodic images of the
+// first and last planes come from two edge planes copied first.  Returns after the conversion.
+static int import_lattice_pipelined(rbc_handle *h, const double *fn, const WallVel &w)
+{
+    const Geom &g = h->geo;
+    const long long plane_vals = (long long)g.nxr * g.ny * Q;
+    const size_t plane_bytes = sizeof(double) * (size_t)plane_vals;
+    int rc = ensure_import_ring(h);
+    if (rc) return rc;
+    const int P = h->imp_planes;
+    const ImportPlanes src{h->imp_ring, h->imp_ring + (long long)IMPORT_SLOTS * P * plane_vals, IMPORT_SLOTS * P,
+                           plane_vals};
+    cudaStream_t cs = h->side, ks = h->stream;
+    // internal plane z is reference plane z + 2
+    auto ref_plane = [&](int z) { return fn + (long long)(z + 2) * plane_vals; };
+    const int nch = (g.nzc + P - 1) / P;
+    // the copy stream starts after the main stream's earlier work (it may still read the ring)
+    CK(cudaEventRecord(h->imp_freed[0], ks));
+    CK(cudaStreamWaitEvent(cs, h->imp_freed[0], 0));
+    CK(cudaMemcpyAsync((double *)src.edge, ref_plane(g.nzc - 1), plane_bytes, cudaMemcpyHostToDevice, cs));
+    CK(cudaMemcpyAsync((double *)src.edge + plane_vals, ref_plane(0), plane_bytes, cudaMemcpyHostToDevice, cs));
+    auto convert = [&](int j) {
+        launch_import_lattice(g, h->p.storage, src, h->g[h->cur], h->mask2d, h->scale, w, j * P,
+                              std::min(g.nzc, (j + 1) * P), ks);
+        h->launches++;
+    };
+    for (int c = 0; c < nch; c++) {
+        const int slot = c % IMPORT_SLOTS;
+        // chunk c - IMPORT_SLOTS, in this slot, was last read by slab c - IMPORT_SLOTS + 1
+        if (c >= IMPORT_SLOTS) CK(cudaStreamWaitEvent(cs, h->imp_freed[slot], 0));
+        const int planes = std::min(P, g.nzc - c * P);
+        CK(cudaMemcpyAsync(h->imp_ring + (long long)slot * P * plane_vals, ref_plane(c * P), plane_bytes * planes,
+                           cudaMemcpyHostToDevice, cs));
+        CK(cudaEventRecord(h->imp_copied[slot], cs));
+        if (c >= 1) {
+            CK(cudaStreamWaitEvent(ks, h->imp_copied[slot], 0));
+            convert(c - 1);
+            CK_LAUNCH();
+            if (c >= 2) CK(cudaEventRecord(h->imp_freed[(c - 2) % IMPORT_SLOTS], ks));
+        }
+    }
+    CK(cudaStreamWaitEvent(ks, h->imp_copied[(nch - 1) % IMPORT_SLOTS], 0));
+    convert(nch - 1);
+    CK_LAUNCH();
+    CK(cudaStreamSynchronize(ks));
+    return RBC_OK;
+}
+
 int rbc_import_ref_lattice(rbc_handle *h, const double *fn)
 {
     if (!h || !fn) return RBC_ERR_ARG;
     RBC_DEVICE_GUARD(h);
-    const size_t bytes = sizeof(double) * Q * (size_t)h->nref_nodes;
-    int rc = ensure_staging(h, bytes);
-    if (rc) return rc;
-    CK(cudaMemcpyAsync(h->staging, fn, bytes, cudaMemcpyHostToDevice, h->stream));
-    launch_import_lattice(h->geo, h->p.storage, (const double *)h->staging, h->g[h->cur], h->mask2d, h->scale,
-                          wall_velocities(h, h->iter + 1), h->stream);
-    h->launches++;
-    CK_LAUNCH();
-    CK(cudaStreamSynchronize(h->stream));
-    return RBC_OK;
+    return import_lattice_pipelined(h, fn, wall_velocities(h, h->iter + 1));
 }
 
 int rbc_export_ref_lattice(rbc_handle *h, double *fn, double *dn, double *un, double *vn, double *wn)
@@ -1642,6 +1729,64 @@ int rbc_export_ref_force(rbc_handle *h, double *fx, double *fy, double *fz)
     return RBC_OK;
 }
 
+// Reference cell layouts <-> the handle's, converted on the device: the host
+// only copies the caller's arrays.  The metric conversion rounds each product,
+// the difference and each quotient separately, as the host expression
+// n00 * n11 - n01 * n01 with no contraction would (explicit _rn intrinsics: the
+// device compiler would otherwise fuse the products into a multiply-add).
+__global__ void import_metric_kernel(const double *__restrict__ nd, double4 *__restrict__ gref, long long ne)
+{
+    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= ne) return;
+    const double n00 = nd[4 * e], n01 = nd[4 * e + 1], n11 = nd[4 * e + 3];
+    const double det = __dsub_rn(__dmul_rn(n00, n11), __dmul_rn(n01, n01));
+    // G = n^-1, 1 / det G = det n
+    gref[e] = make_double4(__ddiv_rn(n11, det), __ddiv_rn(-n01, det), __ddiv_rn(n00, det), det);
+}
+
+// [n][3] (AoS, the reference's fem->xd and cel->gx) <-> [3][n] (the handle's)
+__global__ void aos3_to_soa_kernel(const double *__restrict__ in, double *__restrict__ out, long long n)
+{
+    const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    out[j] = in[3 * j]; out[n + j] = in[3 * j + 1]; out[2 * n + j] = in[3 * j + 2];
+}
+
+__global__ void soa3_to_aos_kernel(const double *__restrict__ in, double *__restrict__ out, long long n)
+{
+    const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    out[3 * j] = in[j]; out[3 * j + 1] = in[n + j]; out[3 * j + 2] = in[2 * n + j];
+}
+
+__global__ void f32_to_f64_kernel(const float *__restrict__ in, double *__restrict__ out, long long n)
+{
+    const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < n) out[j] = (double)in[j];
+}
+
+static unsigned blocks_for(long long n) { return (unsigned)((n + 255) / 256); }
+
+// load the layout kernels now (lazy module loading would load each in its first call)
+static cudaError_t cell_io_setup()
+{
+    cudaFuncAttributes fa;
+    cudaError_t e = cudaFuncGetAttributes(&fa, (const void *)import_metric_kernel);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, (const void *)aos3_to_soa_kernel);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, (const void *)soa3_to_aos_kernel);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, (const void *)f32_to_f64_kernel);
+    return e;
+}
+
+// staging of the cell imports ([nv][3] + [ne][4] + [N][3] doubles) and exports ([nv][3] + 6 [nv] + [N][3])
+static size_t cell_staging_bytes(const CellGroup &G)
+{
+    const size_t nv = (size_t)G.nv, ne = (size_t)G.ne, N = (size_t)G.ncell;
+    return sizeof(double) * (std::max(3 * nv + 4 * ne, 9 * nv) + 3 * N);
+}
+
+static int ensure_cell_staging(rbc_handle *h, const CellGroup &G) { return ensure_staging(h, cell_staging_bytes(G)); }
+
 static int import_cells(rbc_handle *h, CellGroup &G, const double *x, const double *y, const double *z,
                         const double *xd, const double *nd, const double *volume0, const double *gx)
 {
@@ -1650,29 +1795,38 @@ static int import_cells(rbc_handle *h, CellGroup &G, const double *x, const doub
     if (G.ncell == 0) return fail(h, RBC_ERR_STATE, "no cells in this population");
     const long long nv = G.nv, ne = G.ne;
     const int N = G.ncell;
-    CK(cudaStreamSynchronize(h->stream));
-    if (x) CK(cudaMemcpy(G.X, x, 8 * nv, cudaMemcpyHostToDevice));
-    if (y) CK(cudaMemcpy(G.X + nv, y, 8 * nv, cudaMemcpyHostToDevice));
-    if (z) CK(cudaMemcpy(G.X + 2 * nv, z, 8 * nv, cudaMemcpyHostToDevice));
+    cudaStream_t s = h->stream;
+    CK(cudaStreamSynchronize(s));
+    // staging: xd [nv][3], nd [ne][4], gx [N][3]
+    const size_t o_nd = 3 * (size_t)nv, o_gx = o_nd + 4 * (size_t)ne;
+    if (xd || nd || gx) {
+        const int rc = ensure_cell_staging(h, G);
+        if (rc) return rc;
+    }
+    double *st = (double *)h->staging;
+    if (x) CK(cudaMemcpyAsync(G.X, x, 8 * nv, cudaMemcpyHostToDevice, s));
+    if (y) CK(cudaMemcpyAsync(G.X + nv, y, 8 * nv, cudaMemcpyHostToDevice, s));
+    if (z) CK(cudaMemcpyAsync(G.X + 2 * nv, z, 8 * nv, cudaMemcpyHostToDevice, s));
     if (xd) {
-        std::vector<double> t(3 * nv);
-        for (long long j = 0; j < nv; j++) for (int k = 0; k < 3; k++) t[k * nv + j] = xd[3 * j + k];
-        CK(cudaMemcpy(G.Xd, t.data(), 8 * 3 * nv, cudaMemcpyHostToDevice));
+        CK(cudaMemcpyAsync(st, xd, 8 * 3 * nv, cudaMemcpyHostToDevice, s));
+        aos3_to_soa_kernel<<<blocks_for(nv), 256, 0, s>>>(st, G.Xd, nv);
+        h->launches++;
+        CK_LAUNCH();
     }
     if (nd) {
-        std::vector<double4> gm(ne);
-        for (long long e = 0; e < ne; e++) {
-            const double n00 = nd[4 * e], n01 = nd[4 * e + 1], n11 = nd[4 * e + 3], det = n00 * n11 - n01 * n01;
-            gm[e] = make_double4(n11 / det, -n01 / det, n00 / det, det);   // G = n^-1, 1 / det G = det n
-        }
-        CK(cudaMemcpy(G.gref, gm.data(), sizeof(double4) * ne, cudaMemcpyHostToDevice));
+        CK(cudaMemcpyAsync(st + o_nd, nd, 8 * 4 * ne, cudaMemcpyHostToDevice, s));
+        import_metric_kernel<<<blocks_for(ne), 256, 0, s>>>(st + o_nd, G.gref, ne);
+        h->launches++;
+        CK_LAUNCH();
     }
-    if (volume0) CK(cudaMemcpy(G.vol0, volume0, 8 * N, cudaMemcpyHostToDevice));
+    if (volume0) CK(cudaMemcpyAsync(G.vol0, volume0, 8 * N, cudaMemcpyHostToDevice, s));
     if (gx) {
-        std::vector<double> t(3 * N);
-        for (int c = 0; c < N; c++) for (int k = 0; k < 3; k++) t[k * N + c] = gx[3 * c + k];
-        CK(cudaMemcpy(G.gx, t.data(), 8 * 3 * N, cudaMemcpyHostToDevice));
+        CK(cudaMemcpyAsync(st + o_gx, gx, 8 * 3 * N, cudaMemcpyHostToDevice, s));
+        aos3_to_soa_kernel<<<blocks_for(N), 256, 0, s>>>(st + o_gx, G.gx, N);
+        h->launches++;
+        CK_LAUNCH();
     }
+    CK(cudaStreamSynchronize(s));
     return RBC_OK;
 }
 
@@ -1704,28 +1858,45 @@ static int export_cells(rbc_handle *h, CellGroup &G, double *x, double *y, doubl
     if (G.ncell == 0) return fail(h, RBC_ERR_STATE, "no cells in this population");
     const long long nv = G.nv;
     const int N = G.ncell;
-    CK(cudaStreamSynchronize(h->stream));
-    if (x) CK(cudaMemcpy(x, G.X, 8 * nv, cudaMemcpyDeviceToHost));
-    if (y) CK(cudaMemcpy(y, G.X + nv, 8 * nv, cudaMemcpyDeviceToHost));
-    if (z) CK(cudaMemcpy(z, G.X + 2 * nv, 8 * nv, cudaMemcpyDeviceToHost));
-    if (xd) {
-        std::vector<double> t(3 * nv);
-        CK(cudaMemcpy(t.data(), G.Xd, 8 * 3 * nv, cudaMemcpyDeviceToHost));
-        for (long long j = 0; j < nv; j++) for (int k = 0; k < 3; k++) xd[3 * j + k] = t[k * nv + j];
+    cudaStream_t s = h->stream;
+    CK(cudaStreamSynchronize(s));
+    double *outs[6] = {u, v, w, fx, fy, fz};
+    const bool vel = u || v || w, frc = fx || fy || fz;
+    // staging: xd [nv][3], u v w [3][nv], fx fy fz [3][nv], gx [N][3]
+    const size_t o_u = 3 * (size_t)nv, o_f = o_u + 3 * (size_t)nv, o_gx = o_f + 3 * (size_t)nv;
+    if (xd || vel || frc || gxo) {
+        const int rc = ensure_cell_staging(h, G);
+        if (rc) return rc;
     }
-    if (u || v || w || fx || fy || fz) {
-        std::vector<float> t(6 * nv);
-        CK(cudaMemcpy(t.data(), G.U, 4 * 3 * nv, cudaMemcpyDeviceToHost));
-        CK(cudaMemcpy(t.data() + 3 * nv, G.Fv, 4 * 3 * nv, cudaMemcpyDeviceToHost));
-        double *outs[6] = {u, v, w, fx, fy, fz};
-        for (int k = 0; k < 6; k++)
-            if (outs[k]) for (long long j = 0; j < nv; j++) outs[k][j] = t[k * nv + j];
+    double *st = (double *)h->staging;
+    if (xd) {
+        soa3_to_aos_kernel<<<blocks_for(nv), 256, 0, s>>>(G.Xd, st, nv);
+        h->launches++;
+        CK_LAUNCH();
+    }
+    if (vel) {
+        f32_to_f64_kernel<<<blocks_for(3 * nv), 256, 0, s>>>(G.U, st + o_u, 3 * nv);
+        h->launches++;
+        CK_LAUNCH();
+    }
+    if (frc) {
+        f32_to_f64_kernel<<<blocks_for(3 * nv), 256, 0, s>>>(G.Fv, st + o_f, 3 * nv);
+        h->launches++;
+        CK_LAUNCH();
     }
     if (gxo) {
-        std::vector<double> t(3 * N);
-        CK(cudaMemcpy(t.data(), G.gx, 8 * 3 * N, cudaMemcpyDeviceToHost));
-        for (int c = 0; c < N; c++) for (int k = 0; k < 3; k++) gxo[3 * c + k] = t[k * N + c];
+        soa3_to_aos_kernel<<<blocks_for(N), 256, 0, s>>>(G.gx, st + o_gx, N);
+        h->launches++;
+        CK_LAUNCH();
     }
+    if (x) CK(cudaMemcpyAsync(x, G.X, 8 * nv, cudaMemcpyDeviceToHost, s));
+    if (y) CK(cudaMemcpyAsync(y, G.X + nv, 8 * nv, cudaMemcpyDeviceToHost, s));
+    if (z) CK(cudaMemcpyAsync(z, G.X + 2 * nv, 8 * nv, cudaMemcpyDeviceToHost, s));
+    if (xd) CK(cudaMemcpyAsync(xd, st, 8 * 3 * nv, cudaMemcpyDeviceToHost, s));
+    for (int k = 0; k < 6; k++)
+        if (outs[k]) CK(cudaMemcpyAsync(outs[k], st + o_u + (size_t)k * nv, 8 * nv, cudaMemcpyDeviceToHost, s));
+    if (gxo) CK(cudaMemcpyAsync(gxo, st + o_gx, 8 * 3 * N, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
     return RBC_OK;
 }
 

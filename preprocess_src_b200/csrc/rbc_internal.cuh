@@ -177,8 +177,14 @@ enum { LBM_ACC_WRITE = 0, LBM_ACC_ADD = 1, LBM_ACC_AVERAGE = 2 };
 void launch_lbm(const Geom &g, int storage, const LbmArgs &a, cudaStream_t s);
 // z velocities of the top and bottom walls in the next step (shear mode; 0 otherwise)
 struct WallVel { double top, bot, Cr; };
-void launch_import_lattice(const Geom &g, int storage, const double *fn_ref, void *gout,
-                           const uint32_t *mask2d, float scale, const WallVel &w, cudaStream_t s);
+// Reference planes an import reads: internal planes 0 .. nzc-1 in a ring of
+// ring_planes planes (plane z at z % ring_planes), and the two periodic images
+// (edge: plane nzc - 1, then plane 0), each plane_vals = nxr * ny * 19 doubles
+struct ImportPlanes { const double *ring, *edge; int ring_planes; long long plane_vals; };
+cudaError_t lattice_io_setup();   // loads the import / export kernels
+// Reference fn -> internal g* for internal planes [z0, z1)
+void launch_import_lattice(const Geom &g, int storage, const ImportPlanes &src, void *gout, const uint32_t *mask2d,
+                           float scale, const WallVel &w, int z0, int z1, cudaStream_t s);
 void launch_export_lattice(const Geom &g, int storage, const void *gin, const uint32_t *mask2d,
                            const float4 *uvr, float inv_scale, double *fn_ref, double *dn, double *un,
                            double *vn, double *wn, const WallVel &w, cudaStream_t s);
