@@ -279,25 +279,38 @@ spread_body(const Geom &g, const double *__restrict__ X, long long nv, int V,
     if (!use_box) return;
     __syncthreads();
     const int rowplane = bx * by;
-    for (int li = tid; li < nbi; li += SPREAD_THREADS) {
-        const int lz = li / psi, r = li - lz * psi;
-        if (r >= rowplane) continue;   // plane padding
-        const int ia = (int)sbox[li], ib = (int)sbox[nbi + li], ic = (int)sbox[2 * nbi + li];
-        if ((ia | ib | ic) == 0) continue;
+    // one item = one box column (x, y) and ZC consecutive planes: the column's lattice
+    // position and wall test once per item, the planes' box reads independent of each other
+    constexpr int ZC = 2;
+    const int items = rowplane * ((bz + ZC - 1) / ZC);
+    for (int it = tid; it < items; it += SPREAD_THREADS) {
+        const int zc = it / rowplane, r = it - zc * rowplane;
         const int ly = r / bx, lx = r - ly * bx;
         const int gx = XPER ? wrap_x(bx0 + lx, g.nx) : bx0 + lx, gy = by0 + ly;
         if (gx < 0 || gx >= g.nx || gy < 0 || gy >= g.ny) continue;   // never written; kept as a guard
         if (!(__ldg(&mask2d[gx + g.nx * gy]) & MASK_FLUID)) continue;   // wall column: the LBM never reads it
-        const int zw = wrap_z(bz0 + lz, g.nzc);
-        const long long xy = gx + (long long)g.nx * gy, gi = (long long)zw * g.plane + xy;
-        long long fa = 0, fb = 0, fc = 0;
-        const bool ok = box_to_fixed(ia, FORCE_FRAC - qe[0], fa) & box_to_fixed(ib, FORCE_FRAC - qe[1], fb) &
-                        box_to_fixed(ic, FORCE_FRAC - qe[2], fc);
-        if (!ok) atomicOr(flags, RBC_FLAG_NONFINITE);
-        if (fa) atomicAdd(reinterpret_cast<unsigned long long *>(&F.F[gi]), (unsigned long long)fa);
-        if (fb) atomicAdd(reinterpret_cast<unsigned long long *>(&F.F[g.nint + gi]), (unsigned long long)fb);
-        if (fc) atomicAdd(reinterpret_cast<unsigned long long *>(&F.F[2 * g.nint + gi]), (unsigned long long)fc);
-        if (fa | fb | fc) atomicOr(&F.bits[(long long)zw * F.wpp + (xy >> 5)], 1u << (xy & 31));
+        const long long xy = gx + (long long)g.nx * gy;
+#pragma unroll
+        for (int u = 0; u < ZC; u++) {
+            const int lz = zc * ZC + u;
+            if (lz >= bz) break;
+            const int li = lz * psi + r;
+            const int ia = (int)sbox[li], ib = (int)sbox[nbi + li], ic = (int)sbox[2 * nbi + li];
+            if ((ia | ib | ic) == 0) continue;
+            int zw = bz0 + lz;   // the box spans less than a period: one correction, the modulo as a fallback
+            if (zw < 0) zw += g.nzc;
+            if (zw >= g.nzc) zw -= g.nzc;
+            if ((unsigned)zw >= (unsigned)g.nzc) zw = wrap_z(zw, g.nzc);
+            const long long gi = (long long)zw * g.plane + xy;
+            long long fa = 0, fb = 0, fc = 0;
+            const bool ok = box_to_fixed(ia, FORCE_FRAC - qe[0], fa) & box_to_fixed(ib, FORCE_FRAC - qe[1], fb) &
+                            box_to_fixed(ic, FORCE_FRAC - qe[2], fc);
+            if (!ok) atomicOr(flags, RBC_FLAG_NONFINITE);
+            if (fa) atomicAdd(reinterpret_cast<unsigned long long *>(&F.F[gi]), (unsigned long long)fa);
+            if (fb) atomicAdd(reinterpret_cast<unsigned long long *>(&F.F[g.nint + gi]), (unsigned long long)fb);
+            if (fc) atomicAdd(reinterpret_cast<unsigned long long *>(&F.F[2 * g.nint + gi]), (unsigned long long)fc);
+            if (fa | fb | fc) atomicOr(&F.bits[(long long)zw * F.wpp + (xy >> 5)], 1u << (xy & 31));
+        }
     }
 }
 
@@ -480,21 +493,28 @@ advect_body(const Geom &g, double *__restrict__ X, double *__restrict__ Xd, floa
         const int nb = bxs * bys * bzs;
         int x = tid % bxs, y = (tid / bxs) % bys, z = tid / (bxs * bys);
         const int sx = ADVECT_THREADS % bxs, sy = (ADVECT_THREADS / bxs) % bys, sz = ADVECT_THREADS / (bxs * bys);
-        // four nodes per thread and round: their loads are issued before any store
-        for (int li = tid; li < nb; li += 4 * ADVECT_THREADS) {
-            float4 q[4];
+        // eight nodes per thread and round, their loads issued before any store: a mean box of
+        // ~2000 nodes is one round, one wait on the L2 instead of two
+        constexpr int UF = 8;
+        for (int li = tid; li < nb; li += UF * ADVECT_THREADS) {
+            float4 q[UF];
 #pragma unroll
-            for (int u = 0; u < 4; u++) {
+            for (int u = 0; u < UF; u++) {
                 const int gx = XPER ? wrap_x(bx0 + x, g.nx) : bx0 + x, gy = by0 + y;
+                // the box spans less than a period: one correction, the modulo only as a fallback
+                int gz = bz0 + z;
+                if (gz < 0) gz += g.nzc;
+                if (gz >= g.nzc) gz -= g.nzc;
+                if ((unsigned)gz >= (unsigned)g.nzc) gz = wrap_z(gz, g.nzc);
                 q[u] = make_float4(0.f, 0.f, 0.f, 0.f);
                 if (li + u * ADVECT_THREADS < nb && gx >= 0 && gx < g.nx && gy >= 0 && gy < g.ny)
-                    q[u] = __ldg(&uvr[(long long)wrap_z(bz0 + z, g.nzc) * g.plane + gx + (long long)g.nx * gy]);
+                    q[u] = __ldg(&uvr[(long long)gz * g.plane + gx + (long long)g.nx * gy]);
                 x += sx; y += sy; z += sz;
                 if (x >= bxs) { x -= bxs; y++; }
                 if (y >= bys) { y -= bys; z++; }
             }
 #pragma unroll
-            for (int u = 0; u < 4; u++)
+            for (int u = 0; u < UF; u++)
                 if (li + u * ADVECT_THREADS < nb) abox[li + u * ADVECT_THREADS] = q[u];
         }
     }
