@@ -96,7 +96,7 @@ spread_body(const Geom &g, const double *__restrict__ X, long long nv, int V,
             const float *__restrict__ Fv, const ForceField &F, const uint32_t *__restrict__ mask2d,
             int *__restrict__ flags, int bid)
 {
-    extern __shared__ unsigned sbox[];
+    extern __shared__ __align__(16) unsigned sbox[];
     // each patch vertex's lattice cell, unwrap shifts and fractions, from the bounds pass
     __shared__ int4 s_cell[MAX_PATCH_VERTICES];      // floor(lx), floor(ly), floor(lz), z unwrap shift
     __shared__ float4 s_frac[MAX_PATCH_VERTICES];    // lx - floor(lx), ly - floor(ly), lz - floor(lz), x shift
@@ -117,6 +117,7 @@ spread_body(const Geom &g, const double *__restrict__ X, long long nv, int V,
     int lo0 = INT_MAX, lo1 = INT_MAX, lo2 = INT_MAX, hi0 = INT_MIN, hi1 = INT_MIN, hi2 = INT_MIN;
     float fmax0 = 0.f, fmax1 = 0.f, fmax2 = 0.f;
     bool nonfinite = false;
+#pragma unroll 2
     for (int k = tid; k < np; k += blockDim.x) {
         const int v = patch_vtx[p0 + k];
         const float afx = fabsf(fxs[v]), afy = fabsf(fys[v]), afz = fabsf(fzs[v]);
@@ -177,7 +178,7 @@ spread_body(const Geom &g, const double *__restrict__ X, long long nv, int V,
         // nodes (x, y) of its stencil in its base plane; a walk down each
         // column then applies 4 k along z with a sliding window.
         unsigned *cnt = sbox + 2 * nbi;
-        for (int i = tid; i < nbi; i += SPREAD_THREADS) cnt[i] = 0u;
+        for (int i = tid; i < nbi / 4; i += SPREAD_THREADS) reinterpret_cast<uint4 *>(cnt)[i] = make_uint4(0u, 0u, 0u, 0u);
         __syncthreads();
         for (int k = tid; k < np; k += SPREAD_THREADS) {
             const int4 cl = s_cell[k];
@@ -209,7 +210,7 @@ spread_body(const Geom &g, const double *__restrict__ X, long long nv, int V,
             qs[k] = exp2f(e);
             qe[k] = (int)e;
         }
-        for (int i = tid; i < 3 * nbi; i += blockDim.x) sbox[i] = 0u;
+        for (int i = tid; i < 3 * nbi / 4; i += blockDim.x) reinterpret_cast<uint4 *>(sbox)[i] = make_uint4(0u, 0u, 0u, 0u);
         __syncthreads();
     }
     // Four tasks per vertex: task i handles stencil plane c = i & 3 of the
