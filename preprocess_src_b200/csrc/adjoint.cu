@@ -680,16 +680,15 @@ volume_adjoint_kernel(const Geom g, const VolumeAdjArgs a)
         const int ia = __ldg(&a.tri[3 * e]), ib = __ldg(&a.tri[3 * e + 1]), ic = __ldg(&a.tri[3 * e + 2]);
         for (int c = 0; c < 3; c++) { A[c] = P[c * V + ia]; B[c] = P[c * V + ib]; Cc[c] = P[c * V + ic]; }
     };
-    auto vol_area = [&](const double *P, double &vol, double &area) {
+    auto vol_area = [&](const double *P, double &vol, double &area) {   // as volume.cu measures them
         double sv = 0.0, sa = 0.0;
         for (int e = tid; e < E; e += T) {
-            double A[3], B[3], Cc[3], n[3], dS, vt;
+            double A[3], B[3], Cc[3];
             tri_at(P, e, A, B, Cc);
-            tri_geom<double>(A, B, Cc, n, dS, vt);
-            sv += vt; sa += dS;
+            tri_measure(A, B, Cc, sv, sa);
         }
-        vol = block_sum_r(sv, red);
-        area = block_sum_r(sa, red);
+        vol = block_sum_r(sv, red) / 18.0;
+        area = block_sum_r(sa, red) / 2.0;
     };
     auto mean_normal = [&](const double *P, int v, double (&nn)[3]) {
         const int k0 = __ldg(&a.v2e_off[v]), k1 = __ldg(&a.v2e_off[v + 1]), nne = k1 - k0;

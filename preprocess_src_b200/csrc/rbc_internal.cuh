@@ -333,6 +333,21 @@ struct BendArgs {
 void launch_bend(const BendArgs &a, cudaStream_t s);
 void launch_membrane(const MembraneArgs &a, bool fp64, cudaStream_t s);
 
+// 18 x the volume contribution and 2 x the area of triangle (a, b, c): with
+// c = (b - a) x (c - a), (a + b + c) . c and |c|.  This is the normal form of
+// CalcEleNormal_GPU / CalcVolume (volume_correction.cu:138-200, 246-281:
+// (r . n) dS / 3 with r the centroid, n = c / |c|, dS = |c| / 2) without its
+// divisions; the volume correction and its adjoint's replay both use it.
+__device__ __forceinline__ void tri_measure(const double (&A)[3], const double (&B)[3], const double (&C)[3],
+                                            double &s18v, double &s2a)
+{
+    const double v1x = B[0] - A[0], v1y = B[1] - A[1], v1z = B[2] - A[2];
+    const double v2x = C[0] - A[0], v2y = C[1] - A[1], v2z = C[2] - A[2];
+    const double c0 = v1y * v2z - v1z * v2y, c1 = v1z * v2x - v1x * v2z, c2 = v1x * v2y - v1y * v2x;
+    s2a += sqrt(c0 * c0 + c1 * c1 + c2 * c2);
+    s18v += (A[0] + B[0] + C[0]) * c0 + (A[1] + B[1] + C[1]) * c1 + (A[2] + B[2] + C[2]) * c2;
+}
+
 struct VolumeArgs {
     double *X; long long nv;
     const int *tri, *v2e_off, *v2e;

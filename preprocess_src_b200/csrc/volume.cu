@@ -23,16 +23,36 @@ constexpr int VC_ITRMAX = 1000;            // volume_correction.cu:487
 
 int volume_smem_bytes(int V) { return 24 * V; }
 
-__device__ __forceinline__ double block_sum_d(double v, double *red) {
+// block sums of K values at once: per value a warp butterfly, then the warps' sums in warp order
+template <int K>
+__device__ __forceinline__ void block_sum_k(double (&v)[K], double *red) {
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+        for (int k = 0; k < K; k++) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
     __syncthreads();
-    if (lane == 0) red[wid] = v;
+    if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < K; k++) red[32 * k + wid] = v[k];
     __syncthreads();
-    double s = 0.0;
-    for (int k = 0; k < nw; k++) s += red[k];
-    return s;
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+        double s = 0.0;
+        for (int w = 0; w < nw; w++) s += red[32 * k + w];
+        v[k] = s;
+    }
+}
+
+// tri_measure of local element e
+__device__ __forceinline__ void ele_measure(const double *__restrict__ p, int V, const int *__restrict__ tri, int e,
+                                            double &s18v, double &s2a)
+{
+    const int na = __ldg(&tri[3 * e]), nb = __ldg(&tri[3 * e + 1]), nc = __ldg(&tri[3 * e + 2]);
+    const double A[3] = {p[na], p[V + na], p[2 * V + na]};
+    const double B[3] = {p[nb], p[V + nb], p[2 * V + nb]};
+    const double C[3] = {p[nc], p[V + nc], p[2 * V + nc]};
+    tri_measure(A, B, C, s18v, s2a);
 }
 
 // unit normal, area and volume contribution of local element e (CalcEleNormal_GPU)
@@ -57,7 +77,7 @@ __device__ __forceinline__ void ele_normal(const double *__restrict__ p, int V, 
 __device__ __forceinline__ void volume_body(const Geom &g, const VolumeArgs &a, int cell)
 {
     extern __shared__ __align__(16) unsigned char smem[];
-    __shared__ double red[32];
+    __shared__ double red[3 * 32];
     double *p = reinterpret_cast<double *>(smem);   // [3][V]
     const int V = a.V, E = a.E, tid = threadIdx.x, T = blockDim.x, N = a.ncell;
     const long long vb = (long long)cell * V, nv = a.nv;
@@ -81,14 +101,11 @@ __device__ __forceinline__ void volume_body(const Geom &g, const VolumeArgs &a, 
     double vol = 0.0, area = 0.0;
     int it = 0;
     for (;;) {
-        double sv = 0.0, sa = 0.0;
-        for (int e = tid; e < E; e += T) {
-            double n[3], dS, vt;
-            ele_normal(p, V, a.tri, e, n, dS, vt);
-            sv += vt; sa += dS;
-        }
-        vol = block_sum_d(sv, red);
-        area = block_sum_d(sa, red);
+        double s[2] = {0.0, 0.0};
+        for (int e = tid; e < E; e += T) ele_measure(p, V, a.tri, e, s[0], s[1]);
+        block_sum_k<2>(s, red);
+        vol = s[0] / 18.0;
+        area = s[1] / 2.0;
         if (!a.correct) break;
         it++;
         if (fabs(vol - V0) / V0 * 100.0 < VC_EPS) break;
@@ -119,12 +136,22 @@ __device__ __forceinline__ void volume_body(const Geom &g, const VolumeArgs &a, 
         __syncthreads();
         if (it >= VC_ITRMAX) { if (tid == 0) atomicOr(a.flags, RBC_FLAG_VC_NOT_CONVERGED); break; }
     }
-    // CalcCenter: vertex mean, wrapped into [zmin, zmax]
-    double sx = 0.0, sy = 0.0, sz = 0.0;
-    for (int v = tid; v < V; v += T) { sx += p[v]; sy += p[V + v]; sz += p[2 * V + v]; }
-    sx = block_sum_d(sx, red) / (double)V;
-    sy = block_sum_d(sy, red) / (double)V;
-    sz = block_sum_d(sz, red) / (double)V;
+    // CalcCenter: vertex mean, wrapped into [zmin, zmax]; with a correction, the same pass
+    // stores the positions (CapsulePeriodicAfter)
+    double sc[3] = {0.0, 0.0, 0.0};
+    for (int v = tid; v < V; v += T) {
+        double x = p[v], z = p[2 * V + v];
+        sc[0] += x; sc[1] += p[V + v]; sc[2] += z;
+        if (a.correct) {
+            if (z < g.zmin) z += g.LZ; else if (z > g.zmax) z -= g.LZ;
+            if (g.xper) { if (x < g.xmin) x += g.LX; else if (x > g.xmax) x -= g.LX; }   // volume_correction.cu:88-91
+            a.X[vb + v] = x;
+            a.X[nv + vb + v] = p[V + v];
+            a.X[2 * nv + vb + v] = z;
+        }
+    }
+    block_sum_k<3>(sc, red);
+    double sx = sc[0] / (double)V, sy = sc[1] / (double)V, sz = sc[2] / (double)V;
     if (sz < g.zmin) sz += g.LZ; else if (sz > g.zmax) sz -= g.LZ;
     if (g.xper) { if (sx < g.xmin) sx += g.LX; else if (sx > g.xmax) sx -= g.LX; }   // volume_correction.cu:319-325
     if (tid == 0) {
@@ -133,16 +160,6 @@ __device__ __forceinline__ void volume_body(const Geom &g, const VolumeArgs &a, 
         double *cen = a.correct ? a.gx : a.cen_out;
         if (cen) { cen[cell] = sx; cen[N + cell] = sy; cen[2 * N + cell] = sz; }
         if (a.correct) { atomicMax(a.vc_max, it - 1); atomicMax(a.vc_last, it - 1); }
-    }
-    if (!a.correct) return;
-    // CapsulePeriodicAfter, then store
-    for (int v = tid; v < V; v += T) {
-        double z = p[2 * V + v], x = p[v];
-        if (z < g.zmin) z += g.LZ; else if (z > g.zmax) z -= g.LZ;
-        if (g.xper) { if (x < g.xmin) x += g.LX; else if (x > g.xmax) x -= g.LX; }   // volume_correction.cu:88-91
-        a.X[vb + v] = x;
-        a.X[nv + vb + v] = p[V + v];
-        a.X[2 * nv + vb + v] = z;
     }
 }
 
