@@ -419,11 +419,11 @@ constexpr int ADVECT_SMEM = ADVECT_BOX_BYTES + ADVECT_MAX_PATCH * (3 * (int)size
 // Stage-1 stencil plane of one lane from the patch's shared-memory box; false
 // when the plane is not inside the box (the caller then gathers from global
 // memory).  (xi, yi, zi) = stencil corner relative to the box origin.
-__device__ __forceinline__ bool box_plane(const float4 *box, int bxs, int bys, int bzs, int xi, int yi, int zi,
-                                          bool zin, unsigned xm, Plane16 &P)
+__device__ __forceinline__ bool box_plane(const float4 *box, int bxs, int bys, int bzs, int bps, int xi, int yi,
+                                          int zi, bool zin, unsigned xm, Plane16 &P)
 {
     if (xi < 0 || xi + 3 >= bxs || yi < 0 || yi + 3 >= bys || zi < 0 || zi >= bzs) return false;
-    const float4 *row = box + ((long long)zi * bys + yi) * bxs + xi;
+    const float4 *row = box + zi * bps + yi * bxs + xi;
 #pragma unroll
     for (int b = 0; b < 4; b++)
 #pragma unroll
@@ -487,10 +487,15 @@ advect_body(const Geom &g, double *__restrict__ X, double *__restrict__ Xd, floa
     }
     const int bx0 = s_lo[0], by0 = s_lo[1], bz0 = s_lo[2];
     const long long bxl = (long long)s_hi[0] - bx0 + 1, byl = (long long)s_hi[1] - by0 + 1, bzl = (long long)s_hi[2] - bz0 + 1;
-    const bool use_box = np > 0 && bxl >= 6 && byl >= 6 && bzl >= 6 && bxl * byl * bzl <= ADVECT_BOX_CAP;
+    // plane stride bps = bxs * bys rounded up to odd: the four planes of a vertex's stencil, read
+    // by four lanes of one quarter-warp, then fall in four different 16-byte bank groups
+    const long long bpl = (bxl * byl) | 1;
+    const bool use_box = np > 0 && bxl >= 6 && byl >= 6 && bzl >= 6 && bpl * bzl <= ADVECT_BOX_CAP;
     const int bxs = use_box ? (int)bxl : 0, bys = use_box ? (int)byl : 0, bzs = use_box ? (int)bzl : 0;
+    const int bps = use_box ? (int)bpl : 0;
     if (use_box) {
-        // node li = (z * bys + y) * bxs + x; each thread steps li by ADVECT_THREADS
+        // node li = (z * bys + y) * bxs + x, stored at z * bps + y * bxs + x; each thread steps li
+        // by ADVECT_THREADS
         const int nb = bxs * bys * bzs;
         int x = tid % bxs, y = (tid / bxs) % bys, z = tid / (bxs * bys);
         const int sx = ADVECT_THREADS % bxs, sy = (ADVECT_THREADS / bxs) % bys, sz = ADVECT_THREADS / (bxs * bys);
@@ -499,8 +504,10 @@ advect_body(const Geom &g, double *__restrict__ X, double *__restrict__ Xd, floa
         constexpr int UF = 8;
         for (int li = tid; li < nb; li += UF * ADVECT_THREADS) {
             float4 q[UF];
+            int si[UF];
 #pragma unroll
             for (int u = 0; u < UF; u++) {
+                si[u] = z * bps + y * bxs + x;
                 const int gx = XPER ? wrap_x(bx0 + x, g.nx) : bx0 + x, gy = by0 + y;
                 // the box spans less than a period: one correction, the modulo only as a fallback
                 int gz = bz0 + z;
@@ -516,7 +523,7 @@ advect_body(const Geom &g, double *__restrict__ X, double *__restrict__ Xd, floa
             }
 #pragma unroll
             for (int u = 0; u < UF; u++)
-                if (li + u * ADVECT_THREADS < nb) abox[li + u * ADVECT_THREADS] = q[u];
+                if (li + u * ADVECT_THREADS < nb) abox[si[u]] = q[u];
         }
     }
     __syncthreads();
@@ -549,7 +556,7 @@ advect_body(const Geom &g, double *__restrict__ X, double *__restrict__ Xd, floa
 #pragma unroll
                 for (int a = 0; a < 4; a++) xm |= (cx + a >= -g.xb && cx + a < g.nx + g.xb) ? (1u << a) : 0u;
             }
-            if (!use_box || !box_plane(abox, bxs, bys, bzs, cx + xsh - bx0, cy - by0, izr + zsh - bz0, zin, xm, P))
+            if (!use_box || !box_plane(abox, bxs, bys, bzs, bps, cx + xsh - bx0, cy - by0, izr + zsh - bz0, zin, xm, P))
                 gather_plane(g, uvr, cx, cy, izr, xm, P);
         };
         fetch(bx, by, bz);
