@@ -165,7 +165,12 @@ const char *rbc_last_error(const rbc_handle *h);
 /* ---- state in and out, reference layouts (synchronous) ---------------- */
 
 /* fn[nx*ny*nz*19]: pre-collision populations as lbm_d3q19 leaves them in
- * ltc->fnD (lbm.cu:1575).  Only COMP nodes are read. */
+ * ltc->fnD (lbm.cu:1575).  Only COMP nodes are read.  The lattice crosses to
+ * the device in chunks of about 16 MB through a ring of four slots while the
+ * chunks already there are converted, so the call takes about the time of the
+ * host-to-device copy (fastest from pinned host memory).  The ring (four
+ * chunks and two planes) is allocated by rbc_create for lattices of more than
+ * four chunks, else by the first import. */
 int rbc_import_ref_lattice(rbc_handle *h, const double *fn);
 /* Any pointer may be NULL.  fn: populations on COMP nodes, 0 elsewhere.
  * dn/un/vn/wn [nx*ny*nz]: density and velocity of the last lbm step with the
@@ -180,7 +185,9 @@ int rbc_export_ref_lattice(rbc_handle *h, double *fn, double *dn, double *un, do
  * rbc_lbm_d3q19 (COMP nodes, folded as ibm.cu:214-296 leaves them). */
 int rbc_export_ref_force(rbc_handle *h, double *fx, double *fy, double *fz);
 /* Any pointer may be NULL.  x,y,z [nv]: cel->x/y/z; xd [3*nv]: fem->xd;
- * nd [4*ne]: fem->nd; volume0 [ncell]; gx [3*ncell]: cel->gx. */
+ * nd [4*ne]: fem->nd; volume0 [ncell]; gx [3*ncell]: cel->gx.  The layout
+ * conversions (xd and gx to [3][n], nd to the covariant metric) run on the
+ * device after plain copies, through a staging buffer rbc_create allocates. */
 int rbc_import_ref_cells(rbc_handle *h, const double *x, const double *y, const double *z,
                          const double *xd, const double *nd, const double *volume0, const double *gx);
 /* Vertex forces cel->fx/fy/fz [nv] as stress() leaves them, for running
