@@ -82,18 +82,27 @@ __device__ __forceinline__ void volume_body(const Geom &g, const VolumeArgs &a, 
     const int V = a.V, E = a.E, tid = threadIdx.x, T = blockDim.x, N = a.ncell;
     const long long vb = (long long)cell * V, nv = a.nv;
     const double gz = a.gx[2 * N + cell], gxx = a.gx[cell];
-    for (int v = tid; v < V; v += T) {
-        double x = a.X[vb + v];
-        if (g.xper) {                                       // CapsulePeriodicBefore, x (shear mode)
-            const double dxx = x - gxx;
-            if (dxx > g.LX * 0.5) x -= g.LX; else if (dxx < -g.LX * 0.5) x += g.LX;
+    // up to four vertices per thread and round, their loads issued before any store
+    for (int v0 = tid; v0 < V; v0 += 4 * T) {
+        double q[4][3];
+#pragma unroll
+        for (int m = 0; m < 4; m++) {
+            const int v = v0 + m * T;
+            if (v < V) { q[m][0] = a.X[vb + v]; q[m][1] = a.X[nv + vb + v]; q[m][2] = a.X[2 * nv + vb + v]; }
         }
-        p[v] = x;
-        p[V + v] = a.X[nv + vb + v];
-        double z = a.X[2 * nv + vb + v];
-        const double dz = z - gz;                           // CapsulePeriodicBefore, z
-        if (dz > g.LZ * 0.5) z -= g.LZ; else if (dz < -g.LZ * 0.5) z += g.LZ;
-        p[2 * V + v] = z;
+#pragma unroll
+        for (int m = 0; m < 4; m++) {
+            const int v = v0 + m * T;
+            if (v >= V) break;
+            double x = q[m][0], z = q[m][2];
+            if (g.xper) {                                   // CapsulePeriodicBefore, x (shear mode)
+                const double dxx = x - gxx;
+                if (dxx > g.LX * 0.5) x -= g.LX; else if (dxx < -g.LX * 0.5) x += g.LX;
+            }
+            const double dz = z - gz;                       // CapsulePeriodicBefore, z
+            if (dz > g.LZ * 0.5) z -= g.LZ; else if (dz < -g.LZ * 0.5) z += g.LZ;
+            p[v] = x; p[V + v] = q[m][1]; p[2 * V + v] = z;
+        }
     }
     __syncthreads();
 
@@ -102,6 +111,7 @@ __device__ __forceinline__ void volume_body(const Geom &g, const VolumeArgs &a, 
     int it = 0;
     for (;;) {
         double s[2] = {0.0, 0.0};
+#pragma unroll 2
         for (int e = tid; e < E; e += T) ele_measure(p, V, a.tri, e, s[0], s[1]);
         block_sum_k<2>(s, red);
         vol = s[0] / 18.0;
